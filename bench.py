@@ -1,0 +1,307 @@
+"""Zone-updates/s of the GAMERA step on B200.
+
+Workload: the 3D MHD blast wave on the warped non-orthogonal grid -- 256^3 active cells on
+[-0.5,0.5]^3, corners mapped by x' = x + 0.04 sin(2 pi y) sin(2 pi z) (cyclic), rho=1, p=0.1 with
+p=10 inside r<0.1, B=(1,1,0)/sqrt(2), gamma=5/3, zero-gradient (outflow) boundaries, CFL 0.3.
+Grid metrics and the initial state are built on the device (Corners2Grid + 12^3-point Gauss ICs).
+
+A step is one full stepGamera (predictor, E field/CT, fluxes, update, CalcDT, BCs); one zone-update is
+one active cell advanced by one step. The state (~2.5 GB per buffer) is far larger than the 126 MB L2,
+so no L2 flush is needed between steps.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--prec fp64|fp32flux] [--impl ours|reference]
+
+Under torchrun every rank advances its own replica (weak scaling); value = all ranks' zone-updates /
+the slowest rank's device time. `--impl reference` times the CPU oracle (the reference restated in
+C++, OpenMP on all host cores; the Fortran reference cannot be compiled on this image) on rank 0.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "zone-updates/s on 1 B200: FP32-flux & learned-closure vs plain FP64, matched L1"
+PEAKS_PATH = os.path.join(ROOT, "MEASURED_PEAKS.json")
+FALLBACK_HBM_GBS = 6650.0
+FP64_NOMINAL_TFLOPS = 37.0   # B200 datasheet FP64 (non-tensor); no measured FP64 peak on this pool
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--n", type=int, default=256, help="active cells per side")
+    ap.add_argument("--prec", default="fp64", choices=["fp64", "fp32flux"])
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-n", type=int, default=64)
+    return ap.parse_args()
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+def workload_config(n, prec, extra=None):
+    cfg = {"workload": f"3D MHD blast wave, warped grid, {n}^3, zero-gradient BCs, {prec}",
+           "cells": [n, n, n], "ghosts": 4, "grid": "x'=x+0.04 sin(2 pi y) sin(2 pi z) cyclic",
+           "ic": "rho=1 p=0.1 (p=10 r<0.1) B=(1,1,0)/sqrt(2)", "CFL": 0.3, "recon": "8CENT+PDM pdmb=0.75",
+           "l2": "inputs larger than L2 (state ~2.5 GB/buffer), no flush"}
+    if extra:
+        cfg.update(extra)
+    return cfg
+
+
+def model_for(n):
+    from kaiju_b200 import gamera as gm
+    return gm.Model(n, n, n, CFL=0.3, tFin=1.0e30, bc=(gm.GAM_BC_ZEROGRAD,) * 6)
+
+
+class ClockSampler:
+    """nvidia-smi clocks during the timed region."""
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_rank{index}.csv")
+
+    def __enter__(self):
+        try:
+            os.makedirs(os.path.dirname(self.path), exist_ok=True)
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}",
+                 "--query-gpu=index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+                 "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+                 "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap",
+                 "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+            self.f.close()
+
+    def summary(self):
+        try:
+            rows = [r.split(",") for r in open(self.path).read().strip().splitlines() if r.strip()]
+        except Exception:
+            return None
+        if not rows:
+            return None
+        sm = [float(r[1]) for r in rows if r[1].strip().replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].strip().replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[q] for r in rows for q in range(4) if len(r) > 5 + q and "Active" in r[5 + q]})
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def peaks():
+    try:
+        return json.load(open(PEAKS_PATH)), "measured"
+    except Exception:
+        return {"hbm_gbs": FALLBACK_HBM_GBS}, "fallback"
+
+
+# Algorithmic bytes and flops of the flux kernel (one launch = all interfaces of one direction).
+# Per interface it must read once: half-state primitives (5) and B (3), state-n primitives (5) and
+# B (3) for the limiter, the volume (1), the face triad (9), the area (1) and the half-state normal
+# flux (1) = 28 doubles, and write 5 gas + 3 magnetic fluxes = 8 doubles: 36 doubles = 288 B.
+FLUX_BYTES_PER_IFACE = 36 * 8
+FLUX_FLOPS_PER_IFACE = 700.0
+# Whole-step compulsory traffic per zone-update on a curvilinear grid, FP64: state n and n-1 in,
+# n+1 out (24 doubles) + metrics (volume 1, face 3, edge 3, Tf 27, Te 27, Teb 12, xfc 9, xyzcc 3,
+# di/dj/dk 3 = 88 doubles) = 112 doubles = 896 B.
+STEP_BYTES_PER_ZONE = 896
+
+
+def run_ours(args, rank, world, local):
+    import torch
+    from kaiju_b200 import build as kb, gamera as gm
+    kb.build()
+    torch.cuda.set_device(local)
+    if world > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300))
+    n = args.n
+    model = model_for(n)
+    xyz = gm.corners_warped(model, (-0.5, 0.5) * 3, 0.04)
+    g = gm.GameraGPU.from_corners(model, xyz, "BW")
+    if args.prec == "fp32flux":
+        g.set_precision(gm.GAM_FP32FLUX)
+    zones = n * n * n
+    # warm-up (also builds the two step graphs)
+    g.run_steps(max(args.warmup, 3), check=False)
+    torch.cuda.synchronize()
+    if world > 1:
+        torch.distributed.barrier()
+    with ClockSampler(local) as clk:
+        ms, rc = g.run_steps_timed(args.steps)
+    torch.cuda.synchronize()
+    if world > 1:
+        t = torch.tensor([ms], device="cuda", dtype=torch.float64)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        ms = float(t.item())
+    st = g.status()
+    value = world * zones * args.steps / (ms / 1e3)
+
+    # per-phase device times (eager launches, CUDA events on the library stream)
+    ph = g.profile_phases(2)
+    # end to end through the C ABI with host buffers: per step, State and oState in from pinned host
+    # memory, one stepGamera, State out
+    shapes = gm.array_shapes(model)
+    pin = {}
+    for nm in ("gas", "magflux", "ogas", "omagflux", "bxyz"):
+        tt = torch.empty(int(np.prod(shapes[nm])), dtype=torch.float64, pin_memory=True)
+        pin[nm] = tt.numpy().reshape(shapes[nm], order="F")
+    g.sync_to_host(gas=pin["gas"], magflux=pin["magflux"], bxyz=pin["bxyz"], ogas=pin["ogas"],
+                   omagflux=pin["omagflux"])
+    s0 = g.status()
+    ke = max(1, args.e2e_steps)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(ke):
+        g.sync_to_device(gas=pin["gas"], magflux=pin["magflux"], ogas=pin["ogas"], omagflux=pin["omagflux"],
+                         time=s0["time"], otime=s0["otime"])
+        g.step()
+        g.sync_to_host(gas=pin["gas"], magflux=pin["magflux"], bxyz=pin["bxyz"])
+    torch.cuda.synchronize()
+    e2e_s = (time.perf_counter() - t0) / ke
+    h2d = sum(pin[nm].nbytes for nm in ("gas", "magflux", "ogas", "omagflux"))
+    d2h = sum(pin[nm].nbytes for nm in ("gas", "magflux", "bxyz"))
+    e2e_val = world * zones / e2e_s
+    if world > 1:
+        t = torch.tensor([e2e_s], device="cuda", dtype=torch.float64)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        e2e_val = world * zones / float(t.item())
+    launches_per_step = None
+    try:
+        st2 = g.status()
+        launches_per_step = kernels_per_step_estimate(model)
+    except Exception:
+        pass
+
+    # roofline of the dominant phase
+    pk, pk_kind = peaks()
+    hbm = float(pk.get("hbm_gbs", FALLBACK_HBM_GBS))
+    dom = max(ph, key=ph.get)
+    n_if = (n + 1) * n * n   # interfaces per direction launch
+    flux_launch_ms = ph["fluxes"] / 3.0
+    achieved = FLUX_BYTES_PER_IFACE * n_if / (flux_launch_ms / 1e3) / 1e9
+    roof = {"kernel": "k_fluxes<double>" if args.prec == "fp64" else "k_fluxes<float>",
+            "bound": "hbm", "achieved": round(achieved, 1), "peak": hbm, "unit": "GB/s",
+            "frac": round(achieved / hbm, 4), "traffic": None, "peak_source": pk_kind,
+            "launch_ms": round(flux_launch_ms, 4),
+            "fp64_tflops": round(FLUX_FLOPS_PER_IFACE * n_if / (flux_launch_ms / 1e3) / 1e12, 3),
+            "fp64_peak_nominal_tflops": FP64_NOMINAL_TFLOPS,
+            "dominant_phase": dom, "phase_ms": {k: round(v, 4) for k, v in ph.items()},
+            "step_bytes_per_zone": STEP_BYTES_PER_ZONE,
+            "step_hbm_frac": round(STEP_BYTES_PER_ZONE * zones / (ms / args.steps / 1e3) / 1e9 / hbm, 4)}
+    clocks = clk.summary()
+    g.close()
+    out = {
+        "metric": METRIC, "value": value, "unit": "zone-updates/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64" if args.prec == "fp64" else "f32-flux/f64-state",
+        "data": "synthetic (problem generated on the device)",
+        "config": workload_config(n, args.prec, {"parallelism": f"replicas x{world}"}),
+        "e2e": {"value": e2e_val, "unit": "zone-updates/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                "steps": ke},
+        "gpu_launches": (launches_per_step or 0) * args.steps,
+        "roofline": roof, "clocks": clocks, "status": st["status"], "t_sim": st["t"], "dt": st["dt"],
+    }
+    if rank == 0 and not args.no_cpu_baseline:
+        out["cpu_baseline"] = cpu_baseline(args.cpu_n, steps=2)
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+        dist.destroy_process_group()
+    return out
+
+
+def kernels_per_step_estimate(model):
+    # begin, predict faces, predict cells, E memset + 3 x (mom2face + edge), 3 fluxes, flux2deltas,
+    # e2flux, bflux2fld, update gas, calcdt + finalize, 3 BCs, bflux2fld
+    n = 2 + (1 + 6 if model.doMHD else 0) + (2 if model.do25D else 3) + 1 + 3 + 2 + 3 + 1
+    return n
+
+
+def cpu_baseline(n, steps=2):
+    """The oracle (C++ restatement of the reference, OpenMP) on an n^3 sample of the same problem."""
+    from oracle import pyoracle as po
+    po.build()
+    threads = os.cpu_count() or 1
+    o = po.Oracle(n, n, n, ic="BW", grid="warp", warp_amp=0.04, bounds=(-0.5, 0.5) * 3, CFL=0.3, bc=[1] * 6,
+                  threads=threads)
+    o.step(1)
+    t0 = time.perf_counter()
+    o.step(steps)
+    dt = time.perf_counter() - t0
+    o.close()
+    return {"value": n ** 3 * steps / dt, "unit": "zone-updates/s", "cores": threads, "kind": "port",
+            "sample": f"{n}^3 sample of the same warped blast wave, {steps} timed steps after 1 warm-up "
+                      f"(set-up excluded), OpenMP {threads} threads"}
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return None
+    n = args.cpu_n
+    from oracle import pyoracle as po
+    po.build()
+    threads = os.cpu_count() or 1
+    o = po.Oracle(n, n, n, ic="BW", grid="warp", warp_amp=0.04, bounds=(-0.5, 0.5) * 3, CFL=0.3, bc=[1] * 6,
+                  threads=threads)
+    o.step(max(1, min(args.warmup, 2)))
+    steps = max(1, min(args.steps, 4))
+    t0 = time.perf_counter()
+    o.step(steps)
+    dt = time.perf_counter() - t0
+    o.close()
+    v = n ** 3 * steps / dt
+    sample = (f"{n}^3 sample of the same warped blast wave (256^3 is the GPU workload), {steps} timed steps, "
+              f"OpenMP {threads} threads; C++ restatement of the Fortran reference (no Fortran compiler on "
+              f"this image)")
+    return {"metric": METRIC, "value": v, "unit": "zone-updates/s", "n_gpus": world, "steps": steps,
+            "warmup": args.warmup, "ms_per_step": dt / steps * 1e3, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference",
+            "config": workload_config(args.n, "fp64"),
+            "cpu_baseline": {"value": v, "unit": "zone-updates/s", "cores": threads, "kind": "port", "sample": sample},
+            "e2e": {"value": v, "unit": "zone-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+
+
+def main():
+    args = parse()
+    rank, world, local = dist_env()
+    if args.impl == "reference":
+        out = run_reference(args, rank, world)
+    else:
+        out = run_ours(args, rank, world, local)
+    if rank == 0 and out is not None:
+        print(json.dumps(out))
+
+
+if __name__ == "__main__":
+    main()

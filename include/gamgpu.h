@@ -1,0 +1,149 @@
+/* gamgpu.h -- C ABI of the B200 GAMERA ideal-MHD step.
+ *
+ * This is the drop-in boundary for the reference's step call. A Fortran host keeps its Model_T,
+ * Grid_T and State_T (src/base/types/gamtypes.F90:71-286), runs Hatch (src/gamera/init.F90:38-59)
+ * as before, and hands the arrays to gam_gpu_create; stepGamera (src/gamera/gamapp.F90:73-94)
+ * becomes gam_gpu_step and gamAdvanceModel (src/gamera/gamtypessub.F90:78-94) becomes
+ * gam_gpu_advance. Every array argument is a plain double* in the reference's Fortran layout:
+ * column-major, i fastest, ghosts included, lower bounds isg/jsg/ksg, the trailing dimension(s)
+ * being the variable / vector component / transform index exactly as declared in gamtypes.F90.
+ * No torch or CUDA types appear here.
+ *
+ * Return codes are GAM_OK (0) or one of GAM_ERR_*; nothing traps on the device.
+ */
+#ifndef GAMGPU_H
+#define GAMGPU_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define GAM_OK 0
+#define GAM_ERR_NAN 1          /* a CellDT evaluation produced NaN (bad state)                    */
+#define GAM_ERR_DT_COLLAPSE 2  /* CalcDT's isDisaster / isBad (src/gamera/step.F90:103-135)      */
+#define GAM_ERR_CUDA 3         /* a CUDA call failed; the handle should be destroyed              */
+#define GAM_ERR_TIMEOUT 4      /* a bounded device wait gave up                                   */
+#define GAM_ERR_UNSUPPORTED 5  /* a Model option this build does not run on the device           */
+#define GAM_ERR_ARG 6          /* bad argument (null pointer, size, name)                          */
+
+/* precision modes (gam_gpu_set_precision) */
+#define GAM_FP64 0             /* everything in FP64: the parity path                              */
+#define GAM_FP32FLUX 1         /* FP32 reconstruction, limiter, kinetic fluxes and EMF arithmetic;
+                                  FP64 state, accumulation, CT update, C2P with floors and dt      */
+
+/* boundary kinds for gam_model_c.bc[] in the reference's order INI,OUTI,INJ,OUTJ,INK,OUTK
+   (src/base/defs/gdefs.F90:43-45) */
+#define GAM_BC_PERIODIC 0      /* src/gamera/bcs.F90:279-450 */
+#define GAM_BC_ZEROGRAD 1      /* src/gamera/bcs.F90:799-930 */
+
+/* reconstruction (Model sim/rmeth, src/gamera/init.F90:447-462) */
+#define GAM_RM_8CENT 0
+#define GAM_RM_7UP 1
+
+/* sync masks */
+#define GAM_SYNC_STATE 1u      /* State%Gas, State%magFlux (and State%Bxyz on the way out) */
+#define GAM_SYNC_OSTATE 2u     /* oState%Gas, oState%magFlux                                */
+
+typedef struct gam_gpu gam_gpu_t;
+
+/* The Model_T fields the step reads (src/base/types/gamtypes.F90:71-146). */
+typedef struct {
+    int Nip, Njp, Nkp;         /* active cells (Grid_T Nip,Njp,Nkp)                     */
+    int nG;                    /* ghosts per side (Model%nG, 4)                         */
+    double gamma, CFL, pdmb, Vd0, cHogH, cHogM, Ca, dFloor, pFloor, limDT0;
+    double t, tFin, dt, dt0;   /* Model%t, tFin, dt, dt0                                 */
+    int ts;                    /* Model%ts                                              */
+    int doMHD, doBoris, do25D, doLFMLim, rmeth, fixedTimestep;
+    /* options the device path does not run; nonzero -> GAM_ERR_UNSUPPORTED */
+    int doBackground, doGrav, doResistive, doRing, doMultiF, doAB3, nSpc, hasHooks;
+    int bc[6];                 /* GAM_BC_* per face                                      */
+} gam_model_c;
+
+/* The Grid_T metric arrays the step reads (gamtypes.F90:163-245), Fortran layout. */
+typedef struct {
+    const double* xyzcc;   /* (Ni,Nj,Nk,3)            cell centres              */
+    const double* xfc;     /* (Ni+1,Nj+1,Nk+1,3,3)    face centres              */
+    const double* di;      /* (Ni,Nj,Nk)              dt lengths                */
+    const double* dj;
+    const double* dk;
+    const double* volume;  /* (Ni,Nj,Nk)                                       */
+    const double* face;    /* (Ni+1,Nj+1,Nk+1,3)      face areas                */
+    const double* edge;    /* (Ni+1,Nj+1,Nk+1,3)      edge lengths              */
+    const double* Tf;      /* (Ni+1,Nj+1,Nk+1,9,3)    face triads               */
+    const double* Te;      /* (Ni+1,Nj+1,Nk+1,9,3)    edge triads               */
+    const double* Teb;     /* (Ni+1,Nj+1,Nk+1,4,3)    edge B transforms         */
+} gam_grid_c;
+
+typedef struct {
+    double t, dt, dt0, time, otime; /* Model%t/dt/dt0, State%time, oState%time */
+    int ts;
+    int status;                     /* GAM_ERR_* of the last step, 0 if fine    */
+    int nanCells;                   /* cells with NaN CellDT in the last step    */
+    int precision;
+    long long kernelLaunches;       /* kernels launched by this handle so far    */
+} gam_status_c;
+
+/* Mirror a Hatch-ed problem onto the current CUDA device. gas/ogas are State%Gas/oState%Gas
+ * (Ni,Nj,Nk,5); magflux/omagflux are (Ni+1,Nj+1,Nk+1,3). time/otime are State%time/oState%time.
+ * Replaces: the arrays Hatch leaves in gamApp_T (src/gamera/init.F90:150-260). */
+int gam_gpu_create(gam_gpu_t** h, const gam_model_c* m, const gam_grid_c* g, const double* gas,
+                   const double* magflux, const double* ogas, const double* omagflux, double time,
+                   double otime);
+
+/* Build the grid metrics and the initial state on the device from corner coordinates
+ * xyz (Ni+1,Nj+1,Nk+1,3): Corners2Grid (src/gamera/init.F90:801-1145) and the problem set-up that
+ * ends CalcGridInfo (init.F90:204-244: bFlux2Fld, EnforceBCs, CalcDT, oState = State).
+ * ic: GAM_IC_OT2D (src/gamera/prob.F90:74-119) or GAM_IC_BW (prob.F90:190-298, deck defaults). */
+#define GAM_IC_OT2D 0
+#define GAM_IC_BW 1
+int gam_gpu_create_from_corners(gam_gpu_t** h, const gam_model_c* m, const double* xyz, int ic);
+
+/* One stepGamera (src/gamera/gamapp.F90:73-94): AdvanceMHD, ts/t update, CalcDT, EnforceBCs,
+ * bFlux2Fld. Outputs (may be NULL): the new Model%dt, Model%ts, Model%t. */
+int gam_gpu_step(gam_gpu_t* h, double* dt, int* ts, double* t);
+
+/* gamAdvanceModel (src/gamera/gamtypessub.F90:78-94): step at least once, until t >= t0 + dtAdvance. */
+int gam_gpu_advance(gam_gpu_t* h, double dtAdvance);
+
+/* n steps back to back without a host round trip per step (device-resident dt); status is the OR of
+ * the steps' statuses. */
+int gam_gpu_run_steps(gam_gpu_t* h, int n);
+
+/* n steps like gam_gpu_run_steps, timed with CUDA events on the handle's stream; *ms = elapsed time. */
+int gam_gpu_run_steps_timed(gam_gpu_t* h, int n, double* ms);
+
+/* Average per-step device time of each phase of the step over nsteps eager (non-graph) steps, in
+ * the order predictor, E field, fluxes, flux divergence, update (CT + Reynolds/Maxwell), CalcDT,
+ * boundaries + bFlux2Fld. nphase must be >= 7. The steps advance the state. */
+#define GAM_NPHASE 7
+int gam_gpu_profile_phases(gam_gpu_t* h, int nsteps, double* ms, int nphase);
+
+/* Copy state to / from the caller's Fortran arrays (NULL pointers are skipped). */
+int gam_gpu_sync_to_host(gam_gpu_t* h, unsigned what, double* gas, double* magflux, double* bxyz,
+                         double* ogas, double* omagflux);
+int gam_gpu_sync_to_device(gam_gpu_t* h, unsigned what, const double* gas, const double* magflux,
+                           const double* ogas, const double* omagflux, double time, double otime);
+
+/* Model/state scalars, e.g. to resume from a restart (Model%t, dt, dt0, ts; State%time, oState%time) */
+int gam_gpu_get_status(gam_gpu_t* h, gam_status_c* s);
+int gam_gpu_set_scalars(gam_gpu_t* h, double t, double dt, double dt0, int ts, double time, double otime);
+
+/* DivB (src/gamera/gridutils.F90:717-770): sum over active cells of |net face flux| */
+int gam_gpu_divb(gam_gpu_t* h, double* tot);
+
+/* GAM_FP64 or GAM_FP32FLUX */
+int gam_gpu_set_precision(gam_gpu_t* h, int mode);
+
+/* Fetch an internal or grid array in the reference's Fortran layout, by the reference's name:
+ * "gas","magflux","bxyz","ogas","omagflux","obxyz","hgas","hmagflux","hbxyz" (Solver%StateHf),
+ * "efld","vf","dgash","dgasm","gflx","mflx", "volume","xyzcc","xfc","di","dj","dk","face","edge",
+ * "tf","te","teb","xyz". n = number of doubles the caller's buffer holds. */
+int gam_gpu_fetch(gam_gpu_t* h, const char* name, double* out, long long n);
+
+void gam_gpu_destroy(gam_gpu_t* h);
+const char* gam_gpu_errstr(int code);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* GAMGPU_H */

@@ -1,0 +1,541 @@
+// C ABI (include/gamgpu.h): handle lifetime, Fortran-layout mirroring, step / advance entry points.
+#include <cstdio>
+#include <cstring>
+#include <cstdlib>
+#include <new>
+#include <string>
+#include "gamgpu.h"
+#include "gam_common.cuh"
+#include "gam_step.cuh"
+#include "gam_init.cuh"
+
+using namespace gam;
+
+struct gam_gpu {
+    Handle h;
+    double* stage = nullptr;        // contiguous staging for Fortran<->pencil repacking
+    size_t stagePlanes = 0;
+    double* scratch = nullptr;      // reduction partials
+    size_t scratchDoubles = 0;
+    int lastStatus = 0;
+};
+
+namespace {
+
+#define CK(x)                                                                                  \
+    do {                                                                                       \
+        cudaError_t e_ = (x);                                                                  \
+        if (e_ != cudaSuccess) {                                                               \
+            std::fprintf(stderr, "gamgpu: %s failed: %s (%s:%d)\n", #x, cudaGetErrorString(e_),  \
+                         __FILE__, __LINE__);                                                  \
+            return GAM_ERR_CUDA;                                                               \
+        }                                                                                      \
+    } while (0)
+
+__global__ void k_pack_in(Lay L, double* dst, const double* src, int ni, int nj, int nk) {
+    long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    long long n = (long long)ni * nj * nk;
+    if (t >= n) return;
+    int i = (int)(t % ni);
+    long long q = t / ni;
+    int j = (int)(q % nj), k = (int)(q / nj);
+    dst[L.at(i, j, k)] = src[t];
+}
+__global__ void k_pack_out(Lay L, double* dst, const double* src, int ni, int nj, int nk) {
+    long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    long long n = (long long)ni * nj * nk;
+    if (t >= n) return;
+    int i = (int)(t % ni);
+    long long q = t / ni;
+    int j = (int)(q % nj), k = (int)(q / nj);
+    dst[t] = src[L.at(i, j, k)];
+}
+
+// Per-plane extents in the Fortran arrays: cell (Ni,Nj,Nk) or face/edge/corner (Ni+1,Nj+1,Nk+1)
+struct Ext { int ni, nj, nk; long long n() const { return (long long)ni * nj * nk; } };
+Ext cellExt(const Lay& L) { return {L.Ni, L.Nj, L.Nk}; }
+Ext faceExt(const Lay& L) { return {L.Ni + 1, L.Nj + 1, L.Nk + 1}; }
+
+int h2d_planes(gam_gpu* G, double* const* planes, int np, const double* host, Ext e) {
+    Handle& h = G->h;
+    for (int q = 0; q < np; ++q) {
+        CK(cudaMemcpyAsync(G->stage, host + q * e.n(), sizeof(double) * e.n(), cudaMemcpyHostToDevice, h.stream));
+        k_pack_in<<<(unsigned)((e.n() + 255) / 256), 256, 0, h.stream>>>(h.L, planes[q], G->stage, e.ni, e.nj, e.nk);
+        h.launches++;
+    }
+    CK(cudaGetLastError());
+    return GAM_OK;
+}
+int d2h_planes(gam_gpu* G, double* const* planes, int np, double* host, Ext e) {
+    Handle& h = G->h;
+    for (int q = 0; q < np; ++q) {
+        k_pack_out<<<(unsigned)((e.n() + 255) / 256), 256, 0, h.stream>>>(h.L, G->stage, planes[q], e.ni, e.nj, e.nk);
+        h.launches++;
+        CK(cudaMemcpyAsync(host + q * e.n(), G->stage, sizeof(double) * e.n(), cudaMemcpyDeviceToHost, h.stream));
+    }
+    CK(cudaGetLastError());
+    return GAM_OK;
+}
+
+int check_model(const gam_model_c* m) {
+    if (!m) return GAM_ERR_ARG;
+    if (m->doBackground || m->doGrav || m->doResistive || m->doRing || m->doMultiF || m->doAB3 || m->nSpc != 0 ||
+        m->hasHooks)
+        return GAM_ERR_UNSUPPORTED;
+    if (m->nG != 4 || m->Nip < 16 || m->Njp < 1 || m->Nkp < 1) return GAM_ERR_ARG;
+    for (int n = 0; n < 6; ++n)
+        if (m->bc[n] != GAM_BC_PERIODIC && m->bc[n] != GAM_BC_ZEROGRAD) return GAM_ERR_UNSUPPORTED;
+    if (m->rmeth != GAM_RM_8CENT && m->rmeth != GAM_RM_7UP) return GAM_ERR_ARG;
+    return GAM_OK;
+}
+
+// Allocate the pool and carve the planes
+int alloc_handle(gam_gpu* G, const gam_model_c* m) {
+    Handle& h = G->h;
+    Lay& L = h.L;
+    L.Nip = m->Nip; L.Njp = m->Njp; L.Nkp = m->Nkp; L.nG = m->nG;
+    L.Ni = L.Nip + 2 * L.nG; L.Nj = L.Njp + 2 * L.nG; L.Nk = L.Nkp + 2 * L.nG;
+    L.P = ((L.Ni + 1) + 7) / 8 * 8;
+    L.Q = L.Nj + 1; L.R = L.Nk + 1;
+    L.E = (long long)L.P * L.Q * L.R;
+    Par& p = h.p;
+    p.gamma = m->gamma; p.CFL = m->CFL; p.pdmb = m->pdmb; p.Vd0 = m->Vd0; p.cHogH = m->cHogH; p.cHogM = m->cHogM;
+    p.Ca = m->Ca; p.dFloor = m->dFloor; p.pFloor = m->pFloor; p.limDT0 = m->limDT0; p.tFin = m->tFin;
+    p.doMHD = m->doMHD; p.doBoris = m->doBoris; p.do25D = m->do25D; p.doLFMLim = m->doLFMLim; p.rmeth = m->rmeth;
+    p.fixedTimestep = m->fixedTimestep;
+    for (int n = 0; n < 6; ++n) p.bc[n] = m->bc[n];
+
+    CK(cudaGetDevice(&h.device));
+    CK(cudaStreamCreateWithFlags(&h.stream, cudaStreamNonBlocking));
+    h.ownStream = true;
+    const size_t planes = 11 * 3 + 10 + 14 + 24 + 91;
+    h.poolPlanes = planes;
+    CK(cudaMalloc(&h.pool, sizeof(double) * L.E * planes));
+    CK(cudaMemsetAsync(h.pool, 0, sizeof(double) * L.E * planes, h.stream));
+    double* q = h.pool;
+    auto take = [&]() { double* r = q; q += L.E; return r; };
+    for (int s = 0; s < 2; ++s) {
+        for (int v = 0; v < 5; ++v) h.S[s].gas[v] = take();
+        for (int x = 0; x < 3; ++x) h.S[s].mf[x] = take();
+        for (int x = 0; x < 3; ++x) h.S[s].b[x] = take();
+    }
+    for (int v = 0; v < 5; ++v) h.H.gas[v] = take();
+    for (int x = 0; x < 3; ++x) h.H.mf[x] = take();
+    for (int x = 0; x < 3; ++x) h.H.b[x] = take();
+    for (int v = 0; v < 5; ++v) h.Wh[v] = take();
+    for (int v = 0; v < 5; ++v) h.Wn[v] = take();
+    for (int x = 0; x < 3; ++x) h.E[x] = take();   // contiguous: memset as one range
+    for (int x = 0; x < 3; ++x) h.Vf[x] = take();
+    for (int v = 0; v < 5; ++v) h.dGasH[v] = take();
+    for (int x = 0; x < 3; ++x) h.dGasM[x] = take();
+    for (int d = 0; d < 3; ++d) for (int v = 0; v < 5; ++v) h.gflx[d][v] = take();
+    for (int d = 0; d < 3; ++d) for (int x = 0; x < 3; ++x) h.mflx[d][x] = take();
+    h.volume = take();
+    for (int x = 0; x < 3; ++x) h.xyzcc[x] = take();
+    for (int d = 0; d < 3; ++d) for (int x = 0; x < 3; ++x) h.xfc[d][x] = take();
+    h.di = take(); h.dj = take(); h.dk = take();
+    for (int d = 0; d < 3; ++d) h.face[d] = take();
+    for (int d = 0; d < 3; ++d) h.edge[d] = take();
+    for (int d = 0; d < 3; ++d) for (int c = 0; c < 9; ++c) h.Tf[d][c] = take();
+    for (int d = 0; d < 3; ++d) for (int c = 0; c < 9; ++c) h.Te[d][c] = take();
+    for (int d = 0; d < 3; ++d) for (int c = 0; c < 4; ++c) h.Teb[d][c] = take();
+    for (int x = 0; x < 3; ++x) h.xyz[x] = take();
+    if ((size_t)(q - h.pool) != (size_t)L.E * planes) return GAM_ERR_ARG;
+
+    Ext fe = faceExt(L);
+    CK(cudaMalloc(&G->stage, sizeof(double) * fe.n()));
+    G->scratchDoubles = (size_t)((long long)L.Nip * L.Njp * L.Nkp / 256 + 1024);
+    CK(cudaMalloc(&G->scratch, sizeof(double) * G->scratchDoubles));
+    CK(cudaMalloc(&h.dScal, sizeof(Scal)));
+    CK(cudaMallocHost(&h.hScal, sizeof(Scal)));
+    std::memset(h.hScal, 0, sizeof(Scal));
+    h.hScal->t = m->t; h.hScal->dt = m->dt; h.hScal->dt0 = m->dt0; h.hScal->ts = m->ts;
+    h.hScal->dtMinBits = 0x7FF0000000000000ull;
+    CK(cudaMemcpyAsync(h.dScal, h.hScal, sizeof(Scal), cudaMemcpyHostToDevice, h.stream));
+    CK(cudaStreamSynchronize(h.stream));
+    return GAM_OK;
+}
+
+int upload_scalars(gam_gpu* G) {
+    Handle& h = G->h;
+    CK(cudaMemcpyAsync(h.dScal, h.hScal, sizeof(Scal), cudaMemcpyHostToDevice, h.stream));
+    return GAM_OK;
+}
+int download_scalars(gam_gpu* G) {
+    Handle& h = G->h;
+    CK(cudaMemcpyAsync(h.hScal, h.dScal, sizeof(Scal), cudaMemcpyDeviceToHost, h.stream));
+    CK(cudaStreamSynchronize(h.stream));
+    return GAM_OK;
+}
+
+int status_code(int st) {
+    if (st & 4) return GAM_ERR_NAN;
+    if (st & 3) return GAM_ERR_DT_COLLAPSE;
+    return GAM_OK;
+}
+
+void destroy_graphs(Handle& h) {
+    for (int c = 0; c < 2; ++c)
+        if (h.graph[c]) { cudaGraphExecDestroy(h.graph[c]); h.graph[c] = nullptr; }
+}
+
+int build_graphs(gam_gpu* G) {
+    Handle& h = G->h;
+    destroy_graphs(h);
+    for (int c = 0; c < 2; ++c) {
+        cudaGraph_t gr;
+        CK(cudaStreamBeginCapture(h.stream, cudaStreamCaptureModeThreadLocal));
+        int rc = step_enqueue(h, c);
+        cudaError_t e = cudaStreamEndCapture(h.stream, &gr);
+        if (rc != 0 || e != cudaSuccess) {
+            std::fprintf(stderr, "gamgpu: step capture failed: %s\n", cudaGetErrorString(e));
+            if (e == cudaSuccess) cudaGraphDestroy(gr);
+            return GAM_ERR_CUDA;
+        }
+        e = cudaGraphInstantiate(&h.graph[c], gr, 0);
+        cudaGraphDestroy(gr);
+        if (e != cudaSuccess) return GAM_ERR_CUDA;
+    }
+    return GAM_OK;
+}
+
+int launch_one_step(gam_gpu* G) {
+    Handle& h = G->h;
+    if (h.useGraph) {
+        if (!h.graph[0]) {
+            int rc = build_graphs(G);
+            if (rc) return rc;
+        }
+        CK(cudaGraphLaunch(h.graph[h.cur], h.stream));
+        h.launches += kernels_per_step(h);
+    } else {
+        if (step_enqueue(h, h.cur) != 0) return GAM_ERR_CUDA;
+    }
+    h.cur ^= 1;
+    return GAM_OK;
+}
+
+}  // namespace
+
+// Shared with gam_init.cu
+namespace gam {
+int capi_alloc(gam_gpu* G, const gam_model_c* m) { return alloc_handle(G, m); }
+int capi_upload_scalars(gam_gpu* G) { return upload_scalars(G); }
+int capi_download_scalars(gam_gpu* G) { return download_scalars(G); }
+Handle& capi_handle(gam_gpu* G) { return G->h; }
+double* capi_scratch(gam_gpu* G) { return G->scratch; }
+}  // namespace gam
+
+extern "C" {
+
+const char* gam_gpu_errstr(int code) {
+    switch (code) {
+    case GAM_OK: return "ok";
+    case GAM_ERR_NAN: return "NaN in the state (CellDT)";
+    case GAM_ERR_DT_COLLAPSE: return "timestep collapse (CalcDT isDisaster/isBad)";
+    case GAM_ERR_CUDA: return "CUDA error";
+    case GAM_ERR_TIMEOUT: return "bounded device wait timed out";
+    case GAM_ERR_UNSUPPORTED: return "Model option not supported on the device path";
+    case GAM_ERR_ARG: return "bad argument";
+    default: return "unknown";
+    }
+}
+
+int gam_gpu_create(gam_gpu_t** out, const gam_model_c* m, const gam_grid_c* g, const double* gas,
+                   const double* magflux, const double* ogas, const double* omagflux, double time, double otime) {
+    if (!out || !g || !gas || !magflux || !ogas || !omagflux) return GAM_ERR_ARG;
+    *out = nullptr;
+    int rc = check_model(m);
+    if (rc) return rc;
+    if (!g->xyzcc || !g->xfc || !g->di || !g->dj || !g->dk || !g->volume || !g->face || !g->edge || !g->Tf ||
+        !g->Te || !g->Teb)
+        return GAM_ERR_ARG;
+    gam_gpu* G = new (std::nothrow) gam_gpu();
+    if (!G) return GAM_ERR_ARG;
+    rc = alloc_handle(G, m);
+    if (rc) { gam_gpu_destroy(G); return rc; }
+    Handle& h = G->h;
+    const Lay& L = h.L;
+    Ext ce = cellExt(L), fe = faceExt(L);
+    double* pl[27];
+    rc = h2d_planes(G, &h.volume, 1, g->volume, ce);
+    if (!rc) rc = h2d_planes(G, h.xyzcc, 3, g->xyzcc, ce);
+    if (!rc) { for (int d = 0; d < 3; ++d) for (int x = 0; x < 3; ++x) pl[d * 3 + x] = h.xfc[d][x]; rc = h2d_planes(G, pl, 9, g->xfc, fe); }
+    if (!rc) rc = h2d_planes(G, &h.di, 1, g->di, ce);
+    if (!rc) rc = h2d_planes(G, &h.dj, 1, g->dj, ce);
+    if (!rc) rc = h2d_planes(G, &h.dk, 1, g->dk, ce);
+    if (!rc) rc = h2d_planes(G, h.face, 3, g->face, fe);
+    if (!rc) rc = h2d_planes(G, h.edge, 3, g->edge, fe);
+    if (!rc) { for (int d = 0; d < 3; ++d) for (int c = 0; c < 9; ++c) pl[d * 9 + c] = h.Tf[d][c]; rc = h2d_planes(G, pl, 27, g->Tf, fe); }
+    if (!rc) { for (int d = 0; d < 3; ++d) for (int c = 0; c < 9; ++c) pl[d * 9 + c] = h.Te[d][c]; rc = h2d_planes(G, pl, 27, g->Te, fe); }
+    if (!rc) { for (int d = 0; d < 3; ++d) for (int c = 0; c < 4; ++c) pl[d * 4 + c] = h.Teb[d][c]; rc = h2d_planes(G, pl, 12, g->Teb, fe); }
+    if (rc) { gam_gpu_destroy(G); return rc; }
+    rc = gam_gpu_sync_to_device(G, GAM_SYNC_STATE | GAM_SYNC_OSTATE, gas, magflux, ogas, omagflux, time, otime);
+    if (rc) { gam_gpu_destroy(G); return rc; }
+    *out = G;
+    return GAM_OK;
+}
+
+int gam_gpu_create_from_corners(gam_gpu_t** out, const gam_model_c* m, const double* xyz, int ic) {
+    if (!out || !xyz) return GAM_ERR_ARG;
+    *out = nullptr;
+    int rc = check_model(m);
+    if (rc) return rc;
+    if (ic != GAM_IC_OT2D && ic != GAM_IC_BW) return GAM_ERR_ARG;
+    if ((m->Nip % 8) != 0) return GAM_ERR_ARG;   // Corners2Grid divisibility check (init.F90:830-834)
+    gam_gpu* G = new (std::nothrow) gam_gpu();
+    if (!G) return GAM_ERR_ARG;
+    rc = alloc_handle(G, m);
+    if (rc) { gam_gpu_destroy(G); return rc; }
+    Handle& h = G->h;
+    rc = h2d_planes(G, h.xyz, 3, xyz, faceExt(h.L));
+    if (rc) { gam_gpu_destroy(G); return rc; }
+    h.hScal->time = m->t;   // allocState: State%time = Model%t
+    h.hScal->otime = m->t;
+    rc = upload_scalars(G);
+    if (!rc && init_grid_from_corners(h) != 0) rc = GAM_ERR_CUDA;
+    if (!rc && init_problem(h, ic) != 0) rc = GAM_ERR_CUDA;
+    if (!rc) rc = download_scalars(G);
+    if (rc) { gam_gpu_destroy(G); return rc; }
+    *out = G;
+    return GAM_OK;
+}
+
+int gam_gpu_sync_to_device(gam_gpu_t* G, unsigned what, const double* gas, const double* magflux, const double* ogas,
+                           const double* omagflux, double time, double otime) {
+    if (!G) return GAM_ERR_ARG;
+    Handle& h = G->h;
+    const Lay& L = h.L;
+    Ext ce = cellExt(L), fe = faceExt(L);
+    int rc = GAM_OK;
+    StateP n = h.S[h.cur], o = h.S[h.cur ^ 1];
+    if ((what & GAM_SYNC_STATE) && gas) rc = h2d_planes(G, n.gas, 5, gas, ce);
+    if (!rc && (what & GAM_SYNC_STATE) && magflux) rc = h2d_planes(G, n.mf, 3, magflux, fe);
+    if (!rc && (what & GAM_SYNC_OSTATE) && ogas) rc = h2d_planes(G, o.gas, 5, ogas, ce);
+    if (!rc && (what & GAM_SYNC_OSTATE) && omagflux) rc = h2d_planes(G, o.mf, 3, omagflux, fe);
+    if (rc) return rc;
+    // Bxyz follows from the fluxes (bFlux2Fld), as after a restart read (init.F90:204-210)
+    if (what & GAM_SYNC_STATE) launch_bflux2fld(h, n, h.stream);
+    if (what & GAM_SYNC_OSTATE) launch_bflux2fld(h, o, h.stream);
+    // State%time / oState%time travel with the arrays; the other scalars stay as they are on the device
+    rc = download_scalars(G);
+    if (rc) return rc;
+    if (what & GAM_SYNC_STATE) h.hScal->time = time;
+    if (what & GAM_SYNC_OSTATE) h.hScal->otime = otime;
+    rc = upload_scalars(G);
+    if (rc) return rc;
+    CK(cudaStreamSynchronize(h.stream));
+    return GAM_OK;
+}
+
+int gam_gpu_sync_to_host(gam_gpu_t* G, unsigned what, double* gas, double* magflux, double* bxyz, double* ogas,
+                         double* omagflux) {
+    if (!G) return GAM_ERR_ARG;
+    Handle& h = G->h;
+    const Lay& L = h.L;
+    Ext ce = cellExt(L), fe = faceExt(L);
+    StateP n = h.S[h.cur], o = h.S[h.cur ^ 1];
+    int rc = GAM_OK;
+    if ((what & GAM_SYNC_STATE) && gas) rc = d2h_planes(G, n.gas, 5, gas, ce);
+    if (!rc && (what & GAM_SYNC_STATE) && magflux) rc = d2h_planes(G, n.mf, 3, magflux, fe);
+    if (!rc && (what & GAM_SYNC_STATE) && bxyz) rc = d2h_planes(G, n.b, 3, bxyz, ce);
+    if (!rc && (what & GAM_SYNC_OSTATE) && ogas) rc = d2h_planes(G, o.gas, 5, ogas, ce);
+    if (!rc && (what & GAM_SYNC_OSTATE) && omagflux) rc = d2h_planes(G, o.mf, 3, omagflux, fe);
+    if (rc) return rc;
+    CK(cudaStreamSynchronize(h.stream));
+    return GAM_OK;
+}
+
+int gam_gpu_set_scalars(gam_gpu_t* G, double t, double dt, double dt0, int ts, double time, double otime) {
+    if (!G) return GAM_ERR_ARG;
+    Handle& h = G->h;
+    h.hScal->t = t; h.hScal->dt = dt; h.hScal->dt0 = dt0; h.hScal->ts = ts; h.hScal->time = time;
+    h.hScal->otime = otime; h.hScal->dtMinBits = 0x7FF0000000000000ull; h.hScal->nanCount = 0;
+    h.hScal->status = 0; h.hScal->sticky = 0;
+    int rc = upload_scalars(G);
+    if (rc) return rc;
+    CK(cudaStreamSynchronize(h.stream));
+    return GAM_OK;
+}
+
+int gam_gpu_get_status(gam_gpu_t* G, gam_status_c* s) {
+    if (!G || !s) return GAM_ERR_ARG;
+    int rc = download_scalars(G);
+    if (rc) return rc;
+    Handle& h = G->h;
+    s->t = h.hScal->t; s->dt = h.hScal->dt; s->dt0 = h.hScal->dt0; s->time = h.hScal->time; s->otime = h.hScal->otime;
+    s->ts = h.hScal->ts; s->status = status_code(h.hScal->status); s->nanCells = (int)h.hScal->lastNan;
+    s->precision = h.prec; s->kernelLaunches = h.launches;
+    return GAM_OK;
+}
+
+int gam_gpu_step(gam_gpu_t* G, double* dt, int* ts, double* t) {
+    if (!G) return GAM_ERR_ARG;
+    int rc = launch_one_step(G);
+    if (rc) return rc;
+    rc = download_scalars(G);
+    if (rc) return rc;
+    Handle& h = G->h;
+    if (dt) *dt = h.hScal->dt;
+    if (ts) *ts = h.hScal->ts;
+    if (t) *t = h.hScal->t;
+    G->lastStatus = status_code(h.hScal->status);
+    return G->lastStatus;
+}
+
+int gam_gpu_advance(gam_gpu_t* G, double dtAdvance) {
+    if (!G) return GAM_ERR_ARG;
+    int rc = download_scalars(G);
+    if (rc) return rc;
+    double target = G->h.hScal->t + dtAdvance;
+    double t = 0.0;
+    rc = gam_gpu_step(G, nullptr, nullptr, &t);
+    if (rc) return rc;
+    while (t < target) {
+        rc = gam_gpu_step(G, nullptr, nullptr, &t);
+        if (rc) return rc;
+    }
+    return GAM_OK;
+}
+
+int gam_gpu_run_steps(gam_gpu_t* G, int n) {
+    if (!G || n < 0) return GAM_ERR_ARG;
+    for (int s = 0; s < n; ++s) {
+        int rc = launch_one_step(G);
+        if (rc) return rc;
+    }
+    int rc = download_scalars(G);
+    if (rc) return rc;
+    G->lastStatus = status_code(G->h.hScal->sticky);
+    return G->lastStatus;
+}
+
+int gam_gpu_run_steps_timed(gam_gpu_t* G, int n, double* ms) {
+    if (!G || n < 0 || !ms) return GAM_ERR_ARG;
+    Handle& h = G->h;
+    if (h.useGraph && !h.graph[0]) {
+        int rc = build_graphs(G);
+        if (rc) return rc;
+    }
+    cudaEvent_t e0, e1;
+    CK(cudaEventCreate(&e0));
+    CK(cudaEventCreate(&e1));
+    CK(cudaStreamSynchronize(h.stream));
+    CK(cudaEventRecord(e0, h.stream));
+    for (int s = 0; s < n; ++s) {
+        int rc = launch_one_step(G);
+        if (rc) return rc;
+    }
+    CK(cudaEventRecord(e1, h.stream));
+    CK(cudaEventSynchronize(e1));
+    float f = 0.f;
+    CK(cudaEventElapsedTime(&f, e0, e1));
+    *ms = (double)f;
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    int rc = download_scalars(G);
+    if (rc) return rc;
+    G->lastStatus = status_code(G->h.hScal->sticky);
+    return G->lastStatus;
+}
+
+int gam_gpu_profile_phases(gam_gpu_t* G, int nsteps, double* ms, int nphase) {
+    if (!G || nsteps <= 0 || !ms || nphase < NPHASE) return GAM_ERR_ARG;
+    Handle& h = G->h;
+    cudaEvent_t ev[NPHASE + 1];
+    for (int q = 0; q <= NPHASE; ++q) CK(cudaEventCreate(&ev[q]));
+    for (int q = 0; q < NPHASE; ++q) ms[q] = 0.0;
+    for (int s = 0; s < nsteps; ++s) {
+        if (step_enqueue(h, h.cur, ev) != 0) return GAM_ERR_CUDA;
+        h.cur ^= 1;
+        CK(cudaEventSynchronize(ev[NPHASE]));
+        for (int q = 0; q < NPHASE; ++q) {
+            float f = 0.f;
+            CK(cudaEventElapsedTime(&f, ev[q], ev[q + 1]));
+            ms[q] += f / nsteps;
+        }
+    }
+    for (int q = 0; q <= NPHASE; ++q) cudaEventDestroy(ev[q]);
+    int rc = download_scalars(G);
+    if (rc) return rc;
+    return status_code(G->h.hScal->sticky);
+}
+
+int gam_gpu_divb(gam_gpu_t* G, double* tot) {
+    if (!G || !tot) return GAM_ERR_ARG;
+    *tot = launch_divb(G->h, G->scratch, G->h.stream);
+    CK(cudaGetLastError());
+    return GAM_OK;
+}
+
+int gam_gpu_set_precision(gam_gpu_t* G, int mode) {
+    if (!G) return GAM_ERR_ARG;
+    if (mode != GAM_FP64 && mode != GAM_FP32FLUX) return GAM_ERR_ARG;
+    if (mode != G->h.prec) {
+        G->h.prec = mode;
+        destroy_graphs(G->h);
+    }
+    return GAM_OK;
+}
+
+int gam_gpu_fetch(gam_gpu_t* G, const char* name, double* out, long long n) {
+    if (!G || !name || !out) return GAM_ERR_ARG;
+    Handle& h = G->h;
+    const Lay& L = h.L;
+    Ext ce = cellExt(L), fe = faceExt(L);
+    double* pl[27];
+    int np = 0;
+    Ext e = ce;
+    std::string s(name);
+    StateP cS = h.S[h.cur], oS = h.S[h.cur ^ 1];
+    auto put = [&](double* const* src, int k) { for (int q = 0; q < k; ++q) pl[np++] = src[q]; };
+    if (s == "gas") put(cS.gas, 5);
+    else if (s == "magflux") { put(cS.mf, 3); e = fe; }
+    else if (s == "bxyz") put(cS.b, 3);
+    else if (s == "ogas") put(oS.gas, 5);
+    else if (s == "omagflux") { put(oS.mf, 3); e = fe; }
+    else if (s == "obxyz") put(oS.b, 3);
+    else if (s == "hgas") put(h.H.gas, 5);
+    else if (s == "hmagflux") { put(h.H.mf, 3); e = fe; }
+    else if (s == "hbxyz") put(h.H.b, 3);
+    else if (s == "efld") put(h.E, 3);
+    else if (s == "vf") put(h.Vf, 3);
+    else if (s == "dgash") put(h.dGasH, 5);
+    else if (s == "dgasm") put(h.dGasM, 3);
+    else if (s == "gflx") { for (int d = 0; d < 3; ++d) put(h.gflx[d], 5); }
+    else if (s == "mflx") { for (int d = 0; d < 3; ++d) put(h.mflx[d], 3); }
+    else if (s == "volume") put(&h.volume, 1);
+    else if (s == "xyzcc") put(h.xyzcc, 3);
+    else if (s == "xfc") { for (int d = 0; d < 3; ++d) put(h.xfc[d], 3); e = fe; }
+    else if (s == "di") put(&h.di, 1);
+    else if (s == "dj") put(&h.dj, 1);
+    else if (s == "dk") put(&h.dk, 1);
+    else if (s == "face") { put(h.face, 3); e = fe; }
+    else if (s == "edge") { put(h.edge, 3); e = fe; }
+    else if (s == "tf") { for (int d = 0; d < 3; ++d) put(h.Tf[d], 9); e = fe; }
+    else if (s == "te") { for (int d = 0; d < 3; ++d) put(h.Te[d], 9); e = fe; }
+    else if (s == "teb") { for (int d = 0; d < 3; ++d) put(h.Teb[d], 4); e = fe; }
+    else if (s == "xyz") { put(h.xyz, 3); e = fe; }
+    else return GAM_ERR_ARG;
+    if (n < (long long)np * e.n()) return GAM_ERR_ARG;
+    int rc = d2h_planes(G, pl, np, out, e);
+    if (rc) return rc;
+    CK(cudaStreamSynchronize(h.stream));
+    return GAM_OK;
+}
+
+void gam_gpu_destroy(gam_gpu_t* G) {
+    if (!G) return;
+    Handle& h = G->h;
+    if (h.stream) cudaStreamSynchronize(h.stream);
+    destroy_graphs(h);
+    if (h.pool) cudaFree(h.pool);
+    if (G->stage) cudaFree(G->stage);
+    if (G->scratch) cudaFree(G->scratch);
+    if (h.dScal) cudaFree(h.dScal);
+    if (h.hScal) cudaFreeHost(h.hScal);
+    if (h.stream && h.ownStream) cudaStreamDestroy(h.stream);
+    delete G;
+}
+
+}  // extern "C"

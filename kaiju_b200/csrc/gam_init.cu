@@ -1,0 +1,446 @@
+// Device-side set-up: Corners2Grid metrics (12-point Gauss-Legendre face and volume quadrature, face
+// and edge triads, 6th-order edge B transforms) and the OT2D / blast-wave initial conditions.
+// At 256^3 the reference's host quadrature is ~3e10 integrand evaluations; here every face, cell and
+// edge is one thread.
+#include <cstdio>
+#include "gam_common.cuh"
+#include "gam_step.cuh"
+#include "gam_init.cuh"
+
+namespace gam {
+
+// quadrature.F90:9-26
+__constant__ double c_gA[12] = {0.1252334085114689154724, 0.3678314989981801937527, 0.5873179542866174472967,
+                                0.7699026741943046870369, 0.9041172563704748566785, 0.9815606342467192506906,
+                                -0.1252334085114689154724, -0.3678314989981801937527, -0.5873179542866174472967,
+                                -0.7699026741943046870369, -0.9041172563704748566785, -0.9815606342467192506906};
+__constant__ double c_gW[12] = {0.2491470458134027850006, 0.233492536538354808761, 0.203167426723065921749,
+                                0.160078328543346226335, 0.1069393259953184309603, 0.0471753363865118271946,
+                                0.2491470458134027850006, 0.233492536538354808761, 0.203167426723065921749,
+                                0.160078328543346226335, 0.1069393259953184309603, 0.0471753363865118271946};
+
+struct Corners { const double* x[3]; };
+
+// gfortran's NORM2 expansion (scaled sum of squares)
+__device__ double norm2v3(const double* a) {
+    double scale = 0.0, ssq = 1.0;
+    for (int i = 0; i < 3; ++i) {
+        if (a[i] != 0.0) {
+            double ax = fabs(a[i]);
+            if (scale < ax) { ssq = 1.0 + ssq * sq(scale / ax); scale = ax; }
+            else ssq = ssq + sq(ax / scale);
+        }
+    }
+    return scale * sqrt(ssq);
+}
+__device__ __forceinline__ void cross3(const double* a, const double* b, double* c) {
+    c[0] = a[1] * b[2] - a[2] * b[1];
+    c[1] = a[2] * b[0] - a[0] * b[2];
+    c[2] = a[0] * b[1] - a[1] * b[0];
+}
+__device__ __forceinline__ void corner(const Lay& L, const Corners& X, int i, int j, int k, double* v) {
+    long long c = L.at(i, j, k);
+    v[0] = X.x[0][c]; v[1] = X.x[1][c]; v[2] = X.x[2][c];
+}
+
+struct Out3 { double* v[3]; };
+struct Out9 { double* v[9]; };
+
+__global__ void k_fill(double* a, long long n, double v) {
+    long long l = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (l < n) a[l] = v;
+}
+
+// Face areas, centres and triads (init.F90:852-911; GaussianFaceIntegral quadrature.F90:159-221)
+__global__ void k_grid_faces(Lay L, Corners X, int d, double* face, Out3 xfc, Out9 Tf) {
+    int DelI = d == 0, DelJ = d == 1, DelK = d == 2;
+    int ni = L.Ni + DelI, nj = L.Nj + DelJ, nk = L.Nk + DelK;
+    long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (t >= (long long)ni * nj * nk) return;
+    int i = (int)(t % ni);
+    long long q = t / ni;
+    int j = (int)(q % nj), k = (int)(q / nj);
+    double f0[3], f1[3], f2[3], f3[3];
+    corner(L, X, i, j, k, f0);
+    if (d == 0) { corner(L, X, i, j + 1, k, f1); corner(L, X, i, j, k + 1, f2); corner(L, X, i, j + 1, k + 1, f3); }
+    else if (d == 1) { corner(L, X, i, j, k + 1, f1); corner(L, X, i + 1, j, k, f2); corner(L, X, i + 1, j, k + 1, f3); }
+    else { corner(L, X, i + 1, j, k, f1); corner(L, X, i, j + 1, k, f2); corner(L, X, i + 1, j + 1, k, f3); }
+    double dx[3], dy[3], dz[3];
+    dx[0] = f1[0] - f0[0]; dx[1] = f2[0] - f0[0]; dx[2] = f3[0] + f0[0] - f2[0] - f1[0];
+    dy[0] = f1[1] - f0[1]; dy[1] = f2[1] - f0[1]; dy[2] = f3[1] + f0[1] - f2[1] - f1[1];
+    dz[0] = f1[2] - f0[2]; dz[1] = f2[2] - f0[2]; dz[2] = f3[2] + f0[2] - f2[2] - f1[2];
+    double fA = 0.0, fC[3] = {0.0, 0.0, 0.0};
+    for (int a = 0; a < 12; ++a)
+        for (int b = 0; b < 12; ++b) {
+            double eta = 0.5 * (1 + c_gA[a]), psi = 0.5 * (1 + c_gA[b]);
+            double w = c_gW[a] * c_gW[b];
+            double xp = f0[0] + dx[0] * eta + dx[1] * psi + dx[2] * eta * psi;
+            double yp = f0[1] + dy[0] * eta + dy[1] * psi + dy[2] * eta * psi;
+            double zp = f0[2] + dz[0] * eta + dz[1] * psi + dz[2] * eta * psi;
+            double etaV[3] = {dx[0] + dx[2] * psi, dy[0] + dy[2] * psi, dz[0] + dz[2] * psi};
+            double psiV[3] = {dx[1] + dx[2] * eta, dy[1] + dy[2] * eta, dz[1] + dz[2] * eta};
+            double cr[3];
+            cross3(etaV, psiV, cr);
+            double area = 0.25 * norm2v3(cr) * w;
+            fA = fA + area * 1.0;
+            fC[0] = fC[0] + area * xp; fC[1] = fC[1] + area * yp; fC[2] = fC[2] + area * zp;
+        }
+    long long c = L.at(i, j, k);
+    face[c] = fA;
+    for (int x = 0; x < 3; ++x) xfc.v[x][c] = fC[x] / fA;
+    double a0[3], a1[3], a2[3], a3[3], dT1[3], dT2[3];
+    if (d == 0) {
+        corner(L, X, i, j + 1, k + 1, a0); corner(L, X, i, j, k + 1, a1); corner(L, X, i, j + 1, k, a2); corner(L, X, i, j, k, a3);
+        for (int x = 0; x < 3; ++x) dT1[x] = 0.5 * (a0[x] - a1[x]) + 0.5 * (a2[x] - a3[x]);
+        double b1[3];
+        corner(L, X, i, j + 1, k, b1);
+        for (int x = 0; x < 3; ++x) dT2[x] = 0.5 * (a0[x] - b1[x]) + 0.5 * (a1[x] - a3[x]);
+    } else if (d == 1) {
+        corner(L, X, i + 1, j, k + 1, a0); corner(L, X, i + 1, j, k, a1); corner(L, X, i, j, k + 1, a2); corner(L, X, i, j, k, a3);
+        for (int x = 0; x < 3; ++x) dT1[x] = 0.5 * (a0[x] - a1[x]) + 0.5 * (a2[x] - a3[x]);
+        for (int x = 0; x < 3; ++x) dT2[x] = 0.5 * (a0[x] - a2[x]) + 0.5 * (a1[x] - a3[x]);
+    } else {
+        corner(L, X, i + 1, j + 1, k, a0); corner(L, X, i, j + 1, k, a1); corner(L, X, i + 1, j, k, a2); corner(L, X, i, j, k, a3);
+        for (int x = 0; x < 3; ++x) dT1[x] = 0.5 * (a0[x] - a1[x]) + 0.5 * (a2[x] - a3[x]);
+        for (int x = 0; x < 3; ++x) dT2[x] = 0.5 * (a0[x] - a2[x]) + 0.5 * (a1[x] - a3[x]);
+    }
+    double cr[3], eN[3], eT1[3], eT2[3];
+    cross3(dT1, dT2, cr);
+    double ncr = norm2v3(cr);
+    for (int x = 0; x < 3; ++x) eN[x] = cr[x] / ncr;
+    double nT2 = norm2v3(dT2);
+    for (int x = 0; x < 3; ++x) eT2[x] = dT2[x] / nT2;
+    cross3(eT2, eN, cr);
+    ncr = norm2v3(cr);
+    for (int x = 0; x < 3; ++x) eT1[x] = cr[x] / ncr;
+    for (int x = 0; x < 3; ++x) { Tf.v[x][c] = eN[x]; Tf.v[3 + x][c] = eT1[x]; Tf.v[6 + x][c] = eT2[x]; }
+}
+
+// DetJ (math.F90:470-478)
+__device__ __forceinline__ double detJ(const double J[3][3]) {
+    return J[0][0] * (J[1][1] * J[2][2] - J[1][2] * J[2][1]) - J[0][1] * (J[1][0] * J[2][2] - J[1][2] * J[2][0]) +
+           J[0][2] * (J[1][0] * J[2][1] - J[1][1] * J[2][0]);
+}
+
+// GaussianVolumeIntegral (quadrature.F90:42-100) of W over the hexahedron xyzC (corner order of cellCoords)
+template <typename F>
+__device__ void volumeIntegral(const double (*xyzC)[3], F W, double* wInt) {
+    const int iS[8] = {-1, +1, +1, -1, -1, +1, +1, -1}, jS[8] = {-1, -1, +1, +1, -1, -1, +1, +1},
+              kS[8] = {-1, -1, -1, -1, +1, +1, +1, +1};
+    for (int v = 0; v < 5; ++v) wInt[v] = 0.0;
+    for (int a = 0; a < 12; ++a)
+        for (int b = 0; b < 12; ++b)
+            for (int cq = 0; cq < 12; ++cq) {
+                double wijk = c_gW[a] * c_gW[b] * c_gW[cq];
+                double xp[3], J[3][3];
+                for (int x = 0; x < 3; ++x) {
+                    double s = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
+                    for (int pp = 0; pp < 8; ++pp) {
+                        double is_ = iS[pp] < 0 ? (1 - c_gA[a]) : (1 + c_gA[a]);
+                        double js_ = jS[pp] < 0 ? (1 - c_gA[b]) : (1 + c_gA[b]);
+                        double ks_ = kS[pp] < 0 ? (1 - c_gA[cq]) : (1 + c_gA[cq]);
+                        s = s + xyzC[pp][x] * (is_ * js_ * ks_);
+                        s1 = s1 + xyzC[pp][x] * (iS[pp] * js_ * ks_);
+                        s2 = s2 + xyzC[pp][x] * (is_ * jS[pp] * ks_);
+                        s3 = s3 + xyzC[pp][x] * (is_ * js_ * kS[pp]);
+                    }
+                    xp[x] = 0.125 * s;
+                    J[x][0] = 0.125 * s1; J[x][1] = 0.125 * s2; J[x][2] = 0.125 * s3;
+                }
+                double dJ = fabs(detJ(J));
+                double Wp[5];
+                W(xp[0], xp[1], xp[2], Wp);
+                for (int v = 0; v < 5; ++v) wInt[v] = wInt[v] + dJ * wijk * Wp[v];
+            }
+}
+
+__device__ void cellCorners(const Lay& L, const Corners& X, int i, int j, int k, double (*xyzC)[3]) {
+    const int di[8] = {0, 1, 1, 0, 0, 1, 1, 0}, dj[8] = {0, 0, 1, 1, 0, 0, 1, 1}, dk[8] = {0, 0, 0, 0, 1, 1, 1, 1};
+    for (int pp = 0; pp < 8; ++pp) corner(L, X, i + di[pp], j + dj[pp], k + dk[pp], xyzC[pp]);
+}
+
+struct CellDVf {
+    __device__ void operator()(double x, double y, double z, double* W) const { W[0] = 1; W[1] = x; W[2] = y; W[3] = z; W[4] = 0; }
+};
+
+// Cell volumes and barycentres (init.F90:922-948)
+__global__ void k_grid_volumes(Lay L, Corners X, double* vol, Out3 xyzcc) {
+    long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (t >= (long long)L.Ni * L.Nj * L.Nk) return;
+    int i = (int)(t % L.Ni);
+    long long q = t / L.Ni;
+    int j = (int)(q % L.Nj), k = (int)(q / L.Nj);
+    double xyzC[8][3], w[5];
+    cellCorners(L, X, i, j, k, xyzC);
+    volumeIntegral(xyzC, CellDVf(), w);
+    long long c = L.at(i, j, k);
+    vol[c] = w[0];
+    for (int x = 0; x < 3; ++x) xyzcc.v[x][c] = w[1 + x] / w[0];
+}
+// di,dj,dk = volume / larger face area (init.F90:951-965)
+__global__ void k_grid_dl(Lay L, const double* vol, Out3 face, double* di, double* dj, double* dk) {
+    long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (t >= (long long)L.Ni * L.Nj * L.Nk) return;
+    int i = (int)(t % L.Ni);
+    long long q = t / L.Ni;
+    int j = (int)(q % L.Nj), k = (int)(q / L.Nj);
+    long long c = L.at(i, j, k);
+    double fA = dmax(face.v[0][c + 1], face.v[0][c]);
+    di[c] = vol[c] / fA;
+    fA = dmax(face.v[1][c + L.P], face.v[1][c]);
+    dj[c] = vol[c] / fA;
+    fA = dmax(face.v[2][c + (long long)L.P * L.Q], face.v[2][c]);
+    dk[c] = vol[c] / fA;
+}
+
+// Edge lengths and edge triads (init.F90:978-1048)
+__global__ void k_grid_edges(Lay L, Corners X, int d, int i0, int ni, int j0, int nj, int k0, int nk, double* edge,
+                             Out9 Te) {
+    long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (t >= (long long)ni * nj * nk) return;
+    int i = i0 + (int)(t % ni);
+    long long q = t / ni;
+    int j = j0 + (int)(q % nj), k = k0 + (int)(q / nj);
+    double p0[3], p1[3], a[3], b[3], c2[3], d2[3], dEdge[3], eAvg[3];
+    corner(L, X, i, j, k, p0);
+    if (d == 0) {
+        corner(L, X, i + 1, j, k, p1);
+        corner(L, X, i, j, k + 1, a); corner(L, X, i, j, k - 1, b); corner(L, X, i + 1, j, k + 1, c2); corner(L, X, i + 1, j, k - 1, d2);
+    } else if (d == 1) {
+        corner(L, X, i, j + 1, k, p1);
+        corner(L, X, i + 1, j, k, a); corner(L, X, i - 1, j, k, b); corner(L, X, i + 1, j + 1, k, c2); corner(L, X, i - 1, j + 1, k, d2);
+    } else {
+        corner(L, X, i, j, k + 1, p1);
+        corner(L, X, i, j + 1, k, a); corner(L, X, i, j - 1, k, b); corner(L, X, i, j + 1, k + 1, c2); corner(L, X, i, j - 1, k + 1, d2);
+    }
+    for (int x = 0; x < 3; ++x) { dEdge[x] = p1[x] - p0[x]; eAvg[x] = 0.5 * (a[x] - b[x] + c2[x] - d2[x]); }
+    double nE = norm2v3(dEdge), eN[3], eT1[3], eT2[3], cr[3];
+    for (int x = 0; x < 3; ++x) eN[x] = dEdge[x] / nE;
+    cross3(eAvg, eN, cr);
+    double ncr = norm2v3(cr);
+    for (int x = 0; x < 3; ++x) eT1[x] = cr[x] / ncr;
+    cross3(eN, eT1, cr);
+    ncr = norm2v3(cr);
+    for (int x = 0; x < 3; ++x) eT2[x] = cr[x] / ncr;
+    long long c = L.at(i, j, k);
+    edge[c] = norm2v3(dEdge);
+    for (int x = 0; x < 3; ++x) { Te.v[x][c] = eN[x]; Te.v[3 + x][c] = eT1[x]; Te.v[6 + x][c] = eT2[x]; }
+}
+
+// ebGeom (init.F90:1083-1145): face normals of the dT1 faces, interpolated with the 6th-order
+// weights along dT2 onto the dNorm edge and projected on the edge's T1/T2.
+__global__ void k_grid_teb(Lay L, const double* faceT1, const double* N0, const double* N1, const double* N2,
+                           const double* T1x, const double* T1y, const double* T1z, const double* T2x,
+                           const double* T2y, const double* T2z, int dT2, double* out0, double* out1) {
+    long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    int ni = L.Nip + 1, nj = L.Njp + 1, nk = L.Nkp + 1;
+    if (t >= (long long)ni * nj * nk) return;
+    int i = L.is() + (int)(t % ni);
+    long long q = t / ni;
+    int j = L.js() + (int)(q % nj), k = L.ks() + (int)(q / nj);
+    long long c = L.at(i, j, k), s = L.stride(dT2);
+    const double w6[8] = {0.0 / 60.0, 1.0 / 60.0, -8.0 / 60.0, 37.0 / 60.0, 37.0 / 60.0, -8.0 / 60.0, 1.0 / 60.0, 0.0 / 60.0};
+    double fAi = 0.0, Nx = 0.0, Ny = 0.0, Nz = 0.0;
+    for (int n = 0; n < 8; ++n) {
+        long long cn = c + (n - 4) * s;
+        double f = faceT1[cn];
+        fAi = fAi + w6[n] * f;
+        Nx = Nx + (N0[cn] * f) * w6[n];
+        Ny = Ny + (N1[cn] * f) * w6[n];
+        Nz = Nz + (N2[cn] * f) * w6[n];
+    }
+    Nx = Nx / fAi; Ny = Ny / fAi; Nz = Nz / fAi;
+    double dxT = Nx * T1x[c] + Ny * T1y[c] + Nz * T1z[c];
+    double dyT = Nx * T2x[c] + Ny * T2y[c] + Nz * T2z[c];
+    double dScl = sqrt(sq(dxT) + sq(dyT));
+    if (dScl <= TINY) dScl = 1.0;
+    out0[c] = dxT / dScl;
+    out1[c] = dyT / dScl;
+}
+
+// ------------------------------------------------------------------------------------ initial conditions
+// initOT2D (prob.F90:74-119)
+__global__ void k_ic_ot2d(Lay L, Par p, GridP g, StateP s) {
+    int ni = L.Nip + 1, nj = L.Njp + 1, nk = L.Nkp + 1;
+    long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (t >= (long long)ni * nj * nk) return;
+    int i = L.is() + (int)(t % ni);
+    long long q = t / ni;
+    int j = L.js() + (int)(q % nj), k = L.ks() + (int)(q / nj);
+    long long c = L.at(i, j, k);
+    double Rho0 = 25.0 / (36.0 * PI), P0 = 5 / (12.0 * PI), B0 = 1 / sqrt(4.0 * PI);
+    double xc = g.xyzcc[0][c], yc = g.xyzcc[1][c];
+    double Vx = -sin(2 * PI * yc), Vy = sin(2 * PI * xc), Vz = 0.0;
+    double KinE = 0.5 * Rho0 * (sq(Vx) + sq(Vy) + sq(Vz));
+    s.gas[0][c] = Rho0;
+    s.gas[1][c] = Vx * Rho0; s.gas[2][c] = Vy * Rho0; s.gas[3][c] = Vz * Rho0;
+    s.gas[4][c] = KinE + P0 / (p.gamma - 1);
+    s.mf[0][c] = (-B0 * sin(2 * PI * yc)) * g.face[0][c];
+    s.mf[1][c] = (B0 * sin(4 * PI * xc)) * g.face[1][c];
+    s.mf[2][c] = 0.0;
+}
+
+// initBW with the deck defaults (prob.F90:190-298): D0=1, P0=0.1, pRat=100, dRat=1, rC=0.1, B0=1
+struct BWGas {
+    __device__ void operator()(double x, double y, double z, double* W) const {
+        double R = sqrt(sq(x - 0.0) + sq(y - 0.0) + sq(z - 0.0));
+        double D = 1.0, P = 0.1;
+        if (R <= 0.1) { D = 1.0 * D; P = 100.0 * P; }
+        W[0] = D; W[1] = 0.0; W[2] = 0.0; W[3] = 0.0; W[4] = P;
+    }
+};
+// GasIC2State (gridutils.F90:144-189) on active cells
+__global__ void k_ic_bw_gas(Lay L, Par p, Corners X, const double* vol, StateP s) {
+    long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (t >= (long long)L.Nip * L.Njp * L.Nkp) return;
+    int i = L.is() + (int)(t % L.Nip);
+    long long q = t / L.Nip;
+    int j = L.js() + (int)(q % L.Njp), k = L.ks() + (int)(q / L.Njp);
+    double xyzC[8][3], w[5];
+    cellCorners(L, X, i, j, k, xyzC);
+    volumeIntegral(xyzC, BWGas(), w);
+    long long c = L.at(i, j, k);
+    double dV = vol[c];
+    for (int v = 0; v < 5; ++v) w[v] = w[v] / dV;
+    double D = w[0], Mx = D * w[1], My = D * w[2], Mz = D * w[3], P = w[4];
+    double KinE = 0.5 * (sq(Mx) + sq(My) + sq(Mz)) / D;
+    double IntE = P / (p.gamma - 1.0);
+    s.gas[0][c] = D; s.gas[1][c] = Mx; s.gas[2][c] = My; s.gas[3][c] = Mz; s.gas[4][c] = IntE + KinE;
+}
+// VectorPot2Flux (gridutils.F90:193-237), A = (0, bSclz*x, bScl*(y-x)), bScl = 1/sqrt(2.0) in single
+// precision as the reference literal, bSclz = 0; edge integrals with the 12-point rule
+__device__ double edgeIntegralA(const double* e1, const double* e2, double bScl) {
+    double dR2[3], xBar[3], eInt[3] = {0.0, 0.0, 0.0};
+    for (int x = 0; x < 3; ++x) { dR2[x] = 0.5 * (e2[x] - e1[x]); xBar[x] = 0.5 * (e2[x] + e1[x]); }
+    for (int a = 0; a < 12; ++a) {
+        double xp[3];
+        for (int x = 0; x < 3; ++x) xp[x] = xBar[x] + c_gA[a] * dR2[x];
+        double Ap[3] = {0.0, 0.0 * xp[0], bScl * (xp[1] - xp[0])};
+        for (int x = 0; x < 3; ++x) eInt[x] = eInt[x] + 0.5 * c_gW[a] * Ap[x];
+    }
+    double dR[3] = {e1[0] - e2[0], e1[1] - e2[1], e1[2] - e2[2]};
+    return eInt[0] * dR[0] + eInt[1] * dR[1] + eInt[2] * dR[2];
+}
+__global__ void k_ic_bw_la(Lay L, Corners X, Out3 lA, double bScl) {
+    int ni = L.Ni - 1, nj = L.Nj - 1, nk = L.Nk - 1;
+    long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (t >= (long long)ni * nj * nk) return;
+    int i = (int)(t % ni);
+    long long q = t / ni;
+    int j = (int)(q % nj), k = (int)(q / nj);
+    double e0[3], eI[3], eJ[3], eK[3];
+    corner(L, X, i, j, k, e0); corner(L, X, i + 1, j, k, eI); corner(L, X, i, j + 1, k, eJ); corner(L, X, i, j, k + 1, eK);
+    long long c = L.at(i, j, k);
+    lA.v[0][c] = edgeIntegralA(eI, e0, bScl);
+    lA.v[1][c] = edgeIntegralA(eJ, e0, bScl);
+    lA.v[2][c] = edgeIntegralA(eK, e0, bScl);
+}
+__global__ void k_ic_bw_flux(Lay L, Out3 lA, StateP s) {
+    int ni = L.Ni - 1, nj = L.Nj - 1, nk = L.Nk - 1;
+    long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (t >= (long long)ni * nj * nk) return;
+    int i = (int)(t % ni);
+    long long q = t / ni;
+    int j = (int)(q % nj), k = (int)(q / nj);
+    long long c = L.at(i, j, k), cj = c + L.P, ck = c + (long long)L.P * L.Q;
+    const double* A0 = lA.v[0]; const double* A1 = lA.v[1]; const double* A2 = lA.v[2];
+    s.mf[0][c] = A1[c] - A1[ck] + A2[cj] - A2[c];
+    s.mf[1][c] = -(A0[c] - A0[ck] + A2[c + 1] - A2[c]);
+    s.mf[2][c] = A0[c] - A0[cj] + A1[c + 1] - A1[c];
+}
+
+__global__ void k_copy_state(long long E, StateP src, StateP dst) {
+    long long l = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (l >= E) return;
+    for (int v = 0; v < 5; ++v) dst.gas[v][l] = src.gas[v][l];
+    for (int x = 0; x < 3; ++x) { dst.mf[x][l] = src.mf[x][l]; dst.b[x][l] = src.b[x][l]; }
+}
+__global__ void k_set_otime(Scal* sc) { sc->otime = sc->time - sc->dt; }
+
+static inline unsigned nb(long long n, int b) { return (unsigned)((n + b - 1) / b); }
+
+int init_grid_from_corners(Handle& h) {
+    const Lay& L = h.L;
+    cudaStream_t st = h.stream;
+    Corners X = {{h.xyz[0], h.xyz[1], h.xyz[2]}};
+    // reference initial values: face = 1, edge = 1, Teb = 1, the rest 0
+    for (int d = 0; d < 3; ++d) {
+        k_fill<<<nb(L.E, 256), 256, 0, st>>>(h.face[d], L.E, 1.0);
+        k_fill<<<nb(L.E, 256), 256, 0, st>>>(h.edge[d], L.E, 1.0);
+        for (int q = 0; q < 4; ++q) k_fill<<<nb(L.E, 256), 256, 0, st>>>(h.Teb[d][q], L.E, 1.0);
+    }
+    for (int d = 0; d < 3; ++d) {
+        Out3 xf = {{h.xfc[d][0], h.xfc[d][1], h.xfc[d][2]}};
+        Out9 tf;
+        for (int q = 0; q < 9; ++q) tf.v[q] = h.Tf[d][q];
+        long long n = (long long)(L.Ni + (d == 0)) * (L.Nj + (d == 1)) * (L.Nk + (d == 2));
+        k_grid_faces<<<nb(n, 128), 128, 0, st>>>(L, X, d, h.face[d], xf, tf);
+    }
+    long long nc = (long long)L.Ni * L.Nj * L.Nk;
+    Out3 cc = {{h.xyzcc[0], h.xyzcc[1], h.xyzcc[2]}};
+    k_grid_volumes<<<nb(nc, 128), 128, 0, st>>>(L, X, h.volume, cc);
+    Out3 fc = {{h.face[0], h.face[1], h.face[2]}};
+    k_grid_dl<<<nb(nc, 256), 256, 0, st>>>(L, h.volume, fc, h.di, h.dj, h.dk);
+    for (int d = 0; d < 3; ++d) {
+        int is = 0, ie = L.Ni, js = 0, je = L.Nj, ks = 0, ke = L.Nk;   // maximal bounds (corner index space)
+        if (d == 0) { ie = L.Ni - 1; ks = 1; ke = L.Nk - 1; }
+        else if (d == 1) { je = L.Nj - 1; is = 1; ie = L.Ni - 1; }
+        else { ke = L.Nk - 1; js = 1; je = L.Nj - 1; }
+        Out9 te;
+        for (int q = 0; q < 9; ++q) te.v[q] = h.Te[d][q];
+        long long n = (long long)(ie - is + 1) * (je - js + 1) * (ke - ks + 1);
+        k_grid_edges<<<nb(n, 128), 128, 0, st>>>(L, X, d, is, ie - is + 1, js, je - js + 1, ks, ke - ks + 1, h.edge[d], te);
+    }
+    for (int dN = 0; dN < 3; ++dN) {
+        int T1 = (dN == 0) ? 1 : (dN == 1 ? 2 : 0);
+        int T2 = (dN == 0) ? 2 : (dN == 1 ? 0 : 1);
+        long long n = (long long)(L.Nip + 1) * (L.Njp + 1) * (L.Nkp + 1);
+        for (int pass = 0; pass < 2; ++pass) {
+            int dT1 = pass == 0 ? T1 : T2, dT2 = pass == 0 ? T2 : T1;
+            k_grid_teb<<<nb(n, 128), 128, 0, st>>>(L, h.face[dT1], h.Tf[dT1][0], h.Tf[dT1][1], h.Tf[dT1][2],
+                                                   h.Te[dN][3], h.Te[dN][4], h.Te[dN][5], h.Te[dN][6], h.Te[dN][7],
+                                                   h.Te[dN][8], dT2, h.Teb[dN][2 * pass], h.Teb[dN][2 * pass + 1]);
+        }
+    }
+    h.launches += 27;
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) { std::fprintf(stderr, "gamgpu: grid init: %s\n", cudaGetErrorString(e)); return 3; }
+    return 0;
+}
+
+int init_problem(Handle& h, int ic) {
+    const Lay& L = h.L;
+    cudaStream_t st = h.stream;
+    GridP g = h.gridP();
+    StateP s = h.S[h.cur];
+    if (ic == 0) {
+        long long n = (long long)(L.Nip + 1) * (L.Njp + 1) * (L.Nkp + 1);
+        k_ic_ot2d<<<nb(n, 256), 256, 0, st>>>(L, h.p, g, s);
+        h.launches++;
+    } else {
+        Corners X = {{h.xyz[0], h.xyz[1], h.xyz[2]}};
+        long long n = (long long)L.Nip * L.Njp * L.Nkp;
+        k_ic_bw_gas<<<nb(n, 128), 128, 0, st>>>(L, h.p, X, h.volume, s);
+        if (h.p.doMHD) {
+            Out3 lA = {{h.E[0], h.E[1], h.E[2]}};   // E planes as scratch for the edge integrals of A
+            double bScl = 1.0 / (double)sqrtf(2.0f);
+            long long ne = (long long)(L.Ni - 1) * (L.Nj - 1) * (L.Nk - 1);
+            k_ic_bw_la<<<nb(ne, 128), 128, 0, st>>>(L, X, lA, bScl);
+            k_ic_bw_flux<<<nb(ne, 256), 256, 0, st>>>(L, lA, s);
+            h.launches += 2;
+        }
+        h.launches++;
+    }
+    // CalcGridInfo tail (init.F90:204-244)
+    if (h.p.doMHD) launch_bflux2fld(h, s, st);
+    launch_bcs(h, s, st);
+    k_copy_state<<<nb(L.E, 256), 256, 0, st>>>(L.E, s, h.S[h.cur ^ 1]);
+    launch_calcdt(h, s, 1, st);
+    k_set_otime<<<1, 1, 0, st>>>(h.dScal);
+    h.launches += 2;
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) { std::fprintf(stderr, "gamgpu: problem init: %s\n", cudaGetErrorString(e)); return 3; }
+    return 0;
+}
+
+}  // namespace gam

@@ -1,0 +1,891 @@
+// GAMERA ideal-MHD step on sm_100a: predictor, constrained-transport E field, interface fluxes,
+// update, CFL dt and boundary conditions. One stepGamera (src/gamera/gamapp.F90:73-94) is a fixed
+// sequence of kernels on one stream; with the time scalars on the device the sequence is captured
+// once per buffer parity as a CUDA graph and replayed.
+//
+// The flux and E-field kernels compute the reconstruction, limiter and kinetic fluxes in the
+// arithmetic type T (double for the plain path, float for the FP32-flux path); state, accumulation,
+// CT update, C2P with floors and the dt reduction stay FP64 in both.
+#include <cstdio>
+#include <cmath>
+#include "gam_common.cuh"
+#include "gam_step.cuh"
+
+namespace gam {
+
+struct Reg {
+    int i0, ni, j0, nj, k0, nk;
+    __host__ __device__ long long n() const { return (long long)ni * nj * nk; }
+};
+__device__ __forceinline__ bool reg_ijk(const Reg& r, long long t, int& i, int& j, int& k) {
+    if (t >= r.n()) return false;
+    i = r.i0 + (int)(t % r.ni);
+    long long q = t / r.ni;
+    j = r.j0 + (int)(q % r.nj);
+    k = r.k0 + (int)(q / r.nj);
+    return true;
+}
+static inline Reg mkreg(int i0, int i1, int j0, int j1, int k0, int k1) {
+    Reg r;
+    r.i0 = i0; r.ni = i1 - i0 + 1; r.j0 = j0; r.nj = j1 - j0 + 1; r.k0 = k0; r.nk = k1 - k0 + 1;
+    return r;
+}
+static inline unsigned nblk(long long n, int b) { return (unsigned)((n + b - 1) / b); }
+
+struct PrimP { double* w[5]; };
+struct Vec3P { double* v[3]; };
+struct FluxP { double* g[5]; double* m[3]; };
+
+// ================================================================================ step scalars
+// AdvanceMHD trap (mhdgroup.F90:26-28) and the predictor time factors (:459)
+__global__ void k_step_begin(Scal* sc) {
+    if (fabs(sc->otime - sc->time) < TINY) sc->otime = sc->time - sc->dt;
+    sc->pdt = 0.5 * sc->dt;
+    sc->odt = sc->time - sc->otime;
+    sc->dtMinBits = 0x7FF0000000000000ull;  // +inf
+    sc->nanCount = 0u;
+}
+
+// ================================================================================ predictor
+// Predictor magFlux part (mhdgroup.F90:466-488): AB2 on every face element, ghosts included
+__global__ void k_predict_faces(long long E, Vec3P mf, Vec3P omf, Vec3P hmf, const Scal* sc) {
+    long long l = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (l >= E) return;
+    double pdt = sc->pdt, odt = sc->odt;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+        double Q = mf.v[c][l], oQ = omf.v[c][l];
+        double dQ = (Q - oQ) / odt;
+        hmf.v[c][l] = Q + pdt * dQ;
+    }
+}
+
+// bFlux2Fld of the half state + PredictCell (mhdgroup.F90:492-518, 529-563) on every cell, plus the
+// BlockCon2Prim primitives of the half state and of state n used by the interface reconstruction.
+__global__ void k_predict_cells(Lay L, Par p, GridP g, StateP n, StateP o, StateP h, PrimP Wh, PrimP Wn,
+                                const Scal* sc) {
+    Reg r = {0, L.Ni, 0, L.Nj, 0, L.Nk};
+    int i, j, k;
+    if (!reg_ijk(r, blockIdx.x * (long long)blockDim.x + threadIdx.x, i, j, k)) return;
+    long long c = L.at(i, j, k);
+    double B[3] = {0.0, 0.0, 0.0};
+    cellBxyz(L, g, h.mf, c, B);
+    h.b[0][c] = B[0]; h.b[1][c] = B[1]; h.b[2][c] = B[2];
+    double Q[5], oQ[5], W[5], oW[5], pW[5], pQ[5];
+#pragma unroll
+    for (int v = 0; v < 5; ++v) { Q[v] = n.gas[v][c]; oQ[v] = o.gas[v][c]; }
+    cellC2P(p, oQ, oW);
+    cellC2P(p, Q, W);
+    double pdt = sc->pdt, odt = sc->odt;
+#pragma unroll
+    for (int v = 0; v < 5; ++v) { double dQ = (W[v] - oW[v]) / odt; pW[v] = W[v] + pdt * dQ; }
+    pW[0] = dmax(pW[0], p.dFloor);
+    pW[4] = dmax(pW[4], p.pFloor);
+    cellP2C(p, pW, pQ);
+#pragma unroll
+    for (int v = 0; v < 5; ++v) h.gas[v][c] = pQ[v];
+    double w[5];
+    blockC2P(p, pQ, w);
+#pragma unroll
+    for (int v = 0; v < 5; ++v) Wh.w[v][c] = w[v];
+    blockC2P(p, Q, w);
+#pragma unroll
+    for (int v = 0; v < 5; ++v) Wn.w[v][c] = w[v];
+}
+
+// ================================================================================ electric field
+// Mom2Face (fields.F90:235-285): volume-weighted Central8 of rho*v along dT1 onto the dT1 faces
+__global__ void k_mom2face(Lay L, Par p, GridP g, StateP h, Vec3P Vf, Reg r, int dT1) {
+    int i, j, k;
+    if (!reg_ijk(r, blockIdx.x * (long long)blockDim.x + threadIdx.x, i, j, k)) return;
+    long long c = L.at(i, j, k), s = L.stride(dT1);
+    double VolB[8], VelB[3][8];
+#pragma unroll
+    for (int n = 0; n < 8; ++n) {
+        long long cn = c + (n - 4) * s;
+        double vol = g.volume[cn];
+        double den = dmax(h.gas[0][cn], p.dFloor);
+        VolB[n] = vol;
+#pragma unroll
+        for (int x = 0; x < 3; ++x) VelB[x][n] = vol * h.gas[1 + x][cn] / den;
+    }
+    double dV = dmax(central8<double>(VolB), TINY);
+#pragma unroll
+    for (int x = 0; x < 3; ++x) Vf.v[x][c] = central8<double>(VelB[x]) / dV;
+}
+
+// EdgeLRs (fields.F90:288-362): limited L/R of flux/area of the dA faces along dS, times the area
+template <typename T>
+__device__ __forceinline__ void edgeLR(const Lay& L, const Par& p, const GridP& g, double* const* hmf,
+                                       double* const* nmf, long long c, int dA, int dS, T& bL, T& bR, T& fA) {
+    long long s = L.stride(dS);
+    const double* A = g.face[dA];
+    T Ab[8], Mb[8], nMb[4];
+#pragma unroll
+    for (int n = 0; n < 8; ++n) {
+        double a = A[c + (n - 4) * s];
+        Ab[n] = T(a);
+        Mb[n] = T(hmf[dA][c + (n - 4) * s] / dmax(a, TINY));
+    }
+    double* const* lim = p.doLFMLim ? nmf : hmf;
+#pragma unroll
+    for (int m = 0; m < 4; ++m) {
+        double a = A[c + (m - 2) * s];
+        nMb[m] = T(lim[dA][c + (m - 2) * s] / dmax(a, TINY));
+    }
+    T Vi = central8<T>(Ab);
+    T l, rr;
+    getLR<T>(p.rmeth, T(p.pdmb), Ab, Mb, nMb, Vi, l, rr);
+    fA = Vi;   // dot_product(interpWgt, AreaB) is the same sum as Central8(VolB) with VolB = AreaB
+    bL = l * fA;
+    bR = rr * fA;
+}
+
+// GetCornerV/GetCornerD/GetCornerB and the EMF (fields.F90:186-225, 365-517) on the eD edges
+template <typename T>
+__global__ void k_edge_emf(Lay L, Par p, GridP g, StateP n, StateP h, Vec3P Vf, double* Eout, Reg r, int eD,
+                           int dT1, int dT2, const Scal* sc) {
+    int i, j, k;
+    if (!reg_ijk(r, blockIdx.x * (long long)blockDim.x + threadIdx.x, i, j, k)) return;
+    long long c = L.at(i, j, k);
+    // GetCornerV: area-weighted Central8 of the face velocities along dT2, mapped with Te
+    long long s2 = L.stride(dT2);
+    T Ab[8];
+#pragma unroll
+    for (int m = 0; m < 8; ++m) Ab[m] = T(g.face[dT1][c + (m - 4) * s2]);
+    T dA = central8<T>(Ab);
+    dA = dA > T(TINY) ? dA : T(TINY);
+    T Vc[3];
+#pragma unroll
+    for (int x = 0; x < 3; ++x) {
+        T s = T(0);
+#pragma unroll
+        for (int m = 0; m < 8; ++m) s = s + T(wC8(m)) * (Ab[m] * T(Vf.v[x][c + (m - 4) * s2]));
+        Vc[x] = s / dA;
+    }
+    T v1 = Vc[0] * T(g.Te[eD][3][c]) + Vc[1] * T(g.Te[eD][4][c]) + Vc[2] * T(g.Te[eD][5][c]);
+    T v2 = Vc[0] * T(g.Te[eD][6][c]) + Vc[1] * T(g.Te[eD][7][c]) + Vc[2] * T(g.Te[eD][8][c]);
+    T vDiff = sqrt(v1 * v1 + v2 * v2);
+    // GetCornerD: 4-point average of the half-state density around the edge (getNormalPlane)
+    int e1 = (eD == IDIR) ? JDIR : IDIR;
+    int e2 = (eD == KDIR) ? JDIR : KDIR;
+    long long se1 = L.stride(e1), se2 = L.stride(e2);
+    T Dc = T(0.25 * (h.gas[0][c] + h.gas[0][c - se1] + h.gas[0][c - se2] + h.gas[0][c - se1 - se2]));
+    // GetCornerB
+    T bT1L, bT1R, fA1, bT2L, bT2R, fA2;
+    edgeLR<T>(L, p, g, h.mf, n.mf, c, dT1, dT2, bT1L, bT1R, fA1);
+    edgeLR<T>(L, p, g, h.mf, n.mf, c, dT2, dT1, bT2L, bT2R, fA2);
+    T xni = T(g.Teb[eD][0][c]), yni = T(g.Teb[eD][1][c]), xnj = T(g.Teb[eD][2][c]), ynj = T(g.Teb[eD][3][c]);
+    T detT = T(1) / (xni * ynj - xnj * yni);
+    T bT1 = T(0.5) * (bT1L + bT1R) / fA1;
+    T bT2 = T(0.5) * (bT2L + bT2R) / fA2;
+    T db1 = (bT1R - bT1L) / fA1;
+    T db2 = (bT2R - bT2L) / fA2;
+    T Jd = db2 - db1;
+    T b1 = detT * (ynj * bT1 - yni * bT2);
+    T b2 = detT * (-(xnj * bT1) + xni * bT2);
+    // diffusive speed and EMF
+    T vA = sqrt(b1 * b1 + b2 * b2) / sqrt(Dc);
+    if (p.doBoris) { T Ca = T(p.Ca); vA = Ca * vA / sqrt(Ca * Ca + vA * vA); }
+    vDiff = vDiff + vA;
+    double edg = g.edge[eD][c];
+    T lim = T(p.CFL * edg / sc->dt);
+    vDiff = vDiff < lim ? vDiff : lim;
+    T e = -(v1 * b2 - v2 * b1) + T(p.Vd0) * vDiff * Jd;
+    Eout[c] = double(e) * edg;
+}
+
+// ================================================================================ fluxes
+// One-sided gas kinetic flux (stress.F90:432-511)
+template <typename T>
+__device__ __forceinline__ void gasKin(T gm1, T sg, const T* W, const T* Tf, T* gF, T* dW) {
+    T D = W[0], Vx = W[1], Vy = W[2], Vz = W[3], P = W[4];
+    T E = T(0.5) * D * (Vx * Vx + Vy * Vy + Vz * Vz) + P / gm1;
+    T lambda = D / (T(2) * P);
+    T Vn = Tf[0] * Vx + Tf[1] * Vy + Tf[2] * Vz;
+    T Vt1 = Tf[3] * Vx + Tf[4] * Vy + Tf[5] * Vz;
+    T Vt2 = Tf[6] * Vx + Tf[7] * Vy + Tf[8] * Vz;
+    T Vn0 = T(0.5) * erfc(sg * sqrt(lambda) * Vn);
+    T Vn1 = Vn * Vn0 - T(0.5) * sg * exp(-(lambda * Vn * Vn)) / sqrt(T(PI) * lambda);
+    gF[0] = gF[0] + D * Vn1;
+    gF[4] = gF[4] + (E + T(0.5) * P) * Vn1 + T(0.5) * P * Vn0 * Vn;
+    T fMn = D * Vn * Vn1 + P * Vn0;
+    T fMt1 = D * Vt1 * Vn1;
+    T fMt2 = D * Vt2 * Vn1;
+    gF[1] = gF[1] + (Tf[0] * fMn + Tf[3] * fMt1 + Tf[6] * fMt2);
+    gF[2] = gF[2] + (Tf[1] * fMn + Tf[4] * fMt1 + Tf[7] * fMt2);
+    gF[3] = gF[3] + (Tf[2] * fMn + Tf[5] * fMt1 + Tf[8] * fMt2);
+    dW[0] = dW[0] + sg * D;
+    dW[1] = dW[1] + sg * D * Vx;
+    dW[2] = dW[2] + sg * D * Vy;
+    dW[3] = dW[3] + sg * D * Vz;
+    dW[4] = dW[4] + sg * E;
+}
+// One-sided magnetic stress (stress.F90:513-599, no background field)
+template <typename T>
+__device__ __forceinline__ void magKin(const Par& p, T sg, const T* W, const T* B, T Bn, const T* Tf, T* mF, T& bbD,
+                                       T& VaD) {
+    T D = W[0], P = W[4];
+    T dPb = T(0.5) * (B[0] * B[0] + B[1] * B[1] + B[2] * B[2]);
+    T Va2 = T(2) * dPb / D;
+    bbD = bbD + T(0.5) * (B[0] * B[0] + B[1] * B[1] + B[2] * B[2]);
+    T Vac2 = Va2;
+    if (p.doBoris) { T Ca = T(p.Ca); Vac2 = Va2 / (T(1) + (Va2 / (Ca * Ca))); }
+    T Vn = Tf[0] * W[1] + Tf[1] * W[2] + Tf[2] * W[3];
+    T lambda = T(1) / (T(2) * P / D + Vac2);
+    T Vn0 = T(0.5) * erfc(sg * sqrt(lambda) * Vn);
+    VaD = VaD + T(0.5) * sqrt(Vac2);
+    mF[0] = mF[0] + Vn0 * (dPb * Tf[0] - B[0] * Bn);
+    mF[1] = mF[1] + Vn0 * (dPb * Tf[1] - B[1] * Bn);
+    mF[2] = mF[2] + Vn0 * (dPb * Tf[2] - B[2] * Bn);
+}
+
+// Fluxes (stress.F90:204-429) at every interface of direction d: reconstruction + limiter of the
+// half-state primitives and B (limited on state n), magnetic and gas kinetic fluxes, HOGS diffusion,
+// scaled by the face area.
+template <typename T>
+__global__ void __launch_bounds__(128) k_fluxes(Lay L, Par p, GridP g, StateP n, StateP h, PrimP Wh, PrimP Wn,
+                                                FluxP F, Reg r, int d) {
+    int i, j, k;
+    if (!reg_ijk(r, blockIdx.x * (long long)blockDim.x + threadIdx.x, i, j, k)) return;
+    long long c = L.at(i, j, k), s = L.stride(d);
+    T Vol[8];
+#pragma unroll
+    for (int m = 0; m < 8; ++m) Vol[m] = T(g.volume[c + (m - 4) * s]);
+    T Vi = central8<T>(Vol);
+    T pdmb = T(p.pdmb);
+    T WL[5], WR[5];
+#pragma unroll
+    for (int v = 0; v < 5; ++v) {
+        T Q[8], nQ[4];
+#pragma unroll
+        for (int m = 0; m < 8; ++m) Q[m] = T(Wh.w[v][c + (m - 4) * s]);
+#pragma unroll
+        for (int m = 0; m < 4; ++m) nQ[m] = T((p.doLFMLim ? Wn.w[v] : Wh.w[v])[c + (m - 2) * s]);
+        getLR<T>(p.rmeth, pdmb, Vol, Q, nQ, Vi, WL[v], WR[v]);
+    }
+    T Tf[9];
+#pragma unroll
+    for (int q = 0; q < 9; ++q) Tf[q] = T(g.Tf[d][q][c]);
+    double faB = g.face[d][c];
+    T VaD = T(0), bbD = T(0);
+    if (p.doMHD) {
+        T BL[3], BR[3];
+#pragma unroll
+        for (int x = 0; x < 3; ++x) {
+            T Q[8], nQ[4];
+#pragma unroll
+            for (int m = 0; m < 8; ++m) Q[m] = T(h.b[x][c + (m - 4) * s]);
+#pragma unroll
+            for (int m = 0; m < 4; ++m) nQ[m] = T((p.doLFMLim ? n.b[x] : h.b[x])[c + (m - 2) * s]);
+            getLR<T>(p.rmeth, pdmb, Vol, Q, nQ, Vi, BL[x], BR[x]);
+        }
+        T Bn = T(h.mf[d][c] / faB);
+        T mF[3] = {T(0), T(0), T(0)};
+        magKin<T>(p, T(-1), WL, BL, Bn, Tf, mF, bbD, VaD);
+        magKin<T>(p, T(1), WR, BR, Bn, Tf, mF, bbD, VaD);
+        if (p.doBoris) {
+            T Ca2 = T(p.Ca) * T(p.Ca);
+#pragma unroll
+            for (int x = 0; x < 3; ++x) {
+                T deeV = WR[1 + x] - WL[1 + x];
+                T deeP = bbD * deeV / Ca2;
+                mF[x] = mF[x] - T(p.cHogM) * VaD * deeP;
+            }
+        }
+#pragma unroll
+        for (int x = 0; x < 3; ++x) F.m[x][c] = faB * double(mF[x]);
+    }
+    T gF[5] = {T(0), T(0), T(0), T(0), T(0)}, dW[5] = {T(0), T(0), T(0), T(0), T(0)};
+    T gm1 = T(p.gamma - 1);
+    gasKin<T>(gm1, T(-1), WL, Tf, gF, dW);
+    gasKin<T>(gm1, T(1), WR, Tf, gF, dW);
+    T cH = T(p.cHogH);
+#pragma unroll
+    for (int v = 0; v < 5; ++v) gF[v] = gF[v] - cH * VaD * dW[v];
+    if (p.doBoris) {  // nuclear option, stress.F90:399-417 (cLim = 1.5)
+        T vL = sqrt(WL[1] * WL[1] + WL[2] * WL[2] + WL[3] * WL[3]);
+        T vR = sqrt(WR[1] * WR[1] + WR[2] * WR[2] + WR[3] * WR[3]);
+        T Vn = sqrt(vL * vL + vR * vR) / T((double)sqrtf(2.0f));
+        if (Vn >= T(1.5) * T(p.Ca)) {
+#pragma unroll
+            for (int v = 0; v < 5; ++v) gF[v] = gF[v] - T(p.Ca) * T(h.gas[v][c] - h.gas[v][c - s]);
+        }
+    }
+#pragma unroll
+    for (int v = 0; v < 5; ++v) F.g[v][c] = faB * double(gF[v]);
+}
+
+// Flux2Deltas (stress.F90:150-196)
+__global__ void k_flux2deltas(Lay L, Par p, GridP g, FluxP FI, FluxP FJ, FluxP FK, PrimP dGH, Vec3P dGM) {
+    Reg r = {L.is(), L.Nip, L.js(), L.Njp, L.ks(), L.Nkp};
+    int i, j, k;
+    if (!reg_ijk(r, blockIdx.x * (long long)blockDim.x + threadIdx.x, i, j, k)) return;
+    long long c = L.at(i, j, k), cj = c + L.P, ck = c + (long long)L.P * L.Q;
+    double dV = g.volume[c];
+#pragma unroll
+    for (int v = 0; v < 5; ++v)
+        dGH.w[v][c] = (FI.g[v][c] - FI.g[v][c + 1] + FJ.g[v][c] - FJ.g[v][cj] + FK.g[v][c] - FK.g[v][ck]) / dV;
+    if (p.doMHD) {
+#pragma unroll
+        for (int x = 0; x < 3; ++x)
+            dGM.v[x][c] = (FI.m[x][c] - FI.m[x][c + 1] + FJ.m[x][c] - FJ.m[x][cj] + FK.m[x][c] - FK.m[x][ck]) / dV;
+    }
+}
+
+// ================================================================================ update
+// E2Flux (fields.F90:18-51) on the active faces; every other face element carries State n over
+// (the reference updates State in place after copying it to oState).
+__global__ void k_e2flux(Lay L, Par p, Vec3P E, StateP nS, StateP oNew, const Scal* sc) {
+    Reg r = {0, L.Ni + 1, 0, L.Nj + 1, 0, L.Nk + 1};
+    int i, j, k;
+    if (!reg_ijk(r, blockIdx.x * (long long)blockDim.x + threadIdx.x, i, j, k)) return;
+    long long c = L.at(i, j, k);
+    double m0 = nS.mf[0][c], m1 = nS.mf[1][c], m2 = nS.mf[2][c];
+    bool act = p.doMHD && i >= L.is() && i <= L.ie() + 1 && j >= L.js() && j <= L.je() + 1 && k >= L.ks() &&
+               k <= L.ke() + 1;
+    if (act) {
+        double dt = sc->dt;
+        long long cj = c + L.P, ck = c + (long long)L.P * L.Q;
+        const double* Ei = E.v[0]; const double* Ej = E.v[1]; const double* Ek = E.v[2];
+        double dfi = Ek[cj] - Ek[c] - Ej[ck] + Ej[c];
+        double dfj = Ei[ck] - Ei[c] - Ek[c + 1] + Ek[c];
+        double dfk = Ej[c + 1] - Ej[c] - Ei[cj] + Ei[c];
+        m0 = m0 - dt * dfi;
+        m1 = m1 - dt * dfj;
+        m2 = m2 - dt * dfk;
+    }
+    oNew.mf[0][c] = m0; oNew.mf[1][c] = m1; oNew.mf[2][c] = m2;
+}
+
+__global__ void k_bflux2fld(Lay L, GridP g, StateP s) {
+    Reg r = {0, L.Ni, 0, L.Nj, 0, L.Nk};
+    int i, j, k;
+    if (!reg_ijk(r, blockIdx.x * (long long)blockDim.x + threadIdx.x, i, j, k)) return;
+    long long c = L.at(i, j, k);
+    double B[3];
+    cellBxyz(L, g, s.mf, c, B);
+    s.b[0][c] = B[0]; s.b[1][c] = B[1]; s.b[2][c] = B[2];
+}
+__global__ void k_copy_b(Lay L, StateP src, StateP dst) {
+    long long l = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (l >= L.E) return;
+    dst.b[0][l] = src.b[0][l]; dst.b[1][l] = src.b[1][l]; dst.b[2][l] = src.b[2][l];
+}
+
+__device__ __forceinline__ void normVec3(const double* a, double* o) {
+    double nA = sqrt(a[0] * a[0] + a[1] * a[1] + a[2] * a[2]);
+    if (nA <= TINY) { o[0] = o[1] = o[2] = 0.0; }
+    else { o[0] = a[0] / nA; o[1] = a[1] / nA; o[2] = a[2] / nA; }
+}
+// CellBoris (mhdgroup.F90:337-390), single fluid
+__device__ void cellBoris(const Par& p, double* U2, const double* U0, const double* B2, const double* B0,
+                          const double* dGH, const double* dGM, double dt) {
+    double W2[5];
+    cellC2P(p, U2, W2);
+    double D2 = dmax(W2[0], p.dFloor), P2 = dmax(W2[4], p.pFloor);
+    double D0 = dmax(U0[0], p.dFloor);
+    double V0[3] = {U0[1] / D0, U0[2] / D0, U0[3] / D0};
+    double B1[3] = {0.5 * (B2[0] + B0[0]), 0.5 * (B2[1] + B0[1]), 0.5 * (B2[2] + B0[2])};
+    double Ca = p.Ca;
+    double alpha = (B1[0] * B1[0] + B1[1] * B1[1] + B1[2] * B1[2]) / (D2 * Ca * Ca);
+    double dRho = dt * dGH[0];
+    double dPGas[3], dPMag[3], dMom[3];
+    for (int c = 0; c < 3; ++c) { dPGas[c] = dt * dGH[1 + c]; dPMag[c] = dt * dGM[c]; }
+    double pCon = 1.0 / (1.0 + alpha);
+    double bh[3];
+    normVec3(B1, bh);
+    if (alpha > TINY) {
+        double s[3] = {dPGas[0] + dPMag[0], dPGas[1] + dPMag[1], dPGas[2] + dPMag[2]};
+        double pg = dPGas[0] * bh[0] + dPGas[1] * bh[1] + dPGas[2] * bh[2];
+        double ps = s[0] * bh[0] + s[1] * bh[1] + s[2] * bh[2];
+        double pv = V0[0] * bh[0] + V0[1] * bh[1] + V0[2] * bh[2];
+        for (int c = 0; c < 3; ++c) {
+            double para = pg * bh[c];
+            double perpS = s[c] - ps * bh[c];
+            double perpV = V0[c] - pv * bh[c];
+            dMom[c] = (para + pCon * perpS) + alpha * pCon * dRho * perpV;
+        }
+    } else {
+        for (int c = 0; c < 3; ++c) dMom[c] = dPGas[c] + dPMag[c];
+    }
+    double Wn[5] = {D2, (D0 * V0[0] + dMom[0]) / D2, (D0 * V0[1] + dMom[1]) / D2, (D0 * V0[2] + dMom[2]) / D2, P2};
+    cellP2C(p, Wn, U2);
+}
+
+// CellReynolds + CellMaxwell/CellBoris (mhdgroup.F90:113-126, 170-197, 263-330) on active cells;
+// ghost cells carry State n over.
+__global__ void k_update_gas(Lay L, Par p, StateP nS, StateP oNew, PrimP dGH, Vec3P dGM, const Scal* sc) {
+    Reg r = {0, L.Ni, 0, L.Nj, 0, L.Nk};
+    int i, j, k;
+    if (!reg_ijk(r, blockIdx.x * (long long)blockDim.x + threadIdx.x, i, j, k)) return;
+    long long c = L.at(i, j, k);
+    double U[5];
+#pragma unroll
+    for (int v = 0; v < 5; ++v) U[v] = nS.gas[v][c];
+    bool act = i >= L.is() && i <= L.ie() && j >= L.js() && j <= L.je() && k >= L.ks() && k <= L.ke();
+    if (act) {
+        double dt = sc->dt;
+        double U0[5];
+#pragma unroll
+        for (int v = 0; v < 5; ++v) { U0[v] = U[v]; U[v] = U[v] + dt * dGH.w[v][c]; }
+        if (p.doMHD) {
+            double dPm[3] = {dGM.v[0][c], dGM.v[1][c], dGM.v[2][c]};
+            if (p.doBoris) {
+                double B2[3] = {oNew.b[0][c], oNew.b[1][c], oNew.b[2][c]};
+                double B0[3] = {nS.b[0][c], nS.b[1][c], nS.b[2][c]};
+                double dPg[5];
+                for (int v = 0; v < 5; ++v) dPg[v] = dGH.w[v][c];
+                cellBoris(p, U, U0, B2, B0, dPg, dPm, dt);
+            } else {
+                double D = dmax(U[0], p.dFloor), Mx = U[1], My = U[2], Mz = U[3], TotE = U[4];
+                double KinE = 0.5 * (sq(Mx) + sq(My) + sq(Mz)) / D;
+                double P = dmax((p.gamma - 1) * (TotE - KinE), p.pFloor);
+                Mx = Mx + dt * dPm[0];
+                My = My + dt * dPm[1];
+                Mz = Mz + dt * dPm[2];
+                KinE = 0.5 * (sq(Mx) + sq(My) + sq(Mz)) / D;
+                U[0] = D; U[1] = Mx; U[2] = My; U[3] = Mz; U[4] = KinE + P / (p.gamma - 1);
+            }
+        }
+    }
+#pragma unroll
+    for (int v = 0; v < 5; ++v) oNew.gas[v][c] = U[v];
+}
+
+// ================================================================================ timestep
+// CellDT (gridutils.F90:49-106) over the dt domain (one ghost layer at physical boundaries), min-reduced
+__global__ void k_calcdt(Lay L, Par p, GridP g, StateP s, Scal* sc) {
+    Reg r = {L.is() - 1, L.Nip + 2, L.js() - 1, L.Njp + 2, L.ks() - 1, L.Nkp + 2};
+    int i, j, k;
+    double dtijk = HUGEV * 2.0;
+    bool isnan_ = false;
+    if (reg_ijk(r, blockIdx.x * (long long)blockDim.x + threadIdx.x, i, j, k)) {
+        long long c = L.at(i, j, k);
+        double rho = s.gas[0][c];
+        double Vx = s.gas[1][c] / rho, Vy = s.gas[2][c] / rho, Vz = s.gas[3][c] / rho;
+        double MagV = sqrt(sq(Vx) + sq(Vy) + sq(Vz));
+        double ke = 0.5 * rho * sq(MagV);
+        double e = s.gas[4][c] - ke;
+        double P = (p.gamma - 1) * e;
+        double Cs = sqrt(p.gamma * P / rho);
+        double Valf = 0.0;
+        if (p.doMHD) {
+            double MagB = sqrt(sq(s.b[0][c]) + sq(s.b[1][c]) + sq(s.b[2][c]));
+            Valf = MagB / sqrt(rho);
+            if (p.doBoris) Valf = p.Ca * Valf / sqrt(p.Ca * p.Ca + Valf * Valf);
+        }
+        double vCFL = MagV + sqrt(sq(Cs) + sq(Valf)) + 0.0;
+        double dl = g.di[c];
+        if (g.dj[c] < dl) dl = g.dj[c];
+        if (g.dk[c] < dl) dl = g.dk[c];
+        dtijk = p.CFL * dl / vCFL;
+        if (dtijk != dtijk) { isnan_ = true; dtijk = HUGEV * 2.0; }
+    }
+    // bit patterns of non-negative doubles order like the values
+    unsigned long long bits = __double_as_longlong(dtijk);
+    if (dtijk < 0.0) bits = 0ull;
+    for (int off = 16; off > 0; off >>= 1) {
+        unsigned long long o = __shfl_down_sync(0xffffffffu, bits, off);
+        bits = o < bits ? o : bits;
+    }
+    unsigned nn = __popc(__ballot_sync(0xffffffffu, isnan_));
+    __shared__ unsigned long long wmin[32];
+    __shared__ unsigned wnan[32];
+    int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    if (lane == 0) { wmin[w] = bits; wnan[w] = nn; }
+    __syncthreads();
+    if (w == 0) {
+        int nw = blockDim.x >> 5;
+        bits = lane < nw ? wmin[lane] : ~0ull;
+        nn = lane < nw ? wnan[lane] : 0u;
+        for (int off = 16; off > 0; off >>= 1) {
+            unsigned long long o = __shfl_down_sync(0xffffffffu, bits, off);
+            bits = o < bits ? o : bits;
+            nn += __shfl_down_sync(0xffffffffu, nn, off);
+        }
+        if (lane == 0) {
+            atomicMin(&sc->dtMinBits, bits);
+            if (nn) atomicAdd(&sc->nanCount, nn);
+        }
+    }
+}
+
+// UpdateStateData time bookkeeping (gamapp.F90:113-114, mhdgroup.F90:104-105) and the rest of CalcDT
+// (step.F90:103-166): checks, the tFin clamp and the 10*dt0 clamp. mode 1 = initial dt (Hatch).
+__global__ void k_dt_finalize(Par p, Scal* sc, int mode) {
+    if (mode == 0) {
+        sc->otime = sc->time;
+        sc->time = sc->time + sc->dt;
+        sc->ts = sc->ts + 1;
+        sc->t = sc->t + sc->dt;
+    }
+    if (p.fixedTimestep) { sc->status = 0; return; }
+    double dtOld = sc->dt;
+    double dtMin = __longlong_as_double((long long)sc->dtMinBits);
+    if (sc->dtMinBits >= 0x7FF0000000000000ull || dtMin > HUGEV) dtMin = HUGEV;
+    int st = 0;
+    if (dtMin == HUGEV) st |= 1;
+    if (sc->ts > 0) {
+        if (dtOld / dtMin >= 10) st |= 2;
+        if ((sc->dt0 > TINY) && (dtMin / sc->dt0 <= p.limDT0)) st |= 2;
+        if (dtMin <= TINY) st |= 1;
+    }
+    if (sc->nanCount) st |= 4;
+    double r = dtMin;
+    if ((sc->t + r) > p.tFin) r = dmax(p.tFin - sc->t, TINY);
+    if (sc->dt0 > TINY && r > 10.0 * sc->dt0) r = 10.0 * sc->dt0;
+    sc->dt = r;
+    sc->status = st;
+    sc->sticky |= st;
+    sc->lastNan = sc->nanCount;
+    sc->dtMinBits = 0x7FF0000000000000ull;
+    sc->nanCount = 0u;
+}
+
+// ================================================================================ boundary conditions
+__device__ __forceinline__ void cpcell(const StateP& s, long long dst, long long src, bool withB) {
+#pragma unroll
+    for (int v = 0; v < 5; ++v) s.gas[v][dst] = s.gas[v][src];
+    if (withB) { s.b[0][dst] = s.b[0][src]; s.b[1][dst] = s.b[1][src]; s.b[2][dst] = s.b[2][src]; }
+}
+__device__ __forceinline__ void cpmf(const StateP& s, long long dst, long long src) {
+    s.mf[0][dst] = s.mf[0][src]; s.mf[1][dst] = s.mf[1][src]; s.mf[2][dst] = s.mf[2][src];
+}
+
+// I faces: periodic (bcs.F90:279-327) or zero gradient (bcs.F90:799-843), inner and outer side
+__global__ void k_bc_i(Lay L, Par p, GridP g, StateP s) {
+    long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    int nj = L.Nj + 1;
+    if (t >= (long long)nj * (L.Nk + 1)) return;
+    int j = (int)(t % nj), k = (int)(t / nj);
+    bool cell = (j < L.Nj) && (k < L.Nk);
+    int is = L.is(), ie = L.ie(), nG = L.nG;
+    if (p.bc[0] == BC_PERIODIC) {
+        for (int n = 1; n <= nG; ++n) {
+            long long d = L.at(is - n, j, k), sidx = L.at(ie - n + 1, j, k);
+            if (cell) cpcell(s, d, sidx, true);
+            cpmf(s, d, sidx);
+        }
+    } else if (cell) {
+        for (int n = 1; n <= nG; ++n) {
+            long long d = L.at(is - n, j, k), sidx = L.at(is, j, k);
+            cpcell(s, d, sidx, false);
+            cpmf(s, d, sidx);
+        }
+    }
+    if (p.bc[1] == BC_PERIODIC) {
+        for (int n = 1; n <= nG; ++n) {
+            long long d = L.at(ie + n, j, k), sidx = L.at(is + n - 1, j, k);
+            if (cell) cpcell(s, d, sidx, true);
+            s.mf[1][d] = s.mf[1][sidx];
+            s.mf[2][d] = s.mf[2][sidx];
+            s.mf[0][d + 1] = s.mf[0][L.at(is + n, j, k)];
+        }
+    } else if (cell) {
+        double B[3];
+        cellBxyz(L, g, s.mf, L.at(ie, j, k), B);
+        for (int n = 1; n <= nG; ++n) {
+            int ig = ie + n;
+            long long d = L.at(ig, j, k);
+            cpcell(s, d, L.at(ie, j, k), false);
+            long long dI = d + 1;
+            s.mf[0][dI] = g.face[0][dI] * (B[0] * g.Tf[0][0][dI] + B[1] * g.Tf[0][1][dI] + B[2] * g.Tf[0][2][dI]);
+            s.mf[1][d] = g.face[1][d] * (B[0] * g.Tf[1][0][d] + B[1] * g.Tf[1][1][d] + B[2] * g.Tf[1][2][d]);
+            s.mf[2][d] = g.face[2][d] * (B[0] * g.Tf[2][0][d] + B[1] * g.Tf[2][1][d] + B[2] * g.Tf[2][2][d]);
+        }
+    }
+}
+
+// J faces: periodic (bcs.F90:329-378) or zero gradient (bcs.F90:845-888)
+__global__ void k_bc_j(Lay L, Par p, StateP s) {
+    long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    int ni = L.Ni + 1;
+    if (t >= (long long)ni * (L.Nk + 1)) return;
+    int i = (int)(t % ni), k = (int)(t / ni);
+    bool cell = (i < L.Ni) && (k < L.Nk);
+    int js = L.js(), je = L.je(), nG = L.nG;
+    if (p.bc[2] == BC_PERIODIC) {
+        for (int n = 1; n <= nG; ++n) {
+            long long d = L.at(i, js - n, k), sidx = L.at(i, je - n + 1, k);
+            if (cell) cpcell(s, d, sidx, true);
+            cpmf(s, d, sidx);
+        }
+    } else if (cell) {
+        for (int n = 1; n <= nG; ++n) {
+            long long d = L.at(i, js - n, k), sidx = L.at(i, js, k);
+            cpcell(s, d, sidx, false);
+            cpmf(s, d, sidx);
+        }
+    }
+    if (p.bc[3] == BC_PERIODIC) {
+        for (int n = 1; n <= nG; ++n) {
+            long long d = L.at(i, je + n, k), sidx = L.at(i, js + n - 1, k);
+            if (cell) cpcell(s, d, sidx, true);
+            s.mf[0][d] = s.mf[0][sidx];
+            s.mf[2][d] = s.mf[2][sidx];
+            s.mf[1][L.at(i, je + n + 1, k)] = s.mf[1][L.at(i, js + n, k)];
+        }
+    } else if (cell) {
+        for (int n = 1; n <= nG; ++n) {
+            long long d = L.at(i, je + n, k), sidx = L.at(i, je, k);
+            cpcell(s, d, sidx, false);
+            s.mf[0][d] = s.mf[0][sidx];
+            s.mf[2][d] = s.mf[2][sidx];
+            s.mf[1][L.at(i, je + n + 1, k)] = s.mf[1][L.at(i, je + 1, k)];
+        }
+    }
+}
+
+// K faces: periodic (bcs.F90:380-450, 2.5D replication included) or zero gradient (bcs.F90:890-930)
+__global__ void k_bc_k(Lay L, Par p, StateP s) {
+    long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    int ni = L.Ni + 1;
+    if (t >= (long long)ni * (L.Nj + 1)) return;
+    int i = (int)(t % ni), j = (int)(t / ni);
+    bool cell = (i < L.Ni) && (j < L.Nj);
+    int ks = L.ks(), ke = L.ke(), nG = L.nG;
+    if (p.bc[4] == BC_PERIODIC) {
+        for (int n = 1; n <= nG; ++n) {
+            long long d = L.at(i, j, ks - n), sidx = p.do25D ? L.at(i, j, ks) : L.at(i, j, ke - n + 1);
+            if (cell) cpcell(s, d, sidx, true);
+            cpmf(s, d, sidx);
+        }
+    } else if (cell) {
+        for (int n = 1; n <= nG; ++n) {
+            long long d = L.at(i, j, ks - n), sidx = L.at(i, j, ks);
+            cpcell(s, d, sidx, false);
+            cpmf(s, d, sidx);
+        }
+    }
+    if (p.bc[5] == BC_PERIODIC) {
+        for (int n = 1; n <= nG; ++n) {
+            if (p.do25D) {
+                long long d = L.at(i, j, ks + n), sidx = L.at(i, j, ks);
+                if (cell) cpcell(s, d, sidx, true);
+                cpmf(s, d, sidx);
+            } else {
+                long long d = L.at(i, j, ke + n), sidx = L.at(i, j, ks + n - 1);
+                if (cell) cpcell(s, d, sidx, true);
+                s.mf[0][d] = s.mf[0][sidx];
+                s.mf[1][d] = s.mf[1][sidx];
+                s.mf[2][L.at(i, j, ke + n + 1)] = s.mf[2][L.at(i, j, ks + n)];
+            }
+        }
+    } else if (cell) {
+        for (int n = 1; n <= nG; ++n) {
+            long long d = L.at(i, j, ke + n), sidx = L.at(i, j, ke);
+            cpcell(s, d, sidx, false);
+            s.mf[0][d] = s.mf[0][sidx];
+            s.mf[1][d] = s.mf[1][sidx];
+            // bcs.F90:924 writes the J component of face ke+1 into the K faces above it; kept for parity
+            s.mf[2][L.at(i, j, ke + n + 1)] = s.mf[1][L.at(i, j, ke + 1)];
+        }
+    }
+}
+
+// DivB (gridutils.F90:717-770) partial sums, one per block, reduced in a fixed order afterwards
+__global__ void k_divb_partial(Lay L, StateP s, double* partial) {
+    Reg r = {L.is(), L.Nip, L.js(), L.Njp, L.ks(), L.Nkp};
+    int i, j, k;
+    double v = 0.0;
+    if (reg_ijk(r, blockIdx.x * (long long)blockDim.x + threadIdx.x, i, j, k)) {
+        long long c = L.at(i, j, k);
+        double dFi = s.mf[0][c] - s.mf[0][c + 1];
+        double dFj = s.mf[1][c] - s.mf[1][c + L.P];
+        double dFk = s.mf[2][c] - s.mf[2][c + (long long)L.P * L.Q];
+        v = fabs(dFi + dFj + dFk);
+    }
+    for (int off = 16; off > 0; off >>= 1) v += __shfl_down_sync(0xffffffffu, v, off);
+    __shared__ double ws[32];
+    int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    if (lane == 0) ws[w] = v;
+    __syncthreads();
+    if (w == 0) {
+        int nw = blockDim.x >> 5;
+        v = lane < nw ? ws[lane] : 0.0;
+        for (int off = 16; off > 0; off >>= 1) v += __shfl_down_sync(0xffffffffu, v, off);
+        if (lane == 0) partial[blockIdx.x] = v;
+    }
+}
+__global__ void k_sum_partials(const double* partial, int n, double* out) {
+    __shared__ double ws[32];
+    double v = 0.0;
+    for (int b = threadIdx.x; b < n; b += blockDim.x) v += partial[b];
+    for (int off = 16; off > 0; off >>= 1) v += __shfl_down_sync(0xffffffffu, v, off);
+    int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    if (lane == 0) ws[w] = v;
+    __syncthreads();
+    if (w == 0) {
+        int nw = blockDim.x >> 5;
+        v = lane < nw ? ws[lane] : 0.0;
+        for (int off = 16; off > 0; off >>= 1) v += __shfl_down_sync(0xffffffffu, v, off);
+        if (lane == 0) *out = v;
+    }
+}
+
+// ================================================================================ host side
+GridP Handle::gridP() const {
+    GridP g;
+    g.volume = volume;
+    for (int x = 0; x < 3; ++x) g.xyzcc[x] = xyzcc[x];
+    for (int d = 0; d < 3; ++d) for (int x = 0; x < 3; ++x) g.xfc[d][x] = xfc[d][x];
+    g.di = di; g.dj = dj; g.dk = dk;
+    for (int d = 0; d < 3; ++d) {
+        g.face[d] = face[d]; g.edge[d] = edge[d];
+        for (int q = 0; q < 9; ++q) { g.Tf[d][q] = Tf[d][q]; g.Te[d][q] = Te[d][q]; }
+        for (int q = 0; q < 4; ++q) g.Teb[d][q] = Teb[d][q];
+    }
+    return g;
+}
+
+static const int TPB = 128;
+
+void launch_bflux2fld(Handle& h, const StateP& s, cudaStream_t st) {
+    long long n = (long long)h.L.Ni * h.L.Nj * h.L.Nk;
+    k_bflux2fld<<<nblk(n, TPB), TPB, 0, st>>>(h.L, h.gridP(), s);
+    h.launches++;
+}
+
+void launch_bcs(Handle& h, const StateP& s, cudaStream_t st) {
+    const Lay& L = h.L;
+    k_bc_i<<<nblk((long long)(L.Nj + 1) * (L.Nk + 1), TPB), TPB, 0, st>>>(L, h.p, h.gridP(), s);
+    k_bc_j<<<nblk((long long)(L.Ni + 1) * (L.Nk + 1), TPB), TPB, 0, st>>>(L, h.p, s);
+    k_bc_k<<<nblk((long long)(L.Ni + 1) * (L.Nj + 1), TPB), TPB, 0, st>>>(L, h.p, s);
+    h.launches += 3;
+}
+
+void launch_calcdt(Handle& h, const StateP& s, int mode, cudaStream_t st) {
+    const Lay& L = h.L;
+    long long n = (long long)(L.Nip + 2) * (L.Njp + 2) * (L.Nkp + 2);
+    k_calcdt<<<nblk(n, 256), 256, 0, st>>>(L, h.p, h.gridP(), s, h.dScal);
+    k_dt_finalize<<<1, 1, 0, st>>>(h.p, h.dScal, mode);
+    h.launches += 2;
+}
+
+int kernels_per_step(const Handle& h) {
+    int n = 1 + 1;                      // begin, predict cells
+    if (h.p.doMHD) n += 1 + 1 + 6;      // predict faces, E memset (counted), 3x(mom2face + edge)
+    n += (h.p.do25D ? 2 : 3) + 1;       // fluxes + flux2deltas
+    n += 1 + 1 + 1;                     // e2flux/copy, bflux2fld, update gas
+    n += 2 + 3 + 1;                     // calcdt + finalize, 3 BC kernels, final bflux2fld
+    return n;
+}
+
+template <typename T>
+static void enqueue_hot(Handle& h, const StateP& nS, cudaStream_t st, cudaEvent_t* ev) {
+    const Lay& L = h.L;
+    const Par& p = h.p;
+    GridP g = h.gridP();
+    PrimP Wh, Wn;
+    for (int v = 0; v < 5; ++v) { Wh.w[v] = h.Wh[v]; Wn.w[v] = h.Wn[v]; }
+    if (p.doMHD) {
+        Vec3P Vf = {{h.Vf[0], h.Vf[1], h.Vf[2]}};
+        cudaMemsetAsync(h.E[0], 0, sizeof(double) * L.E * 3, st);   // E planes are contiguous in the pool
+        for (int eD = 0; eD < 3; ++eD) {
+            int dT1, dT2;
+            Reg rv, re;
+            int is = L.is(), ie = L.ie(), js = L.js(), je = L.je(), ks = L.ks(), ke = L.ke();
+            if (eD == IDIR) {
+                dT1 = JDIR; dT2 = KDIR;
+                rv = mkreg(0, L.Ni - 1, js, je + 1, 0, L.Nk - 1);
+                re = mkreg(is, ie, js, je + 1, ks, ke + 1);
+            } else if (eD == JDIR) {
+                dT1 = KDIR; dT2 = IDIR;
+                rv = mkreg(0, L.Ni - 1, 0, L.Nj - 1, ks, ke + 1);
+                re = mkreg(is, ie + 1, js, je, ks, ke + 1);
+            } else {
+                dT1 = IDIR; dT2 = JDIR;
+                rv = mkreg(is, ie + 1, 0, L.Nj - 1, 0, L.Nk - 1);
+                re = mkreg(is, ie + 1, js, je + 1, ks, ke);
+            }
+            k_mom2face<<<nblk(rv.n(), TPB), TPB, 0, st>>>(L, p, g, h.H, Vf, rv, dT1);
+            k_edge_emf<T><<<nblk(re.n(), TPB), TPB, 0, st>>>(L, p, g, nS, h.H, Vf, h.E[eD], re, eD, dT1, dT2, h.dScal);
+            h.launches += 2;
+        }
+    }
+    if (ev) cudaEventRecord(ev[PH_FLUXES], st);
+    int nF = p.do25D ? 2 : 3;
+    for (int d = 0; d < nF; ++d) {
+        Reg r;
+        int is = L.is(), ie = L.ie(), js = L.js(), je = L.je(), ks = L.ks(), ke = L.ke();
+        if (p.do25D) ke = ks;
+        if (d == IDIR) r = mkreg(is, ie + 1, js, je, ks, ke);
+        else if (d == JDIR) r = mkreg(is, ie, js, je + 1, ks, ke);
+        else r = mkreg(is, ie, js, je, ks, ke + 1);
+        FluxP F;
+        for (int v = 0; v < 5; ++v) F.g[v] = h.gflx[d][v];
+        for (int x = 0; x < 3; ++x) F.m[x] = h.mflx[d][x];
+        k_fluxes<T><<<nblk(r.n(), 128), 128, 0, st>>>(L, p, g, nS, h.H, Wh, Wn, F, r, d);
+        h.launches++;
+    }
+}
+
+int step_enqueue(Handle& h, int cur, cudaEvent_t* ev) {
+    cudaStream_t st = h.stream;
+    auto mark = [&](int ph) { if (ev) cudaEventRecord(ev[ph], st); };
+    mark(PH_PREDICT);
+    const Lay& L = h.L;
+    const Par& p = h.p;
+    GridP g = h.gridP();
+    StateP nS = h.S[cur], oS = h.S[cur ^ 1];
+    k_step_begin<<<1, 1, 0, st>>>(h.dScal);
+    if (p.doMHD) {
+        Vec3P mf = {{nS.mf[0], nS.mf[1], nS.mf[2]}}, omf = {{oS.mf[0], oS.mf[1], oS.mf[2]}},
+              hmf = {{h.H.mf[0], h.H.mf[1], h.H.mf[2]}};
+        k_predict_faces<<<nblk(L.E, 256), 256, 0, st>>>(L.E, mf, omf, hmf, h.dScal);
+        h.launches++;
+    }
+    PrimP Wh, Wn;
+    for (int v = 0; v < 5; ++v) { Wh.w[v] = h.Wh[v]; Wn.w[v] = h.Wn[v]; }
+    long long ncell = (long long)L.Ni * L.Nj * L.Nk;
+    k_predict_cells<<<nblk(ncell, TPB), TPB, 0, st>>>(L, p, g, nS, oS, h.H, Wh, Wn, h.dScal);
+    h.launches += 2;
+    mark(PH_EFIELD);
+    if (h.prec == PREC_FP32FLUX) enqueue_hot<float>(h, nS, st, ev);
+    else enqueue_hot<double>(h, nS, st, ev);
+    mark(PH_DELTAS);
+    FluxP F[3];
+    for (int d = 0; d < 3; ++d) {
+        for (int v = 0; v < 5; ++v) F[d].g[v] = h.gflx[d][v];
+        for (int x = 0; x < 3; ++x) F[d].m[x] = h.mflx[d][x];
+    }
+    PrimP dGH;
+    for (int v = 0; v < 5; ++v) dGH.w[v] = h.dGasH[v];
+    Vec3P dGM = {{h.dGasM[0], h.dGasM[1], h.dGasM[2]}};
+    long long nact = (long long)L.Nip * L.Njp * L.Nkp;
+    k_flux2deltas<<<nblk(nact, TPB), TPB, 0, st>>>(L, p, g, F[0], F[1], F[2], dGH, dGM);
+    mark(PH_UPDATE);
+    // applyUpdate into the oState buffer (which becomes State n+1)
+    Vec3P E = {{h.E[0], h.E[1], h.E[2]}};
+    long long nface = (long long)(L.Ni + 1) * (L.Nj + 1) * (L.Nk + 1);
+    k_e2flux<<<nblk(nface, TPB), TPB, 0, st>>>(L, p, E, nS, oS, h.dScal);
+    if (p.doMHD) k_bflux2fld<<<nblk(ncell, TPB), TPB, 0, st>>>(L, g, oS);
+    else k_copy_b<<<nblk(L.E, 256), 256, 0, st>>>(L, nS, oS);
+    k_update_gas<<<nblk(ncell, TPB), TPB, 0, st>>>(L, p, nS, oS, dGH, dGM, h.dScal);
+    h.launches += 4;
+    // CalcDT, EnforceBCs, bFlux2Fld on the new state
+    mark(PH_DT);
+    launch_calcdt(h, oS, 0, st);
+    mark(PH_BCS);
+    launch_bcs(h, oS, st);
+    launch_bflux2fld(h, oS, st);
+    mark(NPHASE);
+    return (int)cudaGetLastError();
+}
+
+double launch_divb(Handle& h, double* scratchDev, cudaStream_t st) {
+    const Lay& L = h.L;
+    long long n = (long long)L.Nip * L.Njp * L.Nkp;
+    int nb = (int)nblk(n, 256);
+    StateP s = h.S[h.cur];
+    k_divb_partial<<<nb, 256, 0, st>>>(L, s, scratchDev);
+    k_sum_partials<<<1, 1024, 0, st>>>(scratchDev, nb, scratchDev + nb);
+    h.launches += 2;
+    double out = 0.0;
+    cudaMemcpyAsync(&out, scratchDev + nb, sizeof(double), cudaMemcpyDeviceToHost, st);
+    cudaStreamSynchronize(st);
+    return out;
+}
+
+}  // namespace gam

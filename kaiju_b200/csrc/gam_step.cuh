@@ -1,0 +1,64 @@
+// Host-side handle of one GAMERA problem on one GPU and the step launcher.
+#pragma once
+#include <cuda_runtime.h>
+#include <vector>
+#include "gam_common.cuh"
+
+namespace gam {
+
+enum Prec { PREC_FP64 = 0, PREC_FP32FLUX = 1 };
+
+struct Handle {
+    Lay L;
+    Par p;
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    bool ownStream = false;
+    int prec = PREC_FP64;
+
+    // one pool holds every plane; planes are E doubles each
+    double* pool = nullptr;
+    size_t poolPlanes = 0;
+
+    StateP S[2];          // State n and oState, roles swap each step (cur indexes State n)
+    StateP H;             // predictor half state (Solver%StateHf)
+    double* Wh[5];        // primitives of the half state (BlockCon2Prim), for reconstruction
+    double* Wn[5];        // primitives of state n, for the limiter
+    double* E[3];         // Efld (edge-centred, times edge length)
+    double* Vf[3];        // face velocities pushed along dT1
+    double* dGasH[5];
+    double* dGasM[3];
+    double* gflx[3][5];   // interface gas fluxes per direction (area-scaled)
+    double* mflx[3][3];   // interface magnetic stresses per direction
+    // grid metrics (owned)
+    double* volume; double* xyzcc[3]; double* xfc[3][3]; double* di; double* dj; double* dk;
+    double* face[3]; double* edge[3]; double* Tf[3][9]; double* Te[3][9]; double* Teb[3][4];
+    double* xyz[3];       // corners (only kept when the grid was built on the device)
+    // FP32 copies for the FP32-flux mode
+    float* f32pool = nullptr;
+
+    Scal* dScal = nullptr;   // device scalars
+    Scal* hScal = nullptr;   // pinned host mirror
+    int cur = 0;
+
+    cudaGraphExec_t graph[2] = {nullptr, nullptr};
+    bool useGraph = true;
+    long long launches = 0;  // kernel launches issued (for accounting)
+
+    GridP gridP() const;
+    StateP cur_state() const { return S[cur]; }
+    StateP old_state() const { return S[cur ^ 1]; }
+};
+
+// Enqueue one full stepGamera on h.stream with State n = S[cur]. Does not flip cur.
+int step_enqueue(Handle& h, int cur, cudaEvent_t* phaseEv = nullptr);
+// phases recorded by step_enqueue when phaseEv is given (NPHASE+1 events)
+enum { PH_PREDICT = 0, PH_EFIELD, PH_FLUXES, PH_DELTAS, PH_UPDATE, PH_DT, PH_BCS, NPHASE };
+// Kernels used outside the step
+void launch_bflux2fld(Handle& h, const StateP& s, cudaStream_t st);
+void launch_bcs(Handle& h, const StateP& s, cudaStream_t st);
+void launch_calcdt(Handle& h, const StateP& s, int mode, cudaStream_t st);   // mode 0: in-step, 1: initial (no time advance)
+double launch_divb(Handle& h, double* scratchDev, cudaStream_t st);
+int kernels_per_step(const Handle& h);
+
+}  // namespace gam

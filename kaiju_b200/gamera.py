@@ -1,0 +1,373 @@
+"""Host-side front end of the B200 GAMERA step (ctypes over include/gamgpu.h).
+
+Mirrors the reference's application object for this path: ``Model`` carries the Model_T knobs and
+their defaults (src/gamera/init.F90:312-492), ``corners_*`` generate Grid_T corner arrays the way
+genGridXML does (init.F90:572-798), and ``GameraGPU`` is the gamApp_T of the device path:
+``step()`` is stepGamera (src/gamera/gamapp.F90:73-94), ``advance(dt)`` is gamAdvanceModel
+(src/gamera/gamtypessub.F90:78-94). Arrays crossing the boundary use the reference's Fortran layout
+(numpy arrays in order='F', ghosts included).
+
+The compute path is libgamgpu.so (built in-tree by kaiju_b200/build.py); there is no CPU fallback --
+loading fails loudly when the library or a GPU is missing.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import dataclasses
+import os
+from typing import Optional, Sequence
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libgamgpu.so")
+
+GAM_OK, GAM_ERR_NAN, GAM_ERR_DT_COLLAPSE, GAM_ERR_CUDA, GAM_ERR_TIMEOUT, GAM_ERR_UNSUPPORTED, GAM_ERR_ARG = range(7)
+GAM_FP64, GAM_FP32FLUX = 0, 1
+GAM_BC_PERIODIC, GAM_BC_ZEROGRAD = 0, 1
+GAM_RM_8CENT, GAM_RM_7UP = 0, 1
+GAM_SYNC_STATE, GAM_SYNC_OSTATE = 1, 2
+GAM_IC_OT2D, GAM_IC_BW = 0, 1
+TINY, HUGE = 1.0e-12, 1.0e12
+
+
+class GamError(RuntimeError):
+    def __init__(self, code: int, what: str):
+        self.code = code
+        super().__init__(f"{what}: {errstr(code)} (code {code})")
+
+
+class ModelC(C.Structure):
+    _fields_ = [
+        ("Nip", C.c_int), ("Njp", C.c_int), ("Nkp", C.c_int), ("nG", C.c_int),
+        ("gamma", C.c_double), ("CFL", C.c_double), ("pdmb", C.c_double), ("Vd0", C.c_double),
+        ("cHogH", C.c_double), ("cHogM", C.c_double), ("Ca", C.c_double), ("dFloor", C.c_double),
+        ("pFloor", C.c_double), ("limDT0", C.c_double),
+        ("t", C.c_double), ("tFin", C.c_double), ("dt", C.c_double), ("dt0", C.c_double),
+        ("ts", C.c_int),
+        ("doMHD", C.c_int), ("doBoris", C.c_int), ("do25D", C.c_int), ("doLFMLim", C.c_int),
+        ("rmeth", C.c_int), ("fixedTimestep", C.c_int),
+        ("doBackground", C.c_int), ("doGrav", C.c_int), ("doResistive", C.c_int), ("doRing", C.c_int),
+        ("doMultiF", C.c_int), ("doAB3", C.c_int), ("nSpc", C.c_int), ("hasHooks", C.c_int),
+        ("bc", C.c_int * 6),
+    ]
+
+
+class GridC(C.Structure):
+    _fields_ = [(n, C.POINTER(C.c_double)) for n in
+                ("xyzcc", "xfc", "di", "dj", "dk", "volume", "face", "edge", "Tf", "Te", "Teb")]
+
+
+class StatusC(C.Structure):
+    _fields_ = [("t", C.c_double), ("dt", C.c_double), ("dt0", C.c_double), ("time", C.c_double),
+                ("otime", C.c_double), ("ts", C.c_int), ("status", C.c_int), ("nanCells", C.c_int),
+                ("precision", C.c_int), ("kernelLaunches", C.c_longlong)]
+
+
+# every entry point declared in include/gamgpu.h with its ctypes signature
+_DP = C.POINTER(C.c_double)
+SIGNATURES = {
+    "gam_gpu_create": (C.c_int, [C.POINTER(C.c_void_p), C.POINTER(ModelC), C.POINTER(GridC), _DP, _DP, _DP, _DP,
+                                 C.c_double, C.c_double]),
+    "gam_gpu_create_from_corners": (C.c_int, [C.POINTER(C.c_void_p), C.POINTER(ModelC), _DP, C.c_int]),
+    "gam_gpu_step": (C.c_int, [C.c_void_p, _DP, C.POINTER(C.c_int), _DP]),
+    "gam_gpu_advance": (C.c_int, [C.c_void_p, C.c_double]),
+    "gam_gpu_run_steps": (C.c_int, [C.c_void_p, C.c_int]),
+    "gam_gpu_run_steps_timed": (C.c_int, [C.c_void_p, C.c_int, _DP]),
+    "gam_gpu_profile_phases": (C.c_int, [C.c_void_p, C.c_int, _DP, C.c_int]),
+    "gam_gpu_sync_to_host": (C.c_int, [C.c_void_p, C.c_uint, _DP, _DP, _DP, _DP, _DP]),
+    "gam_gpu_sync_to_device": (C.c_int, [C.c_void_p, C.c_uint, _DP, _DP, _DP, _DP, C.c_double, C.c_double]),
+    "gam_gpu_get_status": (C.c_int, [C.c_void_p, C.POINTER(StatusC)]),
+    "gam_gpu_set_scalars": (C.c_int, [C.c_void_p, C.c_double, C.c_double, C.c_double, C.c_int, C.c_double,
+                                      C.c_double]),
+    "gam_gpu_divb": (C.c_int, [C.c_void_p, _DP]),
+    "gam_gpu_set_precision": (C.c_int, [C.c_void_p, C.c_int]),
+    "gam_gpu_fetch": (C.c_int, [C.c_void_p, C.c_char_p, _DP, C.c_longlong]),
+    "gam_gpu_destroy": (None, [C.c_void_p]),
+    "gam_gpu_errstr": (C.c_char_p, [C.c_int]),
+}
+
+_lib = None
+
+
+def load_library(path: str = LIB_PATH):
+    """Load libgamgpu.so; raises if it is missing (no fallback path exists)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(path):
+            raise RuntimeError(f"libgamgpu.so not built ({path}); run `python kaiju_b200/build.py`")
+        L = C.CDLL(path)
+        for name, (res, args) in SIGNATURES.items():
+            f = getattr(L, name)
+            f.restype = res
+            f.argtypes = args
+        _lib = L
+    return _lib
+
+
+def errstr(code: int) -> str:
+    try:
+        return load_library().gam_gpu_errstr(code).decode()
+    except Exception:
+        return str(code)
+
+
+def _dp(a: Optional[np.ndarray]):
+    if a is None:
+        return None
+    assert a.dtype == np.float64 and a.flags["F_CONTIGUOUS"], "arrays must be float64, Fortran order"
+    return a.ctypes.data_as(_DP)
+
+
+@dataclasses.dataclass
+class Model:
+    """Model_T knobs used by the step, with the reference's defaults (init.F90:312-492)."""
+    Nip: int
+    Njp: int
+    Nkp: int
+    nG: int = 4
+    gamma: float = 5.0 / 3.0
+    pdmb: float = 0.75
+    CFL: Optional[float] = None           # default min(0.5/(pdmb+0.5), MaxCFL); MaxCFL is the real(4) 0.3
+    Vd0: float = 0.5
+    doHogs: bool = True
+    cHogH: float = 0.25
+    cHogM: float = 0.25
+    Ca: float = HUGE
+    dFloor: float = TINY
+    pFloor: float = TINY
+    limDT0: float = 1.0e-3
+    t: float = 0.0
+    tFin: float = 1.0
+    dt: float = 0.0
+    dt0: float = 0.0
+    ts: int = 0
+    doMHD: bool = True
+    doBoris: bool = False
+    doLFMLim: bool = True
+    rmeth: str = "8CENT"
+    fixedTimestep: bool = False
+    bc: Sequence[int] = (GAM_BC_PERIODIC,) * 6
+
+    @property
+    def do25D(self) -> bool:
+        return self.Nkp == 1
+
+    def cfl(self) -> float:
+        if self.CFL is not None:
+            return self.CFL
+        maxcfl = float(np.float32(0.3))
+        return min(0.5 / (self.pdmb + 0.5), maxcfl)
+
+    def to_c(self) -> ModelC:
+        m = ModelC()
+        m.Nip, m.Njp, m.Nkp, m.nG = self.Nip, self.Njp, self.Nkp, self.nG
+        m.gamma, m.CFL, m.pdmb, m.Vd0 = self.gamma, self.cfl(), self.pdmb, self.Vd0
+        m.cHogH = self.cHogH if self.doHogs else 0.0
+        m.cHogM = self.cHogM if self.doHogs else 0.0
+        m.Ca = self.Ca if self.doBoris else HUGE
+        m.dFloor, m.pFloor, m.limDT0 = self.dFloor, self.pFloor, self.limDT0
+        m.t, m.tFin, m.dt, m.dt0, m.ts = self.t, self.tFin, self.dt, self.dt0, self.ts
+        m.doMHD, m.doBoris, m.do25D, m.doLFMLim = int(self.doMHD), int(self.doBoris), int(self.do25D), int(self.doLFMLim)
+        m.rmeth = {"8CENT": GAM_RM_8CENT, "8C": GAM_RM_8CENT, "7UP": GAM_RM_7UP}[self.rmeth.upper()]
+        m.fixedTimestep = int(self.fixedTimestep)
+        for n in range(6):
+            m.bc[n] = int(self.bc[n])
+        return m
+
+    @property
+    def shape(self):
+        return (self.Nip + 2 * self.nG, self.Njp + 2 * self.nG, self.Nkp + 2 * self.nG)
+
+
+def corners_uniform(model: Model, bounds) -> np.ndarray:
+    """Cartesian corners of genGridXML (init.F90:669-731): xyz(isg:ieg+1, jsg:jeg+1, ksg:keg+1, 3)."""
+    Ni, Nj, Nk = model.shape
+    xmin, xmax, ymin, ymax, zmin, zmax = bounds
+    dx = (xmax - xmin) / model.Nip
+    dy = (ymax - ymin) / model.Njp
+    dz = (zmax - zmin) / model.Nkp
+    g = model.nG
+    i = np.arange(-g + 1, model.Nip + g + 2)     # Fortran i = isg..ieg+1 with is = 1
+    j = np.arange(-g + 1, model.Njp + g + 2)
+    k = np.arange(-g + 1, model.Nkp + g + 2)
+    x = xmin + (i - 1) * dx
+    y = ymin + (j - 1) * dy
+    z = zmin + (k - 1) * dz
+    xyz = np.zeros((Ni + 1, Nj + 1, Nk + 1, 3), order="F")
+    xyz[..., 0] = x[:, None, None]
+    xyz[..., 1] = y[None, :, None]
+    xyz[..., 2] = z[None, None, :]
+    return xyz
+
+
+def corners_warped(model: Model, bounds, amp: float) -> np.ndarray:
+    """Non-orthogonal corners x' = x + a sin(2 pi y) sin(2 pi z), cyclic in (x,y,z), applied to the
+    uniform corners; the project-supplied grid of the 3D blast-wave problem."""
+    xyz = corners_uniform(model, bounds)
+    x, y, z = xyz[..., 0].copy(), xyz[..., 1].copy(), xyz[..., 2].copy()
+    tp = 2.0 * np.pi
+    xyz[..., 0] = x + amp * np.sin(tp * y) * np.sin(tp * z)
+    xyz[..., 1] = y + amp * np.sin(tp * z) * np.sin(tp * x)
+    xyz[..., 2] = z + amp * np.sin(tp * x) * np.sin(tp * y)
+    return np.asfortranarray(xyz)
+
+
+def array_shapes(model: Model):
+    Ni, Nj, Nk = model.shape
+    c = (Ni, Nj, Nk)
+    f = (Ni + 1, Nj + 1, Nk + 1)
+    return {
+        "gas": c + (5,), "ogas": c + (5,), "hgas": c + (5,),
+        "magflux": f + (3,), "omagflux": f + (3,), "hmagflux": f + (3,),
+        "bxyz": c + (3,), "obxyz": c + (3,), "hbxyz": c + (3,), "efld": c + (3,),
+        "gflx": c + (5, 3), "mflx": c + (3, 3), "vf": c + (3,), "dgash": c + (5,), "dgasm": c + (3,),
+        "xyz": f + (3,), "xyzcc": c + (3,), "xfc": f + (3, 3), "di": c, "dj": c, "dk": c, "volume": c,
+        "tf": f + (9, 3), "te": f + (9, 3), "teb": f + (4, 3), "face": f + (3,), "edge": f + (3,),
+    }
+
+
+class GameraGPU:
+    """One GAMERA problem resident on the current CUDA device."""
+
+    def __init__(self, model: Model, handle: C.c_void_p):
+        self.model = model
+        self.h = handle
+        self.shapes = array_shapes(model)
+
+    # ---- construction
+    @classmethod
+    def from_arrays(cls, model: Model, grid: dict, gas, magflux, ogas, omagflux, time: float, otime: float):
+        """Drop-in path: the host ran Hatch; mirror its Grid_T/State_T arrays onto the device."""
+        L = load_library()
+        keep = {k: np.asfortranarray(v, dtype=np.float64) for k, v in grid.items()}
+        g = GridC()
+        for cname, key in (("xyzcc", "xyzcc"), ("xfc", "xfc"), ("di", "di"), ("dj", "dj"), ("dk", "dk"),
+                           ("volume", "volume"), ("face", "face"), ("edge", "edge"), ("Tf", "tf"), ("Te", "te"),
+                           ("Teb", "teb")):
+            setattr(g, cname, _dp(keep[key]))
+        arrs = [np.asfortranarray(a, dtype=np.float64) for a in (gas, magflux, ogas, omagflux)]
+        h = C.c_void_p()
+        m = model.to_c()
+        rc = L.gam_gpu_create(C.byref(h), C.byref(m), C.byref(g), *[_dp(a) for a in arrs], time, otime)
+        if rc:
+            raise GamError(rc, "gam_gpu_create")
+        return cls(model, h)
+
+    @classmethod
+    def from_corners(cls, model: Model, xyz: np.ndarray, ic: str):
+        """Corners2Grid + initial condition + initial BCs/dt on the device."""
+        L = load_library()
+        xyz = np.asfortranarray(xyz, dtype=np.float64)
+        h = C.c_void_p()
+        m = model.to_c()
+        rc = L.gam_gpu_create_from_corners(C.byref(h), C.byref(m), _dp(xyz),
+                                           {"OT2D": GAM_IC_OT2D, "BW": GAM_IC_BW}[ic])
+        if rc:
+            raise GamError(rc, "gam_gpu_create_from_corners")
+        return cls(model, h)
+
+    def close(self):
+        if self.h:
+            load_library().gam_gpu_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    # ---- stepping
+    def step(self):
+        dt = C.c_double()
+        ts = C.c_int()
+        t = C.c_double()
+        rc = load_library().gam_gpu_step(self.h, C.byref(dt), C.byref(ts), C.byref(t))
+        if rc:
+            raise GamError(rc, "gam_gpu_step")
+        return dt.value, ts.value, t.value
+
+    def advance(self, dt: float):
+        rc = load_library().gam_gpu_advance(self.h, dt)
+        if rc:
+            raise GamError(rc, "gam_gpu_advance")
+
+    def run_steps(self, n: int, check: bool = True) -> int:
+        rc = load_library().gam_gpu_run_steps(self.h, n)
+        if rc and check:
+            raise GamError(rc, "gam_gpu_run_steps")
+        return rc
+
+    def run_steps_timed(self, n: int):
+        """n graph-replayed steps timed with CUDA events on the library's stream; returns (ms, status)."""
+        ms = C.c_double()
+        rc = load_library().gam_gpu_run_steps_timed(self.h, n, C.byref(ms))
+        if rc not in (GAM_OK, GAM_ERR_NAN, GAM_ERR_DT_COLLAPSE):
+            raise GamError(rc, "gam_gpu_run_steps_timed")
+        return ms.value, rc
+
+    PHASES = ("predictor", "efield", "fluxes", "deltas", "update", "calcdt", "bcs")
+
+    def profile_phases(self, nsteps: int = 2) -> dict:
+        out = np.zeros(7)
+        rc = load_library().gam_gpu_profile_phases(self.h, nsteps, _dp(np.asfortranarray(out)), 7)
+        if rc not in (GAM_OK, GAM_ERR_NAN, GAM_ERR_DT_COLLAPSE):
+            raise GamError(rc, "gam_gpu_profile_phases")
+        return dict(zip(self.PHASES, out.tolist()))
+
+    def set_precision(self, mode: int):
+        rc = load_library().gam_gpu_set_precision(self.h, mode)
+        if rc:
+            raise GamError(rc, "gam_gpu_set_precision")
+
+    # ---- data movement
+    def fetch(self, name: str) -> np.ndarray:
+        shp = self.shapes[name]
+        out = np.zeros(shp, order="F")
+        rc = load_library().gam_gpu_fetch(self.h, name.encode(), _dp(out), out.size)
+        if rc:
+            raise GamError(rc, f"gam_gpu_fetch({name})")
+        return out
+
+    def sync_to_host(self, gas=None, magflux=None, bxyz=None, ogas=None, omagflux=None):
+        what = (GAM_SYNC_STATE if any(a is not None for a in (gas, magflux, bxyz)) else 0) | \
+               (GAM_SYNC_OSTATE if any(a is not None for a in (ogas, omagflux)) else 0)
+        rc = load_library().gam_gpu_sync_to_host(self.h, what, _dp(gas), _dp(magflux), _dp(bxyz), _dp(ogas),
+                                                 _dp(omagflux))
+        if rc:
+            raise GamError(rc, "gam_gpu_sync_to_host")
+
+    def sync_to_device(self, gas=None, magflux=None, ogas=None, omagflux=None, time=0.0, otime=0.0):
+        what = (GAM_SYNC_STATE if (gas is not None or magflux is not None) else 0) | \
+               (GAM_SYNC_OSTATE if (ogas is not None or omagflux is not None) else 0)
+        rc = load_library().gam_gpu_sync_to_device(self.h, what, _dp(gas), _dp(magflux), _dp(ogas), _dp(omagflux),
+                                                   time, otime)
+        if rc:
+            raise GamError(rc, "gam_gpu_sync_to_device")
+
+    def set_scalars(self, t, dt, dt0, ts, time, otime):
+        rc = load_library().gam_gpu_set_scalars(self.h, t, dt, dt0, int(ts), time, otime)
+        if rc:
+            raise GamError(rc, "gam_gpu_set_scalars")
+
+    def status(self) -> dict:
+        s = StatusC()
+        rc = load_library().gam_gpu_get_status(self.h, C.byref(s))
+        if rc:
+            raise GamError(rc, "gam_gpu_get_status")
+        return dict(t=s.t, dt=s.dt, dt0=s.dt0, time=s.time, otime=s.otime, ts=s.ts, status=s.status,
+                    nanCells=s.nanCells, precision=s.precision, kernelLaunches=s.kernelLaunches)
+
+    def divb(self) -> float:
+        v = C.c_double()
+        rc = load_library().gam_gpu_divb(self.h, C.byref(v))
+        if rc:
+            raise GamError(rc, "gam_gpu_divb")
+        return v.value

@@ -1,0 +1,1647 @@
+// CPU FP64 restatement of the GAMERA ideal-MHD step (kaiju v1.25.1) -- TEST INFRASTRUCTURE ONLY.
+//
+// This file is the oracle: the parity tests, the smoke check and the bench's CPU-baseline leg call it
+// as the checker. The product path (kaiju_b200/csrc, libgamgpu.so) never links or calls it.
+//
+// It restates, routine by routine and in the Fortran evaluation order, the reference's
+//   src/gamera/mhdgroup.F90   AdvanceMHD :16-76, applyUpdate :79-259, CellReynolds :263-297,
+//                             CellMaxwell :300-330, CellBoris :337-442, Predictor :445-525,
+//                             PredictCell :529-616, ExtrapAB2 :710-718
+//   src/gamera/stress.F90     CalcStress :41-198, Fluxes :204-429, GasKinFlux :432-511, MagKinFlux :513-599
+//   src/gamera/recon.F90      weights :22-32, BlockStateLRs :39-93, BlockLRs :96-122, Cen8LRs :125-158,
+//                             Up7LRs :162-198, Central8 :202-214, pdmLR :231-272, PDM :275-301, Up7 :303-310
+//   src/gamera/fields.F90     E2Flux :18-51, CalcElecField :70-232, Mom2Face :235-285, EdgeLRs :288-362,
+//                             GetCornerB :365-424, GetCornerD :427-454, GetCornerV :457-517
+//   src/gamera/gamutils.F90   gamLoadBlock/gamLoadBlockI :63-130, CellC2P :301-321, CellP2C :362-383
+//   src/gamera/gridutils.F90  CellDT :49-106, GasIC2State :144-189, VectorPot2Flux :193-237,
+//                             bFlux2Fld :281-301, gamCellBxyz :648-680, DivB :717-770
+//   src/gamera/step.F90       EnforceBCs :17-55, CalcDT :58-168
+//   src/gamera/bcs.F90        periodic :279-450, zeroGrad :799-930
+//   src/gamera/init.F90       CalcGridInfo :150-260, initModel defaults :312-492, SetDomain :519-538,
+//                             genGridXML :572-798, Corners2Grid :801-1080, ebGeom :1083-1145
+//   src/gamera/quadrature.F90 Gauss-Legendre 12-point tables :9-26, GaussianVolumeIntegral :42-100,
+//                             GaussianFaceIntegral :159-221, GaussianEdgeIntegral :345-370, faceDeltas :373-389
+//   src/gamera/metric.F90     faceCoords :79-108, cellCoords :133-148, CellDV/rVec/IdVec :298-328
+//   src/gamera/prob.F90       initOT2D :74-119, initBW :190-298
+//   src/base/math.F90         cross :265-274, normVec :332-343, Vec2Para/Perp :364-376, DetJ :470-478
+//   src/gamera/gamapp.F90     stepGamera :73-94, UpdateStateData :96-116
+//
+// Build: -O2 -fno-fast-math -ffp-contract=off (no FMA contraction, no reassociation).
+// Assumptions written down where Fortran leaves the compiler a choice:
+//   * x**2.0 is evaluated as x*x (gfortran lowers real exponents equal to 2 that way);
+//   * NORM2 follows gfortran's scaled sum-of-squares expansion;
+//   * DOT_PRODUCT is a left-to-right sum starting from zero;
+//   * real(4) literals (0.3 MaxCFL, sqrt(2.0) in initBW) keep their single-precision values.
+// Parity against the reference binary itself is not pinned (no Fortran compiler is available); the
+// restatement is pinned by the reference's known-answer tests (testgamutils.pf, testmetric.pf) and the
+// property tests of tests/cases/testCases.pf.
+
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <cstdio>
+#include <vector>
+#include <algorithm>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+namespace orc {
+
+static const double PI = 3.14159265358979323846264338327950288;   // kdefs.F90:21 (4*atan(1))
+static const double TINY = 1.0e-12, HUGEV = 1.0e12;                 // kdefs.F90:23
+enum { NVAR = 5, NDIM = 3, recLen = 8, limLen = 4, vecLen = 16, Nr2 = 4, Nl2 = 2 };
+enum { DEN = 1, MOMX, MOMY, MOMZ, ENERGY };
+enum { VELX = 2, VELY, VELZ, PRESSURE };
+enum { XDIR = 1, YDIR, ZDIR };
+enum { IDIR = 1, JDIR, KDIR };
+enum { NORMX = 1, NORMY, NORMZ, TAN1X, TAN1Y, TAN1Z, TAN2X, TAN2Y, TAN2Z };
+enum { XNQI = 1, YNQI, XNQJ, YNQJ };
+enum { INI = 1, OUTI, INJ, OUTJ, INK, OUTK };
+enum { BC_PERIODIC = 0, BC_ZEROGRAD = 1 };
+enum { RM_8CENT = 0, RM_7UP = 1 };
+
+static inline int ijkD(int a, int b) { return a == b ? 1 : 0; }
+
+// Fortran-ordered array with arbitrary lower bounds (column-major, first index fastest).
+struct Arr {
+    std::vector<double> d;
+    int lb[5] = {0, 0, 0, 0, 0};
+    int n[5] = {1, 1, 1, 1, 1};
+    long st[5] = {1, 1, 1, 1, 1};
+    void alloc(int nd, const int* lo, const int* hi) {
+        long s = 1;
+        for (int a = 0; a < 5; ++a) {
+            if (a < nd) { lb[a] = lo[a]; n[a] = hi[a] - lo[a] + 1; } else { lb[a] = 0; n[a] = 1; }
+            st[a] = s; s *= n[a];
+        }
+        d.assign((size_t)s, 0.0);
+    }
+    long size() const { return (long)d.size(); }
+    double* data() { return d.data(); }
+    inline long off(int i, int j, int k, int l = 0, int m = 0) const {
+        return (long)(i - lb[0]) + st[1] * (j - lb[1]) + st[2] * (k - lb[2]) + st[3] * (l - lb[3]) + st[4] * (m - lb[4]);
+    }
+    inline double& operator()(int i, int j, int k) { return d[off(i, j, k, lb[3], lb[4])]; }
+    inline double& operator()(int i, int j, int k, int l) { return d[off(i, j, k, l, lb[4])]; }
+    inline double& operator()(int i, int j, int k, int l, int m) { return d[off(i, j, k, l, m)]; }
+    inline double operator()(int i, int j, int k) const { return d[off(i, j, k, lb[3], lb[4])]; }
+    inline double operator()(int i, int j, int k, int l) const { return d[off(i, j, k, l, lb[4])]; }
+    inline double operator()(int i, int j, int k, int l, int m) const { return d[off(i, j, k, l, m)]; }
+};
+
+struct Model {
+    int nSpc = 0, nG = 4;
+    double CFL = 0.3, gamma = 5.0 / 3.0, Vd0 = 0.5;
+    double t = 0.0, tFin = 1.0, dt = 0.0, dt0 = 0.0;
+    bool fixedTimestep = false;
+    int ts = 0;
+    bool doMHD = true, do25D = false, doBoris = false, doHogs = true, doLFMLim = true;
+    double cHogH = 0.25, cHogM = 0.25, Ca = HUGEV;
+    double limDT0 = 1.0e-3;
+    double pdmb = 0.75, dFloor = TINY, pFloor = TINY;
+    int rmeth = RM_8CENT;
+    int status = 0;   // bit0: disaster (dt<=TINY or no dt<HUGE), bit1: bad (10x drop / limDT0)
+};
+
+struct Grid {
+    int Nip, Njp, Nkp, Ni, Nj, Nk;
+    int is, ie, js, je, ks, ke, isg, ieg, jsg, jeg, ksg, keg;
+    int isDT, ieDT, jsDT, jeDT, ksDT, keDT;
+    Arr xyz, xyzcc, xfc, di, dj, dk, volume, Tf, Te, Teb, face, edge;
+    int bc[6] = {BC_PERIODIC, BC_PERIODIC, BC_PERIODIC, BC_PERIODIC, BC_PERIODIC, BC_PERIODIC};
+};
+
+struct State {
+    double time = 0.0;
+    Arr Gas, magFlux, Efld, Bxyz;
+};
+
+struct Solver {
+    Arr gFlx, mFlx, Vf, dGasH, dGasM;
+    State StateHf;
+};
+
+struct App {
+    Model M;
+    Grid G;
+    State S, oS;
+    Solver V;
+};
+
+// ---------------------------------------------------------------- helpers (math.F90, gfortran intrinsics)
+static inline double sq(double x) { return x * x; }   // x**2.0
+static inline double fsign1(double b) { return std::copysign(1.0, b); }  // sign(1.0_rp,b)
+static inline double fmaxd(double a, double b) { return (a > b) ? a : b; }
+static inline double fmind(double a, double b) { return (a < b) ? a : b; }
+
+// gfortran NORM2: scaled sum of squares (avoids overflow), then scale*sqrt(ssq).
+static double norm2v(const double* a, int n) {
+    double scale = 0.0, ssq = 1.0;
+    for (int i = 0; i < n; ++i) {
+        if (a[i] != 0.0) {
+            double ax = std::fabs(a[i]);
+            if (scale < ax) { ssq = 1.0 + ssq * sq(scale / ax); scale = ax; }
+            else { ssq = ssq + sq(ax / scale); }
+        }
+    }
+    return scale * std::sqrt(ssq);
+}
+static inline void cross3(const double* a, const double* b, double* c) {
+    c[0] = a[1] * b[2] - a[2] * b[1];
+    c[1] = a[2] * b[0] - a[0] * b[2];
+    c[2] = a[0] * b[1] - a[1] * b[0];
+}
+static inline double dot(const double* a, const double* b, int n) {
+    double s = 0.0;
+    for (int i = 0; i < n; ++i) s = s + a[i] * b[i];
+    return s;
+}
+
+// recon.F90:22-32 weights, initialised from integers / 840 so the sum is exactly one
+static double interpWgt[8], interpWgt6[8], Up7C[7];
+static void initWeights() {
+    const int w8[8] = {-3, 29, -139, 533, 533, -139, 29, -3};
+    const int w6[8] = {0, 1, -8, 37, 37, -8, 1, 0};
+    const int u7[7] = {-3, 25, -101, 319, 214, -38, 4};
+    for (int n = 0; n < 8; ++n) { interpWgt[n] = (double)w8[n] / 840.0; interpWgt6[n] = (double)w6[n] / 60.0; }
+    for (int n = 0; n < 7; ++n) Up7C[n] = (double)u7[n] / 420.0;
+}
+
+// ---------------------------------------------------------------- cell conversions (gamutils.F90)
+static void CellC2P(const Model& M, const double* Con, double* Prim) {  // gamutils.F90:301-321
+    double rho = Con[0];
+    double Vx = Con[1] / rho, Vy = Con[2] / rho, Vz = Con[3] / rho;
+    double E = Con[4];
+    double KinE = 0.5 * rho * (sq(Vx) + sq(Vy) + sq(Vz));
+    Prim[0] = fmaxd(rho, M.dFloor);
+    Prim[1] = Vx; Prim[2] = Vy; Prim[3] = Vz;
+    Prim[4] = fmaxd((M.gamma - 1) * (E - KinE), M.pFloor);
+}
+static void CellP2C(const Model& M, const double* Prim, double* Con) {  // gamutils.F90:362-383
+    double rho = fmaxd(Prim[0], M.dFloor);
+    double Vx = Prim[1], Vy = Prim[2], Vz = Prim[3];
+    double IntE = fmaxd(Prim[4], M.pFloor) / (M.gamma - 1);
+    double KinE = 0.5 * rho * (sq(Vx) + sq(Vy) + sq(Vz));
+    Con[0] = rho; Con[1] = rho * Vx; Con[2] = rho * Vy; Con[3] = rho * Vz; Con[4] = IntE + KinE;
+}
+
+// ---------------------------------------------------------------- block loaders (gamutils.F90:63-130)
+// Qb(vecLen, -Nx2:Nx2-1) stored as Qb[n+Nx2][i]; zero beyond iMax.
+static void loadBlock(const Grid& G, double (*Qb)[vecLen], const double* Q, int iS, int j, int k, int iMax,
+                      int d, int Nx2, bool iface) {
+    long nSi = 1, nSj, nSk;
+    long l0;
+    if (iface) {
+        nSj = G.Ni + 1; nSk = (long)(G.Ni + 1) * (G.Nj + 1);
+        l0 = (iS - G.isg) + nSj * (j - G.jsg) + nSk * (k - G.ksg);
+    } else {
+        nSj = G.Ni; nSk = (long)G.Ni * G.Nj;
+        l0 = (iS - G.isg) + nSj * (j - G.jsg) + nSk * (k - G.ksg);
+    }
+    long nSt = nSi * ijkD(d, IDIR) + nSj * ijkD(d, JDIR) + nSk * ijkD(d, KDIR);
+    for (int n = -Nx2; n <= Nx2 - 1; ++n) {
+        long l = l0 + nSt * n;
+        for (int i = 0; i < vecLen; ++i) Qb[n + Nx2][i] = (i < iMax) ? Q[l + i] : 0.0;
+    }
+}
+
+// ---------------------------------------------------------------- reconstruction (recon.F90)
+static double pdmb_g = 0.75;
+
+static void pdmLR(const double (*Qb)[vecLen], const double* Qi, double* Ql, double* Qr) {  // recon.F90:231-272
+    for (int i = 0; i < vecLen; ++i) {
+        double v0 = Qb[0][i], v1 = Qb[1][i], v2 = Qb[2][i], v3 = Qb[3][i];
+        double maxV = fmaxd(v1, v2), minV = fmind(v1, v2);
+        double vN = fmaxd(minV, fmind(Qi[i], maxV));
+        double dv0 = pdmb_g * (v1 - v0), dv1 = pdmb_g * (v2 - v1), dv2 = pdmb_g * (v3 - v2);
+        double s0 = fsign1(dv0), s1 = fsign1(dv1), s2 = fsign1(dv2);
+        double q0 = std::fabs(s0 + s1), q1 = std::fabs(s1 + s2);
+        double dvL = vN - v1, dvR = v2 - vN;
+        Ql[i] = vN - s1 * fmaxd(0.0, std::fabs(dvL) - q0 * std::fabs(dv0));
+        Qr[i] = vN + s1 * fmaxd(0.0, std::fabs(dvR) - q1 * std::fabs(dv2));
+    }
+}
+static double PDM(double q0, double q1, double q2, double qI) {  // recon.F90:275-301
+    double maxQ = fmaxd(q1, q2), minQ = fmind(q1, q2);
+    double qN = fmaxd(minQ, fmind(qI, maxQ));
+    double dq0 = pdmb_g * (q1 - q0), dq1 = pdmb_g * (q2 - q1);
+    double s0 = fsign1(dq0), s1 = fsign1(dq1);
+    double s01 = std::fabs(s0 + s1);
+    double dqL = qN - q1;
+    return qN - s1 * fmaxd(0.0, std::fabs(dqL) - s01 * std::fabs(dq0));
+}
+static double Up7(double q0, double q1, double q2, double q3, double q4, double q5, double q6) {  // recon.F90:303-310
+    return q0 * Up7C[0] + q1 * Up7C[1] + q2 * Up7C[2] + q3 * Up7C[3] + q4 * Up7C[4] + q5 * Up7C[5] + q6 * Up7C[6];
+}
+static void Central8(const double (*Qb)[vecLen], double* Qi) {  // recon.F90:202-214
+    for (int i = 0; i < vecLen; ++i) {
+        double s = 0.0;
+        for (int n = 0; n < recLen; ++n) s = s + interpWgt[n] * Qb[n][i];
+        Qi[i] = s;
+    }
+}
+// GetLRs: Cen8LRs (recon.F90:125-158) or Up7LRs (:162-198)
+static void GetLRs(int rmeth, const double (*dV)[vecLen], const double (*nQ)[vecLen], const double (*Q)[vecLen],
+                   const double* Vi, double* Ql, double* Qr) {
+    double QdV[recLen][vecLen];
+    for (int n = 0; n < recLen; ++n)
+        for (int i = 0; i < vecLen; ++i) QdV[n][i] = dV[n][i] * Q[n][i];
+    if (rmeth == RM_8CENT) {
+        double Qi[vecLen];
+        Central8(QdV, Qi);
+        for (int i = 0; i < vecLen; ++i) Qi[i] = Qi[i] / Vi[i];
+        pdmLR(nQ, Qi, Ql, Qr);
+    } else {
+        for (int i = 0; i < vecLen; ++i) {
+            Ql[i] = Up7(QdV[0][i], QdV[1][i], QdV[2][i], QdV[3][i], QdV[4][i], QdV[5][i], QdV[6][i]) / Vi[i];
+            Qr[i] = Up7(QdV[7][i], QdV[6][i], QdV[5][i], QdV[4][i], QdV[3][i], QdV[2][i], QdV[1][i]) / Vi[i];
+            Ql[i] = PDM(nQ[0][i], nQ[1][i], nQ[2][i], Ql[i]);
+            Qr[i] = PDM(nQ[3][i], nQ[2][i], nQ[1][i], Qr[i]);
+        }
+    }
+}
+// BlockLRs (recon.F90:96-122): Qb[nv][n][i]
+static void BlockLRs(int rmeth, const double (*VolB)[vecLen], const double (*nQb)[limLen][vecLen],
+                     const double (*Qb)[recLen][vecLen], double (*Ql)[vecLen], double (*Qr)[vecLen], int NumV) {
+    double Vi[vecLen];
+    Central8(VolB, Vi);
+    for (int nv = 0; nv < NumV; ++nv) GetLRs(rmeth, VolB, nQb[nv], Qb[nv], Vi, Ql[nv], Qr[nv]);
+}
+// BlockCon2Prim (recon.F90:66-92)
+static void BlockCon2Prim(const Model& M, const double (*inCon)[vecLen], double (*oPrim)[vecLen], int xLen,
+                          int stride /* per-variable stride in rows */) {
+    // inCon[nv*stride + n][i]
+    for (int n = 0; n < xLen; ++n)
+        for (int i = 0; i < vecLen; ++i) {
+            double D = fmaxd(inCon[0 * stride + n][i], M.dFloor);
+            double Mx = inCon[1 * stride + n][i], My = inCon[2 * stride + n][i], Mz = inCon[3 * stride + n][i];
+            double E = inCon[4 * stride + n][i];
+            double KinE = 0.5 * (sq(Mx) + sq(My) + sq(Mz)) / D;
+            double P = fmaxd((M.gamma - 1) * (E - KinE), M.pFloor);
+            oPrim[0 * stride + n][i] = D;
+            oPrim[1 * stride + n][i] = Mx / D;
+            oPrim[2 * stride + n][i] = My / D;
+            oPrim[3 * stride + n][i] = Mz / D;
+            oPrim[4 * stride + n][i] = P;
+        }
+}
+
+// ---------------------------------------------------------------- kinetic fluxes (stress.F90)
+static const int SgnLR[2] = {-1, 1};
+
+static void GasKinFlux(const Model& M, int q, const double (*Prim)[vecLen], const double (*TfB)[vecLen],
+                       double (*gFlxB)[vecLen], double (*dW)[vecLen]) {  // stress.F90:432-511
+    double sg = (double)SgnLR[q];
+    for (int i = 0; i < vecLen; ++i) {
+        double D = Prim[0][i], P = Prim[4][i], Vx = Prim[1][i], Vy = Prim[2][i], Vz = Prim[3][i];
+        double E = 0.5 * D * (sq(Vx) + sq(Vy) + sq(Vz)) + P / (M.gamma - 1);
+        double lambda = D / (2 * P);
+        double Vn = TfB[NORMX - 1][i] * Vx + TfB[NORMY - 1][i] * Vy + TfB[NORMZ - 1][i] * Vz;
+        double Vt1 = TfB[TAN1X - 1][i] * Vx + TfB[TAN1Y - 1][i] * Vy + TfB[TAN1Z - 1][i] * Vz;
+        double Vt2 = TfB[TAN2X - 1][i] * Vx + TfB[TAN2Y - 1][i] * Vy + TfB[TAN2Z - 1][i] * Vz;
+        double Vn0 = 0.5 * std::erfc(sg * std::sqrt(lambda) * Vn);
+        double Vn1 = Vn * Vn0 - 0.5 * sg * std::exp(-(lambda * Vn * Vn)) / std::sqrt(PI * lambda);
+        gFlxB[DEN - 1][i] = gFlxB[DEN - 1][i] + D * Vn1;
+        gFlxB[ENERGY - 1][i] = gFlxB[ENERGY - 1][i] + (E + 0.5 * P) * Vn1 + 0.5 * P * Vn0 * Vn;
+        double fMn = D * Vn * Vn1 + P * Vn0;
+        double fMt1 = D * Vt1 * Vn1;
+        double fMt2 = D * Vt2 * Vn1;
+        double fMx = TfB[NORMX - 1][i] * fMn + TfB[TAN1X - 1][i] * fMt1 + TfB[TAN2X - 1][i] * fMt2;
+        double fMy = TfB[NORMY - 1][i] * fMn + TfB[TAN1Y - 1][i] * fMt1 + TfB[TAN2Y - 1][i] * fMt2;
+        double fMz = TfB[NORMZ - 1][i] * fMn + TfB[TAN1Z - 1][i] * fMt1 + TfB[TAN2Z - 1][i] * fMt2;
+        gFlxB[MOMX - 1][i] = gFlxB[MOMX - 1][i] + fMx;
+        gFlxB[MOMY - 1][i] = gFlxB[MOMY - 1][i] + fMy;
+        gFlxB[MOMZ - 1][i] = gFlxB[MOMZ - 1][i] + fMz;
+        dW[DEN - 1][i] = dW[DEN - 1][i] + sg * D;
+        dW[MOMX - 1][i] = dW[MOMX - 1][i] + sg * D * Vx;
+        dW[MOMY - 1][i] = dW[MOMY - 1][i] + sg * D * Vy;
+        dW[MOMZ - 1][i] = dW[MOMZ - 1][i] + sg * D * Vz;
+        dW[ENERGY - 1][i] = dW[ENERGY - 1][i] + sg * E;
+    }
+}
+
+static void MagKinFlux(const Model& M, int q, const double (*Prim)[vecLen], const double (*Mag)[vecLen],
+                       const double* Bn, const double (*TfB)[vecLen], double (*mFlxB)[vecLen], double* bbD,
+                       double* VaD) {  // stress.F90:513-599 (no background field)
+    double sg = (double)SgnLR[q];
+    for (int i = 0; i < vecLen; ++i) {
+        double D = Prim[0][i], P = Prim[4][i];
+        double Bx = Mag[0][i], By = Mag[1][i], Bz = Mag[2][i];
+        double dPb = 0.5 * (sq(Bx) + sq(By) + sq(Bz));
+        double Va2 = 2 * dPb / D;
+        bbD[i] = bbD[i] + 0.5 * (sq(Bx) + sq(By) + sq(Bz));
+        double Vac2;
+        if (M.doBoris) Vac2 = Va2 / (1 + (Va2 / sq(M.Ca)));
+        else Vac2 = Va2;
+        double Vx = Prim[1][i], Vy = Prim[2][i], Vz = Prim[3][i];
+        double Nx = TfB[NORMX - 1][i], Ny = TfB[NORMY - 1][i], Nz = TfB[NORMZ - 1][i];
+        double Vn = Nx * Vx + Ny * Vy + Nz * Vz;
+        double lambda = 1 / (2 * P / D + Vac2);
+        double Vn0 = 0.5 * std::erfc(sg * std::sqrt(lambda) * Vn);
+        VaD[i] = VaD[i] + 0.5 * std::sqrt(Vac2);
+        mFlxB[0][i] = mFlxB[0][i] + Vn0 * (dPb * Nx - Bx * Bn[i]);
+        mFlxB[1][i] = mFlxB[1][i] + Vn0 * (dPb * Ny - By * Bn[i]);
+        mFlxB[2][i] = mFlxB[2][i] + Vn0 * (dPb * Nz - Bz * Bn[i]);
+    }
+}
+
+// Fluxes (stress.F90:204-429) for one brick (iB:iB+vecLen-1, j, k) in direction dN
+static void Fluxes(const Model& M, const Grid& G, const State& nS, const State& hS, int iB, int j, int k, int dN,
+                   Arr& gFlx, Arr& mFlx) {
+    double VolB[recLen][vecLen];
+    double ConB[NVAR][recLen][vecLen];
+    double MagB[NDIM][recLen][vecLen];
+    double TfB[9][vecLen];
+    double faB[vecLen];
+    double nConB[NVAR][limLen][vecLen];
+    double nMagB[NDIM][limLen][vecLen];
+    double PrimL[NVAR][vecLen], PrimR[NVAR][vecLen], MagL[NDIM][vecLen], MagR[NDIM][vecLen];
+    double gFlxB[NVAR][vecLen], mFlxB[NDIM][vecLen], dW[NVAR][vecLen], VaD[vecLen], Bn[vecLen], bbD[vecLen];
+
+    int ie = G.ie + ijkD(dN, IDIR);
+    int iMax = std::min((int)vecLen, ie - iB + 1);
+    int isB = iB;
+    std::memset(gFlxB, 0, sizeof gFlxB); std::memset(mFlxB, 0, sizeof mFlxB); std::memset(dW, 0, sizeof dW);
+    std::memset(VaD, 0, sizeof VaD); std::memset(bbD, 0, sizeof bbD); std::memset(TfB, 0, sizeof TfB);
+    std::memset(Bn, 0, sizeof Bn); std::memset(faB, 0, sizeof faB);
+
+    loadBlock(G, VolB, G.volume.d.data(), iB, j, k, iMax, dN, Nr2, false);
+    for (int i = 0; i < iMax; ++i) {
+        for (int c = 0; c < 9; ++c) TfB[c][i] = G.Tf(isB + i, j, k, c + 1, dN);
+        faB[i] = G.face(isB + i, j, k, dN);
+    }
+    const long cellN = (long)G.Ni * G.Nj * G.Nk;
+    const long faceN = (long)(G.Ni + 1) * (G.Nj + 1) * (G.Nk + 1);
+    if (M.doMHD) {
+        for (int nv = 0; nv < NDIM; ++nv) {
+            loadBlock(G, MagB[nv], hS.Bxyz.d.data() + nv * cellN, iB, j, k, iMax, dN, Nr2, false);
+            const State& lS = M.doLFMLim ? nS : hS;
+            loadBlock(G, nMagB[nv], lS.Bxyz.d.data() + nv * cellN, iB, j, k, iMax, dN, Nl2, false);
+        }
+        BlockLRs(M.rmeth, VolB, nMagB, MagB, MagL, MagR, NDIM);
+        for (int i = 0; i < iMax; ++i) Bn[i] = hS.magFlux(isB + i, j, k, dN) / faB[i];
+        (void)faceN;
+    }
+    for (int nv = 0; nv < NVAR; ++nv) {
+        loadBlock(G, ConB[nv], hS.Gas.d.data() + nv * cellN, iB, j, k, iMax, dN, Nr2, false);
+        const State& lS = M.doLFMLim ? nS : hS;
+        loadBlock(G, nConB[nv], lS.Gas.d.data() + nv * cellN, iB, j, k, iMax, dN, Nl2, false);
+    }
+    // BlockStateLRs (recon.F90:39-93)
+    {
+        double PrimB[NVAR][recLen][vecLen], nPrimB[NVAR][limLen][vecLen];
+        BlockCon2Prim(M, &nConB[0][0], &nPrimB[0][0], limLen, limLen);
+        BlockCon2Prim(M, &ConB[0][0], &PrimB[0][0], recLen, recLen);
+        BlockLRs(M.rmeth, VolB, nPrimB, PrimB, PrimL, PrimR, NVAR);
+    }
+    if (M.doMHD) {
+        MagKinFlux(M, 0, PrimL, MagL, Bn, TfB, mFlxB, bbD, VaD);
+        MagKinFlux(M, 1, PrimR, MagR, Bn, TfB, mFlxB, bbD, VaD);
+        if (M.doBoris) {
+            for (int i = 0; i < iMax; ++i) {
+                double deeV[3], deeP[3];
+                for (int c = 0; c < 3; ++c) deeV[c] = PrimR[1 + c][i] - PrimL[1 + c][i];
+                for (int c = 0; c < 3; ++c) deeP[c] = bbD[i] * deeV[c] / sq(M.Ca);
+                for (int c = 0; c < 3; ++c) mFlxB[c][i] = mFlxB[c][i] - M.cHogM * VaD[i] * deeP[c];
+            }
+        }
+        for (int nv = 0; nv < NDIM; ++nv)
+            for (int i = 0; i < iMax; ++i) mFlx(isB + i, j, k, nv + 1, dN) = faB[i] * mFlxB[nv][i];
+    }
+    std::memset(gFlxB, 0, sizeof gFlxB); std::memset(dW, 0, sizeof dW);
+    GasKinFlux(M, 0, PrimL, TfB, gFlxB, dW);
+    GasKinFlux(M, 1, PrimR, TfB, gFlxB, dW);
+    for (int nv = 0; nv < NVAR; ++nv)
+        for (int i = 0; i < iMax; ++i) {
+            double alphaS = 1.0;
+            gFlxB[nv][i] = gFlxB[nv][i] - alphaS * M.cHogH * VaD[i] * dW[nv][i];
+        }
+    if (M.doBoris) {  // nuclear option (stress.F90:399-417), cLim = 1.5 (single precision literal)
+        const double cLim = 1.5;
+        for (int i = 0; i < iMax; ++i) {
+            double a[3] = {PrimL[1][i], PrimL[2][i], PrimL[3][i]}, b[3] = {PrimR[1][i], PrimR[2][i], PrimR[3][i]};
+            double vL = norm2v(a, 3), vR = norm2v(b, 3);
+            double Vn = std::sqrt(sq(vL) + sq(vR)) / (double)std::sqrt(2.0f);
+            if (Vn >= cLim * M.Ca) {
+                for (int nv = 0; nv < NVAR; ++nv) {
+                    double dCon = ConB[nv][Nr2][i] - ConB[nv][Nr2 - 1][i];
+                    gFlxB[nv][i] = gFlxB[nv][i] - M.Ca * dCon;
+                }
+            }
+        }
+    }
+    for (int nv = 0; nv < NVAR; ++nv)
+        for (int i = 0; i < iMax; ++i) gFlx(isB + i, j, k, nv + 1, dN) = faB[i] * gFlxB[nv][i];
+}
+
+static void CalcStress(const Model& M, const Grid& G, const State& nS, const State& hS, Arr& gFlx, Arr& mFlx,
+                       Arr& dGasH, Arr& dGasM) {  // stress.F90:41-198
+    int nFlx = NDIM, ks = G.ks, ke = G.ke;
+    if (M.do25D) { nFlx = 2; ks = G.ks; ke = G.ks; }
+    for (int d = 1; d <= nFlx; ++d) {
+        if (d == IDIR) {
+#pragma omp parallel for collapse(2) schedule(static)
+            for (int k = ks; k <= ke; ++k)
+                for (int j = G.js; j <= G.je; ++j)
+                    for (int iB = G.is; iB <= G.ie + 1; iB += vecLen) Fluxes(M, G, nS, hS, iB, j, k, d, gFlx, mFlx);
+        } else if (d == JDIR) {
+#pragma omp parallel for collapse(2) schedule(static)
+            for (int k = ks; k <= ke; ++k)
+                for (int iB = G.is; iB <= G.ie; iB += vecLen)
+                    for (int j = G.js; j <= G.je + 1; ++j) Fluxes(M, G, nS, hS, iB, j, k, d, gFlx, mFlx);
+        } else {
+#pragma omp parallel for collapse(2) schedule(static)
+            for (int j = G.js; j <= G.je; ++j)
+                for (int iB = G.is; iB <= G.ie; iB += vecLen)
+                    for (int k = ks; k <= ke + 1; ++k) Fluxes(M, G, nS, hS, iB, j, k, d, gFlx, mFlx);
+        }
+    }
+    bool doMaxwell = M.doMHD;
+#pragma omp parallel for collapse(2) schedule(static)
+    for (int k = G.ks; k <= G.ke; ++k)
+        for (int j = G.js; j <= G.je; ++j)
+            for (int i = G.is; i <= G.ie; ++i) {
+                double dV = G.volume(i, j, k);
+                for (int nv = 1; nv <= NVAR; ++nv)
+                    dGasH(i, j, k, nv) = (gFlx(i, j, k, nv, IDIR) - gFlx(i + 1, j, k, nv, IDIR) + gFlx(i, j, k, nv, JDIR) -
+                                          gFlx(i, j + 1, k, nv, JDIR) + gFlx(i, j, k, nv, KDIR) - gFlx(i, j, k + 1, nv, KDIR)) / dV;
+                if (doMaxwell)
+                    for (int c = 1; c <= NDIM; ++c)
+                        dGasM(i, j, k, c) = (mFlx(i, j, k, c, IDIR) - mFlx(i + 1, j, k, c, IDIR) + mFlx(i, j, k, c, JDIR) -
+                                             mFlx(i, j + 1, k, c, JDIR) + mFlx(i, j, k, c, KDIR) - mFlx(i, j, k + 1, c, KDIR)) / dV;
+            }
+}
+
+// ---------------------------------------------------------------- B from flux (gridutils.F90:281-301,648-680)
+static void gamCellBxyz(const Grid& G, const Arr& mf, int i, int j, int k, double* B) {
+    double dV = G.volume(i, j, k);
+    double fI = mf(i, j, k, IDIR), fJ = mf(i, j, k, JDIR), fK = mf(i, j, k, KDIR);
+    double fIp = mf(i + 1, j, k, IDIR), fJp = mf(i, j + 1, k, JDIR), fKp = mf(i, j, k + 1, KDIR);
+    double Div = fIp - fI + fJp - fJ + fKp - fK;
+    for (int c = 1; c <= 3; ++c) {
+        double xfI = G.xfc(i, j, k, c, IDIR), xfJ = G.xfc(i, j, k, c, JDIR), xfK = G.xfc(i, j, k, c, KDIR);
+        double xfIp = G.xfc(i + 1, j, k, c, IDIR), xfJp = G.xfc(i, j + 1, k, c, JDIR), xfKp = G.xfc(i, j, k + 1, c, KDIR);
+        double b = (fIp * xfIp + fJp * xfJp + fKp * xfKp - fI * xfI - fJ * xfJ - fK * xfK) / dV;
+        b = b - Div * G.xyzcc(i, j, k, c) / dV;
+        B[c - 1] = b;
+    }
+}
+static void bFlux2Fld(const Grid& G, const Arr& mf, Arr& B) {
+#pragma omp parallel for collapse(2) schedule(static)
+    for (int k = G.ksg; k <= G.keg; ++k)
+        for (int j = G.jsg; j <= G.jeg; ++j)
+            for (int i = G.isg; i <= G.ieg; ++i) {
+                double b[3];
+                gamCellBxyz(G, mf, i, j, k, b);
+                for (int c = 0; c < 3; ++c) B(i, j, k, c + 1) = b[c];
+            }
+}
+
+// ---------------------------------------------------------------- predictor (mhdgroup.F90:445-616)
+static void Predictor(const Model& M, const Grid& G, const State& S, const State& oS, State& pS, double pdt) {
+    double odt = S.time - oS.time;
+    if (M.doMHD) {
+        long N = S.magFlux.size();
+#pragma omp parallel for schedule(static)
+        for (long l = 0; l < N; ++l) {
+            double Q = S.magFlux.d[l], oQ = oS.magFlux.d[l];
+            double dQ = (Q - oQ) / odt;
+            pS.magFlux.d[l] = Q + pdt * dQ;
+        }
+    }
+    bFlux2Fld(G, pS.magFlux, pS.Bxyz);
+#pragma omp parallel for collapse(2) schedule(static)
+    for (int k = G.ksg; k <= G.keg; ++k)
+        for (int j = G.jsg; j <= G.jeg; ++j)
+            for (int i = G.isg; i <= G.ieg; ++i) {
+                double Q[5], oQ[5], W[5], oW[5], pW[5], pQ[5];
+                for (int v = 0; v < 5; ++v) { Q[v] = S.Gas(i, j, k, v + 1); oQ[v] = oS.Gas(i, j, k, v + 1); }
+                CellC2P(M, oQ, oW);
+                CellC2P(M, Q, W);
+                for (int v = 0; v < 5; ++v) { double dQ = (W[v] - oW[v]) / odt; pW[v] = W[v] + pdt * dQ; }
+                pW[0] = fmaxd(pW[0], M.dFloor);
+                pW[4] = fmaxd(pW[4], M.pFloor);
+                CellP2C(M, pW, pQ);
+                for (int v = 0; v < 5; ++v) pS.Gas(i, j, k, v + 1) = pQ[v];
+            }
+}
+
+// ---------------------------------------------------------------- electric field (fields.F90)
+static void Mom2Face(const Model& M, const Grid& G, const State& hS, double (*VfB)[vecLen], int iB, int j, int k,
+                     int iMax, int dT) {  // fields.F90:235-285
+    double VolB[recLen][vecLen], DenB[recLen][vecLen], MomB[3][recLen][vecLen], VelB[3][recLen][vecLen];
+    const long cellN = (long)G.Ni * G.Nj * G.Nk;
+    loadBlock(G, VolB, G.volume.d.data(), iB, j, k, iMax, dT, Nr2, false);
+    loadBlock(G, DenB, hS.Gas.d.data() + 0 * cellN, iB, j, k, iMax, dT, Nr2, false);
+    for (int c = 0; c < 3; ++c) loadBlock(G, MomB[c], hS.Gas.d.data() + (1 + c) * cellN, iB, j, k, iMax, dT, Nr2, false);
+    for (int n = 0; n < recLen; ++n)
+        for (int i = 0; i < iMax; ++i)
+            for (int c = 0; c < 3; ++c) VelB[c][n][i] = VolB[n][i] * MomB[c][n][i] / fmaxd(DenB[n][i], M.dFloor);
+    for (int c = 0; c < 3; ++c) for (int i = 0; i < vecLen; ++i) VfB[c][i] = 0.0;
+    double dV[vecLen];
+    for (int i = 0; i < iMax; ++i) {
+        double s = 0.0;
+        for (int n = 0; n < recLen; ++n) s = s + interpWgt[n] * VolB[n][i];
+        dV[i] = fmaxd(s, TINY);
+    }
+    for (int c = 0; c < 3; ++c)
+        for (int i = 0; i < iMax; ++i) {
+            double s = 0.0;
+            for (int n = 0; n < recLen; ++n) s = s + interpWgt[n] * VelB[c][n][i];
+            VfB[c][i] = s / dV[i];
+        }
+}
+
+static void EdgeLRs(const Model& M, const Grid& G, const Arr& bFluxn, const Arr& bFluxHf, double* bL, double* bR,
+                    double* fA, int iB, int j, int k, int iMax, int dN, int dT1, int dT2) {  // fields.F90:288-362
+    (void)dN;
+    double AreaB[recLen][vecLen], VolB[recLen][vecLen], nAreaB[limLen][vecLen];
+    double MagB[1][recLen][vecLen], nMagB[1][limLen][vecLen], MagLB[1][vecLen], MagRB[1][vecLen];
+    const long faceN = (long)(G.Ni + 1) * (G.Nj + 1) * (G.Nk + 1);
+    for (int i = 0; i < vecLen; ++i) { fA[i] = 0.0; bL[i] = 0.0; bR[i] = 0.0; }
+    for (int n = 0; n < recLen; ++n) for (int i = 0; i < vecLen; ++i) VolB[n][i] = 0.0;
+    loadBlock(G, AreaB, G.face.d.data() + (dT1 - 1) * faceN, iB, j, k, iMax, dT2, Nr2, true);
+    loadBlock(G, MagB[0], bFluxHf.d.data() + (dT1 - 1) * faceN, iB, j, k, iMax, dT2, Nr2, true);
+    loadBlock(G, nAreaB, G.face.d.data() + (dT1 - 1) * faceN, iB, j, k, iMax, dT2, Nl2, true);
+    const Arr& lim = M.doLFMLim ? bFluxn : bFluxHf;
+    loadBlock(G, nMagB[0], lim.d.data() + (dT1 - 1) * faceN, iB, j, k, iMax, dT2, Nl2, true);
+    for (int i = 0; i < iMax; ++i) {
+        for (int n = 0; n < recLen; ++n) {
+            VolB[n][i] = AreaB[n][i];
+            MagB[0][n][i] = MagB[0][n][i] / fmaxd(AreaB[n][i], TINY);
+        }
+        for (int n = 0; n < limLen; ++n) nMagB[0][n][i] = nMagB[0][n][i] / fmaxd(nAreaB[n][i], TINY);
+    }
+    BlockLRs(M.rmeth, VolB, nMagB, MagB, MagLB, MagRB, 1);
+    for (int i = 0; i < vecLen; ++i) { bL[i] = MagLB[0][i]; bR[i] = MagRB[0][i]; }
+    for (int i = 0; i < iMax; ++i) {
+        double s = 0.0;
+        for (int n = 0; n < recLen; ++n) s = s + interpWgt[n] * AreaB[n][i];
+        fA[i] = s;
+        bL[i] = bL[i] * fA[i];
+        bR[i] = bR[i] * fA[i];
+    }
+}
+
+static void GetCornerB(const Model& M, const Grid& G, const Arr& bFluxn, const Arr& bFluxHf, double* b1, double* b2,
+                       double* Jd, int iB, int j, int k, int iMax, int dN, int dT1, int dT2) {  // fields.F90:365-424
+    double bT1L[vecLen], bT1R[vecLen], fA1[vecLen], bT2L[vecLen], bT2R[vecLen], fA2[vecLen];
+    EdgeLRs(M, G, bFluxn, bFluxHf, bT1L, bT1R, fA1, iB, j, k, iMax, dN, dT1, dT2);
+    EdgeLRs(M, G, bFluxn, bFluxHf, bT2L, bT2R, fA2, iB, j, k, iMax, dN, dT2, dT1);
+    for (int i = 0; i < iMax; ++i) {
+        int iG = iB + i;
+        double xni = G.Teb(iG, j, k, XNQI, dN), yni = G.Teb(iG, j, k, YNQI, dN);
+        double xnj = G.Teb(iG, j, k, XNQJ, dN), ynj = G.Teb(iG, j, k, YNQJ, dN);
+        double detT = 1.0 / (xni * ynj - xnj * yni);
+        double bT1 = 0.5 * (bT1L[i] + bT1R[i]) / fA1[i];
+        double bT2 = 0.5 * (bT2L[i] + bT2R[i]) / fA2[i];
+        double db1 = (bT1R[i] - bT1L[i]) / fA1[i];
+        double db2 = (bT2R[i] - bT2L[i]) / fA2[i];
+        Jd[i] = db2 - db1;
+        b1[i] = detT * (ynj * bT1 - yni * bT2);
+        b2[i] = detT * (-(xnj * bT1) + xni * bT2);
+    }
+}
+
+static void GetCornerD(const Grid& G, const Arr& Gas, double* Dc, int iB, int j, int k, int iMax, int dN) {
+    int e1[3], e2[3];  // metric.F90:151-167 getNormalPlane
+    if (dN == IDIR) { e1[0] = 0; e1[1] = 1; e1[2] = 0; e2[0] = 0; e2[1] = 0; e2[2] = 1; }
+    else if (dN == JDIR) { e1[0] = 1; e1[1] = 0; e1[2] = 0; e2[0] = 0; e2[1] = 0; e2[2] = 1; }
+    else { e1[0] = 1; e1[1] = 0; e1[2] = 0; e2[0] = 0; e2[1] = 1; e2[2] = 0; }
+    for (int i = 0; i < iMax; ++i) {
+        int iG = iB + i;
+        Dc[i] = 0.25 * (Gas(iG, j, k, DEN) + Gas(iG - e1[0], j - e1[1], k - e1[2], DEN) +
+                        Gas(iG - e2[0], j - e2[1], k - e2[2], DEN) +
+                        Gas(iG - e1[0] - e2[0], j - e1[1] - e2[1], k - e1[2] - e2[2], DEN));
+    }
+}
+
+static void GetCornerV(const Grid& G, const Arr& Vf, double* v1, double* v2, double* vDiff, int iB, int j, int k,
+                       int iMax, int dN, int dT1, int dT2) {  // fields.F90:457-517
+    double VelB[3][recLen][vecLen], AreaB[recLen][vecLen], VxyzC[3][vecLen], dA[vecLen];
+    const long faceN = (long)(G.Ni + 1) * (G.Nj + 1) * (G.Nk + 1);
+    const long cellN = (long)G.Ni * G.Nj * G.Nk;
+    loadBlock(G, AreaB, G.face.d.data() + (dT1 - 1) * faceN, iB, j, k, iMax, dT2, Nr2, true);
+    for (int i = 0; i < iMax; ++i) {
+        double s = 0.0;
+        for (int n = 0; n < recLen; ++n) s = s + interpWgt[n] * AreaB[n][i];
+        dA[i] = fmaxd(s, TINY);
+    }
+    for (int d = 0; d < 3; ++d) {
+        loadBlock(G, VelB[d], Vf.d.data() + d * cellN, iB, j, k, iMax, dT2, Nr2, false);
+        for (int i = 0; i < iMax; ++i) {
+            double s = 0.0;
+            for (int n = 0; n < recLen; ++n) s = s + interpWgt[n] * (AreaB[n][i] * VelB[d][n][i]);
+            VxyzC[d][i] = s / dA[i];
+        }
+    }
+    for (int i = 0; i < iMax; ++i) {
+        int iG = iB + i;
+        v1[i] = VxyzC[0][i] * G.Te(iG, j, k, TAN1X, dN) + VxyzC[1][i] * G.Te(iG, j, k, TAN1Y, dN) +
+                VxyzC[2][i] * G.Te(iG, j, k, TAN1Z, dN);
+        v2[i] = VxyzC[0][i] * G.Te(iG, j, k, TAN2X, dN) + VxyzC[1][i] * G.Te(iG, j, k, TAN2Y, dN) +
+                VxyzC[2][i] * G.Te(iG, j, k, TAN2Z, dN);
+        vDiff[i] = std::sqrt(sq(v1[i]) + sq(v2[i]));
+    }
+}
+
+static void CalcElecField(const Model& M, const Grid& G, const State& nS, const State& hS, Arr& Vf, Arr& E) {
+    std::fill(E.d.begin(), E.d.end(), 0.0);
+    for (int eD = 1; eD <= NDIM; ++eD) {
+        int dT1, dT2, ie, je, ke;
+        if (eD == IDIR) {
+            dT1 = JDIR; dT2 = KDIR; ie = G.ie; je = G.je + 1; ke = G.ke + 1;
+#pragma omp parallel for collapse(2) schedule(static)
+            for (int k = G.ksg; k <= G.keg; ++k)
+                for (int iB = G.isg; iB <= G.ieg; iB += vecLen)
+                    for (int j = G.js; j <= G.je + 1; ++j) {
+                        int iMax = std::min((int)vecLen, G.ieg - iB + 1);
+                        double VelB[3][vecLen];
+                        Mom2Face(M, G, hS, VelB, iB, j, k, iMax, dT1);
+                        for (int i = 0; i < iMax; ++i) for (int c = 0; c < 3; ++c) Vf(iB + i, j, k, c + 1) = VelB[c][i];
+                    }
+        } else if (eD == JDIR) {
+            dT1 = KDIR; dT2 = IDIR; ie = G.ie + 1; je = G.je; ke = G.ke + 1;
+#pragma omp parallel for collapse(2) schedule(static)
+            for (int j = G.jsg; j <= G.jeg; ++j)
+                for (int iB = G.isg; iB <= G.ieg; iB += vecLen)
+                    for (int k = G.ks; k <= G.ke + 1; ++k) {
+                        int iMax = std::min((int)vecLen, G.ieg - iB + 1);
+                        double VelB[3][vecLen];
+                        Mom2Face(M, G, hS, VelB, iB, j, k, iMax, dT1);
+                        for (int i = 0; i < iMax; ++i) for (int c = 0; c < 3; ++c) Vf(iB + i, j, k, c + 1) = VelB[c][i];
+                    }
+        } else {
+            dT1 = IDIR; dT2 = JDIR; ie = G.ie + 1; je = G.je + 1; ke = G.ke;
+#pragma omp parallel for collapse(2) schedule(static)
+            for (int k = G.ksg; k <= G.keg; ++k)
+                for (int j = G.jsg; j <= G.jeg; ++j)
+                    for (int iB = G.is; iB <= G.ie + 1; iB += vecLen) {
+                        int iMax = std::min((int)vecLen, G.ie + 1 - iB + 1);
+                        double VelB[3][vecLen];
+                        Mom2Face(M, G, hS, VelB, iB, j, k, iMax, dT1);
+                        for (int i = 0; i < iMax; ++i) for (int c = 0; c < 3; ++c) Vf(iB + i, j, k, c + 1) = VelB[c][i];
+                    }
+        }
+#pragma omp parallel for collapse(2) schedule(static)
+        for (int k = G.ks; k <= ke; ++k)
+            for (int j = G.js; j <= je; ++j)
+                for (int iB = G.is; iB <= ie; iB += vecLen) {
+                    int iMax = std::min((int)vecLen, ie - iB + 1);
+                    double v1[vecLen], v2[vecLen], b1[vecLen], b2[vecLen], Jd[vecLen], Dc[vecLen], vDiff[vecLen];
+                    for (int i = 0; i < vecLen; ++i) vDiff[i] = 0.0;
+                    GetCornerV(G, Vf, v1, v2, vDiff, iB, j, k, iMax, eD, dT1, dT2);
+                    GetCornerD(G, hS.Gas, Dc, iB, j, k, iMax, eD);
+                    GetCornerB(M, G, nS.magFlux, hS.magFlux, b1, b2, Jd, iB, j, k, iMax, eD, dT1, dT2);
+                    for (int i = 0; i < iMax; ++i) {
+                        int iG = iB + i;
+                        double vA = std::sqrt(sq(b1[i]) + sq(b2[i])) / std::sqrt(Dc[i]);
+                        if (M.doBoris) vA = M.Ca * vA / std::sqrt(sq(M.Ca) + sq(vA));
+                        vDiff[i] = vDiff[i] + vA;
+                        vDiff[i] = fmind(vDiff[i], M.CFL * G.edge(iG, j, k, eD) / M.dt);
+                        double e = -(v1[i] * b2[i] - v2[i] * b1[i]) + M.Vd0 * vDiff[i] * Jd[i];
+                        E(iG, j, k, eD) = e * G.edge(iG, j, k, eD);
+                    }
+                }
+    }
+}
+
+static void E2Flux(const Grid& G, Arr& mf, const Arr& E, double dt) {  // fields.F90:18-51
+#pragma omp parallel for collapse(2) schedule(static)
+    for (int k = G.ks; k <= G.ke + 1; ++k)
+        for (int j = G.js; j <= G.je + 1; ++j)
+            for (int i = G.is; i <= G.ie + 1; ++i) {
+                double dfi = E(i, j + 1, k, KDIR) - E(i, j, k, KDIR) - E(i, j, k + 1, JDIR) + E(i, j, k, JDIR);
+                double dfj = E(i, j, k + 1, IDIR) - E(i, j, k, IDIR) - E(i + 1, j, k, KDIR) + E(i, j, k, KDIR);
+                double dfk = E(i + 1, j, k, JDIR) - E(i, j, k, JDIR) - E(i, j + 1, k, IDIR) + E(i, j, k, IDIR);
+                mf(i, j, k, IDIR) = mf(i, j, k, IDIR) - dt * dfi;
+                mf(i, j, k, JDIR) = mf(i, j, k, JDIR) - dt * dfj;
+                mf(i, j, k, KDIR) = mf(i, j, k, KDIR) - dt * dfk;
+            }
+}
+
+// ---------------------------------------------------------------- update (mhdgroup.F90:79-442)
+static inline double dot3(const double* a, const double* b) { return dot(a, b, 3); }
+static void normVec3(const double* a, double* o) {
+    double nA = std::sqrt(dot3(a, a));
+    if (nA <= TINY) { o[0] = o[1] = o[2] = 0.0; }
+    else { o[0] = a[0] / nA; o[1] = a[1] / nA; o[2] = a[2] / nA; }
+}
+static void Vec2Para(const double* A, const double* n, double* o) {
+    double s = dot3(A, n);
+    for (int c = 0; c < 3; ++c) o[c] = s * n[c];
+}
+static void Vec2Perp(const double* A, const double* n, double* o) {
+    double p[3];
+    Vec2Para(A, n, p);
+    for (int c = 0; c < 3; ++c) o[c] = A[c] - p[c];
+}
+static void CellMaxwell(const Model& M, double* U, const double* dGasM, double dt) {  // mhdgroup.F90:300-330
+    double D = fmaxd(U[0], M.dFloor), Mx = U[1], My = U[2], Mz = U[3], TotE = U[4];
+    double KinE = 0.5 * (sq(Mx) + sq(My) + sq(Mz)) / D;
+    double P = fmaxd((M.gamma - 1) * (TotE - KinE), M.pFloor);
+    Mx = Mx + dt * dGasM[0];
+    My = My + dt * dGasM[1];
+    Mz = Mz + dt * dGasM[2];
+    KinE = 0.5 * (sq(Mx) + sq(My) + sq(Mz)) / D;
+    U[0] = D; U[1] = Mx; U[2] = My; U[3] = Mz; U[4] = KinE + P / (M.gamma - 1);
+}
+static void CellBoris(const Model& M, double* U2, const double* U0, const double* B2, const double* B0,
+                      const double* dGasH, const double* dGasM, double Ca, double dt) {  // mhdgroup.F90:337-390
+    double W2[5];
+    CellC2P(M, U2, W2);
+    double D2 = fmaxd(W2[0], M.dFloor), P2 = fmaxd(W2[4], M.pFloor);
+    double D0 = U0[0];
+    D0 = fmaxd(D0, M.dFloor);
+    double V0[3] = {U0[1] / D0, U0[2] / D0, U0[3] / D0};
+    double B1[3];
+    for (int c = 0; c < 3; ++c) B1[c] = 0.5 * (B2[c] + B0[c]);
+    double alpha = dot3(B1, B1) / (D2 * Ca * Ca);
+    double dRho = dt * dGasH[0];
+    double dPGas[3], dPMag[3], dMom[3];
+    for (int c = 0; c < 3; ++c) { dPGas[c] = dt * dGasH[1 + c]; dPMag[c] = dt * dGasM[c]; }
+    double pCon = 1.0 / (1.0 + alpha);
+    double bhat1[3];
+    normVec3(B1, bhat1);
+    if (alpha > TINY) {
+        double a[3], s[3], b[3], c3[3], d[3];
+        Vec2Para(dPGas, bhat1, a);
+        for (int c = 0; c < 3; ++c) s[c] = dPGas[c] + dPMag[c];
+        Vec2Perp(s, bhat1, b);
+        Vec2Perp(V0, bhat1, c3);
+        for (int c = 0; c < 3; ++c) { d[c] = a[c] + pCon * b[c]; dMom[c] = d[c] + alpha * pCon * dRho * c3[c]; }
+    } else {
+        for (int c = 0; c < 3; ++c) dMom[c] = dPGas[c] + dPMag[c];
+    }
+    double V2[3];
+    for (int c = 0; c < 3; ++c) V2[c] = (D0 * V0[c] + dMom[c]) / D2;
+    W2[0] = D2; W2[1] = V2[0]; W2[2] = V2[1]; W2[3] = V2[2]; W2[4] = P2;
+    CellP2C(M, W2, U2);
+}
+
+// applyUpdate with the buffer roles of the reference: CopyState(State->oState) then in-place update of State
+static void applyUpdate(Model& M, const Grid& G, State& S, State& oS, double dt, const Arr& dGasH, const Arr& dGasM,
+                        Arr& E) {
+    oS.Gas.d = S.Gas.d;
+    oS.Bxyz.d = S.Bxyz.d;
+    oS.magFlux.d = S.magFlux.d;
+    oS.time = S.time;
+    S.time = S.time + dt;
+#pragma omp parallel for collapse(2) schedule(static)
+    for (int k = G.ks; k <= G.ke; ++k)
+        for (int j = G.js; j <= G.je; ++j)
+            for (int i = G.is; i <= G.ie; ++i)
+                for (int v = 1; v <= NVAR; ++v) S.Gas(i, j, k, v) = S.Gas(i, j, k, v) + M.dt * dGasH(i, j, k, v);
+    if (!M.doMHD) return;
+    E2Flux(G, S.magFlux, E, dt);
+    bFlux2Fld(G, S.magFlux, S.Bxyz);
+    bool Boris = M.doBoris;
+#pragma omp parallel for collapse(2) schedule(static)
+    for (int k = G.ks; k <= G.ke; ++k)
+        for (int j = G.js; j <= G.je; ++j)
+            for (int i = G.is; i <= G.ie; ++i) {
+                double U[5], dPm[3];
+                for (int v = 0; v < 5; ++v) U[v] = S.Gas(i, j, k, v + 1);
+                for (int c = 0; c < 3; ++c) dPm[c] = dGasM(i, j, k, c + 1);
+                if (Boris) {
+                    double oU[5], B[3], oB[3], dPg[5];
+                    for (int v = 0; v < 5; ++v) { oU[v] = oS.Gas(i, j, k, v + 1); dPg[v] = dGasH(i, j, k, v + 1); }
+                    for (int c = 0; c < 3; ++c) { B[c] = S.Bxyz(i, j, k, c + 1); oB[c] = oS.Bxyz(i, j, k, c + 1); }
+                    CellBoris(M, U, oU, B, oB, dPg, dPm, M.Ca, dt);
+                } else {
+                    CellMaxwell(M, U, dPm, dt);
+                }
+                for (int v = 0; v < 5; ++v) S.Gas(i, j, k, v + 1) = U[v];
+            }
+}
+
+// ---------------------------------------------------------------- dt (gridutils.F90:49-106, step.F90:58-168)
+static double CellDT(const Model& M, const Grid& G, const State& S, int i, int j, int k) {
+    double rho = S.Gas(i, j, k, DEN);
+    double Vx = S.Gas(i, j, k, MOMX) / rho, Vy = S.Gas(i, j, k, MOMY) / rho, Vz = S.Gas(i, j, k, MOMZ) / rho;
+    double MagV = std::sqrt(sq(Vx) + sq(Vy) + sq(Vz));
+    double ke = 0.5 * rho * sq(MagV);
+    double e = S.Gas(i, j, k, ENERGY) - ke;
+    double P = (M.gamma - 1) * e;
+    double Cs = std::sqrt(M.gamma * P / rho);
+    double Vfl = MagV, Valf = 0.0, Vdiff = 0.0;
+    if (M.doMHD) {
+        double Bx = S.Bxyz(i, j, k, XDIR), By = S.Bxyz(i, j, k, YDIR), Bz = S.Bxyz(i, j, k, ZDIR);
+        double MagB = std::sqrt(sq(Bx) + sq(By) + sq(Bz));
+        Valf = MagB / std::sqrt(rho);
+        if (M.doBoris) Valf = M.Ca * Valf / std::sqrt(M.Ca * M.Ca + Valf * Valf);
+    }
+    double vCFL = Vfl + std::sqrt(sq(Cs) + sq(Valf)) + Vdiff;
+    double dl = G.di(i, j, k);
+    if (G.dj(i, j, k) < dl) dl = G.dj(i, j, k);
+    if (G.dk(i, j, k) < dl) dl = G.dk(i, j, k);
+    return M.CFL * dl / vCFL;
+}
+
+static double CalcDT(Model& M, const Grid& G, const State& S) {
+    if (M.fixedTimestep) return M.dt;
+    double dtOld = M.dt;
+    double dtMin = HUGEV;
+    bool isDisaster = false, isBad = false;
+#pragma omp parallel for collapse(2) reduction(min : dtMin) schedule(static)
+    for (int k = G.ksDT; k <= G.keDT; ++k)
+        for (int j = G.jsDT; j <= G.jeDT; ++j)
+            for (int i = G.isDT; i <= G.ieDT; ++i) {
+                double dtijk = CellDT(M, G, S, i, j, k);
+                dtMin = fmind(dtijk, dtMin);
+            }
+    if (dtMin == HUGEV) isDisaster = true;
+    double r = dtMin;
+    if (M.ts > 0) {
+        if (dtOld / dtMin >= 10) isBad = true;
+        if ((M.dt0 > TINY) && (dtMin / M.dt0 <= M.limDT0)) isBad = true;
+        if (dtMin <= TINY) isDisaster = true;
+    }
+    M.status = (isDisaster ? 1 : 0) | (isBad ? 2 : 0);
+    if ((M.t + r) > M.tFin) r = fmaxd(M.tFin - M.t, TINY);
+    if (M.dt0 > TINY && r > (10.0 * M.dt0)) r = 10.0 * M.dt0;
+    return r;
+}
+
+// ---------------------------------------------------------------- boundary conditions (bcs.F90)
+static void copyCellVec(Arr& A, int i, int j, int k, int si, int sj, int sk, int nc) {
+    for (int c = 1; c <= nc; ++c) A(i, j, k, c) = A(si, sj, sk, c);
+}
+static void periodicBC(const Model& M, const Grid& G, State& S, int dir) {  // bcs.F90:279-450
+    const int nG = M.nG;
+    switch (dir) {
+    case INI:
+        for (int k = G.ksg; k <= G.keg + 1; ++k)
+            for (int j = G.jsg; j <= G.jeg + 1; ++j)
+                for (int n = 1; n <= nG; ++n) {
+                    int ig = G.is - n;
+                    if (j <= G.jeg && k <= G.keg) {
+                        copyCellVec(S.Gas, ig, j, k, G.ie - n + 1, j, k, 5);
+                        copyCellVec(S.Bxyz, ig, j, k, G.ie - n + 1, j, k, 3);
+                    }
+                    copyCellVec(S.magFlux, ig, j, k, G.ie - n + 1, j, k, 3);
+                }
+        break;
+    case OUTI:
+        for (int k = G.ksg; k <= G.keg + 1; ++k)
+            for (int j = G.jsg; j <= G.jeg + 1; ++j)
+                for (int n = 1; n <= nG; ++n) {
+                    int ig = G.ie + n;
+                    if (j <= G.jeg && k <= G.keg) {
+                        copyCellVec(S.Gas, ig, j, k, G.is + n - 1, j, k, 5);
+                        copyCellVec(S.Bxyz, ig, j, k, G.is + n - 1, j, k, 3);
+                    }
+                    S.magFlux(ig, j, k, JDIR) = S.magFlux(G.is + n - 1, j, k, JDIR);
+                    S.magFlux(ig, j, k, KDIR) = S.magFlux(G.is + n - 1, j, k, KDIR);
+                    S.magFlux(ig + 1, j, k, IDIR) = S.magFlux(G.is + n, j, k, IDIR);
+                }
+        break;
+    case INJ:
+        for (int k = G.ksg; k <= G.keg + 1; ++k)
+            for (int i = G.isg; i <= G.ieg + 1; ++i)
+                for (int n = 1; n <= nG; ++n) {
+                    int jg = G.js - n;
+                    if (i <= G.ieg && k <= G.keg) {
+                        copyCellVec(S.Gas, i, jg, k, i, G.je - n + 1, k, 5);
+                        copyCellVec(S.Bxyz, i, jg, k, i, G.je - n + 1, k, 3);
+                    }
+                    copyCellVec(S.magFlux, i, jg, k, i, G.je - n + 1, k, 3);
+                }
+        break;
+    case OUTJ:
+        for (int k = G.ksg; k <= G.keg + 1; ++k)
+            for (int i = G.isg; i <= G.ieg + 1; ++i)
+                for (int n = 1; n <= nG; ++n) {
+                    int jg = G.je + n;
+                    if (i <= G.ieg && k <= G.keg) {
+                        copyCellVec(S.Gas, i, jg, k, i, G.js + n - 1, k, 5);
+                        copyCellVec(S.Bxyz, i, jg, k, i, G.js + n - 1, k, 3);
+                    }
+                    S.magFlux(i, jg, k, IDIR) = S.magFlux(i, G.js + n - 1, k, IDIR);
+                    S.magFlux(i, jg, k, KDIR) = S.magFlux(i, G.js + n - 1, k, KDIR);
+                    S.magFlux(i, jg + 1, k, JDIR) = S.magFlux(i, G.js + n, k, JDIR);
+                }
+        break;
+    case INK:
+        if (M.do25D) {
+            for (int n = 1; n <= nG; ++n)
+                for (int j = G.jsg; j <= G.jeg + 1; ++j)
+                    for (int i = G.isg; i <= G.ieg + 1; ++i) {
+                        if (i <= G.ieg && j <= G.jeg) {
+                            copyCellVec(S.Gas, i, j, G.ks - n, i, j, G.ks, 5);
+                            copyCellVec(S.Bxyz, i, j, G.ks - n, i, j, G.ks, 3);
+                        }
+                        copyCellVec(S.magFlux, i, j, G.ks - n, i, j, G.ks, 3);
+                    }
+        } else {
+            for (int j = G.jsg; j <= G.jeg + 1; ++j)
+                for (int i = G.isg; i <= G.ieg + 1; ++i)
+                    for (int n = 1; n <= nG; ++n) {
+                        int kg = G.ks - n;
+                        if (i <= G.ieg && j <= G.jeg) {
+                            copyCellVec(S.Gas, i, j, kg, i, j, G.ke - n + 1, 5);
+                            copyCellVec(S.Bxyz, i, j, kg, i, j, G.ke - n + 1, 3);
+                        }
+                        copyCellVec(S.magFlux, i, j, kg, i, j, G.ke - n + 1, 3);
+                    }
+        }
+        break;
+    case OUTK:
+        if (M.do25D) {
+            for (int n = 1; n <= nG; ++n)
+                for (int j = G.jsg; j <= G.jeg + 1; ++j)
+                    for (int i = G.isg; i <= G.ieg + 1; ++i) {
+                        if (i <= G.ieg && j <= G.jeg) {
+                            copyCellVec(S.Gas, i, j, G.ks + n, i, j, G.ks, 5);
+                            copyCellVec(S.Bxyz, i, j, G.ks + n, i, j, G.ks, 3);
+                        }
+                        copyCellVec(S.magFlux, i, j, G.ks + n, i, j, G.ks, 3);
+                    }
+        } else {
+            for (int j = G.jsg; j <= G.jeg + 1; ++j)
+                for (int i = G.isg; i <= G.ieg + 1; ++i)
+                    for (int n = 1; n <= nG; ++n) {
+                        int kg = G.ke + n;
+                        if (i <= G.ieg && j <= G.jeg) {
+                            copyCellVec(S.Gas, i, j, kg, i, j, G.ks + n - 1, 5);
+                            copyCellVec(S.Bxyz, i, j, kg, i, j, G.ks + n - 1, 3);
+                        }
+                        S.magFlux(i, j, kg, IDIR) = S.magFlux(i, j, G.ks + n - 1, IDIR);
+                        S.magFlux(i, j, kg, JDIR) = S.magFlux(i, j, G.ks + n - 1, JDIR);
+                        S.magFlux(i, j, kg + 1, KDIR) = S.magFlux(i, j, G.ks + n, KDIR);
+                    }
+        }
+        break;
+    }
+}
+// isCellCenterG is true for cell-centred indices inside the allocated cell range; the guards above
+// (i<=ieg, j<=jeg, k<=keg) restate it for the loops that run to the +1 face index.
+
+static void zeroGradBC(const Model& M, const Grid& G, State& S, int dir) {  // bcs.F90:799-930
+    const int nG = M.nG;
+    switch (dir) {
+    case INI:
+        for (int k = G.ksg; k <= G.keg; ++k)
+            for (int j = G.jsg; j <= G.jeg; ++j)
+                for (int n = 1; n <= nG; ++n) {
+                    copyCellVec(S.Gas, G.is - n, j, k, G.is, j, k, 5);
+                    copyCellVec(S.magFlux, G.is - n, j, k, G.is, j, k, 3);
+                }
+        break;
+    case OUTI:
+        for (int k = G.ksg; k <= G.keg; ++k)
+            for (int j = G.jsg; j <= G.jeg; ++j) {
+                double B[3];
+                gamCellBxyz(G, S.magFlux, G.ie, j, k, B);
+                for (int n = 1; n <= nG; ++n) {
+                    int ig = G.ie + n;
+                    copyCellVec(S.Gas, ig, j, k, G.ie, j, k, 5);
+                    double t1[3] = {G.Tf(ig + 1, j, k, NORMX, IDIR), G.Tf(ig + 1, j, k, NORMY, IDIR), G.Tf(ig + 1, j, k, NORMZ, IDIR)};
+                    double t2[3] = {G.Tf(ig, j, k, NORMX, JDIR), G.Tf(ig, j, k, NORMY, JDIR), G.Tf(ig, j, k, NORMZ, JDIR)};
+                    double t3[3] = {G.Tf(ig, j, k, NORMX, KDIR), G.Tf(ig, j, k, NORMY, KDIR), G.Tf(ig, j, k, NORMZ, KDIR)};
+                    S.magFlux(ig + 1, j, k, IDIR) = G.face(ig + 1, j, k, IDIR) * dot3(B, t1);
+                    S.magFlux(ig, j, k, JDIR) = G.face(ig, j, k, JDIR) * dot3(B, t2);
+                    S.magFlux(ig, j, k, KDIR) = G.face(ig, j, k, KDIR) * dot3(B, t3);
+                }
+            }
+        break;
+    case INJ:
+        for (int k = G.ksg; k <= G.keg; ++k)
+            for (int n = 1; n <= nG; ++n)
+                for (int i = G.isg; i <= G.ieg; ++i) {
+                    copyCellVec(S.Gas, i, G.js - n, k, i, G.js, k, 5);
+                    copyCellVec(S.magFlux, i, G.js - n, k, i, G.js, k, 3);
+                }
+        break;
+    case OUTJ:
+        for (int k = G.ksg; k <= G.keg; ++k)
+            for (int n = 1; n <= nG; ++n)
+                for (int i = G.isg; i <= G.ieg; ++i) {
+                    copyCellVec(S.Gas, i, G.je + n, k, i, G.je, k, 5);
+                    S.magFlux(i, G.je + n, k, IDIR) = S.magFlux(i, G.je, k, IDIR);
+                    S.magFlux(i, G.je + n, k, KDIR) = S.magFlux(i, G.je, k, KDIR);
+                    S.magFlux(i, G.je + n + 1, k, JDIR) = S.magFlux(i, G.je + 1, k, JDIR);
+                }
+        break;
+    case INK:
+        for (int n = 1; n <= nG; ++n)
+            for (int j = G.jsg; j <= G.jeg; ++j)
+                for (int i = G.isg; i <= G.ieg; ++i) {
+                    copyCellVec(S.Gas, i, j, G.ks - n, i, j, G.ks, 5);
+                    copyCellVec(S.magFlux, i, j, G.ks - n, i, j, G.ks, 3);
+                }
+        break;
+    case OUTK:
+        for (int n = 1; n <= nG; ++n)
+            for (int j = G.jsg; j <= G.jeg; ++j)
+                for (int i = G.isg; i <= G.ieg; ++i) {
+                    copyCellVec(S.Gas, i, j, G.ke + n, i, j, G.ke, 5);
+                    S.magFlux(i, j, G.ke + n, XDIR) = S.magFlux(i, j, G.ke, IDIR);
+                    S.magFlux(i, j, G.ke + n, YDIR) = S.magFlux(i, j, G.ke, JDIR);
+                    // bcs.F90:924 copies the J component of face ke+1 into the K faces above it; kept as is.
+                    S.magFlux(i, j, G.ke + n + 1, ZDIR) = S.magFlux(i, j, G.ke + 1, JDIR);
+                }
+        break;
+    }
+}
+
+static void EnforceBCs(const Model& M, const Grid& G, State& S) {  // step.F90:17-55
+    for (int n = 1; n <= 6; ++n) {
+        if (G.bc[n - 1] == BC_PERIODIC) periodicBC(M, G, S, n);
+        else zeroGradBC(M, G, S, n);
+    }
+}
+
+// ---------------------------------------------------------------- one step (gamapp.F90:73-116, mhdgroup.F90:16-76)
+static void AdvanceMHD(App& A, double dt) {
+    Model& M = A.M;
+    if (std::fabs(A.oS.time - A.S.time) < TINY) A.oS.time = A.S.time - M.dt;
+    Predictor(M, A.G, A.S, A.oS, A.V.StateHf, 0.5 * dt);
+    if (M.doMHD) CalcElecField(M, A.G, A.S, A.V.StateHf, A.V.Vf, A.S.Efld);
+    CalcStress(M, A.G, A.S, A.V.StateHf, A.V.gFlx, A.V.mFlx, A.V.dGasH, A.V.dGasM);
+    applyUpdate(M, A.G, A.S, A.oS, dt, A.V.dGasH, A.V.dGasM, A.S.Efld);
+}
+static void stepGamera(App& A) {
+    AdvanceMHD(A, A.M.dt);
+    A.M.ts = A.M.ts + 1;
+    A.M.t = A.M.t + A.M.dt;
+    A.M.dt = CalcDT(A.M, A.G, A.S);
+    EnforceBCs(A.M, A.G, A.S);
+    bFlux2Fld(A.G, A.S.magFlux, A.S.Bxyz);
+}
+
+// ---------------------------------------------------------------- setup (init.F90, quadrature.F90, metric.F90)
+static const double gA[12] = {0.1252334085114689154724, 0.3678314989981801937527, 0.5873179542866174472967,
+                              0.7699026741943046870369, 0.9041172563704748566785, 0.9815606342467192506906,
+                              -0.1252334085114689154724, -0.3678314989981801937527, -0.5873179542866174472967,
+                              -0.7699026741943046870369, -0.9041172563704748566785, -0.9815606342467192506906};
+static const double gWgt[12] = {0.2491470458134027850006, 0.233492536538354808761, 0.203167426723065921749,
+                                0.160078328543346226335, 0.1069393259953184309603, 0.0471753363865118271946,
+                                0.2491470458134027850006, 0.233492536538354808761, 0.203167426723065921749,
+                                0.160078328543346226335, 0.1069393259953184309603, 0.0471753363865118271946};
+
+static void faceCoords(const Grid& G, int i, int j, int k, int d, double* f0, double* f1, double* f2, double* f3) {
+    for (int c = 0; c < 3; ++c) {
+        f0[c] = G.xyz(i, j, k, c + 1);
+        if (d == IDIR) { f1[c] = G.xyz(i, j + 1, k, c + 1); f2[c] = G.xyz(i, j, k + 1, c + 1); f3[c] = G.xyz(i, j + 1, k + 1, c + 1); }
+        else if (d == JDIR) { f1[c] = G.xyz(i, j, k + 1, c + 1); f2[c] = G.xyz(i + 1, j, k, c + 1); f3[c] = G.xyz(i + 1, j, k + 1, c + 1); }
+        else { f1[c] = G.xyz(i + 1, j, k, c + 1); f2[c] = G.xyz(i, j + 1, k, c + 1); f3[c] = G.xyz(i + 1, j + 1, k, c + 1); }
+    }
+}
+static void cellCoords(const Grid& G, int i, int j, int k, double xyzC[8][3]) {
+    const int di[8] = {0, 1, 1, 0, 0, 1, 1, 0}, dj[8] = {0, 0, 1, 1, 0, 0, 1, 1}, dk[8] = {0, 0, 0, 0, 1, 1, 1, 1};
+    for (int p = 0; p < 8; ++p) for (int c = 0; c < 3; ++c) xyzC[p][c] = G.xyz(i + di[p], j + dj[p], k + dk[p], c + 1);
+}
+
+typedef void (*VecFun)(double, double, double, double*, void*);
+typedef void (*GasFun)(double, double, double, double*, void*);
+
+// GaussianFaceIntegral (quadrature.F90:159-221), returns fInt only (fInt2/fIntX are unused by the callers here)
+static void GaussianFaceIntegral(const double* f0, const double* f1, const double* f2, const double* f3, VecFun A,
+                                 void* ctx, double* fInt) {
+    double dx[3], dy[3], dz[3];
+    dx[0] = f1[0] - f0[0]; dx[1] = f2[0] - f0[0]; dx[2] = f3[0] + f0[0] - f2[0] - f1[0];
+    dy[0] = f1[1] - f0[1]; dy[1] = f2[1] - f0[1]; dy[2] = f3[1] + f0[1] - f2[1] - f1[1];
+    dz[0] = f1[2] - f0[2]; dz[1] = f2[2] - f0[2]; dz[2] = f3[2] + f0[2] - f2[2] - f1[2];
+    fInt[0] = fInt[1] = fInt[2] = 0.0;
+    for (int i = 0; i < 12; ++i)
+        for (int j = 0; j < 12; ++j) {
+            double eta = 0.5 * (1 + gA[i]), psi = 0.5 * (1 + gA[j]);
+            double w = gWgt[i] * gWgt[j];
+            double xp = f0[0] + dx[0] * eta + dx[1] * psi + dx[2] * eta * psi;
+            double yp = f0[1] + dy[0] * eta + dy[1] * psi + dy[2] * eta * psi;
+            double zp = f0[2] + dz[0] * eta + dz[1] * psi + dz[2] * eta * psi;
+            double Ap[3];
+            A(xp, yp, zp, Ap, ctx);
+            double etaV[3] = {dx[0] + dx[2] * psi, dy[0] + dy[2] * psi, dz[0] + dz[2] * psi};
+            double psiV[3] = {dx[1] + dx[2] * eta, dy[1] + dy[2] * eta, dz[1] + dz[2] * eta};
+            double cr[3];
+            cross3(etaV, psiV, cr);
+            double area = 0.25 * norm2v(cr, 3) * w;
+            fInt[0] = fInt[0] + area * Ap[0];
+            fInt[1] = fInt[1] + area * Ap[1];
+            fInt[2] = fInt[2] + area * Ap[2];
+        }
+}
+static double DetJ(double J[3][3]) {  // math.F90:470-478, J[row][col]
+    return J[0][0] * (J[1][1] * J[2][2] - J[1][2] * J[2][1]) - J[0][1] * (J[1][0] * J[2][2] - J[1][2] * J[2][0]) +
+           J[0][2] * (J[1][0] * J[2][1] - J[1][1] * J[2][0]);
+}
+// GaussianVolumeIntegral (quadrature.F90:42-100)
+static void GaussianVolumeIntegral(double xyzC[8][3], GasFun W, void* ctx, double* wInt) {
+    const int iS[8] = {-1, +1, +1, -1, -1, +1, +1, -1}, jS[8] = {-1, -1, +1, +1, -1, -1, +1, +1},
+              kS[8] = {-1, -1, -1, -1, +1, +1, +1, +1};
+    for (int v = 0; v < 5; ++v) wInt[v] = 0.0;
+    for (int i = 0; i < 12; ++i)
+        for (int j = 0; j < 12; ++j)
+            for (int k = 0; k < 12; ++k) {
+                double wijk = gWgt[i] * gWgt[j] * gWgt[k];
+                double iScl[8], jScl[8], kScl[8];
+                for (int p = 0; p < 8; ++p) {
+                    iScl[p] = (iS[p] < 0) ? (1 - gA[i]) : (1 + gA[i]);
+                    jScl[p] = (jS[p] < 0) ? (1 - gA[j]) : (1 + gA[j]);
+                    kScl[p] = (kS[p] < 0) ? (1 - gA[k]) : (1 + gA[k]);
+                }
+                double xp[3], Jac[3][3];
+                for (int c = 0; c < 3; ++c) {
+                    double s = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
+                    for (int p = 0; p < 8; ++p) s = s + xyzC[p][c] * (iScl[p] * jScl[p] * kScl[p]);
+                    for (int p = 0; p < 8; ++p) s1 = s1 + xyzC[p][c] * (iS[p] * jScl[p] * kScl[p]);
+                    for (int p = 0; p < 8; ++p) s2 = s2 + xyzC[p][c] * (iScl[p] * jS[p] * kScl[p]);
+                    for (int p = 0; p < 8; ++p) s3 = s3 + xyzC[p][c] * (iScl[p] * jScl[p] * kS[p]);
+                    xp[c] = 0.125 * s;
+                    Jac[c][0] = 0.125 * s1; Jac[c][1] = 0.125 * s2; Jac[c][2] = 0.125 * s3;
+                }
+                double dJ = std::fabs(DetJ(Jac));
+                double Wp[5];
+                W(xp[0], xp[1], xp[2], Wp, ctx);
+                for (int v = 0; v < 5; ++v) wInt[v] = wInt[v] + dJ * wijk * Wp[v];
+            }
+}
+// GaussianEdgeIntegral (quadrature.F90:345-370)
+static void GaussianEdgeIntegral(const double* e1, const double* e2, VecFun A, void* ctx, double* eInt) {
+    double dR2[3], xBar[3];
+    for (int c = 0; c < 3; ++c) { dR2[c] = 0.5 * (e2[c] - e1[c]); xBar[c] = 0.5 * (e2[c] + e1[c]); }
+    eInt[0] = eInt[1] = eInt[2] = 0.0;
+    for (int i = 0; i < 12; ++i) {
+        double xp[3], Ap[3];
+        for (int c = 0; c < 3; ++c) xp[c] = xBar[c] + gA[i] * dR2[c];
+        A(xp[0], xp[1], xp[2], Ap, ctx);
+        for (int c = 0; c < 3; ++c) eInt[c] = eInt[c] + 0.5 * gWgt[i] * Ap[c];
+    }
+}
+static void IdVec(double, double, double, double* A, void*) { A[0] = A[1] = A[2] = 1.0; }
+static void rVec(double x, double y, double z, double* A, void*) { A[0] = x; A[1] = y; A[2] = z; }
+static void CellDV(double x, double y, double z, double* W, void*) { W[0] = 1; W[1] = x; W[2] = y; W[3] = z; W[4] = 0; }
+
+static void allocGrid(const Model& M, Grid& G) {
+    G.Ni = G.Nip + 2 * M.nG; G.Nj = G.Njp + 2 * M.nG; G.Nk = G.Nkp + 2 * M.nG;
+    G.is = 1; G.ie = G.Nip; G.js = 1; G.je = G.Njp; G.ks = 1; G.ke = G.Nkp;
+    G.isg = G.is - M.nG; G.ieg = G.ie + M.nG; G.jsg = G.js - M.nG; G.jeg = G.je + M.nG;
+    G.ksg = G.ks - M.nG; G.keg = G.ke + M.nG;
+    int lo4[4] = {G.isg, G.jsg, G.ksg, 1};
+    int hi4p[4] = {G.ieg + 1, G.jeg + 1, G.keg + 1, 3};
+    G.xyz.alloc(4, lo4, hi4p);
+}
+
+// SetDomain (init.F90:519-538) for a single untiled grid
+static void SetDomain(Grid& G) {
+    G.isDT = G.is - 1; G.ieDT = G.ie + 1; G.jsDT = G.js - 1; G.jeDT = G.je + 1; G.ksDT = G.ks - 1; G.keDT = G.ke + 1;
+}
+
+static int Corners2Grid(const Model& M, Grid& G) {  // init.F90:801-1080
+    if ((G.ie - G.is + 1) < vecLen) return -1;
+    if (((G.ie - G.is + 1) % 8) != 0) return -2;
+    int lo[5], hi[5];
+    lo[0] = G.isg; lo[1] = G.jsg; lo[2] = G.ksg; lo[3] = 1; lo[4] = 1;
+    hi[0] = G.ieg; hi[1] = G.jeg; hi[2] = G.keg; hi[3] = 3;
+    G.xyzcc.alloc(4, lo, hi);
+    hi[0] = G.ieg + 1; hi[1] = G.jeg + 1; hi[2] = G.keg + 1; hi[3] = 3; hi[4] = 3;
+    G.xfc.alloc(5, lo, hi);
+    G.face.alloc(4, lo, hi);
+    std::fill(G.face.d.begin(), G.face.d.end(), 1.0);
+    hi[3] = 9; hi[4] = 3;
+    G.Tf.alloc(5, lo, hi);
+    for (int d = 1; d <= 3; ++d) {
+        int DelI = ijkD(d, IDIR), DelJ = ijkD(d, JDIR), DelK = ijkD(d, KDIR);
+#pragma omp parallel for collapse(2) schedule(static)
+        for (int k = G.ksg; k <= G.keg + DelK; ++k)
+            for (int j = G.jsg; j <= G.jeg + DelJ; ++j)
+                for (int i = G.isg; i <= G.ieg + DelI; ++i) {
+                    double f0[3], f1[3], f2[3], f3[3], fInt[3];
+                    faceCoords(G, i, j, k, d, f0, f1, f2, f3);
+                    GaussianFaceIntegral(f0, f1, f2, f3, IdVec, nullptr, fInt);
+                    double fA = fInt[0];
+                    GaussianFaceIntegral(f0, f1, f2, f3, rVec, nullptr, fInt);
+                    for (int c = 0; c < 3; ++c) G.xfc(i, j, k, c + 1, d) = fInt[c] / fA;
+                    G.face(i, j, k, d) = fA;
+                    double dT1[3], dT2[3];
+                    for (int c = 1; c <= 3; ++c) {
+                        if (d == IDIR) {
+                            dT1[c - 1] = 0.5 * (G.xyz(i, j + 1, k + 1, c) - G.xyz(i, j, k + 1, c)) + 0.5 * (G.xyz(i, j + 1, k, c) - G.xyz(i, j, k, c));
+                            dT2[c - 1] = 0.5 * (G.xyz(i, j + 1, k + 1, c) - G.xyz(i, j + 1, k, c)) + 0.5 * (G.xyz(i, j, k + 1, c) - G.xyz(i, j, k, c));
+                        } else if (d == JDIR) {
+                            dT1[c - 1] = 0.5 * (G.xyz(i + 1, j, k + 1, c) - G.xyz(i + 1, j, k, c)) + 0.5 * (G.xyz(i, j, k + 1, c) - G.xyz(i, j, k, c));
+                            dT2[c - 1] = 0.5 * (G.xyz(i + 1, j, k + 1, c) - G.xyz(i, j, k + 1, c)) + 0.5 * (G.xyz(i + 1, j, k, c) - G.xyz(i, j, k, c));
+                        } else {
+                            dT1[c - 1] = 0.5 * (G.xyz(i + 1, j + 1, k, c) - G.xyz(i, j + 1, k, c)) + 0.5 * (G.xyz(i + 1, j, k, c) - G.xyz(i, j, k, c));
+                            dT2[c - 1] = 0.5 * (G.xyz(i + 1, j + 1, k, c) - G.xyz(i + 1, j, k, c)) + 0.5 * (G.xyz(i, j + 1, k, c) - G.xyz(i, j, k, c));
+                        }
+                    }
+                    double cr[3], eN[3], eT1[3], eT2[3];
+                    cross3(dT1, dT2, cr);
+                    double ncr = norm2v(cr, 3);
+                    for (int c = 0; c < 3; ++c) eN[c] = cr[c] / ncr;
+                    double nT2 = norm2v(dT2, 3);
+                    for (int c = 0; c < 3; ++c) eT2[c] = dT2[c] / nT2;
+                    cross3(eT2, eN, cr);
+                    ncr = norm2v(cr, 3);
+                    for (int c = 0; c < 3; ++c) eT1[c] = cr[c] / ncr;
+                    for (int c = 0; c < 3; ++c) {
+                        G.Tf(i, j, k, NORMX + c, d) = eN[c];
+                        G.Tf(i, j, k, TAN1X + c, d) = eT1[c];
+                        G.Tf(i, j, k, TAN2X + c, d) = eT2[c];
+                    }
+                }
+    }
+    hi[0] = G.ieg; hi[1] = G.jeg; hi[2] = G.keg;
+    G.volume.alloc(3, lo, hi); G.di.alloc(3, lo, hi); G.dj.alloc(3, lo, hi); G.dk.alloc(3, lo, hi);
+#pragma omp parallel for collapse(2) schedule(static)
+    for (int k = G.ksg; k <= G.keg; ++k)
+        for (int j = G.jsg; j <= G.jeg; ++j)
+            for (int i = G.isg; i <= G.ieg; ++i) {
+                double dI[3], dJ[3], dK[3];
+                for (int c = 1; c <= 3; ++c) {
+                    dI[c - 1] = G.xfc(i + 1, j, k, c, IDIR) - G.xfc(i, j, k, c, IDIR);
+                    dJ[c - 1] = G.xfc(i, j + 1, k, c, JDIR) - G.xfc(i, j, k, c, JDIR);
+                    dK[c - 1] = G.xfc(i, j, k + 1, c, KDIR) - G.xfc(i, j, k, c, KDIR);
+                }
+                G.di(i, j, k) = norm2v(dI, 3); G.dj(i, j, k) = norm2v(dJ, 3); G.dk(i, j, k) = norm2v(dK, 3);
+                double xyzC[8][3], ijkDV[5];
+                cellCoords(G, i, j, k, xyzC);
+                GaussianVolumeIntegral(xyzC, CellDV, nullptr, ijkDV);
+                G.volume(i, j, k) = ijkDV[0];
+                for (int c = 0; c < 3; ++c) G.xyzcc(i, j, k, c + 1) = ijkDV[1 + c] / ijkDV[0];
+            }
+#pragma omp parallel for collapse(2) schedule(static)
+    for (int k = G.ksg; k <= G.keg; ++k)
+        for (int j = G.jsg; j <= G.jeg; ++j)
+            for (int i = G.isg; i <= G.ieg; ++i) {
+                double fA = fmaxd(G.face(i + 1, j, k, IDIR), G.face(i, j, k, IDIR));
+                G.di(i, j, k) = G.volume(i, j, k) / fA;
+                fA = fmaxd(G.face(i, j + 1, k, JDIR), G.face(i, j, k, JDIR));
+                G.dj(i, j, k) = G.volume(i, j, k) / fA;
+                fA = fmaxd(G.face(i, j, k + 1, KDIR), G.face(i, j, k, KDIR));
+                G.dk(i, j, k) = G.volume(i, j, k) / fA;
+            }
+    hi[0] = G.ieg + 1; hi[1] = G.jeg + 1; hi[2] = G.keg + 1; hi[3] = 3;
+    G.edge.alloc(4, lo, hi);
+    std::fill(G.edge.d.begin(), G.edge.d.end(), 1.0);
+    hi[3] = 9; hi[4] = 3;
+    G.Te.alloc(5, lo, hi);
+    for (int d = 1; d <= 3; ++d) {
+        int is = G.isg, ie = G.ieg + 1, js = G.jsg, je = G.jeg + 1, ks = G.ksg, ke = G.keg + 1;
+        if (d == IDIR) { ie = G.ieg; ks = G.ksg + 1; ke = G.keg; }
+        else if (d == JDIR) { je = G.jeg; is = G.isg + 1; ie = G.ieg; }
+        else { ke = G.keg; js = G.jsg + 1; je = G.jeg; }
+#pragma omp parallel for collapse(2) schedule(static)
+        for (int k = ks; k <= ke; ++k)
+            for (int j = js; j <= je; ++j)
+                for (int i = is; i <= ie; ++i) {
+                    double dEdge[3], eAvg[3];
+                    for (int c = 1; c <= 3; ++c) {
+                        if (d == IDIR) {
+                            dEdge[c - 1] = G.xyz(i + 1, j, k, c) - G.xyz(i, j, k, c);
+                            eAvg[c - 1] = 0.5 * (G.xyz(i, j, k + 1, c) - G.xyz(i, j, k - 1, c) + G.xyz(i + 1, j, k + 1, c) - G.xyz(i + 1, j, k - 1, c));
+                        } else if (d == JDIR) {
+                            dEdge[c - 1] = G.xyz(i, j + 1, k, c) - G.xyz(i, j, k, c);
+                            eAvg[c - 1] = 0.5 * (G.xyz(i + 1, j, k, c) - G.xyz(i - 1, j, k, c) + G.xyz(i + 1, j + 1, k, c) - G.xyz(i - 1, j + 1, k, c));
+                        } else {
+                            dEdge[c - 1] = G.xyz(i, j, k + 1, c) - G.xyz(i, j, k, c);
+                            eAvg[c - 1] = 0.5 * (G.xyz(i, j + 1, k, c) - G.xyz(i, j - 1, k, c) + G.xyz(i, j + 1, k + 1, c) - G.xyz(i, j - 1, k + 1, c));
+                        }
+                    }
+                    double nE = norm2v(dEdge, 3), eN[3], eT1[3], eT2[3], cr[3];
+                    for (int c = 0; c < 3; ++c) eN[c] = dEdge[c] / nE;
+                    cross3(eAvg, eN, cr);
+                    double ncr = norm2v(cr, 3);
+                    for (int c = 0; c < 3; ++c) eT1[c] = cr[c] / ncr;
+                    cross3(eN, eT1, cr);
+                    ncr = norm2v(cr, 3);
+                    for (int c = 0; c < 3; ++c) eT2[c] = cr[c] / ncr;
+                    G.edge(i, j, k, d) = norm2v(dEdge, 3);
+                    for (int c = 0; c < 3; ++c) {
+                        G.Te(i, j, k, NORMX + c, d) = eN[c];
+                        G.Te(i, j, k, TAN1X + c, d) = eT1[c];
+                        G.Te(i, j, k, TAN2X + c, d) = eT2[c];
+                    }
+                }
+    }
+    hi[3] = 4; hi[4] = 3;
+    G.Teb.alloc(5, lo, hi);
+    std::fill(G.Teb.d.begin(), G.Teb.d.end(), 1.0);   // ebGeom initialises nQ = 1.0 everywhere
+    const long faceN = (long)(G.Ni + 1) * (G.Nj + 1) * (G.Nk + 1);
+    for (int dNorm = 1; dNorm <= 3; ++dNorm) {
+        int T1, T2;
+        if (dNorm == IDIR) { T1 = JDIR; T2 = KDIR; } else if (dNorm == JDIR) { T1 = KDIR; T2 = IDIR; } else { T1 = IDIR; T2 = JDIR; }
+        for (int pass = 0; pass < 2; ++pass) {  // ebGeom (init.F90:1083-1145)
+            int dT1 = pass == 0 ? T1 : T2, dT2 = pass == 0 ? T2 : T1;
+            int c0 = pass == 0 ? XNQI : XNQJ;
+            int ie = G.ie + 1;
+#pragma omp parallel for collapse(2) schedule(static)
+            for (int k = G.ks; k <= G.ke + 1; ++k)
+                for (int j = G.js; j <= G.je + 1; ++j)
+                    for (int iB = G.is; iB <= ie; iB += vecLen) {
+                        int iMax = std::min((int)vecLen, ie - iB + 1);
+                        double fArB[recLen][vecLen], NB[3][recLen][vecLen];
+                        loadBlock(G, fArB, G.face.d.data() + (dT1 - 1) * faceN, iB, j, k, iMax, dT2, Nr2, true);
+                        for (int c = 0; c < 3; ++c)
+                            loadBlock(G, NB[c], G.Tf.d.data() + (long)(NORMX - 1 + c) * faceN + (long)(dT1 - 1) * 9 * faceN, iB, j, k, iMax, dT2, Nr2, true);
+                        for (int i = 0; i < iMax; ++i) {
+                            int iG = iB + i;
+                            double fAi = 0.0;
+                            for (int n = 0; n < recLen; ++n) fAi = fAi + interpWgt6[n] * fArB[n][i];
+                            double Nec[3];
+                            for (int c = 0; c < 3; ++c) {
+                                double s = 0.0;
+                                for (int n = 0; n < recLen; ++n) s = s + (NB[c][n][i] * fArB[n][i]) * interpWgt6[n];
+                                Nec[c] = s / fAi;
+                            }
+                            double t1[3] = {G.Te(iG, j, k, TAN1X, dNorm), G.Te(iG, j, k, TAN1Y, dNorm), G.Te(iG, j, k, TAN1Z, dNorm)};
+                            double t2[3] = {G.Te(iG, j, k, TAN2X, dNorm), G.Te(iG, j, k, TAN2Y, dNorm), G.Te(iG, j, k, TAN2Z, dNorm)};
+                            double dxT = dot3(Nec, t1), dyT = dot3(Nec, t2);
+                            double dScl = std::sqrt(sq(dxT) + sq(dyT));
+                            if (dScl <= TINY) dScl = 1.0;
+                            G.Teb(iG, j, k, c0, dNorm) = dxT / dScl;
+                            G.Teb(iG, j, k, c0 + 1, dNorm) = dyT / dScl;
+                        }
+                    }
+        }
+    }
+    return 0;
+}
+
+static void allocState(const Model& M, const Grid& G, State& S) {
+    int lo[4] = {G.isg, G.jsg, G.ksg, 1};
+    int hi[4] = {G.ieg, G.jeg, G.keg, 5};
+    S.Gas.alloc(4, lo, hi);
+    hi[3] = 3;
+    S.Efld.alloc(4, lo, hi);
+    S.Bxyz.alloc(4, lo, hi);
+    int hip[4] = {G.ieg + 1, G.jeg + 1, G.keg + 1, 3};
+    S.magFlux.alloc(4, lo, hip);
+    S.time = M.t;
+}
+
+// ICs (prob.F90)
+static void initOT2D(const Model& M, Grid& G, State& S) {  // prob.F90:74-119
+    double Rho0 = 25.0 / (36.0 * PI), P0 = 5 / (12.0 * PI), B0 = 1 / std::sqrt(4.0 * PI);
+    for (int k = G.ks; k <= G.ke + 1; ++k)
+        for (int j = G.js; j <= G.je + 1; ++j)
+            for (int i = G.is; i <= G.ie + 1; ++i) {
+                double xc = G.xyzcc(i, j, k, 1), yc = G.xyzcc(i, j, k, 2);
+                S.Gas(i, j, k, DEN) = Rho0;
+                double Vx = -std::sin(2 * PI * yc), Vy = std::sin(2 * PI * xc), Vz = 0.0;
+                double KinE = 0.5 * Rho0 * (sq(Vx) + sq(Vy) + sq(Vz));
+                S.Gas(i, j, k, MOMX) = Vx * Rho0;
+                S.Gas(i, j, k, MOMY) = Vy * Rho0;
+                S.Gas(i, j, k, MOMZ) = Vz * Rho0;
+                S.Gas(i, j, k, ENERGY) = KinE + P0 / (M.gamma - 1);
+                S.magFlux(i, j, k, XDIR) = (-B0 * std::sin(2 * PI * yc)) * G.face(i, j, k, XDIR);
+                S.magFlux(i, j, k, YDIR) = (B0 * std::sin(4 * PI * xc)) * G.face(i, j, k, YDIR);
+                S.magFlux(i, j, k, ZDIR) = 0.0;
+            }
+}
+
+struct BWctx { double x0, y0, z0, Vx0, Vy0, Vz0, P0, pRat, dRat, D0, rC, bScl, bSclz; };
+static void GasIC_BW(double x, double y, double z, double* W, void* c) {  // prob.F90:280-297
+    BWctx* b = (BWctx*)c;
+    double R = std::sqrt(sq(x - b->x0) + sq(y - b->y0) + sq(z - b->z0));
+    double D = b->D0, P = b->P0;
+    if (R <= b->rC) { D = b->dRat * D; P = b->pRat * P; }
+    W[0] = D; W[1] = b->Vx0; W[2] = b->Vy0; W[3] = b->Vz0; W[4] = P;
+}
+static void VectorPot_BW(double x, double y, double z, double* A, void* c) {  // prob.F90:271-278
+    (void)z;
+    BWctx* b = (BWctx*)c;
+    A[0] = 0.0; A[1] = b->bSclz * x; A[2] = b->bScl * (y - x);
+}
+static void GasIC2State(const Model& M, const Grid& G, State& S, GasFun W, void* ctx) {  // gridutils.F90:144-189
+#pragma omp parallel for collapse(2) schedule(dynamic)
+    for (int k = G.ks; k <= G.ke; ++k)
+        for (int j = G.js; j <= G.je; ++j)
+            for (int i = G.is; i <= G.ie; ++i) {
+                double xyzC[8][3], ijkW[5];
+                cellCoords(G, i, j, k, xyzC);
+                double dV = G.volume(i, j, k);
+                GaussianVolumeIntegral(xyzC, W, ctx, ijkW);
+                for (int v = 0; v < 5; ++v) ijkW[v] = ijkW[v] / dV;
+                double D = ijkW[0], Mx = D * ijkW[1], My = D * ijkW[2], Mz = D * ijkW[3], P = ijkW[4];
+                double KinE = 0.5 * (sq(Mx) + sq(My) + sq(Mz)) / D;
+                double IntE = P / (M.gamma - 1.0);
+                S.Gas(i, j, k, DEN) = D; S.Gas(i, j, k, MOMX) = Mx; S.Gas(i, j, k, MOMY) = My;
+                S.Gas(i, j, k, MOMZ) = Mz; S.Gas(i, j, k, ENERGY) = IntE + KinE;
+            }
+}
+static void VectorPot2Flux(const Grid& G, State& S, VecFun Axyz, void* ctx) {  // gridutils.F90:193-237
+    Arr lA;
+    int lo[4] = {G.isg, G.jsg, G.ksg, 1}, hi[4] = {G.ieg, G.jeg, G.keg, 3};
+    lA.alloc(4, lo, hi);
+#pragma omp parallel for collapse(2) schedule(static)
+    for (int k = G.ksg; k <= G.keg - 1; ++k)
+        for (int j = G.jsg; j <= G.jeg - 1; ++j)
+            for (int i = G.isg; i <= G.ieg - 1; ++i) {
+                double e0[3], eI[3], eJ[3], eK[3], I[3], d[3];
+                for (int c = 0; c < 3; ++c) {
+                    e0[c] = G.xyz(i, j, k, c + 1); eI[c] = G.xyz(i + 1, j, k, c + 1);
+                    eJ[c] = G.xyz(i, j + 1, k, c + 1); eK[c] = G.xyz(i, j, k + 1, c + 1);
+                }
+                GaussianEdgeIntegral(eI, e0, Axyz, ctx, I);
+                for (int c = 0; c < 3; ++c) d[c] = eI[c] - e0[c];
+                lA(i, j, k, IDIR) = dot3(I, d);
+                GaussianEdgeIntegral(eJ, e0, Axyz, ctx, I);
+                for (int c = 0; c < 3; ++c) d[c] = eJ[c] - e0[c];
+                lA(i, j, k, JDIR) = dot3(I, d);
+                GaussianEdgeIntegral(eK, e0, Axyz, ctx, I);
+                for (int c = 0; c < 3; ++c) d[c] = eK[c] - e0[c];
+                lA(i, j, k, KDIR) = dot3(I, d);
+            }
+#pragma omp parallel for collapse(2) schedule(static)
+    for (int k = G.ksg; k <= G.keg - 1; ++k)
+        for (int j = G.jsg; j <= G.jeg - 1; ++j)
+            for (int i = G.isg; i <= G.ieg - 1; ++i) {
+                S.magFlux(i, j, k, IDIR) = lA(i, j, k, JDIR) - lA(i, j, k + 1, JDIR) + lA(i, j + 1, k, KDIR) - lA(i, j, k, KDIR);
+                S.magFlux(i, j, k, JDIR) = -(lA(i, j, k, IDIR) - lA(i, j, k + 1, IDIR) + lA(i + 1, j, k, KDIR) - lA(i, j, k, KDIR));
+                S.magFlux(i, j, k, KDIR) = lA(i, j, k, IDIR) - lA(i, j + 1, k, IDIR) + lA(i + 1, j, k, JDIR) - lA(i, j, k, JDIR);
+            }
+}
+static void initBW(const Model& M, Grid& G, State& S) {  // prob.F90:190-255 with the deck defaults
+    BWctx b;
+    b.x0 = b.y0 = b.z0 = 0.0; b.Vx0 = b.Vy0 = b.Vz0 = 0.0;
+    double B0_BW = 1.0;
+    b.P0 = 0.1; b.pRat = 100.0; b.dRat = 1.0; b.D0 = 1.0; b.rC = 0.1;
+    b.bScl = B0_BW / (double)std::sqrt(2.0f);   // sqrt(2.0) is a default-real (single precision) literal
+    b.bSclz = 0.0;
+    GasIC2State(M, G, S, GasIC_BW, &b);
+    if (M.doMHD) VectorPot2Flux(G, S, VectorPot_BW, &b);
+}
+
+}  // namespace orc
+
+// =========================================================================================== C ABI
+using namespace orc;
+
+extern "C" {
+
+struct orc_params {
+    int Nip, Njp, Nkp;
+    int icType;            // 0 = OT2D, 1 = BW
+    int gridType;          // 0 = uniform Cartesian, 1 = sinusoidal warp x'=x+A sin(2 pi y) sin(2 pi z) (cyclic)
+    double xyzBds[6];
+    double warpAmp;
+    double CFL, gamma, pdmb, Vd0, cHogH, cHogM, Ca, tFin;
+    int doMHD, doBoris, rmeth, doLFMLim;
+    int bc[6];             // 0 periodic, 1 zeroGrad
+    int nThreads;
+};
+
+void* orc_create(const orc_params* p) {
+    initWeights();
+    App* A = new App();
+    Model& M = A->M;
+    Grid& G = A->G;
+    M.CFL = p->CFL; M.gamma = p->gamma; M.pdmb = p->pdmb; pdmb_g = p->pdmb;
+    M.Vd0 = p->Vd0; M.cHogH = p->cHogH; M.cHogM = p->cHogM; M.Ca = p->Ca; M.tFin = p->tFin;
+    M.doMHD = p->doMHD != 0; M.doBoris = p->doBoris != 0; M.rmeth = p->rmeth; M.doLFMLim = p->doLFMLim != 0;
+#ifdef _OPENMP
+    if (p->nThreads > 0) omp_set_num_threads(p->nThreads);
+#endif
+    G.Nip = p->Nip; G.Njp = p->Njp; G.Nkp = p->Nkp;
+    M.do25D = (G.Nkp == 1);
+    for (int n = 0; n < 6; ++n) G.bc[n] = p->bc[n];
+    allocGrid(M, G);
+    // genGridXML (init.F90:572-798): uniform corners, then the optional warp
+    double dx = (p->xyzBds[1] - p->xyzBds[0]) / G.Nip, dy = (p->xyzBds[3] - p->xyzBds[2]) / G.Njp,
+           dz = (p->xyzBds[5] - p->xyzBds[4]) / G.Nkp;
+    for (int k = G.ksg; k <= G.keg + 1; ++k)
+        for (int j = G.jsg; j <= G.jeg + 1; ++j)
+            for (int i = G.isg; i <= G.ieg + 1; ++i) {
+                double x = p->xyzBds[0] + (i - 1) * dx, y = p->xyzBds[2] + (j - 1) * dy, z = p->xyzBds[4] + (k - 1) * dz;
+                if (p->gridType == 1) {
+                    double a = p->warpAmp;
+                    double xw = x + a * std::sin(2 * PI * y) * std::sin(2 * PI * z);
+                    double yw = y + a * std::sin(2 * PI * z) * std::sin(2 * PI * x);
+                    double zw = z + a * std::sin(2 * PI * x) * std::sin(2 * PI * y);
+                    x = xw; y = yw; z = zw;
+                }
+                G.xyz(i, j, k, 1) = x; G.xyz(i, j, k, 2) = y; G.xyz(i, j, k, 3) = z;
+            }
+    SetDomain(G);
+    if (Corners2Grid(M, G) != 0) { delete A; return nullptr; }
+    allocState(M, G, A->S);
+    allocState(M, G, A->oS);
+    if (p->icType == 0) initOT2D(M, G, A->S); else initBW(M, G, A->S);
+    // CalcGridInfo (init.F90:204-244)
+    if (M.doMHD) bFlux2Fld(G, A->S.magFlux, A->S.Bxyz);
+    EnforceBCs(M, G, A->S);
+    A->oS.Gas.d = A->S.Gas.d; A->oS.magFlux.d = A->S.magFlux.d; A->oS.Bxyz.d = A->S.Bxyz.d;
+    A->oS.time = A->S.time;
+    M.dt = CalcDT(M, G, A->S);
+    A->oS.time = A->S.time - M.dt;
+    // initSolver (init.F90:494-516)
+    Solver& V = A->V;
+    int lo[6] = {G.isg, G.jsg, G.ksg, 1, 1, 0};
+    int hi[6] = {G.ieg, G.jeg, G.keg, 5, 3, 0};
+    V.gFlx.alloc(5, lo, hi);
+    hi[3] = 3;
+    V.mFlx.alloc(5, lo, hi);
+    V.Vf.alloc(4, lo, hi);
+    V.dGasM.alloc(4, lo, hi);
+    hi[3] = 5;
+    V.dGasH.alloc(4, lo, hi);
+    allocState(M, G, V.StateHf);
+    return A;
+}
+
+void orc_destroy(void* h) { delete (App*)h; }
+
+void orc_step(void* h) { stepGamera(*(App*)h); }
+
+void orc_get_scalars(void* h, double* out) {  // t, dt, dt0, S.time, oS.time, ts, status
+    App* A = (App*)h;
+    out[0] = A->M.t; out[1] = A->M.dt; out[2] = A->M.dt0; out[3] = A->S.time; out[4] = A->oS.time;
+    out[5] = (double)A->M.ts; out[6] = (double)A->M.status;
+}
+void orc_set_scalars(void* h, const double* in) {
+    App* A = (App*)h;
+    A->M.t = in[0]; A->M.dt = in[1]; A->M.dt0 = in[2]; A->S.time = in[3]; A->oS.time = in[4]; A->M.ts = (int)in[5];
+}
+
+static Arr* lookup(App* A, const char* name) {
+    struct { const char* n; Arr* a; } tab[] = {
+        {"gas", &A->S.Gas}, {"magflux", &A->S.magFlux}, {"bxyz", &A->S.Bxyz}, {"efld", &A->S.Efld},
+        {"ogas", &A->oS.Gas}, {"omagflux", &A->oS.magFlux}, {"obxyz", &A->oS.Bxyz},
+        {"hgas", &A->V.StateHf.Gas}, {"hmagflux", &A->V.StateHf.magFlux}, {"hbxyz", &A->V.StateHf.Bxyz},
+        {"gflx", &A->V.gFlx}, {"mflx", &A->V.mFlx}, {"vf", &A->V.Vf}, {"dgash", &A->V.dGasH}, {"dgasm", &A->V.dGasM},
+        {"xyz", &A->G.xyz}, {"xyzcc", &A->G.xyzcc}, {"xfc", &A->G.xfc}, {"di", &A->G.di}, {"dj", &A->G.dj},
+        {"dk", &A->G.dk}, {"volume", &A->G.volume}, {"tf", &A->G.Tf}, {"te", &A->G.Te}, {"teb", &A->G.Teb},
+        {"face", &A->G.face}, {"edge", &A->G.edge},
+    };
+    for (auto& t : tab) if (std::strcmp(t.n, name) == 0) return t.a;
+    return nullptr;
+}
+long orc_size(void* h, const char* name) { Arr* a = lookup((App*)h, name); return a ? a->size() : -1; }
+int orc_get(void* h, const char* name, double* out) {
+    Arr* a = lookup((App*)h, name);
+    if (!a) return -1;
+    std::memcpy(out, a->d.data(), sizeof(double) * a->size());
+    return 0;
+}
+int orc_set(void* h, const char* name, const double* in) {
+    Arr* a = lookup((App*)h, name);
+    if (!a) return -1;
+    std::memcpy(a->d.data(), in, sizeof(double) * a->size());
+    return 0;
+}
+// Recompute State%Bxyz from State%magFlux (bFlux2Fld) after a host-side edit.
+void orc_bflux2fld(void* h) { App* A = (App*)h; bFlux2Fld(A->G, A->S.magFlux, A->S.Bxyz); bFlux2Fld(A->G, A->oS.magFlux, A->oS.Bxyz); }
+
+double orc_divb(void* h) {  // gridutils.F90:717-770 (no background)
+    App* A = (App*)h;
+    const Grid& G = A->G;
+    const Arr& mf = A->S.magFlux;
+    double tot = 0.0;
+    for (int k = G.ks; k <= G.ke; ++k)
+        for (int j = G.js; j <= G.je; ++j)
+            for (int i = G.is; i <= G.ie; ++i) {
+                double dFi = mf(i, j, k, IDIR) - mf(i + 1, j, k, IDIR);
+                double dFj = mf(i, j, k, JDIR) - mf(i, j + 1, k, JDIR);
+                double dFk = mf(i, j, k, KDIR) - mf(i, j, k + 1, KDIR);
+                tot = tot + std::fabs(dFi + dFj + dFk + 0.0 + 0.0 + 0.0);
+            }
+    return tot;
+}
+
+// Known-answer helpers for the reference's unit tests
+void orc_c2p(double gamma, const double* con, double* prim) { Model M; M.gamma = gamma; CellC2P(M, con, prim); }
+void orc_p2c(double gamma, const double* prim, double* con) { Model M; M.gamma = gamma; CellP2C(M, prim, con); }
+double orc_norm2(const double* a, int n) { return norm2v(a, n); }
+void orc_face_integral_area(const double* f0, const double* f1, const double* f2, const double* f3, double* area,
+                            double* ctr) {
+    double fI[3];
+    GaussianFaceIntegral(f0, f1, f2, f3, IdVec, nullptr, fI);
+    *area = fI[0];
+    GaussianFaceIntegral(f0, f1, f2, f3, rVec, nullptr, fI);
+    for (int c = 0; c < 3; ++c) ctr[c] = fI[c] / *area;
+}
+void orc_volume_integral(const double* xyzC /*8x3 row-major*/, double* vol, double* ctr) {
+    double c8[8][3];
+    for (int p = 0; p < 8; ++p) for (int c = 0; c < 3; ++c) c8[p][c] = xyzC[p * 3 + c];
+    double w[5];
+    GaussianVolumeIntegral(c8, CellDV, nullptr, w);
+    *vol = w[0];
+    for (int c = 0; c < 3; ++c) ctr[c] = w[1 + c] / w[0];
+}
+// PDM / reconstruction kernels on a single 8-point stencil (for unit tests of the limiter)
+void orc_recon_lr(int rmeth, double pdmb, const double* vol8, const double* q8, const double* nq4, double* lr) {
+    initWeights();
+    double save = pdmb_g;
+    pdmb_g = pdmb;
+    double dV[recLen][vecLen], Q[recLen][vecLen], nQ[limLen][vecLen], Vi[vecLen], Ql[vecLen], Qr[vecLen];
+    for (int n = 0; n < recLen; ++n) for (int i = 0; i < vecLen; ++i) { dV[n][i] = vol8[n]; Q[n][i] = q8[n]; }
+    for (int n = 0; n < limLen; ++n) for (int i = 0; i < vecLen; ++i) nQ[n][i] = nq4[n];
+    Central8(dV, Vi);
+    GetLRs(rmeth, dV, nQ, Q, Vi, Ql, Qr);
+    lr[0] = Ql[0]; lr[1] = Qr[0];
+    pdmb_g = save;
+}
+int orc_num_threads(void) {
+#ifdef _OPENMP
+    return omp_get_max_threads();
+#else
+    return 1;
+#endif
+}
+
+}  // extern "C"

@@ -1,0 +1,69 @@
+"""Shared helpers: build matched oracle / device problems and compare arrays."""
+import numpy as np
+
+GRID_NAMES = ("xyzcc", "xfc", "di", "dj", "dk", "volume", "face", "edge", "tf", "te", "teb")
+
+
+def rel_linf(a, b):
+    a = np.asarray(a)
+    b = np.asarray(b)
+    den = np.max(np.abs(b))
+    if den == 0.0:
+        return float(np.max(np.abs(a)))
+    return float(np.max(np.abs(a - b)) / den)
+
+
+def per_var_rel(a, b):
+    """Relative L-infinity per trailing component (variable / vector component)."""
+    if a.ndim == 3:
+        return [rel_linf(a, b)]
+    a2 = a.reshape(a.shape[:3] + (-1,), order="F")
+    b2 = b.reshape(b.shape[:3] + (-1,), order="F")
+    return [rel_linf(a2[..., v], b2[..., v]) for v in range(a2.shape[3])]
+
+
+def problem(kind, n=(32, 32, 4), **kw):
+    """Oracle keyword arguments and the matching Model settings for a named test problem."""
+    from kaiju_b200 import gamera as gm
+    Nip, Njp, Nkp = n
+    if kind == "ot":
+        okw = dict(ic="OT2D", grid="uniform", bounds=(0.0, 1.0, 0.0, 1.0, 0.0, 4.0 / 128.0 * (Nkp / 4.0)),
+                   CFL=0.3, bc=[0] * 6)
+        if Nkp == 1:
+            okw["bounds"] = (0.0, 1.0, 0.0, 1.0, -0.5, 0.5)
+    elif kind == "bw":
+        okw = dict(ic="BW", grid="warp", warp_amp=0.04, bounds=(-0.5, 0.5, -0.5, 0.5, -0.5, 0.5),
+                   CFL=0.3, bc=[1] * 6)
+    else:
+        raise ValueError(kind)
+    okw.update(kw)
+    mkw = dict(Nip=Nip, Njp=Njp, Nkp=Nkp, CFL=okw["CFL"], bc=tuple(okw["bc"]))
+    for k in ("pdmb", "Vd0", "cHogH", "cHogM", "Ca", "doMHD", "doBoris", "rmeth", "doLFMLim", "tFin", "gamma"):
+        if k in okw:
+            mkw[k] = okw[k]
+    if okw.get("doBoris"):
+        mkw["Ca"] = okw["Ca"]
+    mkw.setdefault("tFin", okw.get("tFin", 1.0e30))
+    okw.setdefault("tFin", mkw["tFin"])
+    return okw, gm.Model(**mkw)
+
+
+def oracle_and_gpu(kind, n=(32, 32, 4), **kw):
+    from oracle.pyoracle import Oracle
+    from kaiju_b200 import gamera as gm
+    okw, model = problem(kind, n, **kw)
+    o = Oracle(*n, **okw)
+    grid = {name: o.get(name) for name in GRID_NAMES}
+    sc = o.scalars()
+    g = gm.GameraGPU.from_arrays(model, grid, o.get("gas"), o.get("magflux"), o.get("ogas"), o.get("omagflux"),
+                                 sc["time"], sc["otime"])
+    g.set_scalars(sc["t"], sc["dt"], sc["dt0"], sc["ts"], sc["time"], sc["otime"])
+    return o, g
+
+
+def resync(o, g):
+    """Put the device on exactly the oracle's current state (State, oState and scalars)."""
+    sc = o.scalars()
+    g.sync_to_device(gas=o.get("gas"), magflux=o.get("magflux"), ogas=o.get("ogas"), omagflux=o.get("omagflux"),
+                     time=sc["time"], otime=sc["otime"])
+    g.set_scalars(sc["t"], sc["dt"], sc["dt0"], sc["ts"], sc["time"], sc["otime"])

@@ -1,0 +1,122 @@
+"""Device step vs the CPU oracle on identical inputs (relative L-infinity per variable <= 1e-10).
+
+Each case builds the problem with the oracle (Hatch-equivalent set-up on the CPU), mirrors the
+oracle's Grid/State arrays onto the GPU through the C ABI (gam_gpu_create), advances both by one
+stepGamera and compares the intermediates (predictor half state, E field, deltas) and the final state.
+Multi-step cases re-synchronise the device to the oracle before every step so chaotic growth of
+round-off differences does not mask kernel errors.
+"""
+import numpy as np
+import pytest
+
+from helpers import oracle_and_gpu, per_var_rel, rel_linf, resync
+
+pytestmark = pytest.mark.gpu
+TOL = 1e-10
+
+
+def _cmp(o, g, names, tol=TOL, where=""):
+    for name in names:
+        a, b = g.fetch(name), o.get(name)
+        errs = per_var_rel(a, b)
+        assert max(errs) <= tol, f"{where}{name}: {errs}"
+
+
+CASES = [
+    ("ot3d", "ot", (32, 32, 4), {}),
+    ("ot25d", "ot", (32, 32, 1), {}),
+    ("bw_warp", "bw", (32, 16, 16), {}),
+    ("bw_7up", "bw", (32, 16, 16), dict(rmeth="7UP", pdmb=4.0)),
+    ("bw_hydro", "bw", (16, 16, 16), dict(doMHD=False)),
+    ("bw_boris", "bw", (16, 16, 16), dict(doBoris=True, Ca=2.0)),
+    ("ot_nolfmlim", "ot", (32, 32, 4), dict(doLFMLim=False)),
+]
+
+
+@pytest.mark.parametrize("name,kind,n,kw", CASES, ids=[c[0] for c in CASES])
+def test_one_step_intermediates(gpu_lib, oracle_lib, name, kind, n, kw):
+    o, g = oracle_and_gpu(kind, n, **kw)
+    with g:
+        # inputs mirrored exactly
+        _cmp(o, g, ["gas", "magflux", "bxyz", "ogas", "omagflux"], tol=0.0, where="input ")
+        o.step()
+        dt, ts, t = g.step()
+        sc = o.scalars()
+        assert ts == sc["ts"] == 1
+        assert abs(dt - sc["dt"]) <= TOL * sc["dt"]
+        assert abs(t - sc["t"]) <= TOL * abs(sc["t"])
+        inter = ["hgas", "dgash"]
+        if kw.get("doMHD", True):
+            inter += ["hmagflux", "hbxyz", "efld", "dgasm"]
+        _cmp(o, g, inter, where=f"{name} ")
+        _cmp(o, g, ["gas", "magflux", "bxyz"], where=f"{name} ")
+
+
+@pytest.mark.parametrize("name,kind,n,kw", CASES[:3], ids=[c[0] for c in CASES[:3]])
+def test_resynced_steps(gpu_lib, oracle_lib, name, kind, n, kw):
+    o, g = oracle_and_gpu(kind, n, **kw)
+    with g:
+        for s in range(6):
+            o.step()
+            dt, ts, t = g.step()
+            sc = o.scalars()
+            assert abs(dt - sc["dt"]) <= TOL * sc["dt"], (s, dt, sc["dt"])
+            _cmp(o, g, ["gas", "magflux"], where=f"step {s} ")
+            resync(o, g)
+
+
+def test_free_running_trajectory(gpu_lib, oracle_lib):
+    """Without re-synchronisation the trajectories stay together to near round-off over 20 steps."""
+    o, g = oracle_and_gpu("bw", (32, 16, 16))
+    with g:
+        o.step(20)
+        g.run_steps(20)
+        st = g.status()
+        assert st["ts"] == 20
+        for v, e in enumerate(per_var_rel(g.fetch("gas"), o.get("gas"))):
+            assert e < 1e-8, (v, e)
+
+
+def test_divb_roundoff(gpu_lib, oracle_lib):
+    o, g = oracle_and_gpu("bw", (32, 16, 16))
+    with g:
+        g.run_steps(10)
+        mf = g.fetch("magflux")
+        scale = np.abs(mf).max() * 32 * 16 * 16
+        assert g.divb() <= 1e-12 * scale
+
+
+def test_device_grid_matches_oracle(gpu_lib, oracle_lib):
+    """Corners2Grid + IC + Hatch tail on the device vs the oracle's host set-up, same corners."""
+    from helpers import problem
+    from kaiju_b200 import gamera as gm
+    for kind, n in (("bw", (32, 16, 16)), ("ot", (32, 32, 4))):
+        okw, model = problem(kind, n)
+        o = oracle_lib.Oracle(*n, **okw)
+        xyz = o.get("xyz")
+        with gm.GameraGPU.from_corners(model, xyz, "BW" if kind == "bw" else "OT2D") as g:
+            for name in ("volume", "xyzcc", "xfc", "face", "edge", "di", "dj", "dk", "tf", "te", "teb"):
+                errs = per_var_rel(g.fetch(name), o.get(name))
+                assert max(errs) <= 1e-12, (kind, name, errs)
+            for name in ("gas", "magflux", "bxyz"):
+                errs = per_var_rel(g.fetch(name), o.get(name))
+                assert max(errs) <= 1e-12, (kind, name, errs)
+            st = g.status()
+            sc = o.scalars()
+            assert abs(st["dt"] - sc["dt"]) <= 1e-12 * sc["dt"]
+            assert abs(st["otime"] - sc["otime"]) <= 1e-12 * sc["dt"]
+
+
+def test_fp32_flux_error(gpu_lib, oracle_lib):
+    """FP32 reconstruction/limiter/fluxes, FP64 state: L1 error against the FP64 oracle after 10 steps."""
+    from kaiju_b200 import gamera as gm
+    o, g = oracle_and_gpu("bw", (32, 16, 16))
+    with g:
+        g.set_precision(gm.GAM_FP32FLUX)
+        o.step(10)
+        g.run_steps(10)
+        a, b = g.fetch("gas")[4:36, 4:20, 4:20], o.get("gas")[4:36, 4:20, 4:20]
+        for v in range(5):
+            l1 = np.abs(a[..., v] - b[..., v]).sum() / np.abs(b[..., v]).sum() if np.abs(b[..., v]).sum() > 0 else \
+                np.abs(a[..., v]).mean()
+            assert l1 <= 1e-5, (v, l1)
