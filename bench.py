@@ -112,7 +112,7 @@ class ClockSampler:
         sm = [float(r[1]) for r in rows if r[1].strip().replace(".", "").isdigit()]
         mx = [float(r[2]) for r in rows if r[2].strip().replace(".", "").isdigit()]
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[q] for r in rows for q in range(4) if len(r) > 5 + q and "Active" in r[5 + q]})
+        reasons = sorted({names[q] for r in rows for q in range(4) if len(r) > 5 + q and r[5 + q].strip() == "Active"})
         return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
                 "reasons": reasons, "samples": len(rows)}
 

@@ -84,11 +84,13 @@ typedef struct {
 } gam_status_c;
 
 /* Mirror a Hatch-ed problem onto the current CUDA device. gas/ogas are State%Gas/oState%Gas
- * (Ni,Nj,Nk,5); magflux/omagflux are (Ni+1,Nj+1,Nk+1,3). time/otime are State%time/oState%time.
- * Replaces: the arrays Hatch leaves in gamApp_T (src/gamera/init.F90:150-260). */
+ * (Ni,Nj,Nk,5); magflux/omagflux are (Ni+1,Nj+1,Nk+1,3); bxyz/obxyz are State%Bxyz/oState%Bxyz
+ * (Ni,Nj,Nk,3) -- pass them as Hatch left them (its EnforceBCs runs after bFlux2Fld, so ghost cells
+ * may differ from a fresh bFlux2Fld); NULL recomputes them with bFlux2Fld. time/otime are
+ * State%time/oState%time. Replaces: the arrays Hatch leaves in gamApp_T (src/gamera/init.F90:150-260). */
 int gam_gpu_create(gam_gpu_t** h, const gam_model_c* m, const gam_grid_c* g, const double* gas,
-                   const double* magflux, const double* ogas, const double* omagflux, double time,
-                   double otime);
+                   const double* magflux, const double* bxyz, const double* ogas, const double* omagflux,
+                   const double* obxyz, double time, double otime);
 
 /* Build the grid metrics and the initial state on the device from corner coordinates
  * xyz (Ni+1,Nj+1,Nk+1,3): Corners2Grid (src/gamera/init.F90:801-1145) and the problem set-up that
@@ -118,11 +120,13 @@ int gam_gpu_run_steps_timed(gam_gpu_t* h, int n, double* ms);
 #define GAM_NPHASE 7
 int gam_gpu_profile_phases(gam_gpu_t* h, int nsteps, double* ms, int nphase);
 
-/* Copy state to / from the caller's Fortran arrays (NULL pointers are skipped). */
+/* Copy state to / from the caller's Fortran arrays (NULL pointers are skipped; on the way in a NULL
+ * Bxyz is recomputed from the fluxes with bFlux2Fld, as after a restart read, init.F90:204-210). */
 int gam_gpu_sync_to_host(gam_gpu_t* h, unsigned what, double* gas, double* magflux, double* bxyz,
                          double* ogas, double* omagflux);
 int gam_gpu_sync_to_device(gam_gpu_t* h, unsigned what, const double* gas, const double* magflux,
-                           const double* ogas, const double* omagflux, double time, double otime);
+                           const double* bxyz, const double* ogas, const double* omagflux,
+                           const double* obxyz, double time, double otime);
 
 /* Model/state scalars, e.g. to resume from a restart (Model%t, dt, dt0, ts; State%time, oState%time) */
 int gam_gpu_get_status(gam_gpu_t* h, gam_status_c* s);

@@ -106,9 +106,11 @@ int alloc_handle(gam_gpu* G, const gam_model_c* m) {
     for (int n = 0; n < 6; ++n) p.bc[n] = m->bc[n];
 
     CK(cudaGetDevice(&h.device));
+    flux_kernels_init();
+    efield_kernels_init();
     CK(cudaStreamCreateWithFlags(&h.stream, cudaStreamNonBlocking));
     h.ownStream = true;
-    const size_t planes = 11 * 3 + 10 + 14 + 24 + 91;
+    const size_t planes = 11 * 3 + 10 + 14 + 9 + 24 + 91;
     h.poolPlanes = planes;
     CK(cudaMalloc(&h.pool, sizeof(double) * L.E * planes));
     CK(cudaMemsetAsync(h.pool, 0, sizeof(double) * L.E * planes, h.stream));
@@ -126,6 +128,9 @@ int alloc_handle(gam_gpu* G, const gam_model_c* m) {
     for (int v = 0; v < 5; ++v) h.Wn[v] = take();
     for (int x = 0; x < 3; ++x) h.E[x] = take();   // contiguous: memset as one range
     for (int x = 0; x < 3; ++x) h.Vf[x] = take();
+    for (int x = 0; x < 3; ++x) h.VdV[x] = take();
+    for (int x = 0; x < 3; ++x) h.hbA[x] = take();
+    for (int x = 0; x < 3; ++x) h.nbA[x] = take();
     for (int v = 0; v < 5; ++v) h.dGasH[v] = take();
     for (int x = 0; x < 3; ++x) h.dGasM[x] = take();
     for (int d = 0; d < 3; ++d) for (int v = 0; v < 5; ++v) h.gflx[d][v] = take();
@@ -242,7 +247,8 @@ const char* gam_gpu_errstr(int code) {
 }
 
 int gam_gpu_create(gam_gpu_t** out, const gam_model_c* m, const gam_grid_c* g, const double* gas,
-                   const double* magflux, const double* ogas, const double* omagflux, double time, double otime) {
+                   const double* magflux, const double* bxyz, const double* ogas, const double* omagflux,
+                   const double* obxyz, double time, double otime) {
     if (!out || !g || !gas || !magflux || !ogas || !omagflux) return GAM_ERR_ARG;
     *out = nullptr;
     int rc = check_model(m);
@@ -270,7 +276,8 @@ int gam_gpu_create(gam_gpu_t** out, const gam_model_c* m, const gam_grid_c* g, c
     if (!rc) { for (int d = 0; d < 3; ++d) for (int c = 0; c < 9; ++c) pl[d * 9 + c] = h.Te[d][c]; rc = h2d_planes(G, pl, 27, g->Te, fe); }
     if (!rc) { for (int d = 0; d < 3; ++d) for (int c = 0; c < 4; ++c) pl[d * 4 + c] = h.Teb[d][c]; rc = h2d_planes(G, pl, 12, g->Teb, fe); }
     if (rc) { gam_gpu_destroy(G); return rc; }
-    rc = gam_gpu_sync_to_device(G, GAM_SYNC_STATE | GAM_SYNC_OSTATE, gas, magflux, ogas, omagflux, time, otime);
+    rc = gam_gpu_sync_to_device(G, GAM_SYNC_STATE | GAM_SYNC_OSTATE, gas, magflux, bxyz, ogas, omagflux, obxyz, time,
+                                otime);
     if (rc) { gam_gpu_destroy(G); return rc; }
     *out = G;
     return GAM_OK;
@@ -301,8 +308,8 @@ int gam_gpu_create_from_corners(gam_gpu_t** out, const gam_model_c* m, const dou
     return GAM_OK;
 }
 
-int gam_gpu_sync_to_device(gam_gpu_t* G, unsigned what, const double* gas, const double* magflux, const double* ogas,
-                           const double* omagflux, double time, double otime) {
+int gam_gpu_sync_to_device(gam_gpu_t* G, unsigned what, const double* gas, const double* magflux, const double* bxyz,
+                           const double* ogas, const double* omagflux, const double* obxyz, double time, double otime) {
     if (!G) return GAM_ERR_ARG;
     Handle& h = G->h;
     const Lay& L = h.L;
@@ -314,9 +321,16 @@ int gam_gpu_sync_to_device(gam_gpu_t* G, unsigned what, const double* gas, const
     if (!rc && (what & GAM_SYNC_OSTATE) && ogas) rc = h2d_planes(G, o.gas, 5, ogas, ce);
     if (!rc && (what & GAM_SYNC_OSTATE) && omagflux) rc = h2d_planes(G, o.mf, 3, omagflux, fe);
     if (rc) return rc;
-    // Bxyz follows from the fluxes (bFlux2Fld), as after a restart read (init.F90:204-210)
-    if (what & GAM_SYNC_STATE) launch_bflux2fld(h, n, h.stream);
-    if (what & GAM_SYNC_OSTATE) launch_bflux2fld(h, o, h.stream);
+    // Bxyz as given, else from the fluxes (bFlux2Fld), as after a restart read (init.F90:204-210)
+    if (what & GAM_SYNC_STATE) {
+        if (bxyz) rc = h2d_planes(G, n.b, 3, bxyz, ce);
+        else launch_bflux2fld(h, n, h.stream);
+    }
+    if (!rc && (what & GAM_SYNC_OSTATE)) {
+        if (obxyz) rc = h2d_planes(G, o.b, 3, obxyz, ce);
+        else launch_bflux2fld(h, o, h.stream);
+    }
+    if (rc) return rc;
     // State%time / oState%time travel with the arrays; the other scalars stay as they are on the device
     rc = download_scalars(G);
     if (rc) return rc;

@@ -1,0 +1,147 @@
+// Kernel-side helpers shared by the step kernels: launch regions, pointer bundles, the one-sided
+// kinetic fluxes, and cooperative staging of a box of a pencil plane into shared memory.
+#pragma once
+#include "gam_common.cuh"
+
+namespace gam {
+
+struct Reg {
+    int i0, ni, j0, nj, k0, nk;
+    __host__ __device__ long long n() const { return (long long)ni * nj * nk; }
+};
+__device__ __forceinline__ bool reg_ijk(const Reg& r, long long t, int& i, int& j, int& k) {
+    if (t >= r.n()) return false;
+    i = r.i0 + (int)(t % r.ni);
+    long long q = t / r.ni;
+    j = r.j0 + (int)(q % r.nj);
+    k = r.k0 + (int)(q / r.nj);
+    return true;
+}
+// 3-D launch over a region: threadIdx.x runs along i (coalesced)
+__device__ __forceinline__ bool reg3(const Reg& r, int& i, int& j, int& k) {
+    i = r.i0 + (int)(blockIdx.x * blockDim.x + threadIdx.x);
+    j = r.j0 + (int)(blockIdx.y * blockDim.y + threadIdx.y);
+    k = r.k0 + (int)(blockIdx.z * blockDim.z + threadIdx.z);
+    return (i < r.i0 + r.ni) && (j < r.j0 + r.nj) && (k < r.k0 + r.nk);
+}
+static inline dim3 grid3(const Reg& r, dim3 b) {
+    return dim3((unsigned)((r.ni + b.x - 1) / b.x), (unsigned)((r.nj + b.y - 1) / b.y), (unsigned)((r.nk + b.z - 1) / b.z));
+}
+static inline Reg mkreg(int i0, int i1, int j0, int j1, int k0, int k1) {
+    Reg r;
+    r.i0 = i0; r.ni = i1 - i0 + 1; r.j0 = j0; r.nj = j1 - j0 + 1; r.k0 = k0; r.nk = k1 - k0 + 1;
+    return r;
+}
+static inline unsigned nblk(long long n, int b) { return (unsigned)((n + b - 1) / b); }
+
+struct PrimP { double* w[5]; };
+struct Vec3P { double* v[3]; };
+struct FluxP { double* g[5]; double* m[3]; };
+
+// One-sided gas kinetic flux (stress.F90:432-511)
+template <typename T>
+__device__ __forceinline__ void gasKin(T gm1, T sg, const T* W, const T* Tf, T* gF, T* dW) {
+    T D = W[0], Vx = W[1], Vy = W[2], Vz = W[3], P = W[4];
+    T E = T(0.5) * D * (Vx * Vx + Vy * Vy + Vz * Vz) + P / gm1;
+    T lambda = D / (T(2) * P);
+    T Vn = Tf[0] * Vx + Tf[1] * Vy + Tf[2] * Vz;
+    T Vt1 = Tf[3] * Vx + Tf[4] * Vy + Tf[5] * Vz;
+    T Vt2 = Tf[6] * Vx + Tf[7] * Vy + Tf[8] * Vz;
+    T Vn0 = T(0.5) * erfc(sg * sqrt(lambda) * Vn);
+    T Vn1 = Vn * Vn0 - T(0.5) * sg * exp(-(lambda * Vn * Vn)) / sqrt(T(PI) * lambda);
+    gF[0] = gF[0] + D * Vn1;
+    gF[4] = gF[4] + (E + T(0.5) * P) * Vn1 + T(0.5) * P * Vn0 * Vn;
+    T fMn = D * Vn * Vn1 + P * Vn0;
+    T fMt1 = D * Vt1 * Vn1;
+    T fMt2 = D * Vt2 * Vn1;
+    gF[1] = gF[1] + (Tf[0] * fMn + Tf[3] * fMt1 + Tf[6] * fMt2);
+    gF[2] = gF[2] + (Tf[1] * fMn + Tf[4] * fMt1 + Tf[7] * fMt2);
+    gF[3] = gF[3] + (Tf[2] * fMn + Tf[5] * fMt1 + Tf[8] * fMt2);
+    dW[0] = dW[0] + sg * D;
+    dW[1] = dW[1] + sg * D * Vx;
+    dW[2] = dW[2] + sg * D * Vy;
+    dW[3] = dW[3] + sg * D * Vz;
+    dW[4] = dW[4] + sg * E;
+}
+// One-sided magnetic stress (stress.F90:513-599, no background field)
+template <typename T>
+__device__ __forceinline__ void magKin(const Par& p, T sg, const T* W, const T* B, T Bn, const T* Tf, T* mF, T& bbD,
+                                       T& VaD) {
+    T D = W[0], P = W[4];
+    T dPb = T(0.5) * (B[0] * B[0] + B[1] * B[1] + B[2] * B[2]);
+    T Va2 = T(2) * dPb / D;
+    bbD = bbD + T(0.5) * (B[0] * B[0] + B[1] * B[1] + B[2] * B[2]);
+    T Vac2 = Va2;
+    if (p.doBoris) { T Ca = T(p.Ca); Vac2 = Va2 / (T(1) + (Va2 / (Ca * Ca))); }
+    T Vn = Tf[0] * W[1] + Tf[1] * W[2] + Tf[2] * W[3];
+    T lambda = T(1) / (T(2) * P / D + Vac2);
+    T Vn0 = T(0.5) * erfc(sg * sqrt(lambda) * Vn);
+    VaD = VaD + T(0.5) * sqrt(Vac2);
+    mF[0] = mF[0] + Vn0 * (dPb * Tf[0] - B[0] * Bn);
+    mF[1] = mF[1] + Vn0 * (dPb * Tf[1] - B[1] * Bn);
+    mF[2] = mF[2] + Vn0 * (dPb * Tf[2] - B[2] * Bn);
+}
+
+// Cooperative copy of the box [bi0,bi0+ni) x [bj0,bj0+nj) x [bk0,bk0+nk) of one pencil plane into
+// shared memory (i fastest), converting to T. Elements outside the allocated index range are zero;
+// they only ever feed interfaces/edges outside the launch region.
+template <typename T>
+__device__ __forceinline__ void stage_box(T* dst, const double* __restrict__ src, const Lay& L, int bi0, int ni, int bj0,
+                                          int nj, int bk0, int nk, int tid, int nth) {
+    int n = ni * nj * nk;
+    for (int t = tid; t < n; t += nth) {
+        int a = t % ni;
+        int q = t / ni;
+        int b = q % nj;
+        int c = q / nj;
+        int i = bi0 + a, j = bj0 + b, k = bk0 + c;
+        T v = T(0);
+        if (i >= 0 && i <= L.Ni && j >= 0 && j <= L.Nj && k >= 0 && k <= L.Nk) v = T(__ldg(&src[L.at(i, j, k)]));
+        dst[t] = v;
+    }
+}
+
+// Asynchronous global->shared copies (cp.async, 8 bytes each): every thread keeps all of its copies in
+// flight at once instead of one load at a time.
+__device__ __forceinline__ void cp_async8(void* smem, const void* gmem) {
+    unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(sa), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+
+// stage_box with cp.async for double planes; the caller waits with cp_async_wait_all + __syncthreads
+__device__ __forceinline__ void stage_box_async(double* dst, const double* __restrict__ src, const Lay& L, int bi0,
+                                                int ni, int bj0, int nj, int bk0, int nk, int tid, int nth) {
+    int n = ni * nj * nk;
+    for (int t = tid; t < n; t += nth) {
+        int a = t % ni;
+        int q = t / ni;
+        int b = q % nj;
+        int c = q / nj;
+        int i = bi0 + a, j = bj0 + b, k = bk0 + c;
+        if (i >= 0 && i <= L.Ni && j >= 0 && j <= L.Nj && k >= 0 && k <= L.Nk) cp_async8(dst + t, src + L.at(i, j, k));
+        else dst[t] = 0.0;
+    }
+}
+
+// Row-wise staging: the box [gi0,gi0+ni) x [gj0,gj0+nj) x [gk0,gk0+nk) (absolute pencil indices) is
+// copied row by row, one warp per row, lanes along i, one cp.async per element; each row's address is
+// computed once. Out-of-range elements are zero.
+__device__ __forceinline__ void stage_rows(double* dst, const double* __restrict__ src, const Lay& L, int gi0, int ni,
+                                           int gj0, int nj, int gk0, int nk, int warp, int nwarp, int lane) {
+    const int nrow = nj * nk;
+    for (int rr = warp; rr < nrow; rr += nwarp) {
+        int b = rr % nj, c = rr / nj;
+        int j = gj0 + b, k = gk0 + c;
+        double* drow = dst + rr * ni;
+        bool ok = (j >= 0) && (j <= L.Nj) && (k >= 0) && (k <= L.Nk);
+        const double* srow = src + L.at(0, ok ? j : 0, ok ? k : 0);
+        for (int a = lane; a < ni; a += 32) {
+            int i = gi0 + a;
+            if (ok && i >= 0 && i <= L.Ni) cp_async8(drow + a, srow + i);
+            else drow[a] = 0.0;
+        }
+    }
+}
+
+}  // namespace gam

@@ -10,31 +10,9 @@
 #include <cmath>
 #include "gam_common.cuh"
 #include "gam_step.cuh"
+#include "gam_kern.cuh"
 
 namespace gam {
-
-struct Reg {
-    int i0, ni, j0, nj, k0, nk;
-    __host__ __device__ long long n() const { return (long long)ni * nj * nk; }
-};
-__device__ __forceinline__ bool reg_ijk(const Reg& r, long long t, int& i, int& j, int& k) {
-    if (t >= r.n()) return false;
-    i = r.i0 + (int)(t % r.ni);
-    long long q = t / r.ni;
-    j = r.j0 + (int)(q % r.nj);
-    k = r.k0 + (int)(q / r.nj);
-    return true;
-}
-static inline Reg mkreg(int i0, int i1, int j0, int j1, int k0, int k1) {
-    Reg r;
-    r.i0 = i0; r.ni = i1 - i0 + 1; r.j0 = j0; r.nj = j1 - j0 + 1; r.k0 = k0; r.nk = k1 - k0 + 1;
-    return r;
-}
-static inline unsigned nblk(long long n, int b) { return (unsigned)((n + b - 1) / b); }
-
-struct PrimP { double* w[5]; };
-struct Vec3P { double* v[3]; };
-struct FluxP { double* g[5]; double* m[3]; };
 
 // ================================================================================ step scalars
 // AdvanceMHD trap (mhdgroup.F90:26-28) and the predictor time factors (:459)
@@ -47,8 +25,11 @@ __global__ void k_step_begin(Scal* sc) {
 }
 
 // ================================================================================ predictor
-// Predictor magFlux part (mhdgroup.F90:466-488): AB2 on every face element, ghosts included
-__global__ void k_predict_faces(long long E, Vec3P mf, Vec3P omf, Vec3P hmf, const Scal* sc) {
+// Predictor magFlux part (mhdgroup.F90:466-488): AB2 on every face element, ghosts included. Also the
+// per-face values EdgeLRs divides out at every stencil point (fields.F90:335-336): flux/max(area,TINY)
+// for the half state (reconstruction) and for the limiting state.
+__global__ void k_predict_faces(long long E, Par p, GridP g, Vec3P mf, Vec3P omf, Vec3P hmf, Vec3P hbA, Vec3P nbA,
+                                const Scal* sc) {
     long long l = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (l >= E) return;
     double pdt = sc->pdt, odt = sc->odt;
@@ -56,13 +37,17 @@ __global__ void k_predict_faces(long long E, Vec3P mf, Vec3P omf, Vec3P hmf, con
     for (int c = 0; c < 3; ++c) {
         double Q = mf.v[c][l], oQ = omf.v[c][l];
         double dQ = (Q - oQ) / odt;
-        hmf.v[c][l] = Q + pdt * dQ;
+        double H = Q + pdt * dQ;
+        hmf.v[c][l] = H;
+        double a = dmax(g.face[c][l], TINY);
+        hbA.v[c][l] = H / a;
+        nbA.v[c][l] = (p.doLFMLim ? Q : H) / a;
     }
 }
 
 // bFlux2Fld of the half state + PredictCell (mhdgroup.F90:492-518, 529-563) on every cell, plus the
 // BlockCon2Prim primitives of the half state and of state n used by the interface reconstruction.
-__global__ void k_predict_cells(Lay L, Par p, GridP g, StateP n, StateP o, StateP h, PrimP Wh, PrimP Wn,
+__global__ void k_predict_cells(Lay L, Par p, GridP g, StateP n, StateP o, StateP h, PrimP Wh, PrimP Wn, Vec3P VdV,
                                 const Scal* sc) {
     Reg r = {0, L.Ni, 0, L.Nj, 0, L.Nk};
     int i, j, k;
@@ -84,6 +69,13 @@ __global__ void k_predict_cells(Lay L, Par p, GridP g, StateP n, StateP o, State
     cellP2C(p, pW, pQ);
 #pragma unroll
     for (int v = 0; v < 5; ++v) h.gas[v][c] = pQ[v];
+    // Mom2Face summand VolB*MomB/max(DenB,dFloor) (fields.F90:265-271), a pointwise cell value
+    {
+        double vol = g.volume[c], den = dmax(pQ[0], p.dFloor);
+        VdV.v[0][c] = vol * pQ[1] / den;
+        VdV.v[1][c] = vol * pQ[2] / den;
+        VdV.v[2][c] = vol * pQ[3] / den;
+    }
     double w[5];
     blockC2P(p, pQ, w);
 #pragma unroll
@@ -91,229 +83,6 @@ __global__ void k_predict_cells(Lay L, Par p, GridP g, StateP n, StateP o, State
     blockC2P(p, Q, w);
 #pragma unroll
     for (int v = 0; v < 5; ++v) Wn.w[v][c] = w[v];
-}
-
-// ================================================================================ electric field
-// Mom2Face (fields.F90:235-285): volume-weighted Central8 of rho*v along dT1 onto the dT1 faces
-__global__ void k_mom2face(Lay L, Par p, GridP g, StateP h, Vec3P Vf, Reg r, int dT1) {
-    int i, j, k;
-    if (!reg_ijk(r, blockIdx.x * (long long)blockDim.x + threadIdx.x, i, j, k)) return;
-    long long c = L.at(i, j, k), s = L.stride(dT1);
-    double VolB[8], VelB[3][8];
-#pragma unroll
-    for (int n = 0; n < 8; ++n) {
-        long long cn = c + (n - 4) * s;
-        double vol = g.volume[cn];
-        double den = dmax(h.gas[0][cn], p.dFloor);
-        VolB[n] = vol;
-#pragma unroll
-        for (int x = 0; x < 3; ++x) VelB[x][n] = vol * h.gas[1 + x][cn] / den;
-    }
-    double dV = dmax(central8<double>(VolB), TINY);
-#pragma unroll
-    for (int x = 0; x < 3; ++x) Vf.v[x][c] = central8<double>(VelB[x]) / dV;
-}
-
-// EdgeLRs (fields.F90:288-362): limited L/R of flux/area of the dA faces along dS, times the area
-template <typename T>
-__device__ __forceinline__ void edgeLR(const Lay& L, const Par& p, const GridP& g, double* const* hmf,
-                                       double* const* nmf, long long c, int dA, int dS, T& bL, T& bR, T& fA) {
-    long long s = L.stride(dS);
-    const double* A = g.face[dA];
-    T Ab[8], Mb[8], nMb[4];
-#pragma unroll
-    for (int n = 0; n < 8; ++n) {
-        double a = A[c + (n - 4) * s];
-        Ab[n] = T(a);
-        Mb[n] = T(hmf[dA][c + (n - 4) * s] / dmax(a, TINY));
-    }
-    double* const* lim = p.doLFMLim ? nmf : hmf;
-#pragma unroll
-    for (int m = 0; m < 4; ++m) {
-        double a = A[c + (m - 2) * s];
-        nMb[m] = T(lim[dA][c + (m - 2) * s] / dmax(a, TINY));
-    }
-    T Vi = central8<T>(Ab);
-    T l, rr;
-    getLR<T>(p.rmeth, T(p.pdmb), Ab, Mb, nMb, Vi, l, rr);
-    fA = Vi;   // dot_product(interpWgt, AreaB) is the same sum as Central8(VolB) with VolB = AreaB
-    bL = l * fA;
-    bR = rr * fA;
-}
-
-// GetCornerV/GetCornerD/GetCornerB and the EMF (fields.F90:186-225, 365-517) on the eD edges
-template <typename T>
-__global__ void k_edge_emf(Lay L, Par p, GridP g, StateP n, StateP h, Vec3P Vf, double* Eout, Reg r, int eD,
-                           int dT1, int dT2, const Scal* sc) {
-    int i, j, k;
-    if (!reg_ijk(r, blockIdx.x * (long long)blockDim.x + threadIdx.x, i, j, k)) return;
-    long long c = L.at(i, j, k);
-    // GetCornerV: area-weighted Central8 of the face velocities along dT2, mapped with Te
-    long long s2 = L.stride(dT2);
-    T Ab[8];
-#pragma unroll
-    for (int m = 0; m < 8; ++m) Ab[m] = T(g.face[dT1][c + (m - 4) * s2]);
-    T dA = central8<T>(Ab);
-    dA = dA > T(TINY) ? dA : T(TINY);
-    T Vc[3];
-#pragma unroll
-    for (int x = 0; x < 3; ++x) {
-        T s = T(0);
-#pragma unroll
-        for (int m = 0; m < 8; ++m) s = s + T(wC8(m)) * (Ab[m] * T(Vf.v[x][c + (m - 4) * s2]));
-        Vc[x] = s / dA;
-    }
-    T v1 = Vc[0] * T(g.Te[eD][3][c]) + Vc[1] * T(g.Te[eD][4][c]) + Vc[2] * T(g.Te[eD][5][c]);
-    T v2 = Vc[0] * T(g.Te[eD][6][c]) + Vc[1] * T(g.Te[eD][7][c]) + Vc[2] * T(g.Te[eD][8][c]);
-    T vDiff = sqrt(v1 * v1 + v2 * v2);
-    // GetCornerD: 4-point average of the half-state density around the edge (getNormalPlane)
-    int e1 = (eD == IDIR) ? JDIR : IDIR;
-    int e2 = (eD == KDIR) ? JDIR : KDIR;
-    long long se1 = L.stride(e1), se2 = L.stride(e2);
-    T Dc = T(0.25 * (h.gas[0][c] + h.gas[0][c - se1] + h.gas[0][c - se2] + h.gas[0][c - se1 - se2]));
-    // GetCornerB
-    T bT1L, bT1R, fA1, bT2L, bT2R, fA2;
-    edgeLR<T>(L, p, g, h.mf, n.mf, c, dT1, dT2, bT1L, bT1R, fA1);
-    edgeLR<T>(L, p, g, h.mf, n.mf, c, dT2, dT1, bT2L, bT2R, fA2);
-    T xni = T(g.Teb[eD][0][c]), yni = T(g.Teb[eD][1][c]), xnj = T(g.Teb[eD][2][c]), ynj = T(g.Teb[eD][3][c]);
-    T detT = T(1) / (xni * ynj - xnj * yni);
-    T bT1 = T(0.5) * (bT1L + bT1R) / fA1;
-    T bT2 = T(0.5) * (bT2L + bT2R) / fA2;
-    T db1 = (bT1R - bT1L) / fA1;
-    T db2 = (bT2R - bT2L) / fA2;
-    T Jd = db2 - db1;
-    T b1 = detT * (ynj * bT1 - yni * bT2);
-    T b2 = detT * (-(xnj * bT1) + xni * bT2);
-    // diffusive speed and EMF
-    T vA = sqrt(b1 * b1 + b2 * b2) / sqrt(Dc);
-    if (p.doBoris) { T Ca = T(p.Ca); vA = Ca * vA / sqrt(Ca * Ca + vA * vA); }
-    vDiff = vDiff + vA;
-    double edg = g.edge[eD][c];
-    T lim = T(p.CFL * edg / sc->dt);
-    vDiff = vDiff < lim ? vDiff : lim;
-    T e = -(v1 * b2 - v2 * b1) + T(p.Vd0) * vDiff * Jd;
-    Eout[c] = double(e) * edg;
-}
-
-// ================================================================================ fluxes
-// One-sided gas kinetic flux (stress.F90:432-511)
-template <typename T>
-__device__ __forceinline__ void gasKin(T gm1, T sg, const T* W, const T* Tf, T* gF, T* dW) {
-    T D = W[0], Vx = W[1], Vy = W[2], Vz = W[3], P = W[4];
-    T E = T(0.5) * D * (Vx * Vx + Vy * Vy + Vz * Vz) + P / gm1;
-    T lambda = D / (T(2) * P);
-    T Vn = Tf[0] * Vx + Tf[1] * Vy + Tf[2] * Vz;
-    T Vt1 = Tf[3] * Vx + Tf[4] * Vy + Tf[5] * Vz;
-    T Vt2 = Tf[6] * Vx + Tf[7] * Vy + Tf[8] * Vz;
-    T Vn0 = T(0.5) * erfc(sg * sqrt(lambda) * Vn);
-    T Vn1 = Vn * Vn0 - T(0.5) * sg * exp(-(lambda * Vn * Vn)) / sqrt(T(PI) * lambda);
-    gF[0] = gF[0] + D * Vn1;
-    gF[4] = gF[4] + (E + T(0.5) * P) * Vn1 + T(0.5) * P * Vn0 * Vn;
-    T fMn = D * Vn * Vn1 + P * Vn0;
-    T fMt1 = D * Vt1 * Vn1;
-    T fMt2 = D * Vt2 * Vn1;
-    gF[1] = gF[1] + (Tf[0] * fMn + Tf[3] * fMt1 + Tf[6] * fMt2);
-    gF[2] = gF[2] + (Tf[1] * fMn + Tf[4] * fMt1 + Tf[7] * fMt2);
-    gF[3] = gF[3] + (Tf[2] * fMn + Tf[5] * fMt1 + Tf[8] * fMt2);
-    dW[0] = dW[0] + sg * D;
-    dW[1] = dW[1] + sg * D * Vx;
-    dW[2] = dW[2] + sg * D * Vy;
-    dW[3] = dW[3] + sg * D * Vz;
-    dW[4] = dW[4] + sg * E;
-}
-// One-sided magnetic stress (stress.F90:513-599, no background field)
-template <typename T>
-__device__ __forceinline__ void magKin(const Par& p, T sg, const T* W, const T* B, T Bn, const T* Tf, T* mF, T& bbD,
-                                       T& VaD) {
-    T D = W[0], P = W[4];
-    T dPb = T(0.5) * (B[0] * B[0] + B[1] * B[1] + B[2] * B[2]);
-    T Va2 = T(2) * dPb / D;
-    bbD = bbD + T(0.5) * (B[0] * B[0] + B[1] * B[1] + B[2] * B[2]);
-    T Vac2 = Va2;
-    if (p.doBoris) { T Ca = T(p.Ca); Vac2 = Va2 / (T(1) + (Va2 / (Ca * Ca))); }
-    T Vn = Tf[0] * W[1] + Tf[1] * W[2] + Tf[2] * W[3];
-    T lambda = T(1) / (T(2) * P / D + Vac2);
-    T Vn0 = T(0.5) * erfc(sg * sqrt(lambda) * Vn);
-    VaD = VaD + T(0.5) * sqrt(Vac2);
-    mF[0] = mF[0] + Vn0 * (dPb * Tf[0] - B[0] * Bn);
-    mF[1] = mF[1] + Vn0 * (dPb * Tf[1] - B[1] * Bn);
-    mF[2] = mF[2] + Vn0 * (dPb * Tf[2] - B[2] * Bn);
-}
-
-// Fluxes (stress.F90:204-429) at every interface of direction d: reconstruction + limiter of the
-// half-state primitives and B (limited on state n), magnetic and gas kinetic fluxes, HOGS diffusion,
-// scaled by the face area.
-template <typename T>
-__global__ void __launch_bounds__(128) k_fluxes(Lay L, Par p, GridP g, StateP n, StateP h, PrimP Wh, PrimP Wn,
-                                                FluxP F, Reg r, int d) {
-    int i, j, k;
-    if (!reg_ijk(r, blockIdx.x * (long long)blockDim.x + threadIdx.x, i, j, k)) return;
-    long long c = L.at(i, j, k), s = L.stride(d);
-    T Vol[8];
-#pragma unroll
-    for (int m = 0; m < 8; ++m) Vol[m] = T(g.volume[c + (m - 4) * s]);
-    T Vi = central8<T>(Vol);
-    T pdmb = T(p.pdmb);
-    T WL[5], WR[5];
-#pragma unroll
-    for (int v = 0; v < 5; ++v) {
-        T Q[8], nQ[4];
-#pragma unroll
-        for (int m = 0; m < 8; ++m) Q[m] = T(Wh.w[v][c + (m - 4) * s]);
-#pragma unroll
-        for (int m = 0; m < 4; ++m) nQ[m] = T((p.doLFMLim ? Wn.w[v] : Wh.w[v])[c + (m - 2) * s]);
-        getLR<T>(p.rmeth, pdmb, Vol, Q, nQ, Vi, WL[v], WR[v]);
-    }
-    T Tf[9];
-#pragma unroll
-    for (int q = 0; q < 9; ++q) Tf[q] = T(g.Tf[d][q][c]);
-    double faB = g.face[d][c];
-    T VaD = T(0), bbD = T(0);
-    if (p.doMHD) {
-        T BL[3], BR[3];
-#pragma unroll
-        for (int x = 0; x < 3; ++x) {
-            T Q[8], nQ[4];
-#pragma unroll
-            for (int m = 0; m < 8; ++m) Q[m] = T(h.b[x][c + (m - 4) * s]);
-#pragma unroll
-            for (int m = 0; m < 4; ++m) nQ[m] = T((p.doLFMLim ? n.b[x] : h.b[x])[c + (m - 2) * s]);
-            getLR<T>(p.rmeth, pdmb, Vol, Q, nQ, Vi, BL[x], BR[x]);
-        }
-        T Bn = T(h.mf[d][c] / faB);
-        T mF[3] = {T(0), T(0), T(0)};
-        magKin<T>(p, T(-1), WL, BL, Bn, Tf, mF, bbD, VaD);
-        magKin<T>(p, T(1), WR, BR, Bn, Tf, mF, bbD, VaD);
-        if (p.doBoris) {
-            T Ca2 = T(p.Ca) * T(p.Ca);
-#pragma unroll
-            for (int x = 0; x < 3; ++x) {
-                T deeV = WR[1 + x] - WL[1 + x];
-                T deeP = bbD * deeV / Ca2;
-                mF[x] = mF[x] - T(p.cHogM) * VaD * deeP;
-            }
-        }
-#pragma unroll
-        for (int x = 0; x < 3; ++x) F.m[x][c] = faB * double(mF[x]);
-    }
-    T gF[5] = {T(0), T(0), T(0), T(0), T(0)}, dW[5] = {T(0), T(0), T(0), T(0), T(0)};
-    T gm1 = T(p.gamma - 1);
-    gasKin<T>(gm1, T(-1), WL, Tf, gF, dW);
-    gasKin<T>(gm1, T(1), WR, Tf, gF, dW);
-    T cH = T(p.cHogH);
-#pragma unroll
-    for (int v = 0; v < 5; ++v) gF[v] = gF[v] - cH * VaD * dW[v];
-    if (p.doBoris) {  // nuclear option, stress.F90:399-417 (cLim = 1.5)
-        T vL = sqrt(WL[1] * WL[1] + WL[2] * WL[2] + WL[3] * WL[3]);
-        T vR = sqrt(WR[1] * WR[1] + WR[2] * WR[2] + WR[3] * WR[3]);
-        T Vn = sqrt(vL * vL + vR * vR) / T((double)sqrtf(2.0f));
-        if (Vn >= T(1.5) * T(p.Ca)) {
-#pragma unroll
-            for (int v = 0; v < 5; ++v) gF[v] = gF[v] - T(p.Ca) * T(h.gas[v][c] - h.gas[v][c - s]);
-        }
-    }
-#pragma unroll
-    for (int v = 0; v < 5; ++v) F.g[v][c] = faB * double(gF[v]);
 }
 
 // Flux2Deltas (stress.F90:150-196)
@@ -772,53 +541,11 @@ int kernels_per_step(const Handle& h) {
     return n;
 }
 
-template <typename T>
 static void enqueue_hot(Handle& h, const StateP& nS, cudaStream_t st, cudaEvent_t* ev) {
-    const Lay& L = h.L;
     const Par& p = h.p;
-    GridP g = h.gridP();
-    PrimP Wh, Wn;
-    for (int v = 0; v < 5; ++v) { Wh.w[v] = h.Wh[v]; Wn.w[v] = h.Wn[v]; }
-    if (p.doMHD) {
-        Vec3P Vf = {{h.Vf[0], h.Vf[1], h.Vf[2]}};
-        cudaMemsetAsync(h.E[0], 0, sizeof(double) * L.E * 3, st);   // E planes are contiguous in the pool
-        for (int eD = 0; eD < 3; ++eD) {
-            int dT1, dT2;
-            Reg rv, re;
-            int is = L.is(), ie = L.ie(), js = L.js(), je = L.je(), ks = L.ks(), ke = L.ke();
-            if (eD == IDIR) {
-                dT1 = JDIR; dT2 = KDIR;
-                rv = mkreg(0, L.Ni - 1, js, je + 1, 0, L.Nk - 1);
-                re = mkreg(is, ie, js, je + 1, ks, ke + 1);
-            } else if (eD == JDIR) {
-                dT1 = KDIR; dT2 = IDIR;
-                rv = mkreg(0, L.Ni - 1, 0, L.Nj - 1, ks, ke + 1);
-                re = mkreg(is, ie + 1, js, je, ks, ke + 1);
-            } else {
-                dT1 = IDIR; dT2 = JDIR;
-                rv = mkreg(is, ie + 1, 0, L.Nj - 1, 0, L.Nk - 1);
-                re = mkreg(is, ie + 1, js, je + 1, ks, ke);
-            }
-            k_mom2face<<<nblk(rv.n(), TPB), TPB, 0, st>>>(L, p, g, h.H, Vf, rv, dT1);
-            k_edge_emf<T><<<nblk(re.n(), TPB), TPB, 0, st>>>(L, p, g, nS, h.H, Vf, h.E[eD], re, eD, dT1, dT2, h.dScal);
-            h.launches += 2;
-        }
-    }
+    if (p.doMHD) enqueue_efield(h, nS, st);
     if (ev) cudaEventRecord(ev[PH_FLUXES], st);
-    int nF = p.do25D ? 2 : 3;
-    for (int d = 0; d < nF; ++d) {
-        Reg r;
-        int is = L.is(), ie = L.ie(), js = L.js(), je = L.je(), ks = L.ks(), ke = L.ke();
-        if (p.do25D) ke = ks;
-        if (d == IDIR) r = mkreg(is, ie + 1, js, je, ks, ke);
-        else if (d == JDIR) r = mkreg(is, ie, js, je + 1, ks, ke);
-        else r = mkreg(is, ie, js, je, ks, ke + 1);
-        FluxP F;
-        for (int v = 0; v < 5; ++v) F.g[v] = h.gflx[d][v];
-        for (int x = 0; x < 3; ++x) F.m[x] = h.mflx[d][x];
-        k_fluxes<T><<<nblk(r.n(), 128), 128, 0, st>>>(L, p, g, nS, h.H, Wh, Wn, F, r, d);
-        h.launches++;
-    }
+    enqueue_fluxes(h, nS, st);
 }
 
 int step_enqueue(Handle& h, int cur, cudaEvent_t* ev) {
@@ -832,18 +559,19 @@ int step_enqueue(Handle& h, int cur, cudaEvent_t* ev) {
     k_step_begin<<<1, 1, 0, st>>>(h.dScal);
     if (p.doMHD) {
         Vec3P mf = {{nS.mf[0], nS.mf[1], nS.mf[2]}}, omf = {{oS.mf[0], oS.mf[1], oS.mf[2]}},
-              hmf = {{h.H.mf[0], h.H.mf[1], h.H.mf[2]}};
-        k_predict_faces<<<nblk(L.E, 256), 256, 0, st>>>(L.E, mf, omf, hmf, h.dScal);
+              hmf = {{h.H.mf[0], h.H.mf[1], h.H.mf[2]}}, hbA = {{h.hbA[0], h.hbA[1], h.hbA[2]}},
+              nbA = {{h.nbA[0], h.nbA[1], h.nbA[2]}};
+        k_predict_faces<<<nblk(L.E, 256), 256, 0, st>>>(L.E, p, g, mf, omf, hmf, hbA, nbA, h.dScal);
         h.launches++;
     }
     PrimP Wh, Wn;
     for (int v = 0; v < 5; ++v) { Wh.w[v] = h.Wh[v]; Wn.w[v] = h.Wn[v]; }
     long long ncell = (long long)L.Ni * L.Nj * L.Nk;
-    k_predict_cells<<<nblk(ncell, TPB), TPB, 0, st>>>(L, p, g, nS, oS, h.H, Wh, Wn, h.dScal);
+    Vec3P VdV = {{h.VdV[0], h.VdV[1], h.VdV[2]}};
+    k_predict_cells<<<nblk(ncell, TPB), TPB, 0, st>>>(L, p, g, nS, oS, h.H, Wh, Wn, VdV, h.dScal);
     h.launches += 2;
     mark(PH_EFIELD);
-    if (h.prec == PREC_FP32FLUX) enqueue_hot<float>(h, nS, st, ev);
-    else enqueue_hot<double>(h, nS, st, ev);
+    enqueue_hot(h, nS, st, ev);
     mark(PH_DELTAS);
     FluxP F[3];
     for (int d = 0; d < 3; ++d) {

@@ -25,6 +25,9 @@ struct Handle {
     double* Wh[5];        // primitives of the half state (BlockCon2Prim), for reconstruction
     double* Wn[5];        // primitives of state n, for the limiter
     double* E[3];         // Efld (edge-centred, times edge length)
+    double* VdV[3];       // half-state volume * momentum / max(rho, dFloor) per cell (Mom2Face summand)
+    double* hbA[3];       // half-state face flux / max(face area, TINY) (EdgeLRs reconstruction values)
+    double* nbA[3];       // limiter-state face flux / max(face area, TINY) (EdgeLRs limiter values)
     double* Vf[3];        // face velocities pushed along dT1
     double* dGasH[5];
     double* dGasM[3];
@@ -60,5 +63,11 @@ void launch_bcs(Handle& h, const StateP& s, cudaStream_t st);
 void launch_calcdt(Handle& h, const StateP& s, int mode, cudaStream_t st);   // mode 0: in-step, 1: initial (no time advance)
 double launch_divb(Handle& h, double* scratchDev, cudaStream_t st);
 int kernels_per_step(const Handle& h);
+// interface fluxes of all directions (gam_flux.cu)
+void enqueue_fluxes(Handle& h, const StateP& nS, cudaStream_t st);
+void flux_kernels_init();
+// E field of all edge directions (gam_efield.cu): Mom2Face + tiled EMF
+void enqueue_efield(Handle& h, const StateP& nS, cudaStream_t st);
+void efield_kernels_init();
 
 }  // namespace gam

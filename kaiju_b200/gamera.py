@@ -67,8 +67,8 @@ class StatusC(C.Structure):
 # every entry point declared in include/gamgpu.h with its ctypes signature
 _DP = C.POINTER(C.c_double)
 SIGNATURES = {
-    "gam_gpu_create": (C.c_int, [C.POINTER(C.c_void_p), C.POINTER(ModelC), C.POINTER(GridC), _DP, _DP, _DP, _DP,
-                                 C.c_double, C.c_double]),
+    "gam_gpu_create": (C.c_int, [C.POINTER(C.c_void_p), C.POINTER(ModelC), C.POINTER(GridC), _DP, _DP, _DP, _DP, _DP,
+                                 _DP, C.c_double, C.c_double]),
     "gam_gpu_create_from_corners": (C.c_int, [C.POINTER(C.c_void_p), C.POINTER(ModelC), _DP, C.c_int]),
     "gam_gpu_step": (C.c_int, [C.c_void_p, _DP, C.POINTER(C.c_int), _DP]),
     "gam_gpu_advance": (C.c_int, [C.c_void_p, C.c_double]),
@@ -76,7 +76,8 @@ SIGNATURES = {
     "gam_gpu_run_steps_timed": (C.c_int, [C.c_void_p, C.c_int, _DP]),
     "gam_gpu_profile_phases": (C.c_int, [C.c_void_p, C.c_int, _DP, C.c_int]),
     "gam_gpu_sync_to_host": (C.c_int, [C.c_void_p, C.c_uint, _DP, _DP, _DP, _DP, _DP]),
-    "gam_gpu_sync_to_device": (C.c_int, [C.c_void_p, C.c_uint, _DP, _DP, _DP, _DP, C.c_double, C.c_double]),
+    "gam_gpu_sync_to_device": (C.c_int, [C.c_void_p, C.c_uint, _DP, _DP, _DP, _DP, _DP, _DP, C.c_double,
+                                         C.c_double]),
     "gam_gpu_get_status": (C.c_int, [C.c_void_p, C.POINTER(StatusC)]),
     "gam_gpu_set_scalars": (C.c_int, [C.c_void_p, C.c_double, C.c_double, C.c_double, C.c_int, C.c_double,
                                       C.c_double]),
@@ -237,8 +238,10 @@ class GameraGPU:
 
     # ---- construction
     @classmethod
-    def from_arrays(cls, model: Model, grid: dict, gas, magflux, ogas, omagflux, time: float, otime: float):
-        """Drop-in path: the host ran Hatch; mirror its Grid_T/State_T arrays onto the device."""
+    def from_arrays(cls, model: Model, grid: dict, gas, magflux, ogas, omagflux, time: float, otime: float,
+                    bxyz=None, obxyz=None):
+        """Drop-in path: the host ran Hatch; mirror its Grid_T/State_T arrays onto the device.
+        bxyz/obxyz: State%Bxyz/oState%Bxyz as Hatch left them (None: recompute with bFlux2Fld)."""
         L = load_library()
         keep = {k: np.asfortranarray(v, dtype=np.float64) for k, v in grid.items()}
         g = GridC()
@@ -246,7 +249,8 @@ class GameraGPU:
                            ("volume", "volume"), ("face", "face"), ("edge", "edge"), ("Tf", "tf"), ("Te", "te"),
                            ("Teb", "teb")):
             setattr(g, cname, _dp(keep[key]))
-        arrs = [np.asfortranarray(a, dtype=np.float64) for a in (gas, magflux, ogas, omagflux)]
+        arrs = [None if a is None else np.asfortranarray(a, dtype=np.float64)
+                for a in (gas, magflux, bxyz, ogas, omagflux, obxyz)]
         h = C.c_void_p()
         m = model.to_c()
         rc = L.gam_gpu_create(C.byref(h), C.byref(m), C.byref(g), *[_dp(a) for a in arrs], time, otime)
@@ -344,11 +348,12 @@ class GameraGPU:
         if rc:
             raise GamError(rc, "gam_gpu_sync_to_host")
 
-    def sync_to_device(self, gas=None, magflux=None, ogas=None, omagflux=None, time=0.0, otime=0.0):
+    def sync_to_device(self, gas=None, magflux=None, ogas=None, omagflux=None, time=0.0, otime=0.0, bxyz=None,
+                       obxyz=None):
         what = (GAM_SYNC_STATE if (gas is not None or magflux is not None) else 0) | \
                (GAM_SYNC_OSTATE if (ogas is not None or omagflux is not None) else 0)
-        rc = load_library().gam_gpu_sync_to_device(self.h, what, _dp(gas), _dp(magflux), _dp(ogas), _dp(omagflux),
-                                                   time, otime)
+        rc = load_library().gam_gpu_sync_to_device(self.h, what, _dp(gas), _dp(magflux), _dp(bxyz), _dp(ogas),
+                                                   _dp(omagflux), _dp(obxyz), time, otime)
         if rc:
             raise GamError(rc, "gam_gpu_sync_to_device")
 

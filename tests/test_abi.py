@@ -39,10 +39,10 @@ def test_errstr_and_argument_checks(lib):
     h = C.c_void_p()
     m = gm.Model(32, 32, 4).to_c()
     # missing arrays: rejected before any CUDA call
-    assert lib.gam_gpu_create(C.byref(h), C.byref(m), None, None, None, None, None, 0.0, 0.0) == gm.GAM_ERR_ARG
+    assert lib.gam_gpu_create(C.byref(h), C.byref(m), None, None, None, None, None, None, None, 0.0, 0.0) == gm.GAM_ERR_ARG
     m.doResistive = 1
     g = gm.GridC()
-    assert lib.gam_gpu_create(C.byref(h), C.byref(m), C.byref(g), None, None, None, None, 0.0, 0.0) == gm.GAM_ERR_ARG
+    assert lib.gam_gpu_create(C.byref(h), C.byref(m), C.byref(g), None, None, None, None, None, None, 0.0, 0.0) == gm.GAM_ERR_ARG
     assert lib.gam_gpu_step(None, None, None, None) == gm.GAM_ERR_ARG
     assert lib.gam_gpu_fetch(None, b"gas", None, 0) == gm.GAM_ERR_ARG
 
