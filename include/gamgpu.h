@@ -145,6 +145,21 @@ int gam_gpu_set_precision(gam_gpu_t* h, int mode);
 int gam_gpu_fetch(gam_gpu_t* h, const char* name, double* out, long long n);
 
 void gam_gpu_destroy(gam_gpu_t* h);
+
+/* DivB for callers that cannot allocate device memory (no counterpart in the reference).
+ * Some hosts cannot call cudaMalloc: device arrays owned by another runtime (OpenACC or CUDA Fortran
+ * data regions, a coupler's memory pool) or code running where an allocation would synchronise the
+ * device or upset its memory accounting. This entry point needs no handle and allocates nothing: it
+ * reads magflux_dev, a device copy of State%magFlux in the Fortran layout (Ni+1,Nj+1,Nk+1,3) with
+ * Ni = Nip+2*nG etc., and writes the sum over active cells of |net face flux| (DivB,
+ * src/gamera/gridutils.F90:717-770) to the device double *tot_dev. Its only scratch is a file-scope
+ * device array sized for GAM_DIVB_NOALLOC_MAX_CELLS active cells (512 KiB per GPU that loads the
+ * library, held until exit); larger grids are rejected with GAM_ERR_ARG. The first call on a device
+ * looks up that array's device address, so make it before capturing a stream. Kernels run on the
+ * legacy default stream; synchronise before reading *tot_dev. All calls share the scratch array, so
+ * calls that overlap on the GPU (from several host threads or streams) race. */
+#define GAM_DIVB_NOALLOC_MAX_CELLS (256LL * 256LL * 256LL)
+int gam_divb_noalloc(const double* magflux_dev, int Nip, int Njp, int Nkp, int nG, double* tot_dev);
 const char* gam_gpu_errstr(int code);
 
 #ifdef __cplusplus

@@ -86,6 +86,7 @@ SIGNATURES = {
     "gam_gpu_fetch": (C.c_int, [C.c_void_p, C.c_char_p, _DP, C.c_longlong]),
     "gam_gpu_destroy": (None, [C.c_void_p]),
     "gam_gpu_errstr": (C.c_char_p, [C.c_int]),
+    "gam_divb_noalloc": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_void_p]),
 }
 
 _lib = None

@@ -11,7 +11,7 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 def declared_symbols():
     text = open(os.path.join(ROOT, "include", "gamgpu.h")).read()
     text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
-    return sorted(set(re.findall(r"\b(gam_gpu_\w+)\s*\(", text)))
+    return sorted(set(re.findall(r"\b(gam_\w+)\s*\(", text)))
 
 
 @pytest.fixture(scope="module")
