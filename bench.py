@@ -117,6 +117,18 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(rows)}
 
 
+def traffic_per_unit(kernel, prec):
+    """DRAM bytes per interface/edge of a kernel from the committed ncu summary (profiles/), or None."""
+    try:
+        for line in open(os.path.join(ROOT, "profiles", "roofline_traffic.txt")):
+            f = line.split()
+            if len(f) >= 3 and not line.startswith("#") and f[0] == kernel and f[1] == prec:
+                return float(f[2])
+    except OSError:
+        pass
+    return None
+
+
 def peaks():
     try:
         return json.load(open(PEAKS_PATH)), "measured"
@@ -210,9 +222,11 @@ def run_ours(args, rank, world, local):
     n_if = (n + 1) * n * n   # interfaces per direction launch
     flux_launch_ms = ph["fluxes"] / 3.0
     achieved = FLUX_BYTES_PER_IFACE * n_if / (flux_launch_ms / 1e3) / 1e9
-    roof = {"kernel": "k_fluxes<double>" if args.prec == "fp64" else "k_fluxes<float>",
+    tpu = traffic_per_unit("k_flux_tile", args.prec)
+    roof = {"kernel": "k_flux_tile<double>" if args.prec == "fp64" else "k_flux_tile<float>",
             "bound": "hbm", "achieved": round(achieved, 1), "peak": hbm, "unit": "GB/s",
-            "frac": round(achieved / hbm, 4), "traffic": None, "peak_source": pk_kind,
+            "frac": round(achieved / hbm, 4), "traffic": (round(tpu * n_if) if tpu else None),
+            "algorithmic_bytes": FLUX_BYTES_PER_IFACE * n_if, "peak_source": pk_kind,
             "launch_ms": round(flux_launch_ms, 4),
             "fp64_tflops": round(FLUX_FLOPS_PER_IFACE * n_if / (flux_launch_ms / 1e3) / 1e12, 3),
             "fp64_peak_nominal_tflops": FP64_NOMINAL_TFLOPS,
