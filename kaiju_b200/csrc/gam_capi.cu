@@ -485,6 +485,7 @@ int gam_gpu_divb(gam_gpu_t* G, double* tot) {
 int gam_gpu_set_precision(gam_gpu_t* G, int mode) {
     if (!G) return GAM_ERR_ARG;
     if (mode != GAM_FP64 && mode != GAM_FP32FLUX) return GAM_ERR_ARG;
+    if (mode == GAM_FP32FLUX && ensure_f32(G->h) != 0) return GAM_ERR_CUDA;
     if (mode != G->h.prec) {
         G->h.prec = mode;
         destroy_graphs(G->h);
@@ -544,6 +545,7 @@ void gam_gpu_destroy(gam_gpu_t* G) {
     if (h.stream) cudaStreamSynchronize(h.stream);
     destroy_graphs(h);
     if (h.pool) cudaFree(h.pool);
+    if (h.f32pool) cudaFree(h.f32pool);
     if (G->stage) cudaFree(G->stage);
     if (G->scratch) cudaFree(G->scratch);
     if (h.dScal) cudaFree(h.dScal);

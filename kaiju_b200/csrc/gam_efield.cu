@@ -9,6 +9,7 @@
 //     field; the 2x2 corner densities -- and evaluates GetCornerV, GetCornerD, GetCornerB (two limited
 //     EdgeLRs) and the EMF for its edge from shared memory.
 #include <cstdio>
+#include <type_traits>
 #include "gam_common.cuh"
 #include "gam_kern.cuh"
 #include "gam_step.cuh"
@@ -16,7 +17,8 @@
 namespace gam {
 
 // ------------------------------------------------------------------ Mom2Face (fields.F90:235-285)
-__global__ void k_mom2face2(Lay L, GridP g, Vec3P VdV, Vec3P Vf, Reg r, int dT1) {
+struct Vec3F { float* v[3]; };
+__global__ void k_mom2face2(Lay L, GridP g, Vec3P VdV, Vec3P Vf, Vec3F Vf32, Reg r, int dT1) {
     int i, j, k;
     if (!reg3(r, i, j, k)) return;
     long long c = L.at(i, j, k), s = L.stride(dT1);
@@ -31,6 +33,10 @@ __global__ void k_mom2face2(Lay L, GridP g, Vec3P VdV, Vec3P Vf, Reg r, int dT1)
         s2 = s2 + w * __ldg(&VdV.v[2][cn]);
     }
     double dV = dmax(sV, TINY);
+    if (Vf32.v[0]) {   // FP32-flux path stores the face velocities as float
+        Vf32.v[0][c] = float(s0 / dV); Vf32.v[1][c] = float(s1 / dV); Vf32.v[2][c] = float(s2 / dV);
+        return;
+    }
     Vf.v[0][c] = s0 / dV;
     Vf.v[1][c] = s1 / dV;
     Vf.v[2][c] = s2 / dV;
@@ -66,29 +72,28 @@ __device__ __forceinline__ int bidx(BoxC b, int di, int dj, int dk) {
     return (di - b.oi) + b.ni * ((dj - b.oj) + b.nj * (dk - b.ok));
 }
 
-template <typename T, int ED>
-__global__ void __launch_bounds__(256, 2) k_edge_tile(Lay L, Par p, GridP g, StateP h, Vec3P Vf, Vec3P hbA,
-                                                      Vec3P nbA, double* Eout, Reg r, const Scal* sc) {
+template <typename T, typename S, int ED>
+__global__ void __launch_bounds__(256, 2) k_edge_tile(Lay L, Par p, EdgeSrc<S> in, double* Eout, Reg r, const Scal* sc) {
     using TL = ETile<ED>;
     constexpr int dT1 = TL::dT1, dT2 = TL::dT2;
     extern __shared__ __align__(16) unsigned char smraw[];
-    double* sm = reinterpret_cast<double*>(smraw);
+    S* sm = reinterpret_cast<S*>(smraw);
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int ti = lane, tj = (tid >> 5) % TL::TJ, tk = (tid >> 5) / TL::TJ;
     const int i0 = r.i0 + blockIdx.x * TL::TI, j0 = r.j0 + blockIdx.y * TL::TJ, k0 = r.k0 + blockIdx.z * TL::TK;
     constexpr BoxC b8t2 = TL::b8t2, b4t2 = TL::b4t2, b8t1 = TL::b8t1, b4t1 = TL::b4t1, bR = TL::bR;
-    auto stage = [&](double* dst, const double* src, BoxC b) {
-        stage_rows(dst, src, L, i0 + b.oi, b.ni, j0 + b.oj, b.nj, k0 + b.ok, b.nk, warp, 8, lane);
+    auto stage = [&](S* dst, const S* src, BoxC b) {
+        stage_rows<S>(dst, src, L, i0 + b.oi, b.ni, j0 + b.oj, b.nj, k0 + b.ok, b.nk, warp, 8, lane);
     };
 #pragma unroll
-    for (int x = 0; x < 3; ++x) stage(sm + TL::oVf + x * TL::n8t2, Vf.v[x], b8t2);
-    stage(sm + TL::oA1, g.face[dT1], b8t2);
-    stage(sm + TL::oB1, hbA.v[dT1], b8t2);
-    stage(sm + TL::oN1, nbA.v[dT1], b4t2);
-    stage(sm + TL::oA2, g.face[dT2], b8t1);
-    stage(sm + TL::oB2, hbA.v[dT2], b8t1);
-    stage(sm + TL::oN2, nbA.v[dT2], b4t1);
-    stage(sm + TL::oR, h.gas[0], bR);
+    for (int x = 0; x < 3; ++x) stage(sm + TL::oVf + x * TL::n8t2, in.Vf[x], b8t2);
+    stage(sm + TL::oA1, in.face[dT1], b8t2);
+    stage(sm + TL::oB1, in.hbA[dT1], b8t2);
+    stage(sm + TL::oN1, in.nbA[dT1], b4t2);
+    stage(sm + TL::oA2, in.face[dT2], b8t1);
+    stage(sm + TL::oB2, in.hbA[dT2], b8t1);
+    stage(sm + TL::oN2, in.nbA[dT2], b4t1);
+    stage(sm + TL::oR, in.rho, bR);
     cp_async_wait_all();
     __syncthreads();
     const int i = i0 + ti, j = j0 + tj, k = k0 + tk;
@@ -115,8 +120,8 @@ __global__ void __launch_bounds__(256, 2) k_edge_tile(Lay L, Par p, GridP g, Sta
     T fA1 = central8<T>(Ab);
     T dA = fA1 > T(TINY) ? fA1 : T(TINY);
     Vc0 = Vc0 / dA; Vc1 = Vc1 / dA; Vc2 = Vc2 / dA;
-    T v1 = Vc0 * T(__ldg(&g.Te[ED][3][c])) + Vc1 * T(__ldg(&g.Te[ED][4][c])) + Vc2 * T(__ldg(&g.Te[ED][5][c]));
-    T v2 = Vc0 * T(__ldg(&g.Te[ED][6][c])) + Vc1 * T(__ldg(&g.Te[ED][7][c])) + Vc2 * T(__ldg(&g.Te[ED][8][c]));
+    T v1 = Vc0 * T(__ldg(&in.Te[ED][0][c])) + Vc1 * T(__ldg(&in.Te[ED][1][c])) + Vc2 * T(__ldg(&in.Te[ED][2][c]));
+    T v2 = Vc0 * T(__ldg(&in.Te[ED][3][c])) + Vc1 * T(__ldg(&in.Te[ED][4][c])) + Vc2 * T(__ldg(&in.Te[ED][5][c]));
     T vDiff = sqrt(v1 * v1 + v2 * v2);
     // GetCornerD (fields.F90:427-454), getNormalPlane order: e1 = first transverse of (I,J,K) \ eD
     constexpr int e1 = ED == 0 ? 1 : 0, e2 = ED == 2 ? 1 : 2;
@@ -128,7 +133,9 @@ __global__ void __launch_bounds__(256, 2) k_edge_tile(Lay L, Par p, GridP g, Sta
         int dk = a0k - (e1 == 2 ? d1 : 0) - (e2 == 2 ? d2 : 0);
         return sm[TL::oR + bidx(bR, di, dj, dk)];
     };
-    T Dc = T(0.25 * (rho(0, 0) + rho(1, 0) + rho(0, 1) + rho(1, 1)));
+    T Dc;
+    if constexpr (std::is_same<S, double>::value) Dc = T(0.25 * (rho(0, 0) + rho(1, 0) + rho(0, 1) + rho(1, 1)));
+    else Dc = T(0.25) * (T(rho(0, 0)) + T(rho(1, 0)) + T(rho(0, 1)) + T(rho(1, 1)));
     // GetCornerB (fields.F90:365-424): EdgeLRs of the dT1 faces along dT2 ...
 #pragma unroll
     for (int m = 0; m < 4; ++m) {
@@ -160,8 +167,8 @@ __global__ void __launch_bounds__(256, 2) k_edge_tile(Lay L, Par p, GridP g, Sta
     T l2, r2;
     getLR<T>(p.rmeth, pdmb, A2, B2, nB2, fA2, l2, r2);
     T bT2L = l2 * fA2, bT2R = r2 * fA2;
-    T xni = T(__ldg(&g.Teb[ED][0][c])), yni = T(__ldg(&g.Teb[ED][1][c]));
-    T xnj = T(__ldg(&g.Teb[ED][2][c])), ynj = T(__ldg(&g.Teb[ED][3][c]));
+    T xni = T(__ldg(&in.Teb[ED][0][c])), yni = T(__ldg(&in.Teb[ED][1][c]));
+    T xnj = T(__ldg(&in.Teb[ED][2][c])), ynj = T(__ldg(&in.Teb[ED][3][c]));
     T detT = T(1) / (xni * ynj - xnj * yni);
     T bT1 = T(0.5) * (bT1L + bT1R) / fA1;
     T bT2 = T(0.5) * (bT2L + bT2R) / fA2;
@@ -174,32 +181,37 @@ __global__ void __launch_bounds__(256, 2) k_edge_tile(Lay L, Par p, GridP g, Sta
     T vA = sqrt(b1 * b1 + b2 * b2) / sqrt(Dc);
     if (p.doBoris) { T Ca = T(p.Ca); vA = Ca * vA / sqrt(Ca * Ca + vA * vA); }
     vDiff = vDiff + vA;
-    double edg = __ldg(&g.edge[ED][c]);
+    double edg = double(__ldg(&in.edge[ED][c]));
     T lim = T(p.CFL * edg / sc->dt);
     vDiff = vDiff < lim ? vDiff : lim;
     T e = -(v1 * b2 - v2 * b1) + T(p.Vd0) * vDiff * Jd;
     Eout[c] = double(e) * edg;
 }
 
-template <typename T, int ED>
-static void launch_edge(Handle& h, const Reg& re, cudaStream_t st) {
+template <typename T, typename S, int ED>
+static void launch_edge(Handle& h, const EdgeSrc<S>& in, const Reg& re, cudaStream_t st) {
     using TL = ETile<ED>;
     dim3 grid((unsigned)((re.ni + TL::TI - 1) / TL::TI), (unsigned)((re.nj + TL::TJ - 1) / TL::TJ),
               (unsigned)((re.nk + TL::TK - 1) / TL::TK));
-    Vec3P Vf = {{h.Vf[0], h.Vf[1], h.Vf[2]}}, hbA = {{h.hbA[0], h.hbA[1], h.hbA[2]}}, nbA = {{h.nbA[0], h.nbA[1], h.nbA[2]}};
-    k_edge_tile<T, ED><<<grid, 256, sizeof(double) * TL::total, st>>>(h.L, h.p, h.gridP(), h.H, Vf, hbA, nbA, h.E[ED],
-                                                                       re, h.dScal);
+    k_edge_tile<T, S, ED><<<grid, 256, sizeof(S) * TL::total, st>>>(h.L, h.p, in, h.E[ED], re, h.dScal);
     h.launches++;
 }
 
-template <typename T, int ED>
+template <typename T, typename S, int ED>
 static void set_edge_smem() {
-    cudaFuncSetAttribute(k_edge_tile<T, ED>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         (int)(sizeof(double) * ETile<ED>::total));
+    cudaFuncSetAttribute(k_edge_tile<T, S, ED>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)(sizeof(S) * ETile<ED>::total));
 }
 void efield_kernels_init() {
-    set_edge_smem<double, 0>(); set_edge_smem<double, 1>(); set_edge_smem<double, 2>();
-    set_edge_smem<float, 0>(); set_edge_smem<float, 1>(); set_edge_smem<float, 2>();
+    set_edge_smem<double, double, 0>(); set_edge_smem<double, double, 1>(); set_edge_smem<double, double, 2>();
+    set_edge_smem<float, float, 0>(); set_edge_smem<float, float, 1>(); set_edge_smem<float, float, 2>();
+}
+
+template <typename T, typename S>
+static void launch_edge_dir(Handle& h, const EdgeSrc<S>& in, int eD, const Reg& re, cudaStream_t st) {
+    if (eD == 0) launch_edge<T, S, 0>(h, in, re, st);
+    else if (eD == 1) launch_edge<T, S, 1>(h, in, re, st);
+    else launch_edge<T, S, 2>(h, in, re, st);
 }
 
 // CalcElecField (fields.F90:70-232): E = 0, then for eD = I, J, K: Mom2Face along dT1, EMF on the edges
@@ -209,6 +221,27 @@ void enqueue_efield(Handle& h, const StateP& nS, cudaStream_t st) {
     cudaMemsetAsync(h.E[0], 0, sizeof(double) * L.E * 3, st);   // E planes are contiguous in the pool
     Vec3P Vf = {{h.Vf[0], h.Vf[1], h.Vf[2]}}, VdV = {{h.VdV[0], h.VdV[1], h.VdV[2]}};
     GridP g = h.gridP();
+    Vec3F Vf32{};
+    EdgeSrc<double> in64;
+    EdgeSrc<float> in32;
+    if (h.prec == PREC_FP32FLUX) {
+        const F32Planes& f = h.f32;
+        for (int x = 0; x < 3; ++x) { Vf32.v[x] = f.Vf[x]; in32.Vf[x] = f.Vf[x]; }
+        for (int d = 0; d < 3; ++d) {
+            in32.face[d] = f.face[d]; in32.hbA[d] = f.hbA[d]; in32.nbA[d] = f.nbA[d]; in32.edge[d] = f.edge[d];
+            for (int c = 0; c < 6; ++c) in32.Te[d][c] = f.Te[d][c];
+            for (int c = 0; c < 4; ++c) in32.Teb[d][c] = f.Teb[d][c];
+        }
+        in32.rho = f.rho;
+    } else {
+        for (int x = 0; x < 3; ++x) in64.Vf[x] = h.Vf[x];
+        for (int d = 0; d < 3; ++d) {
+            in64.face[d] = h.face[d]; in64.hbA[d] = h.hbA[d]; in64.nbA[d] = h.nbA[d]; in64.edge[d] = h.edge[d];
+            for (int c = 0; c < 6; ++c) in64.Te[d][c] = h.Te[d][3 + c];
+            for (int c = 0; c < 4; ++c) in64.Teb[d][c] = h.Teb[d][c];
+        }
+        in64.rho = h.H.gas[0];
+    }
     int is = L.is(), ie = L.ie(), js = L.js(), je = L.je(), ks = L.ks(), ke = L.ke();
     bool f32 = h.prec == PREC_FP32FLUX;
     for (int eD = 0; eD < 3; ++eD) {
@@ -228,11 +261,10 @@ void enqueue_efield(Handle& h, const StateP& nS, cudaStream_t st) {
             re = mkreg(is, ie + 1, js, je + 1, ks, ke);
         }
         dim3 bv = dT1 == 2 ? dim3(32, 1, 4) : dim3(32, 4, 1);
-        k_mom2face2<<<grid3(rv, bv), bv, 0, st>>>(L, g, VdV, Vf, rv, dT1);
+        k_mom2face2<<<grid3(rv, bv), bv, 0, st>>>(L, g, VdV, Vf, Vf32, rv, dT1);
         h.launches++;
-        if (eD == 0) { if (f32) launch_edge<float, 0>(h, re, st); else launch_edge<double, 0>(h, re, st); }
-        else if (eD == 1) { if (f32) launch_edge<float, 1>(h, re, st); else launch_edge<double, 1>(h, re, st); }
-        else { if (f32) launch_edge<float, 2>(h, re, st); else launch_edge<double, 2>(h, re, st); }
+        if (f32) launch_edge_dir<float, float>(h, in32, eD, re, st);
+        else launch_edge_dir<double, double>(h, in64, eD, re, st);
     }
 }
 

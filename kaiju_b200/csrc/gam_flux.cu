@@ -11,6 +11,7 @@
 // The arithmetic type T is double for the plain path and float for the FP32-flux path (staged
 // values are converted while they are copied in).
 #include <cstdio>
+#include <type_traits>
 #include "gam_common.cuh"
 #include "gam_kern.cuh"
 #include "gam_step.cuh"
@@ -22,14 +23,13 @@ constexpr int FR = 8;    // rows per tile
 
 template <int D> __host__ __device__ constexpr int rec_box() { return D == 0 ? (FL + 8) * FR : FL * (FR + 7); }
 template <int D> __host__ __device__ constexpr int lim_box() { return D == 0 ? (FL + 4) * FR : FL * (FR + 3); }
-template <typename T, int D> constexpr size_t flux_smem() { return sizeof(double) * (9 * rec_box<D>() + 8 * lim_box<D>()); }
+template <typename S, int D> constexpr size_t flux_smem() { return sizeof(S) * (9 * rec_box<D>() + 8 * lim_box<D>()); }
 
-template <typename T, int D, bool MHD>
-__global__ void __launch_bounds__(256, 2) k_flux_tile(Lay L, Par p, GridP g, StateP n, StateP h, PrimP Wh, PrimP Wn,
-                                                   FluxP F, Reg r) {
+template <typename T, typename S, int D, bool MHD>
+__global__ void __launch_bounds__(256, 2) k_flux_tile(Lay L, Par p, FluxSrc<S> in, StateP h, FluxP F, Reg r) {
     extern __shared__ __align__(16) unsigned char smraw[];
-    double* sRec = reinterpret_cast<double*>(smraw);   // staged as double, converted to T on use
-    double* sLim = sRec + 9 * rec_box<D>();
+    S* sRec = reinterpret_cast<S*>(smraw);   // staged in the storage type, converted to T on use
+    S* sLim = sRec + 9 * rec_box<D>();
     constexpr int RB = rec_box<D>(), LB = lim_box<D>();
     const int tid = threadIdx.x, lane = tid & 31, row = tid >> 5;
     const int i0 = r.i0 + blockIdx.x * FL;
@@ -39,28 +39,26 @@ __global__ void __launch_bounds__(256, 2) k_flux_tile(Lay L, Par p, GridP g, Sta
 
     // ---- stage the stencil footprint (rows of 32..40 doubles, one warp per row)
     const int warp = tid >> 5;
-    const double* const* limW = p.doLFMLim ? Wn.w : Wh.w;
-    const double* const* limB = p.doLFMLim ? n.b : h.b;
-    auto stage_rec = [&](double* dst, const double* src) {
-        if (D == 0) stage_rows(dst, src, L, i0 - 4, FL + 8, a0, FR, k, 1, warp, 8, lane);
-        else if (D == 1) stage_rows(dst, src, L, i0, FL, a0 - 4, FR + 7, k, 1, warp, 8, lane);
-        else stage_rows(dst, src, L, i0, FL, j, 1, a0 - 4, FR + 7, warp, 8, lane);
+    auto stage_rec = [&](S* dst, const S* src) {
+        if (D == 0) stage_rows<S>(dst, src, L, i0 - 4, FL + 8, a0, FR, k, 1, warp, 8, lane);
+        else if (D == 1) stage_rows<S>(dst, src, L, i0, FL, a0 - 4, FR + 7, k, 1, warp, 8, lane);
+        else stage_rows<S>(dst, src, L, i0, FL, j, 1, a0 - 4, FR + 7, warp, 8, lane);
     };
-    auto stage_lim = [&](double* dst, const double* src) {
-        if (D == 0) stage_rows(dst, src, L, i0 - 2, FL + 4, a0, FR, k, 1, warp, 8, lane);
-        else if (D == 1) stage_rows(dst, src, L, i0, FL, a0 - 2, FR + 3, k, 1, warp, 8, lane);
-        else stage_rows(dst, src, L, i0, FL, j, 1, a0 - 2, FR + 3, warp, 8, lane);
+    auto stage_lim = [&](S* dst, const S* src) {
+        if (D == 0) stage_rows<S>(dst, src, L, i0 - 2, FL + 4, a0, FR, k, 1, warp, 8, lane);
+        else if (D == 1) stage_rows<S>(dst, src, L, i0, FL, a0 - 2, FR + 3, k, 1, warp, 8, lane);
+        else stage_rows<S>(dst, src, L, i0, FL, j, 1, a0 - 2, FR + 3, warp, 8, lane);
     };
 #pragma unroll
-    for (int q = 0; q < 5; ++q) stage_rec(sRec + q * RB, Wh.w[q]);
-    stage_rec(sRec + 5 * RB, g.volume);
+    for (int q = 0; q < 5; ++q) stage_rec(sRec + q * RB, in.W[q]);
+    stage_rec(sRec + 5 * RB, in.vol);
 #pragma unroll
-    for (int q = 0; q < 5; ++q) stage_lim(sLim + q * LB, limW[q]);
+    for (int q = 0; q < 5; ++q) stage_lim(sLim + q * LB, in.Wl[q]);
     if (MHD) {
 #pragma unroll
         for (int x = 0; x < 3; ++x) {
-            stage_rec(sRec + (6 + x) * RB, h.b[x]);
-            stage_lim(sLim + (5 + x) * LB, limB[x]);
+            stage_rec(sRec + (6 + x) * RB, in.B[x]);
+            stage_lim(sLim + (5 + x) * LB, in.Bl[x]);
         }
     }
     cp_async_wait_all();
@@ -89,8 +87,8 @@ __global__ void __launch_bounds__(256, 2) k_flux_tile(Lay L, Par p, GridP g, Sta
     }
     T Tf[9];
 #pragma unroll
-    for (int q = 0; q < 9; ++q) Tf[q] = T(__ldg(&g.Tf[D][q][c]));
-    double faB = __ldg(&g.face[D][c]);
+    for (int q = 0; q < 9; ++q) Tf[q] = T(__ldg(&in.Tf[D][q][c]));
+    double faB = double(__ldg(&in.face[D][c]));
     T VaD = T(0), bbD = T(0);
     if (MHD) {
         T BL[3], BR[3];
@@ -103,7 +101,10 @@ __global__ void __launch_bounds__(256, 2) k_flux_tile(Lay L, Par p, GridP g, Sta
             for (int m = 0; m < 4; ++m) nQ[m] = T(sLim[(5 + x) * LB + lo(m)]);
             getLR<T>(p.rmeth, pdmb, Vol, Q, nQ, Vi, BL[x], BR[x]);
         }
-        T Bn = T(__ldg(&h.mf[D][c]) / faB);
+        // FP64: the half-state flux over the area (stress.F90:301); FP32: the stored flux/area
+        T Bn;
+        if constexpr (std::is_same<S, double>::value) Bn = T(__ldg(&in.bn[D][c]) / faB);
+        else Bn = T(__ldg(&in.bn[D][c]));
         T mF[3] = {T(0), T(0), T(0)};
         magKin<T>(p, T(-1), WL, BL, Bn, Tf, mF, bbD, VaD);
         magKin<T>(p, T(1), WR, BR, Bn, Tf, mF, bbD, VaD);
@@ -139,46 +140,66 @@ __global__ void __launch_bounds__(256, 2) k_flux_tile(Lay L, Par p, GridP g, Sta
     for (int v = 0; v < 5; ++v) F.g[v][c] = faB * double(gF[v]);
 }
 
-template <typename T, int D>
-static void launch_flux_dir(Handle& h, const StateP& nS, const Reg& r, cudaStream_t st) {
+template <typename T, typename S, int D>
+static void launch_flux_dir(Handle& h, const FluxSrc<S>& in, const Reg& r, cudaStream_t st) {
     const Par& p = h.p;
-    PrimP Wh, Wn;
-    for (int v = 0; v < 5; ++v) { Wh.w[v] = h.Wh[v]; Wn.w[v] = h.Wn[v]; }
     FluxP F;
     for (int v = 0; v < 5; ++v) F.g[v] = h.gflx[D][v];
     for (int x = 0; x < 3; ++x) F.m[x] = h.mflx[D][x];
     dim3 grid((unsigned)((r.ni + FL - 1) / FL), 0, 0);
     if (D == 2) { grid.y = (unsigned)((r.nk + FR - 1) / FR); grid.z = (unsigned)r.nj; }
     else { grid.y = (unsigned)((r.nj + FR - 1) / FR); grid.z = (unsigned)r.nk; }
-    if (p.doMHD) k_flux_tile<T, D, true><<<grid, 256, flux_smem<T, D>(), st>>>(h.L, p, h.gridP(), nS, h.H, Wh, Wn, F, r);
-    else k_flux_tile<T, D, false><<<grid, 256, flux_smem<T, D>(), st>>>(h.L, p, h.gridP(), nS, h.H, Wh, Wn, F, r);
+    if (p.doMHD) k_flux_tile<T, S, D, true><<<grid, 256, flux_smem<S, D>(), st>>>(h.L, p, in, h.H, F, r);
+    else k_flux_tile<T, S, D, false><<<grid, 256, flux_smem<S, D>(), st>>>(h.L, p, in, h.H, F, r);
     h.launches++;
 }
 
-template <typename T, int D>
+template <typename T, typename S, int D>
 static void set_flux_smem() {
-    cudaFuncSetAttribute(k_flux_tile<T, D, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)flux_smem<T, D>());
-    cudaFuncSetAttribute(k_flux_tile<T, D, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)flux_smem<T, D>());
+    cudaFuncSetAttribute(k_flux_tile<T, S, D, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)flux_smem<S, D>());
+    cudaFuncSetAttribute(k_flux_tile<T, S, D, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)flux_smem<S, D>());
 }
 void flux_kernels_init() {
-    set_flux_smem<double, 0>(); set_flux_smem<double, 1>(); set_flux_smem<double, 2>();
-    set_flux_smem<float, 0>(); set_flux_smem<float, 1>(); set_flux_smem<float, 2>();
+    set_flux_smem<double, double, 0>(); set_flux_smem<double, double, 1>(); set_flux_smem<double, double, 2>();
+    set_flux_smem<float, float, 0>(); set_flux_smem<float, float, 1>(); set_flux_smem<float, float, 2>();
 }
 
 // CalcStress flux loop (stress.F90:84-128): I, J and (unless 2.5D) K interfaces
-void enqueue_fluxes(Handle& h, const StateP& nS, cudaStream_t st) {
+template <typename T, typename S>
+static void fluxes_all(Handle& h, const FluxSrc<S>& in, cudaStream_t st) {
     const Lay& L = h.L;
     int is = L.is(), ie = L.ie(), js = L.js(), je = L.je(), ks = L.ks(), ke = L.ke();
     if (h.p.do25D) ke = ks;
-    Reg rI = mkreg(is, ie + 1, js, je, ks, ke), rJ = mkreg(is, ie, js, je + 1, ks, ke), rK = mkreg(is, ie, js, je, ks, ke + 1);
+    launch_flux_dir<T, S, 0>(h, in, mkreg(is, ie + 1, js, je, ks, ke), st);
+    launch_flux_dir<T, S, 1>(h, in, mkreg(is, ie, js, je + 1, ks, ke), st);
+    if (!h.p.do25D) launch_flux_dir<T, S, 2>(h, in, mkreg(is, ie, js, je, ks, ke + 1), st);
+}
+
+void enqueue_fluxes(Handle& h, const StateP& nS, cudaStream_t st) {
+    const bool lfm = h.p.doLFMLim != 0;
     if (h.prec == PREC_FP32FLUX) {
-        launch_flux_dir<float, 0>(h, nS, rI, st);
-        launch_flux_dir<float, 1>(h, nS, rJ, st);
-        if (!h.p.do25D) launch_flux_dir<float, 2>(h, nS, rK, st);
+        const F32Planes& f = h.f32;
+        FluxSrc<float> in;
+        for (int v = 0; v < 5; ++v) { in.W[v] = f.Wh[v]; in.Wl[v] = lfm ? f.Wn[v] : f.Wh[v]; }
+        for (int x = 0; x < 3; ++x) { in.B[x] = f.hb[x]; in.Bl[x] = lfm ? f.nb[x] : f.hb[x]; }
+        in.vol = f.volume;
+        for (int d = 0; d < 3; ++d) {
+            for (int q = 0; q < 9; ++q) in.Tf[d][q] = f.Tf[d][q];
+            in.face[d] = f.face[d];
+            in.bn[d] = f.hbA[d];
+        }
+        fluxes_all<float, float>(h, in, st);
     } else {
-        launch_flux_dir<double, 0>(h, nS, rI, st);
-        launch_flux_dir<double, 1>(h, nS, rJ, st);
-        if (!h.p.do25D) launch_flux_dir<double, 2>(h, nS, rK, st);
+        FluxSrc<double> in;
+        for (int v = 0; v < 5; ++v) { in.W[v] = h.Wh[v]; in.Wl[v] = lfm ? h.Wn[v] : h.Wh[v]; }
+        for (int x = 0; x < 3; ++x) { in.B[x] = h.H.b[x]; in.Bl[x] = lfm ? nS.b[x] : h.H.b[x]; }
+        in.vol = h.volume;
+        for (int d = 0; d < 3; ++d) {
+            for (int q = 0; q < 9; ++q) in.Tf[d][q] = h.Tf[d][q];
+            in.face[d] = h.face[d];
+            in.bn[d] = h.H.mf[d];
+        }
+        fluxes_all<double, double>(h, in, st);
     }
 }
 

@@ -35,6 +35,28 @@ static inline Reg mkreg(int i0, int i1, int j0, int j1, int k0, int k1) {
 static inline unsigned nblk(long long n, int b) { return (unsigned)((n + b - 1) / b); }
 
 struct PrimP { double* w[5]; };
+// Inputs of the flux kernels in storage type S (double planes for FP64, float copies for FP32-flux)
+template <typename S> struct FluxSrc {
+    const S* W[5];      // half-state primitives (reconstruction)
+    const S* Wl[5];     // limiter primitives (state n, or the half state without LFM limiting)
+    const S* B[3];      // half-state B
+    const S* Bl[3];     // limiter B
+    const S* vol;
+    const S* Tf[3][9];
+    const S* face[3];
+    const S* bn[3];     // normal field on the face: half-state flux / area
+};
+// Inputs of the edge kernels
+template <typename S> struct EdgeSrc {
+    const S* Vf[3];
+    const S* face[3];
+    const S* hbA[3];
+    const S* nbA[3];
+    const S* rho;       // half-state density
+    const S* Te[3][6];  // T1 (x,y,z), T2 (x,y,z) of each edge direction
+    const S* Teb[3][4];
+    const S* edge[3];
+};
 struct Vec3P { double* v[3]; };
 struct FluxP { double* g[5]; double* m[3]; };
 
@@ -124,22 +146,31 @@ __device__ __forceinline__ void stage_box_async(double* dst, const double* __res
     }
 }
 
+__device__ __forceinline__ void cp_async4(void* smem, const void* gmem) {
+    unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(sa), "l"(gmem) : "memory");
+}
+template <typename S> __device__ __forceinline__ void cp_async_elem(S* smem, const S* gmem);
+template <> __device__ __forceinline__ void cp_async_elem<double>(double* smem, const double* gmem) { cp_async8(smem, gmem); }
+template <> __device__ __forceinline__ void cp_async_elem<float>(float* smem, const float* gmem) { cp_async4(smem, gmem); }
+
 // Row-wise staging: the box [gi0,gi0+ni) x [gj0,gj0+nj) x [gk0,gk0+nk) (absolute pencil indices) is
 // copied row by row, one warp per row, lanes along i, one cp.async per element; each row's address is
 // computed once. Out-of-range elements are zero.
-__device__ __forceinline__ void stage_rows(double* dst, const double* __restrict__ src, const Lay& L, int gi0, int ni,
+template <typename S>
+__device__ __forceinline__ void stage_rows(S* dst, const S* __restrict__ src, const Lay& L, int gi0, int ni,
                                            int gj0, int nj, int gk0, int nk, int warp, int nwarp, int lane) {
     const int nrow = nj * nk;
     for (int rr = warp; rr < nrow; rr += nwarp) {
         int b = rr % nj, c = rr / nj;
         int j = gj0 + b, k = gk0 + c;
-        double* drow = dst + rr * ni;
+        S* drow = dst + rr * ni;
         bool ok = (j >= 0) && (j <= L.Nj) && (k >= 0) && (k <= L.Nk);
-        const double* srow = src + L.at(0, ok ? j : 0, ok ? k : 0);
+        const S* srow = src + L.at(0, ok ? j : 0, ok ? k : 0);
         for (int a = lane; a < ni; a += 32) {
             int i = gi0 + a;
-            if (ok && i >= 0 && i <= L.Ni) cp_async8(drow + a, srow + i);
-            else drow[a] = 0.0;
+            if (ok && i >= 0 && i <= L.Ni) cp_async_elem<S>(drow + a, srow + i);
+            else drow[a] = S(0);
         }
     }
 }

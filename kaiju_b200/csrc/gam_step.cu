@@ -28,8 +28,11 @@ __global__ void k_step_begin(Scal* sc) {
 // Predictor magFlux part (mhdgroup.F90:466-488): AB2 on every face element, ghosts included. Also the
 // per-face values EdgeLRs divides out at every stencil point (fields.F90:335-336): flux/max(area,TINY)
 // for the half state (reconstruction) and for the limiting state.
+struct F32FaceOut { float* hbA[3]; float* nbA[3]; };
+struct F32CellOut { float* Wh[5]; float* Wn[5]; float* hb[3]; float* nb[3]; float* rho; };
+
 __global__ void k_predict_faces(long long E, Par p, GridP g, Vec3P mf, Vec3P omf, Vec3P hmf, Vec3P hbA, Vec3P nbA,
-                                const Scal* sc) {
+                                F32FaceOut o, const Scal* sc) {
     long long l = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (l >= E) return;
     double pdt = sc->pdt, odt = sc->odt;
@@ -40,15 +43,16 @@ __global__ void k_predict_faces(long long E, Par p, GridP g, Vec3P mf, Vec3P omf
         double H = Q + pdt * dQ;
         hmf.v[c][l] = H;
         double a = dmax(g.face[c][l], TINY);
-        hbA.v[c][l] = H / a;
-        nbA.v[c][l] = (p.doLFMLim ? Q : H) / a;
+        double hb = H / a, nb = (p.doLFMLim ? Q : H) / a;
+        if (o.hbA[0]) { o.hbA[c][l] = float(hb); o.nbA[c][l] = float(nb); }
+        else { hbA.v[c][l] = hb; nbA.v[c][l] = nb; }
     }
 }
 
 // bFlux2Fld of the half state + PredictCell (mhdgroup.F90:492-518, 529-563) on every cell, plus the
 // BlockCon2Prim primitives of the half state and of state n used by the interface reconstruction.
 __global__ void k_predict_cells(Lay L, Par p, GridP g, StateP n, StateP o, StateP h, PrimP Wh, PrimP Wn, Vec3P VdV,
-                                const Scal* sc) {
+                                F32CellOut f, const Scal* sc) {
     Reg r = {0, L.Ni, 0, L.Nj, 0, L.Nk};
     int i, j, k;
     if (!reg_ijk(r, blockIdx.x * (long long)blockDim.x + threadIdx.x, i, j, k)) return;
@@ -77,6 +81,18 @@ __global__ void k_predict_cells(Lay L, Par p, GridP g, StateP n, StateP o, State
         VdV.v[2][c] = vol * pQ[3] / den;
     }
     double w[5];
+    if (f.Wh[0]) {   // FP32-flux path: float copies of every stencil input
+        blockC2P(p, pQ, w);
+#pragma unroll
+        for (int v = 0; v < 5; ++v) f.Wh[v][c] = float(w[v]);
+        blockC2P(p, Q, w);
+#pragma unroll
+        for (int v = 0; v < 5; ++v) f.Wn[v][c] = float(w[v]);
+#pragma unroll
+        for (int x = 0; x < 3; ++x) { f.hb[x][c] = float(B[x]); f.nb[x][c] = float(n.b[x][c]); }
+        f.rho[c] = float(pQ[0]);
+        return;
+    }
     blockC2P(p, pQ, w);
 #pragma unroll
     for (int v = 0; v < 5; ++v) Wh.w[v][c] = w[v];
@@ -532,6 +548,46 @@ void launch_calcdt(Handle& h, const StateP& s, int mode, cudaStream_t st) {
     h.launches += 2;
 }
 
+__global__ void k_to_f32(const double* src, float* dst, long long n) {
+    long long l = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (l < n) dst[l] = float(src[l]);
+}
+
+int ensure_f32(Handle& h) {
+    if (h.f32pool) return 0;
+    const long long E = h.L.E;
+    const int nplanes = 26 + 64;
+    if (cudaMalloc(&h.f32pool, sizeof(float) * E * nplanes) != cudaSuccess) return 3;
+    cudaMemsetAsync(h.f32pool, 0, sizeof(float) * E * nplanes, h.stream);
+    float* q = h.f32pool;
+    auto take = [&]() { float* r = q; q += E; return r; };
+    F32Planes& f = h.f32;
+    for (int v = 0; v < 5; ++v) f.Wh[v] = take();
+    for (int v = 0; v < 5; ++v) f.Wn[v] = take();
+    for (int x = 0; x < 3; ++x) f.hb[x] = take();
+    for (int x = 0; x < 3; ++x) f.nb[x] = take();
+    for (int x = 0; x < 3; ++x) f.hbA[x] = take();
+    for (int x = 0; x < 3; ++x) f.nbA[x] = take();
+    for (int x = 0; x < 3; ++x) f.Vf[x] = take();
+    f.rho = take();
+    f.volume = take();
+    for (int d = 0; d < 3; ++d) f.face[d] = take();
+    for (int d = 0; d < 3; ++d) f.edge[d] = take();
+    for (int d = 0; d < 3; ++d) for (int c = 0; c < 9; ++c) f.Tf[d][c] = take();
+    for (int d = 0; d < 3; ++d) for (int c = 0; c < 6; ++c) f.Te[d][c] = take();
+    for (int d = 0; d < 3; ++d) for (int c = 0; c < 4; ++c) f.Teb[d][c] = take();
+    auto cv = [&](const double* s_, float* d_) { k_to_f32<<<nblk(E, 256), 256, 0, h.stream>>>(s_, d_, E); h.launches++; };
+    cv(h.volume, f.volume);
+    for (int d = 0; d < 3; ++d) {
+        cv(h.face[d], f.face[d]);
+        cv(h.edge[d], f.edge[d]);
+        for (int c = 0; c < 9; ++c) cv(h.Tf[d][c], f.Tf[d][c]);
+        for (int c = 0; c < 6; ++c) cv(h.Te[d][3 + c], f.Te[d][c]);
+        for (int c = 0; c < 4; ++c) cv(h.Teb[d][c], f.Teb[d][c]);
+    }
+    return cudaGetLastError() == cudaSuccess ? 0 : 3;
+}
+
 int kernels_per_step(const Handle& h) {
     int n = 1 + 1;                      // begin, predict cells
     if (h.p.doMHD) n += 1 + 1 + 6;      // predict faces, E memset (counted), 3x(mom2face + edge)
@@ -561,14 +617,23 @@ int step_enqueue(Handle& h, int cur, cudaEvent_t* ev) {
         Vec3P mf = {{nS.mf[0], nS.mf[1], nS.mf[2]}}, omf = {{oS.mf[0], oS.mf[1], oS.mf[2]}},
               hmf = {{h.H.mf[0], h.H.mf[1], h.H.mf[2]}}, hbA = {{h.hbA[0], h.hbA[1], h.hbA[2]}},
               nbA = {{h.nbA[0], h.nbA[1], h.nbA[2]}};
-        k_predict_faces<<<nblk(L.E, 256), 256, 0, st>>>(L.E, p, g, mf, omf, hmf, hbA, nbA, h.dScal);
+        F32FaceOut fo{};
+        if (h.prec == PREC_FP32FLUX)
+            for (int x = 0; x < 3; ++x) { fo.hbA[x] = h.f32.hbA[x]; fo.nbA[x] = h.f32.nbA[x]; }
+        k_predict_faces<<<nblk(L.E, 256), 256, 0, st>>>(L.E, p, g, mf, omf, hmf, hbA, nbA, fo, h.dScal);
         h.launches++;
     }
     PrimP Wh, Wn;
     for (int v = 0; v < 5; ++v) { Wh.w[v] = h.Wh[v]; Wn.w[v] = h.Wn[v]; }
     long long ncell = (long long)L.Ni * L.Nj * L.Nk;
     Vec3P VdV = {{h.VdV[0], h.VdV[1], h.VdV[2]}};
-    k_predict_cells<<<nblk(ncell, TPB), TPB, 0, st>>>(L, p, g, nS, oS, h.H, Wh, Wn, VdV, h.dScal);
+    F32CellOut fc{};
+    if (h.prec == PREC_FP32FLUX) {
+        for (int v = 0; v < 5; ++v) { fc.Wh[v] = h.f32.Wh[v]; fc.Wn[v] = h.f32.Wn[v]; }
+        for (int x = 0; x < 3; ++x) { fc.hb[x] = h.f32.hb[x]; fc.nb[x] = h.f32.nb[x]; }
+        fc.rho = h.f32.rho;
+    }
+    k_predict_cells<<<nblk(ncell, TPB), TPB, 0, st>>>(L, p, g, nS, oS, h.H, Wh, Wn, VdV, fc, h.dScal);
     h.launches += 2;
     mark(PH_EFIELD);
     enqueue_hot(h, nS, st, ev);

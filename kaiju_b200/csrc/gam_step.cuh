@@ -8,6 +8,13 @@ namespace gam {
 
 enum Prec { PREC_FP64 = 0, PREC_FP32FLUX = 1 };
 
+// float copies used by the FP32-flux path: stencil inputs written by the predictor each step and
+// metric planes converted once
+struct F32Planes {
+    float* Wh[5]; float* Wn[5]; float* hb[3]; float* nb[3]; float* hbA[3]; float* nbA[3]; float* Vf[3]; float* rho;
+    float* volume; float* face[3]; float* edge[3]; float* Tf[3][9]; float* Te[3][6]; float* Teb[3][4];
+};
+
 struct Handle {
     Lay L;
     Par p;
@@ -37,8 +44,9 @@ struct Handle {
     double* volume; double* xyzcc[3]; double* xfc[3][3]; double* di; double* dj; double* dk;
     double* face[3]; double* edge[3]; double* Tf[3][9]; double* Te[3][9]; double* Teb[3][4];
     double* xyz[3];       // corners (only kept when the grid was built on the device)
-    // FP32 copies for the FP32-flux mode
+    // FP32 copies for the FP32-flux mode (allocated on first use)
     float* f32pool = nullptr;
+    F32Planes f32{};
 
     Scal* dScal = nullptr;   // device scalars
     Scal* hScal = nullptr;   // pinned host mirror
@@ -69,5 +77,7 @@ void flux_kernels_init();
 // E field of all edge directions (gam_efield.cu): Mom2Face + tiled EMF
 void enqueue_efield(Handle& h, const StateP& nS, cudaStream_t st);
 void efield_kernels_init();
+// allocate the float planes and convert the metrics (first switch to GAM_FP32FLUX)
+int ensure_f32(Handle& h);
 
 }  // namespace gam
