@@ -238,6 +238,20 @@ __global__ void k_update_gas(Lay L, Par p, StateP nS, StateP oNew, PrimP dGH, Ve
     for (int v = 0; v < 5; ++v) oNew.gas[v][c] = U[v];
 }
 
+// bFlux2Fld after EnforceBCs restricted to ghost cells: outside 2.5D the BCs only rewrite faces of
+// ghost cells (outer I/J/K faces from ie+2/je+2/ke+2 on, inner ones below is/js/ks), so active cells
+// keep the B of the update.
+__global__ void k_bflux2fld_ghost(Lay L, GridP g, StateP s) {
+    Reg r = {0, L.Ni, 0, L.Nj, 0, L.Nk};
+    int i, j, k;
+    if (!reg_ijk(r, blockIdx.x * (long long)blockDim.x + threadIdx.x, i, j, k)) return;
+    if (i >= L.is() && i <= L.ie() && j >= L.js() && j <= L.je() && k >= L.ks() && k <= L.ke()) return;
+    long long c = L.at(i, j, k);
+    double B[3];
+    cellBxyz(L, g, s.mf, c, B);
+    s.b[0][c] = B[0]; s.b[1][c] = B[1]; s.b[2][c] = B[2];
+}
+
 // ================================================================================ timestep
 // CellDT (gridutils.F90:49-106) over the dt domain (one ghost layer at physical boundaries), min-reduced
 __global__ void k_calcdt(Lay L, Par p, GridP g, StateP s, Scal* sc) {
@@ -662,7 +676,11 @@ int step_enqueue(Handle& h, int cur, cudaEvent_t* ev) {
     launch_calcdt(h, oS, 0, st);
     mark(PH_BCS);
     launch_bcs(h, oS, st);
-    launch_bflux2fld(h, oS, st);
+    if (p.do25D) launch_bflux2fld(h, oS, st);   // the 2.5D K replication rewrites an active cell's upper face
+    else {
+        k_bflux2fld_ghost<<<nblk(ncell, TPB), TPB, 0, st>>>(L, g, oS);
+        h.launches++;
+    }
     mark(NPHASE);
     return (int)cudaGetLastError();
 }
