@@ -54,7 +54,9 @@ typedef struct {
     double t, tFin, dt, dt0;   /* Model%t, tFin, dt, dt0                                 */
     int ts;                    /* Model%ts                                              */
     int doMHD, doBoris, do25D, doLFMLim, rmeth, fixedTimestep;
-    /* options the device path does not run; nonzero -> GAM_ERR_UNSUPPORTED */
+    /* doBackground: a background field B0 (gam_grid_c fcB0..dpB0) enters the fluxes, E field, CalcDT and
+     * Boris update (src/gamera/background.F90). The other options are not run on the device;
+     * nonzero -> GAM_ERR_UNSUPPORTED */
     int doBackground, doGrav, doResistive, doRing, doMultiF, doAB3, nSpc, hasHooks;
     int bc[6];                 /* GAM_BC_* per face                                      */
 } gam_model_c;
@@ -72,6 +74,12 @@ typedef struct {
     const double* Tf;      /* (Ni+1,Nj+1,Nk+1,9,3)    face triads               */
     const double* Te;      /* (Ni+1,Nj+1,Nk+1,9,3)    edge triads               */
     const double* Teb;     /* (Ni+1,Nj+1,Nk+1,4,3)    edge B transforms         */
+    /* background field from AddB0 (src/gamera/background.F90:20-167); NULL unless Model%doBackground */
+    const double* fcB0;    /* (Ni,Nj,Nk,3,3)          face-averaged B0 [xyz, face dir]   */
+    const double* edgB0;   /* (Ni,Nj,Nk,2,3)          edge-frame B0 [tangent, edge dir]  */
+    const double* B0;      /* (Ni,Nj,Nk,3)            cell-averaged B0                   */
+    const double* bFlux0;  /* (Ni,Nj,Nk,3)            B0 flux through the lower faces    */
+    const double* dpB0;    /* (Ni,Nj,Nk,3)            background momentum source          */
 } gam_grid_c;
 
 typedef struct {
@@ -99,6 +107,19 @@ int gam_gpu_create(gam_gpu_t** h, const gam_model_c* m, const gam_grid_c* g, con
 #define GAM_IC_OT2D 0
 #define GAM_IC_BW 1
 int gam_gpu_create_from_corners(gam_gpu_t** h, const gam_model_c* m, const double* xyz, int ic);
+
+/* gam_gpu_create_from_corners with a background field (Model%doBackground must be set): AddB0
+ * (src/gamera/background.F90:20-167) runs on the device after the IC, as CalcGridInfo does
+ * (init.F90:180-184), with a built-in Model%B0:
+ *   GAM_B0_UNIFORM: B0 = (par[0], par[1], par[2]), the blast wave's BlastB0 (prob.F90:261-269). With
+ *                   GAM_IC_BW it replaces the blast field (prob/doBack: residual field starts at 0).
+ *   GAM_B0_DIPOLE:  B0 = 3 (m.r) r/|r|^5 - m/|r|^3, m = (0, 0, par[3]), r measured from
+ *                   (par[0], par[1], par[2]) (Dipole, apps/msphutils.F90:534-551, centred at the origin
+ *                   there). */
+#define GAM_B0_UNIFORM 1
+#define GAM_B0_DIPOLE 2
+int gam_gpu_create_from_corners_b0(gam_gpu_t** h, const gam_model_c* m, const double* xyz, int ic, int b0Kind,
+                                   const double* b0Par);
 
 /* One stepGamera (src/gamera/gamapp.F90:73-94): AdvanceMHD, ts/t update, CalcDT, EnforceBCs,
  * bFlux2Fld. Outputs (may be NULL): the new Model%dt, Model%ts, Model%t. */

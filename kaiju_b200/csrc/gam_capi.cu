@@ -77,9 +77,27 @@ int d2h_planes(gam_gpu* G, double* const* planes, int np, double* host, Ext e) {
     return GAM_OK;
 }
 
+// Grid_T background arrays (Fortran layout, cell-sized) into the background planes
+int upload_background(gam_gpu* G, const double* fcB0, const double* edgB0, const double* B0, const double* bFlux0,
+                      const double* dpB0) {
+    Handle& h = G->h;
+    if (!h.bgpool) return GAM_ERR_ARG;
+    Ext ce = cellExt(h.L);
+    double* pl[9];
+    for (int d = 0; d < 3; ++d) for (int x = 0; x < 3; ++x) pl[d * 3 + x] = h.fcB0[d][x];
+    int rc = h2d_planes(G, pl, 9, fcB0, ce);
+    for (int d = 0; d < 3; ++d) for (int c = 0; c < 2; ++c) pl[d * 2 + c] = h.edgB0[d][c];
+    if (!rc) rc = h2d_planes(G, pl, 6, edgB0, ce);
+    if (!rc) rc = h2d_planes(G, h.B0, 3, B0, ce);
+    if (!rc) rc = h2d_planes(G, h.bFlux0, 3, bFlux0, ce);
+    if (!rc) rc = h2d_planes(G, h.dpB0, 3, dpB0, ce);
+    if (!rc) refresh_f32_background(h);
+    return rc;
+}
+
 int check_model(const gam_model_c* m) {
     if (!m) return GAM_ERR_ARG;
-    if (m->doBackground || m->doGrav || m->doResistive || m->doRing || m->doMultiF || m->doAB3 || m->nSpc != 0 ||
+    if (m->doGrav || m->doResistive || m->doRing || m->doMultiF || m->doAB3 || m->nSpc != 0 ||
         m->hasHooks)
         return GAM_ERR_UNSUPPORTED;
     if (m->nG != 4 || m->Nip < 16 || m->Njp < 1 || m->Nkp < 1) return GAM_ERR_ARG;
@@ -103,6 +121,7 @@ int alloc_handle(gam_gpu* G, const gam_model_c* m) {
     p.Ca = m->Ca; p.dFloor = m->dFloor; p.pFloor = m->pFloor; p.limDT0 = m->limDT0; p.tFin = m->tFin;
     p.doMHD = m->doMHD; p.doBoris = m->doBoris; p.do25D = m->do25D; p.doLFMLim = m->doLFMLim; p.rmeth = m->rmeth;
     p.fixedTimestep = m->fixedTimestep;
+    p.doBackground = m->doBackground ? 1 : 0;
     for (int n = 0; n < 6; ++n) p.bc[n] = m->bc[n];
 
     CK(cudaGetDevice(&h.device));
@@ -146,6 +165,17 @@ int alloc_handle(gam_gpu* G, const gam_model_c* m) {
     for (int d = 0; d < 3; ++d) for (int c = 0; c < 4; ++c) h.Teb[d][c] = take();
     for (int x = 0; x < 3; ++x) h.xyz[x] = take();
     if ((size_t)(q - h.pool) != (size_t)L.E * planes) return GAM_ERR_ARG;
+    if (p.doBackground) {   // fcB0 (9), edgB0 (6), B0, bFlux0, dpB0 (3 each)
+        const size_t bgPlanes = 24;
+        CK(cudaMalloc(&h.bgpool, sizeof(double) * L.E * bgPlanes));
+        CK(cudaMemsetAsync(h.bgpool, 0, sizeof(double) * L.E * bgPlanes, h.stream));
+        q = h.bgpool;
+        for (int d = 0; d < 3; ++d) for (int x = 0; x < 3; ++x) h.fcB0[d][x] = take();
+        for (int d = 0; d < 3; ++d) for (int c = 0; c < 2; ++c) h.edgB0[d][c] = take();
+        for (int x = 0; x < 3; ++x) h.B0[x] = take();
+        for (int d = 0; d < 3; ++d) h.bFlux0[d] = take();
+        for (int x = 0; x < 3; ++x) h.dpB0[x] = take();
+    }
 
     Ext fe = faceExt(L);
     CK(cudaMalloc(&G->stage, sizeof(double) * fe.n()));
@@ -256,6 +286,7 @@ int gam_gpu_create(gam_gpu_t** out, const gam_model_c* m, const gam_grid_c* g, c
     if (!g->xyzcc || !g->xfc || !g->di || !g->dj || !g->dk || !g->volume || !g->face || !g->edge || !g->Tf ||
         !g->Te || !g->Teb)
         return GAM_ERR_ARG;
+    if (m->doBackground && (!g->fcB0 || !g->edgB0 || !g->B0 || !g->bFlux0 || !g->dpB0)) return GAM_ERR_ARG;
     gam_gpu* G = new (std::nothrow) gam_gpu();
     if (!G) return GAM_ERR_ARG;
     rc = alloc_handle(G, m);
@@ -275,6 +306,7 @@ int gam_gpu_create(gam_gpu_t** out, const gam_model_c* m, const gam_grid_c* g, c
     if (!rc) { for (int d = 0; d < 3; ++d) for (int c = 0; c < 9; ++c) pl[d * 9 + c] = h.Tf[d][c]; rc = h2d_planes(G, pl, 27, g->Tf, fe); }
     if (!rc) { for (int d = 0; d < 3; ++d) for (int c = 0; c < 9; ++c) pl[d * 9 + c] = h.Te[d][c]; rc = h2d_planes(G, pl, 27, g->Te, fe); }
     if (!rc) { for (int d = 0; d < 3; ++d) for (int c = 0; c < 4; ++c) pl[d * 4 + c] = h.Teb[d][c]; rc = h2d_planes(G, pl, 12, g->Teb, fe); }
+    if (!rc && m->doBackground) rc = upload_background(G, g->fcB0, g->edgB0, g->B0, g->bFlux0, g->dpB0);
     if (rc) { gam_gpu_destroy(G); return rc; }
     rc = gam_gpu_sync_to_device(G, GAM_SYNC_STATE | GAM_SYNC_OSTATE, gas, magflux, bxyz, ogas, omagflux, obxyz, time,
                                 otime);
@@ -283,13 +315,14 @@ int gam_gpu_create(gam_gpu_t** out, const gam_model_c* m, const gam_grid_c* g, c
     return GAM_OK;
 }
 
-int gam_gpu_create_from_corners(gam_gpu_t** out, const gam_model_c* m, const double* xyz, int ic) {
+static int create_from_corners(gam_gpu_t** out, const gam_model_c* m, const double* xyz, int ic, const BgSpec* bg) {
     if (!out || !xyz) return GAM_ERR_ARG;
     *out = nullptr;
     int rc = check_model(m);
     if (rc) return rc;
     if (ic != GAM_IC_OT2D && ic != GAM_IC_BW) return GAM_ERR_ARG;
     if ((m->Nip % 8) != 0) return GAM_ERR_ARG;   // Corners2Grid divisibility check (init.F90:830-834)
+    if ((bg != nullptr) != (m->doBackground != 0)) return GAM_ERR_ARG;
     gam_gpu* G = new (std::nothrow) gam_gpu();
     if (!G) return GAM_ERR_ARG;
     rc = alloc_handle(G, m);
@@ -301,11 +334,24 @@ int gam_gpu_create_from_corners(gam_gpu_t** out, const gam_model_c* m, const dou
     h.hScal->otime = m->t;
     rc = upload_scalars(G);
     if (!rc && init_grid_from_corners(h) != 0) rc = GAM_ERR_CUDA;
-    if (!rc && init_problem(h, ic) != 0) rc = GAM_ERR_CUDA;
+    if (!rc && init_problem(h, ic, bg) != 0) rc = GAM_ERR_CUDA;
     if (!rc) rc = download_scalars(G);
     if (rc) { gam_gpu_destroy(G); return rc; }
     *out = G;
     return GAM_OK;
+}
+
+int gam_gpu_create_from_corners(gam_gpu_t** out, const gam_model_c* m, const double* xyz, int ic) {
+    return create_from_corners(out, m, xyz, ic, nullptr);
+}
+
+int gam_gpu_create_from_corners_b0(gam_gpu_t** out, const gam_model_c* m, const double* xyz, int ic, int b0Kind,
+                                   const double* b0Par) {
+    if (!b0Par || (b0Kind != GAM_B0_UNIFORM && b0Kind != GAM_B0_DIPOLE)) return GAM_ERR_ARG;
+    BgSpec bg;
+    bg.type = b0Kind;
+    for (int n = 0; n < 4; ++n) bg.par[n] = b0Par[n];
+    return create_from_corners(out, m, xyz, ic, &bg);
 }
 
 int gam_gpu_sync_to_device(gam_gpu_t* G, unsigned what, const double* gas, const double* magflux, const double* bxyz,
@@ -531,6 +577,11 @@ int gam_gpu_fetch(gam_gpu_t* G, const char* name, double* out, long long n) {
     else if (s == "te") { for (int d = 0; d < 3; ++d) put(h.Te[d], 9); e = fe; }
     else if (s == "teb") { for (int d = 0; d < 3; ++d) put(h.Teb[d], 4); e = fe; }
     else if (s == "xyz") { put(h.xyz, 3); e = fe; }
+    else if (h.bgpool && s == "fcb0") { for (int d = 0; d < 3; ++d) put(h.fcB0[d], 3); }
+    else if (h.bgpool && s == "edgb0") { for (int d = 0; d < 3; ++d) put(h.edgB0[d], 2); }
+    else if (h.bgpool && s == "b0") put(h.B0, 3);
+    else if (h.bgpool && s == "bflux0") put(h.bFlux0, 3);
+    else if (h.bgpool && s == "dpb0") put(h.dpB0, 3);
     else return GAM_ERR_ARG;
     if (n < (long long)np * e.n()) return GAM_ERR_ARG;
     int rc = d2h_planes(G, pl, np, out, e);
@@ -545,6 +596,7 @@ void gam_gpu_destroy(gam_gpu_t* G) {
     if (h.stream) cudaStreamSynchronize(h.stream);
     destroy_graphs(h);
     if (h.pool) cudaFree(h.pool);
+    if (h.bgpool) cudaFree(h.bgpool);
     if (h.f32pool) cudaFree(h.f32pool);
     if (G->stage) cudaFree(G->stage);
     if (G->scratch) cudaFree(G->scratch);

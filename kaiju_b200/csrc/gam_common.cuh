@@ -43,6 +43,7 @@ struct Lay {
 struct Par {
     double gamma, CFL, pdmb, Vd0, cHogH, cHogM, Ca, dFloor, pFloor, limDT0, tFin;
     int doMHD, doBoris, do25D, doLFMLim, rmeth, fixedTimestep;
+    int doBackground;      // background field B0 present (Model%doBackground)
     int bc[6];
 };
 
@@ -76,6 +77,12 @@ struct GridP {
     const double* Tf[3][9];    // [dir][component]
     const double* Te[3][9];
     const double* Teb[3][4];
+    // background field (Grid_T fcB0, edgB0, B0, bFlux0, dpB0; gamtypes.F90:225-236); null without one
+    const double* fcB0[3][3];  // [face dir][xyz] face-averaged B0
+    const double* edgB0[3][2]; // [edge dir][tangent 1, 2] edge-averaged B0 in the edge frame
+    const double* B0[3];       // cell-averaged B0
+    const double* bFlux0[3];   // B0 flux through the lower faces
+    const double* dpB0[3];     // -div(B0 Maxwell stress)/volume, the background momentum source
 };
 
 // ------------------------------------------------------------------------------------------------ helpers

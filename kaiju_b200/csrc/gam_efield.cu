@@ -177,6 +177,10 @@ __global__ void __launch_bounds__(256, 2) k_edge_tile(Lay L, Par p, EdgeSrc<S> i
     T Jd = db2 - db1;
     T b1 = detT * (ynj * bT1 - yni * bT2);
     T b2 = detT * (-(xnj * bT1) + xni * bT2);
+    if (p.doBackground) {   // total corner field (fields.F90:417-420)
+        b1 = b1 + T(__ldg(&in.edgB0[ED][0][c]));
+        b2 = b2 + T(__ldg(&in.edgB0[ED][1][c]));
+    }
     // diffusive speed and EMF (fields.F90:204-221)
     T vA = sqrt(b1 * b1 + b2 * b2) / sqrt(Dc);
     if (p.doBoris) { T Ca = T(p.Ca); vA = Ca * vA / sqrt(Ca * Ca + vA * vA); }
@@ -231,6 +235,7 @@ void enqueue_efield(Handle& h, const StateP& nS, cudaStream_t st) {
             in32.face[d] = f.face[d]; in32.hbA[d] = f.hbA[d]; in32.nbA[d] = f.nbA[d]; in32.edge[d] = f.edge[d];
             for (int c = 0; c < 6; ++c) in32.Te[d][c] = f.Te[d][c];
             for (int c = 0; c < 4; ++c) in32.Teb[d][c] = f.Teb[d][c];
+            for (int c = 0; c < 2; ++c) in32.edgB0[d][c] = f.edgB0[d][c];
         }
         in32.rho = f.rho;
     } else {
@@ -239,6 +244,7 @@ void enqueue_efield(Handle& h, const StateP& nS, cudaStream_t st) {
             in64.face[d] = h.face[d]; in64.hbA[d] = h.hbA[d]; in64.nbA[d] = h.nbA[d]; in64.edge[d] = h.edge[d];
             for (int c = 0; c < 6; ++c) in64.Te[d][c] = h.Te[d][3 + c];
             for (int c = 0; c < 4; ++c) in64.Teb[d][c] = h.Teb[d][c];
+            for (int c = 0; c < 2; ++c) in64.edgB0[d][c] = h.edgB0[d][c];
         }
         in64.rho = h.H.gas[0];
     }

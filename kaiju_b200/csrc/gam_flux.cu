@@ -25,7 +25,7 @@ template <int D> __host__ __device__ constexpr int rec_box() { return D == 0 ? (
 template <int D> __host__ __device__ constexpr int lim_box() { return D == 0 ? (FL + 4) * FR : FL * (FR + 3); }
 template <typename S, int D> constexpr size_t flux_smem() { return sizeof(S) * (9 * rec_box<D>() + 8 * lim_box<D>()); }
 
-template <typename T, typename S, int D, bool MHD>
+template <typename T, typename S, int D, bool MHD, bool BG>
 __global__ void __launch_bounds__(256, 2) k_flux_tile(Lay L, Par p, FluxSrc<S> in, StateP h, FluxP F, Reg r) {
     extern __shared__ __align__(16) unsigned char smraw[];
     S* sRec = reinterpret_cast<S*>(smraw);   // staged in the storage type, converted to T on use
@@ -106,8 +106,19 @@ __global__ void __launch_bounds__(256, 2) k_flux_tile(Lay L, Par p, FluxSrc<S> i
         if constexpr (std::is_same<S, double>::value) Bn = T(__ldg(&in.bn[D][c]) / faB);
         else Bn = T(__ldg(&in.bn[D][c]));
         T mF[3] = {T(0), T(0), T(0)};
-        magKin<T>(p, T(-1), WL, BL, Bn, Tf, mF, bbD, VaD);
-        magKin<T>(p, T(1), WR, BR, Bn, Tf, mF, bbD, VaD);
+        if constexpr (BG) {   // background field on the face (stress.F90:302-305)
+            T B0[3];
+#pragma unroll
+            for (int x = 0; x < 3; ++x) B0[x] = T(__ldg(&in.fcB0[D][x][c]));
+            T B0n;
+            if constexpr (std::is_same<S, double>::value) B0n = T(__ldg(&in.b0[D][c]) / faB);
+            else B0n = T(__ldg(&in.b0[D][c]));
+            magKin<T, true>(p, T(-1), WL, BL, Bn, Tf, mF, bbD, VaD, B0, B0n);
+            magKin<T, true>(p, T(1), WR, BR, Bn, Tf, mF, bbD, VaD, B0, B0n);
+        } else {
+            magKin<T>(p, T(-1), WL, BL, Bn, Tf, mF, bbD, VaD);
+            magKin<T>(p, T(1), WR, BR, Bn, Tf, mF, bbD, VaD);
+        }
         if (p.doBoris) {
             T Ca2 = T(p.Ca) * T(p.Ca);
 #pragma unroll
@@ -149,15 +160,21 @@ static void launch_flux_dir(Handle& h, const FluxSrc<S>& in, const Reg& r, cudaS
     dim3 grid((unsigned)((r.ni + FL - 1) / FL), 0, 0);
     if (D == 2) { grid.y = (unsigned)((r.nk + FR - 1) / FR); grid.z = (unsigned)r.nj; }
     else { grid.y = (unsigned)((r.nj + FR - 1) / FR); grid.z = (unsigned)r.nk; }
-    if (p.doMHD) k_flux_tile<T, S, D, true><<<grid, 256, flux_smem<S, D>(), st>>>(h.L, p, in, h.H, F, r);
-    else k_flux_tile<T, S, D, false><<<grid, 256, flux_smem<S, D>(), st>>>(h.L, p, in, h.H, F, r);
+    if (p.doMHD && p.doBackground)
+        k_flux_tile<T, S, D, true, true><<<grid, 256, flux_smem<S, D>(), st>>>(h.L, p, in, h.H, F, r);
+    else if (p.doMHD) k_flux_tile<T, S, D, true, false><<<grid, 256, flux_smem<S, D>(), st>>>(h.L, p, in, h.H, F, r);
+    else k_flux_tile<T, S, D, false, false><<<grid, 256, flux_smem<S, D>(), st>>>(h.L, p, in, h.H, F, r);
     h.launches++;
 }
 
 template <typename T, typename S, int D>
 static void set_flux_smem() {
-    cudaFuncSetAttribute(k_flux_tile<T, S, D, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)flux_smem<S, D>());
-    cudaFuncSetAttribute(k_flux_tile<T, S, D, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)flux_smem<S, D>());
+    cudaFuncSetAttribute(k_flux_tile<T, S, D, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)flux_smem<S, D>());
+    cudaFuncSetAttribute(k_flux_tile<T, S, D, true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)flux_smem<S, D>());
+    cudaFuncSetAttribute(k_flux_tile<T, S, D, false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)flux_smem<S, D>());
 }
 void flux_kernels_init() {
     set_flux_smem<double, double, 0>(); set_flux_smem<double, double, 1>(); set_flux_smem<double, double, 2>();
@@ -187,6 +204,8 @@ void enqueue_fluxes(Handle& h, const StateP& nS, cudaStream_t st) {
             for (int q = 0; q < 9; ++q) in.Tf[d][q] = f.Tf[d][q];
             in.face[d] = f.face[d];
             in.bn[d] = f.hbA[d];
+            for (int x = 0; x < 3; ++x) in.fcB0[d][x] = f.fcB0[d][x];
+            in.b0[d] = f.b0n[d];
         }
         fluxes_all<float, float>(h, in, st);
     } else {
@@ -198,6 +217,8 @@ void enqueue_fluxes(Handle& h, const StateP& nS, cudaStream_t st) {
             for (int q = 0; q < 9; ++q) in.Tf[d][q] = h.Tf[d][q];
             in.face[d] = h.face[d];
             in.bn[d] = h.H.mf[d];
+            for (int x = 0; x < 3; ++x) in.fcB0[d][x] = h.fcB0[d][x];
+            in.b0[d] = h.bFlux0[d];
         }
         fluxes_all<double, double>(h, in, st);
     }

@@ -349,6 +349,111 @@ __global__ void k_ic_bw_flux(Lay L, Out3 lA, StateP s) {
     s.mf[2][c] = A0[c] - A0[cj] + A1[c + 1] - A1[c];
 }
 
+// ------------------------------------------------------------------------------------ background field
+// AddB0 (background.F90:20-167) for the built-in background functions: per cell, the 12x12-point face
+// flux, face average and Maxwell stress of B0 on its three lower faces, the 12-point edge averages on
+// its three lower edges (mapped to the edge frame T1/T2), and the 12^3-point cell average.
+struct B0Fn {
+    int type;                // GAM_B0_UNIFORM (1): (bx, by, bz); GAM_B0_DIPOLE (2): moment M0 along z at (bx, by, bz)
+    double bx, by, bz, M0;
+    __device__ void operator()(double x, double y, double z, double* A) const {
+        if (type == 1) { A[0] = bx; A[1] = by; A[2] = bz; return; }
+        // Dipole (apps/msphutils.F90:534-551): 3 (m.r) r / rad**5 - m / rad**3
+        double r[3] = {x - bx, y - by, z - bz};
+        double rad = norm2v3(r);
+        double m[3] = {0.0, 0.0, M0};
+        double mr = m[0] * r[0] + m[1] * r[1] + m[2] * r[2];
+        for (int c = 0; c < 3; ++c) A[c] = 3 * mr * r[c] / pow(rad, 5.0) - m[c] / pow(rad, 3.0);
+    }
+};
+struct B0Vol {   // the vector wrapped as a 5-variable integrand for volumeIntegral
+    B0Fn F;
+    __device__ void operator()(double x, double y, double z, double* W) const {
+        double A[3];
+        F(x, y, z, A);
+        W[0] = A[0]; W[1] = A[1]; W[2] = A[2]; W[3] = 0.0; W[4] = 0.0;
+    }
+};
+struct BgOut { double* fcB0[3][3]; double* bFlux0[3]; double* edgB0[3][2]; double* B0[3]; double* fS[3][3]; };
+
+__global__ void k_add_b0_cell(Lay L, Corners X, B0Fn F, GridP g, BgOut o) {
+    long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (t >= (long long)L.Ni * L.Nj * L.Nk) return;
+    int i = (int)(t % L.Ni);
+    long long q = t / L.Ni;
+    int j = (int)(q % L.Nj), k = (int)(q / L.Nj);
+    long long c = L.at(i, j, k);
+    for (int d = 0; d < 3; ++d) {
+        double f0[3], f1[3], f2[3], f3[3];
+        corner(L, X, i, j, k, f0);
+        if (d == 0) { corner(L, X, i, j + 1, k, f1); corner(L, X, i, j, k + 1, f2); corner(L, X, i, j + 1, k + 1, f3); }
+        else if (d == 1) { corner(L, X, i, j, k + 1, f1); corner(L, X, i + 1, j, k, f2); corner(L, X, i + 1, j, k + 1, f3); }
+        else { corner(L, X, i + 1, j, k, f1); corner(L, X, i, j + 1, k, f2); corner(L, X, i + 1, j + 1, k, f3); }
+        double dx[3], dy[3], dz[3];   // faceDeltas (quadrature.F90:373-389)
+        dx[0] = f1[0] - f0[0]; dx[1] = f2[0] - f0[0]; dx[2] = f3[0] + f0[0] - f2[0] - f1[0];
+        dy[0] = f1[1] - f0[1]; dy[1] = f2[1] - f0[1]; dy[2] = f3[1] + f0[1] - f2[1] - f1[1];
+        dz[0] = f1[2] - f0[2]; dz[1] = f2[2] - f0[2]; dz[2] = f3[2] + f0[2] - f2[2] - f1[2];
+        // GaussianFaceFlux / GaussianFaceStress (quadrature.F90:105-151, 223-280) and
+        // GaussianFaceIntegral (:159-221) share the quadrature points
+        double flx = 0.0, Mbb[3] = {0.0, 0.0, 0.0}, fI[3] = {0.0, 0.0, 0.0};
+        for (int a = 0; a < 12; ++a)
+            for (int b = 0; b < 12; ++b) {
+                double eta = 0.5 * (1 + c_gA[a]), psi = 0.5 * (1 + c_gA[b]);
+                double w = c_gW[a] * c_gW[b];
+                double xp = f0[0] + dx[0] * eta + dx[1] * psi + dx[2] * eta * psi;
+                double yp = f0[1] + dy[0] * eta + dy[1] * psi + dy[2] * eta * psi;
+                double zp = f0[2] + dz[0] * eta + dz[1] * psi + dz[2] * eta * psi;
+                double Ap[3];
+                F(xp, yp, zp, Ap);
+                double etaV[3] = {dx[0] + dx[2] * psi, dy[0] + dy[2] * psi, dz[0] + dz[2] * psi};
+                double psiV[3] = {dx[1] + dx[2] * eta, dy[1] + dy[2] * eta, dz[1] + dz[2] * eta};
+                double cr[3], N[3];
+                cross3(etaV, psiV, cr);
+                for (int x = 0; x < 3; ++x) N[x] = 0.25 * w * cr[x];
+                flx = flx + (N[0] * Ap[0] + N[1] * Ap[1] + N[2] * Ap[2]);
+                double B0B0 = Ap[0] * Ap[0] + Ap[1] * Ap[1] + Ap[2] * Ap[2];
+                double B0dS = Ap[0] * N[0] + Ap[1] * N[1] + Ap[2] * N[2];
+                for (int x = 0; x < 3; ++x) Mbb[x] = Mbb[x] + 0.5 * B0B0 * N[x] - Ap[x] * B0dS;
+                double area = 0.25 * norm2v3(cr) * w;
+                for (int x = 0; x < 3; ++x) fI[x] = fI[x] + area * Ap[x];
+            }
+        o.bFlux0[d][c] = flx;
+        double fa = g.face[d][c];
+        for (int x = 0; x < 3; ++x) { o.fcB0[d][x][c] = fI[x] / fa; o.fS[d][x][c] = Mbb[x]; }
+    }
+    for (int d = 0; d < 3; ++d) {   // GaussianEdgeIntegral (quadrature.F90:345-370), edge frame from Te
+        double e1[3], e2[3], dR2[3], xBar[3], eInt[3] = {0.0, 0.0, 0.0};
+        corner(L, X, i, j, k, e1);
+        corner(L, X, i + (d == 0), j + (d == 1), k + (d == 2), e2);
+        for (int x = 0; x < 3; ++x) { dR2[x] = 0.5 * (e2[x] - e1[x]); xBar[x] = 0.5 * (e2[x] + e1[x]); }
+        for (int a = 0; a < 12; ++a) {
+            double xp[3], Ap[3];
+            for (int x = 0; x < 3; ++x) xp[x] = xBar[x] + c_gA[a] * dR2[x];
+            F(xp[0], xp[1], xp[2], Ap);
+            for (int x = 0; x < 3; ++x) eInt[x] = eInt[x] + 0.5 * c_gW[a] * Ap[x];
+        }
+        o.edgB0[d][0][c] = eInt[0] * g.Te[d][3][c] + eInt[1] * g.Te[d][4][c] + eInt[2] * g.Te[d][5][c];
+        o.edgB0[d][1][c] = eInt[0] * g.Te[d][6][c] + eInt[1] * g.Te[d][7][c] + eInt[2] * g.Te[d][8][c];
+    }
+    double xyzC[8][3], w[5];
+    cellCorners(L, X, i, j, k, xyzC);
+    volumeIntegral(xyzC, B0Vol{F}, w);
+    double dV = g.volume[c];
+    for (int x = 0; x < 3; ++x) o.B0[x][c] = w[x] / dV;
+}
+// dpB0 = -div(face stress)/volume on active cells
+__global__ void k_add_b0_dp(Lay L, GridP g, BgOut o, Out3 dp) {
+    long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (t >= (long long)L.Nip * L.Njp * L.Nkp) return;
+    int i = L.is() + (int)(t % L.Nip);
+    long long q = t / L.Nip;
+    int j = L.js() + (int)(q % L.Njp), k = L.ks() + (int)(q / L.Njp);
+    long long c = L.at(i, j, k), cj = c + L.P, ck = c + (long long)L.P * L.Q;
+    for (int x = 0; x < 3; ++x)
+        dp.v[x][c] = -(o.fS[0][x][c + 1] - o.fS[0][x][c] + o.fS[1][x][cj] - o.fS[1][x][c] + o.fS[2][x][ck] -
+                       o.fS[2][x][c]) / g.volume[c];
+}
+
 __global__ void k_copy_state(long long E, StateP src, StateP dst) {
     long long l = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (l >= E) return;
@@ -408,7 +513,31 @@ int init_grid_from_corners(Handle& h) {
     return 0;
 }
 
-int init_problem(Handle& h, int ic) {
+int add_background(Handle& h, const BgSpec& bg) {
+    const Lay& L = h.L;
+    cudaStream_t st = h.stream;
+    if (!h.bgpool) return 1;
+    Corners X = {{h.xyz[0], h.xyz[1], h.xyz[2]}};
+    B0Fn F{bg.type, bg.par[0], bg.par[1], bg.par[2], bg.par[3]};
+    BgOut o;
+    for (int d = 0; d < 3; ++d) {
+        for (int x = 0; x < 3; ++x) { o.fcB0[d][x] = h.fcB0[d][x]; o.fS[d][x] = h.gflx[d][x]; }   // gflx: scratch
+        o.bFlux0[d] = h.bFlux0[d]; o.B0[d] = h.B0[d];
+        for (int c = 0; c < 2; ++c) o.edgB0[d][c] = h.edgB0[d][c];
+    }
+    GridP g = h.gridP();
+    long long nc = (long long)L.Ni * L.Nj * L.Nk;
+    k_add_b0_cell<<<nb(nc, 64), 64, 0, st>>>(L, X, F, g, o);
+    Out3 dp = {{h.dpB0[0], h.dpB0[1], h.dpB0[2]}};
+    long long na = (long long)L.Nip * L.Njp * L.Nkp;
+    k_add_b0_dp<<<nb(na, 256), 256, 0, st>>>(L, g, o, dp);
+    h.launches += 2;
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) { std::fprintf(stderr, "gamgpu: background: %s\n", cudaGetErrorString(e)); return 3; }
+    return 0;
+}
+
+int init_problem(Handle& h, int ic, const BgSpec* bg) {
     const Lay& L = h.L;
     cudaStream_t st = h.stream;
     GridP g = h.gridP();
@@ -421,7 +550,10 @@ int init_problem(Handle& h, int ic) {
         Corners X = {{h.xyz[0], h.xyz[1], h.xyz[2]}};
         long long n = (long long)L.Nip * L.Njp * L.Nkp;
         k_ic_bw_gas<<<nb(n, 128), 128, 0, st>>>(L, h.p, X, h.volume, s);
-        if (h.p.doMHD) {
+        // prob/doBack (prob.F90:228-269): with a uniform background the blast field is held as B0 and
+        // the residual field starts at zero
+        bool fieldAsBackground = bg && bg->type == 1;
+        if (h.p.doMHD && !fieldAsBackground) {
             Out3 lA = {{h.E[0], h.E[1], h.E[2]}};   // E planes as scratch for the edge integrals of A
             double bScl = 1.0 / (double)sqrtf(2.0f);
             long long ne = (long long)(L.Ni - 1) * (L.Nj - 1) * (L.Nk - 1);
@@ -431,7 +563,11 @@ int init_problem(Handle& h, int ic) {
         }
         h.launches++;
     }
-    // CalcGridInfo tail (init.F90:204-244)
+    // CalcGridInfo: AddB0 after the IC (init.F90:180-184), then the tail (init.F90:204-244)
+    if (bg) {
+        int rc = add_background(h, *bg);
+        if (rc) return rc;
+    }
     if (h.p.doMHD) launch_bflux2fld(h, s, st);
     launch_bcs(h, s, st);
     k_copy_state<<<nb(L.E, 256), 256, 0, st>>>(L.E, s, h.S[h.cur ^ 1]);

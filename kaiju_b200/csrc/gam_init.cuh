@@ -5,7 +5,13 @@
 namespace gam {
 // Corners2Grid (src/gamera/init.F90:801-1145) from the corner planes h.xyz[3] already on the device.
 int init_grid_from_corners(Handle& h);
-// Initial condition ic (0 = OT2D, 1 = BW) into State n, then the end of CalcGridInfo
-// (init.F90:204-244): bFlux2Fld, EnforceBCs, oState = State, CalcDT, oState%time = State%time - dt.
-int init_problem(Handle& h, int ic);
+// A built-in background field: type 1 uniform par[0..2]; type 2 dipole of moment par[3] along z
+// centred at par[0..2]
+struct BgSpec { int type; double par[4]; };
+// AddB0 (src/gamera/background.F90:20-167) of bg into the background planes
+int add_background(Handle& h, const BgSpec& bg);
+// Initial condition ic (0 = OT2D, 1 = BW) into State n, AddB0 when bg is given, then the end of
+// CalcGridInfo (init.F90:204-244): bFlux2Fld, EnforceBCs, oState = State, CalcDT,
+// oState%time = State%time - dt.
+int init_problem(Handle& h, int ic, const BgSpec* bg = nullptr);
 }  // namespace gam

@@ -45,6 +45,9 @@ template <typename S> struct FluxSrc {
     const S* Tf[3][9];
     const S* face[3];
     const S* bn[3];     // normal field on the face: half-state flux / area
+    const S* fcB0[3][3];  // background: face-averaged B0 per face direction
+    const S* b0[3];       // background normal field: bFlux0 (divided by the area in the kernel) for
+                          // double storage, bFlux0/area for float storage
 };
 // Inputs of the edge kernels
 template <typename S> struct EdgeSrc {
@@ -56,6 +59,7 @@ template <typename S> struct EdgeSrc {
     const S* Te[3][6];  // T1 (x,y,z), T2 (x,y,z) of each edge direction
     const S* Teb[3][4];
     const S* edge[3];
+    const S* edgB0[3][2]; // background: edge-frame B0 (tangents 1, 2) per edge direction
 };
 struct Vec3P { double* v[3]; };
 struct FluxP { double* g[5]; double* m[3]; };
@@ -85,14 +89,23 @@ __device__ __forceinline__ void gasKin(T gm1, T sg, const T* W, const T* Tf, T* 
     dW[3] = dW[3] + sg * D * Vz;
     dW[4] = dW[4] + sg * E;
 }
-// One-sided magnetic stress (stress.F90:513-599, no background field)
-template <typename T>
+// One-sided magnetic stress (stress.F90:513-599). With a background field (BG) the Alfven speed and
+// bbD use the total field and the stress gains the B0 cross terms; B0 is the face-averaged background
+// and B0n its normal component.
+template <typename T, bool BG = false>
 __device__ __forceinline__ void magKin(const Par& p, T sg, const T* W, const T* B, T Bn, const T* Tf, T* mF, T& bbD,
-                                       T& VaD) {
+                                       T& VaD, const T* B0 = nullptr, T B0n = T(0)) {
     T D = W[0], P = W[4];
     T dPb = T(0.5) * (B[0] * B[0] + B[1] * B[1] + B[2] * B[2]);
-    T Va2 = T(2) * dPb / D;
-    bbD = bbD + T(0.5) * (B[0] * B[0] + B[1] * B[1] + B[2] * B[2]);
+    T Va2;
+    if constexpr (BG) {
+        T Bt0 = B[0] + B0[0], Bt1 = B[1] + B0[1], Bt2 = B[2] + B0[2];
+        Va2 = (Bt0 * Bt0 + Bt1 * Bt1 + Bt2 * Bt2) / D;
+        bbD = bbD + T(0.5) * (Bt0 * Bt0 + Bt1 * Bt1 + Bt2 * Bt2);
+    } else {
+        Va2 = T(2) * dPb / D;
+        bbD = bbD + T(0.5) * (B[0] * B[0] + B[1] * B[1] + B[2] * B[2]);
+    }
     T Vac2 = Va2;
     if (p.doBoris) { T Ca = T(p.Ca); Vac2 = Va2 / (T(1) + (Va2 / (Ca * Ca))); }
     T Vn = Tf[0] * W[1] + Tf[1] * W[2] + Tf[2] * W[3];
@@ -102,6 +115,12 @@ __device__ __forceinline__ void magKin(const Par& p, T sg, const T* W, const T* 
     mF[0] = mF[0] + Vn0 * (dPb * Tf[0] - B[0] * Bn);
     mF[1] = mF[1] + Vn0 * (dPb * Tf[1] - B[1] * Bn);
     mF[2] = mF[2] + Vn0 * (dPb * Tf[2] - B[2] * Bn);
+    if constexpr (BG) {
+        T BdB0 = B0[0] * B[0] + B0[1] * B[1] + B0[2] * B[2];
+        mF[0] = mF[0] + Vn0 * (-B0[0] * Bn - B[0] * B0n + BdB0 * Tf[0]);
+        mF[1] = mF[1] + Vn0 * (-B0[1] * Bn - B[1] * B0n + BdB0 * Tf[1]);
+        mF[2] = mF[2] + Vn0 * (-B0[2] * Bn - B[2] * B0n + BdB0 * Tf[2]);
+    }
 }
 
 // Cooperative copy of the box [bi0,bi0+ni) x [bj0,bj0+nj) x [bk0,bk0+nk) of one pencil plane into

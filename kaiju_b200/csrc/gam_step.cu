@@ -115,6 +115,10 @@ __global__ void k_flux2deltas(Lay L, Par p, GridP g, FluxP FI, FluxP FJ, FluxP F
 #pragma unroll
         for (int x = 0; x < 3; ++x)
             dGM.v[x][c] = (FI.m[x][c] - FI.m[x][c + 1] + FJ.m[x][c] - FJ.m[x][cj] + FK.m[x][c] - FK.m[x][ck]) / dV;
+        if (p.doBackground) {   // background momentum source (stress.F90:185-188)
+#pragma unroll
+            for (int x = 0; x < 3; ++x) dGM.v[x][c] = dGM.v[x][c] + g.dpB0[x][c];
+        }
     }
 }
 
@@ -200,7 +204,7 @@ __device__ void cellBoris(const Par& p, double* U2, const double* U0, const doub
 
 // CellReynolds + CellMaxwell/CellBoris (mhdgroup.F90:113-126, 170-197, 263-330) on active cells;
 // ghost cells carry State n over.
-__global__ void k_update_gas(Lay L, Par p, StateP nS, StateP oNew, PrimP dGH, Vec3P dGM, const Scal* sc) {
+__global__ void k_update_gas(Lay L, Par p, GridP g, StateP nS, StateP oNew, PrimP dGH, Vec3P dGM, const Scal* sc) {
     Reg r = {0, L.Ni, 0, L.Nj, 0, L.Nk};
     int i, j, k;
     if (!reg_ijk(r, blockIdx.x * (long long)blockDim.x + threadIdx.x, i, j, k)) return;
@@ -219,6 +223,10 @@ __global__ void k_update_gas(Lay L, Par p, StateP nS, StateP oNew, PrimP dGH, Ve
             if (p.doBoris) {
                 double B2[3] = {oNew.b[0][c], oNew.b[1][c], oNew.b[2][c]};
                 double B0[3] = {nS.b[0][c], nS.b[1][c], nS.b[2][c]};
+                if (p.doBackground) {   // total fields (mhdgroup.F90:180-183)
+#pragma unroll
+                    for (int x = 0; x < 3; ++x) { B2[x] = B2[x] + g.B0[x][c]; B0[x] = B0[x] + g.B0[x][c]; }
+                }
                 double dPg[5];
                 for (int v = 0; v < 5; ++v) dPg[v] = dGH.w[v][c];
                 cellBoris(p, U, U0, B2, B0, dPg, dPm, dt);
@@ -270,7 +278,9 @@ __global__ void k_calcdt(Lay L, Par p, GridP g, StateP s, Scal* sc) {
         double Cs = sqrt(p.gamma * P / rho);
         double Valf = 0.0;
         if (p.doMHD) {
-            double MagB = sqrt(sq(s.b[0][c]) + sq(s.b[1][c]) + sq(s.b[2][c]));
+            double Bx = s.b[0][c], By = s.b[1][c], Bz = s.b[2][c];
+            if (p.doBackground) { Bx = Bx + g.B0[0][c]; By = By + g.B0[1][c]; Bz = Bz + g.B0[2][c]; }  // gridutils.F90:82-86
+            double MagB = sqrt(sq(Bx) + sq(By) + sq(Bz));
             Valf = MagB / sqrt(rho);
             if (p.doBoris) Valf = p.Ca * Valf / sqrt(p.Ca * p.Ca + Valf * Valf);
         }
@@ -484,7 +494,7 @@ __global__ void k_bc_k(Lay L, Par p, StateP s) {
 }
 
 // DivB (gridutils.F90:717-770) partial sums, one per block, reduced in a fixed order afterwards
-__global__ void k_divb_partial(Lay L, StateP s, double* partial) {
+__global__ void k_divb_partial(Lay L, GridP g, int bg, StateP s, double* partial) {
     Reg r = {L.is(), L.Nip, L.js(), L.Njp, L.ks(), L.Nkp};
     int i, j, k;
     double v = 0.0;
@@ -493,7 +503,13 @@ __global__ void k_divb_partial(Lay L, StateP s, double* partial) {
         double dFi = s.mf[0][c] - s.mf[0][c + 1];
         double dFj = s.mf[1][c] - s.mf[1][c + L.P];
         double dFk = s.mf[2][c] - s.mf[2][c + (long long)L.P * L.Q];
-        v = fabs(dFi + dFj + dFk);
+        double dFi0 = 0.0, dFj0 = 0.0, dFk0 = 0.0;
+        if (bg) {   // total divergence includes the background flux (gridutils.F90:754-758)
+            dFi0 = g.bFlux0[0][c] - g.bFlux0[0][c + 1];
+            dFj0 = g.bFlux0[1][c] - g.bFlux0[1][c + L.P];
+            dFk0 = g.bFlux0[2][c] - g.bFlux0[2][c + (long long)L.P * L.Q];
+        }
+        v = fabs(dFi + dFj + dFk + dFi0 + dFj0 + dFk0);
     }
     for (int off = 16; off > 0; off >>= 1) v += __shfl_down_sync(0xffffffffu, v, off);
     __shared__ double ws[32];
@@ -534,6 +550,9 @@ GridP Handle::gridP() const {
         g.face[d] = face[d]; g.edge[d] = edge[d];
         for (int q = 0; q < 9; ++q) { g.Tf[d][q] = Tf[d][q]; g.Te[d][q] = Te[d][q]; }
         for (int q = 0; q < 4; ++q) g.Teb[d][q] = Teb[d][q];
+        for (int x = 0; x < 3; ++x) g.fcB0[d][x] = fcB0[d][x];
+        for (int q = 0; q < 2; ++q) g.edgB0[d][q] = edgB0[d][q];
+        g.B0[d] = B0[d]; g.bFlux0[d] = bFlux0[d]; g.dpB0[d] = dpB0[d];
     }
     return g;
 }
@@ -567,10 +586,28 @@ __global__ void k_to_f32(const double* src, float* dst, long long n) {
     if (l < n) dst[l] = float(src[l]);
 }
 
+__global__ void k_ratio_f32(const double* num, const double* den, float* dst, long long n) {
+    long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (t < n) { double d = den[t]; dst[t] = d != 0.0 ? float(num[t] / d) : 0.0f; }
+}
+
+// float copies of the background planes (fcB0, bFlux0/face, edgB0)
+void refresh_f32_background(Handle& h) {
+    if (!h.f32pool || !h.p.doBackground) return;
+    const long long E = h.L.E;
+    F32Planes& f = h.f32;
+    for (int d = 0; d < 3; ++d) {
+        for (int x = 0; x < 3; ++x) { k_to_f32<<<nblk(E, 256), 256, 0, h.stream>>>(h.fcB0[d][x], f.fcB0[d][x], E); }
+        for (int c = 0; c < 2; ++c) { k_to_f32<<<nblk(E, 256), 256, 0, h.stream>>>(h.edgB0[d][c], f.edgB0[d][c], E); }
+        k_ratio_f32<<<nblk(E, 256), 256, 0, h.stream>>>(h.bFlux0[d], h.face[d], f.b0n[d], E);
+        h.launches += 6;
+    }
+}
+
 int ensure_f32(Handle& h) {
     if (h.f32pool) return 0;
     const long long E = h.L.E;
-    const int nplanes = 26 + 64;
+    const int nplanes = 26 + 64 + (h.p.doBackground ? 18 : 0);
     if (cudaMalloc(&h.f32pool, sizeof(float) * E * nplanes) != cudaSuccess) return 3;
     cudaMemsetAsync(h.f32pool, 0, sizeof(float) * E * nplanes, h.stream);
     float* q = h.f32pool;
@@ -590,6 +627,13 @@ int ensure_f32(Handle& h) {
     for (int d = 0; d < 3; ++d) for (int c = 0; c < 9; ++c) f.Tf[d][c] = take();
     for (int d = 0; d < 3; ++d) for (int c = 0; c < 6; ++c) f.Te[d][c] = take();
     for (int d = 0; d < 3; ++d) for (int c = 0; c < 4; ++c) f.Teb[d][c] = take();
+    if (h.p.doBackground) {
+        for (int d = 0; d < 3; ++d) {
+            for (int x = 0; x < 3; ++x) f.fcB0[d][x] = take();
+            for (int c = 0; c < 2; ++c) f.edgB0[d][c] = take();
+            f.b0n[d] = take();
+        }
+    }
     auto cv = [&](const double* s_, float* d_) { k_to_f32<<<nblk(E, 256), 256, 0, h.stream>>>(s_, d_, E); h.launches++; };
     cv(h.volume, f.volume);
     for (int d = 0; d < 3; ++d) {
@@ -599,6 +643,7 @@ int ensure_f32(Handle& h) {
         for (int c = 0; c < 6; ++c) cv(h.Te[d][3 + c], f.Te[d][c]);
         for (int c = 0; c < 4; ++c) cv(h.Teb[d][c], f.Teb[d][c]);
     }
+    refresh_f32_background(h);
     return cudaGetLastError() == cudaSuccess ? 0 : 3;
 }
 
@@ -669,7 +714,7 @@ int step_enqueue(Handle& h, int cur, cudaEvent_t* ev) {
     k_e2flux<<<nblk(nface, TPB), TPB, 0, st>>>(L, p, E, nS, oS, h.dScal);
     if (p.doMHD) k_bflux2fld<<<nblk(ncell, TPB), TPB, 0, st>>>(L, g, oS);
     else k_copy_b<<<nblk(L.E, 256), 256, 0, st>>>(L, nS, oS);
-    k_update_gas<<<nblk(ncell, TPB), TPB, 0, st>>>(L, p, nS, oS, dGH, dGM, h.dScal);
+    k_update_gas<<<nblk(ncell, TPB), TPB, 0, st>>>(L, p, g, nS, oS, dGH, dGM, h.dScal);
     h.launches += 4;
     // CalcDT, EnforceBCs, bFlux2Fld on the new state
     mark(PH_DT);
@@ -690,7 +735,7 @@ double launch_divb(Handle& h, double* scratchDev, cudaStream_t st) {
     long long n = (long long)L.Nip * L.Njp * L.Nkp;
     int nb = (int)nblk(n, 256);
     StateP s = h.S[h.cur];
-    k_divb_partial<<<nb, 256, 0, st>>>(L, s, scratchDev);
+    k_divb_partial<<<nb, 256, 0, st>>>(L, h.gridP(), h.p.doBackground, s, scratchDev);
     k_sum_partials<<<1, 1024, 0, st>>>(scratchDev, nb, scratchDev + nb);
     h.launches += 2;
     double out = 0.0;

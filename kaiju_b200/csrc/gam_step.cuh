@@ -13,6 +13,8 @@ enum Prec { PREC_FP64 = 0, PREC_FP32FLUX = 1 };
 struct F32Planes {
     float* Wh[5]; float* Wn[5]; float* hb[3]; float* nb[3]; float* hbA[3]; float* nbA[3]; float* Vf[3]; float* rho;
     float* volume; float* face[3]; float* edge[3]; float* Tf[3][9]; float* Te[3][6]; float* Teb[3][4];
+    // background field: fcB0, bFlux0/face and edgB0 (only with a background)
+    float* fcB0[3][3]; float* b0n[3]; float* edgB0[3][2];
 };
 
 struct Handle {
@@ -44,6 +46,9 @@ struct Handle {
     double* volume; double* xyzcc[3]; double* xfc[3][3]; double* di; double* dj; double* dk;
     double* face[3]; double* edge[3]; double* Tf[3][9]; double* Te[3][9]; double* Teb[3][4];
     double* xyz[3];       // corners (only kept when the grid was built on the device)
+    // background field planes (own allocation, only with Model%doBackground), Grid_T layout per plane
+    double* bgpool = nullptr;
+    double* fcB0[3][3] = {}; double* edgB0[3][2] = {}; double* B0[3] = {}; double* bFlux0[3] = {}; double* dpB0[3] = {};
     // FP32 copies for the FP32-flux mode (allocated on first use)
     float* f32pool = nullptr;
     F32Planes f32{};
@@ -79,5 +84,7 @@ void enqueue_efield(Handle& h, const StateP& nS, cudaStream_t st);
 void efield_kernels_init();
 // allocate the float planes and convert the metrics (first switch to GAM_FP32FLUX)
 int ensure_f32(Handle& h);
+// re-convert the background planes into the float copies (after the background changed)
+void refresh_f32_background(Handle& h);
 
 }  // namespace gam

@@ -28,6 +28,7 @@ GAM_BC_PERIODIC, GAM_BC_ZEROGRAD = 0, 1
 GAM_RM_8CENT, GAM_RM_7UP = 0, 1
 GAM_SYNC_STATE, GAM_SYNC_OSTATE = 1, 2
 GAM_IC_OT2D, GAM_IC_BW = 0, 1
+GAM_B0_UNIFORM, GAM_B0_DIPOLE = 1, 2
 TINY, HUGE = 1.0e-12, 1.0e12
 
 
@@ -55,7 +56,8 @@ class ModelC(C.Structure):
 
 class GridC(C.Structure):
     _fields_ = [(n, C.POINTER(C.c_double)) for n in
-                ("xyzcc", "xfc", "di", "dj", "dk", "volume", "face", "edge", "Tf", "Te", "Teb")]
+                ("xyzcc", "xfc", "di", "dj", "dk", "volume", "face", "edge", "Tf", "Te", "Teb",
+                 "fcB0", "edgB0", "B0", "bFlux0", "dpB0")]
 
 
 class StatusC(C.Structure):
@@ -70,6 +72,8 @@ SIGNATURES = {
     "gam_gpu_create": (C.c_int, [C.POINTER(C.c_void_p), C.POINTER(ModelC), C.POINTER(GridC), _DP, _DP, _DP, _DP, _DP,
                                  _DP, C.c_double, C.c_double]),
     "gam_gpu_create_from_corners": (C.c_int, [C.POINTER(C.c_void_p), C.POINTER(ModelC), _DP, C.c_int]),
+    "gam_gpu_create_from_corners_b0": (C.c_int, [C.POINTER(C.c_void_p), C.POINTER(ModelC), _DP, C.c_int, C.c_int,
+                                                 _DP]),
     "gam_gpu_step": (C.c_int, [C.c_void_p, _DP, C.POINTER(C.c_int), _DP]),
     "gam_gpu_advance": (C.c_int, [C.c_void_p, C.c_double]),
     "gam_gpu_run_steps": (C.c_int, [C.c_void_p, C.c_int]),
@@ -149,6 +153,7 @@ class Model:
     doLFMLim: bool = True
     rmeth: str = "8CENT"
     fixedTimestep: bool = False
+    doBackground: bool = False            # background field B0 (grid arrays fcB0, edgB0, B0, bFlux0, dpB0)
     bc: Sequence[int] = (GAM_BC_PERIODIC,) * 6
 
     @property
@@ -173,6 +178,7 @@ class Model:
         m.doMHD, m.doBoris, m.do25D, m.doLFMLim = int(self.doMHD), int(self.doBoris), int(self.do25D), int(self.doLFMLim)
         m.rmeth = {"8CENT": GAM_RM_8CENT, "8C": GAM_RM_8CENT, "7UP": GAM_RM_7UP}[self.rmeth.upper()]
         m.fixedTimestep = int(self.fixedTimestep)
+        m.doBackground = int(self.doBackground)
         for n in range(6):
             m.bc[n] = int(self.bc[n])
         return m
@@ -226,7 +232,11 @@ def array_shapes(model: Model):
         "gflx": c + (5, 3), "mflx": c + (3, 3), "vf": c + (3,), "dgash": c + (5,), "dgasm": c + (3,),
         "xyz": f + (3,), "xyzcc": c + (3,), "xfc": f + (3, 3), "di": c, "dj": c, "dk": c, "volume": c,
         "tf": f + (9, 3), "te": f + (9, 3), "teb": f + (4, 3), "face": f + (3,), "edge": f + (3,),
+        "fcb0": c + (3, 3), "edgb0": c + (2, 3), "b0": c + (3,), "bflux0": c + (3,), "dpb0": c + (3,),
     }
+
+
+BACKGROUND_NAMES = (("fcB0", "fcb0"), ("edgB0", "edgb0"), ("B0", "b0"), ("bFlux0", "bflux0"), ("dpB0", "dpb0"))
 
 
 class GameraGPU:
@@ -250,6 +260,9 @@ class GameraGPU:
                            ("volume", "volume"), ("face", "face"), ("edge", "edge"), ("Tf", "tf"), ("Te", "te"),
                            ("Teb", "teb")):
             setattr(g, cname, _dp(keep[key]))
+        if model.doBackground:
+            for cname, key in BACKGROUND_NAMES:
+                setattr(g, cname, _dp(keep[key]))
         arrs = [None if a is None else np.asfortranarray(a, dtype=np.float64)
                 for a in (gas, magflux, bxyz, ogas, omagflux, obxyz)]
         h = C.c_void_p()
@@ -260,14 +273,30 @@ class GameraGPU:
         return cls(model, h)
 
     @classmethod
-    def from_corners(cls, model: Model, xyz: np.ndarray, ic: str):
-        """Corners2Grid + initial condition + initial BCs/dt on the device."""
+    def from_corners(cls, model: Model, xyz: np.ndarray, ic: str, b0=None):
+        """Corners2Grid + initial condition (+ AddB0) + initial BCs/dt on the device.
+        b0: None, ("uniform", bx, by, bz) or ("dipole", M0[, (cx, cy, cz)]); needs model.doBackground."""
         L = load_library()
         xyz = np.asfortranarray(xyz, dtype=np.float64)
         h = C.c_void_p()
         m = model.to_c()
-        rc = L.gam_gpu_create_from_corners(C.byref(h), C.byref(m), _dp(xyz),
-                                           {"OT2D": GAM_IC_OT2D, "BW": GAM_IC_BW}[ic])
+        icn = {"OT2D": GAM_IC_OT2D, "BW": GAM_IC_BW}[ic]
+        if b0 is None:
+            rc = L.gam_gpu_create_from_corners(C.byref(h), C.byref(m), _dp(xyz), icn)
+        else:
+            par = np.zeros(4)
+            if b0[0] == "uniform":
+                kind = GAM_B0_UNIFORM
+                par[:3] = b0[1:4]
+            elif b0[0] == "dipole":
+                kind = GAM_B0_DIPOLE
+                par[3] = b0[1]
+                if len(b0) > 2:
+                    par[:3] = b0[2]
+            else:
+                raise ValueError(b0)
+            rc = L.gam_gpu_create_from_corners_b0(C.byref(h), C.byref(m), _dp(xyz), icn, kind,
+                                                  par.ctypes.data_as(_DP))
         if rc:
             raise GamError(rc, "gam_gpu_create_from_corners")
         return cls(model, h)

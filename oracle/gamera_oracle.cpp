@@ -102,6 +102,7 @@ struct Model {
     double pdmb = 0.75, dFloor = TINY, pFloor = TINY;
     int rmeth = RM_8CENT;
     int status = 0;   // bit0: disaster (dt<=TINY or no dt<HUGE), bit1: bad (10x drop / limDT0)
+    bool doBackground = false;
 };
 
 struct Grid {
@@ -109,6 +110,7 @@ struct Grid {
     int is, ie, js, je, ks, ke, isg, ieg, jsg, jeg, ksg, keg;
     int isDT, ieDT, jsDT, jeDT, ksDT, keDT;
     Arr xyz, xyzcc, xfc, di, dj, dk, volume, Tf, Te, Teb, face, edge;
+    Arr fcB0, edgB0, B0, bFlux0, dpB0;   // background field (background.F90:20-167), cell-sized arrays
     int bc[6] = {BC_PERIODIC, BC_PERIODIC, BC_PERIODIC, BC_PERIODIC, BC_PERIODIC, BC_PERIODIC};
 };
 
@@ -323,14 +325,21 @@ static void GasKinFlux(const Model& M, int q, const double (*Prim)[vecLen], cons
 
 static void MagKinFlux(const Model& M, int q, const double (*Prim)[vecLen], const double (*Mag)[vecLen],
                        const double* Bn, const double (*TfB)[vecLen], double (*mFlxB)[vecLen], double* bbD,
-                       double* VaD) {  // stress.F90:513-599 (no background field)
+                       double* VaD, const double (*B0)[vecLen], const double* B0n) {  // stress.F90:513-599
     double sg = (double)SgnLR[q];
     for (int i = 0; i < vecLen; ++i) {
         double D = Prim[0][i], P = Prim[4][i];
         double Bx = Mag[0][i], By = Mag[1][i], Bz = Mag[2][i];
+        double B0x = B0[0][i], B0y = B0[1][i], B0z = B0[2][i];
         double dPb = 0.5 * (sq(Bx) + sq(By) + sq(Bz));
-        double Va2 = 2 * dPb / D;
-        bbD[i] = bbD[i] + 0.5 * (sq(Bx) + sq(By) + sq(Bz));
+        double Va2;
+        if (M.doBackground) {
+            Va2 = (sq(Bx + B0x) + sq(By + B0y) + sq(Bz + B0z)) / D;
+            bbD[i] = bbD[i] + 0.5 * (sq(Bx + B0x) + sq(By + B0y) + sq(Bz + B0z));
+        } else {
+            Va2 = 2 * dPb / D;
+            bbD[i] = bbD[i] + 0.5 * (sq(Bx) + sq(By) + sq(Bz));
+        }
         double Vac2;
         if (M.doBoris) Vac2 = Va2 / (1 + (Va2 / sq(M.Ca)));
         else Vac2 = Va2;
@@ -343,6 +352,12 @@ static void MagKinFlux(const Model& M, int q, const double (*Prim)[vecLen], cons
         mFlxB[0][i] = mFlxB[0][i] + Vn0 * (dPb * Nx - Bx * Bn[i]);
         mFlxB[1][i] = mFlxB[1][i] + Vn0 * (dPb * Ny - By * Bn[i]);
         mFlxB[2][i] = mFlxB[2][i] + Vn0 * (dPb * Nz - Bz * Bn[i]);
+        if (M.doBackground) {
+            double BdB0 = B0x * Bx + B0y * By + B0z * Bz;
+            mFlxB[0][i] = mFlxB[0][i] + Vn0 * (-B0x * Bn[i] - Bx * B0n[i] + BdB0 * Nx);
+            mFlxB[1][i] = mFlxB[1][i] + Vn0 * (-B0y * Bn[i] - By * B0n[i] + BdB0 * Ny);
+            mFlxB[2][i] = mFlxB[2][i] + Vn0 * (-B0z * Bn[i] - Bz * B0n[i] + BdB0 * Nz);
+        }
     }
 }
 
@@ -358,6 +373,7 @@ static void Fluxes(const Model& M, const Grid& G, const State& nS, const State& 
     double nMagB[NDIM][limLen][vecLen];
     double PrimL[NVAR][vecLen], PrimR[NVAR][vecLen], MagL[NDIM][vecLen], MagR[NDIM][vecLen];
     double gFlxB[NVAR][vecLen], mFlxB[NDIM][vecLen], dW[NVAR][vecLen], VaD[vecLen], Bn[vecLen], bbD[vecLen];
+    double B0[NDIM][vecLen], B0n[vecLen];
 
     int ie = G.ie + ijkD(dN, IDIR);
     int iMax = std::min((int)vecLen, ie - iB + 1);
@@ -365,6 +381,7 @@ static void Fluxes(const Model& M, const Grid& G, const State& nS, const State& 
     std::memset(gFlxB, 0, sizeof gFlxB); std::memset(mFlxB, 0, sizeof mFlxB); std::memset(dW, 0, sizeof dW);
     std::memset(VaD, 0, sizeof VaD); std::memset(bbD, 0, sizeof bbD); std::memset(TfB, 0, sizeof TfB);
     std::memset(Bn, 0, sizeof Bn); std::memset(faB, 0, sizeof faB);
+    std::memset(B0, 0, sizeof B0); std::memset(B0n, 0, sizeof B0n);
 
     loadBlock(G, VolB, G.volume.d.data(), iB, j, k, iMax, dN, Nr2, false);
     for (int i = 0; i < iMax; ++i) {
@@ -381,6 +398,12 @@ static void Fluxes(const Model& M, const Grid& G, const State& nS, const State& 
         }
         BlockLRs(M.rmeth, VolB, nMagB, MagB, MagL, MagR, NDIM);
         for (int i = 0; i < iMax; ++i) Bn[i] = hS.magFlux(isB + i, j, k, dN) / faB[i];
+        if (M.doBackground) {
+            for (int i = 0; i < iMax; ++i) {
+                for (int c = 0; c < 3; ++c) B0[c][i] = G.fcB0(isB + i, j, k, c + 1, dN);
+                B0n[i] = G.bFlux0(isB + i, j, k, dN) / faB[i];
+            }
+        }
         (void)faceN;
     }
     for (int nv = 0; nv < NVAR; ++nv) {
@@ -396,8 +419,8 @@ static void Fluxes(const Model& M, const Grid& G, const State& nS, const State& 
         BlockLRs(M.rmeth, VolB, nPrimB, PrimB, PrimL, PrimR, NVAR);
     }
     if (M.doMHD) {
-        MagKinFlux(M, 0, PrimL, MagL, Bn, TfB, mFlxB, bbD, VaD);
-        MagKinFlux(M, 1, PrimR, MagR, Bn, TfB, mFlxB, bbD, VaD);
+        MagKinFlux(M, 0, PrimL, MagL, Bn, TfB, mFlxB, bbD, VaD, B0, B0n);
+        MagKinFlux(M, 1, PrimR, MagR, Bn, TfB, mFlxB, bbD, VaD, B0, B0n);
         if (M.doBoris) {
             for (int i = 0; i < iMax; ++i) {
                 double deeV[3], deeP[3];
@@ -466,10 +489,13 @@ static void CalcStress(const Model& M, const Grid& G, const State& nS, const Sta
                 for (int nv = 1; nv <= NVAR; ++nv)
                     dGasH(i, j, k, nv) = (gFlx(i, j, k, nv, IDIR) - gFlx(i + 1, j, k, nv, IDIR) + gFlx(i, j, k, nv, JDIR) -
                                           gFlx(i, j + 1, k, nv, JDIR) + gFlx(i, j, k, nv, KDIR) - gFlx(i, j, k + 1, nv, KDIR)) / dV;
-                if (doMaxwell)
+                if (doMaxwell) {
                     for (int c = 1; c <= NDIM; ++c)
                         dGasM(i, j, k, c) = (mFlx(i, j, k, c, IDIR) - mFlx(i + 1, j, k, c, IDIR) + mFlx(i, j, k, c, JDIR) -
                                              mFlx(i, j + 1, k, c, JDIR) + mFlx(i, j, k, c, KDIR) - mFlx(i, j, k + 1, c, KDIR)) / dV;
+                    if (M.doBackground)
+                        for (int c = 1; c <= NDIM; ++c) dGasM(i, j, k, c) = dGasM(i, j, k, c) + G.dpB0(i, j, k, c);
+                }
             }
 }
 
@@ -601,6 +627,10 @@ static void GetCornerB(const Model& M, const Grid& G, const Arr& bFluxn, const A
         Jd[i] = db2 - db1;
         b1[i] = detT * (ynj * bT1 - yni * bT2);
         b2[i] = detT * (-(xnj * bT1) + xni * bT2);
+        if (M.doBackground) {
+            b1[i] = b1[i] + G.edgB0(iG, j, k, 1, dN);
+            b2[i] = b2[i] + G.edgB0(iG, j, k, 2, dN);
+        }
     }
 }
 
@@ -808,6 +838,8 @@ static void applyUpdate(Model& M, const Grid& G, State& S, State& oS, double dt,
                     double oU[5], B[3], oB[3], dPg[5];
                     for (int v = 0; v < 5; ++v) { oU[v] = oS.Gas(i, j, k, v + 1); dPg[v] = dGasH(i, j, k, v + 1); }
                     for (int c = 0; c < 3; ++c) { B[c] = S.Bxyz(i, j, k, c + 1); oB[c] = oS.Bxyz(i, j, k, c + 1); }
+                    if (M.doBackground)
+                        for (int c = 0; c < 3; ++c) { B[c] = B[c] + G.B0(i, j, k, c + 1); oB[c] = oB[c] + G.B0(i, j, k, c + 1); }
                     CellBoris(M, U, oU, B, oB, dPg, dPm, M.Ca, dt);
                 } else {
                     CellMaxwell(M, U, dPm, dt);
@@ -828,6 +860,11 @@ static double CellDT(const Model& M, const Grid& G, const State& S, int i, int j
     double Vfl = MagV, Valf = 0.0, Vdiff = 0.0;
     if (M.doMHD) {
         double Bx = S.Bxyz(i, j, k, XDIR), By = S.Bxyz(i, j, k, YDIR), Bz = S.Bxyz(i, j, k, ZDIR);
+        if (M.doBackground) {
+            Bx = Bx + G.B0(i, j, k, XDIR);
+            By = By + G.B0(i, j, k, YDIR);
+            Bz = Bz + G.B0(i, j, k, ZDIR);
+        }
         double MagB = std::sqrt(sq(Bx) + sq(By) + sq(Bz));
         Valf = MagB / std::sqrt(rho);
         if (M.doBoris) Valf = M.Ca * Valf / std::sqrt(M.Ca * M.Ca + Valf * Valf);
@@ -1456,7 +1493,109 @@ static void VectorPot2Flux(const Grid& G, State& S, VecFun Axyz, void* ctx) {  /
                 S.magFlux(i, j, k, KDIR) = lA(i, j, k, IDIR) - lA(i, j + 1, k, IDIR) + lA(i + 1, j, k, JDIR) - lA(i, j, k, JDIR);
             }
 }
-static void initBW(const Model& M, Grid& G, State& S) {  // prob.F90:190-255 with the deck defaults
+// ---------------------------------------------------------------- background field (background.F90:20-167)
+// type 1: uniform (bx,by,bz); 2: dipole of moment M0 along z centred at (bx,by,bz) (the reference's
+// magnetosphere dipole is the centre-at-origin case; the offset keeps the singularity off a test domain)
+struct B0ctx { int type; double bx, by, bz, M0; };
+static void B0fun(double x, double y, double z, double* A, void* c) {
+    B0ctx* b = (B0ctx*)c;
+    if (b->type == 1) { A[0] = b->bx; A[1] = b->by; A[2] = b->bz; return; }
+    // Dipole (apps/msphutils.F90:534-551): 3 (m.r) r / rad**5 - m / rad**3
+    double r[3] = {x - b->bx, y - b->by, z - b->bz};
+    double rad = norm2v(r, 3);
+    double m[3] = {0.0, 0.0, b->M0};
+    double mr = dot(m, r, 3);
+    for (int c = 0; c < 3; ++c) A[c] = 3 * mr * r[c] / std::pow(rad, 5.0) - m[c] / std::pow(rad, 3.0);
+}
+static void B0Wrap(double x, double y, double z, double* W, void* c) {
+    double A[3];
+    B0fun(x, y, z, A, c);
+    W[0] = A[0]; W[1] = A[1]; W[2] = A[2]; W[3] = 0.0; W[4] = 0.0;
+}
+static void faceDeltas(const double* f0, const double* f1, const double* f2, const double* f3, double* dx, double* dy,
+                       double* dz) {  // quadrature.F90:373-389
+    dx[0] = f1[0] - f0[0]; dx[1] = f2[0] - f0[0]; dx[2] = f3[0] + f0[0] - f2[0] - f1[0];
+    dy[0] = f1[1] - f0[1]; dy[1] = f2[1] - f0[1]; dy[2] = f3[1] + f0[1] - f2[1] - f1[1];
+    dz[0] = f1[2] - f0[2]; dz[1] = f2[2] - f0[2]; dz[2] = f3[2] + f0[2] - f2[2] - f1[2];
+}
+// GaussianFaceFlux (quadrature.F90:105-151) and GaussianFaceStress (:223-280) of A over one face
+static void GaussianFaceFluxStress(const double* f0, const double* f1, const double* f2, const double* f3, VecFun A,
+                                   void* ctx, double* flx, double* Mbb) {
+    double dx[3], dy[3], dz[3];
+    faceDeltas(f0, f1, f2, f3, dx, dy, dz);
+    *flx = 0.0;
+    Mbb[0] = Mbb[1] = Mbb[2] = 0.0;
+    for (int i = 0; i < 12; ++i)
+        for (int j = 0; j < 12; ++j) {
+            double eta = 0.5 * (1 + gA[i]), psi = 0.5 * (1 + gA[j]);
+            double w = gWgt[i] * gWgt[j];
+            double xp = f0[0] + dx[0] * eta + dx[1] * psi + dx[2] * eta * psi;
+            double yp = f0[1] + dy[0] * eta + dy[1] * psi + dy[2] * eta * psi;
+            double zp = f0[2] + dz[0] * eta + dz[1] * psi + dz[2] * eta * psi;
+            double Ap[3];
+            A(xp, yp, zp, Ap, ctx);
+            double etaV[3] = {dx[0] + dx[2] * psi, dy[0] + dy[2] * psi, dz[0] + dz[2] * psi};
+            double psiV[3] = {dx[1] + dx[2] * eta, dy[1] + dy[2] * eta, dz[1] + dz[2] * eta};
+            double cr[3], N[3];
+            cross3(etaV, psiV, cr);
+            for (int c = 0; c < 3; ++c) N[c] = 0.25 * w * cr[c];
+            *flx = *flx + dot(N, Ap, 3);
+            double B0B0 = dot(Ap, Ap, 3), B0dS = dot(Ap, N, 3);
+            for (int c = 0; c < 3; ++c) Mbb[c] = Mbb[c] + 0.5 * B0B0 * N[c] - Ap[c] * B0dS;
+        }
+}
+static void AddB0(const Model& M, Grid& G, B0ctx* ctx) {
+    (void)M;
+    int lo[5] = {G.isg, G.jsg, G.ksg, 1, 1}, hi[5] = {G.ieg, G.jeg, G.keg, 3, 3};
+    G.fcB0.alloc(5, lo, hi);
+    hi[3] = 2;
+    G.edgB0.alloc(5, lo, hi);
+    hi[3] = 3;
+    G.B0.alloc(4, lo, hi); G.bFlux0.alloc(4, lo, hi); G.dpB0.alloc(4, lo, hi);
+    Arr faceStress;
+    faceStress.alloc(5, lo, hi);
+#pragma omp parallel for collapse(2) schedule(dynamic)
+    for (int k = G.ksg; k <= G.keg; ++k)
+        for (int j = G.jsg; j <= G.jeg; ++j)
+            for (int i = G.isg; i <= G.ieg; ++i) {
+                for (int d = 1; d <= 3; ++d) {
+                    double f0[3], f1[3], f2[3], f3[3], fI[3], flx, Mbb[3];
+                    faceCoords(G, i, j, k, d, f0, f1, f2, f3);
+                    GaussianFaceFluxStress(f0, f1, f2, f3, B0fun, ctx, &flx, Mbb);
+                    G.bFlux0(i, j, k, d) = flx;
+                    GaussianFaceIntegral(f0, f1, f2, f3, B0fun, ctx, fI);
+                    for (int c = 0; c < 3; ++c) G.fcB0(i, j, k, c + 1, d) = fI[c] / G.face(i, j, k, d);
+                    for (int c = 0; c < 3; ++c) faceStress(i, j, k, d, c + 1) = Mbb[c];
+                }
+                for (int d = 1; d <= 3; ++d) {   // edge integrals mapped with the edge velocity triad
+                    double e1[3], e2[3], eInt[3];
+                    for (int c = 0; c < 3; ++c) {
+                        e1[c] = G.xyz(i, j, k, c + 1);
+                        e2[c] = G.xyz(i + (d == IDIR), j + (d == JDIR), k + (d == KDIR), c + 1);
+                    }
+                    GaussianEdgeIntegral(e1, e2, B0fun, ctx, eInt);
+                    G.edgB0(i, j, k, 1, d) = eInt[0] * G.Te(i, j, k, TAN1X, d) + eInt[1] * G.Te(i, j, k, TAN1Y, d) +
+                                             eInt[2] * G.Te(i, j, k, TAN1Z, d);
+                    G.edgB0(i, j, k, 2, d) = eInt[0] * G.Te(i, j, k, TAN2X, d) + eInt[1] * G.Te(i, j, k, TAN2Y, d) +
+                                             eInt[2] * G.Te(i, j, k, TAN2Z, d);
+                }
+                double xyzC[8][3], w[5];
+                cellCoords(G, i, j, k, xyzC);
+                GaussianVolumeIntegral(xyzC, B0Wrap, ctx, w);
+                for (int c = 0; c < 3; ++c) G.B0(i, j, k, c + 1) = w[c] / G.volume(i, j, k);
+            }
+#pragma omp parallel for collapse(2) schedule(static)
+    for (int k = G.ks; k <= G.ke; ++k)
+        for (int j = G.js; j <= G.je; ++j)
+            for (int i = G.is; i <= G.ie; ++i)
+                for (int c = 1; c <= 3; ++c)
+                    G.dpB0(i, j, k, c) = -(faceStress(i + 1, j, k, IDIR, c) - faceStress(i, j, k, IDIR, c) +
+                                           faceStress(i, j + 1, k, JDIR, c) - faceStress(i, j, k, JDIR, c) +
+                                           faceStress(i, j, k + 1, KDIR, c) - faceStress(i, j, k, KDIR, c)) /
+                                         G.volume(i, j, k);
+}
+
+static void initBW(const Model& M, Grid& G, State& S, bool fieldAsBackground) {  // prob.F90:190-255, deck defaults
     BWctx b;
     b.x0 = b.y0 = b.z0 = 0.0; b.Vx0 = b.Vy0 = b.Vz0 = 0.0;
     double B0_BW = 1.0;
@@ -1464,7 +1603,7 @@ static void initBW(const Model& M, Grid& G, State& S) {  // prob.F90:190-255 wit
     b.bScl = B0_BW / (double)std::sqrt(2.0f);   // sqrt(2.0) is a default-real (single precision) literal
     b.bSclz = 0.0;
     GasIC2State(M, G, S, GasIC_BW, &b);
-    if (M.doMHD) VectorPot2Flux(G, S, VectorPot_BW, &b);
+    if (M.doMHD && !fieldAsBackground) VectorPot2Flux(G, S, VectorPot_BW, &b);   // prob/doBack = F
 }
 
 }  // namespace orc
@@ -1484,6 +1623,8 @@ struct orc_params {
     int doMHD, doBoris, rmeth, doLFMLim;
     int bc[6];             // 0 periodic, 1 zeroGrad
     int nThreads;
+    int b0Type;            // 0 none, 1 uniform (b0[0..2]), 2 dipole (moment b0[3] along z, centre b0[0..2])
+    double b0[4];
 };
 
 void* orc_create(const orc_params* p) {
@@ -1521,7 +1662,14 @@ void* orc_create(const orc_params* p) {
     if (Corners2Grid(M, G) != 0) { delete A; return nullptr; }
     allocState(M, G, A->S);
     allocState(M, G, A->oS);
-    if (p->icType == 0) initOT2D(M, G, A->S); else initBW(M, G, A->S);
+    if (p->icType == 0) initOT2D(M, G, A->S);
+    else initBW(M, G, A->S, p->b0Type == 1);
+    if (p->b0Type != 0) {   // CalcGridInfo: AddB0 after the IC (init.F90:180-184)
+        M.doBackground = true;
+        B0ctx bc;
+        bc.type = p->b0Type; bc.bx = p->b0[0]; bc.by = p->b0[1]; bc.bz = p->b0[2]; bc.M0 = p->b0[3];
+        AddB0(M, G, &bc);
+    }
     // CalcGridInfo (init.F90:204-244)
     if (M.doMHD) bFlux2Fld(G, A->S.magFlux, A->S.Bxyz);
     EnforceBCs(M, G, A->S);
@@ -1567,6 +1715,7 @@ static Arr* lookup(App* A, const char* name) {
         {"xyz", &A->G.xyz}, {"xyzcc", &A->G.xyzcc}, {"xfc", &A->G.xfc}, {"di", &A->G.di}, {"dj", &A->G.dj},
         {"dk", &A->G.dk}, {"volume", &A->G.volume}, {"tf", &A->G.Tf}, {"te", &A->G.Te}, {"teb", &A->G.Teb},
         {"face", &A->G.face}, {"edge", &A->G.edge},
+        {"fcb0", &A->G.fcB0}, {"edgb0", &A->G.edgB0}, {"b0", &A->G.B0}, {"bflux0", &A->G.bFlux0}, {"dpb0", &A->G.dpB0},
     };
     for (auto& t : tab) if (std::strcmp(t.n, name) == 0) return t.a;
     return nullptr;
@@ -1587,7 +1736,7 @@ int orc_set(void* h, const char* name, const double* in) {
 // Recompute State%Bxyz from State%magFlux (bFlux2Fld) after a host-side edit.
 void orc_bflux2fld(void* h) { App* A = (App*)h; bFlux2Fld(A->G, A->S.magFlux, A->S.Bxyz); bFlux2Fld(A->G, A->oS.magFlux, A->oS.Bxyz); }
 
-double orc_divb(void* h) {  // gridutils.F90:717-770 (no background)
+double orc_divb(void* h) {  // gridutils.F90:717-770
     App* A = (App*)h;
     const Grid& G = A->G;
     const Arr& mf = A->S.magFlux;
@@ -1598,7 +1747,13 @@ double orc_divb(void* h) {  // gridutils.F90:717-770 (no background)
                 double dFi = mf(i, j, k, IDIR) - mf(i + 1, j, k, IDIR);
                 double dFj = mf(i, j, k, JDIR) - mf(i, j + 1, k, JDIR);
                 double dFk = mf(i, j, k, KDIR) - mf(i, j, k + 1, KDIR);
-                tot = tot + std::fabs(dFi + dFj + dFk + 0.0 + 0.0 + 0.0);
+                double dFi0 = 0.0, dFj0 = 0.0, dFk0 = 0.0;
+                if (A->M.doBackground) {
+                    dFi0 = G.bFlux0(i, j, k, IDIR) - G.bFlux0(i + 1, j, k, IDIR);
+                    dFj0 = G.bFlux0(i, j, k, JDIR) - G.bFlux0(i, j + 1, k, JDIR);
+                    dFk0 = G.bFlux0(i, j, k, KDIR) - G.bFlux0(i, j, k + 1, KDIR);
+                }
+                tot = tot + std::fabs(dFi + dFj + dFk + dFi0 + dFj0 + dFk0);
             }
     return tot;
 }

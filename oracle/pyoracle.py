@@ -32,6 +32,7 @@ class OrcParams(C.Structure):
         ("cHogH", C.c_double), ("cHogM", C.c_double), ("Ca", C.c_double), ("tFin", C.c_double),
         ("doMHD", C.c_int), ("doBoris", C.c_int), ("rmeth", C.c_int), ("doLFMLim", C.c_int),
         ("bc", C.c_int * 6), ("nThreads", C.c_int),
+        ("b0Type", C.c_int), ("b0", C.c_double * 4),
     ]
 
 
@@ -92,6 +93,7 @@ def array_shapes(Nip, Njp, Nkp, nG=4):
         "gflx": c + (5, 3), "mflx": c + (3, 3), "vf": c + (3,), "dgash": c + (5,), "dgasm": c + (3,),
         "xyz": f + (3,), "xyzcc": c + (3,), "xfc": f + (3, 3), "di": c, "dj": c, "dk": c, "volume": c,
         "tf": f + (9, 3), "te": f + (9, 3), "teb": f + (4, 3), "face": f + (3,), "edge": f + (3,),
+        "fcb0": c + (3, 3), "edgb0": c + (2, 3), "b0": c + (3,), "bflux0": c + (3,), "dpb0": c + (3,),
     }
 
 
@@ -100,7 +102,7 @@ class Oracle:
 
     def __init__(self, Nip, Njp, Nkp, ic="OT2D", grid="uniform", bounds=None, warp_amp=0.0, CFL=0.3,
                  gamma=5.0 / 3.0, pdmb=0.75, Vd0=0.5, cHogH=0.25, cHogM=0.25, Ca=1.0e12, tFin=1.0e30,
-                 doMHD=True, doBoris=False, rmeth="8CENT", doLFMLim=True, bc=None, threads=0):
+                 doMHD=True, doBoris=False, rmeth="8CENT", doLFMLim=True, bc=None, threads=0, b0=None):
         p = OrcParams()
         p.Nip, p.Njp, p.Nkp = Nip, Njp, Nkp
         p.icType = {"OT2D": IC_OT2D, "BW": IC_BW}[ic]
@@ -120,6 +122,19 @@ class Oracle:
         for n in range(6):
             p.bc[n] = bc[n]
         p.nThreads = threads
+        # background field: None, ("uniform", bx, by, bz) or ("dipole", M0[, (cx, cy, cz)])
+        p.b0Type = 0
+        if b0 is not None:
+            if b0[0] == "uniform":
+                p.b0Type = 1
+                p.b0[0], p.b0[1], p.b0[2] = b0[1], b0[2], b0[3]
+            elif b0[0] == "dipole":
+                p.b0Type = 2
+                p.b0[3] = b0[1]
+                if len(b0) > 2:
+                    p.b0[0], p.b0[1], p.b0[2] = b0[2]
+            else:
+                raise ValueError(b0)
         self.params = p
         self.shape = (Nip, Njp, Nkp)
         self.h = lib().orc_create(C.byref(p))

@@ -2,6 +2,7 @@
 import numpy as np
 
 GRID_NAMES = ("xyzcc", "xfc", "di", "dj", "dk", "volume", "face", "edge", "tf", "te", "teb")
+BACKGROUND_NAMES = ("fcb0", "edgb0", "b0", "bflux0", "dpb0")
 
 
 def rel_linf(a, b):
@@ -59,6 +60,8 @@ def problem(kind, n=(32, 32, 4), **kw):
     for k in ("pdmb", "Vd0", "cHogH", "cHogM", "Ca", "doMHD", "doBoris", "rmeth", "doLFMLim", "tFin", "gamma"):
         if k in okw:
             mkw[k] = okw[k]
+    if okw.get("b0") is not None:
+        mkw["doBackground"] = True
     if okw.get("doBoris"):
         mkw["Ca"] = okw["Ca"]
     mkw.setdefault("tFin", okw.get("tFin", 1.0e30))
@@ -71,7 +74,8 @@ def oracle_and_gpu(kind, n=(32, 32, 4), **kw):
     from kaiju_b200 import gamera as gm
     okw, model = problem(kind, n, **kw)
     o = Oracle(*n, **okw)
-    grid = {name: o.get(name) for name in GRID_NAMES}
+    names = GRID_NAMES + (BACKGROUND_NAMES if model.doBackground else ())
+    grid = {name: o.get(name) for name in names}
     sc = o.scalars()
     g = gm.GameraGPU.from_arrays(model, grid, o.get("gas"), o.get("magflux"), o.get("ogas"), o.get("omagflux"),
                                  sc["time"], sc["otime"], bxyz=o.get("bxyz"), obxyz=o.get("obxyz"))

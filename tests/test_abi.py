@@ -43,6 +43,15 @@ def test_errstr_and_argument_checks(lib):
     m.doResistive = 1
     g = gm.GridC()
     assert lib.gam_gpu_create(C.byref(h), C.byref(m), C.byref(g), None, None, None, None, None, None, 0.0, 0.0) == gm.GAM_ERR_ARG
+    # background requested without the background arrays: rejected before any CUDA call
+    import numpy as np
+    dummy = np.zeros(8, order="F")
+    m = gm.Model(32, 32, 4, doBackground=True).to_c()
+    g = gm.GridC()
+    for n, _ in gm.GridC._fields_[:11]:
+        setattr(g, n, gm._dp(dummy))
+    dp = gm._dp(dummy)
+    assert lib.gam_gpu_create(C.byref(h), C.byref(m), C.byref(g), dp, dp, dp, dp, dp, dp, 0.0, 0.0) == gm.GAM_ERR_ARG
     assert lib.gam_gpu_step(None, None, None, None) == gm.GAM_ERR_ARG
     assert lib.gam_gpu_fetch(None, b"gas", None, 0) == gm.GAM_ERR_ARG
 

@@ -30,6 +30,11 @@ CASES = [
     ("bw_hydro", "bw", (16, 16, 16), dict(doMHD=False)),
     ("bw_boris", "bw", (16, 16, 16), dict(doBoris=True, Ca=2.0)),
     ("ot_nolfmlim", "ot", (32, 32, 4), dict(doLFMLim=False)),
+    # background field: the blast-wave field held entirely as a uniform B0 (residual field starts at 0)
+    ("bw_bg_uniform", "bw", (32, 16, 16), dict(b0=("uniform", 0.5 ** 0.5, 0.5 ** 0.5, 0.0))),
+    # a dipole background centred off the domain on top of the blast-wave field, with Boris
+    ("bw_bg_dipole", "bw", (32, 16, 16), dict(b0=("dipole", 0.05, (-1.0, 0.1, 0.2)))),
+    ("bw_bg_dipole_boris", "bw", (16, 16, 16), dict(b0=("dipole", 0.05, (-1.0, 0.1, 0.2)), doBoris=True, Ca=2.0)),
 ]
 
 
@@ -136,4 +141,49 @@ def test_fp32_flux_error(gpu_lib, oracle_lib):
         for v in range(5):
             l1 = np.abs(a[..., v] - b[..., v]).sum() / np.abs(b[..., v]).sum() if np.abs(b[..., v]).sum() > 0 else \
                 np.abs(a[..., v]).mean()
+            assert l1 <= 1e-5, (v, l1)
+
+
+@pytest.mark.parametrize("b0", [("uniform", 0.5 ** 0.5, 0.5 ** 0.5, 0.0), ("dipole", 0.05, (-1.0, 0.1, 0.2))],
+                         ids=["uniform", "dipole"])
+def test_device_background_matches_oracle(gpu_lib, oracle_lib, b0):
+    """AddB0 on the device (12x12 face, 12 edge, 12^3 volume quadrature of the built-in B0) vs the
+    oracle's host AddB0 on the same corners; then two steps of the background-field scheme."""
+    from helpers import problem
+    from kaiju_b200 import gamera as gm
+    n = (32, 16, 16)
+    okw, model = problem("bw", n, b0=b0)
+    o = oracle_lib.Oracle(*n, **okw)
+    with gm.GameraGPU.from_corners(model, o.get("xyz"), "BW", b0=b0) as g:
+        b0c = o.get("b0")
+        scale = float((b0c ** 2).sum(-1).max()) * n[0]   # |B0|^2 / dx: the size of a stress divergence
+        for name in ("fcb0", "edgb0", "b0", "bflux0"):
+            errs = per_var_rel(g.fetch(name), o.get(name))
+            assert max(errs) <= 1e-12, (name, errs)
+        assert np.abs(g.fetch("dpb0") - o.get("dpb0")).max() <= 1e-12 * scale
+        for name in ("gas", "magflux", "bxyz"):
+            a, b = g.fetch(name), o.get(name)
+            if np.abs(b).max() == 0.0:
+                assert np.abs(a).max() == 0.0, name
+            else:
+                assert max(per_var_rel(a, b)) <= 1e-12, name
+        sc = o.scalars()
+        assert abs(g.status()["dt"] - sc["dt"]) <= 1e-12 * sc["dt"]
+        o.step(2)
+        g.run_steps(2)
+        _cmp(o, g, ["gas"], tol=1e-9, where="after 2 steps ")
+
+
+def test_fp32_flux_error_background(gpu_lib, oracle_lib):
+    """FP32-flux path with a dipole background (float copies of fcB0, bFlux0/face, edgB0)."""
+    from kaiju_b200 import gamera as gm
+    o, g = oracle_and_gpu("bw", (32, 16, 16), b0=("dipole", 0.05, (-1.0, 0.1, 0.2)))
+    with g:
+        g.set_precision(gm.GAM_FP32FLUX)
+        o.step(10)
+        g.run_steps(10)
+        a, b = g.fetch("gas")[4:36, 4:20, 4:20], o.get("gas")[4:36, 4:20, 4:20]
+        for v in range(5):
+            den = np.abs(b[..., v]).sum()
+            l1 = np.abs(a[..., v] - b[..., v]).sum() / den if den > 0 else np.abs(a[..., v]).mean()
             assert l1 <= 1e-5, (v, l1)

@@ -103,3 +103,36 @@ def test_rejects_short_grid(oracle_lib):
     """Corners2Grid's checks (init.F90:825-834): Nip >= 16 and a multiple of 8."""
     with pytest.raises(ValueError):
         oracle_lib.Oracle(12, 16, 4)
+
+
+def test_background_dipole_is_force_free(oracle_lib):
+    """AddB0 (background.F90:20-167) of a curl-free dipole: the background momentum source dpB0 and the
+    net B0 flux out of every cell vanish to round-off (12-point Gauss quadrature per face)."""
+    o = oracle_lib.Oracle(16, 16, 16, ic="BW", grid="warp", warp_amp=0.04, bounds=(-0.5, 0.5) * 3, CFL=0.3,
+                          bc=[1] * 6, b0=("dipole", 0.05, (-1.0, 0.1, 0.2)))
+    a = slice(4, 20)
+    b0 = o.get("b0")[a, a, a]
+    bf = o.get("bflux0")
+    div = (bf[5:21, a, a, 0] - bf[a, a, a, 0] + bf[a, 5:21, a, 1] - bf[a, a, a, 1] + bf[a, a, 5:21, 2] - bf[a, a, a, 2])
+    assert np.abs(div).max() <= 1e-13 * np.abs(bf).max()
+    scale = (b0 ** 2).sum(-1).max() * 16   # |B0|^2 / dx
+    assert np.abs(o.get("dpb0")[a, a, a]).max() <= 1e-12 * scale
+
+
+def test_background_uniform_equilibrium(oracle_lib):
+    """Uniform gas at rest in a uniform background field with no residual field stays at rest (Cartesian
+    grid: on the warped grid the non-planar faces' area vectors do not close exactly, and uniform
+    pressure alone drives a small flow)."""
+    o = oracle_lib.Oracle(16, 16, 16, ic="BW", grid="uniform", bounds=(-0.5, 0.5) * 3, CFL=0.3,
+                          bc=[1] * 6, b0=("uniform", 0.3, -0.2, 0.5))
+    gas = o.get("gas")
+    gas[..., 0] = 1.0
+    gas[..., 1:4] = 0.0
+    gas[..., 4] = 0.1 / (5.0 / 3.0 - 1.0)
+    for nm in ("gas", "ogas"):
+        o.set(nm, gas)
+    o.step(3)
+    g = o.get("gas")
+    assert np.abs(g[..., 1:4]).max() <= 1e-13
+    assert np.abs(g[..., 0] - 1.0).max() <= 1e-13
+    assert np.abs(o.get("magflux")).max() <= 1e-15
