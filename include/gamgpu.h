@@ -35,6 +35,14 @@ extern "C" {
    (src/base/defs/gdefs.F90:43-45) */
 #define GAM_BC_PERIODIC 0      /* src/gamera/bcs.F90:279-450 */
 #define GAM_BC_ZEROGRAD 1      /* src/gamera/bcs.F90:799-930 */
+#define GAM_BC_LFMPOLE 2       /* INJ/OUTJ across the LFM axis: lfmIn/lfmOut, src/gamera/bcs.F90:1020-1106 */
+#define GAM_BC_LFMBW 3         /* INI/OUTI fixed-gas shells of the LFM blast wave: bw_ibcI/bw_obcI,
+                                  src/gamera/ICs/lfmbw.F90:141-225 (gas state gam_model_c.bwD0/bwP0) */
+
+/* ring reconstruction (ring/rngrec, src/gamera/init.F90:466-478) */
+#define GAM_RING_PLM 0
+#define GAM_RING_PPM 1
+#define GAM_RING_PCM 2
 
 /* reconstruction (Model sim/rmeth, src/gamera/init.F90:447-462) */
 #define GAM_RM_8CENT 0
@@ -55,10 +63,23 @@ typedef struct {
     int ts;                    /* Model%ts                                              */
     int doMHD, doBoris, do25D, doLFMLim, rmeth, fixedTimestep;
     /* doBackground: a background field B0 (gam_grid_c fcB0..dpB0) enters the fluxes, E field, CalcDT and
-     * Boris update (src/gamera/background.F90). The other options are not run on the device;
-     * nonzero -> GAM_ERR_UNSUPPORTED */
+     * Boris update (src/gamera/background.F90). doRing: ring averaging about the LFM axis (the ring
+     * fields below). The other options are not run on the device; nonzero -> GAM_ERR_UNSUPPORTED */
     int doBackground, doGrav, doResistive, doRing, doMultiF, doAB3, nSpc, hasHooks;
     int bc[6];                 /* GAM_BC_* per face                                      */
+    /* ring averaging about the LFM axis (doRing with ring/gid = lfm; src/gamera/ringav.F90,
+     * ringutils.F90): Model%Ring%NumR and Nch(1:NumR) as InitRings set them (ringutils.F90:37-226),
+     * the ring reconstruction, and Model%Ring%doS/doE (both 1 on an untiled grid) */
+    int ringNumR;
+    int ringNch[32];
+    int ringRecon;             /* GAM_RING_*                                              */
+    int ringDoS, ringDoE;
+    /* problem pieces the LFM blast wave (src/gamera/ICs/lfmbw.F90) sets: its predictor fix
+     * (HackPredictor => PredFix, :227-248), the gas state of its GAM_BC_LFMBW shells, and its
+     * timestep domain (DT bounds = active cells, :86-92) */
+    int predFixLFM;
+    double bwD0, bwP0;
+    int dtActive;              /* 1: CalcDT over the active cells only; 0: one ghost layer more */
 } gam_model_c;
 
 /* The Grid_T metric arrays the step reads (gamtypes.F90:163-245), Fortran layout. */
@@ -106,6 +127,8 @@ int gam_gpu_create(gam_gpu_t** h, const gam_model_c* m, const gam_grid_c* g, con
  * ic: GAM_IC_OT2D (src/gamera/prob.F90:74-119) or GAM_IC_BW (prob.F90:190-298, deck defaults). */
 #define GAM_IC_OT2D 0
 #define GAM_IC_BW 1
+#define GAM_IC_LFMBW 2   /* the LFM blast wave with the deck of tests/gamera/lfmbw.xml (x0=-50, y0=30, z0=0,
+                            rC=20, P0=0.1, pRat=10, D0=1, B0=1): ICs/lfmbw.F90:33-104 */
 int gam_gpu_create_from_corners(gam_gpu_t** h, const gam_model_c* m, const double* xyz, int ic);
 
 /* gam_gpu_create_from_corners with a background field (Model%doBackground must be set): AddB0

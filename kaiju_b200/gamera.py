@@ -24,10 +24,11 @@ LIB_PATH = os.path.join(HERE, "libgamgpu.so")
 
 GAM_OK, GAM_ERR_NAN, GAM_ERR_DT_COLLAPSE, GAM_ERR_CUDA, GAM_ERR_TIMEOUT, GAM_ERR_UNSUPPORTED, GAM_ERR_ARG = range(7)
 GAM_FP64, GAM_FP32FLUX = 0, 1
-GAM_BC_PERIODIC, GAM_BC_ZEROGRAD = 0, 1
+GAM_BC_PERIODIC, GAM_BC_ZEROGRAD, GAM_BC_LFMPOLE, GAM_BC_LFMBW = 0, 1, 2, 3
+GAM_RING_PLM, GAM_RING_PPM, GAM_RING_PCM = 0, 1, 2
 GAM_RM_8CENT, GAM_RM_7UP = 0, 1
 GAM_SYNC_STATE, GAM_SYNC_OSTATE = 1, 2
-GAM_IC_OT2D, GAM_IC_BW = 0, 1
+GAM_IC_OT2D, GAM_IC_BW, GAM_IC_LFMBW = 0, 1, 2
 GAM_B0_UNIFORM, GAM_B0_DIPOLE = 1, 2
 TINY, HUGE = 1.0e-12, 1.0e12
 
@@ -51,6 +52,9 @@ class ModelC(C.Structure):
         ("doBackground", C.c_int), ("doGrav", C.c_int), ("doResistive", C.c_int), ("doRing", C.c_int),
         ("doMultiF", C.c_int), ("doAB3", C.c_int), ("nSpc", C.c_int), ("hasHooks", C.c_int),
         ("bc", C.c_int * 6),
+        ("ringNumR", C.c_int), ("ringNch", C.c_int * 32), ("ringRecon", C.c_int), ("ringDoS", C.c_int),
+        ("ringDoE", C.c_int), ("predFixLFM", C.c_int), ("bwD0", C.c_double), ("bwP0", C.c_double),
+        ("dtActive", C.c_int),
     ]
 
 
@@ -155,6 +159,11 @@ class Model:
     fixedTimestep: bool = False
     doBackground: bool = False            # background field B0 (grid arrays fcB0, edgB0, B0, bFlux0, dpB0)
     bc: Sequence[int] = (GAM_BC_PERIODIC,) * 6
+    ring: Optional[dict] = None           # ring averaging about the LFM axis: dict(NumR=, Nch=[...], recon="PPM")
+    predFixLFM: bool = False              # the LFM blast wave's predictor fix
+    bwD0: float = 1.0                     # gas state of GAM_BC_LFMBW shells
+    bwP0: float = 0.1
+    dtActive: bool = False                # CalcDT over the active cells only
 
     @property
     def do25D(self) -> bool:
@@ -181,11 +190,67 @@ class Model:
         m.doBackground = int(self.doBackground)
         for n in range(6):
             m.bc[n] = int(self.bc[n])
+        if self.ring is not None:
+            NumR, Nch = ring_config(self.Nkp, self.ring.get("NumR", 0), self.ring.get("Nch", ()))
+            m.doRing = 1
+            m.ringNumR = NumR
+            for n, c in enumerate(Nch):
+                m.ringNch[n] = c
+            m.ringRecon = {"PLM": GAM_RING_PLM, "PPM": GAM_RING_PPM, "PCM": GAM_RING_PCM}[self.ring.get("recon", "PPM")]
+            m.ringDoS = m.ringDoE = 1
+        m.predFixLFM = int(self.predFixLFM)
+        m.bwD0, m.bwP0 = self.bwD0, self.bwP0
+        m.dtActive = int(self.dtActive)
         return m
 
     @property
     def shape(self):
         return (self.Nip + 2 * self.nG, self.Njp + 2 * self.nG, self.Nkp + 2 * self.nG)
+
+
+# default rings per Np = Nkp (InitRings, ringutils.F90:126-200, the non-aggressive set)
+_RING_DEFAULTS = {8: [4], 16: [8], 32: [8, 16], 64: [8, 16, 32, 32], 128: [8, 16, 32, 32, 64, 64, 64, 64],
+                  256: [8, 16, 32, 32, 64, 64, 64, 64, 128, 128, 128, 128],
+                  512: [8, 16, 32, 32, 64, 64, 64, 64, 128, 128, 128, 128, 256, 256, 256, 256]}
+
+
+def ring_config(Np: int, NumR: int = 0, Nch=()):
+    """Model%Ring%NumR and Nch as InitRings sets them: the table for Np, overridden by ring/Nr, ring/Nc<n>."""
+    if Np not in _RING_DEFAULTS:
+        raise ValueError(f"ring averaging needs Nkp in {sorted(_RING_DEFAULTS)}")
+    NCr = _RING_DEFAULTS[Np]
+    NumR = NumR or len(NCr)
+    out = []
+    for iR in range(1, NumR + 1):
+        c = Nch[iR - 1] if iR <= len(Nch) and Nch[iR - 1] else NCr[min(iR, len(NCr)) - 1]
+        if Np % c:
+            raise ValueError("ring chunk count must divide Nkp")
+        out.append(c)
+    return NumR, out
+
+
+def corners_lfm(model: Model, r_in: float, r_out: float, stretch: float, theta0: float) -> np.ndarray:
+    """LFM-type spherical corners about the x axis: i -> r (geometric ratio `stretch` from r_in to r_out),
+    j -> theta uniform on [theta0, pi - theta0], k -> phi uniform on [0, 2 pi); ghosts continue the formulas
+    (theta beyond the axis reflects through it) and repeat exactly with period Nkp in k."""
+    Ni, Nj, Nk = model.shape
+    g = model.nG
+    i = np.arange(-g + 1, model.Nip + g + 2) - 1          # i - is with is = 1
+    j = np.arange(-g + 1, model.Njp + g + 2) - 1
+    k = np.arange(-g + 1, model.Nkp + g + 2) - 1
+    if stretch == 1.0:
+        r = r_in + (r_out - r_in) * i / model.Nip
+    else:
+        dr0 = (r_out - r_in) * (stretch - 1.0) / (stretch ** model.Nip - 1.0)
+        r = r_in + dr0 * (np.power(stretch, i.astype(float)) - 1.0) / (stretch - 1.0)
+    th = theta0 + j * (np.pi - 2.0 * theta0) / model.Njp
+    ph = np.mod(k, model.Nkp) * 2.0 * np.pi / model.Nkp
+    R, TH, PH = np.meshgrid(r, th, ph, indexing="ij")
+    xyz = np.zeros((Ni + 1, Nj + 1, Nk + 1, 3), order="F")
+    xyz[..., 0] = R * np.cos(TH)
+    xyz[..., 1] = R * np.sin(TH) * np.cos(PH)
+    xyz[..., 2] = R * np.sin(TH) * np.sin(PH)
+    return xyz
 
 
 def corners_uniform(model: Model, bounds) -> np.ndarray:
@@ -233,6 +298,7 @@ def array_shapes(model: Model):
         "xyz": f + (3,), "xyzcc": c + (3,), "xfc": f + (3, 3), "di": c, "dj": c, "dk": c, "volume": c,
         "tf": f + (9, 3), "te": f + (9, 3), "teb": f + (4, 3), "face": f + (3,), "edge": f + (3,),
         "fcb0": c + (3, 3), "edgb0": c + (2, 3), "b0": c + (3,), "bflux0": c + (3,), "dpb0": c + (3,),
+        "smoothe": c + (3,),
     }
 
 
@@ -280,7 +346,7 @@ class GameraGPU:
         xyz = np.asfortranarray(xyz, dtype=np.float64)
         h = C.c_void_p()
         m = model.to_c()
-        icn = {"OT2D": GAM_IC_OT2D, "BW": GAM_IC_BW}[ic]
+        icn = {"OT2D": GAM_IC_OT2D, "BW": GAM_IC_BW, "LFMBW": GAM_IC_LFMBW}[ic]
         if b0 is None:
             rc = L.gam_gpu_create_from_corners(C.byref(h), C.byref(m), _dp(xyz), icn)
         else:

@@ -58,7 +58,23 @@ enum { IDIR = 1, JDIR, KDIR };
 enum { NORMX = 1, NORMY, NORMZ, TAN1X, TAN1Y, TAN1Z, TAN2X, TAN2Y, TAN2Z };
 enum { XNQI = 1, YNQI, XNQJ, YNQJ };
 enum { INI = 1, OUTI, INJ, OUTJ, INK, OUTK };
-enum { BC_PERIODIC = 0, BC_ZEROGRAD = 1 };
+// Boundary classes: periodic, zero-gradient, the LFM axis (lfmIn/lfmOut, bcs.F90:1020-1106) for INJ/OUTJ,
+// and the LFM blast-wave problem's fixed inner/outer shells (ICs/lfmbw.F90:141-249) for INI/OUTI
+enum { BC_PERIODIC = 0, BC_ZEROGRAD = 1, BC_LFMPOLE = 2, BC_LFMBW = 3 };
+enum { SPOLE = 1, EPOLE = 2 };
+enum { RR_PLM = 0, RR_PPM = 1, RR_PCM = 2, RR_WENO = 3 };
+static const int NFTMAX = 2;
+
+// Ring-average configuration for an LFM-type grid (ringutils.F90:37-226, Model%Ring)
+struct Ring {
+    int NumR = 0;
+    int Nch[32] = {0};
+    int Np = 0, nSi = 0, nSe = 0;
+    bool doS = true, doE = true, doMassRA = false;
+    int recon = RR_PPM;                 // ring/rngrec (init.F90:466-478)
+    int NFTMAG = 1;                     // Fourier modes removed from the face fluxes
+    bool doCleanLoop = true, doFastLoop = true;
+};
 enum { RM_8CENT = 0, RM_7UP = 1 };
 
 static inline int ijkD(int a, int b) { return a == b ? 1 : 0; }
@@ -103,6 +119,10 @@ struct Model {
     int rmeth = RM_8CENT;
     int status = 0;   // bit0: disaster (dt<=TINY or no dt<HUGE), bit1: bad (10x drop / limDT0)
     bool doBackground = false;
+    bool doRing = false;
+    Ring R;
+    bool predFixLFM = false;   // the LFM blast-wave problem's HackPredictor (ICs/lfmbw.F90:227-248)
+    double bwD0 = 1.0, bwP0 = 0.1;   // its fixed-shell gas state (prob/D0, prob/P0)
 };
 
 struct Grid {
@@ -121,6 +141,7 @@ struct State {
 
 struct Solver {
     Arr gFlx, mFlx, Vf, dGasH, dGasM;
+    Arr SmoothE;   // ring-average smoothing E field (ringav.F90:30)
     State StateHf;
 };
 
@@ -458,6 +479,35 @@ static void Fluxes(const Model& M, const Grid& G, const State& nS, const State& 
         for (int i = 0; i < iMax; ++i) gFlx(isB + i, j, k, nv + 1, dN) = faB[i] * gFlxB[nv][i];
 }
 
+// RingFlux (ringutils.F90:663-680): no flux through the faces on the axis; FixGasFluxLFM
+// (gamdebug.F90:91-124) makes the K fluxes at ks and ke+1 agree
+static void RingFlux(const Model& M, const Grid& G, Arr& gFlx, Arr& mFlx) {
+    auto zeroJ = [&](int j) {
+        for (int k = G.ksg; k <= G.keg; ++k)
+            for (int i = G.isg; i <= G.ieg; ++i) {
+                for (int v = 1; v <= NVAR; ++v) gFlx(i, j, k, v, JDIR) = 0.0;
+                if (M.doMHD)
+                    for (int c = 1; c <= NDIM; ++c) mFlx(i, j, k, c, JDIR) = 0.0;
+            }
+    };
+    if (M.R.doS) zeroJ(G.js);
+    if (M.R.doE) zeroJ(G.je + 1);
+    if (!M.doMHD) return;
+    for (int j = G.js; j <= G.je; ++j)
+        for (int i = G.is; i <= G.ie; ++i) {
+            for (int v = 1; v <= NVAR; ++v) {
+                double gF = 0.5 * (gFlx(i, j, G.ks, v, KDIR) + gFlx(i, j, G.ke + 1, v, KDIR));
+                gFlx(i, j, G.ks, v, KDIR) = gF;
+                gFlx(i, j, G.ke + 1, v, KDIR) = gF;
+            }
+            for (int c = 1; c <= NDIM; ++c) {
+                double mF = 0.5 * (mFlx(i, j, G.ks, c, KDIR) + mFlx(i, j, G.ke + 1, c, KDIR));
+                mFlx(i, j, G.ks, c, KDIR) = mF;
+                mFlx(i, j, G.ke + 1, c, KDIR) = mF;
+            }
+        }
+}
+
 static void CalcStress(const Model& M, const Grid& G, const State& nS, const State& hS, Arr& gFlx, Arr& mFlx,
                        Arr& dGasH, Arr& dGasM) {  // stress.F90:41-198
     int nFlx = NDIM, ks = G.ks, ke = G.ke;
@@ -480,6 +530,7 @@ static void CalcStress(const Model& M, const Grid& G, const State& nS, const Sta
                     for (int k = ks; k <= ke + 1; ++k) Fluxes(M, G, nS, hS, iB, j, k, d, gFlx, mFlx);
         }
     }
+    if (M.doRing) RingFlux(M, G, gFlx, mFlx);   // stress.F90:134-139
     bool doMaxwell = M.doMHD;
 #pragma omp parallel for collapse(2) schedule(static)
     for (int k = G.ks; k <= G.ke; ++k)
@@ -499,6 +550,62 @@ static void CalcStress(const Model& M, const Grid& G, const State& nS, const Sta
             }
 }
 
+// ---------------------------------------------------------------- LFM axis index maps (ringutils.F90:482-660)
+static int WrapK(int k, int Np) {   // ringutils.F90:652-660
+    int kp = k + Np / 2;
+    if (kp > Np) kp = kp - Np;
+    return kp;
+}
+// cell-centred conjugate across the axis (lfmIJKcc, ringutils.F90:482-514)
+static void lfmIJKcc(const Model& M, const Grid& G, int i, int j, int k, int& ip, int& jp, int& kp) {
+    int Np = G.Nkp;
+    ip = i;
+    if (k < G.ks) kp = k + Np;
+    else if (k > G.ke) kp = k - Np;
+    else kp = k;
+    jp = j;
+    if (M.R.doS && j < G.js) { jp = G.js + (G.js - j) - 1; kp = WrapK(kp, Np); }
+    if (M.R.doE && j > G.je) { jp = G.je - (j - G.je) + 1; kp = WrapK(kp, Np); }
+}
+// face-centred conjugate (lfmIJKfc, ringutils.F90:517-575)
+static void lfmIJKfc(const Model& M, const Grid& G, int d, int i, int j, int k, int& ip, int& jp, int& kp) {
+    int Np = G.Nkp;
+    ip = i;
+    if (d == IDIR) { lfmIJKcc(M, G, i, j, k, ip, jp, kp); return; }
+    kp = k;
+    if (k < G.ks) kp = k + Np;
+    if (d == JDIR && k > G.ke) kp = k - Np;
+    if (d == KDIR && k > G.ke + 1) kp = k - Np;
+    jp = j;
+    if (d == JDIR) {
+        if (M.R.doS && j < G.js) { jp = G.js + (G.js - j); kp = WrapK(k, Np); }
+        if (M.R.doE && j > G.je + 1) { jp = G.je + 1 - (j - G.je) + 1; kp = WrapK(k, Np); }
+    } else {
+        if (M.R.doS && j < G.js) { jp = G.js + (G.js - j) - 1; kp = WrapK(k, Np); }
+        if (M.R.doE && j > G.je) { jp = G.je - (j - G.je) + 1; kp = WrapK(k, Np); }
+    }
+}
+// RingFlux2FieldFix (ringutils.F90:380-433): Bxyz of the cells across the axis from their conjugates
+static void RingFlux2FieldFix(const Model& M, const Grid& G, Arr& B) {
+    if (!M.doRing || (!M.R.doS && !M.R.doE)) return;
+#pragma omp parallel for collapse(2) schedule(static)
+    for (int k = G.ksg; k <= G.keg; ++k)
+        for (int i = G.isg; i <= G.ieg; ++i)
+            for (int n = 1; n <= M.nG; ++n) {
+                int ip, jp, kp;
+                if (M.R.doS) {
+                    int jg = G.js - n;
+                    lfmIJKcc(M, G, i, jg, k, ip, jp, kp);
+                    for (int c = 1; c <= 3; ++c) B(i, jg, k, c) = B(ip, jp, kp, c);
+                }
+                if (M.R.doE) {
+                    int jg = G.je + n;
+                    lfmIJKcc(M, G, i, jg, k, ip, jp, kp);
+                    for (int c = 1; c <= 3; ++c) B(i, jg, k, c) = B(ip, jp, kp, c);
+                }
+            }
+}
+
 // ---------------------------------------------------------------- B from flux (gridutils.F90:281-301,648-680)
 static void gamCellBxyz(const Grid& G, const Arr& mf, int i, int j, int k, double* B) {
     double dV = G.volume(i, j, k);
@@ -513,7 +620,7 @@ static void gamCellBxyz(const Grid& G, const Arr& mf, int i, int j, int k, doubl
         B[c - 1] = b;
     }
 }
-static void bFlux2Fld(const Grid& G, const Arr& mf, Arr& B) {
+static void bFlux2Fld(const Model& M, const Grid& G, const Arr& mf, Arr& B) {
 #pragma omp parallel for collapse(2) schedule(static)
     for (int k = G.ksg; k <= G.keg; ++k)
         for (int j = G.jsg; j <= G.jeg; ++j)
@@ -522,6 +629,7 @@ static void bFlux2Fld(const Grid& G, const Arr& mf, Arr& B) {
                 gamCellBxyz(G, mf, i, j, k, b);
                 for (int c = 0; c < 3; ++c) B(i, j, k, c + 1) = b[c];
             }
+    if (M.doRing) RingFlux2FieldFix(M, G, B);   // gridutils.F90:298-300
 }
 
 // ---------------------------------------------------------------- predictor (mhdgroup.F90:445-616)
@@ -536,7 +644,7 @@ static void Predictor(const Model& M, const Grid& G, const State& S, const State
             pS.magFlux.d[l] = Q + pdt * dQ;
         }
     }
-    bFlux2Fld(G, pS.magFlux, pS.Bxyz);
+    bFlux2Fld(M, G, pS.magFlux, pS.Bxyz);
 #pragma omp parallel for collapse(2) schedule(static)
     for (int k = G.ksg; k <= G.keg; ++k)
         for (int j = G.jsg; j <= G.jeg; ++j)
@@ -551,6 +659,15 @@ static void Predictor(const Model& M, const Grid& G, const State& S, const State
                 CellP2C(M, pW, pQ);
                 for (int v = 0; v < 5; ++v) pS.Gas(i, j, k, v + 1) = pQ[v];
             }
+    if (M.predFixLFM) {   // HackPredictor of the LFM blast wave, PredFix (ICs/lfmbw.F90:227-248)
+        for (int k = G.ksg; k <= G.keg; ++k)
+            for (int j = G.jsg; j <= G.jeg; ++j)
+                for (int n = 1; n <= M.nG; ++n) {
+                    int ig = G.is - n, ix, jp, kp;
+                    lfmIJKcc(M, G, ig, j, k, ix, jp, kp);
+                    for (int c = 1; c <= 3; ++c) pS.Bxyz(ig, j, k, c) = pS.Bxyz(G.is, jp, kp, c);
+                }
+    }
 }
 
 // ---------------------------------------------------------------- electric field (fields.F90)
@@ -810,6 +927,8 @@ static void CellBoris(const Model& M, double* U2, const double* U0, const double
     CellP2C(M, W2, U2);
 }
 
+static void PoleE(const Model& M, const Grid& G, Arr& E);
+
 // applyUpdate with the buffer roles of the reference: CopyState(State->oState) then in-place update of State
 static void applyUpdate(Model& M, const Grid& G, State& S, State& oS, double dt, const Arr& dGasH, const Arr& dGasM,
                         Arr& E) {
@@ -824,8 +943,9 @@ static void applyUpdate(Model& M, const Grid& G, State& S, State& oS, double dt,
             for (int i = G.is; i <= G.ie; ++i)
                 for (int v = 1; v <= NVAR; ++v) S.Gas(i, j, k, v) = S.Gas(i, j, k, v) + M.dt * dGasH(i, j, k, v);
     if (!M.doMHD) return;
+    if (M.doRing && (M.R.doS || M.R.doE)) PoleE(M, G, E);   // mhdgroup.F90:139-142
     E2Flux(G, S.magFlux, E, dt);
-    bFlux2Fld(G, S.magFlux, S.Bxyz);
+    bFlux2Fld(M, G, S.magFlux, S.Bxyz);
     bool Boris = M.doBoris;
 #pragma omp parallel for collapse(2) schedule(static)
     for (int k = G.ks; k <= G.ke; ++k)
@@ -1083,11 +1203,297 @@ static void zeroGradBC(const Model& M, const Grid& G, State& S, int dir) {  // b
     }
 }
 
+// lfmIn / lfmOut (bcs.F90:1020-1106): ghost cells and faces across the axis from their conjugates
+static void lfmPoleBC(const Model& M, const Grid& G, State& S, int dir) {
+    for (int k = G.ksg; k <= G.keg + 1; ++k)
+        for (int i = G.isg; i <= G.ieg + 1; ++i)
+            for (int n = 1; n <= M.nG; ++n) {
+                int ig = i, kg = k, jg = (dir == INJ) ? G.js - n : G.je + n;
+                int ip, jp, kp;
+                if (ig <= G.ieg && kg <= G.keg) {   // isCellCenterG
+                    lfmIJKcc(M, G, ig, jg, kg, ip, jp, kp);
+                    for (int v = 1; v <= NVAR; ++v) S.Gas(ig, jg, kg, v) = S.Gas(ip, jp, kp, v);
+                    for (int c = 1; c <= NDIM; ++c) S.Bxyz(ig, jg, kg, c) = S.Bxyz(ip, jp, kp, c);
+                }
+                lfmIJKfc(M, G, IDIR, ig, jg, kg, ip, jp, kp);
+                S.magFlux(ig, jg, kg, IDIR) = S.magFlux(ip, jp, kp, IDIR);
+                int jf = (dir == INJ) ? jg : jg + 1;   // the first outer J ghost face is je+2
+                lfmIJKfc(M, G, JDIR, ig, jf, kg, ip, jp, kp);
+                S.magFlux(ig, jf, kg, JDIR) = -S.magFlux(ip, jp, kp, JDIR);
+                lfmIJKfc(M, G, KDIR, ig, jg, kg, ip, jp, kp);
+                S.magFlux(ig, jg, kg, KDIR) = -S.magFlux(ip, jp, kp, KDIR);
+            }
+}
+// bw_ibcI / bw_obcI of the LFM blast wave (ICs/lfmbw.F90:141-225): fixed gas in the ghost shells, face
+// fluxes mirrored from the first/last active shell scaled by the face areas
+static void lfmbwShellBC(const Model& M, const Grid& G, State& S, int dir) {
+    const bool inner = (dir == INI);
+    for (int k = G.ksg; k <= G.keg + 1; ++k)
+        for (int j = G.jsg; j <= G.jeg + 1; ++j)
+            for (int n = 1; n <= M.nG; ++n) {
+                int ig = inner ? G.is - n : G.ie + n;
+                if (j <= G.jeg && k <= G.keg) {
+                    S.Gas(ig, j, k, DEN) = M.bwD0;
+                    S.Gas(ig, j, k, MOMX) = 0.0; S.Gas(ig, j, k, MOMY) = 0.0; S.Gas(ig, j, k, MOMZ) = 0.0;
+                    S.Gas(ig, j, k, ENERGY) = M.bwP0 / (M.gamma - 1.0);
+                }
+                double dApm[3] = {1.0, 1.0, 1.0};
+                if (M.R.doS && j < G.js) dApm[1] = dApm[2] = -1.0;
+                if (M.R.doE && j >= G.je + 1) dApm[1] = dApm[2] = -1.0;
+                for (int d = IDIR; d <= KDIR; ++d) {
+                    int di = (!inner && d == IDIR) ? 1 : 0;
+                    int ia = inner ? G.is : G.ie + di;   // the active shell the ghost face copies
+                    int ip, jp, kp;
+                    lfmIJKfc(M, G, d, ig + di, j, k, ip, jp, kp);
+                    double dA = G.face(ig + di, j, k, d) / G.face(ia, jp, kp, d);
+                    S.magFlux(ig + di, j, k, d) = dApm[d - 1] * dA * S.magFlux(ia, jp, kp, d);
+                }
+            }
+}
+
 static void EnforceBCs(const Model& M, const Grid& G, State& S) {  // step.F90:17-55
     for (int n = 1; n <= 6; ++n) {
-        if (G.bc[n - 1] == BC_PERIODIC) periodicBC(M, G, S, n);
+        int kind = G.bc[n - 1];
+        if (kind == BC_PERIODIC) periodicBC(M, G, S, n);
+        else if (kind == BC_LFMPOLE) lfmPoleBC(M, G, S, n);
+        else if (kind == BC_LFMBW) lfmbwShellBC(M, G, S, n);
         else zeroGradBC(M, G, S, n);
     }
+}
+
+// ---------------------------------------------------------------- ring average (ringav.F90, ringrecon.F90)
+static double minmod(double x, double y) {   // math.F90:192-197
+    return 0.5 * (fsign1(x) + fsign1(y)) * fmind(std::fabs(x), std::fabs(y));
+}
+static void RingLR(int meth, double fm2, double fm1, double f, double fp1, double fp2, double& vm, double& vp) {
+    if (meth == RR_PCM) { vm = f; vp = f; return; }   // ringrecon.F90:239-246
+    if (meth == RR_PLM) {                             // ringrecon.F90:251-270
+        double dwL = f - fm1, dwR = fp1 - f, dwC = (fp1 - fm1) / 2.0;
+        double min1 = fmind(2 * std::fabs(dwL), 2 * std::fabs(dwR));
+        double min2 = fmind(min1, std::fabs(dwC));
+        double dwM = std::copysign(min2, dwC);
+        vp = f + 0.5 * dwM; vm = f - 0.5 * dwM;
+        return;
+    }
+    // PPM (ringrecon.F90:282-322)
+    double dvm2 = fm1 - fm2, dvm1 = f - fm1, dvp1 = fp1 - f, dvp2 = fp2 - fp1;
+    double dvc = 0.5 * (dvm2 + dvm1), SM = 2.0 * minmod(dvm2, dvm1), Sm1 = minmod(dvc, SM);
+    dvc = 0.5 * (dvm1 + dvp1); SM = 2.0 * minmod(dvm1, dvp1); double Sp1 = minmod(dvc, SM);
+    dvc = 0.5 * (dvp2 + dvp1); SM = 2.0 * minmod(dvp2, dvp1); double Sp2 = minmod(dvc, SM);
+    vp = 0.5 * (f + fp1) - (Sp2 - Sp1) / 6.0;
+    vm = 0.5 * (f + fm1) - (Sp1 - Sm1) / 6.0;
+    double ap = vp - f, am = vm - f;
+    if (ap * am >= 0.0) { ap = 0.0; am = 0.0; }
+    else {
+        if (std::fabs(ap) >= 2.0 * std::fabs(am)) ap = -2.0 * am;
+        if (std::fabs(am) >= 2.0 * std::fabs(ap)) am = -2.0 * ap;
+    }
+    vp = f + ap; vm = f + am;
+}
+// ReconstructRing (ringrecon.F90:34-98): parabolic interpolant of each chunk from its chunk neighbours
+static void ReconstructRing(const Model& M, double* rW, int Nc) {
+    const int Np = M.R.Np, dJ = Np / Nc, Ng = 2;
+    std::vector<double> chW(Nc + 2 * Ng);
+    auto ch = [&](int n) -> double& { return chW[n - 1 + Ng]; };
+    for (int n = 1; n <= Nc; ++n) ch(n) = rW[(n - 1) * dJ];
+    for (int n = 1; n <= Ng; ++n) { ch(1 - n) = ch(Nc - n + 1); ch(Nc + n) = ch(n); }
+    for (int n = 1; n <= Nc; ++n) {
+        int mS = 1 + (n - 1) * dJ;
+        double fL, fR, f = ch(n);
+        RingLR(M.R.recon, ch(n - 2), ch(n - 1), f, ch(n + 1), ch(n + 2), fL, fR);
+        double a = 3 * (fL + fR - 2 * f), b = 2 * (3 * f - fR - 2 * fL), c = fL;
+        for (int m = 1; m <= dJ; ++m) {
+            double fI = (a / 3.0) * (double)(3 * m * m - 3 * m + 1) / (double)(dJ * dJ) + 0.5 * b * (double)(2 * m - 1) / (double)dJ + c;
+            rW[mS + m - 2] = fI;
+        }
+    }
+}
+// CleanRing / DirtyRing (ringav.F90:416-458): remove / restore the 0..numFT Fourier modes of a ring
+static void CleanRing(const Model& M, double* Q, double cFT[NFTMAX + 1][2], int numFT) {
+    const int Np = M.R.Np;
+    for (int m = 0; m <= NFTMAX; ++m) cFT[m][0] = cFT[m][1] = 0.0;
+    double aScl = (double)(2.0f / (float)Np);   // 2.0/Np in default real
+    double dp = 2.0 * PI / Np;
+    for (int n = 1; n <= Np; ++n) {
+        double phi = dp * n - 0.5 * dp;
+        for (int m = 0; m <= numFT; ++m) {
+            cFT[m][0] = cFT[m][0] + Q[n - 1] * std::cos(1.0 * m * phi);
+            cFT[m][1] = cFT[m][1] + Q[n - 1] * std::sin(1.0 * m * phi);
+        }
+    }
+    cFT[0][0] = 0.5 * aScl * cFT[0][0]; cFT[0][1] = 0.5 * aScl * cFT[0][1];
+    for (int m = 1; m <= numFT; ++m) { cFT[m][0] = 1.0 * aScl * cFT[m][0]; cFT[m][1] = 1.0 * aScl * cFT[m][1]; }
+    for (int n = 1; n <= Np; ++n) {
+        double phi = dp * n - 0.5 * dp;
+        for (int m = 0; m <= numFT; ++m)
+            Q[n - 1] = Q[n - 1] - cFT[m][0] * std::cos(1.0 * m * phi) - cFT[m][1] * std::sin(1.0 * m * phi);
+    }
+}
+static void DirtyRing(const Model& M, double* Q, const double cFT[NFTMAX + 1][2], int numFT) {
+    const int Np = M.R.Np;
+    double dp = 2.0 * PI / Np;
+    for (int n = 1; n <= Np; ++n) {
+        double phi = dp * n - 0.5 * dp;
+        for (int m = 0; m <= numFT; ++m)
+            Q[n - 1] = Q[n - 1] + cFT[m][0] * std::cos(1.0 * m * phi) + cFT[m][1] * std::sin(1.0 * m * phi);
+    }
+}
+// chunk averages (ringav.F90:156-161, 266-273)
+static void ChunkAverage(const double* in, double* out, int Np, int Nc) {
+    int dC = Np / Nc;
+    for (int n = 1; n <= Nc; ++n) {
+        int lRs = 1 + (n - 1) * dC, lRe = lRs + dC - 1;
+        double s = 0.0;
+        for (int m = lRs; m <= lRe; ++m) s = s + in[m - 1];
+        for (int m = lRs; m <= lRe; ++m) out[m - 1] = s / dC;
+    }
+}
+// CalcSmoothE (ringav.F90:203-336) for the LFM axis
+static void CalcSmoothE(const Model& M, const Grid& G, const State& S, Arr& SmoothE, int XPOLE) {
+    const int Np = M.R.Np;
+    const int fDIRS[2] = {JDIR, IDIR}, eDIRS[2] = {IDIR, JDIR};
+    const double eScls[2] = {1.0, -1.0};
+#pragma omp parallel for schedule(static)
+    for (int nS = M.R.nSi; nS <= M.R.nSe + 1; ++nS) {
+        std::vector<double> bFlx(3 * Np), dEr(3 * Np), rFlx(Np), raFlx(Np), dFlx(Np);
+        for (int nR = 1; nR <= M.R.NumR; ++nR) {
+            int NumCh = M.R.Nch[nR - 1], dC = Np / NumCh;
+            for (int q = 0; q < Np; ++q) {   // PullRingI (ringutils.F90:753-787)
+                int k = G.ks + q;
+                if (XPOLE == SPOLE) {
+                    bFlx[q] = S.magFlux(nS, G.js + nR - 1, k, IDIR);
+                    bFlx[Np + q] = S.magFlux(nS, G.js + nR, k, JDIR);
+                    bFlx[2 * Np + q] = S.magFlux(nS, G.js + nR - 1, k, KDIR);
+                } else {
+                    for (int d = 0; d < 3; ++d) bFlx[d * Np + q] = S.magFlux(nS, G.je - nR + 1, k, d + 1);
+                }
+            }
+            std::fill(dEr.begin(), dEr.end(), 0.0);
+            for (int d = 0; d < 2; ++d) {
+                int fD = fDIRS[d], eD = eDIRS[d];
+                double eScl = eScls[d], cFT[NFTMAX + 1][2];
+                for (int q = 0; q < Np; ++q) rFlx[q] = bFlx[(fD - 1) * Np + q];
+                CleanRing(M, rFlx.data(), cFT, M.R.NFTMAG);
+                ChunkAverage(rFlx.data(), raFlx.data(), Np, NumCh);
+                ReconstructRing(M, raFlx.data(), NumCh);
+                DirtyRing(M, raFlx.data(), cFT, M.R.NFTMAG);
+                for (int q = 0; q < Np; ++q) dFlx[q] = raFlx[q] - bFlx[(fD - 1) * Np + q];
+                for (int n = 1; n <= NumCh; ++n) {
+                    int lRs = 1 + (n - 1) * dC;
+                    double cumFlx = -dFlx[lRs - 1];
+                    for (int m = 2; m <= dC; ++m) {
+                        dEr[(eD - 1) * Np + lRs + m - 2] = eScl * cumFlx;
+                        cumFlx = cumFlx - dFlx[lRs + m - 2];
+                    }
+                }
+            }
+            for (int q = 0; q < Np; ++q) {
+                int k = G.ks + q;
+                if (XPOLE == SPOLE) {
+                    SmoothE(nS, G.js + nR, k, IDIR) = dEr[q];
+                    SmoothE(nS, G.js + nR - 1, k, JDIR) = dEr[Np + q];
+                    SmoothE(nS, G.js + nR - 1, k, KDIR) = dEr[2 * Np + q];
+                } else {
+                    for (int d = 0; d < 3; ++d) SmoothE(nS, G.je - nR + 1, k, d + 1) = dEr[d * Np + q];
+                }
+            }
+            if (XPOLE == SPOLE) {
+                SmoothE(nS, G.js + nR, G.ke + 1, IDIR) = SmoothE(nS, G.js + nR, G.ks, IDIR);
+                SmoothE(nS, G.js + nR - 1, G.ke + 1, JDIR) = SmoothE(nS, G.js + nR - 1, G.ks, JDIR);
+            } else {
+                SmoothE(nS, G.je - nR + 1, G.ke + 1, IDIR) = SmoothE(nS, G.je - nR + 1, G.ks, IDIR);
+                SmoothE(nS, G.je - nR + 1, G.ke + 1, JDIR) = SmoothE(nS, G.je - nR + 1, G.ks, JDIR);
+            }
+        }
+    }
+}
+// PoleE (ringav.F90:376-411) for the LFM axis, then FixEFieldLFM (gamdebug.F90:149-175)
+static void PoleE(const Model& M, const Grid& G, Arr& E) {
+    const int Np = M.R.Np;
+    for (int nS = M.R.nSi; nS <= M.R.nSe + 1; ++nS) {
+        auto pole = [&](int j) {
+            double s = 0.0;
+            for (int k = G.ks; k <= G.ke; ++k) s = s + E(nS, j, k, IDIR);
+            double avg = s / Np;
+            for (int k = G.ksg; k <= G.keg; ++k) { E(nS, j, k, KDIR) = 0.0; E(nS, j, k, IDIR) = avg; }
+        };
+        if (M.R.doS) pole(G.js);
+        if (M.R.doE) pole(G.je + 1);
+    }
+    for (int j = G.js; j <= G.je + 1; ++j)
+        for (int i = G.is; i <= G.ie + 1; ++i) {
+            double Ei = 0.5 * (E(i, j, G.ks, IDIR) + E(i, j, G.ke + 1, IDIR));
+            double Ej = 0.5 * (E(i, j, G.ks, JDIR) + E(i, j, G.ke + 1, JDIR));
+            E(i, j, G.ks, IDIR) = Ei; E(i, j, G.ke + 1, IDIR) = Ei;
+            E(i, j, G.ks, JDIR) = Ej; E(i, j, G.ke + 1, JDIR) = Ej;
+        }
+}
+// CleanLoops (ringav.F90:339-373): remove the net K flux around the first/last ring
+static void CleanLoops(const Model& M, const Grid& G, State& S) {
+    const int Np = M.R.Np;
+    double tScl = M.R.doFastLoop ? 1.0 : 1.0 / Np;
+    for (int nS = M.R.nSi; nS <= M.R.nSe + 1; ++nS) {
+        auto clean = [&](int nR) {
+            double s = 0.0;
+            for (int k = G.ks; k <= G.ke; ++k) s = s + S.magFlux(nS, nR, k, KDIR);
+            double avgFlx = s / Np;
+            for (int k = G.ks; k <= G.ke + 1; ++k) S.magFlux(nS, nR, k, KDIR) = S.magFlux(nS, nR, k, KDIR) - tScl * avgFlx;
+        };
+        if (M.R.doS) clean(G.js);
+        if (M.R.doE) clean(G.je);
+    }
+}
+// SmoothGas (ringav.F90:82-200), single fluid, no shift, no velocity cleaning
+static void SmoothGas(const Model& M, const Grid& G, State& S, int XPOLE) {
+    const int Np = M.R.Np;
+#pragma omp parallel for schedule(static)
+    for (int nS = M.R.nSi; nS <= M.R.nSe; ++nS) {
+        std::vector<double> rW(NVAR * Np), raW(NVAR * Np);
+        for (int nR = 1; nR <= M.R.NumR; ++nR) {
+            int NumCh = M.R.Nch[nR - 1];
+            int jR = (XPOLE == SPOLE) ? G.js + nR - 1 : G.je - nR + 1;
+            for (int q = 0; q < Np; ++q)
+                for (int v = 0; v < NVAR; ++v) rW[v * Np + q] = S.Gas(nS, jR, G.ks + q, v + 1);
+            for (int q = 0; q < Np; ++q) {   // Gas2Ring (ringutils.F90:800-826)
+                double D = fmaxd(rW[q], M.dFloor);
+                double Mom[3] = {rW[Np + q], rW[2 * Np + q], rW[3 * Np + q]};
+                double E = rW[4 * Np + q];
+                double KinE = 0.5 * dot3(Mom, Mom) / D;
+                double P = fmaxd((M.gamma - 1) * (E - KinE), M.pFloor);
+                double IntE = P / (M.gamma - 1);
+                rW[q] = D;
+                rW[4 * Np + q] = M.R.doMassRA ? M.gamma * P : IntE;
+            }
+            for (int v = 0; v < NVAR; ++v) ChunkAverage(&rW[v * Np], &raW[v * Np], Np, NumCh);
+            for (int v = 0; v < NVAR; ++v) ReconstructRing(M, &raW[v * Np], NumCh);
+            for (int q = 0; q < Np; ++q) {   // Ring2Gas (ringutils.F90:829-856)
+                double D = fmaxd(raW[q], M.dFloor);
+                double Mom[3] = {raW[Np + q], raW[2 * Np + q], raW[3 * Np + q]};
+                double P;
+                if (!M.R.doMassRA) P = (M.gamma - 1) * raW[4 * Np + q];
+                else P = (raW[4 * Np + q] / D) * D / M.gamma;
+                P = fmaxd(P, M.pFloor);
+                double KinE = 0.5 * dot3(Mom, Mom) / D;
+                double IntE = P / (M.gamma - 1);
+                raW[q] = D;
+                raW[4 * Np + q] = KinE + IntE;
+            }
+            for (int q = 0; q < Np; ++q)
+                for (int v = 0; v < NVAR; ++v) S.Gas(nS, jR, G.ks + q, v + 1) = raW[v * Np + q];
+        }
+    }
+}
+// RingAverage (ringav.F90:26-79)
+static void RingAverage(const Model& M, const Grid& G, State& S, Arr& SmoothE) {
+    std::fill(SmoothE.d.begin(), SmoothE.d.end(), 0.0);
+    if (M.R.doS) CalcSmoothE(M, G, S, SmoothE, SPOLE);
+    if (M.R.doE) CalcSmoothE(M, G, S, SmoothE, EPOLE);
+    PoleE(M, G, SmoothE);
+    E2Flux(G, S.magFlux, SmoothE, 1.0);
+    if (M.R.doCleanLoop) CleanLoops(M, G, S);
+    bFlux2Fld(M, G, S.magFlux, S.Bxyz);
+    if (M.R.doS) SmoothGas(M, G, S, SPOLE);
+    if (M.R.doE) SmoothGas(M, G, S, EPOLE);
 }
 
 // ---------------------------------------------------------------- one step (gamapp.F90:73-116, mhdgroup.F90:16-76)
@@ -1098,6 +1504,7 @@ static void AdvanceMHD(App& A, double dt) {
     if (M.doMHD) CalcElecField(M, A.G, A.S, A.V.StateHf, A.V.Vf, A.S.Efld);
     CalcStress(M, A.G, A.S, A.V.StateHf, A.V.gFlx, A.V.mFlx, A.V.dGasH, A.V.dGasM);
     applyUpdate(M, A.G, A.S, A.oS, dt, A.V.dGasH, A.V.dGasM, A.S.Efld);
+    if (M.doRing && (M.R.doS || M.R.doE)) RingAverage(M, A.G, A.S, A.V.SmoothE);   // mhdgroup.F90:68-74
 }
 static void stepGamera(App& A) {
     AdvanceMHD(A, A.M.dt);
@@ -1105,7 +1512,7 @@ static void stepGamera(App& A) {
     A.M.t = A.M.t + A.M.dt;
     A.M.dt = CalcDT(A.M, A.G, A.S);
     EnforceBCs(A.M, A.G, A.S);
-    bFlux2Fld(A.G, A.S.magFlux, A.S.Bxyz);
+    bFlux2Fld(A.M, A.G, A.S.magFlux, A.S.Bxyz);
 }
 
 // ---------------------------------------------------------------- setup (init.F90, quadrature.F90, metric.F90)
@@ -1227,6 +1634,75 @@ static void SetDomain(Grid& G) {
     G.isDT = G.is - 1; G.ieDT = G.ie + 1; G.jsDT = G.js - 1; G.jeDT = G.je + 1; G.ksDT = G.ks - 1; G.keDT = G.ke + 1;
 }
 
+// InitRings for the LFM axis (ringutils.F90:37-226): Np = Nkp and the default chunking per ring
+static int InitRingsLFM(Model& M, const Grid& G, int NumR, const int* Nch) {
+    Ring& R = M.R;
+    R.Np = G.Nkp; R.nSi = G.is; R.nSe = G.ie;
+    R.doS = true; R.doE = true;   // untiled: both sides of the axis
+    static const int c8[] = {4}, c16[] = {8}, c32[] = {8, 16}, c64[] = {8, 16, 32, 32},
+                     c128[] = {8, 16, 32, 32, 64, 64, 64, 64}, c256[] = {8, 16, 32, 32, 64, 64, 64, 64, 128, 128, 128, 128},
+                     c512[] = {8, 16, 32, 32, 64, 64, 64, 64, 128, 128, 128, 128, 256, 256, 256, 256};
+    const int* NCr = nullptr;
+    int Nr = 0;
+    switch (R.Np) {
+    case 8: NCr = c8; Nr = 1; break;
+    case 16: NCr = c16; Nr = 1; break;
+    case 32: NCr = c32; Nr = 2; break;
+    case 64: NCr = c64; Nr = 4; break;
+    case 128: NCr = c128; Nr = 8; break;
+    case 256: NCr = c256; Nr = 12; break;
+    case 512: NCr = c512; Nr = 16; break;
+    default: return -1;
+    }
+    R.NumR = NumR > 0 ? NumR : Nr;
+    if (R.NumR > 32) return -1;
+    for (int iR = 1; iR <= R.NumR; ++iR) {
+        int iLim = std::min(iR, Nr);
+        R.Nch[iR - 1] = (Nch && Nch[iR - 1] > 0) ? Nch[iR - 1] : NCr[iLim - 1];
+        if (R.Np % R.Nch[iR - 1] != 0) return -1;
+    }
+    if (R.NumR >= G.Njp) return -1;
+    return 0;
+}
+// RingGridFix for the LFM axis (ringutils.F90:229-377): widen dk of the ring cells by the chunk size and copy
+// the ghost metrics across the axis from the conjugate cells/faces (normals of J and K faces flip sign)
+static void RingGridFix(const Model& M, Grid& G) {
+    const int Np = M.R.Np;
+    for (int iR = 1; iR <= M.R.NumR; ++iR) {
+        int dJ = Np / M.R.Nch[iR - 1];
+        for (int k = G.ksg; k <= G.keg; ++k)
+            for (int i = G.isg; i <= G.ieg; ++i) {
+                if (M.R.doS) G.dk(i, G.js + iR - 1, k) = dJ * G.dk(i, G.js + iR - 1, k);
+                if (M.R.doE) G.dk(i, G.je - iR + 1, k) = dJ * G.dk(i, G.je - iR + 1, k);
+            }
+    }
+    for (int k = G.ksg; k <= G.keg + 1; ++k)
+        for (int i = G.isg; i <= G.ieg + 1; ++i)
+            for (int n = 1; n <= M.nG; ++n)
+                for (int side = 0; side < 2; ++side) {
+                    if (side == 0 && !M.R.doS) continue;
+                    if (side == 1 && !M.R.doE) continue;
+                    int ig = i, kg = k, jg = side == 0 ? G.js - n : G.je + n, ip, jp, kp;
+                    if (kg <= G.keg && ig <= G.ieg) {
+                        lfmIJKcc(M, G, ig, jg, kg, ip, jp, kp);
+                        G.volume(ig, jg, kg) = G.volume(ip, jp, kp);
+                        G.di(ig, jg, kg) = G.di(ip, jp, kp);
+                        G.dj(ig, jg, kg) = G.dj(ip, jp, kp);
+                        G.dk(ig, jg, kg) = G.dk(ip, jp, kp);
+                    }
+                    lfmIJKfc(M, G, IDIR, ig, jg, kg, ip, jp, kp);
+                    for (int c = 0; c < 3; ++c) G.Tf(ig, jg, kg, NORMX + c, IDIR) = G.Tf(ip, jp, kp, NORMX + c, IDIR);
+                    G.face(ig, jg, kg, IDIR) = G.face(ip, jp, kp, IDIR);
+                    int jf = side == 0 ? jg : jg + 1;   // the first outer J ghost face is je+2
+                    lfmIJKfc(M, G, JDIR, ig, jf, kg, ip, jp, kp);
+                    for (int c = 0; c < 3; ++c) G.Tf(ig, jf, kg, NORMX + c, JDIR) = -G.Tf(ip, jp, kp, NORMX + c, JDIR);
+                    G.face(ig, jf, kg, JDIR) = G.face(ip, jp, kp, JDIR);
+                    lfmIJKfc(M, G, KDIR, ig, jg, kg, ip, jp, kp);
+                    for (int c = 0; c < 3; ++c) G.Tf(ig, jg, kg, NORMX + c, KDIR) = -G.Tf(ip, jp, kp, NORMX + c, KDIR);
+                    G.face(ig, jg, kg, KDIR) = G.face(ip, jp, kp, KDIR);
+                }
+}
+
 static int Corners2Grid(const Model& M, Grid& G) {  // init.F90:801-1080
     if ((G.ie - G.is + 1) < vecLen) return -1;
     if (((G.ie - G.is + 1) % 8) != 0) return -2;
@@ -1312,6 +1788,7 @@ static int Corners2Grid(const Model& M, Grid& G) {  // init.F90:801-1080
                 fA = fmaxd(G.face(i, j, k + 1, KDIR), G.face(i, j, k, KDIR));
                 G.dk(i, j, k) = G.volume(i, j, k) / fA;
             }
+    if (M.doRing) RingGridFix(M, G);   // init.F90:967-968
     hi[0] = G.ieg + 1; hi[1] = G.jeg + 1; hi[2] = G.keg + 1; hi[3] = 3;
     G.edge.alloc(4, lo, hi);
     std::fill(G.edge.d.begin(), G.edge.d.end(), 1.0);
@@ -1606,6 +2083,36 @@ static void initBW(const Model& M, Grid& G, State& S, bool fieldAsBackground) { 
     if (M.doMHD && !fieldAsBackground) VectorPot2Flux(G, S, VectorPot_BW, &b);   // prob/doBack = F
 }
 
+// LFM-type spherical corners about the x axis: i -> r (geometric), j -> theta, k -> phi; ghost corners continue
+// the same formulas (theta < 0 or > pi reflects through the axis) and repeat exactly with period Nkp in k
+static void lfmCorner(const double* lfm, const Grid& G, int i, int j, int k, double* x, double* y, double* z) {
+    double rin = lfm[0], rout = lfm[1], q = lfm[2], th0 = lfm[3];
+    double r;
+    if (q == 1.0) r = rin + (rout - rin) * (double)(i - G.is) / G.Nip;
+    else {
+        double dr0 = (rout - rin) * (q - 1.0) / (std::pow(q, (double)G.Nip) - 1.0);
+        r = rin + dr0 * (std::pow(q, (double)(i - G.is)) - 1.0) / (q - 1.0);
+    }
+    double th = th0 + (double)(j - G.js) * (PI - 2.0 * th0) / G.Njp;
+    int kk = ((k - G.ks) % G.Nkp + G.Nkp) % G.Nkp;   // exactly periodic in k
+    double ph = (double)kk * 2.0 * PI / G.Nkp;
+    *x = r * std::cos(th);
+    *y = r * std::sin(th) * std::cos(ph);
+    *z = r * std::sin(th) * std::sin(ph);
+}
+// initUser of the LFM blast wave (ICs/lfmbw.F90:33-104): pressure sphere of radius rC at (x0,y0,z0) with
+// pRat*P0, Az = B0/sqrt(2.0) * (y - x) (sqrt of a default-real literal)
+static void initLFMBW(const Model& M, const Grid& G, State& S, const double* bw) {
+    BWctx b;
+    b.x0 = bw[0]; b.y0 = bw[1]; b.z0 = bw[2];
+    b.Vx0 = b.Vy0 = b.Vz0 = 0.0;
+    b.P0 = bw[3]; b.pRat = bw[4]; b.dRat = 1.0; b.D0 = bw[5]; b.rC = bw[6];
+    b.bScl = bw[7] / (double)std::sqrt(2.0f);
+    b.bSclz = 0.0;
+    GasIC2State(M, G, S, GasIC_BW, &b);
+    if (M.doMHD) VectorPot2Flux(G, S, VectorPot_BW, &b);
+}
+
 }  // namespace orc
 
 // =========================================================================================== C ABI
@@ -1625,6 +2132,18 @@ struct orc_params {
     int nThreads;
     int b0Type;            // 0 none, 1 uniform (b0[0..2]), 2 dipole (moment b0[3] along z, centre b0[0..2])
     double b0[4];
+    // gridType 2: LFM-type spherical grid about the x axis, lfm = {r_in, r_out, radial stretch ratio, theta0}:
+    // r geometric from r_in to r_out over Nip cells, theta uniform on [theta0, pi - theta0], phi uniform on [0, 2 pi)
+    double lfm[4];
+    double dFloor, pFloor;  // sim/dFloor, sim/pFloor (0: the TINY defaults)
+    int doRing;             // ring averaging about the LFM axis (ring/doRing, gid = lfm)
+    int ringNumR;           // ring/Nr (0: the default table for Nkp)
+    int ringNch[32];        // ring/Nc1.. (0: default)
+    int ringRecon;          // ring/rngrec: 0 PLM, 1 PPM (default), 2 PCM
+    int dtActive;           // 1: the timestep domain is the active cells only (problem DT bounds)
+    // icType 2: the LFM blast wave (ICs/lfmbw.F90), bw = {x0, y0, z0, P0, pRat, D0, rC, B0}; its INI/OUTI shells
+    // are bc 3 and its predictor fix is on
+    double bw[8];
 };
 
 void* orc_create(const orc_params* p) {
@@ -1640,8 +2159,15 @@ void* orc_create(const orc_params* p) {
 #endif
     G.Nip = p->Nip; G.Njp = p->Njp; G.Nkp = p->Nkp;
     M.do25D = (G.Nkp == 1);
+    if (p->dFloor > 0) M.dFloor = p->dFloor;
+    if (p->pFloor > 0) M.pFloor = p->pFloor;
     for (int n = 0; n < 6; ++n) G.bc[n] = p->bc[n];
     allocGrid(M, G);
+    if (p->doRing) {   // SetRings before Corners2Grid (init.F90:164-165)
+        M.doRing = true;
+        M.R.recon = p->ringRecon == 0 ? RR_PLM : (p->ringRecon == 2 ? RR_PCM : RR_PPM);
+        if (InitRingsLFM(M, G, p->ringNumR, p->ringNch) != 0) { delete A; return nullptr; }
+    }
     // genGridXML (init.F90:572-798): uniform corners, then the optional warp
     double dx = (p->xyzBds[1] - p->xyzBds[0]) / G.Nip, dy = (p->xyzBds[3] - p->xyzBds[2]) / G.Njp,
            dz = (p->xyzBds[5] - p->xyzBds[4]) / G.Nkp;
@@ -1655,14 +2181,22 @@ void* orc_create(const orc_params* p) {
                     double yw = y + a * std::sin(2 * PI * z) * std::sin(2 * PI * x);
                     double zw = z + a * std::sin(2 * PI * x) * std::sin(2 * PI * y);
                     x = xw; y = yw; z = zw;
+                } else if (p->gridType == 2) {
+                    lfmCorner(p->lfm, G, i, j, k, &x, &y, &z);
                 }
                 G.xyz(i, j, k, 1) = x; G.xyz(i, j, k, 2) = y; G.xyz(i, j, k, 3) = z;
             }
     SetDomain(G);
+    if (p->dtActive) { G.isDT = G.is; G.ieDT = G.ie; G.jsDT = G.js; G.jeDT = G.je; G.ksDT = G.ks; G.keDT = G.ke; }
     if (Corners2Grid(M, G) != 0) { delete A; return nullptr; }
     allocState(M, G, A->S);
     allocState(M, G, A->oS);
     if (p->icType == 0) initOT2D(M, G, A->S);
+    else if (p->icType == 2) {
+        M.predFixLFM = true;
+        M.bwD0 = p->bw[5]; M.bwP0 = p->bw[3];
+        initLFMBW(M, G, A->S, p->bw);
+    }
     else initBW(M, G, A->S, p->b0Type == 1);
     if (p->b0Type != 0) {   // CalcGridInfo: AddB0 after the IC (init.F90:180-184)
         M.doBackground = true;
@@ -1671,7 +2205,7 @@ void* orc_create(const orc_params* p) {
         AddB0(M, G, &bc);
     }
     // CalcGridInfo (init.F90:204-244)
-    if (M.doMHD) bFlux2Fld(G, A->S.magFlux, A->S.Bxyz);
+    if (M.doMHD) bFlux2Fld(M, G, A->S.magFlux, A->S.Bxyz);
     EnforceBCs(M, G, A->S);
     A->oS.Gas.d = A->S.Gas.d; A->oS.magFlux.d = A->S.magFlux.d; A->oS.Bxyz.d = A->S.Bxyz.d;
     A->oS.time = A->S.time;
@@ -1688,6 +2222,7 @@ void* orc_create(const orc_params* p) {
     V.dGasM.alloc(4, lo, hi);
     hi[3] = 5;
     V.dGasH.alloc(4, lo, hi);
+    if (M.doRing) { hi[3] = 3; V.SmoothE.alloc(4, lo, hi); }
     allocState(M, G, V.StateHf);
     return A;
 }
@@ -1716,6 +2251,7 @@ static Arr* lookup(App* A, const char* name) {
         {"dk", &A->G.dk}, {"volume", &A->G.volume}, {"tf", &A->G.Tf}, {"te", &A->G.Te}, {"teb", &A->G.Teb},
         {"face", &A->G.face}, {"edge", &A->G.edge},
         {"fcb0", &A->G.fcB0}, {"edgb0", &A->G.edgB0}, {"b0", &A->G.B0}, {"bflux0", &A->G.bFlux0}, {"dpb0", &A->G.dpB0},
+        {"smoothe", &A->V.SmoothE},
     };
     for (auto& t : tab) if (std::strcmp(t.n, name) == 0) return t.a;
     return nullptr;
@@ -1734,7 +2270,11 @@ int orc_set(void* h, const char* name, const double* in) {
     return 0;
 }
 // Recompute State%Bxyz from State%magFlux (bFlux2Fld) after a host-side edit.
-void orc_bflux2fld(void* h) { App* A = (App*)h; bFlux2Fld(A->G, A->S.magFlux, A->S.Bxyz); bFlux2Fld(A->G, A->oS.magFlux, A->oS.Bxyz); }
+void orc_bflux2fld(void* h) {
+    App* A = (App*)h;
+    bFlux2Fld(A->M, A->G, A->S.magFlux, A->S.Bxyz);
+    bFlux2Fld(A->M, A->G, A->oS.magFlux, A->oS.Bxyz);
+}
 
 double orc_divb(void* h) {  // gridutils.F90:717-770
     App* A = (App*)h;

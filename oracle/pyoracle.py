@@ -17,9 +17,11 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "_build", "libgamora.so")
 
-IC_OT2D, IC_BW = 0, 1
-GRID_UNIFORM, GRID_WARP = 0, 1
-BC_PERIODIC, BC_ZEROGRAD = 0, 1
+IC_OT2D, IC_BW, IC_LFMBW = 0, 1, 2
+GRID_UNIFORM, GRID_WARP, GRID_LFM = 0, 1, 2
+BC_PERIODIC, BC_ZEROGRAD, BC_LFMPOLE, BC_LFMBW = 0, 1, 2, 3
+# the reference's LFM blast-wave deck (tests/gamera/lfmbw.xml): prob x0, y0, z0, P0, pRat, D0, rC, B0
+LFMBW_DECK = (-50.0, 30.0, 0.0, 0.1, 10.0, 1.0, 20.0, 1.0)
 RM_8CENT, RM_7UP = 0, 1
 
 
@@ -33,6 +35,9 @@ class OrcParams(C.Structure):
         ("doMHD", C.c_int), ("doBoris", C.c_int), ("rmeth", C.c_int), ("doLFMLim", C.c_int),
         ("bc", C.c_int * 6), ("nThreads", C.c_int),
         ("b0Type", C.c_int), ("b0", C.c_double * 4),
+        ("lfm", C.c_double * 4), ("dFloor", C.c_double), ("pFloor", C.c_double),
+        ("doRing", C.c_int), ("ringNumR", C.c_int), ("ringNch", C.c_int * 32), ("ringRecon", C.c_int),
+        ("dtActive", C.c_int), ("bw", C.c_double * 8),
     ]
 
 
@@ -94,6 +99,7 @@ def array_shapes(Nip, Njp, Nkp, nG=4):
         "xyz": f + (3,), "xyzcc": c + (3,), "xfc": f + (3, 3), "di": c, "dj": c, "dk": c, "volume": c,
         "tf": f + (9, 3), "te": f + (9, 3), "teb": f + (4, 3), "face": f + (3,), "edge": f + (3,),
         "fcb0": c + (3, 3), "edgb0": c + (2, 3), "b0": c + (3,), "bflux0": c + (3,), "dpb0": c + (3,),
+        "smoothe": c + (3,),
     }
 
 
@@ -102,11 +108,25 @@ class Oracle:
 
     def __init__(self, Nip, Njp, Nkp, ic="OT2D", grid="uniform", bounds=None, warp_amp=0.0, CFL=0.3,
                  gamma=5.0 / 3.0, pdmb=0.75, Vd0=0.5, cHogH=0.25, cHogM=0.25, Ca=1.0e12, tFin=1.0e30,
-                 doMHD=True, doBoris=False, rmeth="8CENT", doLFMLim=True, bc=None, threads=0, b0=None):
+                 doMHD=True, doBoris=False, rmeth="8CENT", doLFMLim=True, bc=None, threads=0, b0=None,
+                 lfm=None, dFloor=0.0, pFloor=0.0, ring=None, dtActive=False, bw=LFMBW_DECK):
         p = OrcParams()
         p.Nip, p.Njp, p.Nkp = Nip, Njp, Nkp
-        p.icType = {"OT2D": IC_OT2D, "BW": IC_BW}[ic]
-        p.gridType = {"uniform": GRID_UNIFORM, "warp": GRID_WARP}[grid]
+        p.icType = {"OT2D": IC_OT2D, "BW": IC_BW, "LFMBW": IC_LFMBW}[ic]
+        p.gridType = {"uniform": GRID_UNIFORM, "warp": GRID_WARP, "lfm": GRID_LFM}[grid]
+        if lfm is not None:   # (r_in, r_out, radial stretch ratio, theta0)
+            for n in range(4):
+                p.lfm[n] = lfm[n]
+        p.dFloor, p.pFloor = dFloor, pFloor
+        if ring is not None:  # dict(NumR=..., Nch=[...], recon="PPM"|"PLM"|"PCM")
+            p.doRing = 1
+            p.ringNumR = ring.get("NumR", 0)
+            for n, c in enumerate(ring.get("Nch", [])):
+                p.ringNch[n] = c
+            p.ringRecon = {"PLM": 0, "PPM": 1, "PCM": 2}[ring.get("recon", "PPM")]
+        p.dtActive = int(dtActive)
+        for n in range(8):
+            p.bw[n] = bw[n]
         if bounds is None:
             bounds = (0.0, 1.0, 0.0, 1.0, 0.0, 1.0)
         for n in range(6):
@@ -139,7 +159,8 @@ class Oracle:
         self.shape = (Nip, Njp, Nkp)
         self.h = lib().orc_create(C.byref(p))
         if not self.h:
-            raise ValueError("oracle grid setup rejected the size (Nip must be >= 16 and a multiple of 8)")
+            raise ValueError("oracle set-up rejected the problem (Nip must be >= 16 and a multiple of 8; ring "
+                             "averaging needs Nkp in 8..512 a power of two and fewer rings than Njp)")
         self.shapes = array_shapes(Nip, Njp, Nkp)
 
     def close(self):

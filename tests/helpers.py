@@ -53,6 +53,11 @@ def problem(kind, n=(32, 32, 4), **kw):
     elif kind == "bw":
         okw = dict(ic="BW", grid="warp", warp_amp=0.04, bounds=(-0.5, 0.5, -0.5, 0.5, -0.5, 0.5),
                    CFL=0.3, bc=[1] * 6)
+    elif kind == "lfmbw":
+        # the reference's LFM blast-wave deck (tests/gamera/lfmbw.xml) on a spherical LFM-type grid
+        okw = dict(ic="LFMBW", grid="lfm", lfm=(10.0, 100.0, 1.03, 0.05), CFL=0.3, pdmb=1.0, rmeth="7UP",
+                   dFloor=1e-4, pFloor=1e-6, doBoris=True, Ca=10.0, bc=[3, 3, 2, 2, 0, 0],
+                   ring=dict(NumR=4, Nch=[8, 16, 32, 32]), dtActive=True)
     else:
         raise ValueError(kind)
     okw.update(kw)
@@ -62,6 +67,16 @@ def problem(kind, n=(32, 32, 4), **kw):
             mkw[k] = okw[k]
     if okw.get("b0") is not None:
         mkw["doBackground"] = True
+    if okw.get("ring") is not None:
+        mkw["ring"] = okw["ring"]
+    if okw.get("ic") == "LFMBW":
+        mkw["predFixLFM"] = True
+        mkw["bwD0"], mkw["bwP0"] = 1.0, 0.1
+    for k in ("dFloor", "pFloor"):
+        if okw.get(k):
+            mkw[k] = okw[k]
+    if okw.get("dtActive"):
+        mkw["dtActive"] = True
     if okw.get("doBoris"):
         mkw["Ca"] = okw["Ca"]
     mkw.setdefault("tFin", okw.get("tFin", 1.0e30))

@@ -35,6 +35,9 @@ CASES = [
     # a dipole background centred off the domain on top of the blast-wave field, with Boris
     ("bw_bg_dipole", "bw", (32, 16, 16), dict(b0=("dipole", 0.05, (-1.0, 0.1, 0.2)))),
     ("bw_bg_dipole_boris", "bw", (16, 16, 16), dict(b0=("dipole", 0.05, (-1.0, 0.1, 0.2)), doBoris=True, Ca=2.0)),
+    # LFM-type spherical grid with ring averaging about the axis, the axis BCs and the LFM blast wave's
+    # fixed shells and predictor fix (the reference's lfmbw test problem)
+    ("lfmbw", "lfmbw", (32, 24, 64), {}),
 ]
 
 
@@ -187,3 +190,34 @@ def test_fp32_flux_error_background(gpu_lib, oracle_lib):
             den = np.abs(b[..., v]).sum()
             l1 = np.abs(a[..., v] - b[..., v]).sum() / den if den > 0 else np.abs(a[..., v]).mean()
             assert l1 <= 1e-5, (v, l1)
+
+
+def test_lfmbw_resynced_steps(gpu_lib, oracle_lib):
+    """Ring averaging, axis BCs and the LFM blast wave's shells over re-synchronised steps."""
+    o, g = oracle_and_gpu("lfmbw", (32, 24, 64))
+    with g:
+        for s in range(4):
+            o.step()
+            dt, ts, t = g.step()
+            sc = o.scalars()
+            assert abs(dt - sc["dt"]) <= TOL * sc["dt"], (s, dt, sc["dt"])
+            _cmp(o, g, ["gas", "magflux", "bxyz", "efld"], where=f"step {s} ")
+            resync(o, g)
+
+
+def test_lfmbw_k_periodicity(gpu_lib, oracle_lib):
+    """The reference's testFields (tests/gamera/testfields.pf) on the device run: after free-running steps
+    the K faces of magFlux and the I/J edges of Efld at ks and ke+1 agree exactly, and the trajectory
+    follows the oracle's."""
+    o, g = oracle_and_gpu("lfmbw", (32, 24, 64))
+    Ni, Nj, Nk, G = 32, 24, 64, 4
+    i0, i1, j0, j1, ks, ke = G, G + Ni - 1, G, G + Nj - 1, G, G + Nk - 1
+    with g:
+        o.step(10)
+        g.run_steps(10)
+        mf, e = g.fetch("magflux"), g.fetch("efld")
+        assert np.abs(mf[i0:i1 + 1, j0:j1 + 1, ks, 2] - mf[i0:i1 + 1, j0:j1 + 1, ke + 1, 2]).max() == 0.0
+        assert np.abs(e[i0:i1 + 1, j0:j1 + 2, ks, 0] - e[i0:i1 + 1, j0:j1 + 2, ke + 1, 0]).max() == 0.0
+        assert np.abs(e[i0:i1 + 2, j0:j1 + 1, ks, 1] - e[i0:i1 + 2, j0:j1 + 1, ke + 1, 1]).max() == 0.0
+        for v, err in enumerate(per_var_rel(g.fetch("gas"), o.get("gas"))):
+            assert err < 1e-8, (v, err)

@@ -136,3 +136,29 @@ def test_background_uniform_equilibrium(oracle_lib):
     assert np.abs(g[..., 1:4]).max() <= 1e-13
     assert np.abs(g[..., 0] - 1.0).max() <= 1e-13
     assert np.abs(o.get("magflux")).max() <= 1e-15
+
+
+def test_lfm_ring_k_periodicity(oracle_lib):
+    """testFields (tests/gamera/testfields.pf) on the LFM blast wave with ring averaging: after the run the
+    K faces of Tf, face and magFlux, the I/J edges of Te, Teb, edge and Efld, and the cell volumes at ks
+    and ke+1 agree exactly; div B stays at round-off."""
+    from helpers import problem
+    n = (32, 24, 64)
+    okw, _ = problem("lfmbw", n)
+    o = oracle_lib.Oracle(*n, **okw)
+    d0 = o.divb()
+    o.step(20)
+    G = 4
+    i0, i1, j0, j1, ks, ke = G, G + n[0] - 1, G, G + n[1] - 1, G, G + n[2] - 1
+    I, J, Ip, Jp = slice(i0, i1 + 1), slice(j0, j1 + 1), slice(i0, i1 + 2), slice(j0, j1 + 2)
+    for name in ("tf", "face", "magflux"):
+        a = o.get(name)[..., 2]
+        assert np.abs(a[I, J, ks] - a[I, J, ke + 1]).max() == 0.0, name
+    for name in ("te", "teb", "edge", "efld"):
+        a = o.get(name)
+        assert np.abs(a[..., 0][I, Jp, ks] - a[..., 0][I, Jp, ke + 1]).max() == 0.0, name
+        assert np.abs(a[..., 1][Ip, J, ks] - a[..., 1][Ip, J, ke + 1]).max() == 0.0, name
+    v = o.get("volume")
+    assert np.abs(v[I, J, ks] - v[I, J, ke + 1]).max() == 0.0
+    scale = np.abs(o.get("magflux")).max() * n[0] * n[1] * n[2]
+    assert o.divb() <= d0 + 1e-13 * scale
