@@ -9,7 +9,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libgamgpu.so")
-SOURCES = ["gam_capi.cu", "gam_step.cu", "gam_flux.cu", "gam_efield.cu", "gam_init.cu", "gam_noalloc.cu"]
+SOURCES = ["gam_capi.cu", "gam_step.cu", "gam_flux.cu", "gam_efield.cu", "gam_init.cu", "gam_ring.cu",
+           "gam_noalloc.cu"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 

@@ -97,12 +97,26 @@ int upload_background(gam_gpu* G, const double* fcB0, const double* edgB0, const
 
 int check_model(const gam_model_c* m) {
     if (!m) return GAM_ERR_ARG;
-    if (m->doGrav || m->doResistive || m->doRing || m->doMultiF || m->doAB3 || m->nSpc != 0 ||
+    if (m->doGrav || m->doResistive || m->doMultiF || m->doAB3 || m->nSpc != 0 ||
         m->hasHooks)
         return GAM_ERR_UNSUPPORTED;
     if (m->nG != 4 || m->Nip < 16 || m->Njp < 1 || m->Nkp < 1) return GAM_ERR_ARG;
-    for (int n = 0; n < 6; ++n)
-        if (m->bc[n] != GAM_BC_PERIODIC && m->bc[n] != GAM_BC_ZEROGRAD) return GAM_ERR_UNSUPPORTED;
+    for (int n = 0; n < 6; ++n) {
+        int b = m->bc[n];
+        bool ok = b == GAM_BC_PERIODIC || b == GAM_BC_ZEROGRAD || (b == GAM_BC_LFMPOLE && (n == 2 || n == 3)) ||
+                  (b == GAM_BC_LFMBW && n < 2);
+        if (!ok) return GAM_ERR_UNSUPPORTED;
+        if (b == GAM_BC_LFMPOLE && !m->doRing) return GAM_ERR_ARG;   // the axis maps need Model%Ring
+    }
+    if (m->doRing) {   // InitRings checks (ringutils.F90:203-225) and the device ring sizes
+        int Np = m->Nkp;
+        if (Np < 8 || Np > 512 || (Np & (Np - 1)) != 0) return GAM_ERR_ARG;
+        if (m->ringNumR < 1 || m->ringNumR > 32 || m->ringNumR >= m->Njp) return GAM_ERR_ARG;
+        for (int r = 0; r < m->ringNumR; ++r)
+            if (m->ringNch[r] < 1 || (Np % m->ringNch[r]) != 0) return GAM_ERR_ARG;
+        if (m->ringRecon < GAM_RING_PLM || m->ringRecon > GAM_RING_PCM) return GAM_ERR_ARG;
+        if (!m->ringDoS && !m->ringDoE) return GAM_ERR_ARG;
+    }
     if (m->rmeth != GAM_RM_8CENT && m->rmeth != GAM_RM_7UP) return GAM_ERR_ARG;
     return GAM_OK;
 }
@@ -123,10 +137,22 @@ int alloc_handle(gam_gpu* G, const gam_model_c* m) {
     p.fixedTimestep = m->fixedTimestep;
     p.doBackground = m->doBackground ? 1 : 0;
     for (int n = 0; n < 6; ++n) p.bc[n] = m->bc[n];
+    p.doRing = m->doRing ? 1 : 0;
+    p.ringDoS = m->doRing && m->ringDoS ? 1 : 0;
+    p.ringDoE = m->doRing && m->ringDoE ? 1 : 0;
+    p.predFixLFM = m->predFixLFM ? 1 : 0;
+    p.dtActive = m->dtActive ? 1 : 0;
+    p.bwD0 = m->bwD0; p.bwP0 = m->bwP0;
+    if (m->doRing) {
+        h.ring.NumR = m->ringNumR;
+        for (int r = 0; r < 32; ++r) h.ring.Nch[r] = r < m->ringNumR ? m->ringNch[r] : 0;
+        h.ring.recon = m->ringRecon;
+    }
 
     CK(cudaGetDevice(&h.device));
     flux_kernels_init();
     efield_kernels_init();
+    ring_kernels_init();
     CK(cudaStreamCreateWithFlags(&h.stream, cudaStreamNonBlocking));
     h.ownStream = true;
     const size_t planes = 11 * 3 + 10 + 14 + 9 + 24 + 91;
@@ -165,6 +191,11 @@ int alloc_handle(gam_gpu* G, const gam_model_c* m) {
     for (int d = 0; d < 3; ++d) for (int c = 0; c < 4; ++c) h.Teb[d][c] = take();
     for (int x = 0; x < 3; ++x) h.xyz[x] = take();
     if ((size_t)(q - h.pool) != (size_t)L.E * planes) return GAM_ERR_ARG;
+    if (p.doRing) {   // ring-average smoothing E field, 3 contiguous planes
+        CK(cudaMalloc(&h.ringpool, sizeof(double) * L.E * 3));
+        CK(cudaMemsetAsync(h.ringpool, 0, sizeof(double) * L.E * 3, h.stream));
+        for (int x = 0; x < 3; ++x) h.SmoothE[x] = h.ringpool + (size_t)x * L.E;
+    }
     if (p.doBackground) {   // fcB0 (9), edgB0 (6), B0, bFlux0, dpB0 (3 each)
         const size_t bgPlanes = 24;
         CK(cudaMalloc(&h.bgpool, sizeof(double) * L.E * bgPlanes));
@@ -320,7 +351,7 @@ static int create_from_corners(gam_gpu_t** out, const gam_model_c* m, const doub
     *out = nullptr;
     int rc = check_model(m);
     if (rc) return rc;
-    if (ic != GAM_IC_OT2D && ic != GAM_IC_BW) return GAM_ERR_ARG;
+    if (ic != GAM_IC_OT2D && ic != GAM_IC_BW && ic != GAM_IC_LFMBW) return GAM_ERR_ARG;
     if ((m->Nip % 8) != 0) return GAM_ERR_ARG;   // Corners2Grid divisibility check (init.F90:830-834)
     if ((bg != nullptr) != (m->doBackground != 0)) return GAM_ERR_ARG;
     gam_gpu* G = new (std::nothrow) gam_gpu();
@@ -582,6 +613,7 @@ int gam_gpu_fetch(gam_gpu_t* G, const char* name, double* out, long long n) {
     else if (h.bgpool && s == "b0") put(h.B0, 3);
     else if (h.bgpool && s == "bflux0") put(h.bFlux0, 3);
     else if (h.bgpool && s == "dpb0") put(h.dpB0, 3);
+    else if (h.ringpool && s == "smoothe") put(h.SmoothE, 3);
     else return GAM_ERR_ARG;
     if (n < (long long)np * e.n()) return GAM_ERR_ARG;
     int rc = d2h_planes(G, pl, np, out, e);
@@ -597,6 +629,7 @@ void gam_gpu_destroy(gam_gpu_t* G) {
     destroy_graphs(h);
     if (h.pool) cudaFree(h.pool);
     if (h.bgpool) cudaFree(h.bgpool);
+    if (h.ringpool) cudaFree(h.ringpool);
     if (h.f32pool) cudaFree(h.f32pool);
     if (G->stage) cudaFree(G->stage);
     if (G->scratch) cudaFree(G->scratch);

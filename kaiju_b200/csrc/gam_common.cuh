@@ -21,7 +21,7 @@ constexpr double PI = 3.14159265358979323846264338327950288;
 
 enum { IDIR = 0, JDIR = 1, KDIR = 2 };
 enum { RM_8CENT = 0, RM_7UP = 1 };
-enum { BC_PERIODIC = 0, BC_ZEROGRAD = 1 };
+enum { BC_PERIODIC = 0, BC_ZEROGRAD = 1, BC_LFMPOLE = 2, BC_LFMBW = 3 };
 
 struct Lay {
     int Nip, Njp, Nkp;     // active cells
@@ -45,6 +45,10 @@ struct Par {
     int doMHD, doBoris, do25D, doLFMLim, rmeth, fixedTimestep;
     int doBackground;      // background field B0 present (Model%doBackground)
     int bc[6];
+    int doRing, ringDoS, ringDoE;   // ring averaging about the LFM axis (Model%doRing, Ring%doS/doE)
+    int predFixLFM;                 // the LFM blast wave's predictor fix
+    int dtActive;                   // CalcDT over the active cells only
+    double bwD0, bwP0;              // gas of the LFM blast wave's fixed shells
 };
 
 // Time-dependent scalars kept on the device so a whole step can be captured and replayed.

@@ -281,16 +281,21 @@ __global__ void k_ic_ot2d(Lay L, Par p, GridP g, StateP s) {
 }
 
 // initBW with the deck defaults (prob.F90:190-298): D0=1, P0=0.1, pRat=100, dRat=1, rC=0.1, B0=1
+// GasIC of the blast waves: a sphere of radius rC at (x0,y0,z0) with dRat*D0 and pRat*P0, at rest
 struct BWGas {
+    double x0, y0, z0, D0, P0, pRat, dRat, rC;
     __device__ void operator()(double x, double y, double z, double* W) const {
-        double R = sqrt(sq(x - 0.0) + sq(y - 0.0) + sq(z - 0.0));
-        double D = 1.0, P = 0.1;
-        if (R <= 0.1) { D = 1.0 * D; P = 100.0 * P; }
+        double R = sqrt(sq(x - x0) + sq(y - y0) + sq(z - z0));
+        double D = D0, P = P0;
+        if (R <= rC) { D = dRat * D; P = pRat * P; }
         W[0] = D; W[1] = 0.0; W[2] = 0.0; W[3] = 0.0; W[4] = P;
     }
 };
+// prob.F90:190-298 deck defaults (the Cartesian blast wave) and tests/gamera/lfmbw.xml (ICs/lfmbw.F90:33-104)
+static const BWGas kBW = {0.0, 0.0, 0.0, 1.0, 0.1, 100.0, 1.0, 0.1};
+static const BWGas kLFMBW = {-50.0, 30.0, 0.0, 1.0, 0.1, 10.0, 1.0, 20.0};
 // GasIC2State (gridutils.F90:144-189) on active cells
-__global__ void k_ic_bw_gas(Lay L, Par p, Corners X, const double* vol, StateP s) {
+__global__ void k_ic_bw_gas(Lay L, Par p, Corners X, const double* vol, StateP s, BWGas ic) {
     long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (t >= (long long)L.Nip * L.Njp * L.Nkp) return;
     int i = L.is() + (int)(t % L.Nip);
@@ -298,7 +303,7 @@ __global__ void k_ic_bw_gas(Lay L, Par p, Corners X, const double* vol, StateP s
     int j = L.js() + (int)(q % L.Njp), k = L.ks() + (int)(q / L.Njp);
     double xyzC[8][3], w[5];
     cellCorners(L, X, i, j, k, xyzC);
-    volumeIntegral(xyzC, BWGas(), w);
+    volumeIntegral(xyzC, ic, w);
     long long c = L.at(i, j, k);
     double dV = vol[c];
     for (int v = 0; v < 5; ++v) w[v] = w[v] / dV;
@@ -486,6 +491,7 @@ int init_grid_from_corners(Handle& h) {
     k_grid_volumes<<<nb(nc, 128), 128, 0, st>>>(L, X, h.volume, cc);
     Out3 fc = {{h.face[0], h.face[1], h.face[2]}};
     k_grid_dl<<<nb(nc, 256), 256, 0, st>>>(L, h.volume, fc, h.di, h.dj, h.dk);
+    if (h.p.doRing) launch_ring_grid_fix(h, st);   // init.F90:967-968, before the edge geometry
     for (int d = 0; d < 3; ++d) {
         int is = 0, ie = L.Ni, js = 0, je = L.Nj, ks = 0, ke = L.Nk;   // maximal bounds (corner index space)
         if (d == 0) { ie = L.Ni - 1; ks = 1; ke = L.Nk - 1; }
@@ -549,7 +555,7 @@ int init_problem(Handle& h, int ic, const BgSpec* bg) {
     } else {
         Corners X = {{h.xyz[0], h.xyz[1], h.xyz[2]}};
         long long n = (long long)L.Nip * L.Njp * L.Nkp;
-        k_ic_bw_gas<<<nb(n, 128), 128, 0, st>>>(L, h.p, X, h.volume, s);
+        k_ic_bw_gas<<<nb(n, 128), 128, 0, st>>>(L, h.p, X, h.volume, s, ic == 2 ? kLFMBW : kBW);
         // prob/doBack (prob.F90:228-269): with a uniform background the blast field is held as B0 and
         // the residual field starts at zero
         bool fieldAsBackground = bg && bg->type == 1;

@@ -10,6 +10,7 @@
 #include <cmath>
 #include "gam_common.cuh"
 #include "gam_step.cuh"
+#include "gam_lfm.cuh"
 #include "gam_kern.cuh"
 
 namespace gam {
@@ -264,6 +265,7 @@ __global__ void k_bflux2fld_ghost(Lay L, GridP g, StateP s) {
 // CellDT (gridutils.F90:49-106) over the dt domain (one ghost layer at physical boundaries), min-reduced
 __global__ void k_calcdt(Lay L, Par p, GridP g, StateP s, Scal* sc) {
     Reg r = {L.is() - 1, L.Nip + 2, L.js() - 1, L.Njp + 2, L.ks() - 1, L.Nkp + 2};
+    if (p.dtActive) r = Reg{L.is(), L.Nip, L.js(), L.Njp, L.ks(), L.Nkp};
     int i, j, k;
     double dtijk = HUGEV * 2.0;
     bool isnan_ = false;
@@ -370,7 +372,32 @@ __global__ void k_bc_i(Lay L, Par p, GridP g, StateP s) {
     int j = (int)(t % nj), k = (int)(t / nj);
     bool cell = (j < L.Nj) && (k < L.Nk);
     int is = L.is(), ie = L.ie(), nG = L.nG;
-    if (p.bc[0] == BC_PERIODIC) {
+    // the LFM blast wave's fixed shells (ICs/lfmbw.F90:141-225): fixed gas; ghost face fluxes are the
+    // conjugate active-shell fluxes scaled by the face areas (J/K signs flip across the axis)
+    auto lfmbwShell = [&](bool inner) {
+        double dApm[3] = {1.0, 1.0, 1.0};
+        if (p.ringDoS && j < L.js()) dApm[1] = dApm[2] = -1.0;
+        if (p.ringDoE && j >= L.je() + 1) dApm[1] = dApm[2] = -1.0;
+        for (int n = 1; n <= nG; ++n) {
+            int ig = inner ? is - n : ie + n;
+            if (cell) {
+                long long c = L.at(ig, j, k);
+                s.gas[0][c] = p.bwD0; s.gas[1][c] = 0.0; s.gas[2][c] = 0.0; s.gas[3][c] = 0.0;
+                s.gas[4][c] = p.bwP0 / (p.gamma - 1.0);
+            }
+            for (int d = 0; d < 3; ++d) {
+                int di = (!inner && d == 0) ? 1 : 0;
+                int ia = inner ? is : ie + di;
+                int jp, kp;
+                lfmFC(L, p.ringDoS, p.ringDoE, d, j, k, jp, kp);
+                long long cg = L.at(ig + di, j, k), ca = L.at(ia, jp, kp);
+                double dA = g.face[d][cg] / g.face[d][ca];
+                s.mf[d][cg] = dApm[d] * dA * s.mf[d][ca];
+            }
+        }
+    };
+    if (p.bc[0] == BC_LFMBW) lfmbwShell(true);
+    else if (p.bc[0] == BC_PERIODIC) {
         for (int n = 1; n <= nG; ++n) {
             long long d = L.at(is - n, j, k), sidx = L.at(ie - n + 1, j, k);
             if (cell) cpcell(s, d, sidx, true);
@@ -383,7 +410,8 @@ __global__ void k_bc_i(Lay L, Par p, GridP g, StateP s) {
             cpmf(s, d, sidx);
         }
     }
-    if (p.bc[1] == BC_PERIODIC) {
+    if (p.bc[1] == BC_LFMBW) lfmbwShell(false);
+    else if (p.bc[1] == BC_PERIODIC) {
         for (int n = 1; n <= nG; ++n) {
             long long d = L.at(ie + n, j, k), sidx = L.at(is + n - 1, j, k);
             if (cell) cpcell(s, d, sidx, true);
@@ -414,7 +442,25 @@ __global__ void k_bc_j(Lay L, Par p, StateP s) {
     int i = (int)(t % ni), k = (int)(t / ni);
     bool cell = (i < L.Ni) && (k < L.Nk);
     int js = L.js(), je = L.je(), nG = L.nG;
-    if (p.bc[2] == BC_PERIODIC) {
+    // lfmIn / lfmOut (bcs.F90:1020-1106): ghosts across the axis from their conjugates
+    auto lfmPole = [&](bool in) {
+        for (int n = 1; n <= nG; ++n) {
+            int jg = in ? js - n : je + n, jp, kp;
+            if (cell) {
+                lfmCC(L, p.ringDoS, p.ringDoE, jg, k, jp, kp);
+                cpcell(s, L.at(i, jg, k), L.at(i, jp, kp), true);
+            }
+            lfmFC(L, p.ringDoS, p.ringDoE, 0, jg, k, jp, kp);
+            s.mf[0][L.at(i, jg, k)] = s.mf[0][L.at(i, jp, kp)];
+            int jf = in ? jg : jg + 1;   // the first outer J ghost face is je+2
+            lfmFC(L, p.ringDoS, p.ringDoE, 1, jf, k, jp, kp);
+            s.mf[1][L.at(i, jf, k)] = -s.mf[1][L.at(i, jp, kp)];
+            lfmFC(L, p.ringDoS, p.ringDoE, 2, jg, k, jp, kp);
+            s.mf[2][L.at(i, jg, k)] = -s.mf[2][L.at(i, jp, kp)];
+        }
+    };
+    if (p.bc[2] == BC_LFMPOLE) lfmPole(true);
+    else if (p.bc[2] == BC_PERIODIC) {
         for (int n = 1; n <= nG; ++n) {
             long long d = L.at(i, js - n, k), sidx = L.at(i, je - n + 1, k);
             if (cell) cpcell(s, d, sidx, true);
@@ -427,7 +473,8 @@ __global__ void k_bc_j(Lay L, Par p, StateP s) {
             cpmf(s, d, sidx);
         }
     }
-    if (p.bc[3] == BC_PERIODIC) {
+    if (p.bc[3] == BC_LFMPOLE) lfmPole(false);
+    else if (p.bc[3] == BC_PERIODIC) {
         for (int n = 1; n <= nG; ++n) {
             long long d = L.at(i, je + n, k), sidx = L.at(i, js + n - 1, k);
             if (cell) cpcell(s, d, sidx, true);
@@ -563,6 +610,7 @@ void launch_bflux2fld(Handle& h, const StateP& s, cudaStream_t st) {
     long long n = (long long)h.L.Ni * h.L.Nj * h.L.Nk;
     k_bflux2fld<<<nblk(n, TPB), TPB, 0, st>>>(h.L, h.gridP(), s);
     h.launches++;
+    if (h.p.doRing) launch_ring_bfix(h, s, st);   // gridutils.F90:298-300
 }
 
 void launch_bcs(Handle& h, const StateP& s, cudaStream_t st) {
@@ -653,6 +701,7 @@ int kernels_per_step(const Handle& h) {
     n += (h.p.do25D ? 2 : 3) + 1;       // fluxes + flux2deltas
     n += 1 + 1 + 1;                     // e2flux/copy, bflux2fld, update gas
     n += 2 + 3 + 1;                     // calcdt + finalize, 3 BC kernels, final bflux2fld
+    n += ring_kernels_per_step(h);
     return n;
 }
 
@@ -694,8 +743,11 @@ int step_enqueue(Handle& h, int cur, cudaEvent_t* ev) {
     }
     k_predict_cells<<<nblk(ncell, TPB), TPB, 0, st>>>(L, p, g, nS, oS, h.H, Wh, Wn, VdV, fc, h.dScal);
     h.launches += 2;
+    if (p.doRing) launch_ring_bfix(h, h.H, st, h.prec == PREC_FP32FLUX);   // bFlux2Fld's ring fix
+    if (p.predFixLFM) launch_predfix_lfm(h, h.H, st, h.prec == PREC_FP32FLUX);   // HackPredictor
     mark(PH_EFIELD);
     enqueue_hot(h, nS, st, ev);
+    if (p.doRing) launch_ring_flux(h, st);   // stress.F90:134-139
     mark(PH_DELTAS);
     FluxP F[3];
     for (int d = 0; d < 3; ++d) {
@@ -711,11 +763,15 @@ int step_enqueue(Handle& h, int cur, cudaEvent_t* ev) {
     // applyUpdate into the oState buffer (which becomes State n+1)
     Vec3P E = {{h.E[0], h.E[1], h.E[2]}};
     long long nface = (long long)(L.Ni + 1) * (L.Nj + 1) * (L.Nk + 1);
+    if (p.doRing && p.doMHD) launch_pole_e(h, h.E, st);   // mhdgroup.F90:139-142
     k_e2flux<<<nblk(nface, TPB), TPB, 0, st>>>(L, p, E, nS, oS, h.dScal);
+    // bFlux2Fld of the update; with ring averaging its ring fix is left to the RingAverage bFlux2Fld,
+    // which recomputes every cell before anything reads a ghost B
     if (p.doMHD) k_bflux2fld<<<nblk(ncell, TPB), TPB, 0, st>>>(L, g, oS);
     else k_copy_b<<<nblk(L.E, 256), 256, 0, st>>>(L, nS, oS);
     k_update_gas<<<nblk(ncell, TPB), TPB, 0, st>>>(L, p, g, nS, oS, dGH, dGM, h.dScal);
     h.launches += 4;
+    if (p.doRing) launch_ring_average(h, oS, st);   // mhdgroup.F90:68-74
     // CalcDT, EnforceBCs, bFlux2Fld on the new state
     mark(PH_DT);
     launch_calcdt(h, oS, 0, st);
@@ -725,6 +781,7 @@ int step_enqueue(Handle& h, int cur, cudaEvent_t* ev) {
     else {
         k_bflux2fld_ghost<<<nblk(ncell, TPB), TPB, 0, st>>>(L, g, oS);
         h.launches++;
+        if (p.doRing) launch_ring_bfix(h, oS, st);
     }
     mark(NPHASE);
     return (int)cudaGetLastError();

@@ -17,9 +17,19 @@ struct F32Planes {
     float* fcB0[3][3]; float* b0n[3]; float* edgB0[3][2];
 };
 
+// Ring-average configuration for the LFM axis (Model%Ring, ringutils.F90:37-226)
+struct RingCfg {
+    int NumR = 0;
+    int Nch[32] = {0};
+    int recon = 1;            // 0 PLM, 1 PPM, 2 PCM
+    int NFTMAG = 1;           // Fourier modes (beyond the 0th) removed from the face fluxes
+    int doCleanLoop = 1, doFastLoop = 1, doMassRA = 0;
+};
+
 struct Handle {
     Lay L;
     Par p;
+    RingCfg ring;
     int device = 0;
     cudaStream_t stream = nullptr;
     bool ownStream = false;
@@ -49,6 +59,9 @@ struct Handle {
     // background field planes (own allocation, only with Model%doBackground), Grid_T layout per plane
     double* bgpool = nullptr;
     double* fcB0[3][3] = {}; double* edgB0[3][2] = {}; double* B0[3] = {}; double* bFlux0[3] = {}; double* dpB0[3] = {};
+    // ring-average smoothing E field (own allocation, only with Model%doRing)
+    double* ringpool = nullptr;
+    double* SmoothE[3] = {};
     // FP32 copies for the FP32-flux mode (allocated on first use)
     float* f32pool = nullptr;
     F32Planes f32{};
@@ -82,6 +95,15 @@ void flux_kernels_init();
 // E field of all edge directions (gam_efield.cu): Mom2Face + tiled EMF
 void enqueue_efield(Handle& h, const StateP& nS, cudaStream_t st);
 void efield_kernels_init();
+// ring averaging about the LFM axis (gam_ring.cu)
+void launch_ring_bfix(Handle& h, const StateP& s, cudaStream_t st, bool withF32 = false);  // RingFlux2FieldFix
+void launch_predfix_lfm(Handle& h, const StateP& s, cudaStream_t st, bool withF32 = false);  // lfmbw PredFix
+void launch_ring_flux(Handle& h, cudaStream_t st);                              // RingFlux + FixGasFluxLFM
+void launch_pole_e(Handle& h, double* const* E, cudaStream_t st);               // PoleE + FixEFieldLFM
+void launch_ring_average(Handle& h, const StateP& s, cudaStream_t st);          // RingAverage
+int ring_kernels_per_step(const Handle& h);
+void launch_ring_grid_fix(Handle& h, cudaStream_t st);                          // RingGridFix
+void ring_kernels_init();
 // allocate the float planes and convert the metrics (first switch to GAM_FP32FLUX)
 int ensure_f32(Handle& h);
 // re-convert the background planes into the float copies (after the background changed)

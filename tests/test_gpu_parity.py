@@ -221,3 +221,23 @@ def test_lfmbw_k_periodicity(gpu_lib, oracle_lib):
         assert np.abs(e[i0:i1 + 2, j0:j1 + 1, ks, 1] - e[i0:i1 + 2, j0:j1 + 1, ke + 1, 1]).max() == 0.0
         for v, err in enumerate(per_var_rel(g.fetch("gas"), o.get("gas"))):
             assert err < 1e-8, (v, err)
+
+
+def test_device_lfm_grid_matches_oracle(gpu_lib, oracle_lib):
+    """Corners2Grid with RingGridFix, the LFM blast-wave IC and the Hatch tail on the device vs the oracle's
+    host set-up, same corners."""
+    from helpers import problem
+    from kaiju_b200 import gamera as gm
+    n = (32, 24, 64)
+    okw, model = problem("lfmbw", n)
+    o = oracle_lib.Oracle(*n, **okw)
+    with gm.GameraGPU.from_corners(model, o.get("xyz"), "LFMBW") as g:
+        for name in ("volume", "xyzcc", "xfc", "face", "edge", "di", "dj", "dk", "tf", "te", "teb",
+                     "gas", "magflux", "bxyz"):
+            errs = per_var_rel(g.fetch(name), o.get(name))
+            assert max(errs) <= 1e-12, (name, errs)
+        sc = o.scalars()
+        assert abs(g.status()["dt"] - sc["dt"]) <= 1e-12 * sc["dt"]
+        o.step(2)
+        g.run_steps(2)
+        _cmp(o, g, ["gas", "magflux"], tol=1e-9, where="after 2 steps ")
