@@ -141,6 +141,9 @@ def peaks():
 # B (3) for the limiter, the volume (1), the face triad (9), the area (1) and the half-state normal
 # flux (1) = 28 doubles, and write 5 gas + 3 magnetic fluxes = 8 doubles: 36 doubles = 288 B.
 FLUX_BYTES_PER_IFACE = 36 * 8
+# FP32-flux path: the same 28 inputs as floats (112 B) and the 8 area-scaled fluxes written as doubles
+# (64 B) = 176 B.
+FLUX_BYTES_PER_IFACE_F32 = 28 * 4 + 8 * 8
 FLUX_FLOPS_PER_IFACE = 700.0
 # Whole-step compulsory traffic per zone-update on a curvilinear grid, FP64: state n and n-1 in,
 # n+1 out (24 doubles) + metrics (volume 1, face 3, edge 3, Tf 27, Te 27, Teb 12, xfc 9, xyzcc 3,
@@ -221,14 +224,16 @@ def run_ours(args, rank, world, local):
     dom = max(ph, key=ph.get)
     n_if = (n + 1) * n * n   # interfaces per direction launch
     flux_launch_ms = ph["fluxes"] / 3.0
-    achieved = FLUX_BYTES_PER_IFACE * n_if / (flux_launch_ms / 1e3) / 1e9
+    fbytes = FLUX_BYTES_PER_IFACE if args.prec == "fp64" else FLUX_BYTES_PER_IFACE_F32
+    achieved = fbytes * n_if / (flux_launch_ms / 1e3) / 1e9
     tpu = traffic_per_unit("k_flux_tile", args.prec)
     roof = {"kernel": "k_flux_tile<double>" if args.prec == "fp64" else "k_flux_tile<float>",
             "bound": "hbm", "achieved": round(achieved, 1), "peak": hbm, "unit": "GB/s",
             "frac": round(achieved / hbm, 4), "traffic": (round(tpu * n_if) if tpu else None),
-            "algorithmic_bytes": FLUX_BYTES_PER_IFACE * n_if, "peak_source": pk_kind,
+            "algorithmic_bytes": fbytes * n_if, "peak_source": pk_kind,
             "launch_ms": round(flux_launch_ms, 4),
-            "fp64_tflops": round(FLUX_FLOPS_PER_IFACE * n_if / (flux_launch_ms / 1e3) / 1e12, 3),
+            ("fp64_tflops" if args.prec == "fp64" else "fp32_tflops"):
+                round(FLUX_FLOPS_PER_IFACE * n_if / (flux_launch_ms / 1e3) / 1e12, 3),
             "fp64_peak_nominal_tflops": FP64_NOMINAL_TFLOPS,
             "dominant_phase": dom, "phase_ms": {k: round(v, 4) for k, v in ph.items()},
             "step_bytes_per_zone": STEP_BYTES_PER_ZONE,

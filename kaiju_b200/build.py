@@ -10,7 +10,13 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libgamgpu.so")
 SOURCES = ["gam_capi.cu", "gam_step.cu", "gam_flux.cu", "gam_efield.cu", "gam_init.cu", "gam_ring.cu",
-           "gam_noalloc.cu"]
+           "gam_noalloc.cu", "gam_flux_f32.cu", "gam_efield_f32.cu"]
+# The FP32-flux kernels use approximate single-precision division and square root (their error budget is
+# the FP32 path's 1e-5 L1 bound); every other unit keeps IEEE arithmetic. These flags touch
+# single-precision operations only.
+FAST_F32 = {"gam_flux_f32.cu", "gam_efield_f32.cu"}
+FAST_F32_FLAGS = ["-prec-div=false", "-prec-sqrt=false", "-ftz=true"]
+OBJDIR = os.path.join(HERE, "_build")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
@@ -31,12 +37,23 @@ def needs_build() -> bool:
 def build(force: bool = False, verbose: bool = False) -> str:
     if not force and not needs_build():
         return LIB
-    cmd = [NVCC, *ARCH, "-O3", "-lineinfo", "-std=c++17", "-shared", "-Xcompiler", "-fPIC",
-           "-I", CSRC, "-I", os.path.join(ROOT, "include"), "-o", LIB, *sources()]
+    os.makedirs(OBJDIR, exist_ok=True)
+    common = [NVCC, *ARCH, "-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC",
+              "-I", CSRC, "-I", os.path.join(ROOT, "include")]
     if verbose:
-        cmd.insert(1, "-Xptxas=-v")
-        print(" ".join(cmd), file=sys.stderr)
-    subprocess.run(cmd, check=True)
+        common.insert(1, "-Xptxas=-v")
+    procs, objs = [], []
+    for src in SOURCES:   # one nvcc per unit, in parallel
+        obj = os.path.join(OBJDIR, src.replace(".cu", ".o"))
+        cmd = common + (FAST_F32_FLAGS if src in FAST_F32 else []) + ["-c", os.path.join(CSRC, src), "-o", obj]
+        if verbose:
+            print(" ".join(cmd), file=sys.stderr)
+        procs.append((src, subprocess.Popen(cmd)))
+        objs.append(obj)
+    failed = [src for src, pr in procs if pr.wait() != 0]
+    if failed:
+        raise subprocess.CalledProcessError(1, "nvcc " + " ".join(failed))
+    subprocess.run([NVCC, *ARCH, "-shared", "-o", LIB, *objs], check=True)
     return LIB
 
 

@@ -1,227 +1,31 @@
-// Interface fluxes (stress.F90:204-429) with shared-memory staging.
-//
-// A CTA of 256 threads owns a 32 x 8 tile of interfaces: 32 consecutive i (one warp per row) by 8
-// rows, the rows running along the sweep direction d for J/K sweeps and along j for the I sweep. It
-// first copies, with coalesced row loads, the stencil footprint -- the tile plus the 4-cell halo of
-// the reconstruction stencil (half-state primitives, half-state B, volumes) and the 2-cell halo of
-// the limiter stencil (state-n primitives and B) -- into shared memory, then every thread
-// reconstructs, limits and evaluates the kinetic fluxes of its interface from shared memory. The
-// per-interface data (face triad, area, normal flux) is read once, coalesced, from HBM.
-//
-// The arithmetic type T is double for the plain path and float for the FP32-flux path (staged
-// values are converted while they are copied in).
-#include <cstdio>
-#include <type_traits>
-#include "gam_common.cuh"
-#include "gam_kern.cuh"
-#include "gam_step.cuh"
+// Interface fluxes (stress.F90:204-429), FP64 path; the tile kernel is in gam_flux_tile.cuh.
+#include "gam_flux_tile.cuh"
 
 namespace gam {
 
-constexpr int FL = 32;   // interfaces per tile along i
-constexpr int FR = 8;    // rows per tile
-
-template <int D> __host__ __device__ constexpr int rec_box() { return D == 0 ? (FL + 8) * FR : FL * (FR + 7); }
-template <int D> __host__ __device__ constexpr int lim_box() { return D == 0 ? (FL + 4) * FR : FL * (FR + 3); }
-template <typename S, int D> constexpr size_t flux_smem() { return sizeof(S) * (9 * rec_box<D>() + 8 * lim_box<D>()); }
-
-template <typename T, typename S, int D, bool MHD, bool BG>
-__global__ void __launch_bounds__(256, 2) k_flux_tile(Lay L, Par p, FluxSrc<S> in, StateP h, FluxP F, Reg r) {
-    extern __shared__ __align__(16) unsigned char smraw[];
-    S* sRec = reinterpret_cast<S*>(smraw);   // staged in the storage type, converted to T on use
-    S* sLim = sRec + 9 * rec_box<D>();
-    constexpr int RB = rec_box<D>(), LB = lim_box<D>();
-    const int tid = threadIdx.x, lane = tid & 31, row = tid >> 5;
-    const int i0 = r.i0 + blockIdx.x * FL;
-    int i = i0 + lane, j, k, a0;
-    if (D == 2) { a0 = r.k0 + blockIdx.y * FR; k = a0 + row; j = r.j0 + blockIdx.z; }
-    else { a0 = r.j0 + blockIdx.y * FR; j = a0 + row; k = r.k0 + blockIdx.z; }
-
-    // ---- stage the stencil footprint (rows of 32..40 doubles, one warp per row)
-    const int warp = tid >> 5;
-    auto stage_rec = [&](S* dst, const S* src) {
-        if (D == 0) stage_rows<S>(dst, src, L, i0 - 4, FL + 8, a0, FR, k, 1, warp, 8, lane);
-        else if (D == 1) stage_rows<S>(dst, src, L, i0, FL, a0 - 4, FR + 7, k, 1, warp, 8, lane);
-        else stage_rows<S>(dst, src, L, i0, FL, j, 1, a0 - 4, FR + 7, warp, 8, lane);
-    };
-    auto stage_lim = [&](S* dst, const S* src) {
-        if (D == 0) stage_rows<S>(dst, src, L, i0 - 2, FL + 4, a0, FR, k, 1, warp, 8, lane);
-        else if (D == 1) stage_rows<S>(dst, src, L, i0, FL, a0 - 2, FR + 3, k, 1, warp, 8, lane);
-        else stage_rows<S>(dst, src, L, i0, FL, j, 1, a0 - 2, FR + 3, warp, 8, lane);
-    };
-#pragma unroll
-    for (int q = 0; q < 5; ++q) stage_rec(sRec + q * RB, in.W[q]);
-    stage_rec(sRec + 5 * RB, in.vol);
-#pragma unroll
-    for (int q = 0; q < 5; ++q) stage_lim(sLim + q * LB, in.Wl[q]);
-    if (MHD) {
-#pragma unroll
-        for (int x = 0; x < 3; ++x) {
-            stage_rec(sRec + (6 + x) * RB, in.B[x]);
-            stage_lim(sLim + (5 + x) * LB, in.Bl[x]);
-        }
-    }
-    cp_async_wait_all();
-    __syncthreads();
-    bool valid = (i < r.i0 + r.ni) && (j >= r.j0) && (j < r.j0 + r.nj) && (k >= r.k0) && (k < r.k0 + r.nk);
-    if (!valid) return;
-
-    // stencil offsets in the staged boxes: recon cell m = f-4+m, limiter cell m = f-2+m
-    auto ro = [&](int m) { return D == 0 ? (lane + m) + (FL + 8) * row : lane + FL * (row + m); };
-    auto lo = [&](int m) { return D == 0 ? (lane + m) + (FL + 4) * row : lane + FL * (row + m); };
-    const long long c = L.at(i, j, k), s = L.stride(D);
-    T Vol[8];
-#pragma unroll
-    for (int m = 0; m < 8; ++m) Vol[m] = T(sRec[5 * RB + ro(m)]);
-    T Vi = central8<T>(Vol);
-    T pdmb = T(p.pdmb);
-    T WL[5], WR[5];
-#pragma unroll
-    for (int v = 0; v < 5; ++v) {
-        T Q[8], nQ[4];
-#pragma unroll
-        for (int m = 0; m < 8; ++m) Q[m] = T(sRec[v * RB + ro(m)]);
-#pragma unroll
-        for (int m = 0; m < 4; ++m) nQ[m] = T(sLim[v * LB + lo(m)]);
-        getLR<T>(p.rmeth, pdmb, Vol, Q, nQ, Vi, WL[v], WR[v]);
-    }
-    T Tf[9];
-#pragma unroll
-    for (int q = 0; q < 9; ++q) Tf[q] = T(__ldg(&in.Tf[D][q][c]));
-    double faB = double(__ldg(&in.face[D][c]));
-    T VaD = T(0), bbD = T(0);
-    if (MHD) {
-        T BL[3], BR[3];
-#pragma unroll
-        for (int x = 0; x < 3; ++x) {
-            T Q[8], nQ[4];
-#pragma unroll
-            for (int m = 0; m < 8; ++m) Q[m] = T(sRec[(6 + x) * RB + ro(m)]);
-#pragma unroll
-            for (int m = 0; m < 4; ++m) nQ[m] = T(sLim[(5 + x) * LB + lo(m)]);
-            getLR<T>(p.rmeth, pdmb, Vol, Q, nQ, Vi, BL[x], BR[x]);
-        }
-        // FP64: the half-state flux over the area (stress.F90:301); FP32: the stored flux/area
-        T Bn;
-        if constexpr (std::is_same<S, double>::value) Bn = T(__ldg(&in.bn[D][c]) / faB);
-        else Bn = T(__ldg(&in.bn[D][c]));
-        T mF[3] = {T(0), T(0), T(0)};
-        if constexpr (BG) {   // background field on the face (stress.F90:302-305)
-            T B0[3];
-#pragma unroll
-            for (int x = 0; x < 3; ++x) B0[x] = T(__ldg(&in.fcB0[D][x][c]));
-            T B0n;
-            if constexpr (std::is_same<S, double>::value) B0n = T(__ldg(&in.b0[D][c]) / faB);
-            else B0n = T(__ldg(&in.b0[D][c]));
-            magKin<T, true>(p, T(-1), WL, BL, Bn, Tf, mF, bbD, VaD, B0, B0n);
-            magKin<T, true>(p, T(1), WR, BR, Bn, Tf, mF, bbD, VaD, B0, B0n);
-        } else {
-            magKin<T>(p, T(-1), WL, BL, Bn, Tf, mF, bbD, VaD);
-            magKin<T>(p, T(1), WR, BR, Bn, Tf, mF, bbD, VaD);
-        }
-        if (p.doBoris) {
-            T Ca2 = T(p.Ca) * T(p.Ca);
-#pragma unroll
-            for (int x = 0; x < 3; ++x) {
-                T deeV = WR[1 + x] - WL[1 + x];
-                T deeP = bbD * deeV / Ca2;
-                mF[x] = mF[x] - T(p.cHogM) * VaD * deeP;
-            }
-        }
-#pragma unroll
-        for (int x = 0; x < 3; ++x) F.m[x][c] = faB * double(mF[x]);
-    }
-    T gF[5] = {T(0), T(0), T(0), T(0), T(0)}, dW[5] = {T(0), T(0), T(0), T(0), T(0)};
-    T gm1 = T(p.gamma - 1);
-    gasKin<T>(gm1, T(-1), WL, Tf, gF, dW);
-    gasKin<T>(gm1, T(1), WR, Tf, gF, dW);
-    T cH = T(p.cHogH);
-#pragma unroll
-    for (int v = 0; v < 5; ++v) gF[v] = gF[v] - cH * VaD * dW[v];
-    if (p.doBoris) {  // nuclear option, stress.F90:399-417 (cLim = 1.5)
-        T vL = sqrt(WL[1] * WL[1] + WL[2] * WL[2] + WL[3] * WL[3]);
-        T vR = sqrt(WR[1] * WR[1] + WR[2] * WR[2] + WR[3] * WR[3]);
-        T Vn = sqrt(vL * vL + vR * vR) / T((double)sqrtf(2.0f));
-        if (Vn >= T(1.5) * T(p.Ca)) {
-#pragma unroll
-            for (int v = 0; v < 5; ++v) gF[v] = gF[v] - T(p.Ca) * T(h.gas[v][c] - h.gas[v][c - s]);
-        }
-    }
-#pragma unroll
-    for (int v = 0; v < 5; ++v) F.g[v][c] = faB * double(gF[v]);
-}
-
-template <typename T, typename S, int D>
-static void launch_flux_dir(Handle& h, const FluxSrc<S>& in, const Reg& r, cudaStream_t st) {
-    const Par& p = h.p;
-    FluxP F;
-    for (int v = 0; v < 5; ++v) F.g[v] = h.gflx[D][v];
-    for (int x = 0; x < 3; ++x) F.m[x] = h.mflx[D][x];
-    dim3 grid((unsigned)((r.ni + FL - 1) / FL), 0, 0);
-    if (D == 2) { grid.y = (unsigned)((r.nk + FR - 1) / FR); grid.z = (unsigned)r.nj; }
-    else { grid.y = (unsigned)((r.nj + FR - 1) / FR); grid.z = (unsigned)r.nk; }
-    if (p.doMHD && p.doBackground)
-        k_flux_tile<T, S, D, true, true><<<grid, 256, flux_smem<S, D>(), st>>>(h.L, p, in, h.H, F, r);
-    else if (p.doMHD) k_flux_tile<T, S, D, true, false><<<grid, 256, flux_smem<S, D>(), st>>>(h.L, p, in, h.H, F, r);
-    else k_flux_tile<T, S, D, false, false><<<grid, 256, flux_smem<S, D>(), st>>>(h.L, p, in, h.H, F, r);
-    h.launches++;
-}
-
-template <typename T, typename S, int D>
-static void set_flux_smem() {
-    cudaFuncSetAttribute(k_flux_tile<T, S, D, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         (int)flux_smem<S, D>());
-    cudaFuncSetAttribute(k_flux_tile<T, S, D, true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         (int)flux_smem<S, D>());
-    cudaFuncSetAttribute(k_flux_tile<T, S, D, false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         (int)flux_smem<S, D>());
-}
 void flux_kernels_init() {
     set_flux_smem<double, double, 0>(); set_flux_smem<double, double, 1>(); set_flux_smem<double, double, 2>();
-    set_flux_smem<float, float, 0>(); set_flux_smem<float, float, 1>(); set_flux_smem<float, float, 2>();
-}
-
-// CalcStress flux loop (stress.F90:84-128): I, J and (unless 2.5D) K interfaces
-template <typename T, typename S>
-static void fluxes_all(Handle& h, const FluxSrc<S>& in, cudaStream_t st) {
-    const Lay& L = h.L;
-    int is = L.is(), ie = L.ie(), js = L.js(), je = L.je(), ks = L.ks(), ke = L.ke();
-    if (h.p.do25D) ke = ks;
-    launch_flux_dir<T, S, 0>(h, in, mkreg(is, ie + 1, js, je, ks, ke), st);
-    launch_flux_dir<T, S, 1>(h, in, mkreg(is, ie, js, je + 1, ks, ke), st);
-    if (!h.p.do25D) launch_flux_dir<T, S, 2>(h, in, mkreg(is, ie, js, je, ks, ke + 1), st);
+    flux_kernels_init_f32();
 }
 
 void enqueue_fluxes(Handle& h, const StateP& nS, cudaStream_t st) {
-    const bool lfm = h.p.doLFMLim != 0;
     if (h.prec == PREC_FP32FLUX) {
-        const F32Planes& f = h.f32;
-        FluxSrc<float> in;
-        for (int v = 0; v < 5; ++v) { in.W[v] = f.Wh[v]; in.Wl[v] = lfm ? f.Wn[v] : f.Wh[v]; }
-        for (int x = 0; x < 3; ++x) { in.B[x] = f.hb[x]; in.Bl[x] = lfm ? f.nb[x] : f.hb[x]; }
-        in.vol = f.volume;
-        for (int d = 0; d < 3; ++d) {
-            for (int q = 0; q < 9; ++q) in.Tf[d][q] = f.Tf[d][q];
-            in.face[d] = f.face[d];
-            in.bn[d] = f.hbA[d];
-            for (int x = 0; x < 3; ++x) in.fcB0[d][x] = f.fcB0[d][x];
-            in.b0[d] = f.b0n[d];
-        }
-        fluxes_all<float, float>(h, in, st);
-    } else {
-        FluxSrc<double> in;
-        for (int v = 0; v < 5; ++v) { in.W[v] = h.Wh[v]; in.Wl[v] = lfm ? h.Wn[v] : h.Wh[v]; }
-        for (int x = 0; x < 3; ++x) { in.B[x] = h.H.b[x]; in.Bl[x] = lfm ? nS.b[x] : h.H.b[x]; }
-        in.vol = h.volume;
-        for (int d = 0; d < 3; ++d) {
-            for (int q = 0; q < 9; ++q) in.Tf[d][q] = h.Tf[d][q];
-            in.face[d] = h.face[d];
-            in.bn[d] = h.H.mf[d];
-            for (int x = 0; x < 3; ++x) in.fcB0[d][x] = h.fcB0[d][x];
-            in.b0[d] = h.bFlux0[d];
-        }
-        fluxes_all<double, double>(h, in, st);
+        enqueue_fluxes_f32(h, nS, st);
+        return;
     }
+    const bool lfm = h.p.doLFMLim != 0;
+    FluxSrc<double> in;
+    for (int v = 0; v < 5; ++v) { in.W[v] = h.Wh[v]; in.Wl[v] = lfm ? h.Wn[v] : h.Wh[v]; }
+    for (int x = 0; x < 3; ++x) { in.B[x] = h.H.b[x]; in.Bl[x] = lfm ? nS.b[x] : h.H.b[x]; }
+    in.vol = h.volume;
+    for (int d = 0; d < 3; ++d) {
+        for (int q = 0; q < 9; ++q) in.Tf[d][q] = h.Tf[d][q];
+        in.face[d] = h.face[d];
+        in.bn[d] = h.H.mf[d];
+        for (int x = 0; x < 3; ++x) in.fcB0[d][x] = h.fcB0[d][x];
+        in.b0[d] = h.bFlux0[d];
+    }
+    fluxes_all<double, double>(h, in, st);
 }
 
 }  // namespace gam

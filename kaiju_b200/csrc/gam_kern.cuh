@@ -62,7 +62,9 @@ template <typename S> struct EdgeSrc {
     const S* edgB0[3][2]; // background: edge-frame B0 (tangents 1, 2) per edge direction
 };
 struct Vec3P { double* v[3]; };
-struct FluxP { double* g[5]; double* m[3]; };
+// interface fluxes (area-scaled) of one direction: double planes, or float planes on the FP32-flux path
+template <typename O> struct FluxOut { O* g[5]; O* m[3]; };
+using FluxP = FluxOut<double>;
 
 // One-sided gas kinetic flux (stress.F90:432-511)
 template <typename T>

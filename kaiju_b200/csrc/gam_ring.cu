@@ -35,7 +35,8 @@ inline unsigned nblk1(long long n, int b) { return (unsigned)((n + b - 1) / b); 
 }  // namespace
 
 // ------------------------------------------------------------------ RingFlux2FieldFix (ringutils.F90:380-433)
-__global__ void k_ring_bfix(Lay L, Par p, StateP s, F32B fb) {
+// With floatOnly (the FP32-flux half state, which exists only as floats) the float copies are the source.
+__global__ void k_ring_bfix(Lay L, Par p, StateP s, F32B fb, int floatOnly) {
     long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     long long nrow = (long long)L.Ni * L.Nk;
     if (t >= nrow * L.nG) return;
@@ -49,15 +50,14 @@ __global__ void k_ring_bfix(Lay L, Par p, StateP s, F32B fb) {
         lfmCC(L, p.ringDoS, p.ringDoE, jg, k, jp, kp);
         long long d = L.at(i, jg, k), src = L.at(i, jp, kp);
         for (int x = 0; x < 3; ++x) {
-            double b = s.b[x][src];
-            s.b[x][d] = b;
-            if (fb.v[0]) fb.v[x][d] = float(b);
+            if (floatOnly) { fb.v[x][d] = fb.v[x][src]; continue; }
+            s.b[x][d] = s.b[x][src];
         }
     }
 }
 
 // ------------------------------------------------------------------ PredFix of the LFM blast wave (ICs/lfmbw.F90:227-248)
-__global__ void k_predfix_lfm(Lay L, Par p, StateP s, F32B fb) {
+__global__ void k_predfix_lfm(Lay L, Par p, StateP s, F32B fb, int floatOnly) {
     long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (t >= (long long)L.Nj * L.Nk * L.nG) return;
     int j = (int)(t % L.Nj);
@@ -67,15 +67,15 @@ __global__ void k_predfix_lfm(Lay L, Par p, StateP s, F32B fb) {
     lfmCC(L, p.ringDoS, p.ringDoE, j, k, jp, kp);
     long long d = L.at(ig, j, k), src = L.at(L.is(), jp, kp);
     for (int x = 0; x < 3; ++x) {
-        double b = s.b[x][src];
-        s.b[x][d] = b;
-        if (fb.v[0]) fb.v[x][d] = float(b);
+        if (floatOnly) fb.v[x][d] = fb.v[x][src];
+        else s.b[x][d] = s.b[x][src];
     }
 }
 
 // ------------------------------------------------------------------ RingFlux (ringutils.F90:663-680)
 // J fluxes through the axis faces js and je+1 vanish (every i, k of the flux arrays)
-__global__ void k_ring_flux_zero(Lay L, Par p, FluxP FJ) {
+template <typename O>
+__global__ void k_ring_flux_zero(Lay L, Par p, FluxOut<O> FJ) {
     long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (t >= (long long)L.Ni * L.Nk) return;
     int i = (int)(t % L.Ni), k = (int)(t / L.Ni);
@@ -83,23 +83,24 @@ __global__ void k_ring_flux_zero(Lay L, Par p, FluxP FJ) {
         if (side == 0 && !p.ringDoS) continue;
         if (side == 1 && !p.ringDoE) continue;
         long long c = L.at(i, side == 0 ? L.js() : L.je() + 1, k);
-        for (int v = 0; v < 5; ++v) FJ.g[v][c] = 0.0;
+        for (int v = 0; v < 5; ++v) FJ.g[v][c] = O(0);
         if (p.doMHD)
-            for (int x = 0; x < 3; ++x) FJ.m[x][c] = 0.0;
+            for (int x = 0; x < 3; ++x) FJ.m[x][c] = O(0);
     }
 }
 // FixGasFluxLFM (gamdebug.F90:91-124): the K fluxes at ks and ke+1 take their mean
-__global__ void k_ring_flux_kavg(Lay L, FluxP FK) {
+template <typename O>
+__global__ void k_ring_flux_kavg(Lay L, FluxOut<O> FK) {
     long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (t >= (long long)L.Nip * L.Njp) return;
     int i = L.is() + (int)(t % L.Nip), j = L.js() + (int)(t / L.Nip);
     long long c0 = L.at(i, j, L.ks()), c1 = L.at(i, j, L.ke() + 1);
     for (int v = 0; v < 5; ++v) {
-        double gF = 0.5 * (FK.g[v][c0] + FK.g[v][c1]);
+        O gF = O(0.5) * (FK.g[v][c0] + FK.g[v][c1]);
         FK.g[v][c0] = gF; FK.g[v][c1] = gF;
     }
     for (int x = 0; x < 3; ++x) {
-        double mF = 0.5 * (FK.m[x][c0] + FK.m[x][c1]);
+        O mF = O(0.5) * (FK.m[x][c0] + FK.m[x][c1]);
         FK.m[x][c0] = mF; FK.m[x][c1] = mF;
     }
 }
@@ -439,7 +440,7 @@ void launch_ring_bfix(Handle& h, const StateP& s, cudaStream_t st, bool withF32)
     F32B fb{};
     if (withF32) for (int x = 0; x < 3; ++x) fb.v[x] = h.f32.hb[x];
     long long n = (long long)L.Ni * L.Nk * L.nG;
-    k_ring_bfix<<<nblk1(n, 256), 256, 0, st>>>(L, h.p, s, fb);
+    k_ring_bfix<<<nblk1(n, 256), 256, 0, st>>>(L, h.p, s, fb, withF32 ? 1 : 0);
     h.launches++;
 }
 void launch_predfix_lfm(Handle& h, const StateP& s, cudaStream_t st, bool withF32) {
@@ -447,20 +448,25 @@ void launch_predfix_lfm(Handle& h, const StateP& s, cudaStream_t st, bool withF3
     F32B fb{};
     if (withF32) for (int x = 0; x < 3; ++x) fb.v[x] = h.f32.hb[x];
     long long n = (long long)L.Nj * L.Nk * L.nG;
-    k_predfix_lfm<<<nblk1(n, 256), 256, 0, st>>>(L, h.p, s, fb);
+    k_predfix_lfm<<<nblk1(n, 256), 256, 0, st>>>(L, h.p, s, fb, withF32 ? 1 : 0);
     h.launches++;
 }
-void launch_ring_flux(Handle& h, cudaStream_t st) {
+template <typename O>
+static void ring_flux(Handle& h, O* const (*g)[5], O* const (*m)[3], cudaStream_t st) {
     const Lay& L = h.L;
-    FluxP FJ, FK;
-    for (int v = 0; v < 5; ++v) { FJ.g[v] = h.gflx[1][v]; FK.g[v] = h.gflx[2][v]; }
-    for (int x = 0; x < 3; ++x) { FJ.m[x] = h.mflx[1][x]; FK.m[x] = h.mflx[2][x]; }
-    k_ring_flux_zero<<<nblk1((long long)L.Ni * L.Nk, 256), 256, 0, st>>>(L, h.p, FJ);
+    FluxOut<O> FJ, FK;
+    for (int v = 0; v < 5; ++v) { FJ.g[v] = g[1][v]; FK.g[v] = g[2][v]; }
+    for (int x = 0; x < 3; ++x) { FJ.m[x] = m[1][x]; FK.m[x] = m[2][x]; }
+    k_ring_flux_zero<O><<<nblk1((long long)L.Ni * L.Nk, 256), 256, 0, st>>>(L, h.p, FJ);
     h.launches++;
     if (h.p.doMHD) {
-        k_ring_flux_kavg<<<nblk1((long long)L.Nip * L.Njp, 256), 256, 0, st>>>(L, FK);
+        k_ring_flux_kavg<O><<<nblk1((long long)L.Nip * L.Njp, 256), 256, 0, st>>>(L, FK);
         h.launches++;
     }
+}
+void launch_ring_flux(Handle& h, cudaStream_t st) {
+    if (h.prec == PREC_FP32FLUX) ring_flux<float>(h, h.f32.gflx, h.f32.mflx, st);
+    else ring_flux<double>(h, h.gflx, h.mflx, st);
 }
 void launch_pole_e(Handle& h, double* const* E, cudaStream_t st) {
     const Lay& L = h.L;

@@ -30,7 +30,7 @@ __global__ void k_step_begin(Scal* sc) {
 // per-face values EdgeLRs divides out at every stencil point (fields.F90:335-336): flux/max(area,TINY)
 // for the half state (reconstruction) and for the limiting state.
 struct F32FaceOut { float* hbA[3]; float* nbA[3]; };
-struct F32CellOut { float* Wh[5]; float* Wn[5]; float* hb[3]; float* nb[3]; float* rho; };
+struct F32CellOut { float* Wh[5]; float* Wn[5]; float* hb[3]; float* nb[3]; float* rho; float* VdV[3]; };
 
 __global__ void k_predict_faces(long long E, Par p, GridP g, Vec3P mf, Vec3P omf, Vec3P hmf, Vec3P hbA, Vec3P nbA,
                                 F32FaceOut o, const Scal* sc) {
@@ -42,9 +42,9 @@ __global__ void k_predict_faces(long long E, Par p, GridP g, Vec3P mf, Vec3P omf
         double Q = mf.v[c][l], oQ = omf.v[c][l];
         double dQ = (Q - oQ) / odt;
         double H = Q + pdt * dQ;
-        hmf.v[c][l] = H;
         double a = dmax(g.face[c][l], TINY);
         double hb = H / a, nb = (p.doLFMLim ? Q : H) / a;
+        hmf.v[c][l] = H;   // the half-state flux: bFlux2Fld of the half state reads it
         if (o.hbA[0]) { o.hbA[c][l] = float(hb); o.nbA[c][l] = float(nb); }
         else { hbA.v[c][l] = hb; nbA.v[c][l] = nb; }
     }
@@ -59,8 +59,9 @@ __global__ void k_predict_cells(Lay L, Par p, GridP g, StateP n, StateP o, State
     if (!reg_ijk(r, blockIdx.x * (long long)blockDim.x + threadIdx.x, i, j, k)) return;
     long long c = L.at(i, j, k);
     double B[3] = {0.0, 0.0, 0.0};
+    const bool f32 = f.Wh[0] != nullptr;
     cellBxyz(L, g, h.mf, c, B);
-    h.b[0][c] = B[0]; h.b[1][c] = B[1]; h.b[2][c] = B[2];
+    if (!f32) { h.b[0][c] = B[0]; h.b[1][c] = B[1]; h.b[2][c] = B[2]; }
     double Q[5], oQ[5], W[5], oW[5], pW[5], pQ[5];
 #pragma unroll
     for (int v = 0; v < 5; ++v) { Q[v] = n.gas[v][c]; oQ[v] = o.gas[v][c]; }
@@ -72,17 +73,21 @@ __global__ void k_predict_cells(Lay L, Par p, GridP g, StateP n, StateP o, State
     pW[0] = dmax(pW[0], p.dFloor);
     pW[4] = dmax(pW[4], p.pFloor);
     cellP2C(p, pW, pQ);
+    // the FP32-flux path keeps the half state as floats only; the double gas half state feeds its
+    // Boris flux correction
+    if (!f32 || p.doBoris) {
 #pragma unroll
-    for (int v = 0; v < 5; ++v) h.gas[v][c] = pQ[v];
+        for (int v = 0; v < 5; ++v) h.gas[v][c] = pQ[v];
+    }
     // Mom2Face summand VolB*MomB/max(DenB,dFloor) (fields.F90:265-271), a pointwise cell value
     {
         double vol = g.volume[c], den = dmax(pQ[0], p.dFloor);
-        VdV.v[0][c] = vol * pQ[1] / den;
-        VdV.v[1][c] = vol * pQ[2] / den;
-        VdV.v[2][c] = vol * pQ[3] / den;
+        double v0 = vol * pQ[1] / den, v1 = vol * pQ[2] / den, v2 = vol * pQ[3] / den;
+        if (f32) { f.VdV[0][c] = float(v0); f.VdV[1][c] = float(v1); f.VdV[2][c] = float(v2); }
+        else { VdV.v[0][c] = v0; VdV.v[1][c] = v1; VdV.v[2][c] = v2; }
     }
     double w[5];
-    if (f.Wh[0]) {   // FP32-flux path: float copies of every stencil input
+    if (f32) {   // FP32-flux path: float copies of every stencil input
         blockC2P(p, pQ, w);
 #pragma unroll
         for (int v = 0; v < 5; ++v) f.Wh[v][c] = float(w[v]);
@@ -102,8 +107,11 @@ __global__ void k_predict_cells(Lay L, Par p, GridP g, StateP n, StateP o, State
     for (int v = 0; v < 5; ++v) Wn.w[v][c] = w[v];
 }
 
-// Flux2Deltas (stress.F90:150-196)
-__global__ void k_flux2deltas(Lay L, Par p, GridP g, FluxP FI, FluxP FJ, FluxP FK, PrimP dGH, Vec3P dGM) {
+// Flux2Deltas (stress.F90:150-196); O is the flux storage type (float on the FP32-flux path), the sums
+// run in double
+template <typename O>
+__global__ void k_flux2deltas(Lay L, Par p, GridP g, FluxOut<O> FI, FluxOut<O> FJ, FluxOut<O> FK, PrimP dGH,
+                              Vec3P dGM) {
     Reg r = {L.is(), L.Nip, L.js(), L.Njp, L.ks(), L.Nkp};
     int i, j, k;
     if (!reg_ijk(r, blockIdx.x * (long long)blockDim.x + threadIdx.x, i, j, k)) return;
@@ -111,11 +119,13 @@ __global__ void k_flux2deltas(Lay L, Par p, GridP g, FluxP FI, FluxP FJ, FluxP F
     double dV = g.volume[c];
 #pragma unroll
     for (int v = 0; v < 5; ++v)
-        dGH.w[v][c] = (FI.g[v][c] - FI.g[v][c + 1] + FJ.g[v][c] - FJ.g[v][cj] + FK.g[v][c] - FK.g[v][ck]) / dV;
+        dGH.w[v][c] = (double(FI.g[v][c]) - double(FI.g[v][c + 1]) + double(FJ.g[v][c]) - double(FJ.g[v][cj]) +
+                       double(FK.g[v][c]) - double(FK.g[v][ck])) / dV;
     if (p.doMHD) {
 #pragma unroll
         for (int x = 0; x < 3; ++x)
-            dGM.v[x][c] = (FI.m[x][c] - FI.m[x][c + 1] + FJ.m[x][c] - FJ.m[x][cj] + FK.m[x][c] - FK.m[x][ck]) / dV;
+            dGM.v[x][c] = (double(FI.m[x][c]) - double(FI.m[x][c + 1]) + double(FJ.m[x][c]) - double(FJ.m[x][cj]) +
+                           double(FK.m[x][c]) - double(FK.m[x][ck])) / dV;
         if (p.doBackground) {   // background momentum source (stress.F90:185-188)
 #pragma unroll
             for (int x = 0; x < 3; ++x) dGM.v[x][c] = dGM.v[x][c] + g.dpB0[x][c];
@@ -655,7 +665,7 @@ void refresh_f32_background(Handle& h) {
 int ensure_f32(Handle& h) {
     if (h.f32pool) return 0;
     const long long E = h.L.E;
-    const int nplanes = 26 + 64 + (h.p.doBackground ? 18 : 0);
+    const int nplanes = 29 + 24 + 64 + (h.p.doBackground ? 18 : 0);
     if (cudaMalloc(&h.f32pool, sizeof(float) * E * nplanes) != cudaSuccess) return 3;
     cudaMemsetAsync(h.f32pool, 0, sizeof(float) * E * nplanes, h.stream);
     float* q = h.f32pool;
@@ -669,6 +679,11 @@ int ensure_f32(Handle& h) {
     for (int x = 0; x < 3; ++x) f.nbA[x] = take();
     for (int x = 0; x < 3; ++x) f.Vf[x] = take();
     f.rho = take();
+    for (int x = 0; x < 3; ++x) f.VdV[x] = take();
+    for (int d = 0; d < 3; ++d) {
+        for (int v = 0; v < 5; ++v) f.gflx[d][v] = take();
+        for (int x = 0; x < 3; ++x) f.mflx[d][x] = take();
+    }
     f.volume = take();
     for (int d = 0; d < 3; ++d) f.face[d] = take();
     for (int d = 0; d < 3; ++d) f.edge[d] = take();
@@ -738,7 +753,7 @@ int step_enqueue(Handle& h, int cur, cudaEvent_t* ev) {
     F32CellOut fc{};
     if (h.prec == PREC_FP32FLUX) {
         for (int v = 0; v < 5; ++v) { fc.Wh[v] = h.f32.Wh[v]; fc.Wn[v] = h.f32.Wn[v]; }
-        for (int x = 0; x < 3; ++x) { fc.hb[x] = h.f32.hb[x]; fc.nb[x] = h.f32.nb[x]; }
+        for (int x = 0; x < 3; ++x) { fc.hb[x] = h.f32.hb[x]; fc.nb[x] = h.f32.nb[x]; fc.VdV[x] = h.f32.VdV[x]; }
         fc.rho = h.f32.rho;
     }
     k_predict_cells<<<nblk(ncell, TPB), TPB, 0, st>>>(L, p, g, nS, oS, h.H, Wh, Wn, VdV, fc, h.dScal);
@@ -749,16 +764,25 @@ int step_enqueue(Handle& h, int cur, cudaEvent_t* ev) {
     enqueue_hot(h, nS, st, ev);
     if (p.doRing) launch_ring_flux(h, st);   // stress.F90:134-139
     mark(PH_DELTAS);
-    FluxP F[3];
-    for (int d = 0; d < 3; ++d) {
-        for (int v = 0; v < 5; ++v) F[d].g[v] = h.gflx[d][v];
-        for (int x = 0; x < 3; ++x) F[d].m[x] = h.mflx[d][x];
-    }
     PrimP dGH;
     for (int v = 0; v < 5; ++v) dGH.w[v] = h.dGasH[v];
     Vec3P dGM = {{h.dGasM[0], h.dGasM[1], h.dGasM[2]}};
     long long nact = (long long)L.Nip * L.Njp * L.Nkp;
-    k_flux2deltas<<<nblk(nact, TPB), TPB, 0, st>>>(L, p, g, F[0], F[1], F[2], dGH, dGM);
+    if (h.prec == PREC_FP32FLUX) {
+        FluxOut<float> F[3];
+        for (int d = 0; d < 3; ++d) {
+            for (int v = 0; v < 5; ++v) F[d].g[v] = h.f32.gflx[d][v];
+            for (int x = 0; x < 3; ++x) F[d].m[x] = h.f32.mflx[d][x];
+        }
+        k_flux2deltas<float><<<nblk(nact, TPB), TPB, 0, st>>>(L, p, g, F[0], F[1], F[2], dGH, dGM);
+    } else {
+        FluxP F[3];
+        for (int d = 0; d < 3; ++d) {
+            for (int v = 0; v < 5; ++v) F[d].g[v] = h.gflx[d][v];
+            for (int x = 0; x < 3; ++x) F[d].m[x] = h.mflx[d][x];
+        }
+        k_flux2deltas<double><<<nblk(nact, TPB), TPB, 0, st>>>(L, p, g, F[0], F[1], F[2], dGH, dGM);
+    }
     mark(PH_UPDATE);
     // applyUpdate into the oState buffer (which becomes State n+1)
     Vec3P E = {{h.E[0], h.E[1], h.E[2]}};

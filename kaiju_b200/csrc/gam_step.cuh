@@ -12,6 +12,8 @@ enum Prec { PREC_FP64 = 0, PREC_FP32FLUX = 1 };
 // metric planes converted once
 struct F32Planes {
     float* Wh[5]; float* Wn[5]; float* hb[3]; float* nb[3]; float* hbA[3]; float* nbA[3]; float* Vf[3]; float* rho;
+    float* VdV[3];
+    float* gflx[3][5]; float* mflx[3][3];   // area-scaled interface fluxes
     float* volume; float* face[3]; float* edge[3]; float* Tf[3][9]; float* Te[3][6]; float* Teb[3][4];
     // background field: fcB0, bFlux0/face and edgB0 (only with a background)
     float* fcB0[3][3]; float* b0n[3]; float* edgB0[3][2];
@@ -92,10 +94,14 @@ int kernels_per_step(const Handle& h);
 // interface fluxes of all directions (gam_flux.cu)
 void enqueue_fluxes(Handle& h, const StateP& nS, cudaStream_t st);
 void flux_kernels_init();
+void enqueue_fluxes_f32(Handle& h, const StateP& nS, cudaStream_t st);   // gam_flux_f32.cu
+void flux_kernels_init_f32();
 // E field of all edge directions (gam_efield.cu): Mom2Face + tiled EMF
 void enqueue_efield(Handle& h, const StateP& nS, cudaStream_t st);
 void efield_kernels_init();
+void efield_kernels_init_f32();   // gam_efield_f32.cu
 // ring averaging about the LFM axis (gam_ring.cu)
+// withF32: the FP32-flux half state, whose B exists only as the float copies
 void launch_ring_bfix(Handle& h, const StateP& s, cudaStream_t st, bool withF32 = false);  // RingFlux2FieldFix
 void launch_predfix_lfm(Handle& h, const StateP& s, cudaStream_t st, bool withF32 = false);  // lfmbw PredFix
 void launch_ring_flux(Handle& h, cudaStream_t st);                              // RingFlux + FixGasFluxLFM
