@@ -131,6 +131,14 @@ int gam_gpu_create(gam_gpu_t** h, const gam_model_c* m, const gam_grid_c* g, con
                             rC=20, P0=0.1, pRat=10, D0=1, B0=1): ICs/lfmbw.F90:33-104 */
 int gam_gpu_create_from_corners(gam_gpu_t** h, const gam_model_c* m, const double* xyz, int ic);
 
+/* gam_gpu_create_from_corners for initial conditions with parameters:
+ *   GAM_IC_KH: the Kelvin-Helmholtz shear layer of the batched-ensemble problem (no counterpart in the
+ *   reference), sampled at cell centres: rho = 1, P = 1, Vx = 0.5 tanh((y-0.5)/a), Vy = amp*(2u-1) with u
+ *   a counter-based hash of (seed, i, j, k), B = (Bx, 0, 0). icPar = {a, Bx, amp, seed}, nPar >= 4. */
+#define GAM_IC_KH 3
+int gam_gpu_create_from_corners_ic(gam_gpu_t** h, const gam_model_c* m, const double* xyz, int ic,
+                                   const double* icPar, int nPar);
+
 /* gam_gpu_create_from_corners with a background field (Model%doBackground must be set): AddB0
  * (src/gamera/background.F90:20-167) runs on the device after the IC, as CalcGridInfo does
  * (init.F90:180-184), with a built-in Model%B0:
@@ -189,6 +197,22 @@ int gam_gpu_set_precision(gam_gpu_t* h, int mode);
 int gam_gpu_fetch(gam_gpu_t* h, const char* name, double* out, long long n);
 
 void gam_gpu_destroy(gam_gpu_t* h);
+
+/* Ensembles: independent problems (any sizes, on one device) advanced together. Each batch step is one
+ * CUDA graph launch holding every active member's stepGamera as a concurrent branch; every member keeps
+ * its own dt. No counterpart in the reference, which runs one problem per process. The members stay
+ * owned by the caller and usable on their own between ensemble calls. */
+typedef struct gam_ensemble gam_ensemble_t;
+int gam_gpu_ensemble_create(gam_ensemble_t** e, gam_gpu_t* const* members, int n);
+/* nsteps batch steps; returns the worst member status (GAM_ERR_NAN before GAM_ERR_DT_COLLAPSE) */
+int gam_gpu_ensemble_run_steps(gam_ensemble_t* e, int nsteps);
+/* the same, with the device time of the batch steps (ms) from CUDA events on the ensemble stream */
+int gam_gpu_ensemble_run_steps_timed(gam_ensemble_t* e, int nsteps, double* ms);
+/* advance until every member's Model%t >= tEnd (members drop out as they get there; the host checks
+ * every `chunk` batch steps, so a member may take up to chunk-1 steps past tEnd, of the tiny dt CalcDT
+ * gives once t reaches the member's tFin) or maxSteps batch steps; *steps = batch steps taken */
+int gam_gpu_ensemble_advance(gam_ensemble_t* e, double tEnd, int chunk, int maxSteps, int* steps);
+void gam_gpu_ensemble_destroy(gam_ensemble_t* e);   /* the members are not destroyed */
 
 /* DivB for callers that cannot allocate device memory (no counterpart in the reference).
  * Some hosts cannot call cudaMalloc: device arrays owned by another runtime (OpenACC or CUDA Fortran

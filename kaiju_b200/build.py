@@ -17,6 +17,8 @@ SOURCES = ["gam_capi.cu", "gam_step.cu", "gam_flux.cu", "gam_efield.cu", "gam_in
 FAST_F32 = {"gam_flux_f32.cu", "gam_efield_f32.cu"}
 FAST_F32_FLAGS = ["-prec-div=false", "-prec-sqrt=false", "-ftz=true"]
 OBJDIR = os.path.join(HERE, "_build")
+DRIVER_SRC = os.path.join(HERE, "driver", "gamera_gpu_x.cpp")
+DRIVER = os.path.join(HERE, "driver", "gamera_gpu_x")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
@@ -30,6 +32,9 @@ def needs_build() -> bool:
         return True
     t = os.path.getmtime(LIB)
     deps = sources() + [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".cuh", ".h"))]
+    deps.append(DRIVER_SRC)
+    if not os.path.exists(DRIVER):
+        return True
     deps.append(os.path.join(ROOT, "include", "gamgpu.h"))
     return any(os.path.getmtime(d) > t for d in deps)
 
@@ -54,7 +59,16 @@ def build(force: bool = False, verbose: bool = False) -> str:
     if failed:
         raise subprocess.CalledProcessError(1, "nvcc " + " ".join(failed))
     subprocess.run([NVCC, *ARCH, "-shared", "-o", LIB, *objs], check=True)
+    build_driver()
     return LIB
+
+
+def build_driver() -> str:
+    """The C++ host driver over the C ABI (links libgamgpu.so from the package directory)."""
+    cmd = ["g++", "-O2", "-std=c++17", "-I", os.path.join(ROOT, "include"), DRIVER_SRC, "-o", DRIVER,
+           "-L", HERE, "-lgamgpu", "-Wl,-rpath,$ORIGIN/.."]
+    subprocess.run(cmd, check=True)
+    return DRIVER
 
 
 if __name__ == "__main__":

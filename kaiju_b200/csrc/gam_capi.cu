@@ -1,6 +1,7 @@
 // C ABI (include/gamgpu.h): handle lifetime, Fortran-layout mirroring, step / advance entry points.
 #include <cstdio>
 #include <cstring>
+#include <vector>
 #include <cstdlib>
 #include <new>
 #include <string>
@@ -346,12 +347,13 @@ int gam_gpu_create(gam_gpu_t** out, const gam_model_c* m, const gam_grid_c* g, c
     return GAM_OK;
 }
 
-static int create_from_corners(gam_gpu_t** out, const gam_model_c* m, const double* xyz, int ic, const BgSpec* bg) {
+static int create_from_corners(gam_gpu_t** out, const gam_model_c* m, const double* xyz, int ic, const BgSpec* bg,
+                               const double* icPar = nullptr) {
     if (!out || !xyz) return GAM_ERR_ARG;
     *out = nullptr;
     int rc = check_model(m);
     if (rc) return rc;
-    if (ic != GAM_IC_OT2D && ic != GAM_IC_BW && ic != GAM_IC_LFMBW) return GAM_ERR_ARG;
+    if (ic != GAM_IC_OT2D && ic != GAM_IC_BW && ic != GAM_IC_LFMBW && !(ic == GAM_IC_KH && icPar)) return GAM_ERR_ARG;
     if ((m->Nip % 8) != 0) return GAM_ERR_ARG;   // Corners2Grid divisibility check (init.F90:830-834)
     if ((bg != nullptr) != (m->doBackground != 0)) return GAM_ERR_ARG;
     gam_gpu* G = new (std::nothrow) gam_gpu();
@@ -365,7 +367,7 @@ static int create_from_corners(gam_gpu_t** out, const gam_model_c* m, const doub
     h.hScal->otime = m->t;
     rc = upload_scalars(G);
     if (!rc && init_grid_from_corners(h) != 0) rc = GAM_ERR_CUDA;
-    if (!rc && init_problem(h, ic, bg) != 0) rc = GAM_ERR_CUDA;
+    if (!rc && init_problem(h, ic, bg, icPar) != 0) rc = GAM_ERR_CUDA;
     if (!rc) rc = download_scalars(G);
     if (rc) { gam_gpu_destroy(G); return rc; }
     *out = G;
@@ -374,6 +376,12 @@ static int create_from_corners(gam_gpu_t** out, const gam_model_c* m, const doub
 
 int gam_gpu_create_from_corners(gam_gpu_t** out, const gam_model_c* m, const double* xyz, int ic) {
     return create_from_corners(out, m, xyz, ic, nullptr);
+}
+
+int gam_gpu_create_from_corners_ic(gam_gpu_t** out, const gam_model_c* m, const double* xyz, int ic,
+                                   const double* icPar, int nPar) {
+    if (ic == GAM_IC_KH && (!icPar || nPar < 4 || !(icPar[0] > 0.0) || icPar[3] < 0.0)) return GAM_ERR_ARG;
+    return create_from_corners(out, m, xyz, ic, nullptr, icPar);
 }
 
 int gam_gpu_create_from_corners_b0(gam_gpu_t** out, const gam_model_c* m, const double* xyz, int ic, int b0Kind,
@@ -637,6 +645,173 @@ void gam_gpu_destroy(gam_gpu_t* G) {
     if (h.hScal) cudaFreeHost(h.hScal);
     if (h.stream && h.ownStream) cudaStreamDestroy(h.stream);
     delete G;
+}
+
+}  // extern "C"
+
+// ================================================================================ ensembles
+// A batch of independent problems advanced together. One step of the batch is one CUDA graph launch
+// that holds every active member's whole step as its own branch: the branches run concurrently, so many
+// small grids fill the GPU that one of them alone would leave mostly idle, and the host launches once
+// per batch step instead of once per kernel per member. Each member keeps its own time step. Every step
+// flips each member's buffer parity, so two graphs (the current parities and their complement) cover a
+// run; they are rebuilt when the set of active members changes.
+struct gam_ensemble {
+    std::vector<gam_gpu*> members;
+    std::vector<char> active;
+    cudaStream_t root = nullptr;
+    cudaEvent_t fork = nullptr;
+    std::vector<cudaEvent_t> join;
+    cudaGraphExec_t graph[2] = {nullptr, nullptr};
+    int phase = 0;   // which of the two graphs runs next
+};
+
+namespace {
+void ens_destroy_graphs(gam_ensemble* E) {
+    for (int c = 0; c < 2; ++c)
+        if (E->graph[c]) { cudaGraphExecDestroy(E->graph[c]); E->graph[c] = nullptr; }
+}
+// capture the batch step with member m at parity cur[m] ^ flip
+int ens_capture(gam_ensemble* E, int flip, cudaGraphExec_t* out) {
+    cudaGraph_t gr;
+    CK(cudaStreamBeginCapture(E->root, cudaStreamCaptureModeThreadLocal));
+    cudaEventRecord(E->fork, E->root);
+    int rc = 0;
+    for (size_t m = 0; m < E->members.size(); ++m) {
+        if (!E->active[m]) continue;
+        Handle& h = E->members[m]->h;
+        cudaStreamWaitEvent(h.stream, E->fork, 0);
+        if (step_enqueue(h, h.cur ^ flip) != 0) rc = GAM_ERR_CUDA;
+        cudaEventRecord(E->join[m], h.stream);
+        cudaStreamWaitEvent(E->root, E->join[m], 0);
+    }
+    cudaError_t e = cudaStreamEndCapture(E->root, &gr);
+    if (rc || e != cudaSuccess) {
+        std::fprintf(stderr, "gamgpu: ensemble capture failed: %s\n", cudaGetErrorString(e));
+        if (e == cudaSuccess) cudaGraphDestroy(gr);
+        return GAM_ERR_CUDA;
+    }
+    e = cudaGraphInstantiate(out, gr, 0);
+    cudaGraphDestroy(gr);
+    return e == cudaSuccess ? GAM_OK : GAM_ERR_CUDA;
+}
+int ens_build(gam_ensemble* E) {
+    ens_destroy_graphs(E);
+    for (auto* G : E->members) CK(cudaStreamSynchronize(G->h.stream));
+    int rc = ens_capture(E, 0, &E->graph[0]);
+    if (!rc) rc = ens_capture(E, 1, &E->graph[1]);
+    E->phase = 0;
+    return rc;
+}
+int ens_launch(gam_ensemble* E) {
+    CK(cudaGraphLaunch(E->graph[E->phase], E->root));
+    E->phase ^= 1;
+    for (size_t m = 0; m < E->members.size(); ++m) {
+        if (!E->active[m]) continue;
+        Handle& h = E->members[m]->h;
+        h.cur ^= 1;
+        h.launches += kernels_per_step(h);
+    }
+    return GAM_OK;
+}
+int ens_collect(gam_ensemble* E) {   // scalars of every member back to the host; OR of their statuses
+    CK(cudaStreamSynchronize(E->root));
+    bool nan = false, collapse = false;
+    for (auto* G : E->members) {
+        int rc = download_scalars(G);
+        if (rc) return rc;
+        G->lastStatus = status_code(G->h.hScal->sticky);
+        nan = nan || G->lastStatus == GAM_ERR_NAN;
+        collapse = collapse || G->lastStatus == GAM_ERR_DT_COLLAPSE;
+    }
+    return nan ? GAM_ERR_NAN : (collapse ? GAM_ERR_DT_COLLAPSE : GAM_OK);
+}
+}  // namespace
+
+extern "C" {
+
+int gam_gpu_ensemble_create(gam_ensemble_t** out, gam_gpu_t* const* members, int n) {
+    if (!out || !members || n < 1) return GAM_ERR_ARG;
+    *out = nullptr;
+    int dev0 = members[0] ? members[0]->h.device : -1;
+    for (int m = 0; m < n; ++m) {
+        if (!members[m] || members[m]->h.device != dev0) return GAM_ERR_ARG;
+        for (int q = 0; q < m; ++q)
+            if (members[q] == members[m]) return GAM_ERR_ARG;
+    }
+    gam_ensemble* E = new (std::nothrow) gam_ensemble();
+    if (!E) return GAM_ERR_ARG;
+    E->members.assign(members, members + n);
+    E->active.assign(n, 1);
+    E->join.assign(n, nullptr);
+    bool ok = cudaStreamCreateWithFlags(&E->root, cudaStreamNonBlocking) == cudaSuccess &&
+              cudaEventCreateWithFlags(&E->fork, cudaEventDisableTiming) == cudaSuccess;
+    for (int m = 0; ok && m < n; ++m) ok = cudaEventCreateWithFlags(&E->join[m], cudaEventDisableTiming) == cudaSuccess;
+    if (!ok) { gam_gpu_ensemble_destroy(E); return GAM_ERR_CUDA; }
+    *out = E;
+    return GAM_OK;
+}
+
+int gam_gpu_ensemble_run_steps(gam_ensemble_t* E, int nsteps) {
+    if (!E || nsteps < 0) return GAM_ERR_ARG;
+    if (!E->graph[0]) { int rc = ens_build(E); if (rc) return rc; }
+    for (int s = 0; s < nsteps; ++s) { int rc = ens_launch(E); if (rc) return rc; }
+    return ens_collect(E);
+}
+
+int gam_gpu_ensemble_run_steps_timed(gam_ensemble_t* E, int nsteps, double* ms) {
+    if (!E || nsteps < 0 || !ms) return GAM_ERR_ARG;
+    if (!E->graph[0]) { int rc = ens_build(E); if (rc) return rc; }
+    cudaEvent_t e0, e1;
+    CK(cudaEventCreate(&e0));
+    CK(cudaEventCreate(&e1));
+    CK(cudaStreamSynchronize(E->root));
+    CK(cudaEventRecord(e0, E->root));
+    for (int s = 0; s < nsteps; ++s) { int rc = ens_launch(E); if (rc) return rc; }
+    CK(cudaEventRecord(e1, E->root));
+    CK(cudaEventSynchronize(e1));
+    float f = 0.f;
+    cudaEventElapsedTime(&f, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    *ms = f;
+    return ens_collect(E);
+}
+
+int gam_gpu_ensemble_advance(gam_ensemble_t* E, double tEnd, int chunk, int maxSteps, int* steps) {
+    if (!E || chunk < 1 || maxSteps < 0) return GAM_ERR_ARG;
+    int taken = 0, st = GAM_OK;
+    while (taken < maxSteps) {
+        int rc = ens_collect(E);
+        if (rc == GAM_ERR_CUDA) return rc;
+        st = rc ? rc : st;
+        bool changed = false, any = false;
+        for (size_t m = 0; m < E->members.size(); ++m) {
+            bool act = E->members[m]->h.hScal->t < tEnd;
+            if ((char)act != E->active[m]) { E->active[m] = act; changed = true; }
+            any = any || act;
+        }
+        if (!any) break;
+        if (changed || !E->graph[0]) { rc = ens_build(E); if (rc) return rc; }
+        int n = chunk < maxSteps - taken ? chunk : maxSteps - taken;
+        for (int s = 0; s < n; ++s) { rc = ens_launch(E); if (rc) return rc; }
+        taken += n;
+    }
+    if (steps) *steps = taken;
+    int rc = ens_collect(E);
+    for (size_t m = 0; m < E->members.size(); ++m) E->active[m] = 1;   // later runs step every member again
+    ens_destroy_graphs(E);
+    return rc ? rc : st;
+}
+
+void gam_gpu_ensemble_destroy(gam_ensemble_t* E) {
+    if (!E) return;
+    if (E->root) cudaStreamSynchronize(E->root);
+    ens_destroy_graphs(E);
+    for (auto ev : E->join) if (ev) cudaEventDestroy(ev);
+    if (E->fork) cudaEventDestroy(E->fork);
+    if (E->root) cudaStreamDestroy(E->root);
+    delete E;
 }
 
 }  // extern "C"

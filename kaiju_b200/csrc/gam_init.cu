@@ -280,6 +280,37 @@ __global__ void k_ic_ot2d(Lay L, Par p, GridP g, StateP s) {
     s.mf[2][c] = 0.0;
 }
 
+// Kelvin-Helmholtz shear layer of the batched-ensemble problem, sampled at cell centres (the oracle's
+// initKH): rho = 1, P = 1, Vx = 0.5 tanh((y-0.5)/a), Vy = amp*(2u-1) with u a counter-based hash of
+// (seed, i, j, k) (i,j,k counted from the first active cell = 1), B = (Bx,0,0) as face fluxes Bx*n_x*area
+__device__ __forceinline__ unsigned long long splitmix64(unsigned long long x) {
+    x += 0x9E3779B97F4A7C15ull;
+    unsigned long long z = x;
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    return z ^ (z >> 31);
+}
+struct KHPar { double a, Bx, amp; unsigned long long seed; };
+__global__ void k_ic_kh(Lay L, Par p, GridP g, StateP s, KHPar kh) {
+    int ni = L.Nip + 1, nj = L.Njp + 1, nk = L.Nkp + 1;
+    long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (t >= (long long)ni * nj * nk) return;
+    int i = L.is() + (int)(t % ni);
+    long long q = t / ni;
+    int j = L.js() + (int)(q % nj), k = L.ks() + (int)(q / nj);
+    long long c = L.at(i, j, k);
+    int fi = i - L.nG + 1, fj = j - L.nG + 1, fk = k - L.nG + 1;
+    unsigned long long key = (kh.seed << 40) ^ (unsigned long long)(unsigned int)(fi + 4096 * (fj + 4096 * fk));
+    double u = (double)(splitmix64(key) >> 11) * (1.0 / 9007199254740992.0);
+    double D = 1.0, P = 1.0;
+    double Vx = 0.5 * tanh((g.xyzcc[1][c] - 0.5) / kh.a);
+    double Vy = kh.amp * (2.0 * u - 1.0), Vz = 0.0;
+    double KinE = 0.5 * D * (sq(Vx) + sq(Vy) + sq(Vz));
+    s.gas[0][c] = D; s.gas[1][c] = D * Vx; s.gas[2][c] = D * Vy; s.gas[3][c] = D * Vz;
+    s.gas[4][c] = KinE + P / (p.gamma - 1);
+    for (int d = 0; d < 3; ++d) s.mf[d][c] = kh.Bx * g.Tf[d][0][c] * g.face[d][c];
+}
+
 // initBW with the deck defaults (prob.F90:190-298): D0=1, P0=0.1, pRat=100, dRat=1, rC=0.1, B0=1
 // GasIC of the blast waves: a sphere of radius rC at (x0,y0,z0) with dRat*D0 and pRat*P0, at rest
 struct BWGas {
@@ -543,7 +574,7 @@ int add_background(Handle& h, const BgSpec& bg) {
     return 0;
 }
 
-int init_problem(Handle& h, int ic, const BgSpec* bg) {
+int init_problem(Handle& h, int ic, const BgSpec* bg, const double* icPar) {
     const Lay& L = h.L;
     cudaStream_t st = h.stream;
     GridP g = h.gridP();
@@ -551,6 +582,12 @@ int init_problem(Handle& h, int ic, const BgSpec* bg) {
     if (ic == 0) {
         long long n = (long long)(L.Nip + 1) * (L.Njp + 1) * (L.Nkp + 1);
         k_ic_ot2d<<<nb(n, 256), 256, 0, st>>>(L, h.p, g, s);
+        h.launches++;
+    } else if (ic == 3) {
+        if (!icPar) return 1;
+        KHPar kh{icPar[0], icPar[1], icPar[2], (unsigned long long)icPar[3]};
+        long long n = (long long)(L.Nip + 1) * (L.Njp + 1) * (L.Nkp + 1);
+        k_ic_kh<<<nb(n, 256), 256, 0, st>>>(L, h.p, g, s, kh);
         h.launches++;
     } else {
         Corners X = {{h.xyz[0], h.xyz[1], h.xyz[2]}};

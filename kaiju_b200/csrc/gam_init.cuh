@@ -13,5 +13,6 @@ int add_background(Handle& h, const BgSpec& bg);
 // Initial condition ic (0 = OT2D, 1 = BW) into State n, AddB0 when bg is given, then the end of
 // CalcGridInfo (init.F90:204-244): bFlux2Fld, EnforceBCs, oState = State, CalcDT,
 // oState%time = State%time - dt.
-int init_problem(Handle& h, int ic, const BgSpec* bg = nullptr);
+// icPar: the IC's parameters (GAM_IC_KH: a, Bx, amp, seed)
+int init_problem(Handle& h, int ic, const BgSpec* bg = nullptr, const double* icPar = nullptr);
 }  // namespace gam

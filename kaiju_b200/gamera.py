@@ -28,7 +28,7 @@ GAM_BC_PERIODIC, GAM_BC_ZEROGRAD, GAM_BC_LFMPOLE, GAM_BC_LFMBW = 0, 1, 2, 3
 GAM_RING_PLM, GAM_RING_PPM, GAM_RING_PCM = 0, 1, 2
 GAM_RM_8CENT, GAM_RM_7UP = 0, 1
 GAM_SYNC_STATE, GAM_SYNC_OSTATE = 1, 2
-GAM_IC_OT2D, GAM_IC_BW, GAM_IC_LFMBW = 0, 1, 2
+GAM_IC_OT2D, GAM_IC_BW, GAM_IC_LFMBW, GAM_IC_KH = 0, 1, 2, 3
 GAM_B0_UNIFORM, GAM_B0_DIPOLE = 1, 2
 TINY, HUGE = 1.0e-12, 1.0e12
 
@@ -76,6 +76,13 @@ SIGNATURES = {
     "gam_gpu_create": (C.c_int, [C.POINTER(C.c_void_p), C.POINTER(ModelC), C.POINTER(GridC), _DP, _DP, _DP, _DP, _DP,
                                  _DP, C.c_double, C.c_double]),
     "gam_gpu_create_from_corners": (C.c_int, [C.POINTER(C.c_void_p), C.POINTER(ModelC), _DP, C.c_int]),
+    "gam_gpu_ensemble_create": (C.c_int, [C.POINTER(C.c_void_p), C.POINTER(C.c_void_p), C.c_int]),
+    "gam_gpu_ensemble_run_steps": (C.c_int, [C.c_void_p, C.c_int]),
+    "gam_gpu_ensemble_run_steps_timed": (C.c_int, [C.c_void_p, C.c_int, _DP]),
+    "gam_gpu_ensemble_advance": (C.c_int, [C.c_void_p, C.c_double, C.c_int, C.c_int, C.POINTER(C.c_int)]),
+    "gam_gpu_ensemble_destroy": (None, [C.c_void_p]),
+    "gam_gpu_create_from_corners_ic": (C.c_int, [C.POINTER(C.c_void_p), C.POINTER(ModelC), _DP, C.c_int, _DP,
+                                                 C.c_int]),
     "gam_gpu_create_from_corners_b0": (C.c_int, [C.POINTER(C.c_void_p), C.POINTER(ModelC), _DP, C.c_int, C.c_int,
                                                  _DP]),
     "gam_gpu_step": (C.c_int, [C.c_void_p, _DP, C.POINTER(C.c_int), _DP]),
@@ -339,15 +346,19 @@ class GameraGPU:
         return cls(model, h)
 
     @classmethod
-    def from_corners(cls, model: Model, xyz: np.ndarray, ic: str, b0=None):
+    def from_corners(cls, model: Model, xyz: np.ndarray, ic: str, b0=None, ic_par=None):
         """Corners2Grid + initial condition (+ AddB0) + initial BCs/dt on the device.
         b0: None, ("uniform", bx, by, bz) or ("dipole", M0[, (cx, cy, cz)]); needs model.doBackground."""
         L = load_library()
         xyz = np.asfortranarray(xyz, dtype=np.float64)
         h = C.c_void_p()
         m = model.to_c()
-        icn = {"OT2D": GAM_IC_OT2D, "BW": GAM_IC_BW, "LFMBW": GAM_IC_LFMBW}[ic]
-        if b0 is None:
+        icn = {"OT2D": GAM_IC_OT2D, "BW": GAM_IC_BW, "LFMBW": GAM_IC_LFMBW, "KH": GAM_IC_KH}[ic]
+        if ic_par is not None:
+            par = np.ascontiguousarray(ic_par, dtype=np.float64)
+            rc = L.gam_gpu_create_from_corners_ic(C.byref(h), C.byref(m), _dp(xyz), icn, par.ctypes.data_as(_DP),
+                                                  len(par))
+        elif b0 is None:
             rc = L.gam_gpu_create_from_corners(C.byref(h), C.byref(m), _dp(xyz), icn)
         else:
             par = np.zeros(4)
@@ -472,3 +483,79 @@ class GameraGPU:
         if rc:
             raise GamError(rc, "gam_gpu_divb")
         return v.value
+
+
+class Ensemble:
+    """Independent problems advanced together: one CUDA graph launch per batch step holds every member's
+    step as a concurrent branch (gam_gpu_ensemble_*). The members stay owned by the caller."""
+
+    def __init__(self, members: Sequence[GameraGPU]):
+        L = load_library()
+        self.members = list(members)
+        arr = (C.c_void_p * len(self.members))(*[m.h.value if hasattr(m.h, "value") else m.h for m in self.members])
+        self.e = C.c_void_p()
+        rc = L.gam_gpu_ensemble_create(C.byref(self.e), arr, len(self.members))
+        if rc:
+            raise GamError(rc, "gam_gpu_ensemble_create")
+
+    def run_steps(self, n: int) -> int:
+        return load_library().gam_gpu_ensemble_run_steps(self.e, n)
+
+    def run_steps_timed(self, n: int):
+        ms = C.c_double()
+        rc = load_library().gam_gpu_ensemble_run_steps_timed(self.e, n, C.byref(ms))
+        return rc, ms.value
+
+    def advance(self, t_end: float, chunk: int = 8, max_steps: int = 1 << 30):
+        steps = C.c_int()
+        rc = load_library().gam_gpu_ensemble_advance(self.e, t_end, chunk, max_steps, C.byref(steps))
+        return rc, steps.value
+
+    def close(self):
+        if self.e:
+            load_library().gam_gpu_ensemble_destroy(self.e)
+            self.e = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+# ------------------------------------------------------------------ Kelvin-Helmholtz ensemble problem
+def kh_model(nx: int, fp32: bool = True, tFin: float = 2.0) -> Model:
+    """One member of the Kelvin-Helmholtz ensemble: nx x nx/2 x 4 cells on [0,2] x [0,1] x [0, 8/nx]
+    (square cells), periodic in x and z, zero-gradient in y."""
+    return Model(nx, nx // 2, 4, CFL=0.3, tFin=tFin,
+                 bc=(GAM_BC_PERIODIC, GAM_BC_PERIODIC, GAM_BC_ZEROGRAD, GAM_BC_ZEROGRAD, GAM_BC_PERIODIC,
+                     GAM_BC_PERIODIC))
+
+
+def kh_bounds(nx: int):
+    return (0.0, 2.0, 0.0, 1.0, 0.0, 8.0 / nx)
+
+
+def kh_ensemble_params(n: int = 96, seed: int = 0):
+    """Member sizes and IC parameters drawn with numpy's default_rng(seed): nx uniform in {64,128,256,512},
+    shear width a ~ U[0.01, 0.05], Bx ~ U[0, 0.2]; Vy noise amplitude 0.01, noise seed = member index."""
+    rng = np.random.default_rng(seed)
+    nx = rng.choice([64, 128, 256, 512], size=n)
+    a = rng.uniform(0.01, 0.05, size=n)
+    bx = rng.uniform(0.0, 0.2, size=n)
+    return [dict(nx=int(nx[m]), a=float(a[m]), Bx=float(bx[m]), amp=0.01, seed=m) for m in range(n)]
+
+
+def kh_member(par: dict, fp32: bool = True, tFin: float = 2.0) -> GameraGPU:
+    m = kh_model(par["nx"], fp32, tFin)
+    g = GameraGPU.from_corners(m, corners_uniform(m, kh_bounds(par["nx"])), "KH",
+                               ic_par=(par["a"], par["Bx"], par["amp"], float(par["seed"])))
+    if fp32:
+        g.set_precision(GAM_FP32FLUX)
+    return g

@@ -1908,6 +1908,38 @@ static void initOT2D(const Model& M, Grid& G, State& S) {  // prob.F90:74-119
             }
 }
 
+// Kelvin-Helmholtz shear layer of the batched-ensemble problem (no reference counterpart), sampled at cell
+// centres: rho = 1, P = 1, Vx = 0.5 tanh((y-0.5)/a), Vy = amp*(2u-1) with u a counter-based hash of
+// (seed, i, j, k), B = (Bx, 0, 0) as face fluxes Bx*n_x*area. kh = {a, Bx, amp, seed}.
+static uint64_t splitmix64(uint64_t x) {
+    x += 0x9E3779B97F4A7C15ull;
+    uint64_t z = x;
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    return z ^ (z >> 31);
+}
+static double khNoise(uint64_t seed, int i, int j, int k) {   // u in [0,1), i,j,k counted from is = 1
+    uint64_t key = (seed << 40) ^ (uint64_t)(uint32_t)(i + 4096 * (j + 4096 * k));
+    return (double)(splitmix64(key) >> 11) * (1.0 / 9007199254740992.0);
+}
+static void initKH(const Model& M, Grid& G, State& S, const double* kh) {
+    double a = kh[0], Bx = kh[1], amp = kh[2];
+    uint64_t seed = (uint64_t)kh[3];
+    for (int k = G.ks; k <= G.ke + 1; ++k)
+        for (int j = G.js; j <= G.je + 1; ++j)
+            for (int i = G.is; i <= G.ie + 1; ++i) {
+                double yc = G.xyzcc(i, j, k, 2);
+                double D = 1.0, P = 1.0;
+                double Vx = 0.5 * std::tanh((yc - 0.5) / a);
+                double Vy = amp * (2.0 * khNoise(seed, i, j, k) - 1.0), Vz = 0.0;
+                double KinE = 0.5 * D * (sq(Vx) + sq(Vy) + sq(Vz));
+                S.Gas(i, j, k, DEN) = D;
+                S.Gas(i, j, k, MOMX) = D * Vx; S.Gas(i, j, k, MOMY) = D * Vy; S.Gas(i, j, k, MOMZ) = D * Vz;
+                S.Gas(i, j, k, ENERGY) = KinE + P / (M.gamma - 1);
+                for (int d = 1; d <= 3; ++d) S.magFlux(i, j, k, d) = Bx * G.Tf(i, j, k, NORMX, d) * G.face(i, j, k, d);
+            }
+}
+
 struct BWctx { double x0, y0, z0, Vx0, Vy0, Vz0, P0, pRat, dRat, D0, rC, bScl, bSclz; };
 static void GasIC_BW(double x, double y, double z, double* W, void* c) {  // prob.F90:280-297
     BWctx* b = (BWctx*)c;
@@ -2144,6 +2176,7 @@ struct orc_params {
     // icType 2: the LFM blast wave (ICs/lfmbw.F90), bw = {x0, y0, z0, P0, pRat, D0, rC, B0}; its INI/OUTI shells
     // are bc 3 and its predictor fix is on
     double bw[8];
+    double kh[4];           // icType 3: Kelvin-Helmholtz shear layer {a, Bx, amp, seed}
 };
 
 void* orc_create(const orc_params* p) {
@@ -2192,6 +2225,7 @@ void* orc_create(const orc_params* p) {
     allocState(M, G, A->S);
     allocState(M, G, A->oS);
     if (p->icType == 0) initOT2D(M, G, A->S);
+    else if (p->icType == 3) initKH(M, G, A->S, p->kh);
     else if (p->icType == 2) {
         M.predFixLFM = true;
         M.bwD0 = p->bw[5]; M.bwP0 = p->bw[3];

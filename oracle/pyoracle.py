@@ -17,7 +17,7 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "_build", "libgamora.so")
 
-IC_OT2D, IC_BW, IC_LFMBW = 0, 1, 2
+IC_OT2D, IC_BW, IC_LFMBW, IC_KH = 0, 1, 2, 3
 GRID_UNIFORM, GRID_WARP, GRID_LFM = 0, 1, 2
 BC_PERIODIC, BC_ZEROGRAD, BC_LFMPOLE, BC_LFMBW = 0, 1, 2, 3
 # the reference's LFM blast-wave deck (tests/gamera/lfmbw.xml): prob x0, y0, z0, P0, pRat, D0, rC, B0
@@ -37,7 +37,7 @@ class OrcParams(C.Structure):
         ("b0Type", C.c_int), ("b0", C.c_double * 4),
         ("lfm", C.c_double * 4), ("dFloor", C.c_double), ("pFloor", C.c_double),
         ("doRing", C.c_int), ("ringNumR", C.c_int), ("ringNch", C.c_int * 32), ("ringRecon", C.c_int),
-        ("dtActive", C.c_int), ("bw", C.c_double * 8),
+        ("dtActive", C.c_int), ("bw", C.c_double * 8), ("kh", C.c_double * 4),
     ]
 
 
@@ -109,10 +109,13 @@ class Oracle:
     def __init__(self, Nip, Njp, Nkp, ic="OT2D", grid="uniform", bounds=None, warp_amp=0.0, CFL=0.3,
                  gamma=5.0 / 3.0, pdmb=0.75, Vd0=0.5, cHogH=0.25, cHogM=0.25, Ca=1.0e12, tFin=1.0e30,
                  doMHD=True, doBoris=False, rmeth="8CENT", doLFMLim=True, bc=None, threads=0, b0=None,
-                 lfm=None, dFloor=0.0, pFloor=0.0, ring=None, dtActive=False, bw=LFMBW_DECK):
+                 lfm=None, dFloor=0.0, pFloor=0.0, ring=None, dtActive=False, bw=LFMBW_DECK,
+                 kh=(0.03, 0.1, 0.01, 0)):
         p = OrcParams()
         p.Nip, p.Njp, p.Nkp = Nip, Njp, Nkp
-        p.icType = {"OT2D": IC_OT2D, "BW": IC_BW, "LFMBW": IC_LFMBW}[ic]
+        p.icType = {"OT2D": IC_OT2D, "BW": IC_BW, "LFMBW": IC_LFMBW, "KH": IC_KH}[ic]
+        for n in range(4):   # Kelvin-Helmholtz {a, Bx, amp, seed}
+            p.kh[n] = kh[n]
         p.gridType = {"uniform": GRID_UNIFORM, "warp": GRID_WARP, "lfm": GRID_LFM}[grid]
         if lfm is not None:   # (r_in, r_out, radial stretch ratio, theta0)
             for n in range(4):
