@@ -28,6 +28,7 @@ module gamgpu_mod
         type(c_ptr) :: xyzcc, xfc, di, dj, dk, volume, face, edge, Tf, Te, Teb
         ! background field (Grid%fcB0, edgB0, B0, bFlux0, dpB0); c_null_ptr unless Model%doBackground
         type(c_ptr) :: fcB0 = c_null_ptr, edgB0 = c_null_ptr, B0 = c_null_ptr, bFlux0 = c_null_ptr, dpB0 = c_null_ptr
+        type(c_ptr) :: xyz = c_null_ptr   ! Grid%xyz, for the slice output
     end type gam_grid_c
 
     interface

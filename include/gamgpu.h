@@ -101,6 +101,8 @@ typedef struct {
     const double* B0;      /* (Ni,Nj,Nk,3)            cell-averaged B0                   */
     const double* bFlux0;  /* (Ni,Nj,Nk,3)            B0 flux through the lower faces    */
     const double* dpB0;    /* (Ni,Nj,Nk,3)            background momentum source          */
+    /* Grid%xyz corners (Ni+1,Nj+1,Nk+1,3); optional, needed only by the slice output (current, E) */
+    const double* xyz;
 } gam_grid_c;
 
 typedef struct {
@@ -197,6 +199,22 @@ int gam_gpu_set_precision(gam_gpu_t* h, int mode);
 int gam_gpu_fetch(gam_gpu_t* h, const char* name, double* out, long long n);
 
 void gam_gpu_destroy(gam_gpu_t* h);
+
+/* Slice output: the variables writeSlc computes from State (src/gamera/gioH5.F90:255-602) for the active
+ * cells of a single-fluid problem: D, Vx, Vy, Vz, P, Cs, Bx, By, Bz (total field), Pb, Jx, Jy, Jz (the
+ * current of bFld2Jxyz, gridutils.F90:314-478) and, with GAM_SLICE_FAT (output/doFatIO), Ex, Ey, Ez
+ * (Eijk2xyz) and DivB (plus DivdB with a background field). Each variable is one Fortran-ordered
+ * (is:ie, js:je, ks:ke) block of out, in that order; gam_gpu_slice_count gives the doubles needed. The
+ * handle must know Grid%xyz (gam_grid_c.xyz, or a handle built from corners).
+ * gam_gpu_slice_begin computes the slice of the current State on the step stream and copies it to out on a
+ * separate copy stream, returning at once: steps issued afterwards run while the copy proceeds (with
+ * page-locked out; pageable memory makes the copy synchronous). gam_gpu_slice_wait waits for that copy;
+ * gam_gpu_slice does both. Replaces: the State copy-back and the host loops of writeSlc. */
+#define GAM_SLICE_FAT 1u
+long long gam_gpu_slice_count(gam_gpu_t* h, unsigned flags);
+int gam_gpu_slice_begin(gam_gpu_t* h, unsigned flags, double* out, long long n);
+int gam_gpu_slice_wait(gam_gpu_t* h);
+int gam_gpu_slice(gam_gpu_t* h, unsigned flags, double* out, long long n);
 
 /* Ensembles: independent problems (any sizes, on one device) advanced together. Each batch step is one
  * CUDA graph launch holding every active member's stepGamera as a concurrent branch; every member keeps

@@ -19,6 +19,14 @@ struct gam_gpu {
     double* scratch = nullptr;      // reduction partials
     size_t scratchDoubles = 0;
     int lastStatus = 0;
+    // slice output: device staging, scratch planes, the copy stream and its events (allocated on first use)
+    double* iobuf = nullptr;
+    double* ioscratch = nullptr;
+    size_t iobufDoubles = 0;
+    cudaStream_t copyStream = nullptr;
+    cudaEvent_t ioReady = nullptr, ioDone = nullptr;
+    bool ioPending = false;
+    bool haveCorners = false;
 };
 
 namespace {
@@ -339,6 +347,7 @@ int gam_gpu_create(gam_gpu_t** out, const gam_model_c* m, const gam_grid_c* g, c
     if (!rc) { for (int d = 0; d < 3; ++d) for (int c = 0; c < 9; ++c) pl[d * 9 + c] = h.Te[d][c]; rc = h2d_planes(G, pl, 27, g->Te, fe); }
     if (!rc) { for (int d = 0; d < 3; ++d) for (int c = 0; c < 4; ++c) pl[d * 4 + c] = h.Teb[d][c]; rc = h2d_planes(G, pl, 12, g->Teb, fe); }
     if (!rc && m->doBackground) rc = upload_background(G, g->fcB0, g->edgB0, g->B0, g->bFlux0, g->dpB0);
+    if (!rc && g->xyz) { rc = h2d_planes(G, h.xyz, 3, g->xyz, fe); G->haveCorners = true; }
     if (rc) { gam_gpu_destroy(G); return rc; }
     rc = gam_gpu_sync_to_device(G, GAM_SYNC_STATE | GAM_SYNC_OSTATE, gas, magflux, bxyz, ogas, omagflux, obxyz, time,
                                 otime);
@@ -363,6 +372,7 @@ static int create_from_corners(gam_gpu_t** out, const gam_model_c* m, const doub
     Handle& h = G->h;
     rc = h2d_planes(G, h.xyz, 3, xyz, faceExt(h.L));
     if (rc) { gam_gpu_destroy(G); return rc; }
+    G->haveCorners = true;
     h.hScal->time = m->t;   // allocState: State%time = Model%t
     h.hScal->otime = m->t;
     rc = upload_scalars(G);
@@ -630,6 +640,65 @@ int gam_gpu_fetch(gam_gpu_t* G, const char* name, double* out, long long n) {
     return GAM_OK;
 }
 
+long long gam_gpu_slice_count(gam_gpu_t* G, unsigned flags) {
+    if (!G) return -1;
+    return slice_count(G->h, (flags & GAM_SLICE_FAT) ? 1 : 0);
+}
+
+static int slice_prepare(gam_gpu* G, unsigned flags, long long n, double* out) {
+    Handle& h = G->h;
+    if (!out) return GAM_ERR_ARG;
+    if (!G->haveCorners) return GAM_ERR_ARG;   // J and E need Grid%xyz
+    long long need = slice_count(h, (flags & GAM_SLICE_FAT) ? 1 : 0);
+    if (n < need) return GAM_ERR_ARG;
+    if (!G->copyStream) {
+        CK(cudaStreamCreateWithFlags(&G->copyStream, cudaStreamNonBlocking));
+        CK(cudaEventCreateWithFlags(&G->ioReady, cudaEventDisableTiming));
+        CK(cudaEventCreateWithFlags(&G->ioDone, cudaEventDisableTiming));
+        CK(cudaMalloc(&G->ioscratch, sizeof(double) * h.L.E * 6));
+    }
+    if ((size_t)need > G->iobufDoubles) {
+        if (G->ioPending) CK(cudaEventSynchronize(G->ioDone));
+        if (G->iobuf) cudaFree(G->iobuf);
+        G->iobuf = nullptr;
+        CK(cudaMalloc(&G->iobuf, sizeof(double) * (size_t)need));
+        G->iobufDoubles = (size_t)need;
+    }
+    if (G->ioPending) CK(cudaStreamWaitEvent(h.stream, G->ioDone, 0));   // the staging buffer is free again
+    return GAM_OK;
+}
+
+int gam_gpu_slice_begin(gam_gpu_t* G, unsigned flags, double* out, long long n) {
+    if (!G) return GAM_ERR_ARG;
+    int rc = slice_prepare(G, flags, n, out);
+    if (rc) return rc;
+    Handle& h = G->h;
+    int fat = (flags & GAM_SLICE_FAT) ? 1 : 0;
+    if (enqueue_slice(h, fat, G->iobuf, G->ioscratch, h.stream) != 0) return GAM_ERR_CUDA;
+    CK(cudaEventRecord(G->ioReady, h.stream));
+    CK(cudaStreamWaitEvent(G->copyStream, G->ioReady, 0));
+    CK(cudaMemcpyAsync(out, G->iobuf, sizeof(double) * (size_t)slice_count(h, fat), cudaMemcpyDeviceToHost,
+                       G->copyStream));
+    CK(cudaEventRecord(G->ioDone, G->copyStream));
+    G->ioPending = true;
+    return GAM_OK;
+}
+
+int gam_gpu_slice_wait(gam_gpu_t* G) {
+    if (!G) return GAM_ERR_ARG;
+    if (G->ioPending) {
+        CK(cudaEventSynchronize(G->ioDone));
+        G->ioPending = false;
+    }
+    return GAM_OK;
+}
+
+int gam_gpu_slice(gam_gpu_t* G, unsigned flags, double* out, long long n) {
+    int rc = gam_gpu_slice_begin(G, flags, out, n);
+    if (rc) return rc;
+    return gam_gpu_slice_wait(G);
+}
+
 void gam_gpu_destroy(gam_gpu_t* G) {
     if (!G) return;
     Handle& h = G->h;
@@ -641,6 +710,12 @@ void gam_gpu_destroy(gam_gpu_t* G) {
     if (h.f32pool) cudaFree(h.f32pool);
     if (G->stage) cudaFree(G->stage);
     if (G->scratch) cudaFree(G->scratch);
+    if (G->copyStream) cudaStreamSynchronize(G->copyStream);
+    if (G->iobuf) cudaFree(G->iobuf);
+    if (G->ioscratch) cudaFree(G->ioscratch);
+    if (G->ioReady) cudaEventDestroy(G->ioReady);
+    if (G->ioDone) cudaEventDestroy(G->ioDone);
+    if (G->copyStream) cudaStreamDestroy(G->copyStream);
     if (h.dScal) cudaFree(h.dScal);
     if (h.hScal) cudaFreeHost(h.hScal);
     if (h.stream && h.ownStream) cudaStreamDestroy(h.stream);

@@ -108,6 +108,10 @@ void launch_ring_flux(Handle& h, cudaStream_t st);                              
 void launch_pole_e(Handle& h, double* const* E, cudaStream_t st);               // PoleE + FixEFieldLFM
 void launch_ring_average(Handle& h, const StateP& s, cudaStream_t st);          // RingAverage
 int ring_kernels_per_step(const Handle& h);
+// slice output (gam_io.cu): doubles of a slice, and the kernels that compute one into dst (device) from
+// State n with 6 scratch planes
+long long slice_count(const Handle& h, int fat);
+int enqueue_slice(Handle& h, int fat, double* dst, double* scratch, cudaStream_t st);
 void launch_ring_grid_fix(Handle& h, cudaStream_t st);                          // RingGridFix
 void ring_kernels_init();
 // allocate the float planes and convert the metrics (first switch to GAM_FP32FLUX)

@@ -29,6 +29,7 @@ GAM_RING_PLM, GAM_RING_PPM, GAM_RING_PCM = 0, 1, 2
 GAM_RM_8CENT, GAM_RM_7UP = 0, 1
 GAM_SYNC_STATE, GAM_SYNC_OSTATE = 1, 2
 GAM_IC_OT2D, GAM_IC_BW, GAM_IC_LFMBW, GAM_IC_KH = 0, 1, 2, 3
+GAM_SLICE_FAT = 1
 GAM_B0_UNIFORM, GAM_B0_DIPOLE = 1, 2
 TINY, HUGE = 1.0e-12, 1.0e12
 
@@ -61,7 +62,7 @@ class ModelC(C.Structure):
 class GridC(C.Structure):
     _fields_ = [(n, C.POINTER(C.c_double)) for n in
                 ("xyzcc", "xfc", "di", "dj", "dk", "volume", "face", "edge", "Tf", "Te", "Teb",
-                 "fcB0", "edgB0", "B0", "bFlux0", "dpB0")]
+                 "fcB0", "edgB0", "B0", "bFlux0", "dpB0", "xyz")]
 
 
 class StatusC(C.Structure):
@@ -76,6 +77,10 @@ SIGNATURES = {
     "gam_gpu_create": (C.c_int, [C.POINTER(C.c_void_p), C.POINTER(ModelC), C.POINTER(GridC), _DP, _DP, _DP, _DP, _DP,
                                  _DP, C.c_double, C.c_double]),
     "gam_gpu_create_from_corners": (C.c_int, [C.POINTER(C.c_void_p), C.POINTER(ModelC), _DP, C.c_int]),
+    "gam_gpu_slice_count": (C.c_longlong, [C.c_void_p, C.c_uint]),
+    "gam_gpu_slice_begin": (C.c_int, [C.c_void_p, C.c_uint, _DP, C.c_longlong]),
+    "gam_gpu_slice_wait": (C.c_int, [C.c_void_p]),
+    "gam_gpu_slice": (C.c_int, [C.c_void_p, C.c_uint, _DP, C.c_longlong]),
     "gam_gpu_ensemble_create": (C.c_int, [C.POINTER(C.c_void_p), C.POINTER(C.c_void_p), C.c_int]),
     "gam_gpu_ensemble_run_steps": (C.c_int, [C.c_void_p, C.c_int]),
     "gam_gpu_ensemble_run_steps_timed": (C.c_int, [C.c_void_p, C.c_int, _DP]),
@@ -336,6 +341,8 @@ class GameraGPU:
         if model.doBackground:
             for cname, key in BACKGROUND_NAMES:
                 setattr(g, cname, _dp(keep[key]))
+        if "xyz" in keep:
+            g.xyz = _dp(keep["xyz"])
         arrs = [None if a is None else np.asfortranarray(a, dtype=np.float64)
                 for a in (gas, magflux, bxyz, ogas, omagflux, obxyz)]
         h = C.c_void_p()
@@ -476,6 +483,23 @@ class GameraGPU:
             raise GamError(rc, "gam_gpu_get_status")
         return dict(t=s.t, dt=s.dt, dt0=s.dt0, time=s.time, otime=s.otime, ts=s.ts, status=s.status,
                     nanCells=s.nanCells, precision=s.precision, kernelLaunches=s.kernelLaunches)
+
+    SLICE_NAMES = ("D", "Vx", "Vy", "Vz", "P", "Cs", "Bx", "By", "Bz", "Pb", "Jx", "Jy", "Jz", "Ex", "Ey", "Ez",
+                   "DivB", "DivdB")
+
+    def slice(self, fat: bool = True, out: Optional[np.ndarray] = None) -> dict:
+        """writeSlc's variables of the current State (active cells): name -> (Nip, Njp, Nkp) Fortran array."""
+        L = load_library()
+        flags = GAM_SLICE_FAT if fat else 0
+        n = L.gam_gpu_slice_count(self.h, flags)
+        buf = np.empty(n) if out is None else out
+        rc = L.gam_gpu_slice(self.h, flags, buf.ctypes.data_as(_DP), buf.size)
+        if rc:
+            raise GamError(rc, "gam_gpu_slice")
+        m = self.model
+        nv = n // (m.Nip * m.Njp * m.Nkp)
+        arr = buf[:n].reshape((m.Nip, m.Njp, m.Nkp, nv), order="F")
+        return {self.SLICE_NAMES[v]: arr[..., v] for v in range(nv)}
 
     def divb(self) -> float:
         v = C.c_double()

@@ -2332,6 +2332,209 @@ double orc_divb(void* h) {  // gridutils.F90:717-770
     return tot;
 }
 
+// ---------------------------------------------------------------- slice output (gioH5.F90:255-602)
+// The variables writeSlc computes from State (active cells, no ghosts, single fluid, not a magnetosphere):
+// D, Vx, Vy, Vz, P, Cs, Bx, By, Bz, Pb, Jx, Jy, Jz and, with fat output, Ex, Ey, Ez, DivB (and DivdB with a
+// background field). Each variable is one (is:ie, js:je, ks:ke) Fortran block of out, in that order.
+static void ijkVecC(const Grid& G, int i, int j, int k, int d, double* v) {   // metric.F90:172-201
+    double p[3], m[3];
+    for (int c = 1; c <= 3; ++c) {
+        if (d == IDIR) {
+            p[c - 1] = 0.25 * (G.xyz(i + 1, j, k, c) + G.xyz(i + 1, j + 1, k, c) + G.xyz(i + 1, j, k + 1, c) + G.xyz(i + 1, j + 1, k + 1, c));
+            m[c - 1] = 0.25 * (G.xyz(i, j, k, c) + G.xyz(i, j + 1, k, c) + G.xyz(i, j, k + 1, c) + G.xyz(i, j + 1, k + 1, c));
+        } else if (d == JDIR) {
+            p[c - 1] = 0.25 * (G.xyz(i, j + 1, k, c) + G.xyz(i + 1, j + 1, k, c) + G.xyz(i, j + 1, k + 1, c) + G.xyz(i + 1, j + 1, k + 1, c));
+            m[c - 1] = 0.25 * (G.xyz(i, j, k, c) + G.xyz(i + 1, j, k, c) + G.xyz(i, j, k + 1, c) + G.xyz(i + 1, j, k + 1, c));
+        } else {
+            p[c - 1] = 0.25 * (G.xyz(i, j, k + 1, c) + G.xyz(i + 1, j, k + 1, c) + G.xyz(i, j + 1, k + 1, c) + G.xyz(i + 1, j + 1, k + 1, c));
+            m[c - 1] = 0.25 * (G.xyz(i, j, k, c) + G.xyz(i + 1, j, k, c) + G.xyz(i, j + 1, k, c) + G.xyz(i + 1, j + 1, k, c));
+        }
+    }
+    for (int c = 0; c < 3; ++c) v[c] = p[c] - m[c];
+    double n = norm2v(v, 3);
+    for (int c = 0; c < 3; ++c) v[c] = v[c] / n;
+}
+// CellExyz (gridutils.F90:559-609) from edge fields (EMF / edge length)
+static void cellExyz(const Grid& G, const Arr& Ef, int i, int j, int k, double* E) {
+    auto ef = [&](int a, int b, int c, int d) {
+        double e = G.edge(a, b, c, d);
+        return e == 0.0 ? 0.0 : Ef(a, b, c, d) / e;
+    };
+    double cc[3];
+    cc[0] = 0.25 * (ef(i, j, k, IDIR) + ef(i, j, k + 1, IDIR) + ef(i, j + 1, k, IDIR) + ef(i, j + 1, k + 1, IDIR));
+    cc[1] = 0.25 * (ef(i, j, k, JDIR) + ef(i, j, k + 1, JDIR) + ef(i + 1, j, k, JDIR) + ef(i + 1, j, k + 1, JDIR));
+    cc[2] = 0.25 * (ef(i, j, k, KDIR) + ef(i + 1, j, k, KDIR) + ef(i, j + 1, k, KDIR) + ef(i + 1, j + 1, k, KDIR));
+    double iV[3], jV[3], kV[3], M[3][3];
+    ijkVecC(G, i, j, k, IDIR, iV); ijkVecC(G, i, j, k, JDIR, jV); ijkVecC(G, i, j, k, KDIR, kV);
+    M[0][0] = kV[2] * jV[1] - kV[1] * jV[2]; M[1][0] = kV[0] * jV[2] - kV[2] * jV[0]; M[2][0] = kV[1] * jV[0] - kV[0] * jV[1];
+    M[0][1] = kV[1] * iV[2] - kV[2] * iV[1]; M[1][1] = kV[2] * iV[0] - kV[0] * iV[2]; M[2][1] = kV[0] * iV[1] - kV[1] * iV[0];
+    M[0][2] = jV[2] * iV[1] - jV[1] * iV[2]; M[1][2] = jV[0] * iV[2] - jV[2] * iV[0]; M[2][2] = jV[1] * iV[0] - jV[0] * iV[1];
+    double det = iV[0] * M[0][0] + jV[0] * M[0][1] + kV[0] * M[0][2];
+    for (int r = 0; r < 3; ++r) E[r] = (M[r][0] * cc[0] + M[r][1] * cc[1] + M[r][2] * cc[2]) / det;
+}
+// bFld2Jxyz (gridutils.F90:314-478): B.dl on the edges, circulation per face, then the cell field of the
+// face "fluxes" J.dS; on an LFM grid the two rings next to the axis are re-interpolated toward the pole
+static void bFld2Jxyz(const Model& M, const Grid& G, const Arr& B, Arr& J) {
+    int lo[4] = {G.isg, G.jsg, G.ksg, 1}, hiC[4] = {G.ieg, G.jeg, G.keg, 3}, hiF[4] = {G.ieg + 1, G.jeg + 1, G.keg + 1, 3};
+    Arr bInt, JdS;
+    bInt.alloc(4, lo, hiC);
+    JdS.alloc(4, lo, hiF);
+    std::fill(J.d.begin(), J.d.end(), 0.0);
+    auto goodE = [&](int i, int j, int k, int d) {
+        if (d == IDIR) return i >= G.isg && i <= G.ieg && j >= G.jsg && j <= G.jeg + 1 && k >= G.ksg && k <= G.keg + 1;
+        if (d == JDIR) return i >= G.isg && i <= G.ieg + 1 && j >= G.jsg && j <= G.jeg && k >= G.ksg && k <= G.keg + 1;
+        return i >= G.isg && i <= G.ieg + 1 && j >= G.jsg && j <= G.jeg + 1 && k >= G.ksg && k <= G.keg;
+    };
+    auto goodF = [&](int i, int j, int k, int d) {
+        if (d == IDIR) return i >= G.isg && i <= G.ieg + 1 && j >= G.jsg && j <= G.jeg && k >= G.ksg && k <= G.keg;
+        if (d == JDIR) return i >= G.isg && i <= G.ieg && j >= G.jsg && j <= G.jeg + 1 && k >= G.ksg && k <= G.keg;
+        return i >= G.isg && i <= G.ieg && j >= G.jsg && j <= G.jeg && k >= G.ksg && k <= G.keg + 1;
+    };
+    for (int k = G.ksg + 1; k <= G.keg; ++k)
+        for (int j = G.jsg + 1; j <= G.jeg; ++j)
+            for (int i = G.isg + 1; i <= G.ieg; ++i) {
+                double bA[3], dx[3];
+                if (goodE(i + 1, j, k, IDIR)) {
+                    for (int c = 1; c <= 3; ++c) {
+                        bA[c - 1] = 0.25 * (B(i, j, k, c) + B(i, j - 1, k, c) + B(i, j, k - 1, c) + B(i, j - 1, k - 1, c));
+                        dx[c - 1] = G.xyz(i + 1, j, k, c) - G.xyz(i, j, k, c);
+                    }
+                    bInt(i, j, k, IDIR) = dot3(bA, dx);
+                }
+                if (goodE(i, j + 1, k, JDIR)) {
+                    for (int c = 1; c <= 3; ++c) {
+                        bA[c - 1] = 0.25 * (B(i, j, k, c) + B(i, j, k - 1, c) + B(i - 1, j, k, c) + B(i - 1, j, k - 1, c));
+                        dx[c - 1] = G.xyz(i, j + 1, k, c) - G.xyz(i, j, k, c);
+                    }
+                    bInt(i, j, k, JDIR) = dot3(bA, dx);
+                }
+                if (goodE(i, j, k + 1, KDIR)) {
+                    for (int c = 1; c <= 3; ++c) {
+                        bA[c - 1] = 0.25 * (B(i, j, k, c) + B(i - 1, j, k, c) + B(i, j - 1, k, c) + B(i - 1, j - 1, k, c));
+                        dx[c - 1] = G.xyz(i, j, k + 1, c) - G.xyz(i, j, k, c);
+                    }
+                    bInt(i, j, k, KDIR) = dot3(bA, dx);
+                }
+            }
+    for (int k = G.ksg + 1; k <= G.keg; ++k)
+        for (int j = G.jsg + 1; j <= G.jeg; ++j)
+            for (int i = G.isg + 1; i <= G.ieg; ++i) {
+                if (goodF(i, j + 1, k + 1, IDIR))
+                    JdS(i, j, k, IDIR) = bInt(i, j, k, JDIR) + bInt(i, j + 1, k, KDIR) - bInt(i, j, k + 1, JDIR) - bInt(i, j, k, KDIR);
+                if (goodF(i + 1, j, k + 1, JDIR))
+                    JdS(i, j, k, JDIR) = bInt(i, j, k, KDIR) + bInt(i, j, k + 1, IDIR) - bInt(i + 1, j, k, KDIR) - bInt(i, j, k, IDIR);
+                if (goodF(i + 1, j + 1, k, KDIR))
+                    JdS(i, j, k, KDIR) = bInt(i, j, k, IDIR) + bInt(i + 1, j, k, JDIR) - bInt(i, j + 1, k, IDIR) - bInt(i, j, k, JDIR);
+            }
+    for (int k = G.ksg + 1; k <= G.keg - 1; ++k)
+        for (int j = G.jsg + 1; j <= G.jeg - 1; ++j)
+            for (int i = G.isg + 1; i <= G.ieg - 1; ++i) {
+                double b[3];
+                gamCellBxyz(G, JdS, i, j, k, b);
+                for (int c = 0; c < 3; ++c) J(i, j, k, c + 1) = 1.0 * b[c];
+            }
+    if (M.doRing) {   // gridutils.F90:414-470, active rings only (the ghost copies do not reach the output)
+        const int Nk = G.ke - G.ks + 1;
+        const double a8 = (double)0.8f, a2 = (double)0.2f, a4 = (double)0.4f, a6 = (double)0.6f;
+        for (int i = G.isg + 1; i <= G.ieg - 1; ++i)
+            for (int side = 0; side < 2; ++side) {
+                if ((side == 0 && !M.R.doS) || (side == 1 && !M.R.doE)) continue;
+                int j3 = side == 0 ? G.js + 2 : G.je - 2, j1 = side == 0 ? G.js : G.je, j2 = side == 0 ? G.js + 1 : G.je - 1;
+                double J0[3] = {0.0, 0.0, 0.0};
+                for (int k = G.ks; k <= G.ke; ++k)
+                    for (int c = 0; c < 3; ++c) J0[c] = J0[c] + J(i, j3, k, c + 1);
+                for (int c = 0; c < 3; ++c) J0[c] = J0[c] / Nk;
+                for (int k = G.ks; k <= G.ke; ++k)
+                    for (int c = 0; c < 3; ++c) {
+                        double J3 = J(i, j3, k, c + 1);
+                        J(i, j1, k, c + 1) = a8 * J0[c] + a2 * J3;
+                        J(i, j2, k, c + 1) = a4 * J0[c] + a6 * J3;
+                    }
+            }
+    }
+}
+
+static long sliceCount(const App& A, int fat) {
+    long nv = 13 + (fat ? 4 + (A.M.doBackground ? 1 : 0) : 0);
+    return nv * (long)A.G.Nip * A.G.Njp * A.G.Nkp;
+}
+
+// writeSlc's variables of the current State (see sliceCount for the layout); returns the doubles written
+long orc_slice(void* h, int fat, double* out) {
+    App* A = (App*)h;
+    const Model& M = A->M;
+    const Grid& G = A->G;
+    const State& S = A->S;
+    const long Na = (long)G.Nip * G.Njp * G.Nkp;
+    auto o = [&](int v, int i, int j, int k) -> double& {
+        return out[v * Na + (i - G.is) + (long)G.Nip * ((j - G.js) + (long)G.Njp * (k - G.ks))];
+    };
+    int lo[4] = {G.isg, G.jsg, G.ksg, 1}, hi[4] = {G.ieg, G.jeg, G.keg, 3};
+    Arr J;
+    J.alloc(4, lo, hi);
+    if (M.doMHD) bFld2Jxyz(M, G, S.Bxyz, J);
+    for (int k = G.ks; k <= G.ke; ++k)
+        for (int j = G.js; j <= G.je; ++j)
+            for (int i = G.is; i <= G.ie; ++i) {
+                double D = S.Gas(i, j, k, DEN), Mx = S.Gas(i, j, k, MOMX), My = S.Gas(i, j, k, MOMY), Mz = S.Gas(i, j, k, MOMZ);
+                double En = S.Gas(i, j, k, ENERGY);
+                o(0, i, j, k) = D < 0.0 ? 0.0 : D;   // vacuum mask with the bulk floor 0
+                double V[3] = {0.0, 0.0, 0.0}, P = 0.0;
+                if (D > TINY) {
+                    V[0] = Mx / D; V[1] = My / D; V[2] = Mz / D;
+                    P = (M.gamma - 1) * (En - 0.5 * (Mx * Mx + My * My + Mz * Mz) / D);
+                }
+                o(1, i, j, k) = V[0]; o(2, i, j, k) = V[1]; o(3, i, j, k) = V[2]; o(4, i, j, k) = P;
+                {   // CellPress2Cs (gamutils.F90:324-341)
+                    double rho = fmaxd(D, M.dFloor);
+                    double vx = Mx / rho, vy = My / rho, vz = Mz / rho;
+                    double KinE = 0.5 * rho * (sq(vx) + sq(vy) + sq(vz));
+                    double Pc = fmaxd((M.gamma - 1) * (En - KinE), M.pFloor);
+                    o(5, i, j, k) = std::sqrt(M.gamma * Pc / rho);
+                }
+                double B[3] = {0.0, 0.0, 0.0};
+                if (M.doMHD)
+                    for (int c = 0; c < 3; ++c) B[c] = S.Bxyz(i, j, k, c + 1) + (M.doBackground ? G.B0(i, j, k, c + 1) : 0.0);
+                for (int c = 0; c < 3; ++c) o(6 + c, i, j, k) = B[c];
+                o(9, i, j, k) = 0.5 * (sq(B[0]) + sq(B[1]) + sq(B[2]));
+                for (int c = 0; c < 3; ++c) o(10 + c, i, j, k) = M.doMHD ? J(i, j, k, c + 1) : 0.0;
+                if (!fat) continue;
+                double E[3] = {0.0, 0.0, 0.0};
+                if (M.doMHD) cellExyz(G, S.Efld, i, j, k, E);
+                for (int c = 0; c < 3; ++c) o(13 + c, i, j, k) = E[c];
+                const Arr& mf = S.magFlux;
+                double dF = mf(i, j, k, IDIR) - mf(i + 1, j, k, IDIR) + mf(i, j, k, JDIR) - mf(i, j + 1, k, JDIR) +
+                            mf(i, j, k, KDIR) - mf(i, j, k + 1, KDIR);
+                double dFi = mf(i, j, k, IDIR) - mf(i + 1, j, k, IDIR), dFj = mf(i, j, k, JDIR) - mf(i, j + 1, k, JDIR),
+                       dFk = mf(i, j, k, KDIR) - mf(i, j, k + 1, KDIR);
+                (void)dF;
+                double dFi0 = 0.0, dFj0 = 0.0, dFk0 = 0.0;
+                if (M.doBackground) {
+                    dFi0 = G.bFlux0(i, j, k, IDIR) - G.bFlux0(i + 1, j, k, IDIR);
+                    dFj0 = G.bFlux0(i, j, k, JDIR) - G.bFlux0(i, j + 1, k, JDIR);
+                    dFk0 = G.bFlux0(i, j, k, KDIR) - G.bFlux0(i, j, k + 1, KDIR);
+                }
+                o(16, i, j, k) = std::fabs(dFi + dFj + dFk + dFi0 + dFj0 + dFk0);
+                if (M.doBackground) o(17, i, j, k) = std::fabs(dFi + dFj + dFk + 0.0 + 0.0 + 0.0);
+            }
+    if (fat && M.doRing) {   // FixRAVec (gioH5.F90:577-601, metric.F90:227-300) on E
+        const int Nk = G.ke - G.ks + 1;
+        const double w1 = (double)(2.0f / 3.0f), w2 = (double)(1.0f / 3.0f);
+        for (int i = G.is; i <= G.ie; ++i)
+            for (int side = 0; side < 2; ++side) {
+                if ((side == 0 && !M.R.doS) || (side == 1 && !M.R.doE)) continue;
+                int jin = side == 0 ? G.js : G.je, jout = side == 0 ? G.js + 1 : G.je - 1;
+                for (int c = 0; c < 3; ++c) {
+                    double Q0 = 0.0;
+                    for (int k = G.ks; k <= G.ke; ++k) Q0 = Q0 + o(13 + c, i, jout, k);
+                    Q0 = Q0 / Nk;
+                    for (int k = G.ks; k <= G.ke; ++k) o(13 + c, i, jin, k) = w1 * Q0 + w2 * o(13 + c, i, jout, k);
+                }
+            }
+    }
+    return sliceCount(*A, fat);
+}
+
 // Known-answer helpers for the reference's unit tests
 void orc_c2p(double gamma, const double* con, double* prim) { Model M; M.gamma = gamma; CellC2P(M, con, prim); }
 void orc_p2c(double gamma, const double* prim, double* con) { Model M; M.gamma = gamma; CellP2C(M, prim, con); }

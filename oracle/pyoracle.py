@@ -77,6 +77,8 @@ def lib():
         L.orc_volume_integral.argtypes = [C.POINTER(C.c_double)] * 3
         L.orc_recon_lr.argtypes = [C.c_int, C.c_double] + [C.POINTER(C.c_double)] * 4
         L.orc_num_threads.restype = C.c_int
+        L.orc_slice.restype = C.c_long
+        L.orc_slice.argtypes = [C.c_void_p, C.c_int, C.POINTER(C.c_double)]
         _lib = L
     return _lib
 
@@ -208,6 +210,19 @@ class Oracle:
 
     def divb(self) -> float:
         return lib().orc_divb(self.h)
+
+    SLICE_NAMES = ("D", "Vx", "Vy", "Vz", "P", "Cs", "Bx", "By", "Bz", "Pb", "Jx", "Jy", "Jz", "Ex", "Ey", "Ez",
+                   "DivB", "DivdB")
+
+    def slice(self, fat=True) -> dict:
+        """writeSlc's variables of the current State, active cells, Fortran order: name -> (Nip,Njp,Nkp)."""
+        Nip, Njp, Nkp = self.shape
+        nv = 13 + (4 + (1 if self.params.b0Type else 0) if fat else 0)
+        out = np.zeros(nv * Nip * Njp * Nkp)
+        n = lib().orc_slice(self.h, int(fat), dptr(out))
+        assert n == out.size
+        out = out.reshape((Nip, Njp, Nkp, nv), order="F")
+        return {self.SLICE_NAMES[v]: out[..., v] for v in range(nv)}
 
 
 def c2p(con, gamma=5.0 / 3.0):

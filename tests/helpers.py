@@ -1,7 +1,7 @@
 """Shared helpers: build matched oracle / device problems and compare arrays."""
 import numpy as np
 
-GRID_NAMES = ("xyzcc", "xfc", "di", "dj", "dk", "volume", "face", "edge", "tf", "te", "teb")
+GRID_NAMES = ("xyzcc", "xfc", "di", "dj", "dk", "volume", "face", "edge", "tf", "te", "teb", "xyz")
 BACKGROUND_NAMES = ("fcb0", "edgb0", "b0", "bflux0", "dpb0")
 
 

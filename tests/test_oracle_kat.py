@@ -162,3 +162,12 @@ def test_lfm_ring_k_periodicity(oracle_lib):
     assert np.abs(v[I, J, ks] - v[I, J, ke + 1]).max() == 0.0
     scale = np.abs(o.get("magflux")).max() * n[0] * n[1] * n[2]
     assert o.divb() <= d0 + 1e-13 * scale
+
+
+def test_slice_current_of_uniform_field(oracle_lib):
+    """writeSlc's current of the blast wave's uniform field is zero to round-off; DivB per cell too."""
+    o = oracle_lib.Oracle(16, 16, 16, ic="BW", grid="uniform", bounds=(-0.5, 0.5) * 3, CFL=0.3, bc=[1] * 6)
+    s = o.slice(fat=True)
+    assert max(np.abs(s[c]).max() for c in ("Jx", "Jy", "Jz")) <= 1e-12
+    assert np.abs(s["DivB"]).max() <= 1e-15
+    assert np.allclose(s["Bx"], 0.5 ** 0.5, rtol=1e-6) and np.allclose(s["Bz"], 0.0, atol=1e-14)
