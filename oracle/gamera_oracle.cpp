@@ -60,7 +60,9 @@ enum { XNQI = 1, YNQI, XNQJ, YNQJ };
 enum { INI = 1, OUTI, INJ, OUTJ, INK, OUTK };
 // Boundary classes: periodic, zero-gradient, the LFM axis (lfmIn/lfmOut, bcs.F90:1020-1106) for INJ/OUTJ,
 // and the LFM blast-wave problem's fixed inner/outer shells (ICs/lfmbw.F90:141-249) for INI/OUTI
-enum { BC_PERIODIC = 0, BC_ZEROGRAD = 1, BC_LFMPOLE = 2, BC_LFMBW = 3 };
+// BC_HALO: a tile face inside a decomposed domain (no physical BC; gamapp_mpi.F90's halo exchange fills
+// the ghosts, and the dt domain takes no ghost layer there, init.F90:519-538)
+enum { BC_PERIODIC = 0, BC_ZEROGRAD = 1, BC_LFMPOLE = 2, BC_LFMBW = 3, BC_HALO = 4 };
 enum { SPOLE = 1, EPOLE = 2 };
 enum { RR_PLM = 0, RR_PPM = 1, RR_PCM = 2, RR_WENO = 3 };
 static const int NFTMAX = 2;
@@ -1254,6 +1256,7 @@ static void lfmbwShellBC(const Model& M, const Grid& G, State& S, int dir) {
 static void EnforceBCs(const Model& M, const Grid& G, State& S) {  // step.F90:17-55
     for (int n = 1; n <= 6; ++n) {
         int kind = G.bc[n - 1];
+        if (kind == BC_HALO) continue;
         if (kind == BC_PERIODIC) periodicBC(M, G, S, n);
         else if (kind == BC_LFMPOLE) lfmPoleBC(M, G, S, n);
         else if (kind == BC_LFMBW) lfmbwShellBC(M, G, S, n);
@@ -2177,6 +2180,7 @@ struct orc_params {
     // are bc 3 and its predictor fix is on
     double bw[8];
     double kh[4];           // icType 3: Kelvin-Helmholtz shear layer {a, Bx, amp, seed}
+    const double* xyzIn;    // corners (Ni+1,Nj+1,Nk+1,3), Fortran layout, replacing the generated ones (a tile)
 };
 
 void* orc_create(const orc_params* p) {
@@ -2218,9 +2222,21 @@ void* orc_create(const orc_params* p) {
                     lfmCorner(p->lfm, G, i, j, k, &x, &y, &z);
                 }
                 G.xyz(i, j, k, 1) = x; G.xyz(i, j, k, 2) = y; G.xyz(i, j, k, 3) = z;
+                if (p->xyzIn) {
+                    long nc = (long)(G.Ni + 1) * (G.Nj + 1) * (G.Nk + 1);
+                    long q = (long)(i - G.isg) + (long)(G.Ni + 1) * ((j - G.jsg) + (long)(G.Nj + 1) * (k - G.ksg));
+                    for (int c = 0; c < 3; ++c) G.xyz(i, j, k, c + 1) = p->xyzIn[q + c * nc];
+                }
             }
     SetDomain(G);
     if (p->dtActive) { G.isDT = G.is; G.ieDT = G.ie; G.jsDT = G.js; G.jeDT = G.je; G.ksDT = G.ks; G.keDT = G.ke; }
+    // tile faces: the dt domain stops at the active cells (SetDomain adds a ghost layer only at physical BCs)
+    if (G.bc[0] == BC_HALO) G.isDT = G.is;
+    if (G.bc[1] == BC_HALO) G.ieDT = G.ie;
+    if (G.bc[2] == BC_HALO) G.jsDT = G.js;
+    if (G.bc[3] == BC_HALO) G.jeDT = G.je;
+    if (G.bc[4] == BC_HALO) G.ksDT = G.ks;
+    if (G.bc[5] == BC_HALO) G.keDT = G.ke;
     if (Corners2Grid(M, G) != 0) { delete A; return nullptr; }
     allocState(M, G, A->S);
     allocState(M, G, A->oS);

@@ -19,7 +19,7 @@ LIB_PATH = os.path.join(HERE, "_build", "libgamora.so")
 
 IC_OT2D, IC_BW, IC_LFMBW, IC_KH = 0, 1, 2, 3
 GRID_UNIFORM, GRID_WARP, GRID_LFM = 0, 1, 2
-BC_PERIODIC, BC_ZEROGRAD, BC_LFMPOLE, BC_LFMBW = 0, 1, 2, 3
+BC_PERIODIC, BC_ZEROGRAD, BC_LFMPOLE, BC_LFMBW, BC_HALO = 0, 1, 2, 3, 4
 # the reference's LFM blast-wave deck (tests/gamera/lfmbw.xml): prob x0, y0, z0, P0, pRat, D0, rC, B0
 LFMBW_DECK = (-50.0, 30.0, 0.0, 0.1, 10.0, 1.0, 20.0, 1.0)
 RM_8CENT, RM_7UP = 0, 1
@@ -38,6 +38,7 @@ class OrcParams(C.Structure):
         ("lfm", C.c_double * 4), ("dFloor", C.c_double), ("pFloor", C.c_double),
         ("doRing", C.c_int), ("ringNumR", C.c_int), ("ringNch", C.c_int * 32), ("ringRecon", C.c_int),
         ("dtActive", C.c_int), ("bw", C.c_double * 8), ("kh", C.c_double * 4),
+        ("xyzIn", C.POINTER(C.c_double)),
     ]
 
 
@@ -112,7 +113,7 @@ class Oracle:
                  gamma=5.0 / 3.0, pdmb=0.75, Vd0=0.5, cHogH=0.25, cHogM=0.25, Ca=1.0e12, tFin=1.0e30,
                  doMHD=True, doBoris=False, rmeth="8CENT", doLFMLim=True, bc=None, threads=0, b0=None,
                  lfm=None, dFloor=0.0, pFloor=0.0, ring=None, dtActive=False, bw=LFMBW_DECK,
-                 kh=(0.03, 0.1, 0.01, 0)):
+                 kh=(0.03, 0.1, 0.01, 0), xyz=None):
         p = OrcParams()
         p.Nip, p.Njp, p.Nkp = Nip, Njp, Nkp
         p.icType = {"OT2D": IC_OT2D, "BW": IC_BW, "LFMBW": IC_LFMBW, "KH": IC_KH}[ic]
@@ -132,6 +133,9 @@ class Oracle:
         p.dtActive = int(dtActive)
         for n in range(8):
             p.bw[n] = bw[n]
+        if xyz is not None:   # corners of a tile, (Ni+1, Nj+1, Nk+1, 3) Fortran order
+            self._xyz = np.asfortranarray(xyz, dtype=np.float64)
+            p.xyzIn = self._xyz.ctypes.data_as(C.POINTER(C.c_double))
         if bounds is None:
             bounds = (0.0, 1.0, 0.0, 1.0, 0.0, 1.0)
         for n in range(6):
