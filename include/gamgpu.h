@@ -38,6 +38,9 @@ extern "C" {
 #define GAM_BC_LFMPOLE 2       /* INJ/OUTJ across the LFM axis: lfmIn/lfmOut, src/gamera/bcs.F90:1020-1106 */
 #define GAM_BC_LFMBW 3         /* INI/OUTI fixed-gas shells of the LFM blast wave: bw_ibcI/bw_obcI,
                                   src/gamera/ICs/lfmbw.F90:141-225 (gas state gam_model_c.bwD0/bwP0) */
+#define GAM_BC_HALO 4          /* INK/OUTK of a k-tile inside a decomposed problem: no physical BC, the ghost
+                                  layers are filled from the neighbouring tile (the reference's mpiNullBc_T,
+                                  src/gamera/mpi/gamapp_mpi.F90:428-463); not with doRing or do25D */
 
 /* ring reconstruction (ring/rngrec, src/gamera/init.F90:466-478) */
 #define GAM_RING_PLM 0
@@ -246,6 +249,48 @@ void gam_gpu_ensemble_destroy(gam_ensemble_t* e);   /* the members are not destr
  * calls that overlap on the GPU (from several host threads or streams) race. */
 #define GAM_DIVB_NOALLOC_MAX_CELLS (256LL * 256LL * 256LL)
 int gam_divb_noalloc(const double* magflux_dev, int Nip, int Njp, int Nkp, int nG, double* tot_dev);
+/* ---- tiled runs: one problem split along k into tiles (src/gamera/mpi/gamapp_mpi.F90) ----
+ * A tile is a handle created for its k range (its corners with 4 ghost layers of the global grid)
+ * with GAM_BC_HALO on every k face that borders another tile (both k faces of every tile when the
+ * global K boundary is periodic). Tiles need the same Nip and Njp and at least 4 active k cells. */
+typedef struct gam_tiles gam_tiles_t;
+
+/* All tiles in this process, ordered along k, on one GPU or on GPUs with peer access. Fills the tiles'
+ * halos of State and oState (Bxyz included) from their neighbours and sets every tile's dt to the
+ * minimum over the tiles, as Hatch_mpi leaves a decomposed problem. The tiles stay owned by the caller
+ * and are stepped only through the group from then on. Replaces: Hatch_mpi's halo set-up and
+ * CalcDT_mpi (gamapp_mpi.F90:79-497, :501-518). */
+int gam_tiles_create(gam_tiles_t** g, gam_gpu_t* const* tiles, int n, int periodicK);
+/* nsteps of stepGamera_mpi (gamapp_mpi.F90:665-692) over all tiles; returns the worst status */
+int gam_tiles_run_steps(gam_tiles_t* g, int nsteps);
+int gam_tiles_run_steps_timed(gam_tiles_t* g, int nsteps, double* ms);
+void gam_tiles_destroy(gam_tiles_t* g);   /* the tiles are not destroyed */
+
+/* One process per GPU: the pieces of stepGamera_mpi for a host that moves the halos itself (NCCL
+ * send/recv, MPI). All work is enqueued on the handle's stream (gam_gpu_stream). The dt words are
+ * two 64-bit integers in device memory; the host reduces them with MIN over the tiles between
+ * gam_gpu_step_local and gam_gpu_step_bcs (one all-reduce replaces CalcDT_mpi's MPI_AllReduce,
+ * gamapp_mpi.F90:501-518). A step is:
+ *   step_local(words) ; allreduce MIN(words) ; step_bcs(words) ;
+ *   halo_pack(side 0 and 1, GAM_HALO_STATE) ; exchange ; halo_unpack(side 0 and 1) ; step_ghosts
+ * where side 0 is the lower k neighbour, side 1 the upper, and the message packed for side s is the one
+ * the neighbour there unpacks on side 1-s. Initial set-up: halo_pack/unpack with
+ * GAM_HALO_STATE|GAM_HALO_OSTATE|GAM_HALO_BXYZ, then calcdt_local ; allreduce ; calcdt_finish.
+ * Replaces: haloUpdate and updateMpiBCs (gamapp_mpi.F90:579-663, :694-794). */
+#define GAM_HALO_STATE 1u      /* State (between step_bcs and step_ghosts: the new state)            */
+#define GAM_HALO_OSTATE 2u     /* oState                                                             */
+#define GAM_HALO_BXYZ 4u       /* include Bxyz (set-up only: a step recomputes the halo's Bxyz)       */
+int gam_gpu_stream(gam_gpu_t* h, void** stream);   /* the cudaStream_t the handle enqueues on */
+int gam_gpu_step_local(gam_gpu_t* h, long long* dtWordsDev);
+int gam_gpu_step_bcs(gam_gpu_t* h, const long long* dtWordsDev);
+int gam_gpu_step_ghosts(gam_gpu_t* h);     /* completes the step; returns its status */
+int gam_gpu_calcdt_local(gam_gpu_t* h, long long* dtWordsDev);
+int gam_gpu_calcdt_finish(gam_gpu_t* h, const long long* dtWordsDev);
+/* bytes of the message this tile sends to / receives from its neighbour on `side` */
+int gam_gpu_halo_bytes(gam_gpu_t* h, int side, unsigned what, long long* sendBytes, long long* recvBytes);
+int gam_gpu_halo_pack(gam_gpu_t* h, int side, unsigned what, void* dstDev);          /* 16-byte aligned */
+int gam_gpu_halo_unpack(gam_gpu_t* h, int side, unsigned what, const void* srcDev);  /* 16-byte aligned */
+
 const char* gam_gpu_errstr(int code);
 
 #ifdef __cplusplus

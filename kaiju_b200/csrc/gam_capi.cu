@@ -113,8 +113,11 @@ int check_model(const gam_model_c* m) {
     for (int n = 0; n < 6; ++n) {
         int b = m->bc[n];
         bool ok = b == GAM_BC_PERIODIC || b == GAM_BC_ZEROGRAD || (b == GAM_BC_LFMPOLE && (n == 2 || n == 3)) ||
-                  (b == GAM_BC_LFMBW && n < 2);
+                  (b == GAM_BC_LFMBW && n < 2) || (b == GAM_BC_HALO && n >= 4);
         if (!ok) return GAM_ERR_UNSUPPORTED;
+        // k tiles: ring averaging needs whole rings in k, 2.5D replicates the single k layer
+        if (b == GAM_BC_HALO && (m->doRing || m->do25D)) return GAM_ERR_UNSUPPORTED;
+        if (b == GAM_BC_HALO && m->Nkp < m->nG) return GAM_ERR_ARG;
         if (b == GAM_BC_LFMPOLE && !m->doRing) return GAM_ERR_ARG;   // the axis maps need Model%Ring
     }
     if (m->doRing) {   // InitRings checks (ringutils.F90:203-225) and the device ring sizes

@@ -21,7 +21,9 @@ constexpr double PI = 3.14159265358979323846264338327950288;
 
 enum { IDIR = 0, JDIR = 1, KDIR = 2 };
 enum { RM_8CENT = 0, RM_7UP = 1 };
-enum { BC_PERIODIC = 0, BC_ZEROGRAD = 1, BC_LFMPOLE = 2, BC_LFMBW = 3 };
+// BC_HALO: a face between two k-tiles of one problem; no physical BC runs there, its ghost layers are
+// filled from the neighbouring tile after the step (the reference's mpiNullBc_T, gamapp_mpi.F90:428-463)
+enum { BC_PERIODIC = 0, BC_ZEROGRAD = 1, BC_LFMPOLE = 2, BC_LFMBW = 3, BC_HALO = 4 };
 
 struct Lay {
     int Nip, Njp, Nkp;     // active cells
@@ -62,6 +64,9 @@ struct Scal {
     int sticky;                       // OR of status over steps since the last reset
     unsigned int lastNan;             // nanCount of the last CalcDT
     int pad;
+    // tiled runs: {dtMinBits, ~nanCount} of this tile, reduced with MIN across the tiles (so the second
+    // word carries the largest NaN count) before the dt is finalized
+    unsigned long long red[2];
 };
 
 // Device field bundle. Planes are contiguous arrays of Lay::E doubles.

@@ -276,6 +276,9 @@ __global__ void k_bflux2fld_ghost(Lay L, GridP g, StateP s) {
 __global__ void k_calcdt(Lay L, Par p, GridP g, StateP s, Scal* sc) {
     Reg r = {L.is() - 1, L.Nip + 2, L.js() - 1, L.Njp + 2, L.ks() - 1, L.Nkp + 2};
     if (p.dtActive) r = Reg{L.is(), L.Nip, L.js(), L.Njp, L.ks(), L.Nkp};
+    // a tile face has no ghost layer in the dt domain (ksDT = ks, keDT = ke; gamapp_mpi.F90:441-462)
+    if (!p.dtActive && p.bc[4] == BC_HALO) { r.k0 += 1; r.nk -= 1; }
+    if (!p.dtActive && p.bc[5] == BC_HALO) r.nk -= 1;
     int i, j, k;
     double dtijk = HUGEV * 2.0;
     bool isnan_ = false;
@@ -511,7 +514,9 @@ __global__ void k_bc_k(Lay L, Par p, StateP s) {
     int i = (int)(t % ni), j = (int)(t / ni);
     bool cell = (i < L.Ni) && (j < L.Nj);
     int ks = L.ks(), ke = L.ke(), nG = L.nG;
-    if (p.bc[4] == BC_PERIODIC) {
+    if (p.bc[4] == BC_HALO) {
+        // filled from the lower tile after the step
+    } else if (p.bc[4] == BC_PERIODIC) {
         for (int n = 1; n <= nG; ++n) {
             long long d = L.at(i, j, ks - n), sidx = p.do25D ? L.at(i, j, ks) : L.at(i, j, ke - n + 1);
             if (cell) cpcell(s, d, sidx, true);
@@ -524,7 +529,9 @@ __global__ void k_bc_k(Lay L, Par p, StateP s) {
             cpmf(s, d, sidx);
         }
     }
-    if (p.bc[5] == BC_PERIODIC) {
+    if (p.bc[5] == BC_HALO) {
+        // filled from the upper tile after the step
+    } else if (p.bc[5] == BC_PERIODIC) {
         for (int n = 1; n <= nG; ++n) {
             if (p.do25D) {
                 long long d = L.at(i, j, ks + n), sidx = L.at(i, j, ks);
@@ -631,12 +638,21 @@ void launch_bcs(Handle& h, const StateP& s, cudaStream_t st) {
     h.launches += 3;
 }
 
-void launch_calcdt(Handle& h, const StateP& s, int mode, cudaStream_t st) {
+void launch_calcdt_partial(Handle& h, const StateP& s, cudaStream_t st) {
     const Lay& L = h.L;
     long long n = (long long)(L.Nip + 2) * (L.Njp + 2) * (L.Nkp + 2);
     k_calcdt<<<nblk(n, 256), 256, 0, st>>>(L, h.p, h.gridP(), s, h.dScal);
+    h.launches++;
+}
+
+void launch_dt_finalize(Handle& h, int mode, cudaStream_t st) {
     k_dt_finalize<<<1, 1, 0, st>>>(h.p, h.dScal, mode);
-    h.launches += 2;
+    h.launches++;
+}
+
+void launch_calcdt(Handle& h, const StateP& s, int mode, cudaStream_t st) {
+    launch_calcdt_partial(h, s, st);
+    launch_dt_finalize(h, mode, st);
 }
 
 __global__ void k_to_f32(const double* src, float* dst, long long n) {
@@ -727,7 +743,7 @@ static void enqueue_hot(Handle& h, const StateP& nS, cudaStream_t st, cudaEvent_
     enqueue_fluxes(h, nS, st);
 }
 
-int step_enqueue(Handle& h, int cur, cudaEvent_t* ev) {
+int step_enqueue(Handle& h, int cur, cudaEvent_t* ev, bool split) {
     cudaStream_t st = h.stream;
     auto mark = [&](int ph) { if (ev) cudaEventRecord(ev[ph], st); };
     mark(PH_PREDICT);
@@ -796,19 +812,37 @@ int step_enqueue(Handle& h, int cur, cudaEvent_t* ev) {
     k_update_gas<<<nblk(ncell, TPB), TPB, 0, st>>>(L, p, g, nS, oS, dGH, dGM, h.dScal);
     h.launches += 4;
     if (p.doRing) launch_ring_average(h, oS, st);   // mhdgroup.F90:68-74
-    // CalcDT, EnforceBCs, bFlux2Fld on the new state
+    // CalcDT (the per-cell minimum; finalized below, or after the tiles' minimum for a tiled run)
     mark(PH_DT);
-    launch_calcdt(h, oS, 0, st);
-    mark(PH_BCS);
-    launch_bcs(h, oS, st);
-    if (p.do25D) launch_bflux2fld(h, oS, st);   // the 2.5D K replication rewrites an active cell's upper face
-    else {
-        k_bflux2fld_ghost<<<nblk(ncell, TPB), TPB, 0, st>>>(L, g, oS);
-        h.launches++;
-        if (p.doRing) launch_ring_bfix(h, oS, st);
+    launch_calcdt_partial(h, oS, st);
+    if (!split) {
+        step_enqueue_bcs(h, cur, ev);
+        step_enqueue_ghosts(h, cur);
+        mark(NPHASE);
     }
-    mark(NPHASE);
     return (int)cudaGetLastError();
+}
+
+// The rest of CalcDT, then EnforceBCs on the new state S[cur ^ 1]
+void step_enqueue_bcs(Handle& h, int cur, cudaEvent_t* ev) {
+    cudaStream_t st = h.stream;
+    launch_dt_finalize(h, 0, st);
+    if (ev) cudaEventRecord(ev[PH_BCS], st);
+    launch_bcs(h, h.S[cur ^ 1], st);
+}
+
+// bFlux2Fld of the ghost cells of the new state S[cur ^ 1], after the BCs (and the halo fill of a tile)
+void step_enqueue_ghosts(Handle& h, int cur) {
+    cudaStream_t st = h.stream;
+    const Lay& L = h.L;
+    StateP s = h.S[cur ^ 1];
+    long long ncell = (long long)L.Ni * L.Nj * L.Nk;
+    if (h.p.do25D) launch_bflux2fld(h, s, st);   // the 2.5D K replication rewrites an active cell's upper face
+    else {
+        k_bflux2fld_ghost<<<nblk(ncell, TPB), TPB, 0, st>>>(L, h.gridP(), s);
+        h.launches++;
+        if (h.p.doRing) launch_ring_bfix(h, s, st);
+    }
 }
 
 double launch_divb(Handle& h, double* scratchDev, cudaStream_t st) {

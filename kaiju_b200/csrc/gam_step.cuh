@@ -71,6 +71,7 @@ struct Handle {
     Scal* dScal = nullptr;   // device scalars
     Scal* hScal = nullptr;   // pinned host mirror
     int cur = 0;
+    int tilePhase = 0;       // split-step position of a tile (gam_tiles.cu): 0 between steps
 
     cudaGraphExec_t graph[2] = {nullptr, nullptr};
     bool useGraph = true;
@@ -82,7 +83,13 @@ struct Handle {
 };
 
 // Enqueue one full stepGamera on h.stream with State n = S[cur]. Does not flip cur.
-int step_enqueue(Handle& h, int cur, cudaEvent_t* phaseEv = nullptr);
+int step_enqueue(Handle& h, int cur, cudaEvent_t* phaseEv = nullptr, bool split = false);
+// split = true stops after the per-cell CalcDT minimum (into Scal::dtMinBits); a tiled run then reduces
+// the minimum over its tiles and continues with step_enqueue_bcs, the halo fill and step_enqueue_ghosts
+void step_enqueue_bcs(Handle& h, int cur, cudaEvent_t* phaseEv = nullptr);
+void step_enqueue_ghosts(Handle& h, int cur);
+void launch_calcdt_partial(Handle& h, const StateP& s, cudaStream_t st);
+void launch_dt_finalize(Handle& h, int mode, cudaStream_t st);
 // phases recorded by step_enqueue when phaseEv is given (NPHASE+1 events)
 enum { PH_PREDICT = 0, PH_EFIELD, PH_FLUXES, PH_DELTAS, PH_UPDATE, PH_DT, PH_BCS, NPHASE };
 // Kernels used outside the step

@@ -24,7 +24,8 @@ LIB_PATH = os.path.join(HERE, "libgamgpu.so")
 
 GAM_OK, GAM_ERR_NAN, GAM_ERR_DT_COLLAPSE, GAM_ERR_CUDA, GAM_ERR_TIMEOUT, GAM_ERR_UNSUPPORTED, GAM_ERR_ARG = range(7)
 GAM_FP64, GAM_FP32FLUX = 0, 1
-GAM_BC_PERIODIC, GAM_BC_ZEROGRAD, GAM_BC_LFMPOLE, GAM_BC_LFMBW = 0, 1, 2, 3
+GAM_BC_PERIODIC, GAM_BC_ZEROGRAD, GAM_BC_LFMPOLE, GAM_BC_LFMBW, GAM_BC_HALO = 0, 1, 2, 3, 4
+GAM_HALO_STATE, GAM_HALO_OSTATE, GAM_HALO_BXYZ = 1, 2, 4
 GAM_RING_PLM, GAM_RING_PPM, GAM_RING_PCM = 0, 1, 2
 GAM_RM_8CENT, GAM_RM_7UP = 0, 1
 GAM_SYNC_STATE, GAM_SYNC_OSTATE = 1, 2
@@ -107,6 +108,20 @@ SIGNATURES = {
     "gam_gpu_destroy": (None, [C.c_void_p]),
     "gam_gpu_errstr": (C.c_char_p, [C.c_int]),
     "gam_divb_noalloc": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_void_p]),
+    "gam_tiles_create": (C.c_int, [C.POINTER(C.c_void_p), C.POINTER(C.c_void_p), C.c_int, C.c_int]),
+    "gam_tiles_run_steps": (C.c_int, [C.c_void_p, C.c_int]),
+    "gam_tiles_run_steps_timed": (C.c_int, [C.c_void_p, C.c_int, _DP]),
+    "gam_tiles_destroy": (None, [C.c_void_p]),
+    "gam_gpu_stream": (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p)]),
+    "gam_gpu_step_local": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "gam_gpu_step_bcs": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "gam_gpu_step_ghosts": (C.c_int, [C.c_void_p]),
+    "gam_gpu_calcdt_local": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "gam_gpu_calcdt_finish": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "gam_gpu_halo_bytes": (C.c_int, [C.c_void_p, C.c_int, C.c_uint, C.POINTER(C.c_longlong),
+                                     C.POINTER(C.c_longlong)]),
+    "gam_gpu_halo_pack": (C.c_int, [C.c_void_p, C.c_int, C.c_uint, C.c_void_p]),
+    "gam_gpu_halo_unpack": (C.c_int, [C.c_void_p, C.c_int, C.c_uint, C.c_void_p]),
 }
 
 _lib = None
@@ -539,6 +554,51 @@ class Ensemble:
         if self.e:
             load_library().gam_gpu_ensemble_destroy(self.e)
             self.e = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class TileGroup:
+    """Tiles of one problem split along k, stepped together in this process (gam_tiles_*): the tiles'
+    halos are filled from their neighbours and every tile takes the tiles' minimum dt each step. The
+    tiles stay owned by the caller and are stepped only through the group."""
+
+    def __init__(self, tiles: Sequence[GameraGPU], periodic_k: bool = False):
+        L = load_library()
+        self.tiles = list(tiles)
+        arr = (C.c_void_p * len(self.tiles))(*[t.h.value if hasattr(t.h, "value") else t.h for t in self.tiles])
+        self.g = C.c_void_p()
+        rc = L.gam_tiles_create(C.byref(self.g), arr, len(self.tiles), int(periodic_k))
+        if rc:
+            raise GamError(rc, "gam_tiles_create")
+
+    def run_steps(self, n: int, check: bool = True) -> int:
+        rc = load_library().gam_tiles_run_steps(self.g, n)
+        if rc and check:
+            raise GamError(rc, "gam_tiles_run_steps")
+        return rc
+
+    def run_steps_timed(self, n: int):
+        ms = C.c_double()
+        rc = load_library().gam_tiles_run_steps_timed(self.g, n, C.byref(ms))
+        if rc:
+            raise GamError(rc, "gam_tiles_run_steps_timed")
+        return ms.value
+
+    def close(self):
+        if self.g:
+            load_library().gam_tiles_destroy(self.g)
+            self.g = None
 
     def __enter__(self):
         return self
