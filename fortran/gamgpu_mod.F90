@@ -11,7 +11,9 @@ module gamgpu_mod
     integer(c_int), parameter :: GAM_OK = 0, GAM_ERR_NAN = 1, GAM_ERR_DT_COLLAPSE = 2, GAM_ERR_CUDA = 3, &
                                  GAM_ERR_TIMEOUT = 4, GAM_ERR_UNSUPPORTED = 5, GAM_ERR_ARG = 6
     integer(c_int), parameter :: GAM_FP64 = 0, GAM_FP32FLUX = 1
-    integer(c_int), parameter :: GAM_BC_PERIODIC = 0, GAM_BC_ZEROGRAD = 1
+    integer(c_int), parameter :: GAM_BC_PERIODIC = 0, GAM_BC_ZEROGRAD = 1, GAM_BC_LFMPOLE = 2, GAM_BC_LFMBW = 3, &
+                                 GAM_BC_HALO = 4
+    integer(c_int), parameter :: GAM_HALO_STATE = 1, GAM_HALO_OSTATE = 2, GAM_HALO_BXYZ = 4
     integer(c_int), parameter :: GAM_SYNC_STATE = 1, GAM_SYNC_OSTATE = 2
 
     type, bind(C) :: gam_model_c
@@ -79,6 +81,59 @@ module gamgpu_mod
             import :: c_ptr
             type(c_ptr), value :: h
         end subroutine gam_gpu_destroy
+
+        ! k-decomposed runs, one rank per GPU (stepGamera_mpi, src/gamera/mpi/gamapp_mpi.F90:665-692).
+        ! dtWords and the halo buffers are device addresses.
+        integer(c_int) function gam_gpu_step_local(h, dtWords) bind(C, name="gam_gpu_step_local")
+            import :: c_int, c_ptr
+            type(c_ptr), value :: h, dtWords
+        end function gam_gpu_step_local
+
+        integer(c_int) function gam_gpu_step_bcs(h, dtWords) bind(C, name="gam_gpu_step_bcs")
+            import :: c_int, c_ptr
+            type(c_ptr), value :: h, dtWords
+        end function gam_gpu_step_bcs
+
+        integer(c_int) function gam_gpu_step_ghosts(h) bind(C, name="gam_gpu_step_ghosts")
+            import :: c_int, c_ptr
+            type(c_ptr), value :: h
+        end function gam_gpu_step_ghosts
+
+        integer(c_int) function gam_gpu_calcdt_local(h, dtWords) bind(C, name="gam_gpu_calcdt_local")
+            import :: c_int, c_ptr
+            type(c_ptr), value :: h, dtWords
+        end function gam_gpu_calcdt_local
+
+        integer(c_int) function gam_gpu_calcdt_finish(h, dtWords) bind(C, name="gam_gpu_calcdt_finish")
+            import :: c_int, c_ptr
+            type(c_ptr), value :: h, dtWords
+        end function gam_gpu_calcdt_finish
+
+        integer(c_int) function gam_gpu_halo_bytes(h, side, what, sendBytes, recvBytes) &
+                bind(C, name="gam_gpu_halo_bytes")
+            import :: c_int, c_ptr, c_long_long
+            type(c_ptr), value :: h
+            integer(c_int), value :: side, what
+            integer(c_long_long), intent(out) :: sendBytes, recvBytes
+        end function gam_gpu_halo_bytes
+
+        integer(c_int) function gam_gpu_halo_pack(h, side, what, dst) bind(C, name="gam_gpu_halo_pack")
+            import :: c_int, c_ptr
+            type(c_ptr), value :: h, dst
+            integer(c_int), value :: side, what
+        end function gam_gpu_halo_pack
+
+        integer(c_int) function gam_gpu_halo_unpack(h, side, what, src) bind(C, name="gam_gpu_halo_unpack")
+            import :: c_int, c_ptr
+            type(c_ptr), value :: h, src
+            integer(c_int), value :: side, what
+        end function gam_gpu_halo_unpack
+
+        integer(c_int) function gam_gpu_stream(h, stream) bind(C, name="gam_gpu_stream")
+            import :: c_int, c_ptr
+            type(c_ptr), value :: h
+            type(c_ptr), intent(out) :: stream
+        end function gam_gpu_stream
     end interface
 
 contains
