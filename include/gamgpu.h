@@ -291,6 +291,25 @@ int gam_gpu_halo_bytes(gam_gpu_t* h, int side, unsigned what, long long* sendByt
 int gam_gpu_halo_pack(gam_gpu_t* h, int side, unsigned what, void* dstDev);          /* 16-byte aligned */
 int gam_gpu_halo_unpack(gam_gpu_t* h, int side, unsigned what, const void* srcDev);  /* 16-byte aligned */
 
+/* ---- learned flux closure (no counterpart in the reference; the device analogue of its HackFlux hook,
+ * src/base/types/gamtypes.F90:137-144) ----
+ * A 3D convolution net over a grid's cells: 8 normalised primitives (rho, v, P, B) in, 4 layers of 3x3x3
+ * kernels with 32 channels and GELU, 24 outputs = corrections to the 5 gas fluxes and the 3 magnetic-stress
+ * momentum fluxes through each cell's lower I, J and K face. BF16 weights and activations, FP32
+ * accumulation on the tensor cores (tcgen05); FP32 master weights and Adam moments. Parameters are
+ * W[27][cout][cin] (tap = (di+1) + 3(dj+1) + 9(dk+1)) then b[cout], layer after layer. */
+typedef struct gam_closure gam_closure_t;
+int gam_closure_create(gam_closure_t** c, int Nip, int Njp, int Nkp, unsigned long long seed);
+void gam_closure_destroy(gam_closure_t* c);
+long long gam_closure_num_params(const gam_closure_t* c);
+int gam_closure_set_params(gam_closure_t* c, const float* p, long long n);
+int gam_closure_get_params(gam_closure_t* c, float* p, long long n);
+int gam_closure_get_grads(gam_closure_t* c, float* g, long long n);
+/* the net on host inputs (Ni,Nj,Nk,8), ghosts included, Fortran layout; out: (Nip,Njp,Nkp,24) */
+int gam_closure_forward_host(gam_closure_t* c, const float* in, float* out);
+/* parameter gradients (gam_closure_get_grads) of sum(out * gout) for gout (Nip,Njp,Nkp,24) */
+int gam_closure_backward_host(gam_closure_t* c, const float* in, const float* gout);
+
 const char* gam_gpu_errstr(int code);
 
 #ifdef __cplusplus

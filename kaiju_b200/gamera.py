@@ -74,6 +74,7 @@ class StatusC(C.Structure):
 
 # every entry point declared in include/gamgpu.h with its ctypes signature
 _DP = C.POINTER(C.c_double)
+_FP = C.POINTER(C.c_float)
 SIGNATURES = {
     "gam_gpu_create": (C.c_int, [C.POINTER(C.c_void_p), C.POINTER(ModelC), C.POINTER(GridC), _DP, _DP, _DP, _DP, _DP,
                                  _DP, C.c_double, C.c_double]),
@@ -122,6 +123,14 @@ SIGNATURES = {
                                      C.POINTER(C.c_longlong)]),
     "gam_gpu_halo_pack": (C.c_int, [C.c_void_p, C.c_int, C.c_uint, C.c_void_p]),
     "gam_gpu_halo_unpack": (C.c_int, [C.c_void_p, C.c_int, C.c_uint, C.c_void_p]),
+    "gam_closure_create": (C.c_int, [C.POINTER(C.c_void_p), C.c_int, C.c_int, C.c_int, C.c_ulonglong]),
+    "gam_closure_destroy": (None, [C.c_void_p]),
+    "gam_closure_num_params": (C.c_longlong, [C.c_void_p]),
+    "gam_closure_set_params": (C.c_int, [C.c_void_p, _FP, C.c_longlong]),
+    "gam_closure_get_params": (C.c_int, [C.c_void_p, _FP, C.c_longlong]),
+    "gam_closure_get_grads": (C.c_int, [C.c_void_p, _FP, C.c_longlong]),
+    "gam_closure_forward_host": (C.c_int, [C.c_void_p, _FP, _FP]),
+    "gam_closure_backward_host": (C.c_int, [C.c_void_p, _FP, _FP]),
 }
 
 _lib = None
@@ -605,6 +614,68 @@ class TileGroup:
 
     def __exit__(self, *a):
         self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def _fp(a: np.ndarray):
+    assert a.dtype == np.float32 and (a.flags["F_CONTIGUOUS"] or a.ndim == 1), "float32, Fortran order"
+    return a.ctypes.data_as(_FP)
+
+
+class Closure:
+    """The learned flux closure's network on the current device for grids of Nip x Njp x Nkp active cells
+    (gam_closure_*)."""
+
+    def __init__(self, Nip: int, Njp: int, Nkp: int, seed: int = 0):
+        self.shape = (Nip, Njp, Nkp)
+        self.c = C.c_void_p()
+        rc = load_library().gam_closure_create(C.byref(self.c), Nip, Njp, Nkp, seed)
+        if rc:
+            raise GamError(rc, "gam_closure_create")
+        self.nparams = load_library().gam_closure_num_params(self.c)
+
+    def _call(self, name, *args):
+        rc = getattr(load_library(), name)(self.c, *args)
+        if rc:
+            raise GamError(rc, name)
+
+    def params(self) -> np.ndarray:
+        p = np.zeros(self.nparams, dtype=np.float32)
+        self._call("gam_closure_get_params", _fp(p), self.nparams)
+        return p
+
+    def set_params(self, p: np.ndarray):
+        p = np.ascontiguousarray(p, dtype=np.float32)
+        self._call("gam_closure_set_params", _fp(p), self.nparams)
+
+    def grads(self) -> np.ndarray:
+        g = np.zeros(self.nparams, dtype=np.float32)
+        self._call("gam_closure_get_grads", _fp(g), self.nparams)
+        return g
+
+    def forward_host(self, x: np.ndarray) -> np.ndarray:
+        """x: (Ni, Nj, Nk, 8) float32, ghosts included; returns (Nip, Njp, Nkp, 24)."""
+        Nip, Njp, Nkp = self.shape
+        x = np.asfortranarray(x, dtype=np.float32)
+        out = np.zeros((Nip, Njp, Nkp, 24), dtype=np.float32, order="F")
+        self._call("gam_closure_forward_host", _fp(x), _fp(out))
+        return out
+
+    def backward_host(self, x: np.ndarray, gout: np.ndarray) -> np.ndarray:
+        x = np.asfortranarray(x, dtype=np.float32)
+        gout = np.asfortranarray(gout, dtype=np.float32)
+        self._call("gam_closure_backward_host", _fp(x), _fp(gout))
+        return self.grads()
+
+    def close(self):
+        if self.c:
+            load_library().gam_closure_destroy(self.c)
+            self.c = None
 
     def __del__(self):
         try:
