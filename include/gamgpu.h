@@ -309,6 +309,33 @@ int gam_closure_get_grads(gam_closure_t* c, float* g, long long n);
 int gam_closure_forward_host(gam_closure_t* c, const float* in, float* out);
 /* parameter gradients (gam_closure_get_grads) of sum(out * gout) for gout (Nip,Njp,Nkp,24) */
 int gam_closure_backward_host(gam_closure_t* c, const float* in, const float* gout);
+/* normalisation: net input q = (primitive q - inMean[q]) / inScale[q] for rho, vx, vy, vz, P, Bx, By, Bz;
+ * the face correction of flux v (rho, 3 momenta, energy, 3 magnetic-stress momenta) is the net output times
+ * fluxScale[v] times the face area; the loss divides the residual of each gas variable by resScale[v] */
+int gam_closure_set_norm(gam_closure_t* c, const float* inMean, const float* inScale, const float* fluxScale,
+                         const float* resScale);
+/* training data: n sample slots; a capture stores the net input from the coarse problem's State, takes one
+ * plain coarse step (its dt as set) and stores the residual restrict(fine State) - coarse State of the
+ * 5 gas variables. The fine problem has 2x the cells per direction and sits one coarse step later. */
+int gam_closure_reserve(gam_closure_t* c, int n);
+int gam_closure_capture(gam_closure_t* c, int slot, gam_gpu_t* coarse, gam_gpu_t* fine);
+/* one Adam step per listed slot (forward, loss, backward through the network, Adam) on the loss
+ * mean over active cells of sum_v ((dt/V * div(corrections)_v - residual_v) / resScale_v)^2 */
+int gam_closure_train(gam_closure_t* c, const int* slots, int n, float lr, double* meanLoss);
+int gam_closure_eval(gam_closure_t* c, const int* slots, int n, double* loss, double* lossNone);
+/* rms over the active cells of a sample's residual per gas variable (rms[0..4]) and its dt (rms[5]) */
+int gam_closure_residual_rms(gam_closure_t* c, int slot, double* rms);
+/* attach (c) or detach (NULL) the closure: every step adds its face corrections to the fluxes of State n
+ * before Flux2Deltas; a step whose corrected update would make rho or P non-positive uses the plain
+ * fluxes instead (counted by gam_gpu_closure_rejects). One handle per closure at a time. */
+int gam_gpu_set_closure(gam_gpu_t* h, gam_closure_t* c);
+int gam_gpu_closure_rejects(gam_gpu_t* h, int* n);
+/* restriction of a fine problem's State (2x the cells per direction) into a coarse problem's State
+ * (GAM_SYNC_STATE) or oState (GAM_SYNC_OSTATE): gas volume-weighted, magnetic fluxes summed per face
+ * (divergence-free), then the coarse BCs and Bxyz */
+int gam_gpu_restrict(gam_gpu_t* fine, gam_gpu_t* coarse, unsigned what);
+/* Hatch's initial dt for a state placed with gam_gpu_sync_to_device: CalcDT, oState%time = time - dt */
+int gam_gpu_init_dt(gam_gpu_t* h);
 
 const char* gam_gpu_errstr(int code);
 

@@ -573,6 +573,18 @@ int gam_gpu_profile_phases(gam_gpu_t* G, int nsteps, double* ms, int nphase) {
     return status_code(G->h.hScal->sticky);
 }
 
+int gam_gpu_set_closure(gam_gpu_t* G, gam_closure_t* c) {
+    if (!G) return GAM_ERR_ARG;
+    Handle& h = G->h;
+    if (c) {
+        int rc = closure_attach(h, c);
+        if (rc) return rc;
+    }
+    destroy_graphs(h);   // the step graphs are captured with or without the closure's kernels
+    h.closure = c;
+    return GAM_OK;
+}
+
 int gam_gpu_divb(gam_gpu_t* G, double* tot) {
     if (!G || !tot) return GAM_ERR_ARG;
     *tot = launch_divb(G->h, G->scratch, G->h.stream);

@@ -7,6 +7,7 @@
 #include <random>
 #include <vector>
 
+#include "gam_kern.cuh"
 #include "gam_net.cuh"
 #include "gam_step.cuh"
 #include "gamgpu.h"
@@ -31,6 +32,22 @@ struct gam_closure {
     float* stage = nullptr;      // host-layout staging (largest: NET_OUT or NET_IN planes of the box)
     int* err = nullptr;
     bool packed = false;
+    // normalisation: net input (rho, vx, vy, vz, P, Bx, By, Bz) = (prim - inMean) / inScale; face
+    // correction of variable v = net output * fluxScale[v] * face area; loss terms / resScale[v]
+    float inMean[8] = {0, 0, 0, 0, 0, 0, 0, 0}, inScale[8] = {1, 1, 1, 1, 1, 1, 1, 1};
+    float fluxScale[8] = {1, 1, 1, 1, 1, 1, 1, 1}, resScale[5] = {1, 1, 1, 1, 1};
+    int periodic[3] = {0, 0, 0};
+    float* corr = nullptr;       // 24 face-correction planes
+    float* geom = nullptr;       // volume, face I, J, K (float planes, copied from a solver handle)
+    bool haveGeom = false;
+    float* wts = nullptr;        // loss weights w_v = dL/d(dU_v) * dt / V, 5 planes
+    double* lossAcc = nullptr;   // device loss accumulators [2]
+    float* lossPart = nullptr;   // per-block loss partials
+    // training samples: net input (8 bf16 planes) and residual (5 float planes) per slot, and its dt
+    std::vector<__nv_bfloat16*> sIn;
+    std::vector<float*> sRes;
+    std::vector<double> sDt;
+    __nv_bfloat16* act0 = nullptr;   // the net's own input planes (act[0] is pointed at a sample in training)
 };
 
 namespace {
@@ -82,6 +99,251 @@ __global__ void k_gout_from_fortran(Lay L, const float* src, int nc, __nv_bfloat
     for (int q = 0; q < nc; ++q) dst[(long long)q * L.E + c] = __float2bfloat16_rn(src[t + q * n]);
 }
 
+
+struct NormP {
+    float inMean[8], inScale[8], fluxScale[8], resScale[5];
+    int per[3];
+};
+NormP norm_of(const gam_closure* C) {
+    NormP n;
+    for (int q = 0; q < 8; ++q) { n.inMean[q] = C->inMean[q]; n.inScale[q] = C->inScale[q]; n.fluxScale[q] = C->fluxScale[q]; }
+    for (int q = 0; q < 5; ++q) n.resScale[q] = C->resScale[q];
+    for (int d = 0; d < 3; ++d) n.per[d] = C->periodic[d];
+    return n;
+}
+
+// the net's input planes from a state: normalised rho, v, P, B of every cell (ghosts included)
+__global__ void k_closure_input(Lay L, double gamma, StateP s, NormP n, __nv_bfloat16* in) {
+    const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (t >= (long long)L.Ni * L.Nj * L.Nk) return;
+    const int i = (int)(t % L.Ni), j = (int)((t / L.Ni) % L.Nj), k = (int)(t / ((long long)L.Ni * L.Nj));
+    const long long c = L.at(i, j, k);
+    const double rho = s.gas[0][c];
+    const double vx = s.gas[1][c] / rho, vy = s.gas[2][c] / rho, vz = s.gas[3][c] / rho;
+    const double P = (gamma - 1.0) * (s.gas[4][c] - 0.5 * rho * (vx * vx + vy * vy + vz * vz));
+    const double w[8] = {rho, vx, vy, vz, P, s.b[0][c], s.b[1][c], s.b[2][c]};
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+        float f = (float)((w[q] - n.inMean[q]) / n.inScale[q]);
+        if (!(f == f) || fabsf(f) > 1e4f) f = 0.f;   // keep the net's input finite
+        in[(long long)q * L.E + c] = __float2bfloat16_rn(f);
+    }
+}
+
+// face corrections (area-scaled): plane d*8+v at the index of the lower d-face of the owner cell, for the
+// faces of the active cells and the upper boundary faces. A boundary face of a non-periodic direction gets
+// none; across a periodic one the upper boundary face repeats the lower boundary face.
+__global__ void k_closure_corr(Lay L, const float* out, NormP n, const float* geom, float* corr) {
+    const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    const int ni = L.Nip + 1, nj = L.Njp + 1, nk = L.Nkp + 1;
+    if (t >= (long long)ni * nj * nk) return;
+    const int i = L.is() + (int)(t % ni), j = L.js() + (int)((t / ni) % nj), k = L.ks() + (int)(t / ((long long)ni * nj));
+    const long long c = L.at(i, j, k);
+    const int idx[3] = {i, j, k};
+    const int lo[3] = {L.is(), L.js(), L.ks()}, hi[3] = {L.ie(), L.je(), L.ke()};
+    for (int d = 0; d < 3; ++d) {
+        // the other two indices must be active for a d-face of an active cell
+        bool ok = true;
+        for (int e = 0; e < 3; ++e)
+            if (e != d && idx[e] > hi[e]) ok = false;
+        if (!ok) continue;
+        long long own = c;
+        bool zero = false;
+        if (idx[d] == hi[d] + 1) {
+            if (n.per[d]) own = c - (long long)(hi[d] - lo[d] + 1) * (d == 0 ? 1 : d == 1 ? L.P : (long long)L.P * L.Q);
+            else zero = true;
+        } else if (idx[d] == lo[d] && !n.per[d]) {
+            zero = true;
+        }
+        const float A = geom[(long long)(1 + d) * L.E + c];
+        for (int v = 0; v < 8; ++v) {
+            const long long o = (long long)(d * 8 + v) * L.E;
+            corr[o + c] = zero ? 0.f : out[o + own] * n.fluxScale[v] * A;
+        }
+    }
+}
+
+// closure positivity: the Reynolds stage of the corrected update must keep rho > 0 and P > 0 (before floors)
+__global__ void k_closure_check(Lay L, double gamma, StateP nS, PrimP dGH, const Scal* scIn, Scal* sc) {
+    const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (t >= (long long)L.Nip * L.Njp * L.Nkp) return;
+    const int i = L.is() + (int)(t % L.Nip), j = L.js() + (int)((t / L.Nip) % L.Njp),
+              k = L.ks() + (int)(t / ((long long)L.Nip * L.Njp));
+    const long long c = L.at(i, j, k);
+    const double dt = scIn->dt;
+    double U[5];
+    for (int v = 0; v < 5; ++v) U[v] = nS.gas[v][c] + dt * dGH.w[v][c];
+    bool bad = !(U[0] > 0.0);
+    if (!bad) {
+        const double P = (gamma - 1.0) * (U[4] - 0.5 * (U[1] * U[1] + U[2] * U[2] + U[3] * U[3]) / U[0]);
+        bad = !(P > 0.0);
+    }
+    if (bad) atomicExch(&sc->closureReject, 1);
+}
+__global__ void k_closure_count(Scal* sc) {
+    if (sc->closureReject) sc->closureRejects++;
+}
+
+// the residual of one coarse step: the volume-weighted restriction of the fine state minus the coarse
+// state, gas variables, active coarse cells (fine cells 2x2x2 per coarse cell)
+__global__ void k_closure_residual(Lay Lc, Lay Lf, StateP fine, const double* fineVol, StateP coarse, float* res) {
+    const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (t >= (long long)Lc.Nip * Lc.Njp * Lc.Nkp) return;
+    const int I = (int)(t % Lc.Nip), J = (int)((t / Lc.Nip) % Lc.Njp), K = (int)(t / ((long long)Lc.Nip * Lc.Njp));
+    const long long cc = Lc.at(Lc.is() + I, Lc.js() + J, Lc.ks() + K);
+    double sum[5] = {0, 0, 0, 0, 0}, vol = 0.0;
+    for (int dk = 0; dk < 2; ++dk)
+        for (int dj = 0; dj < 2; ++dj)
+            for (int di = 0; di < 2; ++di) {
+                const long long cf = Lf.at(Lf.is() + 2 * I + di, Lf.js() + 2 * J + dj, Lf.ks() + 2 * K + dk);
+                const double V = fineVol[cf];
+                vol += V;
+                for (int v = 0; v < 5; ++v) sum[v] += fine.gas[v][cf] * V;
+            }
+    for (int v = 0; v < 5; ++v) res[(long long)v * Lc.E + cc] = (float)(sum[v] / vol - coarse.gas[v][cc]);
+}
+
+// restriction into a coarse state: gas volume-weighted, magnetic fluxes summed over the 4 fine faces of
+// each coarse face (so the coarse field stays divergence-free)
+__global__ void k_restrict_gas(Lay Lc, Lay Lf, StateP fine, const double* fineVol, StateP coarse) {
+    const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (t >= (long long)Lc.Nip * Lc.Njp * Lc.Nkp) return;
+    const int I = (int)(t % Lc.Nip), J = (int)((t / Lc.Nip) % Lc.Njp), K = (int)(t / ((long long)Lc.Nip * Lc.Njp));
+    const long long cc = Lc.at(Lc.is() + I, Lc.js() + J, Lc.ks() + K);
+    double sum[5] = {0, 0, 0, 0, 0}, vol = 0.0;
+    for (int dk = 0; dk < 2; ++dk)
+        for (int dj = 0; dj < 2; ++dj)
+            for (int di = 0; di < 2; ++di) {
+                const long long cf = Lf.at(Lf.is() + 2 * I + di, Lf.js() + 2 * J + dj, Lf.ks() + 2 * K + dk);
+                const double V = fineVol[cf];
+                vol += V;
+                for (int v = 0; v < 5; ++v) sum[v] += fine.gas[v][cf] * V;
+            }
+    for (int v = 0; v < 5; ++v) coarse.gas[v][cc] = sum[v] / vol;
+}
+__global__ void k_restrict_flux(Lay Lc, Lay Lf, StateP fine, StateP coarse) {
+    const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    const int ni = Lc.Nip + 1, nj = Lc.Njp + 1, nk = Lc.Nkp + 1;
+    if (t >= (long long)ni * nj * nk) return;
+    const int I = (int)(t % ni), J = (int)((t / ni) % nj), K = (int)(t / ((long long)ni * nj));
+    const long long cc = Lc.at(Lc.is() + I, Lc.js() + J, Lc.ks() + K);
+    const int fi = Lf.is() + 2 * I, fj = Lf.js() + 2 * J, fk = Lf.ks() + 2 * K;
+    if (J < Lc.Njp && K < Lc.Nkp)
+        coarse.mf[0][cc] = fine.mf[0][Lf.at(fi, fj, fk)] + fine.mf[0][Lf.at(fi, fj + 1, fk)] +
+                           fine.mf[0][Lf.at(fi, fj, fk + 1)] + fine.mf[0][Lf.at(fi, fj + 1, fk + 1)];
+    if (I < Lc.Nip && K < Lc.Nkp)
+        coarse.mf[1][cc] = fine.mf[1][Lf.at(fi, fj, fk)] + fine.mf[1][Lf.at(fi + 1, fj, fk)] +
+                           fine.mf[1][Lf.at(fi, fj, fk + 1)] + fine.mf[1][Lf.at(fi + 1, fj, fk + 1)];
+    if (I < Lc.Nip && J < Lc.Njp)
+        coarse.mf[2][cc] = fine.mf[2][Lf.at(fi, fj, fk)] + fine.mf[2][Lf.at(fi + 1, fj, fk)] +
+                           fine.mf[2][Lf.at(fi, fj + 1, fk)] + fine.mf[2][Lf.at(fi + 1, fj + 1, fk)];
+}
+
+__global__ void k_to_float(const double* src, float* dst, long long n) {
+    const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (t < n) dst[t] = (float)src[t];
+}
+
+// loss of one sample: dU = dt / V * (sum of corrections in - out) (momentum also from the magnetic-stress
+// corrections), L = mean over active cells of sum_v ((dU_v - r_v) / resScale_v)^2; stores
+// w_v = dL/d(dU_v) * dt / V for the gradient and per-block partial sums of L
+__global__ void k_loss_w(Lay L, const float* corr, const float* res, const float* geom, NormP n, double dt,
+                         float* w, float* part) {
+    __shared__ float red[256];
+    const long long nact = (long long)L.Nip * L.Njp * L.Nkp;
+    float acc = 0.f;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < nact; t += (long long)gridDim.x * blockDim.x) {
+        const int i = L.is() + (int)(t % L.Nip), j = L.js() + (int)((t / L.Nip) % L.Njp),
+                  k = L.ks() + (int)(t / ((long long)L.Nip * L.Njp));
+        const long long c = L.at(i, j, k);
+        const long long nb[3] = {c + 1, c + L.P, c + (long long)L.P * L.Q};
+        const float f = (float)dt / geom[c];
+        float dU[5];
+        for (int v = 0; v < 5; ++v) {
+            float s = 0.f;
+            for (int d = 0; d < 3; ++d) {
+                const float* q = corr + (long long)(d * 8 + v) * L.E;
+                s += q[c] - q[nb[d]];
+            }
+            dU[v] = s;
+        }
+        for (int x = 0; x < 3; ++x)
+            for (int d = 0; d < 3; ++d) {
+                const float* q = corr + (long long)(d * 8 + 5 + x) * L.E;
+                dU[1 + x] += q[c] - q[nb[d]];
+            }
+        for (int v = 0; v < 5; ++v) {
+            const float e = (f * dU[v] - res[(long long)v * L.E + c]) / n.resScale[v];
+            acc += e * e;
+            w[(long long)v * L.E + c] = 2.f * e / n.resScale[v] / (float)nact * f;
+        }
+    }
+    red[threadIdx.x] = acc / (float)nact;
+    __syncthreads();
+    for (int s2 = blockDim.x / 2; s2 > 0; s2 >>= 1) {
+        if (threadIdx.x < s2) red[threadIdx.x] += red[threadIdx.x + s2];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) part[blockIdx.x] = red[0];
+}
+__global__ void k_loss_sum(const float* part, int nblk, double* acc) {
+    if (threadIdx.x != 0) return;
+    double s = 0.0;
+    for (int b = 0; b < nblk; ++b) s += part[b];
+    acc[0] += s;
+}
+
+// output gradient: dL/dy for the lower d-face of each active cell = fluxScale * A * (w(cell) - w(cell below)),
+// the cell below wrapping across a periodic boundary; a non-periodic boundary face has no correction
+__global__ void k_loss_grad(Lay L, const float* w, const float* geom, NormP n, __nv_bfloat16* gout) {
+    const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (t >= (long long)L.Nip * L.Njp * L.Nkp) return;
+    const int i = L.is() + (int)(t % L.Nip), j = L.js() + (int)((t / L.Nip) % L.Njp),
+              k = L.ks() + (int)(t / ((long long)L.Nip * L.Njp));
+    const long long c = L.at(i, j, k);
+    const int idx[3] = {i, j, k};
+    const int lo[3] = {L.is(), L.js(), L.ks()}, cnt[3] = {L.Nip, L.Njp, L.Nkp};
+    const long long st[3] = {1, L.P, (long long)L.P * L.Q};
+    for (int d = 0; d < 3; ++d) {
+        bool zero = false;
+        long long below = c - st[d];
+        if (idx[d] == lo[d]) {
+            if (n.per[d]) below = c + (long long)(cnt[d] - 1) * st[d];
+            else zero = true;
+        }
+        const float A = geom[(long long)(1 + d) * L.E + c];
+        for (int v = 0; v < 8; ++v) {
+            const int u = v < 5 ? v : v - 4;   // the magnetic-stress corrections act on the momentum
+            const float g = zero ? 0.f
+                                 : n.fluxScale[v] * A * (w[(long long)u * L.E + c] - w[(long long)u * L.E + below]);
+            gout[(long long)(d * 8 + v) * L.E + c] = __float2bfloat16_rn(g);
+        }
+    }
+}
+
+inline unsigned nblk256(long long n) { return (unsigned)((n + 255) / 256); }
+
+// sums of the residual squares per gas variable over the active cells (statistics for the normalisation)
+__global__ void k_res_sq(Lay L, const float* res, double* acc) {
+    __shared__ double red[5][256];
+    double s[5] = {0, 0, 0, 0, 0};
+    const long long nact = (long long)L.Nip * L.Njp * L.Nkp;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < nact; t += (long long)gridDim.x * blockDim.x) {
+        const long long c = L.at(L.is() + (int)(t % L.Nip), L.js() + (int)((t / L.Nip) % L.Njp),
+                                 L.ks() + (int)(t / ((long long)L.Nip * L.Njp)));
+        for (int v = 0; v < 5; ++v) { const double r = res[(long long)v * L.E + c]; s[v] += r * r; }
+    }
+    for (int v = 0; v < 5; ++v) red[v][threadIdx.x] = s[v];
+    __syncthreads();
+    for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+        if (threadIdx.x < w)
+            for (int v = 0; v < 5; ++v) red[v][threadIdx.x] += red[v][threadIdx.x + w];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0)
+        for (int v = 0; v < 5; ++v) atomicAdd(&acc[v], red[v][0]);
+}
+
 int closure_pack(gam_closure* C) {
     if (net_pack_weights(C->params, C->wfwd, C->wbwd, C->stream) != 0) return GAM_ERR_CUDA;
     C->packed = true;
@@ -111,6 +373,7 @@ int gam_closure_create(gam_closure_t** out, int Nip, int Njp, int Nkp, unsigned 
     C->box.c0 = margin;
     C->box.c1 = L.E - margin;
     cudaGetDevice(&C->device);
+    if (net_init() != 0) { delete C; return GAM_ERR_CUDA; }
     C->np = net_num_params();
     int rc = GAM_OK;
     auto fail = [&](int r) { gam_closure_destroy(C); return r; };
@@ -142,6 +405,14 @@ int gam_closure_create(gam_closure_t** out, int Nip, int Njp, int Nkp, unsigned 
     C->nb.out = reinterpret_cast<float*>(q);
     C->nb.partialFloats = net_partial_floats(net_dw_blocks());
     if (cudaMalloc(&C->nb.partial, sizeof(float) * C->nb.partialFloats) != cudaSuccess) return fail(GAM_ERR_CUDA);
+    C->act0 = C->nb.act[0];
+    if (cudaMalloc(&C->corr, sizeof(float) * E * NET_OUT) || cudaMalloc(&C->geom, sizeof(float) * E * 4) ||
+        cudaMalloc(&C->wts, sizeof(float) * E * 5) || cudaMalloc(&C->lossAcc, sizeof(double) * 2) ||
+        cudaMalloc(&C->lossPart, sizeof(float) * 2 * 4096))
+        return fail(GAM_ERR_CUDA);
+    cudaMemsetAsync(C->corr, 0, sizeof(float) * E * NET_OUT, C->stream);
+    cudaMemsetAsync(C->wts, 0, sizeof(float) * E * 5, C->stream);
+    cudaMemsetAsync(C->geom, 0, sizeof(float) * E * 4, C->stream);
     const long long stageFloats = (long long)L.Ni * L.Nj * L.Nk * NET_OUT;
     if (cudaMalloc(&C->stage, sizeof(float) * stageFloats) != cudaSuccess) return fail(GAM_ERR_CUDA);
     cudaMemsetAsync(C->err, 0, sizeof(int), C->stream);
@@ -172,6 +443,9 @@ void gam_closure_destroy(gam_closure_t* C) {
     cudaFree(C->params); cudaFree(C->grads); cudaFree(C->m); cudaFree(C->v); cudaFree(C->err);
     for (int l = 0; l < NET_LAYERS; ++l) { cudaFree(C->wfwd[l]); cudaFree(C->wbwd[l]); }
     cudaFree(C->pool); cudaFree(C->nb.partial); cudaFree(C->stage);
+    cudaFree(C->corr); cudaFree(C->geom); cudaFree(C->wts); cudaFree(C->lossAcc); cudaFree(C->lossPart);
+    for (auto* q : C->sIn) cudaFree(q);
+    for (auto* q : C->sRes) cudaFree(q);
     if (C->stream) cudaStreamDestroy(C->stream);
     delete C;
 }
@@ -225,6 +499,234 @@ int gam_closure_backward_host(gam_closure_t* C, const float* in, const float* go
     k_gout_from_fortran<<<(unsigned)((nAct + 255) / 256), 256, 0, C->stream>>>(L, C->stage, NET_OUT, C->nb.gact[0]);
     if (net_backward(C->box, C->wbwd, C->nb, C->grads, C->err, C->stream) != 0) return GAM_ERR_CUDA;
     return check_err(C);
+}
+
+}  // extern "C"
+
+// ================================================================================ the closure in the step
+namespace gam {
+
+const float* closure_enqueue_corr(Handle& h, const StateP& nS, cudaStream_t st) {
+    gam_closure* C = h.closure;
+    const Lay& L = h.L;
+    NormP n = norm_of(C);
+    C->nb.act[0] = C->act0;
+    k_closure_input<<<nblk256((long long)L.Ni * L.Nj * L.Nk), 256, 0, st>>>(L, h.p.gamma, nS, n, C->act0);
+    net_forward(C->box, C->wfwd, C->params, C->nb, false, C->err, st);
+    const long long nf = (long long)(L.Nip + 1) * (L.Njp + 1) * (L.Nkp + 1);
+    k_closure_corr<<<nblk256(nf), 256, 0, st>>>(L, C->nb.out, n, C->geom, C->corr);
+    h.launches += 2 + NET_LAYERS;
+    return C->corr;
+}
+
+void closure_enqueue_check(Handle& h, const StateP& nS, cudaStream_t st) {
+    const Lay& L = h.L;
+    PrimP dGH;
+    for (int v = 0; v < 5; ++v) dGH.w[v] = h.dGasH[v];
+    k_closure_check<<<nblk256((long long)L.Nip * L.Njp * L.Nkp), 256, 0, st>>>(L, h.p.gamma, nS, dGH, h.dScal, h.dScal);
+    k_closure_count<<<1, 1, 0, st>>>(h.dScal);
+    h.launches += 2;
+}
+
+int closure_kernels_per_step(const Handle& h) { return h.closure ? 2 + NET_LAYERS + 2 : 0; }
+
+// shape check and geometry for a handle the closure is attached to
+int closure_attach(Handle& h, gam_closure* C) {
+    const Lay& L = h.L;
+    if (C->L.Nip != L.Nip || C->L.Njp != L.Njp || C->L.Nkp != L.Nkp || C->device != h.device) return GAM_ERR_ARG;
+    if (h.p.doRing) return GAM_ERR_UNSUPPORTED;
+    for (int d = 0; d < 3; ++d) C->periodic[d] = h.p.bc[2 * d] == BC_PERIODIC && h.p.bc[2 * d + 1] == BC_PERIODIC;
+    k_to_float<<<nblk256(L.E), 256, 0, h.stream>>>(h.volume, C->geom, L.E);
+    for (int d = 0; d < 3; ++d) k_to_float<<<nblk256(L.E), 256, 0, h.stream>>>(h.face[d], C->geom + (1 + d) * L.E, L.E);
+    C->haveGeom = true;
+    return cudaStreamSynchronize(h.stream) == cudaSuccess ? GAM_OK : GAM_ERR_CUDA;
+}
+
+}  // namespace gam
+
+namespace gam {
+Handle& capi_handle(gam_gpu* G);
+int capi_download_scalars(gam_gpu* G);
+}  // namespace gam
+
+extern "C" {
+
+int gam_closure_set_norm(gam_closure_t* C, const float* inMean, const float* inScale, const float* fluxScale,
+                         const float* resScale) {
+    if (!C || !inMean || !inScale || !fluxScale || !resScale) return GAM_ERR_ARG;
+    for (int q = 0; q < 8; ++q) {
+        if (!(inScale[q] > 0.f) || !(fluxScale[q] > 0.f)) return GAM_ERR_ARG;
+        C->inMean[q] = inMean[q]; C->inScale[q] = inScale[q]; C->fluxScale[q] = fluxScale[q];
+    }
+    for (int q = 0; q < 5; ++q) {
+        if (!(resScale[q] > 0.f)) return GAM_ERR_ARG;
+        C->resScale[q] = resScale[q];
+    }
+    return GAM_OK;
+}
+
+int gam_closure_reserve(gam_closure_t* C, int n) {
+    if (!C || n < 0) return GAM_ERR_ARG;
+    const long long E = C->L.E;
+    while ((int)C->sIn.size() < n) {
+        __nv_bfloat16* in = nullptr;
+        float* res = nullptr;
+        if (cudaMalloc(&in, sizeof(__nv_bfloat16) * E * NET_IN) != cudaSuccess) return GAM_ERR_CUDA;
+        if (cudaMalloc(&res, sizeof(float) * E * 5) != cudaSuccess) { cudaFree(in); return GAM_ERR_CUDA; }
+        cudaMemsetAsync(in, 0, sizeof(__nv_bfloat16) * E * NET_IN, C->stream);
+        cudaMemsetAsync(res, 0, sizeof(float) * E * 5, C->stream);
+        C->sIn.push_back(in);
+        C->sRes.push_back(res);
+        C->sDt.push_back(0.0);
+    }
+    CKC(cudaStreamSynchronize(C->stream));
+    return GAM_OK;
+}
+
+int gam_closure_capture(gam_closure_t* C, int slot, gam_gpu_t* coarse, gam_gpu_t* fine) {
+    if (!C || !coarse || !fine || slot < 0 || slot >= (int)C->sIn.size()) return GAM_ERR_ARG;
+    Handle& hc = capi_handle(coarse);
+    Handle& hf = capi_handle(fine);
+    if (hc.closure || hf.L.Nip != 2 * hc.L.Nip || hf.L.Njp != 2 * hc.L.Njp || hf.L.Nkp != 2 * hc.L.Nkp ||
+        hc.device != hf.device)
+        return GAM_ERR_ARG;
+    int rc = closure_attach(hc, C);
+    if (rc) return rc;
+    const Lay& L = hc.L;
+    NormP n = norm_of(C);
+    k_closure_input<<<nblk256((long long)L.Ni * L.Nj * L.Nk), 256, 0, hc.stream>>>(L, hc.p.gamma, hc.S[hc.cur], n,
+                                                                                  C->sIn[slot]);
+    rc = capi_download_scalars(coarse);
+    if (rc) return rc;
+    C->sDt[slot] = hc.hScal->dt;
+    double dt = 0.0, t = 0.0;
+    int ts = 0;
+    rc = gam_gpu_step(coarse, &dt, &ts, &t);   // the plain coarse step
+    if (rc) return rc;
+    CKC(cudaStreamSynchronize(hf.stream));
+    k_closure_residual<<<nblk256((long long)L.Nip * L.Njp * L.Nkp), 256, 0, hc.stream>>>(
+        L, hf.L, hf.S[hf.cur], hf.volume, hc.S[hc.cur], C->sRes[slot]);
+    CKC(cudaStreamSynchronize(hc.stream));
+    return GAM_OK;
+}
+
+// forward, loss and (train) gradient + Adam for one sample, on the closure's stream
+static int closure_sample_pass(gam_closure* C, int slot, bool train, float lr) {
+    const Lay& L = C->L;
+    NormP n = norm_of(C);
+    C->nb.act[0] = C->sIn[slot];
+    if (net_forward(C->box, C->wfwd, C->params, C->nb, train, C->err, C->stream) != 0) return GAM_ERR_CUDA;
+    const long long nf = (long long)(L.Nip + 1) * (L.Njp + 1) * (L.Nkp + 1);
+    k_closure_corr<<<nblk256(nf), 256, 0, C->stream>>>(L, C->nb.out, n, C->geom, C->corr);
+    const int nb = 1024;
+    k_loss_w<<<nb, 256, 0, C->stream>>>(L, C->corr, C->sRes[slot], C->geom, n, C->sDt[slot], C->wts, C->lossPart);
+    k_loss_sum<<<1, 32, 0, C->stream>>>(C->lossPart, nb, C->lossAcc);
+    if (train) {
+        k_loss_grad<<<nblk256((long long)L.Nip * L.Njp * L.Nkp), 256, 0, C->stream>>>(L, C->wts, C->geom, n,
+                                                                                       C->nb.gact[0]);
+        if (net_backward(C->box, C->wbwd, C->nb, C->grads, C->err, C->stream) != 0) return GAM_ERR_CUDA;
+        C->adamStep++;
+        if (net_adam(C->params, C->grads, C->m, C->v, C->np, lr, 0.9f, 0.999f, 1e-8f, C->adamStep, C->stream) != 0)
+            return GAM_ERR_CUDA;
+        if (closure_pack(C)) return GAM_ERR_CUDA;
+    }
+    C->nb.act[0] = C->act0;
+    return GAM_OK;
+}
+
+// one Adam step per listed sample, in order; meanLoss = the mean of their losses before each step
+int gam_closure_train(gam_closure_t* C, const int* slots, int n, float lr, double* meanLoss) {
+    if (!C || !slots || n < 1 || !(lr > 0.f) || !C->haveGeom) return GAM_ERR_ARG;
+    for (int q = 0; q < n; ++q)
+        if (slots[q] < 0 || slots[q] >= (int)C->sIn.size()) return GAM_ERR_ARG;
+    CKC(cudaMemsetAsync(C->lossAcc, 0, sizeof(double) * 2, C->stream));
+    for (int q = 0; q < n; ++q) {
+        int rc = closure_sample_pass(C, slots[q], true, lr);
+        if (rc) return rc;
+    }
+    double acc[2];
+    CKC(cudaMemcpyAsync(acc, C->lossAcc, sizeof(acc), cudaMemcpyDeviceToHost, C->stream));
+    int rc = check_err(C);
+    if (rc) return rc;
+    if (meanLoss) *meanLoss = acc[0] / n;
+    return GAM_OK;
+}
+
+// mean loss over the listed samples with the net (loss) and without any correction (lossNone)
+int gam_closure_eval(gam_closure_t* C, const int* slots, int n, double* loss, double* lossNone) {
+    if (!C || !slots || n < 1 || !C->haveGeom) return GAM_ERR_ARG;
+    for (int q = 0; q < n; ++q)
+        if (slots[q] < 0 || slots[q] >= (int)C->sIn.size()) return GAM_ERR_ARG;
+    const Lay& L = C->L;
+    NormP nrm = norm_of(C);
+    double acc[2] = {0, 0};
+    for (int pass = 0; pass < 2; ++pass) {
+        CKC(cudaMemsetAsync(C->lossAcc, 0, sizeof(double) * 2, C->stream));
+        for (int q = 0; q < n; ++q) {
+            if (pass == 0) {
+                int rc = closure_sample_pass(C, slots[q], false, 0.f);
+                if (rc) return rc;
+            } else {   // no correction: the residual alone
+                CKC(cudaMemsetAsync(C->corr, 0, sizeof(float) * L.E * NET_OUT, C->stream));
+                k_loss_w<<<1024, 256, 0, C->stream>>>(L, C->corr, C->sRes[slots[q]], C->geom, nrm, C->sDt[slots[q]],
+                                                       C->wts, C->lossPart);
+                k_loss_sum<<<1, 32, 0, C->stream>>>(C->lossPart, 1024, C->lossAcc);
+            }
+        }
+        double a[2];
+        CKC(cudaMemcpyAsync(a, C->lossAcc, sizeof(a), cudaMemcpyDeviceToHost, C->stream));
+        CKC(cudaStreamSynchronize(C->stream));
+        acc[pass] = a[0] / n;
+    }
+    if (loss) *loss = acc[0];
+    if (lossNone) *lossNone = acc[1];
+    return check_err(C);
+}
+
+// restriction of a fine problem's State into a coarse problem's State (what = GAM_SYNC_STATE) or oState
+// (GAM_SYNC_OSTATE), then the coarse BCs and Bxyz; the fine grid has 2x the coarse cells per direction
+int gam_gpu_restrict(gam_gpu_t* fine, gam_gpu_t* coarse, unsigned what) {
+    if (!fine || !coarse || (what != GAM_SYNC_STATE && what != GAM_SYNC_OSTATE)) return GAM_ERR_ARG;
+    Handle& hf = capi_handle(fine);
+    Handle& hc = capi_handle(coarse);
+    if (hf.L.Nip != 2 * hc.L.Nip || hf.L.Njp != 2 * hc.L.Njp || hf.L.Nkp != 2 * hc.L.Nkp || hf.device != hc.device)
+        return GAM_ERR_ARG;
+    CKC(cudaStreamSynchronize(hf.stream));
+    const Lay& L = hc.L;
+    StateP dst = what == GAM_SYNC_STATE ? hc.S[hc.cur] : hc.S[hc.cur ^ 1];
+    k_restrict_gas<<<nblk256((long long)L.Nip * L.Njp * L.Nkp), 256, 0, hc.stream>>>(L, hf.L, hf.S[hf.cur], hf.volume, dst);
+    k_restrict_flux<<<nblk256((long long)(L.Nip + 1) * (L.Njp + 1) * (L.Nkp + 1)), 256, 0, hc.stream>>>(L, hf.L,
+                                                                                                        hf.S[hf.cur], dst);
+    launch_bcs(hc, dst, hc.stream);
+    launch_bflux2fld(hc, dst, hc.stream);
+    hc.launches += 2;
+    CKC(cudaStreamSynchronize(hc.stream));
+    return GAM_OK;
+}
+
+int gam_closure_residual_rms(gam_closure_t* C, int slot, double* rms) {
+    if (!C || !rms || slot < 0 || slot >= (int)C->sIn.size()) return GAM_ERR_ARG;
+    double* acc = nullptr;
+    CKC(cudaMalloc(&acc, sizeof(double) * 5));
+    cudaMemsetAsync(acc, 0, sizeof(double) * 5, C->stream);
+    k_res_sq<<<256, 256, 0, C->stream>>>(C->L, C->sRes[slot], acc);
+    double h[5];
+    cudaMemcpyAsync(h, acc, sizeof(h), cudaMemcpyDeviceToHost, C->stream);
+    cudaError_t e = cudaStreamSynchronize(C->stream);
+    cudaFree(acc);
+    if (e != cudaSuccess) return GAM_ERR_CUDA;
+    const double n = (double)C->L.Nip * C->L.Njp * C->L.Nkp;
+    for (int v = 0; v < 5; ++v) rms[v] = std::sqrt(h[v] / n);
+    rms[5] = C->sDt[slot];
+    return GAM_OK;
+}
+
+int gam_gpu_closure_rejects(gam_gpu_t* G, int* n) {
+    if (!G || !n) return GAM_ERR_ARG;
+    int rc = capi_download_scalars(G);
+    if (rc) return rc;
+    *n = capi_handle(G).hScal->closureRejects;
+    return GAM_OK;
 }
 
 }  // extern "C"

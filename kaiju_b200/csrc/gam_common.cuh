@@ -67,6 +67,9 @@ struct Scal {
     // tiled runs: {dtMinBits, ~nanCount} of this tile, reduced with MIN across the tiles (so the second
     // word carries the largest NaN count) before the dt is finalized
     unsigned long long red[2];
+    // learned closure: 1 when this step's corrected update failed positivity and the plain fluxes were used
+    int closureReject;
+    int closureRejects;               // steps that fell back, since the handle was created
 };
 
 // Device field bundle. Planes are contiguous arrays of Lay::E doubles.

@@ -406,8 +406,6 @@ int sm_count() {
 template <int CINP, int COUTP, int MODE>
 void launch_conv(const ConvArgs& a, cudaStream_t st) {
     using S = ConvSmem<CINP, COUTP>;
-    static bool init = false;
-    if (!init) { set_smem(k_conv<CINP, COUTP, MODE>, S::BYTES); init = true; }
     long long ntiles = (a.c1 - a.c0 + 127) / 128;
     long long grid = sm_count() * 3;
     if (grid > ntiles) grid = ntiles;
@@ -416,6 +414,18 @@ void launch_conv(const ConvArgs& a, cudaStream_t st) {
 }
 
 }  // namespace
+
+// shared-memory limits of every kernel instance (set once, outside any stream capture)
+int net_init() {
+    set_smem(k_conv<16, 32, MODE_HIDDEN>, ConvSmem<16, 32>::BYTES);
+    set_smem(k_conv<32, 32, MODE_HIDDEN>, ConvSmem<32, 32>::BYTES);
+    set_smem(k_conv<32, 32, MODE_OUT>, ConvSmem<32, 32>::BYTES);
+    set_smem(k_conv<32, 32, MODE_BWD>, ConvSmem<32, 32>::BYTES);
+    set_smem(k_conv_dw<16, 32>, DwShape<16, 32>::BYTES);
+    set_smem(k_conv_dw<32, 32>, DwShape<32, 32>::BYTES);
+    sm_count();
+    return (int)cudaGetLastError();
+}
 
 int net_dw_blocks() { return sm_count() * 2; }
 long long net_partial_floats(int nblocks) {
@@ -465,8 +475,6 @@ int net_forward(const NetBox& b, __nv_bfloat16* const wfwd[NET_LAYERS], const fl
 template <int CINP, int COUTP>
 static void launch_dw(const DwArgs& a, int nblk, float* gW, cudaStream_t st) {
     using S = DwShape<CINP, COUTP>;
-    static bool init = false;
-    if (!init) { set_smem(k_conv_dw<CINP, COUTP>, S::BYTES); init = true; }
     k_conv_dw<CINP, COUTP><<<nblk, 128, S::BYTES, st>>>(a);
     const int n = 27 * a.cin * a.cout;
     k_dw_reduce<CINP, COUTP><<<(n + 255) / 256, 256, 0, st>>>(a.partial, nblk, gW, a.cin, a.cout);

@@ -71,6 +71,7 @@ int net_backward(const NetBox& b, __nv_bfloat16* const wbwd[NET_LAYERS], NetBuff
                  cudaStream_t st);
 int net_adam(float* params, const float* grads, float* m, float* v, long long n, float lr, float b1, float b2,
              float eps, int step, cudaStream_t st);
+int net_init();
 long long net_partial_floats(int nblocks);
 int net_dw_blocks();
 size_t net_act_bytes(long long E);

@@ -23,6 +23,7 @@ __global__ void k_step_begin(Scal* sc) {
     sc->odt = sc->time - sc->otime;
     sc->dtMinBits = 0x7FF0000000000000ull;  // +inf
     sc->nanCount = 0u;
+    sc->closureReject = 0;
 }
 
 // ================================================================================ predictor
@@ -109,23 +110,34 @@ __global__ void k_predict_cells(Lay L, Par p, GridP g, StateP n, StateP o, State
 
 // Flux2Deltas (stress.F90:150-196); O is the flux storage type (float on the FP32-flux path), the sums
 // run in double
+// corr: the learned closure's face corrections (24 float planes: direction d, variable v at d*8+v; the 5
+// gas fluxes then the 3 magnetic-stress momentum fluxes), added to the face fluxes, or null. With cond set
+// the kernel runs only when the closure's positivity check rejected this step (the plain fallback).
 template <typename O>
 __global__ void k_flux2deltas(Lay L, Par p, GridP g, FluxOut<O> FI, FluxOut<O> FJ, FluxOut<O> FK, PrimP dGH,
-                              Vec3P dGM) {
+                              Vec3P dGM, const float* corr, const Scal* cond) {
+    if (cond && !cond->closureReject) return;
     Reg r = {L.is(), L.Nip, L.js(), L.Njp, L.ks(), L.Nkp};
     int i, j, k;
     if (!reg_ijk(r, blockIdx.x * (long long)blockDim.x + threadIdx.x, i, j, k)) return;
     long long c = L.at(i, j, k), cj = c + L.P, ck = c + (long long)L.P * L.Q;
     double dV = g.volume[c];
+    auto cr = [&](int d, int v, long long lo, long long hi) {
+        if (!corr) return 0.0;
+        const float* q = corr + (long long)(d * 8 + v) * L.E;
+        return double(q[lo]) - double(q[hi]);
+    };
 #pragma unroll
     for (int v = 0; v < 5; ++v)
         dGH.w[v][c] = (double(FI.g[v][c]) - double(FI.g[v][c + 1]) + double(FJ.g[v][c]) - double(FJ.g[v][cj]) +
-                       double(FK.g[v][c]) - double(FK.g[v][ck])) / dV;
+                       double(FK.g[v][c]) - double(FK.g[v][ck]) +
+                       (cr(0, v, c, c + 1) + cr(1, v, c, cj) + cr(2, v, c, ck))) / dV;
     if (p.doMHD) {
 #pragma unroll
         for (int x = 0; x < 3; ++x)
             dGM.v[x][c] = (double(FI.m[x][c]) - double(FI.m[x][c + 1]) + double(FJ.m[x][c]) - double(FJ.m[x][cj]) +
-                           double(FK.m[x][c]) - double(FK.m[x][ck])) / dV;
+                           double(FK.m[x][c]) - double(FK.m[x][ck]) +
+                           (cr(0, 5 + x, c, c + 1) + cr(1, 5 + x, c, cj) + cr(2, 5 + x, c, ck))) / dV;
         if (p.doBackground) {   // background momentum source (stress.F90:185-188)
 #pragma unroll
             for (int x = 0; x < 3; ++x) dGM.v[x][c] = dGM.v[x][c] + g.dpB0[x][c];
@@ -733,6 +745,7 @@ int kernels_per_step(const Handle& h) {
     n += 1 + 1 + 1;                     // e2flux/copy, bflux2fld, update gas
     n += 2 + 3 + 1;                     // calcdt + finalize, 3 BC kernels, final bflux2fld
     n += ring_kernels_per_step(h);
+    if (h.closure) n += closure_kernels_per_step(h) + 1;   // + the conditional Flux2Deltas
     return n;
 }
 
@@ -784,20 +797,29 @@ int step_enqueue(Handle& h, int cur, cudaEvent_t* ev, bool split) {
     for (int v = 0; v < 5; ++v) dGH.w[v] = h.dGasH[v];
     Vec3P dGM = {{h.dGasM[0], h.dGasM[1], h.dGasM[2]}};
     long long nact = (long long)L.Nip * L.Njp * L.Nkp;
-    if (h.prec == PREC_FP32FLUX) {
-        FluxOut<float> F[3];
-        for (int d = 0; d < 3; ++d) {
-            for (int v = 0; v < 5; ++v) F[d].g[v] = h.f32.gflx[d][v];
-            for (int x = 0; x < 3; ++x) F[d].m[x] = h.f32.mflx[d][x];
+    // learned closure: face corrections from the net on State n; a corrected update that fails positivity
+    // falls back to the plain fluxes (the second, conditional Flux2Deltas)
+    const float* corr = h.closure ? closure_enqueue_corr(h, nS, st) : nullptr;
+    for (int pass = 0; pass < (corr ? 2 : 1); ++pass) {
+        const float* cq = pass == 0 ? corr : nullptr;
+        const Scal* cond = pass == 0 ? nullptr : h.dScal;
+        if (h.prec == PREC_FP32FLUX) {
+            FluxOut<float> F[3];
+            for (int d = 0; d < 3; ++d) {
+                for (int v = 0; v < 5; ++v) F[d].g[v] = h.f32.gflx[d][v];
+                for (int x = 0; x < 3; ++x) F[d].m[x] = h.f32.mflx[d][x];
+            }
+            k_flux2deltas<float><<<nblk(nact, TPB), TPB, 0, st>>>(L, p, g, F[0], F[1], F[2], dGH, dGM, cq, cond);
+        } else {
+            FluxP F[3];
+            for (int d = 0; d < 3; ++d) {
+                for (int v = 0; v < 5; ++v) F[d].g[v] = h.gflx[d][v];
+                for (int x = 0; x < 3; ++x) F[d].m[x] = h.mflx[d][x];
+            }
+            k_flux2deltas<double><<<nblk(nact, TPB), TPB, 0, st>>>(L, p, g, F[0], F[1], F[2], dGH, dGM, cq, cond);
         }
-        k_flux2deltas<float><<<nblk(nact, TPB), TPB, 0, st>>>(L, p, g, F[0], F[1], F[2], dGH, dGM);
-    } else {
-        FluxP F[3];
-        for (int d = 0; d < 3; ++d) {
-            for (int v = 0; v < 5; ++v) F[d].g[v] = h.gflx[d][v];
-            for (int x = 0; x < 3; ++x) F[d].m[x] = h.mflx[d][x];
-        }
-        k_flux2deltas<double><<<nblk(nact, TPB), TPB, 0, st>>>(L, p, g, F[0], F[1], F[2], dGH, dGM);
+        if (pass == 0 && corr) closure_enqueue_check(h, nS, st);
+        if (pass == 1) h.launches++;
     }
     mark(PH_UPDATE);
     // applyUpdate into the oState buffer (which becomes State n+1)

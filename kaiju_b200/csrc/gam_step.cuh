@@ -4,6 +4,8 @@
 #include <vector>
 #include "gam_common.cuh"
 
+struct gam_closure;
+
 namespace gam {
 
 enum Prec { PREC_FP64 = 0, PREC_FP32FLUX = 1 };
@@ -72,6 +74,7 @@ struct Handle {
     Scal* hScal = nullptr;   // pinned host mirror
     int cur = 0;
     int tilePhase = 0;       // split-step position of a tile (gam_tiles.cu): 0 between steps
+    ::gam_closure* closure = nullptr;   // learned flux closure applied in the step (gam_closure.cu)
 
     cudaGraphExec_t graph[2] = {nullptr, nullptr};
     bool useGraph = true;
@@ -98,6 +101,12 @@ void launch_bcs(Handle& h, const StateP& s, cudaStream_t st);
 void launch_calcdt(Handle& h, const StateP& s, int mode, cudaStream_t st);   // mode 0: in-step, 1: initial (no time advance)
 double launch_divb(Handle& h, double* scratchDev, cudaStream_t st);
 int kernels_per_step(const Handle& h);
+// learned closure in the step (gam_closure.cu): the net on State n and its face corrections (24 float
+// planes, area-scaled) before Flux2Deltas; after it the positivity check that sets Scal::closureReject
+const float* closure_enqueue_corr(Handle& h, const StateP& nS, cudaStream_t st);
+void closure_enqueue_check(Handle& h, const StateP& nS, cudaStream_t st);
+int closure_kernels_per_step(const Handle& h);
+int closure_attach(Handle& h, ::gam_closure* c);   // shape check, geometry and periodicity from h
 // interface fluxes of all directions (gam_flux.cu)
 void enqueue_fluxes(Handle& h, const StateP& nS, cudaStream_t st);
 void flux_kernels_init();

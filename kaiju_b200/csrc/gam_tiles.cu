@@ -442,6 +442,22 @@ int gam_gpu_stream(gam_gpu_t* G, void** stream) {
     return GAM_OK;
 }
 
+// Hatch's initial dt (init.F90:204-244) for a state placed on the device afterwards (gam_gpu_sync_to_device):
+// CalcDT on State, then oState%time = State%time - dt
+int gam_gpu_init_dt(gam_gpu_t* G) {
+    if (!G) return GAM_ERR_ARG;
+    Handle& h = capi_handle(G);
+    if (h.tilePhase != 0) return GAM_ERR_ARG;
+    k_red_reset<<<1, 1, 0, h.stream>>>(h.dScal);
+    launch_calcdt_partial(h, h.S[h.cur], h.stream);
+    launch_dt_finalize(h, 1, h.stream);
+    k_tiles_set_otime<<<1, 1, 0, h.stream>>>(h.dScal);
+    h.launches += 2;
+    int rc = capi_download_scalars(G);
+    if (rc) return rc;
+    return status_of(h.hScal->status);
+}
+
 int gam_gpu_calcdt_local(gam_gpu_t* G, long long* dtWords) {
     if (!G || !dtWords) return GAM_ERR_ARG;
     Handle& h = capi_handle(G);

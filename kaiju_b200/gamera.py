@@ -131,6 +131,16 @@ SIGNATURES = {
     "gam_closure_get_grads": (C.c_int, [C.c_void_p, _FP, C.c_longlong]),
     "gam_closure_forward_host": (C.c_int, [C.c_void_p, _FP, _FP]),
     "gam_closure_backward_host": (C.c_int, [C.c_void_p, _FP, _FP]),
+    "gam_closure_set_norm": (C.c_int, [C.c_void_p, _FP, _FP, _FP, _FP]),
+    "gam_closure_reserve": (C.c_int, [C.c_void_p, C.c_int]),
+    "gam_closure_capture": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p]),
+    "gam_closure_train": (C.c_int, [C.c_void_p, C.POINTER(C.c_int), C.c_int, C.c_float, _DP]),
+    "gam_closure_eval": (C.c_int, [C.c_void_p, C.POINTER(C.c_int), C.c_int, _DP, _DP]),
+    "gam_closure_residual_rms": (C.c_int, [C.c_void_p, C.c_int, _DP]),
+    "gam_gpu_set_closure": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "gam_gpu_closure_rejects": (C.c_int, [C.c_void_p, C.POINTER(C.c_int)]),
+    "gam_gpu_restrict": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint]),
+    "gam_gpu_init_dt": (C.c_int, [C.c_void_p]),
 }
 
 _lib = None
@@ -525,6 +535,29 @@ class GameraGPU:
         arr = buf[:n].reshape((m.Nip, m.Njp, m.Nkp, nv), order="F")
         return {self.SLICE_NAMES[v]: arr[..., v] for v in range(nv)}
 
+    def set_closure(self, closure: Optional["Closure"]):
+        rc = load_library().gam_gpu_set_closure(self.h, closure.c if closure is not None else None)
+        if rc:
+            raise GamError(rc, "gam_gpu_set_closure")
+        self._closure = closure   # keep it alive while attached
+
+    def closure_rejects(self) -> int:
+        n = C.c_int()
+        rc = load_library().gam_gpu_closure_rejects(self.h, C.byref(n))
+        if rc:
+            raise GamError(rc, "gam_gpu_closure_rejects")
+        return n.value
+
+    def restrict_from(self, fine: "GameraGPU", what: int = GAM_SYNC_STATE):
+        rc = load_library().gam_gpu_restrict(fine.h, self.h, what)
+        if rc:
+            raise GamError(rc, "gam_gpu_restrict")
+
+    def init_dt(self):
+        rc = load_library().gam_gpu_init_dt(self.h)
+        if rc:
+            raise GamError(rc, "gam_gpu_init_dt")
+
     def divb(self) -> float:
         v = C.c_double()
         rc = load_library().gam_gpu_divb(self.h, C.byref(v))
@@ -671,6 +704,34 @@ class Closure:
         gout = np.asfortranarray(gout, dtype=np.float32)
         self._call("gam_closure_backward_host", _fp(x), _fp(gout))
         return self.grads()
+
+    def set_norm(self, in_mean, in_scale, flux_scale, res_scale):
+        a = [np.ascontiguousarray(x, dtype=np.float32) for x in (in_mean, in_scale, flux_scale, res_scale)]
+        assert [len(x) for x in a] == [8, 8, 8, 5]
+        self._call("gam_closure_set_norm", *[_fp(x) for x in a])
+
+    def reserve(self, n: int):
+        self._call("gam_closure_reserve", n)
+
+    def capture(self, slot: int, coarse: "GameraGPU", fine: "GameraGPU"):
+        self._call("gam_closure_capture", slot, coarse.h, fine.h)
+
+    def residual_rms(self, slot: int):
+        out = np.zeros(6)
+        self._call("gam_closure_residual_rms", slot, out.ctypes.data_as(_DP))
+        return out[:5], out[5]
+
+    def train(self, slots, lr: float) -> float:
+        arr = (C.c_int * len(slots))(*slots)
+        loss = C.c_double()
+        self._call("gam_closure_train", arr, len(slots), lr, C.byref(loss))
+        return loss.value
+
+    def eval(self, slots):
+        arr = (C.c_int * len(slots))(*slots)
+        a, b = C.c_double(), C.c_double()
+        self._call("gam_closure_eval", arr, len(slots), C.byref(a), C.byref(b))
+        return a.value, b.value
 
     def close(self):
         if self.c:
