@@ -46,6 +46,8 @@ def parse():
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-n", type=int, default=64)
+    ap.add_argument("--no-extras", action="store_true",
+                    help="skip the FP32-flux and closure side measurements (run on 1 GPU only)")
     return ap.parse_args()
 
 
@@ -251,12 +253,64 @@ def run_ours(args, rank, world, local):
         "gpu_launches": (launches_per_step or 0) * args.steps,
         "roofline": roof, "clocks": clocks, "status": st["status"], "t_sim": st["t"], "dt": st["dt"],
     }
+    if world == 1 and not args.no_extras:
+        out["headline_extras"] = headline_extras(n, args.steps)
     if rank == 0 and not args.no_cpu_baseline:
         out["cpu_baseline"] = cpu_baseline(args.cpu_n, steps=2)
     if world > 1:
         import torch.distributed as dist
         dist.barrier()
         dist.destroy_process_group()
+    return out
+
+
+def headline_extras(n, steps):
+    """The rest of the headline metric on the same GPU: the FP32-flux path against the FP64 path on the
+    same problem (device ms per step and the L1 difference of the gas state after `steps` steps, relative
+    to the mean |value| per variable), and the cost of a step with the learned closure on the coarse
+    turbulence grid next to the plain coarse and the fine step (the closure's accuracy comes from its
+    training run, kaiju_b200/closure_train.py)."""
+    from kaiju_b200 import gamera as gm, turbulence as tu
+    out = {}
+    model = model_for(n)
+    xyz = gm.corners_warped(model, (-0.5, 0.5) * 3, 0.04)
+    g64 = gm.GameraGPU.from_corners(model, xyz, "BW")
+    g32 = gm.GameraGPU.from_corners(model, xyz, "BW")
+    g32.set_precision(gm.GAM_FP32FLUX)
+    ms64, _ = g64.run_steps_timed(steps)
+    ms32, _ = g32.run_steps_timed(steps)
+    a, b = g64.fetch("gas")[4:-4, 4:-4, 4:-4], g32.fetch("gas")[4:-4, 4:-4, 4:-4]
+    l1 = [float(np.mean(np.abs(a[..., v] - b[..., v])) / max(np.mean(np.abs(a[..., v])), 1e-300)) for v in range(5)]
+    g64.close()
+    g32.close()
+    out["fp32flux"] = {"ms_per_step": ms32 / steps, "fp64_ms_per_step": ms64 / steps,
+                       "speedup_vs_fp64": ms64 / ms32, "steps": steps,
+                       "l1_rel_vs_fp64_per_var": l1, "l1_rel_vs_fp64": max(l1),
+                       "value": n ** 3 * steps / (ms32 / 1e3)}
+    # closure cost: 128^3 coarse turbulence with the net attached (its weights do not change the cost)
+    nc = 128
+    fine = tu.turbulence_problem(2 * nc, 64)
+    fine.run_steps(3)
+    msf, _ = fine.run_steps_timed(10)
+    c = tu.coarse_problem(nc)
+    c.restrict_from(fine, gm.GAM_SYNC_STATE)
+    c.restrict_from(fine, gm.GAM_SYNC_OSTATE)
+    fine.close()
+    st = c.status()
+    c.set_scalars(st["t"], 1.0e-3, 0.0, 1, st["time"], st["time"] - 1.0e-3)
+    c.run_steps(3)
+    msp, _ = c.run_steps_timed(10)
+    cl = gm.Closure(nc, nc, nc, seed=0)
+    c.set_closure(cl)
+    c.run_steps(3)
+    msc, _ = c.run_steps_timed(10)
+    c.set_closure(None)
+    c.close()
+    cl.close()
+    out["closure"] = {"coarse_cells": [nc] * 3, "fine_cells": [2 * nc] * 3,
+                      "fine_ms_per_step": msf / 10, "coarse_plain_ms_per_step": msp / 10,
+                      "coarse_closure_ms_per_step": msc / 10,
+                      "fine_over_closure_per_coarse_step": 2 * (msf / 10) / (msc / 10)}
     return out
 
 

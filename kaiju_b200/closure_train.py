@@ -172,6 +172,28 @@ def rollout(closure: gm.Closure, n: int, seed: int, t_end: float):
     return out
 
 
+def step_costs(closure: gm.Closure, n: int, seed: int, steps: int = 20):
+    """Device ms per step (CUDA events over graph-replayed steps) of the fine problem, the plain coarse
+    problem and the coarse problem with the closure."""
+    fine = tu.turbulence_problem(2 * n, seed)
+    out = {}
+    fine.run_steps(3)
+    ms, _ = fine.run_steps_timed(steps)
+    out["fine_ms"] = ms / steps
+    for name in ("plain", "closure"):
+        c = _coarse_from(fine, n, 1.0e30)
+        if name == "closure":
+            c.set_closure(closure)
+        c.run_steps(3)
+        ms, _ = c.run_steps_timed(steps)
+        out[name + "_ms"] = ms / steps
+        if name == "closure":
+            c.set_closure(None)
+        c.close()
+    fine.close()
+    return out
+
+
 def _problem_with_tfin(n, seed, t_end):
     model = tu.turbulence_model(n)
     model.tFin = t_end
@@ -236,6 +258,7 @@ def train_and_evaluate(n, train_seeds, eval_seeds, per_seed, epochs, lr, warm, g
     after_tr = closure.eval(tr)
     after = closure.eval(ev)
     rolls = [rollout(closure, n, s, t_end) for s in eval_seeds[:rollouts]]
+    costs = step_costs(closure, n, eval_seeds[0])
     closure.close()
     return {
         "n_coarse": n, "n_fine": 2 * n, "train_seeds": list(train_seeds), "eval_seeds": list(eval_seeds),
@@ -247,6 +270,7 @@ def train_and_evaluate(n, train_seeds, eval_seeds, per_seed, epochs, lr, warm, g
         "eval_loss": {"untrained": before[0], "net": after[0], "none": after[1],
                       "gain": after[1] / after[0] if after[0] > 0 else None},
         "rollouts": rolls,
+        "step_ms": costs,
     }
 
 
