@@ -172,6 +172,33 @@ def rollout(closure: gm.Closure, n: int, seed: int, t_end: float):
     return out
 
 
+def three_levels(closure: gm.Closure, n: int, seed: int, t_end: float):
+    """Errors against a truth run two levels finer: the truth (4n)^3, the fine (2n)^3 run and the coarse n^3
+    runs (plain and with the closure) all start from restrictions of the truth's initial state and run to
+    t_end; each is compared, restricted to n^3, with the restricted truth. The closure reaches the fine-grid
+    error when its L1 is at most the fine run's."""
+    truth = _problem_with_tfin(4 * n, seed, t_end)
+    fine = _coarse_from(truth, 2 * n, t_end)
+    plain = _coarse_from(fine, n, t_end)
+    cl = _coarse_from(fine, n, t_end)
+    cl.set_closure(closure)
+    out = {"seed": seed, "t_end": t_end, "cells": [n, 2 * n, 4 * n]}
+    for name, g in (("truth", truth), ("fine", fine), ("plain", plain), ("closure", cl)):
+        sec, st = _timed_advance(g, t_end)
+        out[name] = {"seconds": sec, "steps": st}
+    t2 = _coarse_from(truth, 2 * n, t_end)
+    ref = _coarse_from(t2, n, t_end)
+    f1 = _coarse_from(fine, n, t_end)
+    for name, g in (("fine", f1), ("plain", plain), ("closure", cl)):
+        err, per = l1_error(g, ref)
+        out[name].update({"l1": err, "l1_per_var": per})
+    out["closure"]["rejects"] = cl.closure_rejects()
+    cl.set_closure(None)
+    for g in (truth, fine, plain, cl, t2, ref, f1):
+        g.close()
+    return out
+
+
 def step_costs(closure: gm.Closure, n: int, seed: int, steps: int = 20):
     """Device ms per step (CUDA events over graph-replayed steps) of the fine problem, the plain coarse
     problem and the coarse problem with the closure."""
@@ -231,10 +258,12 @@ def main(argv=None):
     ap.add_argument("--gap", type=int, default=6)
     ap.add_argument("--t-end", type=float, default=0.1)
     ap.add_argument("--rollouts", type=int, default=2)
+    ap.add_argument("--three-levels", type=int, default=0,
+                    help="also evaluate this many held-out seeds against a truth run at 4n (needs (4n)^3 to fit)")
     ap.add_argument("--out", default=None)
     a = ap.parse_args(argv)
     report = train_and_evaluate(a.n, _seeds(a.train_seeds), _seeds(a.eval_seeds), a.per_seed, a.epochs, a.lr,
-                                a.warm, a.gap, a.t_end, a.rollouts)
+                                a.warm, a.gap, a.t_end, a.rollouts, three=a.three_levels)
     s = json.dumps(report, indent=1)
     if a.out:
         with open(a.out, "w") as f:
@@ -242,7 +271,8 @@ def main(argv=None):
     print(s)
 
 
-def train_and_evaluate(n, train_seeds, eval_seeds, per_seed, epochs, lr, warm, gap, t_end, rollouts, log=print):
+def train_and_evaluate(n, train_seeds, eval_seeds, per_seed, epochs, lr, warm, gap, t_end, rollouts, log=print,
+                       three=0):
     t0 = time.perf_counter()
     closure = gm.Closure(n, n, n, seed=0)
     closure.reserve(per_seed * (len(train_seeds) + len(eval_seeds)))
@@ -258,6 +288,7 @@ def train_and_evaluate(n, train_seeds, eval_seeds, per_seed, epochs, lr, warm, g
     after_tr = closure.eval(tr)
     after = closure.eval(ev)
     rolls = [rollout(closure, n, s, t_end) for s in eval_seeds[:rollouts]]
+    levels = [three_levels(closure, n, s, t_end) for s in eval_seeds[:three]]
     costs = step_costs(closure, n, eval_seeds[0])
     closure.close()
     return {
@@ -270,6 +301,7 @@ def train_and_evaluate(n, train_seeds, eval_seeds, per_seed, epochs, lr, warm, g
         "eval_loss": {"untrained": before[0], "net": after[0], "none": after[1],
                       "gain": after[1] / after[0] if after[0] > 0 else None},
         "rollouts": rolls,
+        "three_levels": levels,
         "step_ms": costs,
     }
 

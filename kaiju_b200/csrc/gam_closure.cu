@@ -71,14 +71,14 @@ Lay make_lay(int Nip, int Njp, int Nkp) {
     return L;
 }
 
-// Fortran (Ni,Nj,Nk,nc) host layout -> planar bf16 planes at the pencil index
+// Fortran (Ni,Nj,Nk,nc) host layout -> the net's channels-last input at the pencil index
 __global__ void k_in_from_fortran(Lay L, const float* src, int nc, __nv_bfloat16* dst) {
     const long long n = (long long)L.Ni * L.Nj * L.Nk;
     const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (t >= n) return;
     const int i = (int)(t % L.Ni), j = (int)((t / L.Ni) % L.Nj), k = (int)(t / ((long long)L.Ni * L.Nj));
     const long long c = L.at(i, j, k);
-    for (int q = 0; q < nc; ++q) dst[(long long)q * L.E + c] = __float2bfloat16_rn(src[t + q * n]);
+    for (int q = 0; q < nc; ++q) dst[c * NET_IN_PITCH + q] = __float2bfloat16_rn(src[t + q * n]);
 }
 // active cells of fp32 planes -> Fortran (Nip,Njp,Nkp,nc)
 __global__ void k_out_to_fortran(Lay L, const float* src, int nc, float* dst) {
@@ -89,14 +89,14 @@ __global__ void k_out_to_fortran(Lay L, const float* src, int nc, float* dst) {
     const long long c = L.at(i + 4, j + 4, k + 4);
     for (int q = 0; q < nc; ++q) dst[t + q * n] = src[(long long)q * L.E + c];
 }
-// Fortran (Nip,Njp,Nkp,nc) gradient of the active cells -> bf16 planes (zero elsewhere)
+// Fortran (Nip,Njp,Nkp,nc) gradient of the active cells -> channels-last bf16 (zero elsewhere)
 __global__ void k_gout_from_fortran(Lay L, const float* src, int nc, __nv_bfloat16* dst) {
     const long long n = (long long)L.Nip * L.Njp * L.Nkp;
     const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (t >= n) return;
     const int i = (int)(t % L.Nip), j = (int)((t / L.Nip) % L.Njp), k = (int)(t / ((long long)L.Nip * L.Njp));
     const long long c = L.at(i + 4, j + 4, k + 4);
-    for (int q = 0; q < nc; ++q) dst[(long long)q * L.E + c] = __float2bfloat16_rn(src[t + q * n]);
+    for (int q = 0; q < nc; ++q) dst[c * NET_PITCH + q] = __float2bfloat16_rn(src[t + q * n]);
 }
 
 
@@ -112,7 +112,7 @@ NormP norm_of(const gam_closure* C) {
     return n;
 }
 
-// the net's input planes from a state: normalised rho, v, P, B of every cell (ghosts included)
+// the net's input from a state: normalised rho, v, P, B of every cell (ghosts included), channels-last
 __global__ void k_closure_input(Lay L, double gamma, StateP s, NormP n, __nv_bfloat16* in) {
     const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (t >= (long long)L.Ni * L.Nj * L.Nk) return;
@@ -126,7 +126,7 @@ __global__ void k_closure_input(Lay L, double gamma, StateP s, NormP n, __nv_bfl
     for (int q = 0; q < 8; ++q) {
         float f = (float)((w[q] - n.inMean[q]) / n.inScale[q]);
         if (!(f == f) || fabsf(f) > 1e4f) f = 0.f;   // keep the net's input finite
-        in[(long long)q * L.E + c] = __float2bfloat16_rn(f);
+        in[c * NET_IN_PITCH + q] = __float2bfloat16_rn(f);
     }
 }
 
@@ -316,7 +316,7 @@ __global__ void k_loss_grad(Lay L, const float* w, const float* geom, NormP n, _
             const int u = v < 5 ? v : v - 4;   // the magnetic-stress corrections act on the momentum
             const float g = zero ? 0.f
                                  : n.fluxScale[v] * A * (w[(long long)u * L.E + c] - w[(long long)u * L.E + below]);
-            gout[(long long)(d * 8 + v) * L.E + c] = __float2bfloat16_rn(g);
+            gout[c * NET_PITCH + d * 8 + v] = __float2bfloat16_rn(g);
         }
     }
 }
@@ -389,19 +389,18 @@ int gam_closure_create(gam_closure_t** out, int Nip, int Njp, int Nkp, unsigned 
             cudaMalloc(&C->wbwd[l], sizeof(__nv_bfloat16) * 27 * bc * 32))
             return fail(GAM_ERR_CUDA);
     }
-    // activation planes: act (8 + 3*32), pre (3*32), gact (24 + 3*32) bf16; out (24) fp32
+    // channels-last activations: act (16 + 3*32), pre (3*32), grad (4*32) bf16 per cell; out (24) fp32 planes
     const long long E = L.E;
-    const long long bfPlanes = NET_IN + 3 * NET_WIDTH + 3 * NET_WIDTH + NET_OUT + 3 * NET_WIDTH;
-    const size_t bytes = sizeof(__nv_bfloat16) * E * bfPlanes + sizeof(float) * E * NET_OUT;
+    const long long bfPerCell = NET_IN_PITCH + 3 * NET_PITCH + 3 * NET_PITCH + 4 * NET_PITCH;
+    const size_t bytes = sizeof(__nv_bfloat16) * E * bfPerCell + sizeof(float) * E * NET_OUT;
     if (cudaMalloc(&C->pool, bytes) != cudaSuccess) return fail(GAM_ERR_CUDA);
     cudaMemsetAsync(C->pool, 0, bytes, C->stream);
     __nv_bfloat16* q = static_cast<__nv_bfloat16*>(C->pool);
-    C->nb.act[0] = q; q += E * NET_IN;
-    for (int l = 1; l < NET_LAYERS; ++l) { C->nb.act[l] = q; q += E * NET_WIDTH; }
-    for (int l = 0; l < NET_LAYERS - 1; ++l) { C->nb.pre[l] = q; q += E * NET_WIDTH; }
+    C->nb.act[0] = q; q += E * NET_IN_PITCH;
+    for (int l = 1; l < NET_LAYERS; ++l) { C->nb.act[l] = q; q += E * NET_PITCH; }
+    for (int l = 0; l < NET_LAYERS - 1; ++l) { C->nb.pre[l] = q; q += E * NET_PITCH; }
     C->nb.pre[NET_LAYERS - 1] = nullptr;
-    C->nb.gact[0] = q; q += E * NET_OUT;
-    for (int l = 1; l < NET_LAYERS; ++l) { C->nb.gact[l] = q; q += E * NET_WIDTH; }
+    for (int l = 0; l < NET_LAYERS; ++l) { C->nb.grad[l] = q; q += E * NET_PITCH; }
     C->nb.out = reinterpret_cast<float*>(q);
     C->nb.partialFloats = net_partial_floats(net_dw_blocks());
     if (cudaMalloc(&C->nb.partial, sizeof(float) * C->nb.partialFloats) != cudaSuccess) return fail(GAM_ERR_CUDA);
@@ -496,7 +495,7 @@ int gam_closure_backward_host(gam_closure_t* C, const float* in, const float* go
     if (net_forward(C->box, C->wfwd, C->params, C->nb, true, C->err, C->stream) != 0) return GAM_ERR_CUDA;
     CKC(cudaStreamSynchronize(C->stream));
     CKC(cudaMemcpyAsync(C->stage, gout, sizeof(float) * nAct * NET_OUT, cudaMemcpyHostToDevice, C->stream));
-    k_gout_from_fortran<<<(unsigned)((nAct + 255) / 256), 256, 0, C->stream>>>(L, C->stage, NET_OUT, C->nb.gact[0]);
+    k_gout_from_fortran<<<(unsigned)((nAct + 255) / 256), 256, 0, C->stream>>>(L, C->stage, NET_OUT, C->nb.grad[NET_LAYERS - 1]);
     if (net_backward(C->box, C->wbwd, C->nb, C->grads, C->err, C->stream) != 0) return GAM_ERR_CUDA;
     return check_err(C);
 }
@@ -571,9 +570,9 @@ int gam_closure_reserve(gam_closure_t* C, int n) {
     while ((int)C->sIn.size() < n) {
         __nv_bfloat16* in = nullptr;
         float* res = nullptr;
-        if (cudaMalloc(&in, sizeof(__nv_bfloat16) * E * NET_IN) != cudaSuccess) return GAM_ERR_CUDA;
+        if (cudaMalloc(&in, sizeof(__nv_bfloat16) * E * NET_IN_PITCH) != cudaSuccess) return GAM_ERR_CUDA;
         if (cudaMalloc(&res, sizeof(float) * E * 5) != cudaSuccess) { cudaFree(in); return GAM_ERR_CUDA; }
-        cudaMemsetAsync(in, 0, sizeof(__nv_bfloat16) * E * NET_IN, C->stream);
+        cudaMemsetAsync(in, 0, sizeof(__nv_bfloat16) * E * NET_IN_PITCH, C->stream);
         cudaMemsetAsync(res, 0, sizeof(float) * E * 5, C->stream);
         C->sIn.push_back(in);
         C->sRes.push_back(res);
@@ -623,7 +622,7 @@ static int closure_sample_pass(gam_closure* C, int slot, bool train, float lr) {
     k_loss_sum<<<1, 32, 0, C->stream>>>(C->lossPart, nb, C->lossAcc);
     if (train) {
         k_loss_grad<<<nblk256((long long)L.Nip * L.Njp * L.Nkp), 256, 0, C->stream>>>(L, C->wts, C->geom, n,
-                                                                                       C->nb.gact[0]);
+                                                                                       C->nb.grad[NET_LAYERS - 1]);
         if (net_backward(C->box, C->wbwd, C->nb, C->grads, C->err, C->stream) != 0) return GAM_ERR_CUDA;
         C->adamStep++;
         if (net_adam(C->params, C->grads, C->m, C->v, C->np, lr, 0.9f, 0.999f, 1e-8f, C->adamStep, C->stream) != 0)

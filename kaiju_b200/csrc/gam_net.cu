@@ -27,25 +27,30 @@ __device__ __forceinline__ uint32_t pack2(float a, float b) {
 enum { MODE_HIDDEN = 0, MODE_OUT = 1, MODE_BWD = 2 };
 
 struct ConvArgs {
-    const __nv_bfloat16* x;    // input planes [cin][E]
-    const __nv_bfloat16* gz;   // MODE_BWD: the A operand is x * gelu'(gz) when non-null
-    const __nv_bfloat16* w;    // packed weights, 27 taps of [COUTP x CINP] K-major blocks
+    const __nv_bfloat16* x;    // input activations, channels-last with pitch CINP
+    const __nv_bfloat16* gz;   // MODE_BWD: pre-activation of the previous layer (pitch 32): the epilogue
+                               // multiplies the input gradient by its GELU derivative
+    const __nv_bfloat16* w;    // packed weights, 27 taps of [32 x CINP] K-major blocks
     const float* bias;         // [cout] (MODE_HIDDEN, MODE_OUT)
-    __nv_bfloat16* y;          // MODE_HIDDEN: GELU(z); MODE_BWD: the input gradient
-    __nv_bfloat16* z;          // MODE_HIDDEN: pre-activation (null: not kept)
+    __nv_bfloat16* y;          // MODE_HIDDEN: GELU(z); MODE_BWD: the previous layer's gradient (pitch 32)
+    __nv_bfloat16* z;          // MODE_HIDDEN: pre-activation (null: not kept), pitch 32
     float* yf;                 // MODE_OUT: output planes [cout][E]
     long long E, c0, c1;
-    int P, Q, cin, cout;
+    int P, Q, cout;
     int* err;
 };
 
-template <int CINP, int COUTP>
-struct ConvSmem {
-    static constexpr int TAPB = COUTP * CINP * 2;
-    static constexpr int WB = 27 * TAPB;
-    static constexpr int WBA = (WB + 1023) / 1024 * 1024;
-    static constexpr int AB = 128 * CINP * 2;
-    static constexpr int BYTES = WBA + 2 * AB + 1024;
+template <int CINP>
+struct ConvShape {
+    static constexpr int COUTP = 32;
+    static constexpr int ROWS = 130;                   // 128 cells and one on each side (di = -1, +1)
+    static constexpr int KCH = CINP / 8;               // 16-byte channel chunks per cell
+    static constexpr int LBO = ROWS * 16;              // bytes between the channel-chunk blocks of a window
+    static constexpr int WIN = KCH * LBO;
+    static constexpr int TAPB = COUTP * CINP * 2;      // one tap's packed weights
+    static constexpr int STAGE = (WIN + 3 * TAPB + 127) / 128 * 128;   // a window and its three taps' weights
+    static constexpr int NBUF = 3;
+    static constexpr int BYTES = NBUF * STAGE + 1024;
 };
 
 __device__ __forceinline__ unsigned char* align1k(unsigned char* p) {
@@ -53,121 +58,156 @@ __device__ __forceinline__ unsigned char* align1k(unsigned char* p) {
     return p + ((1024u - (s & 1023u)) & 1023u);
 }
 
-// out[cell][n] = sum over taps t and input channels c of A_t[cell][c] * W_t[n][c], 128 cells per tile
-template <int CINP, int COUTP, int MODE>
+__device__ __forceinline__ void cp_async16(void* dst, const void* src, uint32_t bytes) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" :: "r"(tc::smem_u32(dst)), "l"(src), "r"(bytes)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async16_ca(void* dst, const void* src) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 16;" :: "r"(tc::smem_u32(dst)), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" :: "n"(N) : "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+
+// out[cell][n] = sum over taps t and input channels c of in[cell + off(t)][c] * W_t[n][c], 128 cells per tile
+template <int CINP, int MODE>
 __global__ void __launch_bounds__(128) k_conv(ConvArgs a) {
-    static_assert(CINP % 16 == 0 && COUTP % 16 == 0 && COUTP <= 32, "tile shape");
-    using S = ConvSmem<CINP, COUTP>;
+    using S = ConvShape<CINP>;
+    static_assert(CINP % 16 == 0, "K step");
     extern __shared__ unsigned char smraw[];
-    unsigned char* sW = align1k(smraw);
-    unsigned char* sA = sW + S::WBA;
-    __shared__ __align__(8) uint64_t mbar[2];
+    unsigned char* sStage = align1k(smraw);
+    __shared__ __align__(8) uint64_t mbar[S::NBUF];
     __shared__ uint32_t tmemBase;
     const int tid = threadIdx.x, warp = tid >> 5;
 
-    for (int q = tid; q < S::WB / 16; q += 128)
-        reinterpret_cast<uint4*>(sW)[q] = reinterpret_cast<const uint4*>(a.w)[q];
     if (tid == 0) {
-        tc::mbar_init(&mbar[0], 1);
-        tc::mbar_init(&mbar[1], 1);
+        for (int b = 0; b < S::NBUF; ++b) tc::mbar_init(&mbar[b], 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     if (warp == 0) tc::tmem_alloc(&tmemBase, 32);
-    tc::fence_smem_async();
     tc::fence_before_sync();
     __syncthreads();
     tc::fence_after_sync();
     const uint32_t tbase = tmemBase;
-    const uint32_t idesc = tc::idesc_bf16_f32(128, COUTP);
-    constexpr uint32_t SBO = CINP / 8 * 128;
-    const unsigned short* xs = reinterpret_cast<const unsigned short*>(a.x);
-    const bool gated = MODE == MODE_BWD && a.gz != nullptr;
+    const uint32_t idesc = tc::idesc_bf16_f32(128, S::COUTP);
+    constexpr uint32_t SBO_W = CINP / 8 * 128;
 
-    uint32_t use0 = 0, use1 = 0;
-    int ok = 1, it = 0;
     const long long ntiles = (a.c1 - a.c0 + 127) / 128;
-    for (long long tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
-        const long long cell0 = a.c0 + tile * 128;
-        for (int t = 0; t < 27; ++t, ++it) {
-            const int b = it & 1;
-            const uint32_t use = b ? use1 : use0;
-            bool fine = true;
-            if (use > 0) fine = tc::mbar_wait(&mbar[b], (use - 1) & 1u, WAIT_LIMIT);
-            unsigned char* dA = sA + b * S::AB;
-            if (fine) {
-                const long long cell = cell0 + tid + tap_off(t, a.P, a.Q);
+    const long long myTiles = ntiles > blockIdx.x ? (ntiles - 1 - blockIdx.x) / gridDim.x + 1 : 0;
+    const long long nwin = myTiles * 9;
+    // copy window `it` (tile it / 9, offset (dj, dk) = it % 9) and the weights of its three taps (consecutive
+    // in the packed array) into stage it % NBUF
+    auto issue = [&](long long it) {
+        if (it < nwin) {
+            const long long tile = blockIdx.x + (it / 9) * (long long)gridDim.x;
+            const int w = (int)(it % 9), dj = w % 3 - 1, dk = w / 3 - 1;
+            const long long base = a.c0 + tile * 128 - 1 + (long long)a.P * (dj + (long long)a.Q * dk);
+            unsigned char* dst = sStage + (int)(it % S::NBUF) * S::STAGE;
+            for (int id = tid; id < S::ROWS * S::KCH; id += 128) {
+                const int row = id / S::KCH, kc = id % S::KCH;
+                const long long cell = base + row;
                 const bool inb = cell >= 0 && cell < a.E;
-#pragma unroll
-                for (int kc = 0; kc < CINP / 8; ++kc) {
-                    uint32_t pk[4];
-#pragma unroll
-                    for (int e = 0; e < 8; e += 2) {
-                        const int c = kc * 8 + e;
-                        if (!gated) {
-                            uint32_t lo = (inb && c < a.cin) ? xs[(long long)c * a.E + cell] : 0u;
-                            uint32_t hi = (inb && c + 1 < a.cin) ? xs[(long long)(c + 1) * a.E + cell] : 0u;
-                            pk[e / 2] = lo | (hi << 16);
-                        } else {
-                            float f0 = 0.f, f1 = 0.f;
-                            if (inb && c < a.cin)
-                                f0 = bf2f(a.x[(long long)c * a.E + cell]) * gelu_d(bf2f(a.gz[(long long)c * a.E + cell]));
-                            if (inb && c + 1 < a.cin)
-                                f1 = bf2f(a.x[(long long)(c + 1) * a.E + cell]) *
-                                     gelu_d(bf2f(a.gz[(long long)(c + 1) * a.E + cell]));
-                            pk[e / 2] = pack2(f0, f1);
-                        }
-                    }
-                    *reinterpret_cast<uint4*>(dA + tc::kmajor_off(tid, kc * 8, CINP)) =
-                        make_uint4(pk[0], pk[1], pk[2], pk[3]);
-                }
+                const __nv_bfloat16* src = a.x + (inb ? cell : 0) * CINP + kc * 8;
+                cp_async16(dst + kc * S::LBO + row * 16, src, inb ? 16u : 0u);
             }
-            tc::fence_smem_async();
-            if (!__syncthreads_and(fine)) { ok = 0; break; }
-            if (tid == 0) {
-                tc::fence_after_sync();
+            const unsigned char* wsrc = reinterpret_cast<const unsigned char*>(a.w) + (3 * (dj + 1) + 9 * (dk + 1)) * S::TAPB;
+            for (int id = tid; id < 3 * S::TAPB / 16; id += 128) cp_async16_ca(dst + S::WIN + id * 16, wsrc + id * 16);
+        }
+        cp_async_commit();
+    };
+    uint32_t cnt[S::NBUF] = {0, 0, 0};
+    int ok = 1;
+    issue(0);
+    issue(1);
+    for (long long it = 0; it < nwin; ++it) {
+        const int b = (int)(it % S::NBUF);
+        // buffer of window it+2 held window it-1: wait for its MMAs before copying over it
+        bool fine = true;
+        {
+            const long long nx = it + 2;
+            const int bn = (int)(nx % S::NBUF);
+            if (nx < nwin && cnt[bn] > 0) fine = tc::mbar_wait(&mbar[bn], (cnt[bn] - 1) & 1u, WAIT_LIMIT);
+            if (fine) issue(nx);
+            else cp_async_commit();
+        }
+        cp_async_wait<2>();
+        tc::fence_smem_async();
+        if (!__syncthreads_and(fine)) { ok = 0; break; }
+        const int w = (int)(it % 9);
+        if (tid == 0) {
+            tc::fence_after_sync();
+            const uint32_t win = tc::smem_u32(sStage + b * S::STAGE);
+#pragma unroll
+            for (int di = -1; di <= 1; ++di) {
 #pragma unroll
                 for (int ks = 0; ks < CINP / 16; ++ks) {
-                    uint64_t ad = tc::desc_kmajor(tc::smem_u32(dA) + ks * 256, 128, SBO);
-                    uint64_t bd = tc::desc_kmajor(tc::smem_u32(sW + t * S::TAPB) + ks * 256, 128, SBO);
-                    tc::mma_bf16(tbase, ad, bd, idesc, t > 0 || ks > 0);
+                    const uint64_t ad = tc::desc_kmajor(win + (di + 1) * 16 + ks * 2 * S::LBO, S::LBO, 128);
+                    const uint64_t bd = tc::desc_kmajor(win + S::WIN + (di + 1) * S::TAPB + ks * 256, 128, SBO_W);
+                    tc::mma_bf16(tbase, ad, bd, idesc, !(w == 0 && di == -1 && ks == 0));
                 }
-                tc::mma_commit(&mbar[b]);
             }
-            if (b) ++use1; else ++use0;
+            tc::mma_commit(&mbar[b]);
         }
-        if (!ok) break;
-        const int bl = (it - 1) & 1;
-        const uint32_t ul = bl ? use1 : use0;
-        bool fine = tc::mbar_wait(&mbar[bl], (ul - 1) & 1u, WAIT_LIMIT);
-        if (!__syncthreads_and(fine)) { ok = 0; break; }
-        tc::fence_after_sync();
-        float acc[32];
-        tc::tmem_ld32(tbase + ((uint32_t)(warp * 32) << 16), acc);
-        const long long cell = cell0 + tid;
-        if (cell < a.c1) {
+        ++cnt[b];
+        if (w == 8) {   // the tile's last window: wait for its MMAs, then the epilogue
+            fine = tc::mbar_wait(&mbar[b], (cnt[b] - 1) & 1u, WAIT_LIMIT);
+            if (!__syncthreads_and(fine)) { ok = 0; break; }
+            tc::fence_after_sync();
+            float acc[32];
+            tc::tmem_ld32(tbase + ((uint32_t)(warp * 32) << 16), acc);
+            const long long cell = a.c0 + (blockIdx.x + (it / 9) * (long long)gridDim.x) * 128 + tid;
+            if (cell < a.c1) {
+                if (MODE == MODE_OUT) {
 #pragma unroll
-            for (int co = 0; co < 32; ++co) {
-                if (co >= a.cout) break;
-                const long long o = (long long)co * a.E + cell;
-                if (MODE == MODE_HIDDEN) {
-                    float zf = acc[co] + a.bias[co];
-                    if (a.z) a.z[o] = __float2bfloat16_rn(zf);
-                    a.y[o] = __float2bfloat16_rn(gelu(zf));
-                } else if (MODE == MODE_OUT) {
-                    a.yf[o] = acc[co] + a.bias[co];
+                    for (int co = 0; co < 32; ++co)
+                        if (co < a.cout) a.yf[(long long)co * a.E + cell] = acc[co] + a.bias[co];
                 } else {
-                    a.y[o] = __float2bfloat16_rn(acc[co]);
+                    uint32_t py[16], pz[16];
+                    if (MODE == MODE_BWD) {
+                        const uint4* g4 = reinterpret_cast<const uint4*>(a.gz + cell * NET_PITCH);
+                        uint32_t gz[16];
+#pragma unroll
+                        for (int q = 0; q < 4; ++q) {
+                            uint4 u = g4[q];
+                            gz[4 * q] = u.x; gz[4 * q + 1] = u.y; gz[4 * q + 2] = u.z; gz[4 * q + 3] = u.w;
+                        }
+#pragma unroll
+                        for (int q = 0; q < 16; ++q) {
+                            __nv_bfloat162 h = *reinterpret_cast<__nv_bfloat162*>(&gz[q]);
+                            py[q] = pack2(acc[2 * q] * gelu_d(__low2float(h)), acc[2 * q + 1] * gelu_d(__high2float(h)));
+                        }
+                    } else {
+#pragma unroll
+                        for (int q = 0; q < 16; ++q) {
+                            const int c0 = 2 * q, c1 = 2 * q + 1;
+                            const float z0 = c0 < a.cout ? acc[c0] + a.bias[c0] : 0.f;
+                            const float z1 = c1 < a.cout ? acc[c1] + a.bias[c1] : 0.f;
+                            pz[q] = pack2(z0, z1);
+                            py[q] = pack2(gelu(z0), gelu(z1));
+                        }
+                    }
+                    uint4* y4 = reinterpret_cast<uint4*>(a.y + cell * NET_PITCH);
+#pragma unroll
+                    for (int q = 0; q < 4; ++q) y4[q] = make_uint4(py[4 * q], py[4 * q + 1], py[4 * q + 2], py[4 * q + 3]);
+                    if (MODE == MODE_HIDDEN && a.z) {
+                        uint4* z4 = reinterpret_cast<uint4*>(a.z + cell * NET_PITCH);
+#pragma unroll
+                        for (int q = 0; q < 4; ++q)
+                            z4[q] = make_uint4(pz[4 * q], pz[4 * q + 1], pz[4 * q + 2], pz[4 * q + 3]);
+                    }
                 }
             }
+            tc::fence_before_sync();
+            __syncthreads();
         }
-        tc::fence_before_sync();
-        __syncthreads();
     }
+    cp_async_wait_all();
     if (!ok) {
         if (tid == 0) atomicExch(a.err, 1);
         // MMAs still in flight read this CTA's shared memory and write its TMEM: let them finish
-        if (use0) tc::mbar_wait(&mbar[0], (use0 - 1) & 1u, WAIT_LIMIT);
-        if (use1) tc::mbar_wait(&mbar[1], (use1 - 1) & 1u, WAIT_LIMIT);
+        for (int b = 0; b < S::NBUF; ++b)
+            if (cnt[b]) tc::mbar_wait(&mbar[b], (cnt[b] - 1) & 1u, WAIT_LIMIT);
     }
     tc::fence_before_sync();
     __syncthreads();
@@ -176,9 +216,8 @@ __global__ void __launch_bounds__(128) k_conv(ConvArgs a) {
 
 // ------------------------------------------------------------------ weight gradient
 struct DwArgs {
-    const __nv_bfloat16* x;    // layer input planes [cin][E]
-    const __nv_bfloat16* dy;   // gradient w.r.t. the layer output [cout][E]
-    const __nv_bfloat16* z;    // pre-activation of a hidden layer (the gradient is gated by gelu'(z)), or null
+    const __nv_bfloat16* x;    // layer input activations, channels-last with pitch CINP
+    const __nv_bfloat16* dy;   // gradient w.r.t. the layer's pre-activation, channels-last pitch 32
     float* partial;            // [gridDim.x][NG][128][COUTP]
     long long E, c0, c1;
     int P, Q, cin, cout;
@@ -239,36 +278,29 @@ __global__ void __launch_bounds__(128) k_conv_dw(DwArgs a) {
                 const int t = g * S::G + tid / CINP;
                 uint32_t pk[8];
                 const bool live = t < 27 && ci < a.cin;
-                const long long base = (long long)ci * a.E + cell0 + (live ? tap_off(t, a.P, a.Q) : 0);
+                const long long c0 = cell0 + (live ? tap_off(t, a.P, a.Q) : 0);
 #pragma unroll
                 for (int k = 0; k < 16; k += 2) {
-                    const long long c = cell0 + k + (live ? tap_off(t, a.P, a.Q) : 0);
-                    uint32_t lo = (live && c >= 0 && c < a.E) ? xs[base + k] : 0u;
-                    uint32_t hi = (live && c + 1 >= 0 && c + 1 < a.E) ? xs[base + k + 1] : 0u;
+                    const long long c = c0 + k;
+                    uint32_t lo = (live && c >= 0 && c < a.E) ? xs[c * CINP + ci] : 0u;
+                    uint32_t hi = (live && c + 1 >= 0 && c + 1 < a.E) ? xs[(c + 1) * CINP + ci] : 0u;
                     pk[k / 2] = lo | (hi << 16);
                 }
                 unsigned char* dA = st + g * S::AB;
                 *reinterpret_cast<uint4*>(dA + tc::kmajor_off(tid, 0, 16)) = make_uint4(pk[0], pk[1], pk[2], pk[3]);
                 *reinterpret_cast<uint4*>(dA + tc::kmajor_off(tid, 8, 16)) = make_uint4(pk[4], pk[5], pk[6], pk[7]);
             }
-            // B: row n = output channel, 16 cells of the (gated) output gradient
+            // B: row n = output channel, 16 cells of the gradient w.r.t. the pre-activation
             if (tid < COUTP * 2) {
                 const int n = tid >> 1, h = tid & 1;
+                const unsigned short* dys = reinterpret_cast<const unsigned short*>(a.dy);
                 uint32_t pk[4];
 #pragma unroll
                 for (int k = 0; k < 8; k += 2) {
-                    float f[2];
-#pragma unroll
-                    for (int q = 0; q < 2; ++q) {
-                        const long long c = cell0 + h * 8 + k + q;
-                        f[q] = 0.f;
-                        if (n < a.cout && c < a.c1) {
-                            const long long o = (long long)n * a.E + c;
-                            f[q] = bf2f(a.dy[o]);
-                            if (a.z) f[q] *= gelu_d(bf2f(a.z[o]));
-                        }
-                    }
-                    pk[k / 2] = pack2(f[0], f[1]);
+                    const long long c = cell0 + h * 8 + k;
+                    uint32_t lo = (n < a.cout && c < a.c1) ? dys[c * NET_PITCH + n] : 0u;
+                    uint32_t hi = (n < a.cout && c + 1 < a.c1) ? dys[(c + 1) * NET_PITCH + n] : 0u;
+                    pk[k / 2] = lo | (hi << 16);
                 }
                 *reinterpret_cast<uint4*>(st + S::NG * S::AB + tc::kmajor_off(n, h * 8, 16)) =
                     make_uint4(pk[0], pk[1], pk[2], pk[3]);
@@ -329,19 +361,15 @@ __global__ void k_dw_reduce(const float* partial, int nblk, float* gW, int cin, 
     gW[id] = (float)s;
 }
 
-// bias gradient: per-block partial sums of the (gated) output gradient over the cell range, then a fixed-order sum
-__global__ void k_bias_partial(const __nv_bfloat16* dy, const __nv_bfloat16* z, long long E, long long c0,
-                               long long c1, int cout, float* part) {
+// bias gradient: per-block partial sums of the gradient w.r.t. the pre-activation over the cell range, then
+// a fixed-order sum
+__global__ void k_bias_partial(const __nv_bfloat16* dy, long long c0, long long c1, int cout, float* part) {
     __shared__ float red[256];
     for (int co = 0; co < cout; ++co) {
         float s = 0.f;
         for (long long c = c0 + blockIdx.x * (long long)blockDim.x + threadIdx.x; c < c1;
-             c += (long long)gridDim.x * blockDim.x) {
-            const long long o = (long long)co * E + c;
-            float v = bf2f(dy[o]);
-            if (z) v *= gelu_d(bf2f(z[o]));
-            s += v;
-        }
+             c += (long long)gridDim.x * blockDim.x)
+            s += bf2f(dy[c * NET_PITCH + co]);
         red[threadIdx.x] = s;
         __syncthreads();
         for (int w = blockDim.x / 2; w > 0; w >>= 1) {
@@ -403,24 +431,24 @@ int sm_count() {
     return g_sms;
 }
 
-template <int CINP, int COUTP, int MODE>
+template <int CINP, int MODE>
 void launch_conv(const ConvArgs& a, cudaStream_t st) {
-    using S = ConvSmem<CINP, COUTP>;
+    using S = ConvShape<CINP>;
     long long ntiles = (a.c1 - a.c0 + 127) / 128;
-    long long grid = sm_count() * 3;
+    long long grid = sm_count() * (CINP == 16 ? 8 : 4);
     if (grid > ntiles) grid = ntiles;
     if (grid < 1) grid = 1;
-    k_conv<CINP, COUTP, MODE><<<(unsigned)grid, 128, S::BYTES, st>>>(a);
+    k_conv<CINP, MODE><<<(unsigned)grid, 128, S::BYTES, st>>>(a);
 }
 
 }  // namespace
 
 // shared-memory limits of every kernel instance (set once, outside any stream capture)
 int net_init() {
-    set_smem(k_conv<16, 32, MODE_HIDDEN>, ConvSmem<16, 32>::BYTES);
-    set_smem(k_conv<32, 32, MODE_HIDDEN>, ConvSmem<32, 32>::BYTES);
-    set_smem(k_conv<32, 32, MODE_OUT>, ConvSmem<32, 32>::BYTES);
-    set_smem(k_conv<32, 32, MODE_BWD>, ConvSmem<32, 32>::BYTES);
+    set_smem(k_conv<16, MODE_HIDDEN>, ConvShape<16>::BYTES);
+    set_smem(k_conv<32, MODE_HIDDEN>, ConvShape<32>::BYTES);
+    set_smem(k_conv<32, MODE_OUT>, ConvShape<32>::BYTES);
+    set_smem(k_conv<32, MODE_BWD>, ConvShape<32>::BYTES);
     set_smem(k_conv_dw<16, 32>, DwShape<16, 32>::BYTES);
     set_smem(k_conv_dw<32, 32>, DwShape<32, 32>::BYTES);
     sm_count();
@@ -457,16 +485,16 @@ int net_forward(const NetBox& b, __nv_bfloat16* const wfwd[NET_LAYERS], const fl
         a.w = wfwd[l];
         a.bias = params + net_param_offset(l) + 27LL * s.cout[l] * s.cin[l];
         a.E = b.E; a.c0 = b.c0; a.c1 = b.c1; a.P = b.P; a.Q = b.Q;
-        a.cin = s.cin[l]; a.cout = s.cout[l];
+        a.cout = s.cout[l];
         a.err = err;
         if (l < NET_LAYERS - 1) {
             a.y = nb.act[l + 1];
             a.z = keepPre ? nb.pre[l] : nullptr;
-            if (l == 0) launch_conv<16, 32, MODE_HIDDEN>(a, st);
-            else launch_conv<32, 32, MODE_HIDDEN>(a, st);
+            if (l == 0) launch_conv<16, MODE_HIDDEN>(a, st);
+            else launch_conv<32, MODE_HIDDEN>(a, st);
         } else {
             a.yf = nb.out;
-            launch_conv<32, 32, MODE_OUT>(a, st);
+            launch_conv<32, MODE_OUT>(a, st);
         }
     }
     return (int)cudaGetLastError();
@@ -480,31 +508,28 @@ static void launch_dw(const DwArgs& a, int nblk, float* gW, cudaStream_t st) {
     k_dw_reduce<CINP, COUTP><<<(n + 255) / 256, 256, 0, st>>>(a.partial, nblk, gW, a.cin, a.cout);
 }
 
-// gradients of every parameter from the output gradient nb.gact[0] (planar bf16, NET_OUT planes), given
-// the activations and pre-activations of the last forward (keepPre)
+// gradients of every parameter from the output gradient nb.grad[3] (channels-last, pitch 32), given the
+// activations and pre-activations of the last forward (keepPre)
 int net_backward(const NetBox& b, __nv_bfloat16* const wbwd[NET_LAYERS], NetBuffers& nb, float* grads, int* err,
                  cudaStream_t st) {
     NetShape s = net_shape();
     const int nblk = net_dw_blocks();
     for (int l = NET_LAYERS - 1; l >= 0; --l) {
-        // gradient w.r.t. this layer's output, and the gate (its pre-activation) for hidden layers
-        const __nv_bfloat16* dy = l == NET_LAYERS - 1 ? nb.gact[0] : nb.gact[l + 1];
-        const __nv_bfloat16* z = l == NET_LAYERS - 1 ? nullptr : nb.pre[l];
         DwArgs d{};
-        d.x = nb.act[l]; d.dy = dy; d.z = z; d.partial = nb.partial;
+        d.x = nb.act[l]; d.dy = nb.grad[l]; d.partial = nb.partial;
         d.E = b.E; d.c0 = b.c0; d.c1 = b.c1; d.P = b.P; d.Q = b.Q; d.cin = s.cin[l]; d.cout = s.cout[l]; d.err = err;
         float* gW = grads + net_param_offset(l);
         if (l == 0) launch_dw<16, 32>(d, nblk, gW, st);
         else launch_dw<32, 32>(d, nblk, gW, st);
-        k_bias_partial<<<nblk, 256, 0, st>>>(dy, z, b.E, b.c0, b.c1, s.cout[l], nb.partial);
+        k_bias_partial<<<nblk, 256, 0, st>>>(nb.grad[l], b.c0, b.c1, s.cout[l], nb.partial);
         k_bias_reduce<<<1, 32, 0, st>>>(nb.partial, nblk, s.cout[l], gW + 27LL * s.cout[l] * s.cin[l]);
-        if (l > 0) {   // gradient w.r.t. this layer's input (the previous layer's GELU output)
+        if (l > 0) {   // gradient w.r.t. the previous layer's pre-activation: through this layer, then GELU'
             ConvArgs a{};
-            a.x = dy; a.gz = z; a.w = wbwd[l];
-            a.y = nb.gact[l];
+            a.x = nb.grad[l]; a.gz = nb.pre[l - 1]; a.w = wbwd[l];
+            a.y = nb.grad[l - 1];
             a.E = b.E; a.c0 = b.c0; a.c1 = b.c1; a.P = b.P; a.Q = b.Q;
-            a.cin = s.cout[l]; a.cout = s.cin[l]; a.err = err;
-            launch_conv<32, 32, MODE_BWD>(a, st);
+            a.cout = s.cin[l]; a.err = err;
+            launch_conv<32, MODE_BWD>(a, st);
         }
     }
     return (int)cudaGetLastError();

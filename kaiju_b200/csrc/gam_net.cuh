@@ -1,16 +1,19 @@
 // The learned flux closure's network on the device: a 3D convolution net over the solver's cell box
-// (the pencil index space of gam_common.cuh, ghosts included), activations as planar BF16 planes
-// ([channel][cell], one plane per channel like the solver's fields), FP32 master weights.
+// (the pencil index space of gam_common.cuh, ghosts included), activations channels-last in BF16
+// (cell-major, 16 or 32 channels per cell, so the channels of one cell are one to four 16-byte chunks),
+// FP32 master weights.
 //
-//   input 8 (normalised primitives rho, v, P, B) -> 32 -> 32 -> 32 -> 24 (8 face-flux corrections per
-//   direction: the 5 gas fluxes and the 3 magnetic-stress momentum fluxes of each cell's lower face),
-//   3x3x3 kernels, GELU between layers.
+//   input 8 (normalised primitives rho, v, P, B; padded to 16) -> 32 -> 32 -> 32 -> 24 (8 face-flux
+//   corrections per direction: the 5 gas fluxes and the 3 magnetic-stress momentum fluxes of each cell's
+//   lower face), 3x3x3 kernels, GELU between layers.
 //
 // Every convolution is an implicit GEMM on the tensor cores (tcgen05.mma kind::f16, BF16 x BF16 -> FP32
-// in TMEM): a CTA owns 128 consecutive cells (M = 128) and all output channels (N = 32); for each of the
-// 27 taps the cells' shifted input channels are staged in shared memory as the A operand (K = input
-// channels) against that tap's weights (B), double-buffered so the staging of tap t+1 overlaps the MMAs
-// of tap t. The weight gradient contracts over cells instead (M = 128 rows of (tap, input channel),
+// in TMEM): a CTA owns 128 consecutive cells (M = 128) and all output channels (N = 32). For each of the
+// 9 (dj, dk) offsets it copies (cp.async, 16-byte chunks) a window of 130 cells x input channels into
+// shared memory, one block of rows per channel chunk with the rows 16 bytes apart, so the A operand of
+// the three taps di = -1, 0, +1 is the same window read from row 0, 1 or 2 (a 16-byte shift of the
+// descriptor's start address). Windows are triple-buffered: the copy of window w+2 overlaps the MMAs of
+// window w. The weight gradient contracts over cells instead (M = 128 rows of (tap, input channel),
 // N = output channels, K = 16 cells per MMA), each CTA accumulating all taps in TMEM over its cells and
 // writing one partial that a fixed-order reduction sums.
 #pragma once
@@ -52,12 +55,14 @@ struct NetBox {
     long long c0, c1;  // GEMM cell range: every tap of every cell in it stays inside [0, E)
 };
 
+constexpr int NET_IN_PITCH = 16;     // channels per cell of the input activations (8 used)
+constexpr int NET_PITCH = 32;        // channels per cell of every other activation and gradient
+
 struct NetBuffers {
-    // activations and pre-activations of the hidden layers (planar bf16), the output (planar fp32)
-    __nv_bfloat16* act[NET_LAYERS];     // act[0] = input (NET_IN planes); act[l] = GELU output of layer l-1
-    __nv_bfloat16* pre[NET_LAYERS];     // pre-activation of layer l (l < NET_LAYERS - 1)
-    float* out;                         // NET_OUT planes
-    __nv_bfloat16* gact[NET_LAYERS];    // gradient w.r.t. act[l] (l >= 1), and gout for the output (index 0)
+    __nv_bfloat16* act[NET_LAYERS];     // act[0] = input (pitch 16); act[l] = GELU output of layer l-1 (pitch 32)
+    __nv_bfloat16* pre[NET_LAYERS];     // pre-activation of layer l (l < NET_LAYERS - 1), pitch 32
+    float* out;                         // the output layer, planar fp32: NET_OUT planes
+    __nv_bfloat16* grad[NET_LAYERS];    // gradient w.r.t. layer l's pre-activation (grad[3]: the output), pitch 32
     float* partial;                     // weight-gradient partials
     long long partialFloats;
 };
