@@ -1,0 +1,74 @@
+"""Long runs of the spherical configuration on the device: the LFM-type grid with ring averaging about the
+axis, the axis boundaries, Boris and a dipole background (the magnetosphere-like set-up; its solar-wind
+and ionosphere boundaries are not built, so the reference's LFM blast wave supplies the flow), run with
+the plain FP64 path and the FP32-flux path side by side.
+
+    python -m kaiju_b200.runs spherical --n 96 96 128 --steps 2000
+"""
+from __future__ import annotations
+
+import argparse
+import json
+
+import numpy as np
+
+from . import gamera as gm
+
+
+def spherical_model(Nip: int, Njp: int, Nkp: int) -> gm.Model:
+    """The reference's LFM blast-wave deck (tests/gamera/lfmbw.xml: 7UP, pdmb 1, Boris Ca 10, floors 1e-4 /
+    1e-6, fixed-gas shells, predictor fix, dt over the active cells) with a dipole background."""
+    return gm.Model(Nip, Njp, Nkp, CFL=0.3, pdmb=1.0, rmeth="7UP", dFloor=1e-4, pFloor=1e-6, doBoris=True,
+                    Ca=10.0, tFin=1.0e30, bc=(gm.GAM_BC_LFMBW, gm.GAM_BC_LFMBW, gm.GAM_BC_LFMPOLE,
+                                               gm.GAM_BC_LFMPOLE, gm.GAM_BC_PERIODIC, gm.GAM_BC_PERIODIC),
+                    ring=dict(recon="PPM"), predFixLFM=True, bwD0=1.0, bwP0=0.1, dtActive=True,
+                    doBackground=True)
+
+
+def spherical(n=(96, 96, 128), steps=2000, dipole=2000.0, grid=(10.0, 100.0, 1.03, 0.05)):
+    """The FP64 path for `steps` steps (device-timed), then the FP32-flux path from the same start to the
+    same end time (CalcDT's tFin clamp lands it there), and the L1 difference of the two states."""
+    import dataclasses
+    model = spherical_model(*n)
+    xyz = gm.corners_lfm(model, *grid)
+    out = {"cells": list(n), "steps": steps, "dipole_moment": dipole, "grid_r_theta0": list(grid)}
+    cells = n[0] * n[1] * n[2]
+    g64 = gm.GameraGPU.from_corners(model, xyz, "LFMBW", b0=("dipole", dipole))
+    ms, rc = g64.run_steps_timed(steps)
+    t_end = g64.status()["t"]
+    out["fp64"] = {"ms_per_step": ms / steps, "zone_updates_per_s": cells * steps / (ms / 1e3), "status": rc,
+                   "t_end": t_end}
+    m32 = dataclasses.replace(model, tFin=t_end)
+    g32 = gm.GameraGPU.from_corners(m32, xyz, "LFMBW", b0=("dipole", dipole))
+    g32.set_precision(gm.GAM_FP32FLUX)
+    ms32, done = 0.0, 0
+    while g32.status()["t"] < t_end * (1.0 - 1e-14):
+        chunk = 100
+        m, rc32 = g32.run_steps_timed(chunk)
+        ms32 += m
+        done += chunk
+    # the last chunk may have stepped past the clamp at dt = tFin - t (TINY steps); count only real steps
+    st32 = g32.status()
+    out["fp32flux"] = {"ms_per_step": ms32 / done, "zone_updates_per_s": cells * done / (ms32 / 1e3),
+                       "steps_to_t_end": int(st32["ts"]), "t": st32["t"], "status": rc32}
+    a, b = g64.fetch("gas")[4:-4, 4:-4, 4:-4], g32.fetch("gas")[4:-4, 4:-4, 4:-4]
+    l1 = [float(np.mean(np.abs(a[..., v] - b[..., v])) / np.mean(np.abs(a[..., v]))) for v in range(5)]
+    out["fp32flux"]["l1_rel_vs_fp64_per_var"] = l1
+    out["fp32flux"]["speedup_vs_fp64_per_step"] = out["fp64"]["ms_per_step"] / out["fp32flux"]["ms_per_step"]
+    out["divb"] = {"fp64": g64.divb(), "fp32flux": g32.divb()}
+    g64.close()
+    g32.close()
+    return out
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser()
+    ap.add_argument("run", choices=["spherical"])
+    ap.add_argument("--n", type=int, nargs=3, default=[96, 96, 128])
+    ap.add_argument("--steps", type=int, default=2000)
+    a = ap.parse_args(argv)
+    print(json.dumps(spherical(tuple(a.n), a.steps), indent=1))
+
+
+if __name__ == "__main__":
+    main()

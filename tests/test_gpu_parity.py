@@ -38,6 +38,9 @@ CASES = [
     # LFM-type spherical grid with ring averaging about the axis, the axis BCs and the LFM blast wave's
     # fixed shells and predictor fix (the reference's lfmbw test problem)
     ("lfmbw", "lfmbw", (32, 24, 64), {}),
+    # the spherical configuration's physics together: LFM grid, rings, axis BCs, Boris, and a dipole
+    # background centred on the grid's axis (the magnetosphere-like set-up without its wind/ionosphere BCs)
+    ("lfmbw_dipole", "lfmbw", (32, 24, 64), dict(b0=("dipole", 2000.0))),
 ]
 
 
@@ -241,3 +244,20 @@ def test_device_lfm_grid_matches_oracle(gpu_lib, oracle_lib):
         o.step(2)
         g.run_steps(2)
         _cmp(o, g, ["gas", "magflux"], tol=1e-9, where="after 2 steps ")
+
+
+def test_lfm_dipole_fp32_flux_l1(gpu_lib, oracle_lib):
+    """FP32-flux path on the spherical set-up (LFM grid, rings, Boris, dipole background): L1 error of the
+    state after re-synchronised steps within the FP32 path's 1e-5 bound."""
+    from kaiju_b200 import gamera as gm
+    o, g = oracle_and_gpu("lfmbw", (32, 24, 64), b0=("dipole", 2000.0))
+    with g:
+        g.set_precision(gm.GAM_FP32FLUX)
+        for s in range(3):
+            o.step()
+            g.step()
+            a, b = g.fetch("gas"), o.get("gas")
+            for v in range(5):
+                l1 = np.abs(a[..., v] - b[..., v]).mean() / np.abs(b[..., v]).mean()
+                assert l1 <= 1e-5, (s, v, l1)
+            resync(o, g)
