@@ -234,6 +234,13 @@ int gam_gpu_ensemble_run_steps_timed(gam_ensemble_t* e, int nsteps, double* ms);
  * gives once t reaches the member's tFin) or maxSteps batch steps; *steps = batch steps taken */
 int gam_gpu_ensemble_advance(gam_ensemble_t* e, double tEnd, int chunk, int maxSteps, int* steps);
 void gam_gpu_ensemble_destroy(gam_ensemble_t* e);   /* the members are not destroyed */
+/* Tile shapes. GAM_TILE_FLUX_ROWS: rows of interfaces per flux-kernel CTA, 8 (default) or 4; results do
+ * not depend on it. The ensemble autotuner times whole batch steps for each member shape (largest first)
+ * with each height and keeps the fastest (the timed steps are ordinary steps of the run); fluxRows
+ * (optional, one per member) receives the choice. */
+#define GAM_TILE_FLUX_ROWS 1
+int gam_gpu_set_tile(gam_gpu_t* h, int what, int value);
+int gam_gpu_ensemble_autotune(gam_ensemble_t* e, int steps, int* fluxRows);
 
 /* DivB for callers that cannot allocate device memory (no counterpart in the reference).
  * Some hosts cannot call cudaMalloc: device arrays owned by another runtime (OpenACC or CUDA Fortran

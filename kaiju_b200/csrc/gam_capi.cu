@@ -1,4 +1,5 @@
 // C ABI (include/gamgpu.h): handle lifetime, Fortran-layout mirroring, step / advance entry points.
+#include <algorithm>
 #include <cstdio>
 #include <cstring>
 #include <vector>
@@ -573,6 +574,17 @@ int gam_gpu_profile_phases(gam_gpu_t* G, int nsteps, double* ms, int nphase) {
     return status_code(G->h.hScal->sticky);
 }
 
+int gam_gpu_set_tile(gam_gpu_t* G, int what, int value) {
+    if (!G) return GAM_ERR_ARG;
+    Handle& h = G->h;
+    if (what != GAM_TILE_FLUX_ROWS || (value != 4 && value != 8)) return GAM_ERR_ARG;
+    if (h.fluxRows != value) {
+        h.fluxRows = value;
+        destroy_graphs(h);
+    }
+    return GAM_OK;
+}
+
 int gam_gpu_set_closure(gam_gpu_t* G, gam_closure_t* c) {
     if (!G) return GAM_ERR_ARG;
     Handle& h = G->h;
@@ -892,6 +904,61 @@ int gam_gpu_ensemble_advance(gam_ensemble_t* E, double tEnd, int chunk, int maxS
     for (size_t m = 0; m < E->members.size(); ++m) E->active[m] = 1;   // later runs step every member again
     ens_destroy_graphs(E);
     return rc ? rc : st;
+}
+
+// Autotuner: members grouped by grid shape; for each group, largest first, every flux tile height is timed
+// over `steps` batch steps with the other groups fixed, and the fastest kept. The tile height does not
+// change any result (each interface is computed from the same staged values), so the steps it takes are
+// ordinary steps of the run.
+int gam_gpu_ensemble_autotune(gam_ensemble_t* E, int steps, int* fluxRows) {
+    if (!E || steps < 1) return GAM_ERR_ARG;
+    const size_t n = E->members.size();
+    std::vector<long long> key(n);
+    std::vector<long long> groups;
+    for (size_t m = 0; m < n; ++m) {
+        const Lay& L = E->members[m]->h.L;
+        key[m] = ((long long)L.Nip << 40) | ((long long)L.Njp << 20) | (long long)L.Nkp;
+        bool seen = false;
+        for (long long g : groups) seen = seen || g == key[m];
+        if (!seen) groups.push_back(key[m]);
+    }
+    auto cells = [](long long k) { return (k >> 40) * ((k >> 20) & 0xFFFFF) * (k & 0xFFFFF); };
+    std::sort(groups.begin(), groups.end(), [&](long long a, long long b) { return cells(a) > cells(b); });
+    cudaEvent_t e0, e1;
+    CK(cudaEventCreate(&e0));
+    CK(cudaEventCreate(&e1));
+    for (long long g : groups) {
+        int best = 8;
+        float bestMs = 0.f;
+        const int cand[2] = {8, 4};
+        for (int c : cand) {
+            for (size_t m = 0; m < n; ++m)
+                if (key[m] == g) gam_gpu_set_tile(E->members[m], GAM_TILE_FLUX_ROWS, c);
+            int rc = ens_build(E);
+            if (rc) { cudaEventDestroy(e0); cudaEventDestroy(e1); return rc; }
+            rc = ens_launch(E);   // untimed: first launch of the new graphs
+            if (rc) { cudaEventDestroy(e0); cudaEventDestroy(e1); return rc; }
+            CK(cudaEventRecord(e0, E->root));
+            for (int s = 0; s < steps; ++s) {
+                rc = ens_launch(E);
+                if (rc) { cudaEventDestroy(e0); cudaEventDestroy(e1); return rc; }
+            }
+            CK(cudaEventRecord(e1, E->root));
+            CK(cudaEventSynchronize(e1));
+            float ms = 0.f;
+            CK(cudaEventElapsedTime(&ms, e0, e1));
+            if (c == cand[0] || ms < bestMs) { best = c; bestMs = ms; }
+        }
+        for (size_t m = 0; m < n; ++m)
+            if (key[m] == g) gam_gpu_set_tile(E->members[m], GAM_TILE_FLUX_ROWS, best);
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    int rc = ens_build(E);
+    if (rc) return rc;
+    if (fluxRows)
+        for (size_t m = 0; m < n; ++m) fluxRows[m] = E->members[m]->h.fluxRows;
+    return ens_collect(E);
 }
 
 void gam_gpu_ensemble_destroy(gam_ensemble_t* E) {

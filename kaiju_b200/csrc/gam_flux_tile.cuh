@@ -23,18 +23,21 @@
 namespace gam {
 
 constexpr int FL = 32;   // interfaces per tile along i
-constexpr int FR = 8;    // rows per tile
+// FR: rows per tile (one warp per row), 8 by default; 4 gives twice the CTAs, which the ensemble
+// autotuner picks for members too small to fill the GPU
 
-template <int D> __host__ __device__ constexpr int rec_box() { return D == 0 ? (FL + 8) * FR : FL * (FR + 7); }
-template <int D> __host__ __device__ constexpr int lim_box() { return D == 0 ? (FL + 4) * FR : FL * (FR + 3); }
-template <typename S, int D> constexpr size_t flux_smem() { return sizeof(S) * (9 * rec_box<D>() + 8 * lim_box<D>()); }
+template <int D, int FR> __host__ __device__ constexpr int rec_box() { return D == 0 ? (FL + 8) * FR : FL * (FR + 7); }
+template <int D, int FR> __host__ __device__ constexpr int lim_box() { return D == 0 ? (FL + 4) * FR : FL * (FR + 3); }
+template <typename S, int D, int FR> constexpr size_t flux_smem() {
+    return sizeof(S) * (9 * rec_box<D, FR>() + 8 * lim_box<D, FR>());
+}
 
-template <typename T, typename S, int D, bool MHD, bool BG>
-__global__ void __launch_bounds__(256, 2) k_flux_tile(Lay L, Par p, FluxSrc<S> in, StateP h, FluxOut<S> F, Reg r) {
+template <typename T, typename S, int D, bool MHD, bool BG, int FR>
+__global__ void __launch_bounds__(32 * FR, 16 / FR) k_flux_tile(Lay L, Par p, FluxSrc<S> in, StateP h, FluxOut<S> F, Reg r) {
     extern __shared__ __align__(16) unsigned char smraw[];
     S* sRec = reinterpret_cast<S*>(smraw);   // staged in the storage type, converted to T on use
-    S* sLim = sRec + 9 * rec_box<D>();
-    constexpr int RB = rec_box<D>(), LB = lim_box<D>();
+    constexpr int RB = rec_box<D, FR>(), LB = lim_box<D, FR>();
+    S* sLim = sRec + 9 * RB;
     const int tid = threadIdx.x, lane = tid & 31, row = tid >> 5;
     const int i0 = r.i0 + blockIdx.x * FL;
     int i = i0 + lane, j, k, a0;
@@ -44,14 +47,14 @@ __global__ void __launch_bounds__(256, 2) k_flux_tile(Lay L, Par p, FluxSrc<S> i
     // ---- stage the stencil footprint (rows of 32..40 doubles, one warp per row)
     const int warp = tid >> 5;
     auto stage_rec = [&](S* dst, const S* src) {
-        if (D == 0) stage_rows<S>(dst, src, L, i0 - 4, FL + 8, a0, FR, k, 1, warp, 8, lane);
-        else if (D == 1) stage_rows<S>(dst, src, L, i0, FL, a0 - 4, FR + 7, k, 1, warp, 8, lane);
-        else stage_rows<S>(dst, src, L, i0, FL, j, 1, a0 - 4, FR + 7, warp, 8, lane);
+        if (D == 0) stage_rows<S>(dst, src, L, i0 - 4, FL + 8, a0, FR, k, 1, warp, FR, lane);
+        else if (D == 1) stage_rows<S>(dst, src, L, i0, FL, a0 - 4, FR + 7, k, 1, warp, FR, lane);
+        else stage_rows<S>(dst, src, L, i0, FL, j, 1, a0 - 4, FR + 7, warp, FR, lane);
     };
     auto stage_lim = [&](S* dst, const S* src) {
-        if (D == 0) stage_rows<S>(dst, src, L, i0 - 2, FL + 4, a0, FR, k, 1, warp, 8, lane);
-        else if (D == 1) stage_rows<S>(dst, src, L, i0, FL, a0 - 2, FR + 3, k, 1, warp, 8, lane);
-        else stage_rows<S>(dst, src, L, i0, FL, j, 1, a0 - 2, FR + 3, warp, 8, lane);
+        if (D == 0) stage_rows<S>(dst, src, L, i0 - 2, FL + 4, a0, FR, k, 1, warp, FR, lane);
+        else if (D == 1) stage_rows<S>(dst, src, L, i0, FL, a0 - 2, FR + 3, k, 1, warp, FR, lane);
+        else stage_rows<S>(dst, src, L, i0, FL, j, 1, a0 - 2, FR + 3, warp, FR, lane);
     };
 #pragma unroll
     for (int q = 0; q < 5; ++q) stage_rec(sRec + q * RB, in.W[q]);
@@ -155,9 +158,21 @@ __global__ void __launch_bounds__(256, 2) k_flux_tile(Lay L, Par p, FluxSrc<S> i
     for (int v = 0; v < 5; ++v) F.g[v][c] = S(faB * double(gF[v]));
 }
 
+template <typename T, typename S, int D, int FR>
+static void launch_flux_rows(Handle& h, const FluxSrc<S>& in, const FluxOut<S>& F, const Reg& r, cudaStream_t st) {
+    const Par& p = h.p;
+    dim3 grid((unsigned)((r.ni + FL - 1) / FL), 0, 0);
+    if (D == 2) { grid.y = (unsigned)((r.nk + FR - 1) / FR); grid.z = (unsigned)r.nj; }
+    else { grid.y = (unsigned)((r.nj + FR - 1) / FR); grid.z = (unsigned)r.nk; }
+    const size_t sm = flux_smem<S, D, FR>();
+    if (p.doMHD && p.doBackground)
+        k_flux_tile<T, S, D, true, true, FR><<<grid, 32 * FR, sm, st>>>(h.L, p, in, h.H, F, r);
+    else if (p.doMHD) k_flux_tile<T, S, D, true, false, FR><<<grid, 32 * FR, sm, st>>>(h.L, p, in, h.H, F, r);
+    else k_flux_tile<T, S, D, false, false, FR><<<grid, 32 * FR, sm, st>>>(h.L, p, in, h.H, F, r);
+}
+
 template <typename T, typename S, int D>
 static void launch_flux_dir(Handle& h, const FluxSrc<S>& in, const Reg& r, cudaStream_t st) {
-    const Par& p = h.p;
     FluxOut<S> F;
     if constexpr (std::is_same<S, double>::value) {
         for (int v = 0; v < 5; ++v) F.g[v] = h.gflx[D][v];
@@ -166,24 +181,24 @@ static void launch_flux_dir(Handle& h, const FluxSrc<S>& in, const Reg& r, cudaS
         for (int v = 0; v < 5; ++v) F.g[v] = h.f32.gflx[D][v];
         for (int x = 0; x < 3; ++x) F.m[x] = h.f32.mflx[D][x];
     }
-    dim3 grid((unsigned)((r.ni + FL - 1) / FL), 0, 0);
-    if (D == 2) { grid.y = (unsigned)((r.nk + FR - 1) / FR); grid.z = (unsigned)r.nj; }
-    else { grid.y = (unsigned)((r.nj + FR - 1) / FR); grid.z = (unsigned)r.nk; }
-    if (p.doMHD && p.doBackground)
-        k_flux_tile<T, S, D, true, true><<<grid, 256, flux_smem<S, D>(), st>>>(h.L, p, in, h.H, F, r);
-    else if (p.doMHD) k_flux_tile<T, S, D, true, false><<<grid, 256, flux_smem<S, D>(), st>>>(h.L, p, in, h.H, F, r);
-    else k_flux_tile<T, S, D, false, false><<<grid, 256, flux_smem<S, D>(), st>>>(h.L, p, in, h.H, F, r);
+    if (h.fluxRows == 4) launch_flux_rows<T, S, D, 4>(h, in, F, r, st);
+    else launch_flux_rows<T, S, D, 8>(h, in, F, r, st);
     h.launches++;
 }
 
+template <typename T, typename S, int D, int FR>
+static void set_flux_smem_rows() {
+    cudaFuncSetAttribute(k_flux_tile<T, S, D, true, true, FR>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)flux_smem<S, D, FR>());
+    cudaFuncSetAttribute(k_flux_tile<T, S, D, true, false, FR>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)flux_smem<S, D, FR>());
+    cudaFuncSetAttribute(k_flux_tile<T, S, D, false, false, FR>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)flux_smem<S, D, FR>());
+}
 template <typename T, typename S, int D>
 static void set_flux_smem() {
-    cudaFuncSetAttribute(k_flux_tile<T, S, D, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         (int)flux_smem<S, D>());
-    cudaFuncSetAttribute(k_flux_tile<T, S, D, true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         (int)flux_smem<S, D>());
-    cudaFuncSetAttribute(k_flux_tile<T, S, D, false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         (int)flux_smem<S, D>());
+    set_flux_smem_rows<T, S, D, 4>();
+    set_flux_smem_rows<T, S, D, 8>();
 }
 // CalcStress flux loop (stress.F90:84-128): I, J and (unless 2.5D) K interfaces
 template <typename T, typename S>

@@ -49,8 +49,9 @@ struct ConvShape {
     static constexpr int WIN = KCH * LBO;
     static constexpr int TAPB = COUTP * CINP * 2;      // one tap's packed weights
     static constexpr int STAGE = (WIN + 3 * TAPB + 127) / 128 * 128;   // a window and its three taps' weights
-    static constexpr int NBUF = 3;
-    static constexpr int BYTES = NBUF * STAGE + 1024;
+    static constexpr int NS = 4;                       // stages in the ring
+    static constexpr int BYTES = NS * STAGE + 1024;
+    static constexpr int THREADS = 160;                // 4 worker warps (copies, epilogue) + 1 MMA warp
 };
 
 __device__ __forceinline__ unsigned char* align1k(unsigned char* p) {
@@ -65,153 +66,169 @@ __device__ __forceinline__ void cp_async16(void* dst, const void* src, uint32_t 
 __device__ __forceinline__ void cp_async16_ca(void* dst, const void* src) {
     asm volatile("cp.async.ca.shared.global [%0], [%1], 16;" :: "r"(tc::smem_u32(dst)), "l"(src) : "memory");
 }
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
-template <int N>
-__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" :: "n"(N) : "memory"); }
+// arrive on the mbarrier once every cp.async this thread issued so far has landed
+__device__ __forceinline__ void cp_async_arrive(uint64_t* mbar) {
+    asm volatile("cp.async.mbarrier.arrive.noinc.shared::cta.b64 [%0];" :: "r"(tc::smem_u32(mbar)) : "memory");
+}
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+__device__ __forceinline__ void mbar_arrive(uint64_t* mbar) {
+    asm volatile("{\n\t.reg .b64 st;\n\tmbarrier.arrive.shared::cta.b64 st, [%0];\n\t}" :: "r"(tc::smem_u32(mbar))
+                 : "memory");
+}
 
-// out[cell][n] = sum over taps t and input channels c of in[cell + off(t)][c] * W_t[n][c], 128 cells per tile
+// out[cell][n] = sum over taps t and input channels c of in[cell + off(t)][c] * W_t[n][c], 128 cells per tile.
+// Warps 0-3 copy windows into a ring of NS stages (full[s] completes when the 128 threads' copies of a
+// window have landed) and run the epilogue of each finished tile (warp w reads TMEM lanes 32w..32w+31);
+// one thread of warp 4 issues the MMAs of a window once its stage is full and commits them to empty[s]
+// (the stage may be refilled) and, after a tile's last window, to tfull[a] (accumulator a is ready).
+// Two TMEM accumulators alternate between tiles; tempty[a] completes when the workers have read one.
 template <int CINP, int MODE>
-__global__ void __launch_bounds__(128) k_conv(ConvArgs a) {
+__global__ void __launch_bounds__(160) k_conv(ConvArgs a) {
     using S = ConvShape<CINP>;
     static_assert(CINP % 16 == 0, "K step");
     extern __shared__ unsigned char smraw[];
     unsigned char* sStage = align1k(smraw);
-    __shared__ __align__(8) uint64_t mbar[S::NBUF];
+    __shared__ __align__(8) uint64_t full[S::NS], empty[S::NS], tfull[2], tempty[2];
     __shared__ uint32_t tmemBase;
+    __shared__ int failed;
     const int tid = threadIdx.x, warp = tid >> 5;
 
     if (tid == 0) {
-        for (int b = 0; b < S::NBUF; ++b) tc::mbar_init(&mbar[b], 1);
+        for (int q = 0; q < S::NS; ++q) { tc::mbar_init(&full[q], 128); tc::mbar_init(&empty[q], 1); }
+        for (int q = 0; q < 2; ++q) { tc::mbar_init(&tfull[q], 1); tc::mbar_init(&tempty[q], 128); }
+        failed = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
-    if (warp == 0) tc::tmem_alloc(&tmemBase, 32);
+    if (warp == 0) tc::tmem_alloc(&tmemBase, 64);
     tc::fence_before_sync();
     __syncthreads();
     tc::fence_after_sync();
     const uint32_t tbase = tmemBase;
-    const uint32_t idesc = tc::idesc_bf16_f32(128, S::COUTP);
-    constexpr uint32_t SBO_W = CINP / 8 * 128;
 
     const long long ntiles = (a.c1 - a.c0 + 127) / 128;
     const long long myTiles = ntiles > blockIdx.x ? (ntiles - 1 - blockIdx.x) / gridDim.x + 1 : 0;
-    const long long nwin = myTiles * 9;
-    // copy window `it` (tile it / 9, offset (dj, dk) = it % 9) and the weights of its three taps (consecutive
-    // in the packed array) into stage it % NBUF
-    auto issue = [&](long long it) {
-        if (it < nwin) {
-            const long long tile = blockIdx.x + (it / 9) * (long long)gridDim.x;
-            const int w = (int)(it % 9), dj = w % 3 - 1, dk = w / 3 - 1;
-            const long long base = a.c0 + tile * 128 - 1 + (long long)a.P * (dj + (long long)a.Q * dk);
-            unsigned char* dst = sStage + (int)(it % S::NBUF) * S::STAGE;
-            for (int id = tid; id < S::ROWS * S::KCH; id += 128) {
-                const int row = id / S::KCH, kc = id % S::KCH;
-                const long long cell = base + row;
-                const bool inb = cell >= 0 && cell < a.E;
-                const __nv_bfloat16* src = a.x + (inb ? cell : 0) * CINP + kc * 8;
-                cp_async16(dst + kc * S::LBO + row * 16, src, inb ? 16u : 0u);
-            }
-            const unsigned char* wsrc = reinterpret_cast<const unsigned char*>(a.w) + (3 * (dj + 1) + 9 * (dk + 1)) * S::TAPB;
-            for (int id = tid; id < 3 * S::TAPB / 16; id += 128) cp_async16_ca(dst + S::WIN + id * 16, wsrc + id * 16);
-        }
-        cp_async_commit();
-    };
-    uint32_t cnt[S::NBUF] = {0, 0, 0};
-    int ok = 1;
-    issue(0);
-    issue(1);
-    for (long long it = 0; it < nwin; ++it) {
-        const int b = (int)(it % S::NBUF);
-        // buffer of window it+2 held window it-1: wait for its MMAs before copying over it
-        bool fine = true;
-        {
-            const long long nx = it + 2;
-            const int bn = (int)(nx % S::NBUF);
-            if (nx < nwin && cnt[bn] > 0) fine = tc::mbar_wait(&mbar[bn], (cnt[bn] - 1) & 1u, WAIT_LIMIT);
-            if (fine) issue(nx);
-            else cp_async_commit();
-        }
-        cp_async_wait<2>();
-        tc::fence_smem_async();
-        if (!__syncthreads_and(fine)) { ok = 0; break; }
-        const int w = (int)(it % 9);
-        if (tid == 0) {
+
+    if (warp < 4) {
+        // ---------------- workers: copies and epilogues
+        auto epilogue = [&](long long T) -> bool {
+            const int acc = (int)(T & 1);
+            if (!tc::mbar_wait(&tfull[acc], (uint32_t)((T >> 1) & 1), WAIT_LIMIT)) return false;
             tc::fence_after_sync();
-            const uint32_t win = tc::smem_u32(sStage + b * S::STAGE);
-#pragma unroll
-            for (int di = -1; di <= 1; ++di) {
-#pragma unroll
-                for (int ks = 0; ks < CINP / 16; ++ks) {
-                    const uint64_t ad = tc::desc_kmajor(win + (di + 1) * 16 + ks * 2 * S::LBO, S::LBO, 128);
-                    const uint64_t bd = tc::desc_kmajor(win + S::WIN + (di + 1) * S::TAPB + ks * 256, 128, SBO_W);
-                    tc::mma_bf16(tbase, ad, bd, idesc, !(w == 0 && di == -1 && ks == 0));
-                }
-            }
-            tc::mma_commit(&mbar[b]);
-        }
-        ++cnt[b];
-        if (w == 8) {   // the tile's last window: wait for its MMAs, then the epilogue
-            fine = tc::mbar_wait(&mbar[b], (cnt[b] - 1) & 1u, WAIT_LIMIT);
-            if (!__syncthreads_and(fine)) { ok = 0; break; }
-            tc::fence_after_sync();
-            float acc[32];
-            tc::tmem_ld32(tbase + ((uint32_t)(warp * 32) << 16), acc);
-            const long long cell = a.c0 + (blockIdx.x + (it / 9) * (long long)gridDim.x) * 128 + tid;
-            if (cell < a.c1) {
-                if (MODE == MODE_OUT) {
-#pragma unroll
-                    for (int co = 0; co < 32; ++co)
-                        if (co < a.cout) a.yf[(long long)co * a.E + cell] = acc[co] + a.bias[co];
-                } else {
-                    uint32_t py[16], pz[16];
-                    if (MODE == MODE_BWD) {
-                        const uint4* g4 = reinterpret_cast<const uint4*>(a.gz + cell * NET_PITCH);
-                        uint32_t gz[16];
-#pragma unroll
-                        for (int q = 0; q < 4; ++q) {
-                            uint4 u = g4[q];
-                            gz[4 * q] = u.x; gz[4 * q + 1] = u.y; gz[4 * q + 2] = u.z; gz[4 * q + 3] = u.w;
-                        }
-#pragma unroll
-                        for (int q = 0; q < 16; ++q) {
-                            __nv_bfloat162 h = *reinterpret_cast<__nv_bfloat162*>(&gz[q]);
-                            py[q] = pack2(acc[2 * q] * gelu_d(__low2float(h)), acc[2 * q + 1] * gelu_d(__high2float(h)));
-                        }
-                    } else {
-#pragma unroll
-                        for (int q = 0; q < 16; ++q) {
-                            const int c0 = 2 * q, c1 = 2 * q + 1;
-                            const float z0 = c0 < a.cout ? acc[c0] + a.bias[c0] : 0.f;
-                            const float z1 = c1 < a.cout ? acc[c1] + a.bias[c1] : 0.f;
-                            pz[q] = pack2(z0, z1);
-                            py[q] = pack2(gelu(z0), gelu(z1));
-                        }
-                    }
-                    uint4* y4 = reinterpret_cast<uint4*>(a.y + cell * NET_PITCH);
-#pragma unroll
-                    for (int q = 0; q < 4; ++q) y4[q] = make_uint4(py[4 * q], py[4 * q + 1], py[4 * q + 2], py[4 * q + 3]);
-                    if (MODE == MODE_HIDDEN && a.z) {
-                        uint4* z4 = reinterpret_cast<uint4*>(a.z + cell * NET_PITCH);
-#pragma unroll
-                        for (int q = 0; q < 4; ++q)
-                            z4[q] = make_uint4(pz[4 * q], pz[4 * q + 1], pz[4 * q + 2], pz[4 * q + 3]);
-                    }
-                }
-            }
+            float v[32];
+            tc::tmem_ld32(tbase + ((uint32_t)(warp * 32) << 16) + acc * 32, v);
             tc::fence_before_sync();
-            __syncthreads();
+            mbar_arrive(&tempty[acc]);
+            const long long cell = a.c0 + (blockIdx.x + T * (long long)gridDim.x) * 128 + tid;
+            if (cell >= a.c1) return true;
+            if (MODE == MODE_OUT) {
+#pragma unroll
+                for (int co = 0; co < 32; ++co)
+                    if (co < a.cout) a.yf[(long long)co * a.E + cell] = v[co] + a.bias[co];
+                return true;
+            }
+            uint32_t py[16], pz[16];
+            if (MODE == MODE_BWD) {
+                const uint4* g4 = reinterpret_cast<const uint4*>(a.gz + cell * NET_PITCH);
+                uint32_t gz[16];
+#pragma unroll
+                for (int q = 0; q < 4; ++q) {
+                    uint4 u = g4[q];
+                    gz[4 * q] = u.x; gz[4 * q + 1] = u.y; gz[4 * q + 2] = u.z; gz[4 * q + 3] = u.w;
+                }
+#pragma unroll
+                for (int q = 0; q < 16; ++q) {
+                    __nv_bfloat162 h = *reinterpret_cast<__nv_bfloat162*>(&gz[q]);
+                    py[q] = pack2(v[2 * q] * gelu_d(__low2float(h)), v[2 * q + 1] * gelu_d(__high2float(h)));
+                }
+            } else {
+#pragma unroll
+                for (int q = 0; q < 16; ++q) {
+                    const int c0 = 2 * q, c1 = 2 * q + 1;
+                    const float z0 = c0 < a.cout ? v[c0] + a.bias[c0] : 0.f;
+                    const float z1 = c1 < a.cout ? v[c1] + a.bias[c1] : 0.f;
+                    pz[q] = pack2(z0, z1);
+                    py[q] = pack2(gelu(z0), gelu(z1));
+                }
+            }
+            uint4* y4 = reinterpret_cast<uint4*>(a.y + cell * NET_PITCH);
+#pragma unroll
+            for (int q = 0; q < 4; ++q) y4[q] = make_uint4(py[4 * q], py[4 * q + 1], py[4 * q + 2], py[4 * q + 3]);
+            if (MODE == MODE_HIDDEN && a.z) {
+                uint4* z4 = reinterpret_cast<uint4*>(a.z + cell * NET_PITCH);
+#pragma unroll
+                for (int q = 0; q < 4; ++q) z4[q] = make_uint4(pz[4 * q], pz[4 * q + 1], pz[4 * q + 2], pz[4 * q + 3]);
+            }
+            return true;
+        };
+        bool ok = true;
+        for (long long T = 0; T < myTiles && ok; ++T) {
+            const long long cell0 = a.c0 + (blockIdx.x + T * (long long)gridDim.x) * 128;
+            for (int w = 0; w < 9 && ok; ++w) {
+                const long long it = T * 9 + w;
+                const int st = (int)(it % S::NS);
+                const long long use = it / S::NS;
+                if (use > 0 && !tc::mbar_wait(&empty[st], (uint32_t)((use - 1) & 1), WAIT_LIMIT)) { ok = false; break; }
+                const int dj = w % 3 - 1, dk = w / 3 - 1;
+                const long long base = cell0 - 1 + (long long)a.P * (dj + (long long)a.Q * dk);
+                unsigned char* dst = sStage + st * S::STAGE;
+                for (int id = tid; id < S::ROWS * S::KCH; id += 128) {
+                    const int row = id / S::KCH, kc = id % S::KCH;
+                    const long long cell = base + row;
+                    const bool inb = cell >= 0 && cell < a.E;
+                    cp_async16(dst + kc * S::LBO + row * 16, a.x + (inb ? cell : 0) * CINP + kc * 8, inb ? 16u : 0u);
+                }
+                const unsigned char* wsrc = reinterpret_cast<const unsigned char*>(a.w) + (3 * (dj + 1) + 9 * (dk + 1)) * S::TAPB;
+                for (int id = tid; id < 3 * S::TAPB / 16; id += 128) cp_async16_ca(dst + S::WIN + id * 16, wsrc + id * 16);
+                cp_async_arrive(&full[st]);
+            }
+            if (ok && T > 0) ok = epilogue(T - 1);
         }
-    }
-    cp_async_wait_all();
-    if (!ok) {
-        if (tid == 0) atomicExch(a.err, 1);
-        // MMAs still in flight read this CTA's shared memory and write its TMEM: let them finish
-        for (int b = 0; b < S::NBUF; ++b)
-            if (cnt[b]) tc::mbar_wait(&mbar[b], (cnt[b] - 1) & 1u, WAIT_LIMIT);
+        if (ok && myTiles > 0) ok = epilogue(myTiles - 1);
+        if (!ok) failed = 1;
+        cp_async_wait_all();
+    } else if (tid == 128) {
+        // ---------------- MMA issue
+        const uint32_t idesc = tc::idesc_bf16_f32(128, S::COUTP);
+        constexpr uint32_t SBO_W = CINP / 8 * 128;
+        long long issued = 0;   // windows whose MMAs were committed
+        bool ok = true;
+        for (long long T = 0; T < myTiles && ok; ++T) {
+            const int acc = (int)(T & 1);
+            if (T >= 2 && !tc::mbar_wait(&tempty[acc], (uint32_t)(((T >> 1) - 1) & 1), WAIT_LIMIT)) { ok = false; break; }
+            for (int w = 0; w < 9; ++w) {
+                const long long it = T * 9 + w;
+                const int st = (int)(it % S::NS);
+                if (!tc::mbar_wait(&full[st], (uint32_t)((it / S::NS) & 1), WAIT_LIMIT)) { ok = false; break; }
+                tc::fence_smem_async();   // the generic-proxy copies, to the tensor core
+                tc::fence_after_sync();
+                const uint32_t win = tc::smem_u32(sStage + st * S::STAGE);
+#pragma unroll
+                for (int di = -1; di <= 1; ++di) {
+#pragma unroll
+                    for (int ks = 0; ks < CINP / 16; ++ks) {
+                        const uint64_t ad = tc::desc_kmajor(win + (di + 1) * 16 + ks * 2 * S::LBO, S::LBO, 128);
+                        const uint64_t bd = tc::desc_kmajor(win + S::WIN + (di + 1) * S::TAPB + ks * 256, 128, SBO_W);
+                        tc::mma_bf16(tbase + acc * 32, ad, bd, idesc, !(w == 0 && di == -1 && ks == 0));
+                    }
+                }
+                tc::mma_commit(&empty[st]);
+                if (w == 8) tc::mma_commit(&tfull[acc]);
+                ++issued;
+            }
+        }
+        if (!ok) {
+            failed = 1;
+            // the MMAs already issued read shared memory and write TMEM: wait for the last commit
+            if (issued > 0) {
+                const long long it = issued - 1;
+                tc::mbar_wait(&empty[(int)(it % S::NS)], (uint32_t)((it / S::NS) & 1), WAIT_LIMIT);
+            }
+        }
     }
     tc::fence_before_sync();
     __syncthreads();
-    if (warp == 0) tc::tmem_free(tbase, 32);
+    if (tid == 0 && failed) atomicExch(a.err, 1);
+    if (warp == 0) tc::tmem_free(tbase, 64);
 }
 
 // ------------------------------------------------------------------ weight gradient
@@ -435,10 +452,10 @@ template <int CINP, int MODE>
 void launch_conv(const ConvArgs& a, cudaStream_t st) {
     using S = ConvShape<CINP>;
     long long ntiles = (a.c1 - a.c0 + 127) / 128;
-    long long grid = sm_count() * (CINP == 16 ? 8 : 4);
+    long long grid = sm_count() * (CINP == 16 ? 6 : 3);
     if (grid > ntiles) grid = ntiles;
     if (grid < 1) grid = 1;
-    k_conv<CINP, MODE><<<(unsigned)grid, 128, S::BYTES, st>>>(a);
+    k_conv<CINP, MODE><<<(unsigned)grid, S::THREADS, S::BYTES, st>>>(a);
 }
 
 }  // namespace

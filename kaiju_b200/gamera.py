@@ -32,6 +32,7 @@ GAM_SYNC_STATE, GAM_SYNC_OSTATE = 1, 2
 GAM_IC_OT2D, GAM_IC_BW, GAM_IC_LFMBW, GAM_IC_KH = 0, 1, 2, 3
 GAM_SLICE_FAT = 1
 GAM_B0_UNIFORM, GAM_B0_DIPOLE = 1, 2
+GAM_TILE_FLUX_ROWS = 1
 TINY, HUGE = 1.0e-12, 1.0e12
 
 
@@ -88,6 +89,8 @@ SIGNATURES = {
     "gam_gpu_ensemble_run_steps_timed": (C.c_int, [C.c_void_p, C.c_int, _DP]),
     "gam_gpu_ensemble_advance": (C.c_int, [C.c_void_p, C.c_double, C.c_int, C.c_int, C.POINTER(C.c_int)]),
     "gam_gpu_ensemble_destroy": (None, [C.c_void_p]),
+    "gam_gpu_set_tile": (C.c_int, [C.c_void_p, C.c_int, C.c_int]),
+    "gam_gpu_ensemble_autotune": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_int)]),
     "gam_gpu_create_from_corners_ic": (C.c_int, [C.POINTER(C.c_void_p), C.POINTER(ModelC), _DP, C.c_int, _DP,
                                                  C.c_int]),
     "gam_gpu_create_from_corners_b0": (C.c_int, [C.POINTER(C.c_void_p), C.POINTER(ModelC), _DP, C.c_int, C.c_int,
@@ -535,6 +538,11 @@ class GameraGPU:
         arr = buf[:n].reshape((m.Nip, m.Njp, m.Nkp, nv), order="F")
         return {self.SLICE_NAMES[v]: arr[..., v] for v in range(nv)}
 
+    def set_tile(self, what: int, value: int):
+        rc = load_library().gam_gpu_set_tile(self.h, what, value)
+        if rc:
+            raise GamError(rc, "gam_gpu_set_tile")
+
     def set_closure(self, closure: Optional["Closure"]):
         rc = load_library().gam_gpu_set_closure(self.h, closure.c if closure is not None else None)
         if rc:
@@ -586,6 +594,14 @@ class Ensemble:
         ms = C.c_double()
         rc = load_library().gam_gpu_ensemble_run_steps_timed(self.e, n, C.byref(ms))
         return rc, ms.value
+
+    def autotune(self, steps: int = 4):
+        """Flux tile height per member shape, by timing batch steps (the steps advance the run)."""
+        rows = (C.c_int * len(self.members))()
+        rc = load_library().gam_gpu_ensemble_autotune(self.e, steps, rows)
+        if rc:
+            raise GamError(rc, "gam_gpu_ensemble_autotune")
+        return list(rows)
 
     def advance(self, t_end: float, chunk: int = 8, max_steps: int = 1 << 30):
         steps = C.c_int()

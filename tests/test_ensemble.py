@@ -86,3 +86,46 @@ def test_ensemble_advance_to_time(gpu_lib):
     finally:
         for g in members:
             g.close()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("fp32", [False, True])
+def test_flux_tile_height_does_not_change_results(gpu_lib, fp32):
+    """4-row and 8-row flux tiles compute every interface from the same staged values: bit-identical runs."""
+    from kaiju_b200 import gamera as gm
+    par = dict(nx=128, a=0.03, Bx=0.1, amp=0.01, seed=4)
+    a, b = gm.kh_member(par, fp32), gm.kh_member(par, fp32)
+    try:
+        b.set_tile(gm.GAM_TILE_FLUX_ROWS, 4)
+        assert a.run_steps(6) == 0 and b.run_steps(6) == 0
+        for name in ("gas", "magflux"):
+            assert np.array_equal(a.fetch(name), b.fetch(name)), name
+        with pytest.raises(gm.GamError):
+            b.set_tile(gm.GAM_TILE_FLUX_ROWS, 5)
+    finally:
+        a.close()
+        b.close()
+
+
+@pytest.mark.gpu
+def test_ensemble_autotune_is_transparent(gpu_lib):
+    """The autotuner picks a tile height per member shape by timing batch steps; the run it takes part in
+    is bit-identical to the same ensemble stepped without it."""
+    from kaiju_b200 import gamera as gm
+    pars = [dict(nx=64, a=0.02, Bx=0.05, amp=0.01, seed=1), dict(nx=256, a=0.04, Bx=0.15, amp=0.01, seed=2),
+            dict(nx=64, a=0.03, Bx=0.0, amp=0.01, seed=3)]
+    tuned = [gm.kh_member(p, True) for p in pars]
+    plain = [gm.kh_member(p, True) for p in pars]
+    try:
+        with gm.Ensemble(tuned) as e:
+            rows = e.autotune(steps=2)   # 2 shapes x 2 heights x (1 + 2) batch steps
+            assert len(rows) == 3 and set(rows) <= {4, 8} and rows[0] == rows[2]
+            assert e.run_steps(2) == 0
+        with gm.Ensemble(plain) as e:
+            assert e.run_steps(2 * 2 * 3 + 2) == 0
+        for a, b in zip(tuned, plain):
+            assert a.status()["ts"] == b.status()["ts"]
+            assert np.array_equal(a.fetch("gas"), b.fetch("gas"))
+    finally:
+        for g in tuned + plain:
+            g.close()
