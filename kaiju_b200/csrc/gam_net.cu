@@ -48,9 +48,10 @@ struct ConvShape {
     static constexpr int LBO = ROWS * 16;              // bytes between the channel-chunk blocks of a window
     static constexpr int WIN = KCH * LBO;
     static constexpr int TAPB = COUTP * CINP * 2;      // one tap's packed weights
-    static constexpr int STAGE = (WIN + 3 * TAPB + 127) / 128 * 128;   // a window and its three taps' weights
-    static constexpr int NS = 4;                       // stages in the ring
-    static constexpr int BYTES = NS * STAGE + 1024;
+    static constexpr int WB = (27 * TAPB + 1023) / 1024 * 1024;   // all taps, resident for the CTA's life
+    static constexpr int STAGE = (WIN + 127) / 128 * 128;
+    static constexpr int NS = 5;                       // window stages in the ring
+    static constexpr int BYTES = WB + NS * STAGE + 1024;
     static constexpr int THREADS = 160;                // 4 worker warps (copies, epilogue) + 1 MMA warp
 };
 
@@ -63,9 +64,6 @@ __device__ __forceinline__ void cp_async16(void* dst, const void* src, uint32_t 
     asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" :: "r"(tc::smem_u32(dst)), "l"(src), "r"(bytes)
                  : "memory");
 }
-__device__ __forceinline__ void cp_async16_ca(void* dst, const void* src) {
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 16;" :: "r"(tc::smem_u32(dst)), "l"(src) : "memory");
-}
 // arrive on the mbarrier once every cp.async this thread issued so far has landed
 __device__ __forceinline__ void cp_async_arrive(uint64_t* mbar) {
     asm volatile("cp.async.mbarrier.arrive.noinc.shared::cta.b64 [%0];" :: "r"(tc::smem_u32(mbar)) : "memory");
@@ -77,7 +75,7 @@ __device__ __forceinline__ void mbar_arrive(uint64_t* mbar) {
 }
 
 // out[cell][n] = sum over taps t and input channels c of in[cell + off(t)][c] * W_t[n][c], 128 cells per tile.
-// Warps 0-3 copy windows into a ring of NS stages (full[s] completes when the 128 threads' copies of a
+// The weights of all 27 taps stay in shared memory. Warps 0-3 copy windows into a ring of NS stages (full[s] completes when the 128 threads' copies of a
 // window have landed) and run the epilogue of each finished tile (warp w reads TMEM lanes 32w..32w+31);
 // one thread of warp 4 issues the MMAs of a window once its stage is full and commits them to empty[s]
 // (the stage may be refilled) and, after a tile's last window, to tfull[a] (accumulator a is ready).
@@ -87,8 +85,9 @@ __global__ void __launch_bounds__(160) k_conv(ConvArgs a) {
     using S = ConvShape<CINP>;
     static_assert(CINP % 16 == 0, "K step");
     extern __shared__ unsigned char smraw[];
-    unsigned char* sStage = align1k(smraw);
-    __shared__ __align__(8) uint64_t full[S::NS], empty[S::NS], tfull[2], tempty[2];
+    unsigned char* sW = align1k(smraw);
+    unsigned char* sStage = sW + S::WB;
+    __shared__ __align__(8) uint64_t full[S::NS], empty[S::NS], tfull[2], tempty[2], wready;
     __shared__ uint32_t tmemBase;
     __shared__ int failed;
     const int tid = threadIdx.x, warp = tid >> 5;
@@ -96,6 +95,7 @@ __global__ void __launch_bounds__(160) k_conv(ConvArgs a) {
     if (tid == 0) {
         for (int q = 0; q < S::NS; ++q) { tc::mbar_init(&full[q], 128); tc::mbar_init(&empty[q], 1); }
         for (int q = 0; q < 2; ++q) { tc::mbar_init(&tfull[q], 1); tc::mbar_init(&tempty[q], 128); }
+        tc::mbar_init(&wready, 128);
         failed = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
@@ -160,6 +160,10 @@ __global__ void __launch_bounds__(160) k_conv(ConvArgs a) {
             }
             return true;
         };
+        // the weights of all taps, once
+        for (int id = tid; id < 27 * S::TAPB / 16; id += 128)
+            cp_async16(sW + id * 16, reinterpret_cast<const unsigned char*>(a.w) + id * 16, 16u);
+        cp_async_arrive(&wready);
         bool ok = true;
         for (long long T = 0; T < myTiles && ok; ++T) {
             const long long cell0 = a.c0 + (blockIdx.x + T * (long long)gridDim.x) * 128;
@@ -177,8 +181,6 @@ __global__ void __launch_bounds__(160) k_conv(ConvArgs a) {
                     const bool inb = cell >= 0 && cell < a.E;
                     cp_async16(dst + kc * S::LBO + row * 16, a.x + (inb ? cell : 0) * CINP + kc * 8, inb ? 16u : 0u);
                 }
-                const unsigned char* wsrc = reinterpret_cast<const unsigned char*>(a.w) + (3 * (dj + 1) + 9 * (dk + 1)) * S::TAPB;
-                for (int id = tid; id < 3 * S::TAPB / 16; id += 128) cp_async16_ca(dst + S::WIN + id * 16, wsrc + id * 16);
                 cp_async_arrive(&full[st]);
             }
             if (ok && T > 0) ok = epilogue(T - 1);
@@ -191,7 +193,7 @@ __global__ void __launch_bounds__(160) k_conv(ConvArgs a) {
         const uint32_t idesc = tc::idesc_bf16_f32(128, S::COUTP);
         constexpr uint32_t SBO_W = CINP / 8 * 128;
         long long issued = 0;   // windows whose MMAs were committed
-        bool ok = true;
+        bool ok = myTiles == 0 || tc::mbar_wait(&wready, 0u, WAIT_LIMIT);
         for (long long T = 0; T < myTiles && ok; ++T) {
             const int acc = (int)(T & 1);
             if (T >= 2 && !tc::mbar_wait(&tempty[acc], (uint32_t)(((T >> 1) - 1) & 1), WAIT_LIMIT)) { ok = false; break; }
@@ -202,12 +204,13 @@ __global__ void __launch_bounds__(160) k_conv(ConvArgs a) {
                 tc::fence_smem_async();   // the generic-proxy copies, to the tensor core
                 tc::fence_after_sync();
                 const uint32_t win = tc::smem_u32(sStage + st * S::STAGE);
+                const uint32_t wt = tc::smem_u32(sW) + (3 * (w % 3) + 9 * (w / 3)) * S::TAPB;   // taps of (dj, dk)
 #pragma unroll
                 for (int di = -1; di <= 1; ++di) {
 #pragma unroll
                     for (int ks = 0; ks < CINP / 16; ++ks) {
                         const uint64_t ad = tc::desc_kmajor(win + (di + 1) * 16 + ks * 2 * S::LBO, S::LBO, 128);
-                        const uint64_t bd = tc::desc_kmajor(win + S::WIN + (di + 1) * S::TAPB + ks * 256, 128, SBO_W);
+                        const uint64_t bd = tc::desc_kmajor(wt + (di + 1) * S::TAPB + ks * 256, 128, SBO_W);
                         tc::mma_bf16(tbase + acc * 32, ad, bd, idesc, !(w == 0 && di == -1 && ks == 0));
                     }
                 }
@@ -452,7 +455,7 @@ template <int CINP, int MODE>
 void launch_conv(const ConvArgs& a, cudaStream_t st) {
     using S = ConvShape<CINP>;
     long long ntiles = (a.c1 - a.c0 + 127) / 128;
-    long long grid = sm_count() * (CINP == 16 ? 6 : 3);
+    long long grid = sm_count() * (CINP == 16 ? 4 : 2);
     if (grid > ntiles) grid = ntiles;
     if (grid < 1) grid = 1;
     k_conv<CINP, MODE><<<(unsigned)grid, S::THREADS, S::BYTES, st>>>(a);
