@@ -4,6 +4,7 @@ and ionosphere boundaries are not built, so the reference's LFM blast wave suppl
 the plain FP64 path and the FP32-flux path side by side.
 
     python -m kaiju_b200.runs spherical --n 96 96 128 --steps 2000
+    python -m kaiju_b200.runs closure-step --n 128 --steps 20
 """
 from __future__ import annotations
 
@@ -61,13 +62,35 @@ def spherical(n=(96, 96, 128), steps=2000, dipole=2000.0, grid=(10.0, 100.0, 1.0
     return out
 
 
+def closure_step(n: int = 128, steps: int = 20, seed: int = 64):
+    """Device ms per step of the n^3 turbulence problem, plain and with a (freshly initialised) closure
+    attached: the closure's cost does not depend on its weights."""
+    from . import turbulence as tu
+    g = tu.turbulence_problem(n, seed)
+    g.run_steps(3)
+    ms_plain, _ = g.run_steps_timed(steps)
+    c = gm.Closure(n, n, n, seed=0)
+    g.set_closure(c)
+    g.run_steps(3)
+    ms_cl, _ = g.run_steps_timed(steps)
+    out = {"n": n, "steps": steps, "plain_ms": ms_plain / steps, "closure_ms": ms_cl / steps,
+           "rejects": g.closure_rejects()}
+    g.set_closure(None)
+    g.close()
+    c.close()
+    return out
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser()
-    ap.add_argument("run", choices=["spherical"])
-    ap.add_argument("--n", type=int, nargs=3, default=[96, 96, 128])
-    ap.add_argument("--steps", type=int, default=2000)
+    ap.add_argument("run", choices=["spherical", "closure-step"])
+    ap.add_argument("--n", type=int, nargs="+", default=None)
+    ap.add_argument("--steps", type=int, default=None)
     a = ap.parse_args(argv)
-    print(json.dumps(spherical(tuple(a.n), a.steps), indent=1))
+    if a.run == "spherical":
+        print(json.dumps(spherical(tuple(a.n or [96, 96, 128]), a.steps or 2000), indent=1))
+    else:
+        print(json.dumps(closure_step((a.n or [128])[0], a.steps or 20)))
 
 
 if __name__ == "__main__":
