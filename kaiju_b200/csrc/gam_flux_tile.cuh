@@ -33,7 +33,7 @@ template <typename S, int D, int FR> constexpr size_t flux_smem() {
 }
 
 template <typename T, typename S, int D, bool MHD, bool BG, int FR>
-__global__ void __launch_bounds__(32 * FR, 16 / FR) k_flux_tile(Lay L, Par p, FluxSrc<S> in, StateP h, FluxOut<S> F, Reg r) {
+__global__ void __launch_bounds__(32 * FR, (sizeof(S) == 4 ? 32 : 24) / FR) k_flux_tile(Lay L, Par p, FluxSrc<S> in, StateP h, FluxOut<S> F, Reg r) {
     extern __shared__ __align__(16) unsigned char smraw[];
     S* sRec = reinterpret_cast<S*>(smraw);   // staged in the storage type, converted to T on use
     constexpr int RB = rec_box<D, FR>(), LB = lim_box<D, FR>();
