@@ -44,7 +44,7 @@ __device__ __forceinline__ int bidx(BoxC b, int di, int dj, int dk) {
 }
 
 template <typename T, typename S, int ED>
-__global__ void __launch_bounds__(256, 4) k_edge_tile(Lay L, Par p, EdgeSrc<S> in, double* Eout, Reg r, const Scal* sc) {
+__global__ void __launch_bounds__(256, sizeof(S) == 4 ? 6 : 4) k_edge_tile(Lay L, Par p, EdgeSrc<S> in, double* Eout, Reg r, const Scal* sc) {
     using TL = ETile<ED>;
     constexpr int dT1 = TL::dT1, dT2 = TL::dT2;
     extern __shared__ __align__(16) unsigned char smraw[];
