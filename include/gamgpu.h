@@ -239,6 +239,9 @@ void gam_gpu_ensemble_destroy(gam_ensemble_t* e);   /* the members are not destr
  * with each height and keeps the fastest (the timed steps are ordinary steps of the run); fluxRows
  * (optional, one per member) receives the choice. */
 #define GAM_TILE_FLUX_ROWS 1
+/* GAM_TILE_FUSED_UPDATE: 1 (default) the update kernel computes Flux2Deltas itself; 0 keeps the separate
+ * Flux2Deltas kernel, whose dGasH/dGasM planes gam_gpu_fetch can then read. Results do not depend on it. */
+#define GAM_TILE_FUSED_UPDATE 2
 int gam_gpu_set_tile(gam_gpu_t* h, int what, int value);
 int gam_gpu_ensemble_autotune(gam_ensemble_t* e, int steps, int* fluxRows);
 

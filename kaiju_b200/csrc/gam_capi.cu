@@ -577,6 +577,11 @@ int gam_gpu_profile_phases(gam_gpu_t* G, int nsteps, double* ms, int nphase) {
 int gam_gpu_set_tile(gam_gpu_t* G, int what, int value) {
     if (!G) return GAM_ERR_ARG;
     Handle& h = G->h;
+    if (what == GAM_TILE_FUSED_UPDATE) {
+        if (value != 0 && value != 1) return GAM_ERR_ARG;
+        if (h.fuseUpdate != (value != 0)) { h.fuseUpdate = value != 0; destroy_graphs(h); }
+        return GAM_OK;
+    }
     if (what != GAM_TILE_FLUX_ROWS || (value != 4 && value != 8)) return GAM_ERR_ARG;
     if (h.fluxRows != value) {
         h.fluxRows = value;

@@ -110,17 +110,14 @@ __global__ void k_predict_cells(Lay L, Par p, GridP g, StateP n, StateP o, State
 
 // Flux2Deltas (stress.F90:150-196); O is the flux storage type (float on the FP32-flux path), the sums
 // run in double
-// corr: the learned closure's face corrections (24 float planes: direction d, variable v at d*8+v; the 5
-// gas fluxes then the 3 magnetic-stress momentum fluxes), added to the face fluxes, or null. With cond set
-// the kernel runs only when the closure's positivity check rejected this step (the plain fallback).
+// Flux2Deltas of one active cell: dGasH (5) and dGasM (3). corr: the learned closure's face corrections
+// (24 float planes: direction d, variable v at d*8+v; the 5 gas fluxes then the 3 magnetic-stress momentum
+// fluxes), added to the face fluxes, or null.
 template <typename O>
-__global__ void k_flux2deltas(Lay L, Par p, GridP g, FluxOut<O> FI, FluxOut<O> FJ, FluxOut<O> FK, PrimP dGH,
-                              Vec3P dGM, const float* corr, const Scal* cond) {
-    if (cond && !cond->closureReject) return;
-    Reg r = {L.is(), L.Nip, L.js(), L.Njp, L.ks(), L.Nkp};
-    int i, j, k;
-    if (!reg_ijk(r, blockIdx.x * (long long)blockDim.x + threadIdx.x, i, j, k)) return;
-    long long c = L.at(i, j, k), cj = c + L.P, ck = c + (long long)L.P * L.Q;
+__device__ __forceinline__ void cellDeltas(const Lay& L, const Par& p, const GridP& g, const FluxOut<O>& FI,
+                                           const FluxOut<O>& FJ, const FluxOut<O>& FK, const float* corr,
+                                           long long c, double* dh, double* dm) {
+    long long cj = c + L.P, ck = c + (long long)L.P * L.Q;
     double dV = g.volume[c];
     auto cr = [&](int d, int v, long long lo, long long hi) {
         if (!corr) return 0.0;
@@ -129,19 +126,40 @@ __global__ void k_flux2deltas(Lay L, Par p, GridP g, FluxOut<O> FI, FluxOut<O> F
     };
 #pragma unroll
     for (int v = 0; v < 5; ++v)
-        dGH.w[v][c] = (double(FI.g[v][c]) - double(FI.g[v][c + 1]) + double(FJ.g[v][c]) - double(FJ.g[v][cj]) +
-                       double(FK.g[v][c]) - double(FK.g[v][ck]) +
-                       (cr(0, v, c, c + 1) + cr(1, v, c, cj) + cr(2, v, c, ck))) / dV;
+        dh[v] = (double(FI.g[v][c]) - double(FI.g[v][c + 1]) + double(FJ.g[v][c]) - double(FJ.g[v][cj]) +
+                 double(FK.g[v][c]) - double(FK.g[v][ck]) +
+                 (cr(0, v, c, c + 1) + cr(1, v, c, cj) + cr(2, v, c, ck))) / dV;
     if (p.doMHD) {
 #pragma unroll
         for (int x = 0; x < 3; ++x)
-            dGM.v[x][c] = (double(FI.m[x][c]) - double(FI.m[x][c + 1]) + double(FJ.m[x][c]) - double(FJ.m[x][cj]) +
-                           double(FK.m[x][c]) - double(FK.m[x][ck]) +
-                           (cr(0, 5 + x, c, c + 1) + cr(1, 5 + x, c, cj) + cr(2, 5 + x, c, ck))) / dV;
+            dm[x] = (double(FI.m[x][c]) - double(FI.m[x][c + 1]) + double(FJ.m[x][c]) - double(FJ.m[x][cj]) +
+                     double(FK.m[x][c]) - double(FK.m[x][ck]) +
+                     (cr(0, 5 + x, c, c + 1) + cr(1, 5 + x, c, cj) + cr(2, 5 + x, c, ck))) / dV;
         if (p.doBackground) {   // background momentum source (stress.F90:185-188)
 #pragma unroll
-            for (int x = 0; x < 3; ++x) dGM.v[x][c] = dGM.v[x][c] + g.dpB0[x][c];
+            for (int x = 0; x < 3; ++x) dm[x] = dm[x] + g.dpB0[x][c];
         }
+    }
+}
+
+// Flux2Deltas (stress.F90:150-196) into the dGasH/dGasM planes; O is the flux storage type (float on the
+// FP32-flux path), the sums run in double. With cond set the kernel runs only when the closure's
+// positivity check rejected this step (the plain fallback).
+template <typename O>
+__global__ void k_flux2deltas(Lay L, Par p, GridP g, FluxOut<O> FI, FluxOut<O> FJ, FluxOut<O> FK, PrimP dGH,
+                              Vec3P dGM, const float* corr, const Scal* cond) {
+    if (cond && !cond->closureReject) return;
+    Reg r = {L.is(), L.Nip, L.js(), L.Njp, L.ks(), L.Nkp};
+    int i, j, k;
+    if (!reg_ijk(r, blockIdx.x * (long long)blockDim.x + threadIdx.x, i, j, k)) return;
+    long long c = L.at(i, j, k);
+    double dh[5], dm[3] = {0.0, 0.0, 0.0};
+    cellDeltas<O>(L, p, g, FI, FJ, FK, corr, c, dh, dm);
+#pragma unroll
+    for (int v = 0; v < 5; ++v) dGH.w[v][c] = dh[v];
+    if (p.doMHD) {
+#pragma unroll
+        for (int x = 0; x < 3; ++x) dGM.v[x][c] = dm[x];
     }
 }
 
@@ -227,7 +245,11 @@ __device__ void cellBoris(const Par& p, double* U2, const double* U0, const doub
 
 // CellReynolds + CellMaxwell/CellBoris (mhdgroup.F90:113-126, 170-197, 263-330) on active cells;
 // ghost cells carry State n over.
-__global__ void k_update_gas(Lay L, Par p, GridP g, StateP nS, StateP oNew, PrimP dGH, Vec3P dGM, const Scal* sc) {
+// FUSED: the deltas are computed here from the face fluxes (Flux2Deltas of the same cell, same arithmetic)
+// instead of read from the dGasH/dGasM planes
+template <typename O, bool FUSED>
+__global__ void k_update_gas(Lay L, Par p, GridP g, StateP nS, StateP oNew, PrimP dGH, Vec3P dGM, FluxOut<O> FI,
+                             FluxOut<O> FJ, FluxOut<O> FK, const Scal* sc) {
     Reg r = {0, L.Ni, 0, L.Nj, 0, L.Nk};
     int i, j, k;
     if (!reg_ijk(r, blockIdx.x * (long long)blockDim.x + threadIdx.x, i, j, k)) return;
@@ -238,11 +260,18 @@ __global__ void k_update_gas(Lay L, Par p, GridP g, StateP nS, StateP oNew, Prim
     bool act = i >= L.is() && i <= L.ie() && j >= L.js() && j <= L.je() && k >= L.ks() && k <= L.ke();
     if (act) {
         double dt = sc->dt;
+        double dh[5], dm[3] = {0.0, 0.0, 0.0};
+        if (FUSED) cellDeltas<O>(L, p, g, FI, FJ, FK, nullptr, c, dh, dm);
+        else {
+#pragma unroll
+            for (int v = 0; v < 5; ++v) dh[v] = dGH.w[v][c];
+            if (p.doMHD) { dm[0] = dGM.v[0][c]; dm[1] = dGM.v[1][c]; dm[2] = dGM.v[2][c]; }
+        }
         double U0[5];
 #pragma unroll
-        for (int v = 0; v < 5; ++v) { U0[v] = U[v]; U[v] = U[v] + dt * dGH.w[v][c]; }
+        for (int v = 0; v < 5; ++v) { U0[v] = U[v]; U[v] = U[v] + dt * dh[v]; }
         if (p.doMHD) {
-            double dPm[3] = {dGM.v[0][c], dGM.v[1][c], dGM.v[2][c]};
+            double dPm[3] = {dm[0], dm[1], dm[2]};
             if (p.doBoris) {
                 double B2[3] = {oNew.b[0][c], oNew.b[1][c], oNew.b[2][c]};
                 double B0[3] = {nS.b[0][c], nS.b[1][c], nS.b[2][c]};
@@ -250,9 +279,7 @@ __global__ void k_update_gas(Lay L, Par p, GridP g, StateP nS, StateP oNew, Prim
 #pragma unroll
                     for (int x = 0; x < 3; ++x) { B2[x] = B2[x] + g.B0[x][c]; B0[x] = B0[x] + g.B0[x][c]; }
                 }
-                double dPg[5];
-                for (int v = 0; v < 5; ++v) dPg[v] = dGH.w[v][c];
-                cellBoris(p, U, U0, B2, B0, dPg, dPm, dt);
+                cellBoris(p, U, U0, B2, B0, dh, dPm, dt);
             } else {
                 double D = dmax(U[0], p.dFloor), Mx = U[1], My = U[2], Mz = U[3], TotE = U[4];
                 double KinE = 0.5 * (sq(Mx) + sq(My) + sq(Mz)) / D;
@@ -741,7 +768,7 @@ int ensure_f32(Handle& h) {
 int kernels_per_step(const Handle& h) {
     int n = 1 + 1;                      // begin, predict cells
     if (h.p.doMHD) n += 1 + 1 + 6;      // predict faces, E memset (counted), 3x(mom2face + edge)
-    n += (h.p.do25D ? 2 : 3) + 1;       // fluxes + flux2deltas
+    n += (h.p.do25D ? 2 : 3) + ((h.fuseUpdate && !h.closure) ? 0 : 1);   // fluxes + flux2deltas
     n += 1 + 1 + 1;                     // e2flux/copy, bflux2fld, update gas
     n += 2 + 3 + 1;                     // calcdt + finalize, 3 BC kernels, final bflux2fld
     n += ring_kernels_per_step(h);
@@ -797,27 +824,24 @@ int step_enqueue(Handle& h, int cur, cudaEvent_t* ev, bool split) {
     for (int v = 0; v < 5; ++v) dGH.w[v] = h.dGasH[v];
     Vec3P dGM = {{h.dGasM[0], h.dGasM[1], h.dGasM[2]}};
     long long nact = (long long)L.Nip * L.Njp * L.Nkp;
+    FluxOut<float> F32[3];
+    FluxP F64[3];
+    for (int d = 0; d < 3; ++d) {
+        for (int v = 0; v < 5; ++v) { F32[d].g[v] = h.f32.gflx[d][v]; F64[d].g[v] = h.gflx[d][v]; }
+        for (int x = 0; x < 3; ++x) { F32[d].m[x] = h.f32.mflx[d][x]; F64[d].m[x] = h.mflx[d][x]; }
+    }
+    // without a closure the update computes the deltas itself (no dGasH/dGasM round trip through HBM)
+    const bool fuse = h.fuseUpdate && !h.closure;
     // learned closure: face corrections from the net on State n; a corrected update that fails positivity
     // falls back to the plain fluxes (the second, conditional Flux2Deltas)
     const float* corr = h.closure ? closure_enqueue_corr(h, nS, st) : nullptr;
-    for (int pass = 0; pass < (corr ? 2 : 1); ++pass) {
+    for (int pass = 0; pass < (fuse ? 0 : (corr ? 2 : 1)); ++pass) {
         const float* cq = pass == 0 ? corr : nullptr;
         const Scal* cond = pass == 0 ? nullptr : h.dScal;
-        if (h.prec == PREC_FP32FLUX) {
-            FluxOut<float> F[3];
-            for (int d = 0; d < 3; ++d) {
-                for (int v = 0; v < 5; ++v) F[d].g[v] = h.f32.gflx[d][v];
-                for (int x = 0; x < 3; ++x) F[d].m[x] = h.f32.mflx[d][x];
-            }
-            k_flux2deltas<float><<<nblk(nact, TPB), TPB, 0, st>>>(L, p, g, F[0], F[1], F[2], dGH, dGM, cq, cond);
-        } else {
-            FluxP F[3];
-            for (int d = 0; d < 3; ++d) {
-                for (int v = 0; v < 5; ++v) F[d].g[v] = h.gflx[d][v];
-                for (int x = 0; x < 3; ++x) F[d].m[x] = h.mflx[d][x];
-            }
-            k_flux2deltas<double><<<nblk(nact, TPB), TPB, 0, st>>>(L, p, g, F[0], F[1], F[2], dGH, dGM, cq, cond);
-        }
+        if (h.prec == PREC_FP32FLUX)
+            k_flux2deltas<float><<<nblk(nact, TPB), TPB, 0, st>>>(L, p, g, F32[0], F32[1], F32[2], dGH, dGM, cq, cond);
+        else
+            k_flux2deltas<double><<<nblk(nact, TPB), TPB, 0, st>>>(L, p, g, F64[0], F64[1], F64[2], dGH, dGM, cq, cond);
         if (pass == 0 && corr) closure_enqueue_check(h, nS, st);
         if (pass == 1) h.launches++;
     }
@@ -831,7 +855,13 @@ int step_enqueue(Handle& h, int cur, cudaEvent_t* ev, bool split) {
     // which recomputes every cell before anything reads a ghost B
     if (p.doMHD) k_bflux2fld<<<nblk(ncell, TPB), TPB, 0, st>>>(L, g, oS);
     else k_copy_b<<<nblk(L.E, 256), 256, 0, st>>>(L, nS, oS);
-    k_update_gas<<<nblk(ncell, TPB), TPB, 0, st>>>(L, p, g, nS, oS, dGH, dGM, h.dScal);
+    if (h.prec == PREC_FP32FLUX) {
+        if (fuse) k_update_gas<float, true><<<nblk(ncell, TPB), TPB, 0, st>>>(L, p, g, nS, oS, dGH, dGM, F32[0], F32[1], F32[2], h.dScal);
+        else k_update_gas<float, false><<<nblk(ncell, TPB), TPB, 0, st>>>(L, p, g, nS, oS, dGH, dGM, F32[0], F32[1], F32[2], h.dScal);
+    } else {
+        if (fuse) k_update_gas<double, true><<<nblk(ncell, TPB), TPB, 0, st>>>(L, p, g, nS, oS, dGH, dGM, F64[0], F64[1], F64[2], h.dScal);
+        else k_update_gas<double, false><<<nblk(ncell, TPB), TPB, 0, st>>>(L, p, g, nS, oS, dGH, dGM, F64[0], F64[1], F64[2], h.dScal);
+    }
     h.launches += 4;
     if (p.doRing) launch_ring_average(h, oS, st);   // mhdgroup.F90:68-74
     // CalcDT (the per-cell minimum; finalized below, or after the tiles' minimum for a tiled run)

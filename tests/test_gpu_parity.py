@@ -46,8 +46,10 @@ CASES = [
 
 @pytest.mark.parametrize("name,kind,n,kw", CASES, ids=[c[0] for c in CASES])
 def test_one_step_intermediates(gpu_lib, oracle_lib, name, kind, n, kw):
+    from kaiju_b200 import gamera as gm
     o, g = oracle_and_gpu(kind, n, **kw)
     with g:
+        g.set_tile(gm.GAM_TILE_FUSED_UPDATE, 0)   # keep the dGasH/dGasM planes for inspection
         # inputs mirrored exactly
         _cmp(o, g, ["gas", "magflux", "bxyz", "ogas", "omagflux"], tol=0.0, where="input ")
         o.step()
@@ -261,3 +263,21 @@ def test_lfm_dipole_fp32_flux_l1(gpu_lib, oracle_lib):
                 l1 = np.abs(a[..., v] - b[..., v]).mean() / np.abs(b[..., v]).mean()
                 assert l1 <= 1e-5, (s, v, l1)
             resync(o, g)
+
+
+@pytest.mark.parametrize("prec", ["fp64", "fp32flux"])
+def test_fused_update_equals_separate_deltas(gpu_lib, oracle_lib, prec):
+    """The update computing Flux2Deltas itself gives bit-identical states to the separate kernel."""
+    from kaiju_b200 import gamera as gm
+    for kw in ({}, dict(doBoris=True, Ca=2.0)):
+        o, a = oracle_and_gpu("bw", (32, 16, 16), **kw)
+        _, b = oracle_and_gpu("bw", (32, 16, 16), **kw)
+        with a, b:
+            if prec == "fp32flux":
+                a.set_precision(gm.GAM_FP32FLUX)
+                b.set_precision(gm.GAM_FP32FLUX)
+            b.set_tile(gm.GAM_TILE_FUSED_UPDATE, 0)
+            a.run_steps(5)
+            b.run_steps(5)
+            for name in ("gas", "magflux", "bxyz"):
+                assert np.array_equal(a.fetch(name), b.fetch(name)), (kw, name)
