@@ -236,14 +236,20 @@ int gam_gpu_ensemble_advance(gam_ensemble_t* e, double tEnd, int chunk, int maxS
 void gam_gpu_ensemble_destroy(gam_ensemble_t* e);   /* the members are not destroyed */
 /* Tile shapes. GAM_TILE_FLUX_ROWS: rows of interfaces per flux-kernel CTA, 8 (default) or 4; results do
  * not depend on it. The ensemble autotuner times whole batch steps for each member shape (largest first)
- * with each height and keeps the fastest (the timed steps are ordinary steps of the run); fluxRows
- * (optional, one per member) receives the choice. */
+ * with each height and keeps the fastest, then times per-member flux launches against the tile queue
+ * (gam_gpu_ensemble_set_queue) and keeps the faster (the timed steps are ordinary steps of the run);
+ * fluxRows (optional, one per member) and queue (optional) receive the choices. */
+/* Tile queue: with on = 1 every batch step runs the members' predictor and E field as concurrent branches,
+ * then ONE persistent flux kernel whose CTAs take tiles of every member and direction from a shared
+ * counter, then the rest of each member's step as branches (on = 0: each member launches its own flux
+ * kernels). Results do not depend on it. */
+int gam_gpu_ensemble_set_queue(gam_ensemble_t* e, int on);
 #define GAM_TILE_FLUX_ROWS 1
 /* GAM_TILE_FUSED_UPDATE: 1 (default) the update kernel computes Flux2Deltas itself; 0 keeps the separate
  * Flux2Deltas kernel, whose dGasH/dGasM planes gam_gpu_fetch can then read. Results do not depend on it. */
 #define GAM_TILE_FUSED_UPDATE 2
 int gam_gpu_set_tile(gam_gpu_t* h, int what, int value);
-int gam_gpu_ensemble_autotune(gam_ensemble_t* e, int steps, int* fluxRows);
+int gam_gpu_ensemble_autotune(gam_ensemble_t* e, int steps, int* fluxRows, int* queue);
 
 /* DivB for callers that cannot allocate device memory (no counterpart in the reference).
  * Some hosts cannot call cudaMalloc: device arrays owned by another runtime (OpenACC or CUDA Fortran

@@ -9,6 +9,7 @@
 #include "gamgpu.h"
 #include "gam_common.cuh"
 #include "gam_step.cuh"
+#include "gam_kern.cuh"
 #include "gam_init.cuh"
 
 using namespace gam;
@@ -771,6 +772,13 @@ struct gam_ensemble {
     std::vector<cudaEvent_t> join;
     cudaGraphExec_t graph[2] = {nullptr, nullptr};
     int phase = 0;   // which of the two graphs runs next
+    // tile queue: the members' flux kernels replaced by one persistent launch per precision
+    bool queue = false;
+    FluxJob<double>* jobs64[2] = {nullptr, nullptr};
+    FluxJob<float>* jobs32[2] = {nullptr, nullptr};
+    int n64 = 0, n32 = 0;
+    long long tiles64[2] = {0, 0}, tiles32[2] = {0, 0};
+    unsigned long long* counter = nullptr;   // [2]: FP64 and FP32 queues
 };
 
 namespace {
@@ -779,18 +787,66 @@ void ens_destroy_graphs(gam_ensemble* E) {
         if (E->graph[c]) { cudaGraphExecDestroy(E->graph[c]); E->graph[c] = nullptr; }
 }
 // capture the batch step with member m at parity cur[m] ^ flip
+void ens_free_jobs(gam_ensemble* E) {
+    for (int c = 0; c < 2; ++c) {
+        if (E->jobs64[c]) { cudaFree(E->jobs64[c]); E->jobs64[c] = nullptr; }
+        if (E->jobs32[c]) { cudaFree(E->jobs32[c]); E->jobs32[c] = nullptr; }
+    }
+    E->n64 = E->n32 = 0;
+}
+// the queue's jobs for both parities of the active members
+int ens_build_jobs(gam_ensemble* E) {
+    ens_free_jobs(E);
+    for (int flip = 0; flip < 2; ++flip) {
+        std::vector<FluxJob<double>> j64;
+        std::vector<FluxJob<float>> j32;
+        long long f64 = 0, f32 = 0;
+        for (size_t m = 0; m < E->members.size(); ++m) {
+            if (!E->active[m]) continue;
+            Handle& h = E->members[m]->h;
+            if (h.prec == PREC_FP32FLUX) flux_jobs32(h, j32, f32);
+            else flux_jobs64(h, h.cur ^ flip, j64, f64);
+        }
+        E->n64 = (int)j64.size();
+        E->n32 = (int)j32.size();
+        E->tiles64[flip] = f64;
+        E->tiles32[flip] = f32;
+        if (E->n64) {
+            CK(cudaMalloc(&E->jobs64[flip], sizeof(FluxJob<double>) * E->n64));
+            CK(cudaMemcpy(E->jobs64[flip], j64.data(), sizeof(FluxJob<double>) * E->n64, cudaMemcpyHostToDevice));
+        }
+        if (E->n32) {
+            CK(cudaMalloc(&E->jobs32[flip], sizeof(FluxJob<float>) * E->n32));
+            CK(cudaMemcpy(E->jobs32[flip], j32.data(), sizeof(FluxJob<float>) * E->n32, cudaMemcpyHostToDevice));
+        }
+    }
+    return GAM_OK;
+}
 int ens_capture(gam_ensemble* E, int flip, cudaGraphExec_t* out) {
     cudaGraph_t gr;
     CK(cudaStreamBeginCapture(E->root, cudaStreamCaptureModeThreadLocal));
-    cudaEventRecord(E->fork, E->root);
     int rc = 0;
-    for (size_t m = 0; m < E->members.size(); ++m) {
-        if (!E->active[m]) continue;
-        Handle& h = E->members[m]->h;
-        cudaStreamWaitEvent(h.stream, E->fork, 0);
-        if (step_enqueue(h, h.cur ^ flip) != 0) rc = GAM_ERR_CUDA;
-        cudaEventRecord(E->join[m], h.stream);
-        cudaStreamWaitEvent(E->root, E->join[m], 0);
+    // the members' steps as concurrent branches; with the queue, the branches stop before the fluxes and
+    // continue after one persistent flux launch that covers every member's tiles
+    const int parts[2] = {E->queue ? STEP_PRE : STEP_ALL, STEP_POST};
+    for (int pi = 0; pi < (E->queue ? 2 : 1); ++pi) {
+        if (pi == 1) {
+            int sms = 148, dev = 0;
+            cudaGetDevice(&dev);
+            cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+            cudaMemsetAsync(E->counter, 0, 2 * sizeof(unsigned long long), E->root);
+            if (E->n64) launch_flux_queue64(E->jobs64[flip], E->n64, E->tiles64[flip], E->counter, sms * 3, E->root);
+            if (E->n32) launch_flux_queue32(E->jobs32[flip], E->n32, E->tiles32[flip], E->counter + 1, sms * 4, E->root);
+        }
+        cudaEventRecord(E->fork, E->root);
+        for (size_t m = 0; m < E->members.size(); ++m) {
+            if (!E->active[m]) continue;
+            Handle& h = E->members[m]->h;
+            cudaStreamWaitEvent(h.stream, E->fork, 0);
+            if (step_enqueue(h, h.cur ^ flip, nullptr, false, parts[pi]) != 0) rc = GAM_ERR_CUDA;
+            cudaEventRecord(E->join[m], h.stream);
+            cudaStreamWaitEvent(E->root, E->join[m], 0);
+        }
     }
     cudaError_t e = cudaStreamEndCapture(E->root, &gr);
     if (rc || e != cudaSuccess) {
@@ -805,6 +861,10 @@ int ens_capture(gam_ensemble* E, int flip, cudaGraphExec_t* out) {
 int ens_build(gam_ensemble* E) {
     ens_destroy_graphs(E);
     for (auto* G : E->members) CK(cudaStreamSynchronize(G->h.stream));
+    if (E->queue) {
+        int rc = ens_build_jobs(E);
+        if (rc) return rc;
+    }
     int rc = ens_capture(E, 0, &E->graph[0]);
     if (!rc) rc = ens_capture(E, 1, &E->graph[1]);
     E->phase = 0;
@@ -813,11 +873,17 @@ int ens_build(gam_ensemble* E) {
 int ens_launch(gam_ensemble* E) {
     CK(cudaGraphLaunch(E->graph[E->phase], E->root));
     E->phase ^= 1;
+    bool first = true;
     for (size_t m = 0; m < E->members.size(); ++m) {
         if (!E->active[m]) continue;
         Handle& h = E->members[m]->h;
         h.cur ^= 1;
         h.launches += kernels_per_step(h);
+        if (E->queue) {   // its flux launches are the shared queue launches, counted on the first member
+            h.launches -= h.p.do25D ? 2 : 3;
+            if (first) h.launches += (E->n64 ? 1 : 0) + (E->n32 ? 1 : 0) + 1;
+            first = false;
+        }
     }
     return GAM_OK;
 }
@@ -915,7 +981,7 @@ int gam_gpu_ensemble_advance(gam_ensemble_t* E, double tEnd, int chunk, int maxS
 // over `steps` batch steps with the other groups fixed, and the fastest kept. The tile height does not
 // change any result (each interface is computed from the same staged values), so the steps it takes are
 // ordinary steps of the run.
-int gam_gpu_ensemble_autotune(gam_ensemble_t* E, int steps, int* fluxRows) {
+int gam_gpu_ensemble_autotune(gam_ensemble_t* E, int steps, int* fluxRows, int* queue) {
     if (!E || steps < 1) return GAM_ERR_ARG;
     const size_t n = E->members.size();
     std::vector<long long> key(n);
@@ -957,12 +1023,33 @@ int gam_gpu_ensemble_autotune(gam_ensemble_t* E, int steps, int* fluxRows) {
         for (size_t m = 0; m < n; ++m)
             if (key[m] == g) gam_gpu_set_tile(E->members[m], GAM_TILE_FLUX_ROWS, best);
     }
+    // then the flux phase as per-member launches or as one tile-queue launch, whichever is faster
+    {
+        float msMode[2] = {0.f, 0.f};
+        for (int on = 0; on < 2; ++on) {
+            int rc = gam_gpu_ensemble_set_queue(E, on);
+            if (!rc) rc = ens_build(E);
+            if (!rc) rc = ens_launch(E);
+            if (rc) { cudaEventDestroy(e0); cudaEventDestroy(e1); return rc; }
+            CK(cudaEventRecord(e0, E->root));
+            for (int s = 0; s < steps; ++s) {
+                rc = ens_launch(E);
+                if (rc) { cudaEventDestroy(e0); cudaEventDestroy(e1); return rc; }
+            }
+            CK(cudaEventRecord(e1, E->root));
+            CK(cudaEventSynchronize(e1));
+            CK(cudaEventElapsedTime(&msMode[on], e0, e1));
+        }
+        int rc = gam_gpu_ensemble_set_queue(E, msMode[1] < msMode[0] ? 1 : 0);
+        if (rc) { cudaEventDestroy(e0); cudaEventDestroy(e1); return rc; }
+    }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     int rc = ens_build(E);
     if (rc) return rc;
     if (fluxRows)
         for (size_t m = 0; m < n; ++m) fluxRows[m] = E->members[m]->h.fluxRows;
+    if (queue) *queue = E->queue ? 1 : 0;
     return ens_collect(E);
 }
 
@@ -970,10 +1057,23 @@ void gam_gpu_ensemble_destroy(gam_ensemble_t* E) {
     if (!E) return;
     if (E->root) cudaStreamSynchronize(E->root);
     ens_destroy_graphs(E);
+    ens_free_jobs(E);
+    if (E->counter) cudaFree(E->counter);
     for (auto ev : E->join) if (ev) cudaEventDestroy(ev);
     if (E->fork) cudaEventDestroy(E->fork);
     if (E->root) cudaStreamDestroy(E->root);
     delete E;
+}
+
+int gam_gpu_ensemble_set_queue(gam_ensemble_t* E, int on) {
+    if (!E || (on != 0 && on != 1)) return GAM_ERR_ARG;
+    if (on && !E->counter) CK(cudaMalloc(&E->counter, 2 * sizeof(unsigned long long)));
+    if (E->queue != (on != 0)) {
+        for (auto* G : E->members) CK(cudaStreamSynchronize(G->h.stream));
+        ens_destroy_graphs(E);
+        E->queue = on != 0;
+    }
+    return GAM_OK;
 }
 
 }  // extern "C"

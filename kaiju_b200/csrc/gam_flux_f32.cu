@@ -9,10 +9,11 @@ namespace gam {
 
 void flux_kernels_init_f32() {
     set_flux_smem<float, float, 0>(); set_flux_smem<float, float, 1>(); set_flux_smem<float, float, 2>();
+    cudaFuncSetAttribute(k_flux_queue<float, float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)flux_queue_smem<float>());
 }
 
-void enqueue_fluxes_f32(Handle& h, const StateP& nS, cudaStream_t st) {
-    (void)nS;
+static FluxSrc<float> flux_src32(Handle& h) {
     const bool lfm = h.p.doLFMLim != 0;
     const F32Planes& f = h.f32;
     FluxSrc<float> in;
@@ -26,7 +27,26 @@ void enqueue_fluxes_f32(Handle& h, const StateP& nS, cudaStream_t st) {
         for (int x = 0; x < 3; ++x) in.fcB0[d][x] = f.fcB0[d][x];
         in.b0[d] = f.b0n[d];
     }
-    fluxes_all<float, float>(h, in, st);
+    return in;
+}
+
+void enqueue_fluxes_f32(Handle& h, const StateP& nS, cudaStream_t st) {
+    (void)nS;
+    fluxes_all<float, float>(h, flux_src32(h), st);
+}
+
+void flux_jobs32(Handle& h, std::vector<FluxJob<float>>& jobs, long long& first) {
+    FluxOut<float> F[3];
+    for (int d = 0; d < 3; ++d) {
+        for (int v = 0; v < 5; ++v) F[d].g[v] = h.f32.gflx[d][v];
+        for (int x = 0; x < 3; ++x) F[d].m[x] = h.f32.mflx[d][x];
+    }
+    flux_jobs_of<float>(h, flux_src32(h), F, jobs, first);
+}
+
+void launch_flux_queue32(const FluxJob<float>* jobs, int njobs, long long ntiles, unsigned long long* counter,
+                         int grid, cudaStream_t st) {
+    k_flux_queue<float, float><<<grid, 256, flux_queue_smem<float>(), st>>>(jobs, njobs, ntiles, counter);
 }
 
 }  // namespace gam

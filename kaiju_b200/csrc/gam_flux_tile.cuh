@@ -16,6 +16,7 @@
 #pragma once
 #include <cstdio>
 #include <type_traits>
+#include <vector>
 #include "gam_common.cuh"
 #include "gam_kern.cuh"
 #include "gam_step.cuh"
@@ -32,17 +33,20 @@ template <typename S, int D, int FR> constexpr size_t flux_smem() {
     return sizeof(S) * (9 * rec_box<D, FR>() + 8 * lim_box<D, FR>());
 }
 
+// One tile (bx, by, bz) of interfaces: the body of the per-problem flux kernel and of the ensembles'
+// persistent tile-queue kernel. Every thread of the CTA calls it for the same tile.
 template <typename T, typename S, int D, bool MHD, bool BG, int FR>
-__global__ void __launch_bounds__(32 * FR, (sizeof(S) == 4 ? 32 : 24) / FR) k_flux_tile(Lay L, Par p, FluxSrc<S> in, StateP h, FluxOut<S> F, Reg r) {
-    extern __shared__ __align__(16) unsigned char smraw[];
+__device__ __forceinline__ void flux_tile_body(const Lay& L, const Par& p, const FluxSrc<S>& in, const StateP& h,
+                                               const FluxOut<S>& F, const Reg& r, int bx, int by, int bz,
+                                               unsigned char* smraw) {
     S* sRec = reinterpret_cast<S*>(smraw);   // staged in the storage type, converted to T on use
     constexpr int RB = rec_box<D, FR>(), LB = lim_box<D, FR>();
     S* sLim = sRec + 9 * RB;
     const int tid = threadIdx.x, lane = tid & 31, row = tid >> 5;
-    const int i0 = r.i0 + blockIdx.x * FL;
+    const int i0 = r.i0 + bx * FL;
     int i = i0 + lane, j, k, a0;
-    if (D == 2) { a0 = r.k0 + blockIdx.y * FR; k = a0 + row; j = r.j0 + blockIdx.z; }
-    else { a0 = r.j0 + blockIdx.y * FR; j = a0 + row; k = r.k0 + blockIdx.z; }
+    if (D == 2) { a0 = r.k0 + by * FR; k = a0 + row; j = r.j0 + bz; }
+    else { a0 = r.j0 + by * FR; j = a0 + row; k = r.k0 + bz; }
 
     // ---- stage the stencil footprint (rows of 32..40 doubles, one warp per row)
     const int warp = tid >> 5;
@@ -158,6 +162,13 @@ __global__ void __launch_bounds__(32 * FR, (sizeof(S) == 4 ? 32 : 24) / FR) k_fl
     for (int v = 0; v < 5; ++v) F.g[v][c] = S(faB * double(gF[v]));
 }
 
+template <typename T, typename S, int D, bool MHD, bool BG, int FR>
+__global__ void __launch_bounds__(32 * FR, (sizeof(S) == 4 ? 32 : 24) / FR) k_flux_tile(Lay L, Par p, FluxSrc<S> in, StateP h, FluxOut<S> F, Reg r) {
+    extern __shared__ __align__(16) unsigned char smraw[];
+    flux_tile_body<T, S, D, MHD, BG, FR>(L, p, in, h, F, r, blockIdx.x, blockIdx.y, blockIdx.z, smraw);
+}
+
+
 template <typename T, typename S, int D, int FR>
 static void launch_flux_rows(Handle& h, const FluxSrc<S>& in, const FluxOut<S>& F, const Reg& r, cudaStream_t st) {
     const Par& p = h.p;
@@ -200,6 +211,72 @@ static void set_flux_smem() {
     set_flux_smem_rows<T, S, D, 4>();
     set_flux_smem_rows<T, S, D, 8>();
 }
+// ------------------------------------------------------------------ ensembles: one tile queue for all members
+// A job is one flux direction of one problem; its tiles are numbered from `first` in a single sequence
+// over all jobs. The persistent kernel's CTAs take tile numbers from a counter until the sequence is done,
+// find the job (jobs are sorted by `first`) and run the tile body of that problem and direction.
+template <typename T, typename S, int D>
+__device__ __forceinline__ void flux_job_tile(const FluxJob<S>& J, int bx, int by, int bz, unsigned char* sm) {
+    if (J.kind == 2) flux_tile_body<T, S, D, true, true, 8>(J.L, J.p, J.in, J.h, J.F, J.r, bx, by, bz, sm);
+    else if (J.kind == 1) flux_tile_body<T, S, D, true, false, 8>(J.L, J.p, J.in, J.h, J.F, J.r, bx, by, bz, sm);
+    else flux_tile_body<T, S, D, false, false, 8>(J.L, J.p, J.in, J.h, J.F, J.r, bx, by, bz, sm);
+}
+
+template <typename T, typename S>
+__global__ void __launch_bounds__(256, (sizeof(S) == 4 ? 4 : 3)) k_flux_queue(const FluxJob<S>* jobs, int njobs,
+                                                                             long long ntiles,
+                                                                             unsigned long long* counter) {
+    extern __shared__ __align__(16) unsigned char smraw[];
+    __shared__ long long item;
+    for (;;) {
+        if (threadIdx.x == 0) item = (long long)atomicAdd(counter, 1ull);
+        __syncthreads();
+        const long long t = item;
+        if (t >= ntiles) break;
+        int lo = 0, hi = njobs - 1;
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (jobs[mid].first <= t) lo = mid;
+            else hi = mid - 1;
+        }
+        const FluxJob<S>& J = jobs[lo];
+        const long long u = t - J.first;
+        const int bx = (int)(u % J.gx), by = (int)((u / J.gx) % J.gy), bz = (int)(u / ((long long)J.gx * J.gy));
+        if (J.D == 0) flux_job_tile<T, S, 0>(J, bx, by, bz, smraw);
+        else if (J.D == 1) flux_job_tile<T, S, 1>(J, bx, by, bz, smraw);
+        else flux_job_tile<T, S, 2>(J, bx, by, bz, smraw);
+        __syncthreads();   // every thread is done with the staged tile (and has read `item`)
+    }
+}
+
+template <typename S> constexpr size_t flux_queue_smem() {
+    return flux_smem<S, 1, 8>() > flux_smem<S, 0, 8>() ? flux_smem<S, 1, 8>() : flux_smem<S, 0, 8>();
+}
+
+// the jobs of one problem's flux directions, tiles numbered on from `first`
+template <typename S>
+static void flux_jobs_of(Handle& h, const FluxSrc<S>& in, const FluxOut<S> F[3], std::vector<FluxJob<S>>& jobs,
+                         long long& first) {
+    const Lay& L = h.L;
+    int is = L.is(), ie = L.ie(), js = L.js(), je = L.je(), ks = L.ks(), ke = L.ke();
+    if (h.p.do25D) ke = ks;
+    const Reg regs[3] = {mkreg(is, ie + 1, js, je, ks, ke), mkreg(is, ie, js, je + 1, ks, ke),
+                         mkreg(is, ie, js, je, ks, ke + 1)};
+    for (int D = 0; D < (h.p.do25D ? 2 : 3); ++D) {
+        FluxJob<S> J;
+        J.L = L; J.p = h.p; J.in = in; J.h = h.H; J.F = F[D]; J.r = regs[D]; J.D = D;
+        J.kind = h.p.doMHD ? (h.p.doBackground ? 2 : 1) : 0;
+        const Reg& r = regs[D];
+        J.gx = (r.ni + FL - 1) / FL;
+        int gz;
+        if (D == 2) { J.gy = (r.nk + 8 - 1) / 8; gz = r.nj; }
+        else { J.gy = (r.nj + 8 - 1) / 8; gz = r.nk; }
+        J.first = first;
+        first += (long long)J.gx * J.gy * gz;
+        jobs.push_back(J);
+    }
+}
+
 // CalcStress flux loop (stress.F90:84-128): I, J and (unless 2.5D) K interfaces
 template <typename T, typename S>
 static void fluxes_all(Handle& h, const FluxSrc<S>& in, cudaStream_t st) {

@@ -1,6 +1,7 @@
 // Kernel-side helpers shared by the step kernels: launch regions, pointer bundles, the one-sided
 // kinetic fluxes, and cooperative staging of a box of a pencil plane into shared memory.
 #pragma once
+#include <vector>
 #include "gam_common.cuh"
 
 namespace gam {
@@ -65,6 +66,26 @@ struct Vec3P { double* v[3]; };
 // interface fluxes (area-scaled) of one direction: double planes, or float planes on the FP32-flux path
 template <typename O> struct FluxOut { O* g[5]; O* m[3]; };
 using FluxP = FluxOut<double>;
+
+// one flux direction of one problem in the ensembles' tile queue (gam_flux_tile.cuh)
+template <typename S> struct FluxJob {
+    Lay L;
+    Par p;
+    FluxSrc<S> in;
+    StateP h;
+    FluxOut<S> F;
+    Reg r;
+    int D, kind;   // kind: 0 hydro, 1 MHD, 2 MHD with a background field
+    int gx, gy;
+    long long first;
+};
+struct Handle;
+void flux_jobs64(Handle& h, int cur, std::vector<FluxJob<double>>& jobs, long long& first);
+void flux_jobs32(Handle& h, std::vector<FluxJob<float>>& jobs, long long& first);
+void launch_flux_queue64(const FluxJob<double>* jobs, int njobs, long long ntiles, unsigned long long* counter,
+                         int grid, cudaStream_t st);
+void launch_flux_queue32(const FluxJob<float>* jobs, int njobs, long long ntiles, unsigned long long* counter,
+                         int grid, cudaStream_t st);
 
 // One-sided gas kinetic flux (stress.F90:432-511)
 template <typename T>

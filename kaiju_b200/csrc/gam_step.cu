@@ -776,21 +776,16 @@ int kernels_per_step(const Handle& h) {
     return n;
 }
 
-static void enqueue_hot(Handle& h, const StateP& nS, cudaStream_t st, cudaEvent_t* ev) {
-    const Par& p = h.p;
-    if (p.doMHD) enqueue_efield(h, nS, st);
-    if (ev) cudaEventRecord(ev[PH_FLUXES], st);
-    enqueue_fluxes(h, nS, st);
-}
-
-int step_enqueue(Handle& h, int cur, cudaEvent_t* ev, bool split) {
+int step_enqueue(Handle& h, int cur, cudaEvent_t* ev, bool split, int part) {
     cudaStream_t st = h.stream;
     auto mark = [&](int ph) { if (ev) cudaEventRecord(ev[ph], st); };
-    mark(PH_PREDICT);
     const Lay& L = h.L;
     const Par& p = h.p;
     GridP g = h.gridP();
     StateP nS = h.S[cur], oS = h.S[cur ^ 1];
+    long long ncell = (long long)L.Ni * L.Nj * L.Nk;
+    if (part != STEP_POST) {
+    mark(PH_PREDICT);
     k_step_begin<<<1, 1, 0, st>>>(h.dScal);
     if (p.doMHD) {
         Vec3P mf = {{nS.mf[0], nS.mf[1], nS.mf[2]}}, omf = {{oS.mf[0], oS.mf[1], oS.mf[2]}},
@@ -804,7 +799,6 @@ int step_enqueue(Handle& h, int cur, cudaEvent_t* ev, bool split) {
     }
     PrimP Wh, Wn;
     for (int v = 0; v < 5; ++v) { Wh.w[v] = h.Wh[v]; Wn.w[v] = h.Wn[v]; }
-    long long ncell = (long long)L.Ni * L.Nj * L.Nk;
     Vec3P VdV = {{h.VdV[0], h.VdV[1], h.VdV[2]}};
     F32CellOut fc{};
     if (h.prec == PREC_FP32FLUX) {
@@ -817,7 +811,13 @@ int step_enqueue(Handle& h, int cur, cudaEvent_t* ev, bool split) {
     if (p.doRing) launch_ring_bfix(h, h.H, st, h.prec == PREC_FP32FLUX);   // bFlux2Fld's ring fix
     if (p.predFixLFM) launch_predfix_lfm(h, h.H, st, h.prec == PREC_FP32FLUX);   // HackPredictor
     mark(PH_EFIELD);
-    enqueue_hot(h, nS, st, ev);
+    if (p.doMHD) enqueue_efield(h, nS, st);
+    }
+    if (part == STEP_PRE) return (int)cudaGetLastError();
+    if (part == STEP_ALL) {
+        mark(PH_FLUXES);
+        enqueue_fluxes(h, nS, st);
+    }
     if (p.doRing) launch_ring_flux(h, st);   // stress.F90:134-139
     mark(PH_DELTAS);
     PrimP dGH;

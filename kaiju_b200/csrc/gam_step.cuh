@@ -88,7 +88,10 @@ struct Handle {
 };
 
 // Enqueue one full stepGamera on h.stream with State n = S[cur]. Does not flip cur.
-int step_enqueue(Handle& h, int cur, cudaEvent_t* phaseEv = nullptr, bool split = false);
+// part: the whole step, or the part before the fluxes (predictor, E field) / after them (Flux2Deltas on),
+// for the ensembles' tile-queue flux kernel that runs between the two for all members at once
+enum { STEP_ALL = 0, STEP_PRE = 1, STEP_POST = 2 };
+int step_enqueue(Handle& h, int cur, cudaEvent_t* phaseEv = nullptr, bool split = false, int part = STEP_ALL);
 // split = true stops after the per-cell CalcDT minimum (into Scal::dtMinBits); a tiled run then reduces
 // the minimum over its tiles and continues with step_enqueue_bcs, the halo fill and step_enqueue_ghosts
 void step_enqueue_bcs(Handle& h, int cur, cudaEvent_t* phaseEv = nullptr);

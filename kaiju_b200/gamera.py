@@ -90,7 +90,8 @@ SIGNATURES = {
     "gam_gpu_ensemble_advance": (C.c_int, [C.c_void_p, C.c_double, C.c_int, C.c_int, C.POINTER(C.c_int)]),
     "gam_gpu_ensemble_destroy": (None, [C.c_void_p]),
     "gam_gpu_set_tile": (C.c_int, [C.c_void_p, C.c_int, C.c_int]),
-    "gam_gpu_ensemble_autotune": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_int)]),
+    "gam_gpu_ensemble_set_queue": (C.c_int, [C.c_void_p, C.c_int]),
+    "gam_gpu_ensemble_autotune": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
     "gam_gpu_create_from_corners_ic": (C.c_int, [C.POINTER(C.c_void_p), C.POINTER(ModelC), _DP, C.c_int, _DP,
                                                  C.c_int]),
     "gam_gpu_create_from_corners_b0": (C.c_int, [C.POINTER(C.c_void_p), C.POINTER(ModelC), _DP, C.c_int, C.c_int,
@@ -595,12 +596,21 @@ class Ensemble:
         rc = load_library().gam_gpu_ensemble_run_steps_timed(self.e, n, C.byref(ms))
         return rc, ms.value
 
+    def set_queue(self, on: bool = True):
+        """One persistent flux launch over all members' tiles per batch step (gam_gpu_ensemble_set_queue)."""
+        rc = load_library().gam_gpu_ensemble_set_queue(self.e, int(on))
+        if rc:
+            raise GamError(rc, "gam_gpu_ensemble_set_queue")
+
     def autotune(self, steps: int = 4):
-        """Flux tile height per member shape, by timing batch steps (the steps advance the run)."""
+        """Flux tile height per member shape, then per-member flux launches or the tile queue, by timing
+        batch steps (the steps advance the run)."""
         rows = (C.c_int * len(self.members))()
-        rc = load_library().gam_gpu_ensemble_autotune(self.e, steps, rows)
+        queue = C.c_int()
+        rc = load_library().gam_gpu_ensemble_autotune(self.e, steps, rows, C.byref(queue))
         if rc:
             raise GamError(rc, "gam_gpu_ensemble_autotune")
+        self.queue = bool(queue.value)
         return list(rows)
 
     def advance(self, t_end: float, chunk: int = 8, max_steps: int = 1 << 30):

@@ -118,14 +118,39 @@ def test_ensemble_autotune_is_transparent(gpu_lib):
     plain = [gm.kh_member(p, True) for p in pars]
     try:
         with gm.Ensemble(tuned) as e:
-            rows = e.autotune(steps=2)   # 2 shapes x 2 heights x (1 + 2) batch steps
+            rows = e.autotune(steps=2)   # (2 shapes x 2 heights + 2 flux modes) x (1 + 2) batch steps
             assert len(rows) == 3 and set(rows) <= {4, 8} and rows[0] == rows[2]
+            assert e.queue in (True, False)
             assert e.run_steps(2) == 0
         with gm.Ensemble(plain) as e:
-            assert e.run_steps(2 * 2 * 3 + 2) == 0
+            assert e.run_steps((2 * 2 + 2) * 3 + 2) == 0
         for a, b in zip(tuned, plain):
             assert a.status()["ts"] == b.status()["ts"]
             assert np.array_equal(a.fetch("gas"), b.fetch("gas"))
     finally:
         for g in tuned + plain:
+            g.close()
+
+
+@pytest.mark.gpu
+def test_tile_queue_equals_per_member_launches(gpu_lib):
+    """One persistent flux launch over every member's tiles gives bit-identical states to each member
+    launching its own flux kernels (members of two sizes, FP32-flux and FP64 mixed)."""
+    from kaiju_b200 import gamera as gm
+    pars = [dict(nx=64, a=0.02, Bx=0.05, amp=0.01, seed=1), dict(nx=128, a=0.04, Bx=0.15, amp=0.01, seed=2),
+            dict(nx=64, a=0.03, Bx=0.0, amp=0.01, seed=3)]
+    fp32 = [True, False, True]
+    q = [gm.kh_member(p, f) for p, f in zip(pars, fp32)]
+    plain = [gm.kh_member(p, f) for p, f in zip(pars, fp32)]
+    try:
+        with gm.Ensemble(q) as e:
+            e.set_queue(True)
+            assert e.run_steps(4) == 0
+        with gm.Ensemble(plain) as e:
+            assert e.run_steps(4) == 0
+        for a, b in zip(q, plain):
+            for name in ("gas", "magflux"):
+                assert np.array_equal(a.fetch(name), b.fetch(name)), name
+    finally:
+        for g in q + plain:
             g.close()
