@@ -162,12 +162,133 @@ __device__ __forceinline__ void flux_tile_body(const Lay& L, const Par& p, const
     for (int v = 0; v < 5; ++v) F.g[v][c] = S(faB * double(gF[v]));
 }
 
+// The per-problem kernel keeps its own copy of the tile body: calling flux_tile_body from the kernel
+// (by reference or by value) measured 8% slower on the 256^3 FP64 step (7.37 vs 6.83 ms of fluxes).
 template <typename T, typename S, int D, bool MHD, bool BG, int FR>
 __global__ void __launch_bounds__(32 * FR, (sizeof(S) == 4 ? 32 : 24) / FR) k_flux_tile(Lay L, Par p, FluxSrc<S> in, StateP h, FluxOut<S> F, Reg r) {
     extern __shared__ __align__(16) unsigned char smraw[];
-    flux_tile_body<T, S, D, MHD, BG, FR>(L, p, in, h, F, r, blockIdx.x, blockIdx.y, blockIdx.z, smraw);
-}
+    S* sRec = reinterpret_cast<S*>(smraw);   // staged in the storage type, converted to T on use
+    constexpr int RB = rec_box<D, FR>(), LB = lim_box<D, FR>();
+    S* sLim = sRec + 9 * RB;
+    const int tid = threadIdx.x, lane = tid & 31, row = tid >> 5;
+    const int i0 = r.i0 + blockIdx.x * FL;
+    int i = i0 + lane, j, k, a0;
+    if (D == 2) { a0 = r.k0 + blockIdx.y * FR; k = a0 + row; j = r.j0 + blockIdx.z; }
+    else { a0 = r.j0 + blockIdx.y * FR; j = a0 + row; k = r.k0 + blockIdx.z; }
 
+    // ---- stage the stencil footprint (rows of 32..40 doubles, one warp per row)
+    const int warp = tid >> 5;
+    auto stage_rec = [&](S* dst, const S* src) {
+        if (D == 0) stage_rows<S>(dst, src, L, i0 - 4, FL + 8, a0, FR, k, 1, warp, FR, lane);
+        else if (D == 1) stage_rows<S>(dst, src, L, i0, FL, a0 - 4, FR + 7, k, 1, warp, FR, lane);
+        else stage_rows<S>(dst, src, L, i0, FL, j, 1, a0 - 4, FR + 7, warp, FR, lane);
+    };
+    auto stage_lim = [&](S* dst, const S* src) {
+        if (D == 0) stage_rows<S>(dst, src, L, i0 - 2, FL + 4, a0, FR, k, 1, warp, FR, lane);
+        else if (D == 1) stage_rows<S>(dst, src, L, i0, FL, a0 - 2, FR + 3, k, 1, warp, FR, lane);
+        else stage_rows<S>(dst, src, L, i0, FL, j, 1, a0 - 2, FR + 3, warp, FR, lane);
+    };
+#pragma unroll
+    for (int q = 0; q < 5; ++q) stage_rec(sRec + q * RB, in.W[q]);
+    stage_rec(sRec + 5 * RB, in.vol);
+#pragma unroll
+    for (int q = 0; q < 5; ++q) stage_lim(sLim + q * LB, in.Wl[q]);
+    if (MHD) {
+#pragma unroll
+        for (int x = 0; x < 3; ++x) {
+            stage_rec(sRec + (6 + x) * RB, in.B[x]);
+            stage_lim(sLim + (5 + x) * LB, in.Bl[x]);
+        }
+    }
+    cp_async_wait_all();
+    __syncthreads();
+    bool valid = (i < r.i0 + r.ni) && (j >= r.j0) && (j < r.j0 + r.nj) && (k >= r.k0) && (k < r.k0 + r.nk);
+    if (!valid) return;
+
+    // stencil offsets in the staged boxes: recon cell m = f-4+m, limiter cell m = f-2+m
+    auto ro = [&](int m) { return D == 0 ? (lane + m) + (FL + 8) * row : lane + FL * (row + m); };
+    auto lo = [&](int m) { return D == 0 ? (lane + m) + (FL + 4) * row : lane + FL * (row + m); };
+    const long long c = L.at(i, j, k), s = L.stride(D);
+    T Vol[8];
+#pragma unroll
+    for (int m = 0; m < 8; ++m) Vol[m] = T(sRec[5 * RB + ro(m)]);
+    T Vi = central8<T>(Vol);
+    T pdmb = T(p.pdmb);
+    T WL[5], WR[5];
+#pragma unroll
+    for (int v = 0; v < 5; ++v) {
+        T Q[8], nQ[4];
+#pragma unroll
+        for (int m = 0; m < 8; ++m) Q[m] = T(sRec[v * RB + ro(m)]);
+#pragma unroll
+        for (int m = 0; m < 4; ++m) nQ[m] = T(sLim[v * LB + lo(m)]);
+        getLR<T>(p.rmeth, pdmb, Vol, Q, nQ, Vi, WL[v], WR[v]);
+    }
+    T Tf[9];
+#pragma unroll
+    for (int q = 0; q < 9; ++q) Tf[q] = T(__ldg(&in.Tf[D][q][c]));
+    double faB = double(__ldg(&in.face[D][c]));
+    T VaD = T(0), bbD = T(0);
+    if (MHD) {
+        T BL[3], BR[3];
+#pragma unroll
+        for (int x = 0; x < 3; ++x) {
+            T Q[8], nQ[4];
+#pragma unroll
+            for (int m = 0; m < 8; ++m) Q[m] = T(sRec[(6 + x) * RB + ro(m)]);
+#pragma unroll
+            for (int m = 0; m < 4; ++m) nQ[m] = T(sLim[(5 + x) * LB + lo(m)]);
+            getLR<T>(p.rmeth, pdmb, Vol, Q, nQ, Vi, BL[x], BR[x]);
+        }
+        // FP64: the half-state flux over the area (stress.F90:301); FP32: the stored flux/area
+        T Bn;
+        if constexpr (std::is_same<S, double>::value) Bn = T(__ldg(&in.bn[D][c]) / faB);
+        else Bn = T(__ldg(&in.bn[D][c]));
+        T mF[3] = {T(0), T(0), T(0)};
+        if constexpr (BG) {   // background field on the face (stress.F90:302-305)
+            T B0[3];
+#pragma unroll
+            for (int x = 0; x < 3; ++x) B0[x] = T(__ldg(&in.fcB0[D][x][c]));
+            T B0n;
+            if constexpr (std::is_same<S, double>::value) B0n = T(__ldg(&in.b0[D][c]) / faB);
+            else B0n = T(__ldg(&in.b0[D][c]));
+            magKin<T, true>(p, T(-1), WL, BL, Bn, Tf, mF, bbD, VaD, B0, B0n);
+            magKin<T, true>(p, T(1), WR, BR, Bn, Tf, mF, bbD, VaD, B0, B0n);
+        } else {
+            magKin<T>(p, T(-1), WL, BL, Bn, Tf, mF, bbD, VaD);
+            magKin<T>(p, T(1), WR, BR, Bn, Tf, mF, bbD, VaD);
+        }
+        if (p.doBoris) {
+            T Ca2 = T(p.Ca) * T(p.Ca);
+#pragma unroll
+            for (int x = 0; x < 3; ++x) {
+                T deeV = WR[1 + x] - WL[1 + x];
+                T deeP = bbD * deeV / Ca2;
+                mF[x] = mF[x] - T(p.cHogM) * VaD * deeP;
+            }
+        }
+#pragma unroll
+        for (int x = 0; x < 3; ++x) F.m[x][c] = S(faB * double(mF[x]));
+    }
+    T gF[5] = {T(0), T(0), T(0), T(0), T(0)}, dW[5] = {T(0), T(0), T(0), T(0), T(0)};
+    T gm1 = T(p.gamma - 1);
+    gasKin<T>(gm1, T(-1), WL, Tf, gF, dW);
+    gasKin<T>(gm1, T(1), WR, Tf, gF, dW);
+    T cH = T(p.cHogH);
+#pragma unroll
+    for (int v = 0; v < 5; ++v) gF[v] = gF[v] - cH * VaD * dW[v];
+    if (p.doBoris) {  // nuclear option, stress.F90:399-417 (cLim = 1.5)
+        T vL = sqrt(WL[1] * WL[1] + WL[2] * WL[2] + WL[3] * WL[3]);
+        T vR = sqrt(WR[1] * WR[1] + WR[2] * WR[2] + WR[3] * WR[3]);
+        T Vn = sqrt(vL * vL + vR * vR) / T(1.41421353816986083984375);   // sqrt(2.0) of a default-real literal
+        if (Vn >= T(1.5) * T(p.Ca)) {
+#pragma unroll
+            for (int v = 0; v < 5; ++v) gF[v] = gF[v] - T(p.Ca) * T(h.gas[v][c] - h.gas[v][c - s]);
+        }
+    }
+#pragma unroll
+    for (int v = 0; v < 5; ++v) F.g[v][c] = S(faB * double(gF[v]));
+}
 
 template <typename T, typename S, int D, int FR>
 static void launch_flux_rows(Handle& h, const FluxSrc<S>& in, const FluxOut<S>& F, const Reg& r, cudaStream_t st) {

@@ -418,71 +418,65 @@ __device__ __forceinline__ void cpmf(const StateP& s, long long dst, long long s
 
 // I faces: periodic (bcs.F90:279-327) or zero gradient (bcs.F90:799-843), inner and outer side
 __global__ void k_bc_i(Lay L, Par p, GridP g, StateP s) {
+    // one thread per ghost layer n and (j, k) row: the layers are independent (each writes its own ghost
+    // cell and faces, from active cells only)
     long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-    int nj = L.Nj + 1;
-    if (t >= (long long)nj * (L.Nk + 1)) return;
-    int j = (int)(t % nj), k = (int)(t / nj);
-    bool cell = (j < L.Nj) && (k < L.Nk);
-    int is = L.is(), ie = L.ie(), nG = L.nG;
+    const int nG = L.nG, nj = L.Nj + 1;
+    if (t >= (long long)nG * nj * (L.Nk + 1)) return;
+    const int n = 1 + (int)(t % nG);
+    const long long row = t / nG;
+    const int j = (int)(row % nj), k = (int)(row / nj);
+    const bool cell = (j < L.Nj) && (k < L.Nk);
+    const int is = L.is(), ie = L.ie();
     // the LFM blast wave's fixed shells (ICs/lfmbw.F90:141-225): fixed gas; ghost face fluxes are the
     // conjugate active-shell fluxes scaled by the face areas (J/K signs flip across the axis)
     auto lfmbwShell = [&](bool inner) {
         double dApm[3] = {1.0, 1.0, 1.0};
         if (p.ringDoS && j < L.js()) dApm[1] = dApm[2] = -1.0;
         if (p.ringDoE && j >= L.je() + 1) dApm[1] = dApm[2] = -1.0;
-        for (int n = 1; n <= nG; ++n) {
-            int ig = inner ? is - n : ie + n;
-            if (cell) {
-                long long c = L.at(ig, j, k);
-                s.gas[0][c] = p.bwD0; s.gas[1][c] = 0.0; s.gas[2][c] = 0.0; s.gas[3][c] = 0.0;
-                s.gas[4][c] = p.bwP0 / (p.gamma - 1.0);
-            }
-            for (int d = 0; d < 3; ++d) {
-                int di = (!inner && d == 0) ? 1 : 0;
-                int ia = inner ? is : ie + di;
-                int jp, kp;
-                lfmFC(L, p.ringDoS, p.ringDoE, d, j, k, jp, kp);
-                long long cg = L.at(ig + di, j, k), ca = L.at(ia, jp, kp);
-                double dA = g.face[d][cg] / g.face[d][ca];
-                s.mf[d][cg] = dApm[d] * dA * s.mf[d][ca];
-            }
+        int ig = inner ? is - n : ie + n;
+        if (cell) {
+            long long c = L.at(ig, j, k);
+            s.gas[0][c] = p.bwD0; s.gas[1][c] = 0.0; s.gas[2][c] = 0.0; s.gas[3][c] = 0.0;
+            s.gas[4][c] = p.bwP0 / (p.gamma - 1.0);
+        }
+        for (int d = 0; d < 3; ++d) {
+            int di = (!inner && d == 0) ? 1 : 0;
+            int ia = inner ? is : ie + di;
+            int jp, kp;
+            lfmFC(L, p.ringDoS, p.ringDoE, d, j, k, jp, kp);
+            long long cg = L.at(ig + di, j, k), ca = L.at(ia, jp, kp);
+            double dA = g.face[d][cg] / g.face[d][ca];
+            s.mf[d][cg] = dApm[d] * dA * s.mf[d][ca];
         }
     };
     if (p.bc[0] == BC_LFMBW) lfmbwShell(true);
     else if (p.bc[0] == BC_PERIODIC) {
-        for (int n = 1; n <= nG; ++n) {
-            long long d = L.at(is - n, j, k), sidx = L.at(ie - n + 1, j, k);
-            if (cell) cpcell(s, d, sidx, true);
-            cpmf(s, d, sidx);
-        }
+        long long d = L.at(is - n, j, k), sidx = L.at(ie - n + 1, j, k);
+        if (cell) cpcell(s, d, sidx, true);
+        cpmf(s, d, sidx);
     } else if (cell) {
-        for (int n = 1; n <= nG; ++n) {
-            long long d = L.at(is - n, j, k), sidx = L.at(is, j, k);
-            cpcell(s, d, sidx, false);
-            cpmf(s, d, sidx);
-        }
+        long long d = L.at(is - n, j, k), sidx = L.at(is, j, k);
+        cpcell(s, d, sidx, false);
+        cpmf(s, d, sidx);
     }
     if (p.bc[1] == BC_LFMBW) lfmbwShell(false);
     else if (p.bc[1] == BC_PERIODIC) {
-        for (int n = 1; n <= nG; ++n) {
-            long long d = L.at(ie + n, j, k), sidx = L.at(is + n - 1, j, k);
-            if (cell) cpcell(s, d, sidx, true);
-            s.mf[1][d] = s.mf[1][sidx];
-            s.mf[2][d] = s.mf[2][sidx];
-            s.mf[0][d + 1] = s.mf[0][L.at(is + n, j, k)];
-        }
+        long long d = L.at(ie + n, j, k), sidx = L.at(is + n - 1, j, k);
+        if (cell) cpcell(s, d, sidx, true);
+        s.mf[1][d] = s.mf[1][sidx];
+        s.mf[2][d] = s.mf[2][sidx];
+        s.mf[0][d + 1] = s.mf[0][L.at(is + n, j, k)];
     } else if (cell) {
         double B[3];
         cellBxyz(L, g, s.mf, L.at(ie, j, k), B);
-        for (int n = 1; n <= nG; ++n) {
-            int ig = ie + n;
-            long long d = L.at(ig, j, k);
-            cpcell(s, d, L.at(ie, j, k), false);
-            long long dI = d + 1;
-            s.mf[0][dI] = g.face[0][dI] * (B[0] * g.Tf[0][0][dI] + B[1] * g.Tf[0][1][dI] + B[2] * g.Tf[0][2][dI]);
-            s.mf[1][d] = g.face[1][d] * (B[0] * g.Tf[1][0][d] + B[1] * g.Tf[1][1][d] + B[2] * g.Tf[1][2][d]);
-            s.mf[2][d] = g.face[2][d] * (B[0] * g.Tf[2][0][d] + B[1] * g.Tf[2][1][d] + B[2] * g.Tf[2][2][d]);
-        }
+        int ig = ie + n;
+        long long d = L.at(ig, j, k);
+        cpcell(s, d, L.at(ie, j, k), false);
+        long long dI = d + 1;
+        s.mf[0][dI] = g.face[0][dI] * (B[0] * g.Tf[0][0][dI] + B[1] * g.Tf[0][1][dI] + B[2] * g.Tf[0][2][dI]);
+        s.mf[1][d] = g.face[1][d] * (B[0] * g.Tf[1][0][d] + B[1] * g.Tf[1][1][d] + B[2] * g.Tf[1][2][d]);
+        s.mf[2][d] = g.face[2][d] * (B[0] * g.Tf[2][0][d] + B[1] * g.Tf[2][1][d] + B[2] * g.Tf[2][2][d]);
     }
 }
 
@@ -671,7 +665,7 @@ void launch_bflux2fld(Handle& h, const StateP& s, cudaStream_t st) {
 
 void launch_bcs(Handle& h, const StateP& s, cudaStream_t st) {
     const Lay& L = h.L;
-    k_bc_i<<<nblk((long long)(L.Nj + 1) * (L.Nk + 1), TPB), TPB, 0, st>>>(L, h.p, h.gridP(), s);
+    k_bc_i<<<nblk((long long)L.nG * (L.Nj + 1) * (L.Nk + 1), TPB), TPB, 0, st>>>(L, h.p, h.gridP(), s);
     k_bc_j<<<nblk((long long)(L.Ni + 1) * (L.Nk + 1), TPB), TPB, 0, st>>>(L, h.p, s);
     k_bc_k<<<nblk((long long)(L.Ni + 1) * (L.Nj + 1), TPB), TPB, 0, st>>>(L, h.p, s);
     h.launches += 3;
