@@ -249,6 +249,7 @@ int download_scalars(gam_gpu* G) {
 }
 
 int status_code(int st) {
+    if (st & 8) return GAM_ERR_TIMEOUT;
     if (st & 4) return GAM_ERR_NAN;
     if (st & 3) return GAM_ERR_DT_COLLAPSE;
     return GAM_OK;
@@ -581,6 +582,11 @@ int gam_gpu_set_tile(gam_gpu_t* G, int what, int value) {
     if (what == GAM_TILE_FUSED_UPDATE) {
         if (value != 0 && value != 1) return GAM_ERR_ARG;
         if (h.fuseUpdate != (value != 0)) { h.fuseUpdate = value != 0; destroy_graphs(h); }
+        return GAM_OK;
+    }
+    if (what == GAM_TILE_FLUX_TMA) {
+        if (value != 0 && value != 1) return GAM_ERR_ARG;
+        if (h.fluxTma != (value != 0)) { h.fluxTma = value != 0; destroy_graphs(h); }
         return GAM_OK;
     }
     if (what != GAM_TILE_FLUX_ROWS || (value != 4 && value != 8)) return GAM_ERR_ARG;

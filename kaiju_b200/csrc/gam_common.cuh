@@ -60,7 +60,7 @@ struct Scal {
     unsigned long long dtMinBits;     // running min of CellDT (bit pattern of a non-negative double)
     unsigned int nanCount;            // cells whose CellDT was NaN
     int ts;
-    int status;                       // status bits of the last CalcDT (1 disaster, 2 bad, 4 NaN)
+    int status;                       // status bits of the last CalcDT (1 disaster, 2 bad, 4 NaN, 8 wait gave up)
     int sticky;                       // OR of status over steps since the last reset
     unsigned int lastNan;             // nanCount of the last CalcDT
     int pad;
@@ -70,6 +70,9 @@ struct Scal {
     // learned closure: 1 when this step's corrected update failed positivity and the plain fluxes were used
     int closureReject;
     int closureRejects;               // steps that fell back, since the handle was created
+    // nonzero once a kernel's bounded wait on its own asynchronous copies gave up (the step's results are
+    // not valid); CalcDT reports it as status bit 8
+    unsigned int waitFail;
 };
 
 // Device field bundle. Planes are contiguous arrays of Lay::E doubles.

@@ -15,11 +15,13 @@
 // gam_flux_f32.cu, compiled with approximate single-precision division and square root, the FP32 path.
 #pragma once
 #include <cstdio>
+#include <cstring>
 #include <type_traits>
 #include <vector>
 #include "gam_common.cuh"
 #include "gam_kern.cuh"
 #include "gam_step.cuh"
+#include "gam_tma.cuh"
 
 namespace gam {
 
@@ -28,10 +30,19 @@ constexpr int FL = 32;   // interfaces per tile along i
 // autotuner picks for members too small to fill the GPU
 
 template <int D, int FR> __host__ __device__ constexpr int rec_box() { return D == 0 ? (FL + 8) * FR : FL * (FR + 7); }
-template <int D, int FR> __host__ __device__ constexpr int lim_box() { return D == 0 ? (FL + 4) * FR : FL * (FR + 3); }
-template <typename S, int D, int FR> constexpr size_t flux_smem() {
-    return sizeof(S) * (9 * rec_box<D, FR>() + 8 * lim_box<D, FR>());
+// TMA: the I-sweep limiter box starts at i0-4 like the reconstruction box (its x coordinate must be a
+// multiple of 16 bytes), so its rows are FL+8 wide with the stencil 2 cells in
+template <int D, int FR, bool TMA = false> __host__ __device__ constexpr int lim_box() {
+    return D == 0 ? (TMA ? FL + 8 : FL + 4) * FR : FL * (FR + 3);
 }
+template <typename S, int D, int FR, bool TMA = false> constexpr size_t flux_smem() {
+    return sizeof(S) * (9 * rec_box<D, FR>() + 8 * lim_box<D, FR, TMA>()) + (TMA ? 16 : 0);   // + the mbarrier
+}
+
+// Tensor maps of the staged planes: the reconstruction planes (W 0-4, volume, B 0-2) and the limiter
+// planes (W 0-4, B 0-2), each with the box of the sweep direction
+struct FluxMaps { CUtensorMap rec[9]; CUtensorMap lim[8]; };
+constexpr uint32_t FLUX_WAIT = 1u << 20;   // mbarrier polls before the staging wait gives up
 
 // One tile (bx, by, bz) of interfaces: the body of the per-problem flux kernel and of the ensembles'
 // persistent tile-queue kernel. Every thread of the CTA calls it for the same tile.
@@ -164,11 +175,16 @@ __device__ __forceinline__ void flux_tile_body(const Lay& L, const Par& p, const
 
 // The per-problem kernel keeps its own copy of the tile body: calling flux_tile_body from the kernel
 // (by reference or by value) measured 8% slower on the 256^3 FP64 step (7.37 vs 6.83 ms of fluxes).
-template <typename T, typename S, int D, bool MHD, bool BG, int FR>
-__global__ void __launch_bounds__(32 * FR, (sizeof(S) == 4 ? 32 : 24) / FR) k_flux_tile(Lay L, Par p, FluxSrc<S> in, StateP h, FluxOut<S> F, Reg r) {
-    extern __shared__ __align__(16) unsigned char smraw[];
+// TMA: the footprint arrives by tensor copies issued by one thread (no per-element address arithmetic);
+// otherwise by cp.async row copies.
+template <typename T, typename S, int D, bool MHD, bool BG, int FR, bool TMA>
+__global__ void __launch_bounds__(32 * FR, (sizeof(S) == 4 ? 32 : 24) / FR)
+k_flux_tile(Lay L, Par p, const __grid_constant__ FluxMaps maps, FluxSrc<S> in, StateP h, FluxOut<S> F, Reg r,
+            Scal* sc) {
+    extern __shared__ __align__(128) unsigned char smraw[];
     S* sRec = reinterpret_cast<S*>(smraw);   // staged in the storage type, converted to T on use
-    constexpr int RB = rec_box<D, FR>(), LB = lim_box<D, FR>();
+    constexpr int RB = rec_box<D, FR>(), LB = lim_box<D, FR, TMA>();
+    static_assert(!TMA || ((RB * sizeof(S)) % 128 == 0 && (LB * sizeof(S)) % 128 == 0), "box alignment");
     S* sLim = sRec + 9 * RB;
     const int tid = threadIdx.x, lane = tid & 31, row = tid >> 5;
     const int i0 = r.i0 + blockIdx.x * FL;
@@ -176,38 +192,66 @@ __global__ void __launch_bounds__(32 * FR, (sizeof(S) == 4 ? 32 : 24) / FR) k_fl
     if (D == 2) { a0 = r.k0 + blockIdx.y * FR; k = a0 + row; j = r.j0 + blockIdx.z; }
     else { a0 = r.j0 + blockIdx.y * FR; j = a0 + row; k = r.k0 + blockIdx.z; }
 
-    // ---- stage the stencil footprint (rows of 32..40 doubles, one warp per row)
-    const int warp = tid >> 5;
-    auto stage_rec = [&](S* dst, const S* src) {
-        if (D == 0) stage_rows<S>(dst, src, L, i0 - 4, FL + 8, a0, FR, k, 1, warp, FR, lane);
-        else if (D == 1) stage_rows<S>(dst, src, L, i0, FL, a0 - 4, FR + 7, k, 1, warp, FR, lane);
-        else stage_rows<S>(dst, src, L, i0, FL, j, 1, a0 - 4, FR + 7, warp, FR, lane);
-    };
-    auto stage_lim = [&](S* dst, const S* src) {
-        if (D == 0) stage_rows<S>(dst, src, L, i0 - 2, FL + 4, a0, FR, k, 1, warp, FR, lane);
-        else if (D == 1) stage_rows<S>(dst, src, L, i0, FL, a0 - 2, FR + 3, k, 1, warp, FR, lane);
-        else stage_rows<S>(dst, src, L, i0, FL, j, 1, a0 - 2, FR + 3, warp, FR, lane);
-    };
-#pragma unroll
-    for (int q = 0; q < 5; ++q) stage_rec(sRec + q * RB, in.W[q]);
-    stage_rec(sRec + 5 * RB, in.vol);
-#pragma unroll
-    for (int q = 0; q < 5; ++q) stage_lim(sLim + q * LB, in.Wl[q]);
-    if (MHD) {
-#pragma unroll
-        for (int x = 0; x < 3; ++x) {
-            stage_rec(sRec + (6 + x) * RB, in.B[x]);
-            stage_lim(sLim + (5 + x) * LB, in.Bl[x]);
+    if constexpr (TMA) {
+        // ---- stage the stencil footprint by tensor copies: one box per plane, one mbarrier for all
+        uint64_t* bar = reinterpret_cast<uint64_t*>(smraw + (9 * RB + 8 * LB) * sizeof(S));
+        constexpr int NR = MHD ? 9 : 6, NL = MHD ? 8 : 5;
+        if (tid == 0) {
+            tc::mbar_init(bar, 1);
+            tma::fence_barrier_init();
         }
+        __syncthreads();
+        if (tid == 0) {
+            tma::arrive_expect_tx(bar, (uint32_t)((NR * RB + NL * LB) * sizeof(S)));
+            int rx, ry, rz, ly, lz;   // box origins; the limiter box shares x with the reconstruction box
+            if (D == 0) { rx = i0 - 4; ry = a0; rz = k; ly = a0; lz = k; }
+            else if (D == 1) { rx = i0; ry = a0 - 4; rz = k; ly = a0 - 2; lz = k; }
+            else { rx = i0; ry = j; rz = a0 - 4; ly = j; lz = a0 - 2; }
+#pragma unroll
+            for (int q = 0; q < NR; ++q) tma::load3(sRec + q * RB, &maps.rec[q], rx, ry, rz, bar);
+#pragma unroll
+            for (int q = 0; q < NL; ++q) tma::load3(sLim + q * LB, &maps.lim[q], rx, ly, lz, bar);
+        }
+        if (!tc::mbar_wait(bar, 0u, FLUX_WAIT)) {
+            if (tid == 0) atomicOr(&sc->waitFail, 1u);
+            tc::mbar_wait(bar, 0u, FLUX_WAIT);   // let copies in flight land before the CTA's shared memory goes
+            return;
+        }
+    } else {
+        // ---- stage the stencil footprint (rows of 32..40 doubles, one warp per row)
+        const int warp = tid >> 5;
+        auto stage_rec = [&](S* dst, const S* src) {
+            if (D == 0) stage_rows<S>(dst, src, L, i0 - 4, FL + 8, a0, FR, k, 1, warp, FR, lane);
+            else if (D == 1) stage_rows<S>(dst, src, L, i0, FL, a0 - 4, FR + 7, k, 1, warp, FR, lane);
+            else stage_rows<S>(dst, src, L, i0, FL, j, 1, a0 - 4, FR + 7, warp, FR, lane);
+        };
+        auto stage_lim = [&](S* dst, const S* src) {
+            if (D == 0) stage_rows<S>(dst, src, L, i0 - 2, FL + 4, a0, FR, k, 1, warp, FR, lane);
+            else if (D == 1) stage_rows<S>(dst, src, L, i0, FL, a0 - 2, FR + 3, k, 1, warp, FR, lane);
+            else stage_rows<S>(dst, src, L, i0, FL, j, 1, a0 - 2, FR + 3, warp, FR, lane);
+        };
+#pragma unroll
+        for (int q = 0; q < 5; ++q) stage_rec(sRec + q * RB, in.W[q]);
+        stage_rec(sRec + 5 * RB, in.vol);
+#pragma unroll
+        for (int q = 0; q < 5; ++q) stage_lim(sLim + q * LB, in.Wl[q]);
+        if (MHD) {
+#pragma unroll
+            for (int x = 0; x < 3; ++x) {
+                stage_rec(sRec + (6 + x) * RB, in.B[x]);
+                stage_lim(sLim + (5 + x) * LB, in.Bl[x]);
+            }
+        }
+        cp_async_wait_all();
+        __syncthreads();
     }
-    cp_async_wait_all();
-    __syncthreads();
     bool valid = (i < r.i0 + r.ni) && (j >= r.j0) && (j < r.j0 + r.nj) && (k >= r.k0) && (k < r.k0 + r.nk);
     if (!valid) return;
 
     // stencil offsets in the staged boxes: recon cell m = f-4+m, limiter cell m = f-2+m
     auto ro = [&](int m) { return D == 0 ? (lane + m) + (FL + 8) * row : lane + FL * (row + m); };
-    auto lo = [&](int m) { return D == 0 ? (lane + m) + (FL + 4) * row : lane + FL * (row + m); };
+    constexpr int LW = TMA ? FL + 8 : FL + 4, LX = TMA ? 2 : 0;   // I-sweep limiter row width and stencil shift
+    auto lo = [&](int m) { return D == 0 ? (lane + m + LX) + LW * row : lane + FL * (row + m); };
     const long long c = L.at(i, j, k), s = L.stride(D);
     T Vol[8];
 #pragma unroll
@@ -290,17 +334,45 @@ __global__ void __launch_bounds__(32 * FR, (sizeof(S) == 4 ? 32 : 24) / FR) k_fl
     for (int v = 0; v < 5; ++v) F.g[v][c] = S(faB * double(gF[v]));
 }
 
+// Tensor maps of the staged planes of sweep D; false when a plane cannot be mapped or the tiles' x origins
+// (i0-4 for the I sweep, i0 otherwise; tiles step by FL) would not be 16-byte aligned
+template <typename S, int D, int FR>
+static bool flux_maps(const Handle& h, const FluxSrc<S>& in, const Reg& r, bool mhd, FluxMaps& m) {
+    const int x0 = D == 0 ? r.i0 - 4 : r.i0;
+    if ((x0 * (int)sizeof(S)) % 16 != 0) return false;
+    const int rb[3] = {D == 0 ? FL + 8 : FL, D == 0 ? FR : (D == 1 ? FR + 7 : 1), D == 2 ? FR + 7 : 1};
+    const int lb[3] = {D == 0 ? FL + 8 : FL, D == 0 ? FR : (D == 1 ? FR + 3 : 1), D == 2 ? FR + 3 : 1};
+    const S* rec[9] = {in.W[0], in.W[1], in.W[2], in.W[3], in.W[4], in.vol, in.B[0], in.B[1], in.B[2]};
+    const S* lim[8] = {in.Wl[0], in.Wl[1], in.Wl[2], in.Wl[3], in.Wl[4], in.Bl[0], in.Bl[1], in.Bl[2]};
+    for (int q = 0; q < (mhd ? 9 : 6); ++q)
+        if (!tma::plane_map(&m.rec[q], rec[q], (int)sizeof(S), h.L, rb[0], rb[1], rb[2])) return false;
+    for (int q = 0; q < (mhd ? 8 : 5); ++q)
+        if (!tma::plane_map(&m.lim[q], lim[q], (int)sizeof(S), h.L, lb[0], lb[1], lb[2])) return false;
+    return true;
+}
+
 template <typename T, typename S, int D, int FR>
 static void launch_flux_rows(Handle& h, const FluxSrc<S>& in, const FluxOut<S>& F, const Reg& r, cudaStream_t st) {
     const Par& p = h.p;
     dim3 grid((unsigned)((r.ni + FL - 1) / FL), 0, 0);
     if (D == 2) { grid.y = (unsigned)((r.nk + FR - 1) / FR); grid.z = (unsigned)r.nj; }
     else { grid.y = (unsigned)((r.nj + FR - 1) / FR); grid.z = (unsigned)r.nk; }
+    FluxMaps maps;
+    memset(&maps, 0, sizeof(maps));
+    if (h.fluxTma && flux_maps<S, D, FR>(h, in, r, p.doMHD != 0, maps)) {
+        const size_t sm = flux_smem<S, D, FR, true>();
+        if (p.doMHD && p.doBackground)
+            k_flux_tile<T, S, D, true, true, FR, true><<<grid, 32 * FR, sm, st>>>(h.L, p, maps, in, h.H, F, r, h.dScal);
+        else if (p.doMHD)
+            k_flux_tile<T, S, D, true, false, FR, true><<<grid, 32 * FR, sm, st>>>(h.L, p, maps, in, h.H, F, r, h.dScal);
+        else k_flux_tile<T, S, D, false, false, FR, true><<<grid, 32 * FR, sm, st>>>(h.L, p, maps, in, h.H, F, r, h.dScal);
+        return;
+    }
     const size_t sm = flux_smem<S, D, FR>();
     if (p.doMHD && p.doBackground)
-        k_flux_tile<T, S, D, true, true, FR><<<grid, 32 * FR, sm, st>>>(h.L, p, in, h.H, F, r);
-    else if (p.doMHD) k_flux_tile<T, S, D, true, false, FR><<<grid, 32 * FR, sm, st>>>(h.L, p, in, h.H, F, r);
-    else k_flux_tile<T, S, D, false, false, FR><<<grid, 32 * FR, sm, st>>>(h.L, p, in, h.H, F, r);
+        k_flux_tile<T, S, D, true, true, FR, false><<<grid, 32 * FR, sm, st>>>(h.L, p, maps, in, h.H, F, r, h.dScal);
+    else if (p.doMHD) k_flux_tile<T, S, D, true, false, FR, false><<<grid, 32 * FR, sm, st>>>(h.L, p, maps, in, h.H, F, r, h.dScal);
+    else k_flux_tile<T, S, D, false, false, FR, false><<<grid, 32 * FR, sm, st>>>(h.L, p, maps, in, h.H, F, r, h.dScal);
 }
 
 template <typename T, typename S, int D>
@@ -318,14 +390,17 @@ static void launch_flux_dir(Handle& h, const FluxSrc<S>& in, const Reg& r, cudaS
     h.launches++;
 }
 
+template <typename T, typename S, int D, int FR, bool TMA>
+static void set_flux_smem_kind() {
+    const int sm = (int)flux_smem<S, D, FR, TMA>();
+    cudaFuncSetAttribute(k_flux_tile<T, S, D, true, true, FR, TMA>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+    cudaFuncSetAttribute(k_flux_tile<T, S, D, true, false, FR, TMA>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+    cudaFuncSetAttribute(k_flux_tile<T, S, D, false, false, FR, TMA>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+}
 template <typename T, typename S, int D, int FR>
 static void set_flux_smem_rows() {
-    cudaFuncSetAttribute(k_flux_tile<T, S, D, true, true, FR>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         (int)flux_smem<S, D, FR>());
-    cudaFuncSetAttribute(k_flux_tile<T, S, D, true, false, FR>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         (int)flux_smem<S, D, FR>());
-    cudaFuncSetAttribute(k_flux_tile<T, S, D, false, false, FR>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         (int)flux_smem<S, D, FR>());
+    set_flux_smem_kind<T, S, D, FR, false>();
+    set_flux_smem_kind<T, S, D, FR, true>();
 }
 template <typename T, typename S, int D>
 static void set_flux_smem() {
@@ -347,7 +422,7 @@ template <typename T, typename S>
 __global__ void __launch_bounds__(256, (sizeof(S) == 4 ? 4 : 3)) k_flux_queue(const FluxJob<S>* jobs, int njobs,
                                                                              long long ntiles,
                                                                              unsigned long long* counter) {
-    extern __shared__ __align__(16) unsigned char smraw[];
+    extern __shared__ __align__(128) unsigned char smraw[];
     __shared__ long long item;
     for (;;) {
         if (threadIdx.x == 0) item = (long long)atomicAdd(counter, 1ull);

@@ -395,6 +395,7 @@ __global__ void k_dt_finalize(Par p, Scal* sc, int mode) {
         if (dtMin <= TINY) st |= 1;
     }
     if (sc->nanCount) st |= 4;
+    if (sc->waitFail) st |= 8;
     double r = dtMin;
     if ((sc->t + r) > p.tFin) r = dmax(p.tFin - sc->t, TINY);
     if (sc->dt0 > TINY && r > 10.0 * sc->dt0) r = 10.0 * sc->dt0;

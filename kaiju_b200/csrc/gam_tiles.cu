@@ -155,6 +155,7 @@ __global__ void k_tiles_dtmin(Scal* const* sc, int n) {
 }
 
 int status_of(int st) {
+    if (st & 8) return GAM_ERR_TIMEOUT;
     if (st & 4) return GAM_ERR_NAN;
     if (st & 3) return GAM_ERR_DT_COLLAPSE;
     return GAM_OK;
