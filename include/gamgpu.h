@@ -248,10 +248,10 @@ int gam_gpu_ensemble_set_queue(gam_ensemble_t* e, int on);
 /* GAM_TILE_FUSED_UPDATE: 1 (default) the update kernel computes Flux2Deltas itself; 0 keeps the separate
  * Flux2Deltas kernel, whose dGasH/dGasM planes gam_gpu_fetch can then read. Results do not depend on it. */
 #define GAM_TILE_FUSED_UPDATE 2
-/* GAM_TILE_FLUX_TMA: 1 (default) the flux kernel stages its stencil footprint with tensor-memory-accelerator
- * copies (cp.async.bulk.tensor, one thread per tile); 0 with per-element cp.async. Results do not depend
- * on it. */
-#define GAM_TILE_FLUX_TMA 3
+/* GAM_TILE_TMA: 1 (default) the flux and E-field kernels stage their stencil footprints with
+ * tensor-memory-accelerator copies (cp.async.bulk.tensor, one thread per tile); 0 with per-element
+ * cp.async. Results do not depend on it. */
+#define GAM_TILE_TMA 3
 int gam_gpu_set_tile(gam_gpu_t* h, int what, int value);
 int gam_gpu_ensemble_autotune(gam_ensemble_t* e, int steps, int* fluxRows, int* queue);
 

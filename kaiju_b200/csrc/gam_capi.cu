@@ -584,9 +584,9 @@ int gam_gpu_set_tile(gam_gpu_t* G, int what, int value) {
         if (h.fuseUpdate != (value != 0)) { h.fuseUpdate = value != 0; destroy_graphs(h); }
         return GAM_OK;
     }
-    if (what == GAM_TILE_FLUX_TMA) {
+    if (what == GAM_TILE_TMA) {
         if (value != 0 && value != 1) return GAM_ERR_ARG;
-        if (h.fluxTma != (value != 0)) { h.fluxTma = value != 0; destroy_graphs(h); }
+        if (h.tileTma != (value != 0)) { h.tileTma = value != 0; destroy_graphs(h); }
         return GAM_OK;
     }
     if (what != GAM_TILE_FLUX_ROWS || (value != 4 && value != 8)) return GAM_ERR_ARG;

@@ -3,10 +3,12 @@
 // single-precision division and square root, the FP32 path.
 #pragma once
 #include <cstdio>
+#include <cstring>
 #include <type_traits>
 #include "gam_common.cuh"
 #include "gam_kern.cuh"
 #include "gam_step.cuh"
+#include "gam_tma.cuh"
 
 namespace gam {
 
@@ -15,7 +17,10 @@ void launch_edge_dir_f32(Handle& h, const EdgeSrc<float>& in, int eD, const Reg&
 
 // ------------------------------------------------------------------ tile geometry
 struct BoxC { int oi, oj, ok, ni, nj, nk; };
-template <int ED> struct ETile {
+// TMA: a box that reaches below the tile along i starts at i0-4 (a copy's x coordinate must be a multiple of
+// 16 bytes) and every box row is a multiple of 4 elements; each box's region in shared memory starts on a
+// 128-byte boundary (regions padded to 32 elements), with the mbarrier after the last
+template <int ED, bool TMA = false> struct ETile {
     static constexpr int dT1 = ED == 0 ? 1 : (ED == 1 ? 2 : 0);
     static constexpr int dT2 = ED == 0 ? 2 : (ED == 1 ? 0 : 1);
     static constexpr int TI = 32;
@@ -26,47 +31,88 @@ template <int ED> struct ETile {
         return BoxC{s == 0 ? lo : 0, s == 1 ? lo : 0, s == 2 ? lo : 0, TI + (s == 0 ? extra : 0),
                     TJ + (s == 1 ? extra : 0), TK + (s == 2 ? extra : 0)};
     }
-    static constexpr BoxC b8t2 = box(dT2, -4, 7), b4t2 = box(dT2, -2, 3);
-    static constexpr BoxC b8t1 = box(dT1, -4, 7), b4t1 = box(dT1, -2, 3);
+    static constexpr BoxC widen(BoxC b) {
+        if (!TMA) return b;
+        const int oi = b.oi < 0 ? -4 : 0;
+        return BoxC{oi, b.oj, b.ok, (b.ni + b.oi - oi + 3) / 4 * 4, b.nj, b.nk};
+    }
+    static constexpr BoxC b8t2 = widen(box(dT2, -4, 7)), b4t2 = widen(box(dT2, -2, 3));
+    static constexpr BoxC b8t1 = widen(box(dT1, -4, 7)), b4t1 = widen(box(dT1, -2, 3));
     // corner densities: offsets -1 along dT1 and dT2
-    static constexpr BoxC bR = BoxC{(dT1 == 0 || dT2 == 0) ? -1 : 0, (dT1 == 1 || dT2 == 1) ? -1 : 0,
-                                    (dT1 == 2 || dT2 == 2) ? -1 : 0, TI + ((dT1 == 0 || dT2 == 0) ? 1 : 0),
-                                    TJ + ((dT1 == 1 || dT2 == 1) ? 1 : 0), TK + ((dT1 == 2 || dT2 == 2) ? 1 : 0)};
+    static constexpr BoxC bR = widen(BoxC{(dT1 == 0 || dT2 == 0) ? -1 : 0, (dT1 == 1 || dT2 == 1) ? -1 : 0,
+                                          (dT1 == 2 || dT2 == 2) ? -1 : 0, TI + ((dT1 == 0 || dT2 == 0) ? 1 : 0),
+                                          TJ + ((dT1 == 1 || dT2 == 1) ? 1 : 0), TK + ((dT1 == 2 || dT2 == 2) ? 1 : 0)});
     static constexpr int n8t2 = b8t2.ni * b8t2.nj * b8t2.nk, n4t2 = b4t2.ni * b4t2.nj * b4t2.nk;
     static constexpr int n8t1 = b8t1.ni * b8t1.nj * b8t1.nk, n4t1 = b4t1.ni * b4t1.nj * b4t1.nk;
     static constexpr int nR = bR.ni * bR.nj * bR.nk;
-    // layout: Vf[3], A1, B1 (b8t2) | N1 (b4t2) | A2, B2 (b8t1) | N2 (b4t1) | rho (bR)
-    static constexpr int oVf = 0, oA1 = 3 * n8t2, oB1 = 4 * n8t2, oN1 = 5 * n8t2, oA2 = 5 * n8t2 + n4t2,
-                         oB2 = oA2 + n8t1, oN2 = oA2 + 2 * n8t1, oR = oN2 + n4t1, total = oR + nR;
+    static constexpr int pad(int n) { return TMA ? (n + 31) / 32 * 32 : n; }
+    // layout: Vf[3], A1, B1 (b8t2) | N1 (b4t2) | A2, B2 (b8t1) | N2 (b4t1) | rho (bR); sVf: Vf plane stride
+    static constexpr int sVf = pad(n8t2);
+    static constexpr int oVf = 0, oA1 = 3 * sVf, oB1 = 4 * sVf, oN1 = 5 * sVf, oA2 = oN1 + pad(n4t2),
+                         oB2 = oA2 + pad(n8t1), oN2 = oB2 + pad(n8t1), oR = oN2 + pad(n4t1), total = oR + pad(nR);
+    static constexpr int boxed = 5 * n8t2 + n4t2 + 2 * n8t1 + n4t1 + nR;   // elements the copies deliver
 };
+// Tensor maps of the staged planes in layout order: Vf 0-2, face/hbA/nbA of dT1, face/hbA/nbA of dT2, rho
+struct EdgeMaps { CUtensorMap m[10]; };
+constexpr uint32_t EDGE_WAIT = 1u << 20;   // mbarrier polls before the staging wait gives up
 __device__ __forceinline__ int bidx(BoxC b, int di, int dj, int dk) {
     return (di - b.oi) + b.ni * ((dj - b.oj) + b.nj * (dk - b.ok));
 }
 
-template <typename T, typename S, int ED>
-__global__ void __launch_bounds__(256, sizeof(S) == 4 ? 6 : 4) k_edge_tile(Lay L, Par p, EdgeSrc<S> in, double* Eout, Reg r, const Scal* sc) {
-    using TL = ETile<ED>;
+// TMA: the footprint arrives by tensor copies issued by one thread; otherwise by cp.async row copies
+template <typename T, typename S, int ED, bool TMA>
+__global__ void __launch_bounds__(256, sizeof(S) == 4 ? 6 : 4)
+k_edge_tile(Lay L, Par p, const __grid_constant__ EdgeMaps maps, EdgeSrc<S> in, double* Eout, Reg r, Scal* sc) {
+    using TL = ETile<ED, TMA>;
     constexpr int dT1 = TL::dT1, dT2 = TL::dT2;
-    extern __shared__ __align__(16) unsigned char smraw[];
+    extern __shared__ __align__(128) unsigned char smraw[];
     S* sm = reinterpret_cast<S*>(smraw);
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int ti = lane, tj = (tid >> 5) % TL::TJ, tk = (tid >> 5) / TL::TJ;
     const int i0 = r.i0 + blockIdx.x * TL::TI, j0 = r.j0 + blockIdx.y * TL::TJ, k0 = r.k0 + blockIdx.z * TL::TK;
     constexpr BoxC b8t2 = TL::b8t2, b4t2 = TL::b4t2, b8t1 = TL::b8t1, b4t1 = TL::b4t1, bR = TL::bR;
-    auto stage = [&](S* dst, const S* src, BoxC b) {
-        stage_rows<S>(dst, src, L, i0 + b.oi, b.ni, j0 + b.oj, b.nj, k0 + b.ok, b.nk, warp, 8, lane);
-    };
+    if constexpr (TMA) {
+        static_assert((TL::total * sizeof(S)) % 16 == 0, "mbarrier alignment");
+        uint64_t* bar = reinterpret_cast<uint64_t*>(smraw + TL::total * sizeof(S));
+        if (tid == 0) {
+            tc::mbar_init(bar, 1);
+            tma::fence_barrier_init();
+        }
+        __syncthreads();
+        if (tid == 0) {
+            tma::arrive_expect_tx(bar, (uint32_t)(TL::boxed * sizeof(S)));
+            auto ld = [&](int q, int off, BoxC b) { tma::load3(sm + off, &maps.m[q], i0 + b.oi, j0 + b.oj, k0 + b.ok, bar); };
 #pragma unroll
-    for (int x = 0; x < 3; ++x) stage(sm + TL::oVf + x * TL::n8t2, in.Vf[x], b8t2);
-    stage(sm + TL::oA1, in.face[dT1], b8t2);
-    stage(sm + TL::oB1, in.hbA[dT1], b8t2);
-    stage(sm + TL::oN1, in.nbA[dT1], b4t2);
-    stage(sm + TL::oA2, in.face[dT2], b8t1);
-    stage(sm + TL::oB2, in.hbA[dT2], b8t1);
-    stage(sm + TL::oN2, in.nbA[dT2], b4t1);
-    stage(sm + TL::oR, in.rho, bR);
-    cp_async_wait_all();
-    __syncthreads();
+            for (int x = 0; x < 3; ++x) ld(x, TL::oVf + x * TL::sVf, b8t2);
+            ld(3, TL::oA1, b8t2);
+            ld(4, TL::oB1, b8t2);
+            ld(5, TL::oN1, b4t2);
+            ld(6, TL::oA2, b8t1);
+            ld(7, TL::oB2, b8t1);
+            ld(8, TL::oN2, b4t1);
+            ld(9, TL::oR, bR);
+        }
+        if (!tc::mbar_wait(bar, 0u, EDGE_WAIT)) {
+            if (tid == 0) atomicOr(&sc->waitFail, 1u);
+            tc::mbar_wait(bar, 0u, EDGE_WAIT);   // let copies in flight land before the CTA's shared memory goes
+            return;
+        }
+    } else {
+        auto stage = [&](S* dst, const S* src, BoxC b) {
+            stage_rows<S>(dst, src, L, i0 + b.oi, b.ni, j0 + b.oj, b.nj, k0 + b.ok, b.nk, warp, 8, lane);
+        };
+#pragma unroll
+        for (int x = 0; x < 3; ++x) stage(sm + TL::oVf + x * TL::sVf, in.Vf[x], b8t2);
+        stage(sm + TL::oA1, in.face[dT1], b8t2);
+        stage(sm + TL::oB1, in.hbA[dT1], b8t2);
+        stage(sm + TL::oN1, in.nbA[dT1], b4t2);
+        stage(sm + TL::oA2, in.face[dT2], b8t1);
+        stage(sm + TL::oB2, in.hbA[dT2], b8t1);
+        stage(sm + TL::oN2, in.nbA[dT2], b4t1);
+        stage(sm + TL::oR, in.rho, bR);
+        cp_async_wait_all();
+        __syncthreads();
+    }
     const int i = i0 + ti, j = j0 + tj, k = k0 + tk;
     if (!(i < r.i0 + r.ni && j < r.j0 + r.nj && k < r.k0 + r.nk)) return;
     const long long c = L.at(i, j, k);
@@ -85,8 +131,8 @@ __global__ void __launch_bounds__(256, sizeof(S) == 4 ? 6 : 4) k_edge_tile(Lay L
         Bb[m] = T(sm[TL::oB1 + q]);
         T w = T(wC8(m));
         Vc0 = Vc0 + w * (Ab[m] * T(sm[TL::oVf + q]));
-        Vc1 = Vc1 + w * (Ab[m] * T(sm[TL::oVf + TL::n8t2 + q]));
-        Vc2 = Vc2 + w * (Ab[m] * T(sm[TL::oVf + 2 * TL::n8t2 + q]));
+        Vc1 = Vc1 + w * (Ab[m] * T(sm[TL::oVf + TL::sVf + q]));
+        Vc2 = Vc2 + w * (Ab[m] * T(sm[TL::oVf + 2 * TL::sVf + q]));
     }
     T fA1 = central8<T>(Ab);
     T dA = fA1 > T(TINY) ? fA1 : T(TINY);
@@ -163,19 +209,40 @@ __global__ void __launch_bounds__(256, sizeof(S) == 4 ? 6 : 4) k_edge_tile(Lay L
     Eout[c] = double(e) * edg;
 }
 
+// Tensor maps of the staged planes of edge direction ED; false when a plane cannot be mapped or the boxes'
+// x origins (i0 and i0-4; tiles step by 32) would not be 16-byte aligned
+template <typename S, int ED>
+static bool edge_maps(const Handle& h, const EdgeSrc<S>& in, const Reg& re, EdgeMaps& m) {
+    using TL = ETile<ED, true>;
+    if ((re.i0 * (int)sizeof(S)) % 16 != 0) return false;
+    const S* src[10] = {in.Vf[0], in.Vf[1], in.Vf[2], in.face[TL::dT1], in.hbA[TL::dT1], in.nbA[TL::dT1],
+                        in.face[TL::dT2], in.hbA[TL::dT2], in.nbA[TL::dT2], in.rho};
+    const BoxC box[10] = {TL::b8t2, TL::b8t2, TL::b8t2, TL::b8t2, TL::b8t2, TL::b4t2, TL::b8t1, TL::b8t1, TL::b4t1, TL::bR};
+    for (int q = 0; q < 10; ++q)
+        if (!tma::plane_map(&m.m[q], src[q], (int)sizeof(S), h.L, box[q].ni, box[q].nj, box[q].nk)) return false;
+    return true;
+}
+
 template <typename T, typename S, int ED>
 static void launch_edge(Handle& h, const EdgeSrc<S>& in, const Reg& re, cudaStream_t st) {
     using TL = ETile<ED>;
     dim3 grid((unsigned)((re.ni + TL::TI - 1) / TL::TI), (unsigned)((re.nj + TL::TJ - 1) / TL::TJ),
               (unsigned)((re.nk + TL::TK - 1) / TL::TK));
-    k_edge_tile<T, S, ED><<<grid, 256, sizeof(S) * TL::total, st>>>(h.L, h.p, in, h.E[ED], re, h.dScal);
+    EdgeMaps maps;
+    memset(&maps, 0, sizeof(maps));
+    if (h.tileTma && edge_maps<S, ED>(h, in, re, maps))
+        k_edge_tile<T, S, ED, true><<<grid, 256, sizeof(S) * ETile<ED, true>::total + 16, st>>>(h.L, h.p, maps, in, h.E[ED], re, h.dScal);
+    else
+        k_edge_tile<T, S, ED, false><<<grid, 256, sizeof(S) * TL::total, st>>>(h.L, h.p, maps, in, h.E[ED], re, h.dScal);
     h.launches++;
 }
 
 template <typename T, typename S, int ED>
 static void set_edge_smem() {
-    cudaFuncSetAttribute(k_edge_tile<T, S, ED>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    cudaFuncSetAttribute(k_edge_tile<T, S, ED, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          (int)(sizeof(S) * ETile<ED>::total));
+    cudaFuncSetAttribute(k_edge_tile<T, S, ED, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)(sizeof(S) * ETile<ED, true>::total + 16));
 }
 
 template <typename T, typename S>

@@ -359,7 +359,7 @@ static void launch_flux_rows(Handle& h, const FluxSrc<S>& in, const FluxOut<S>& 
     else { grid.y = (unsigned)((r.nj + FR - 1) / FR); grid.z = (unsigned)r.nk; }
     FluxMaps maps;
     memset(&maps, 0, sizeof(maps));
-    if (h.fluxTma && flux_maps<S, D, FR>(h, in, r, p.doMHD != 0, maps)) {
+    if (h.tileTma && flux_maps<S, D, FR>(h, in, r, p.doMHD != 0, maps)) {
         const size_t sm = flux_smem<S, D, FR, true>();
         if (p.doMHD && p.doBackground)
             k_flux_tile<T, S, D, true, true, FR, true><<<grid, 32 * FR, sm, st>>>(h.L, p, maps, in, h.H, F, r, h.dScal);

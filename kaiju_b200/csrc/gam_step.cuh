@@ -75,7 +75,7 @@ struct Handle {
     int cur = 0;
     bool fuseUpdate = true;  // the update computes Flux2Deltas itself (off: dGasH/dGasM planes kept for inspection)
     int fluxRows = 8;        // rows per flux tile (4 or 8), chosen per problem by the ensemble autotuner
-    bool fluxTma = true;     // flux kernel stages by tensor copies (off: per-element cp.async)
+    bool tileTma = true;     // flux and E-field kernels stage by tensor copies (off: per-element cp.async)
     int tilePhase = 0;       // split-step position of a tile (gam_tiles.cu): 0 between steps
     ::gam_closure* closure = nullptr;   // learned flux closure applied in the step (gam_closure.cu)
 

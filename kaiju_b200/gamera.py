@@ -32,7 +32,7 @@ GAM_SYNC_STATE, GAM_SYNC_OSTATE = 1, 2
 GAM_IC_OT2D, GAM_IC_BW, GAM_IC_LFMBW, GAM_IC_KH = 0, 1, 2, 3
 GAM_SLICE_FAT = 1
 GAM_B0_UNIFORM, GAM_B0_DIPOLE = 1, 2
-GAM_TILE_FLUX_ROWS, GAM_TILE_FUSED_UPDATE, GAM_TILE_FLUX_TMA = 1, 2, 3
+GAM_TILE_FLUX_ROWS, GAM_TILE_FUSED_UPDATE, GAM_TILE_TMA = 1, 2, 3
 TINY, HUGE = 1.0e-12, 1.0e12
 
 

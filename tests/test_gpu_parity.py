@@ -286,9 +286,9 @@ def test_fused_update_equals_separate_deltas(gpu_lib, oracle_lib, prec):
 @pytest.mark.parametrize("prec", ["fp64", "fp32flux"])
 @pytest.mark.parametrize("name", ["bw_warp", "bw_hydro", "bw_7up", "ot25d", "lfmbw_dipole"])
 def test_tma_staging_equals_cp_async(gpu_lib, oracle_lib, name, prec):
-    """The flux kernel's footprint staged by tensor copies (one thread per tile) gives bit-identical states
-    to per-element cp.async staging: the I sweep's widened limiter box, the J/K boxes, hydro (no B planes),
-    the 2.5D slab and a background field on the LFM grid."""
+    """The flux and E-field kernels' footprints staged by tensor copies (one thread per tile) give
+    bit-identical states to per-element cp.async staging: the widened boxes along i, the J/K boxes, hydro
+    (no B planes), the 2.5D slab and a background field on the LFM grid."""
     from kaiju_b200 import gamera as gm
     _, kind, n, kw = next(c for c in CASES if c[0] == name)
     o, a = oracle_and_gpu(kind, n, **kw)
@@ -297,7 +297,7 @@ def test_tma_staging_equals_cp_async(gpu_lib, oracle_lib, name, prec):
         if prec == "fp32flux":
             a.set_precision(gm.GAM_FP32FLUX)
             b.set_precision(gm.GAM_FP32FLUX)
-        b.set_tile(gm.GAM_TILE_FLUX_TMA, 0)
+        b.set_tile(gm.GAM_TILE_TMA, 0)
         a.run_steps(4)
         b.run_steps(4)
         assert a.status()["status"] == 0
