@@ -143,9 +143,9 @@ def peaks():
 # B (3) for the limiter, the volume (1), the face triad (9), the area (1) and the half-state normal
 # flux (1) = 28 doubles, and write 5 gas + 3 magnetic fluxes = 8 doubles: 36 doubles = 288 B.
 FLUX_BYTES_PER_IFACE = 36 * 8
-# FP32-flux path: the same 28 inputs as floats (112 B) and the 8 area-scaled fluxes written as doubles
-# (64 B) = 176 B.
-FLUX_BYTES_PER_IFACE_F32 = 28 * 4 + 8 * 8
+# FP32-flux path: the same 28 inputs as floats (112 B) and the 8 area-scaled fluxes written as floats
+# (32 B) = 144 B.
+FLUX_BYTES_PER_IFACE_F32 = 28 * 4 + 8 * 4
 FLUX_FLOPS_PER_IFACE = 700.0
 # Whole-step compulsory traffic per zone-update on a curvilinear grid, FP64: state n and n-1 in,
 # n+1 out (24 doubles) + metrics (volume 1, face 3, edge 3, Tf 27, Te 27, Teb 12, xfc 9, xyzcc 3,

@@ -5,6 +5,8 @@ the plain FP64 path and the FP32-flux path side by side.
 
     python -m kaiju_b200.runs spherical --n 96 96 128 --steps 2000
     python -m kaiju_b200.runs closure-step --n 128 --steps 20
+    python -m kaiju_b200.runs ensemble --steps 20          # 96 Kelvin-Helmholtz members, FP32-flux
+    python -m kaiju_b200.runs tiles --n 256 --steps 10     # the 256^3 blast wave as 1, 2 and 4 k-tiles
 """
 from __future__ import annotations
 
@@ -81,14 +83,76 @@ def closure_step(n: int = 128, steps: int = 20, seed: int = 64):
     return out
 
 
+def ensemble(steps: int = 20, members: int = 96, seed: int = 0):
+    """Device ms per batch step of the Kelvin-Helmholtz ensemble (FP32-flux members of uneven sizes): one
+    graph per batch step with the members as concurrent branches, with the persistent tile-queue flux
+    kernel, after the autotuner's choice, and the members stepped one after another."""
+    import ctypes as C
+    pars = gm.kh_ensemble_params(members, seed)
+    mem = [gm.kh_member(p, True) for p in pars]
+    cells = sum(p["nx"] * (p["nx"] // 2) * 4 for p in pars)
+    out = {"members": members, "cells": cells, "steps": steps}
+    zu = lambda ms: cells * steps / (ms / 1e3)
+    with gm.Ensemble(mem) as e:
+        for name, queue in (("branches", False), ("queue", True)):
+            e.set_queue(queue)
+            e.run_steps(3)
+            rc, ms = e.run_steps_timed(steps)
+            out[name] = {"ms_per_batch_step": ms / steps, "zone_updates_per_s": zu(ms), "status": rc}
+        e.autotune(4)
+        e.run_steps(3)
+        rc, ms = e.run_steps_timed(steps)
+        out["autotuned"] = {"ms_per_batch_step": ms / steps, "zone_updates_per_s": zu(ms), "status": rc,
+                            "queue": bool(e.queue)}
+    tot = 0.0
+    for g in mem:
+        v = C.c_double()
+        gm.load_library().gam_gpu_run_steps_timed(g.h, steps, C.byref(v))
+        tot += v.value
+    out["one_by_one"] = {"ms_per_batch_step": tot / steps, "zone_updates_per_s": zu(tot)}
+    for g in mem:
+        g.close()
+    return out
+
+
+def tiles(n: int = 256, steps: int = 10):
+    """Device ms per step of the n^3 warped blast wave undivided and as 2 and 4 k-tiles on this GPU (one
+    graph per step over all tiles), FP64 and FP32-flux."""
+    from . import tiling as tl
+    out = {"n": n, "steps": steps}
+    for prec in ("fp64", "fp32flux"):
+        model = gm.Model(n, n, n, CFL=0.3, tFin=1.0e30, bc=(gm.GAM_BC_ZEROGRAD,) * 6)
+        xyz = gm.corners_warped(model, (-0.5, 0.5) * 3, 0.04)
+        g = gm.GameraGPU.from_corners(model, xyz, "BW")
+        if prec == "fp32flux":
+            g.set_precision(gm.GAM_FP32FLUX)
+        g.run_steps(3, check=False)
+        ms, _ = g.run_steps_timed(steps)
+        out[f"{prec}_single_ms"] = ms / steps
+        g.close()
+        for T in (2, 4):
+            ts, _ = tl.make_tiles(model, xyz, T, "BW", fp32=(prec == "fp32flux"))
+            grp = gm.TileGroup(ts, periodic_k=False)
+            grp.run_steps(3, check=False)
+            out[f"{prec}_tiles{T}_ms"] = grp.run_steps_timed(steps) / steps
+            grp.close()
+            for t in ts:
+                t.close()
+    return out
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser()
-    ap.add_argument("run", choices=["spherical", "closure-step"])
+    ap.add_argument("run", choices=["spherical", "closure-step", "ensemble", "tiles"])
     ap.add_argument("--n", type=int, nargs="+", default=None)
     ap.add_argument("--steps", type=int, default=None)
     a = ap.parse_args(argv)
     if a.run == "spherical":
         print(json.dumps(spherical(tuple(a.n or [96, 96, 128]), a.steps or 2000), indent=1))
+    elif a.run == "ensemble":
+        print(json.dumps(ensemble(a.steps or 20), indent=1))
+    elif a.run == "tiles":
+        print(json.dumps(tiles((a.n or [256])[0], a.steps or 10), indent=1))
     else:
         print(json.dumps(closure_step((a.n or [128])[0], a.steps or 20)))
 
