@@ -25,6 +25,20 @@ __device__ __forceinline__ bool reg3(const Reg& r, int& i, int& j, int& k) {
     k = r.k0 + (int)(blockIdx.z * blockDim.z + threadIdx.z);
     return (i < r.i0 + r.ni) && (j < r.j0 + r.nj) && (k < r.k0 + r.nk);
 }
+// Launch over a region as (i, j) planes: blockIdx.y is k and the threads run linearly over the plane, i
+// fastest -- one 32-bit division per thread, and idle lanes only in the last block of each plane
+__device__ __forceinline__ bool reg_plane(const Reg& r, int& i, int& j, int& k) {
+    const unsigned t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (unsigned)r.ni * (unsigned)r.nj) return false;
+    const unsigned jj = t / (unsigned)r.ni;
+    i = r.i0 + (int)(t - jj * (unsigned)r.ni);
+    j = r.j0 + (int)jj;
+    k = r.k0 + (int)blockIdx.y;
+    return true;
+}
+static inline dim3 grid_plane(const Reg& r, int tpb) {
+    return dim3((unsigned)(((long long)r.ni * r.nj + tpb - 1) / tpb), (unsigned)r.nk);
+}
 static inline dim3 grid3(const Reg& r, dim3 b) {
     return dim3((unsigned)((r.ni + b.x - 1) / b.x), (unsigned)((r.nj + b.y - 1) / b.y), (unsigned)((r.nk + b.z - 1) / b.z));
 }

@@ -57,7 +57,7 @@ __global__ void k_predict_cells(Lay L, Par p, GridP g, StateP n, StateP o, State
                                 F32CellOut f, const Scal* sc) {
     Reg r = {0, L.Ni, 0, L.Nj, 0, L.Nk};
     int i, j, k;
-    if (!reg_ijk(r, blockIdx.x * (long long)blockDim.x + threadIdx.x, i, j, k)) return;
+    if (!reg_plane(r, i, j, k)) return;
     long long c = L.at(i, j, k);
     double B[3] = {0.0, 0.0, 0.0};
     const bool f32 = f.Wh[0] != nullptr;
@@ -151,7 +151,7 @@ __global__ void k_flux2deltas(Lay L, Par p, GridP g, FluxOut<O> FI, FluxOut<O> F
     if (cond && !cond->closureReject) return;
     Reg r = {L.is(), L.Nip, L.js(), L.Njp, L.ks(), L.Nkp};
     int i, j, k;
-    if (!reg_ijk(r, blockIdx.x * (long long)blockDim.x + threadIdx.x, i, j, k)) return;
+    if (!reg_plane(r, i, j, k)) return;
     long long c = L.at(i, j, k);
     double dh[5], dm[3] = {0.0, 0.0, 0.0};
     cellDeltas<O>(L, p, g, FI, FJ, FK, corr, c, dh, dm);
@@ -169,7 +169,7 @@ __global__ void k_flux2deltas(Lay L, Par p, GridP g, FluxOut<O> FI, FluxOut<O> F
 __global__ void k_e2flux(Lay L, Par p, Vec3P E, StateP nS, StateP oNew, const Scal* sc) {
     Reg r = {0, L.Ni + 1, 0, L.Nj + 1, 0, L.Nk + 1};
     int i, j, k;
-    if (!reg_ijk(r, blockIdx.x * (long long)blockDim.x + threadIdx.x, i, j, k)) return;
+    if (!reg_plane(r, i, j, k)) return;
     long long c = L.at(i, j, k);
     double m0 = nS.mf[0][c], m1 = nS.mf[1][c], m2 = nS.mf[2][c];
     bool act = p.doMHD && i >= L.is() && i <= L.ie() + 1 && j >= L.js() && j <= L.je() + 1 && k >= L.ks() &&
@@ -191,7 +191,7 @@ __global__ void k_e2flux(Lay L, Par p, Vec3P E, StateP nS, StateP oNew, const Sc
 __global__ void k_bflux2fld(Lay L, GridP g, StateP s) {
     Reg r = {0, L.Ni, 0, L.Nj, 0, L.Nk};
     int i, j, k;
-    if (!reg_ijk(r, blockIdx.x * (long long)blockDim.x + threadIdx.x, i, j, k)) return;
+    if (!reg_plane(r, i, j, k)) return;
     long long c = L.at(i, j, k);
     double B[3];
     cellBxyz(L, g, s.mf, c, B);
@@ -252,7 +252,7 @@ __global__ void k_update_gas(Lay L, Par p, GridP g, StateP nS, StateP oNew, Prim
                              FluxOut<O> FJ, FluxOut<O> FK, const Scal* sc) {
     Reg r = {0, L.Ni, 0, L.Nj, 0, L.Nk};
     int i, j, k;
-    if (!reg_ijk(r, blockIdx.x * (long long)blockDim.x + threadIdx.x, i, j, k)) return;
+    if (!reg_plane(r, i, j, k)) return;
     long long c = L.at(i, j, k);
     double U[5];
 #pragma unroll
@@ -299,11 +299,39 @@ __global__ void k_update_gas(Lay L, Par p, GridP g, StateP nS, StateP oNew, Prim
 // bFlux2Fld after EnforceBCs restricted to ghost cells: outside 2.5D the BCs only rewrite faces of
 // ghost cells (outer I/J/K faces from ie+2/je+2/ke+2 on, inner ones below is/js/ks), so active cells
 // keep the B of the update.
+// The ghost cells are enumerated as five slabs so the launch covers only them: k below and above the active
+// range (all i, j), then j below and above (all i, active k), then the i ghosts of the active rows (both
+// ends of a row next to each other, so a warp reads whole ghost runs of neighbouring rows). i runs fastest
+// in every slab.
+__host__ __device__ inline long long ghost_cells(const Lay& L) {
+    return (long long)L.Ni * L.Nj * L.Nk - (long long)L.Nip * L.Njp * L.Nkp;
+}
+__device__ __forceinline__ void ghost_ijk(const Lay& L, long long t, int& i, int& j, int& k) {
+    const long long sK = (long long)L.Ni * L.Nj, sJ = (long long)L.Ni * L.Nkp;
+    const long long nK = sK * (L.Nk - L.Nkp), nJ = sJ * (L.Nj - L.Njp);
+    if (t < nK) {   // k slabs: whole (i, j) planes
+        const int kk = (int)(t / sK), rem = (int)(t % sK);
+        k = kk < L.ks() ? kk : L.ke() + 1 + (kk - L.ks());
+        j = rem / L.Ni; i = rem % L.Ni;
+        return;
+    }
+    t -= nK;
+    if (t < nJ) {   // j slabs within the active k: whole rows
+        const int jj = (int)(t / sJ), rem = (int)(t % sJ);
+        j = jj < L.js() ? jj : L.je() + 1 + (jj - L.js());
+        k = L.ks() + rem / L.Ni; i = rem % L.Ni;
+        return;
+    }
+    t -= nJ;        // the i ghosts of the active rows: nGi = Ni - Nip cells per row
+    const int nGi = L.Ni - L.Nip, ii = (int)(t % nGi), q = (int)(t / nGi);
+    i = ii < L.is() ? ii : L.ie() + 1 + (ii - L.is());
+    j = L.js() + q % L.Njp; k = L.ks() + q / L.Njp;
+}
 __global__ void k_bflux2fld_ghost(Lay L, GridP g, StateP s) {
-    Reg r = {0, L.Ni, 0, L.Nj, 0, L.Nk};
+    const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (t >= ghost_cells(L)) return;
     int i, j, k;
-    if (!reg_ijk(r, blockIdx.x * (long long)blockDim.x + threadIdx.x, i, j, k)) return;
-    if (i >= L.is() && i <= L.ie() && j >= L.js() && j <= L.je() && k >= L.ks() && k <= L.ke()) return;
+    ghost_ijk(L, t, i, j, k);
     long long c = L.at(i, j, k);
     double B[3];
     cellBxyz(L, g, s.mf, c, B);
@@ -312,16 +340,22 @@ __global__ void k_bflux2fld_ghost(Lay L, GridP g, StateP s) {
 
 // ================================================================================ timestep
 // CellDT (gridutils.F90:49-106) over the dt domain (one ghost layer at physical boundaries), min-reduced
-__global__ void k_calcdt(Lay L, Par p, GridP g, StateP s, Scal* sc) {
+// The dt domain: one ghost layer at physical boundaries (init.F90:531-537), the active cells with dtActive;
+// a tile face has no ghost layer in it (ksDT = ks, keDT = ke; gamapp_mpi.F90:441-462)
+__host__ __device__ inline Reg reg_dt(const Lay& L, const Par& p) {
     Reg r = {L.is() - 1, L.Nip + 2, L.js() - 1, L.Njp + 2, L.ks() - 1, L.Nkp + 2};
     if (p.dtActive) r = Reg{L.is(), L.Nip, L.js(), L.Njp, L.ks(), L.Nkp};
-    // a tile face has no ghost layer in the dt domain (ksDT = ks, keDT = ke; gamapp_mpi.F90:441-462)
     if (!p.dtActive && p.bc[4] == BC_HALO) { r.k0 += 1; r.nk -= 1; }
     if (!p.dtActive && p.bc[5] == BC_HALO) r.nk -= 1;
+    return r;
+}
+
+__global__ void k_calcdt(Lay L, Par p, GridP g, StateP s, Scal* sc) {
+    const Reg r = reg_dt(L, p);
     int i, j, k;
     double dtijk = HUGEV * 2.0;
     bool isnan_ = false;
-    if (reg_ijk(r, blockIdx.x * (long long)blockDim.x + threadIdx.x, i, j, k)) {
+    if (reg_plane(r, i, j, k)) {
         long long c = L.at(i, j, k);
         double rho = s.gas[0][c];
         double Vx = s.gas[1][c] / rho, Vy = s.gas[2][c] / rho, Vz = s.gas[3][c] / rho;
@@ -658,8 +692,7 @@ GridP Handle::gridP() const {
 static const int TPB = 128;
 
 void launch_bflux2fld(Handle& h, const StateP& s, cudaStream_t st) {
-    long long n = (long long)h.L.Ni * h.L.Nj * h.L.Nk;
-    k_bflux2fld<<<nblk(n, TPB), TPB, 0, st>>>(h.L, h.gridP(), s);
+    k_bflux2fld<<<grid_plane(Reg{0, h.L.Ni, 0, h.L.Nj, 0, h.L.Nk}, TPB), TPB, 0, st>>>(h.L, h.gridP(), s);
     h.launches++;
     if (h.p.doRing) launch_ring_bfix(h, s, st);   // gridutils.F90:298-300
 }
@@ -674,8 +707,7 @@ void launch_bcs(Handle& h, const StateP& s, cudaStream_t st) {
 
 void launch_calcdt_partial(Handle& h, const StateP& s, cudaStream_t st) {
     const Lay& L = h.L;
-    long long n = (long long)(L.Nip + 2) * (L.Njp + 2) * (L.Nkp + 2);
-    k_calcdt<<<nblk(n, 256), 256, 0, st>>>(L, h.p, h.gridP(), s, h.dScal);
+    k_calcdt<<<grid_plane(reg_dt(L, h.p), 256), 256, 0, st>>>(L, h.p, h.gridP(), s, h.dScal);
     h.launches++;
 }
 
@@ -778,7 +810,7 @@ int step_enqueue(Handle& h, int cur, cudaEvent_t* ev, bool split, int part) {
     const Par& p = h.p;
     GridP g = h.gridP();
     StateP nS = h.S[cur], oS = h.S[cur ^ 1];
-    long long ncell = (long long)L.Ni * L.Nj * L.Nk;
+    const Reg cells = {0, L.Ni, 0, L.Nj, 0, L.Nk}, act = {L.is(), L.Nip, L.js(), L.Njp, L.ks(), L.Nkp};
     if (part != STEP_POST) {
     mark(PH_PREDICT);
     k_step_begin<<<1, 1, 0, st>>>(h.dScal);
@@ -801,7 +833,7 @@ int step_enqueue(Handle& h, int cur, cudaEvent_t* ev, bool split, int part) {
         for (int x = 0; x < 3; ++x) { fc.hb[x] = h.f32.hb[x]; fc.nb[x] = h.f32.nb[x]; fc.VdV[x] = h.f32.VdV[x]; }
         fc.rho = h.f32.rho;
     }
-    k_predict_cells<<<nblk(ncell, TPB), TPB, 0, st>>>(L, p, g, nS, oS, h.H, Wh, Wn, VdV, fc, h.dScal);
+    k_predict_cells<<<grid_plane(Reg{0, L.Ni, 0, L.Nj, 0, L.Nk}, TPB), TPB, 0, st>>>(L, p, g, nS, oS, h.H, Wh, Wn, VdV, fc, h.dScal);
     h.launches += 2;
     if (p.doRing) launch_ring_bfix(h, h.H, st, h.prec == PREC_FP32FLUX);   // bFlux2Fld's ring fix
     if (p.predFixLFM) launch_predfix_lfm(h, h.H, st, h.prec == PREC_FP32FLUX);   // HackPredictor
@@ -818,7 +850,6 @@ int step_enqueue(Handle& h, int cur, cudaEvent_t* ev, bool split, int part) {
     PrimP dGH;
     for (int v = 0; v < 5; ++v) dGH.w[v] = h.dGasH[v];
     Vec3P dGM = {{h.dGasM[0], h.dGasM[1], h.dGasM[2]}};
-    long long nact = (long long)L.Nip * L.Njp * L.Nkp;
     FluxOut<float> F32[3];
     FluxP F64[3];
     for (int d = 0; d < 3; ++d) {
@@ -834,28 +865,27 @@ int step_enqueue(Handle& h, int cur, cudaEvent_t* ev, bool split, int part) {
         const float* cq = pass == 0 ? corr : nullptr;
         const Scal* cond = pass == 0 ? nullptr : h.dScal;
         if (h.prec == PREC_FP32FLUX)
-            k_flux2deltas<float><<<nblk(nact, TPB), TPB, 0, st>>>(L, p, g, F32[0], F32[1], F32[2], dGH, dGM, cq, cond);
+            k_flux2deltas<float><<<grid_plane(act, TPB), TPB, 0, st>>>(L, p, g, F32[0], F32[1], F32[2], dGH, dGM, cq, cond);
         else
-            k_flux2deltas<double><<<nblk(nact, TPB), TPB, 0, st>>>(L, p, g, F64[0], F64[1], F64[2], dGH, dGM, cq, cond);
+            k_flux2deltas<double><<<grid_plane(act, TPB), TPB, 0, st>>>(L, p, g, F64[0], F64[1], F64[2], dGH, dGM, cq, cond);
         if (pass == 0 && corr) closure_enqueue_check(h, nS, st);
         if (pass == 1) h.launches++;
     }
     mark(PH_UPDATE);
     // applyUpdate into the oState buffer (which becomes State n+1)
     Vec3P E = {{h.E[0], h.E[1], h.E[2]}};
-    long long nface = (long long)(L.Ni + 1) * (L.Nj + 1) * (L.Nk + 1);
     if (p.doRing && p.doMHD) launch_pole_e(h, h.E, st);   // mhdgroup.F90:139-142
-    k_e2flux<<<nblk(nface, TPB), TPB, 0, st>>>(L, p, E, nS, oS, h.dScal);
+    k_e2flux<<<grid_plane(Reg{0, L.Ni + 1, 0, L.Nj + 1, 0, L.Nk + 1}, TPB), TPB, 0, st>>>(L, p, E, nS, oS, h.dScal);
     // bFlux2Fld of the update; with ring averaging its ring fix is left to the RingAverage bFlux2Fld,
     // which recomputes every cell before anything reads a ghost B
-    if (p.doMHD) k_bflux2fld<<<nblk(ncell, TPB), TPB, 0, st>>>(L, g, oS);
+    if (p.doMHD) k_bflux2fld<<<grid_plane(cells, TPB), TPB, 0, st>>>(L, g, oS);
     else k_copy_b<<<nblk(L.E, 256), 256, 0, st>>>(L, nS, oS);
     if (h.prec == PREC_FP32FLUX) {
-        if (fuse) k_update_gas<float, true><<<nblk(ncell, TPB), TPB, 0, st>>>(L, p, g, nS, oS, dGH, dGM, F32[0], F32[1], F32[2], h.dScal);
-        else k_update_gas<float, false><<<nblk(ncell, TPB), TPB, 0, st>>>(L, p, g, nS, oS, dGH, dGM, F32[0], F32[1], F32[2], h.dScal);
+        if (fuse) k_update_gas<float, true><<<grid_plane(cells, TPB), TPB, 0, st>>>(L, p, g, nS, oS, dGH, dGM, F32[0], F32[1], F32[2], h.dScal);
+        else k_update_gas<float, false><<<grid_plane(cells, TPB), TPB, 0, st>>>(L, p, g, nS, oS, dGH, dGM, F32[0], F32[1], F32[2], h.dScal);
     } else {
-        if (fuse) k_update_gas<double, true><<<nblk(ncell, TPB), TPB, 0, st>>>(L, p, g, nS, oS, dGH, dGM, F64[0], F64[1], F64[2], h.dScal);
-        else k_update_gas<double, false><<<nblk(ncell, TPB), TPB, 0, st>>>(L, p, g, nS, oS, dGH, dGM, F64[0], F64[1], F64[2], h.dScal);
+        if (fuse) k_update_gas<double, true><<<grid_plane(cells, TPB), TPB, 0, st>>>(L, p, g, nS, oS, dGH, dGM, F64[0], F64[1], F64[2], h.dScal);
+        else k_update_gas<double, false><<<grid_plane(cells, TPB), TPB, 0, st>>>(L, p, g, nS, oS, dGH, dGM, F64[0], F64[1], F64[2], h.dScal);
     }
     h.launches += 4;
     if (p.doRing) launch_ring_average(h, oS, st);   // mhdgroup.F90:68-74
@@ -883,10 +913,9 @@ void step_enqueue_ghosts(Handle& h, int cur) {
     cudaStream_t st = h.stream;
     const Lay& L = h.L;
     StateP s = h.S[cur ^ 1];
-    long long ncell = (long long)L.Ni * L.Nj * L.Nk;
     if (h.p.do25D) launch_bflux2fld(h, s, st);   // the 2.5D K replication rewrites an active cell's upper face
     else {
-        k_bflux2fld_ghost<<<nblk(ncell, TPB), TPB, 0, st>>>(L, h.gridP(), s);
+        k_bflux2fld_ghost<<<nblk(ghost_cells(L), TPB), TPB, 0, st>>>(L, h.gridP(), s);
         h.launches++;
         if (h.p.doRing) launch_ring_bfix(h, s, st);
     }
