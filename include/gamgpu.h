@@ -345,6 +345,21 @@ int gam_closure_train(gam_closure_t* c, const int* slots, int n, float lr, doubl
 int gam_closure_eval(gam_closure_t* c, const int* slots, int n, double* loss, double* lossNone);
 /* rms over the active cells of a sample's residual per gas variable (rms[0..4]) and its dt (rms[5]) */
 int gam_closure_residual_rms(gam_closure_t* c, int slot, double* rms);
+/* Face targets. After each fine step of a sample (reset = 1 on its first), add weight (that step's dt) times
+ * the fine problem's interface fluxes, summed over the 2 x 2 fine sub-faces of every coarse face; the next
+ * capture then also stores the face target: the accumulation over the coarse dt minus the plain coarse
+ * step's flux, the correction that gives the coarse faces the restricted fine fluxes (exact for density and
+ * momentum, whose updates are flux divergences). The fine problem must run FP64. */
+int gam_closure_accum_fine(gam_closure_t* c, gam_gpu_t* fine, double weight, int reset);
+/* the loss gam_closure_train and gam_closure_eval minimise: the cell residual (default) or, with
+ * GAM_CLOSURE_LOSS_FACE, the mean over the lower faces of the active cells and the 24 outputs of
+ * (output - target / (fluxScale[v] * area))^2 */
+#define GAM_CLOSURE_LOSS_CELL 0
+#define GAM_CLOSURE_LOSS_FACE 1
+int gam_closure_set_loss(gam_closure_t* c, int mode);
+/* a slot's face targets: rms[0..7] the rms of target / area per flux; rel[0..4] the relative rms mismatch
+ * of dt / V * div(target) against the cell residual per gas variable */
+int gam_closure_face_stats(gam_closure_t* c, int slot, double* rms, double* rel);
 /* attach (c) or detach (NULL) the closure: every step adds its face corrections to the fluxes of State n
  * before Flux2Deltas; a step whose corrected update would make rho or P non-positive uses the plain
  * fluxes instead (counted by gam_gpu_closure_rejects). One handle per closure at a time. */

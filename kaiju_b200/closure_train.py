@@ -6,7 +6,10 @@ two fine steps apart, the step's dt is the next two fine steps, and the target i
 state at the end. The closure stores the net input of the coarse State and the residual
 restrict(fine) - plain coarse step. Training minimises, by Adam on the device (the net's own tensor-core
 forward and backward kernels), the mean over cells of sum_v ((dt/V * div(corrections)_v - residual_v) /
-rms_v)^2: the face corrections are fitted to what the plain coarse fluxes miss.
+rms_v)^2: the face corrections are fitted to what the plain coarse fluxes miss. With --loss face the
+samples also carry face targets -- the fine fluxes of the two fine steps, time-integrated and summed over
+the fine sub-faces of each coarse face, over the coarse dt, minus the plain coarse step's flux -- and the
+net is fitted to them face by face (the correction that gives the coarse faces the restricted fine fluxes).
 
 Evaluation on held-out seeds: (1) the same loss with the trained net against no correction (the gain of
 the net on one step); (2) rollouts to a common end time: the fine run, the plain coarse run and the coarse
@@ -56,8 +59,9 @@ def primitive_stats(g: gm.GameraGPU):
 
 
 def collect(closure: gm.Closure, n: int, seeds, per_seed: int, warm: int, gap: int, slot0: int = 0,
-            set_input_norm: bool = True):
-    """Samples from fine runs of each seed into consecutive slots from slot0; returns the slots."""
+            set_input_norm: bool = True, faces: bool = False):
+    """Samples from fine runs of each seed into consecutive slots from slot0; returns the slots. faces: also
+    accumulate the two fine steps' fluxes for each sample's face target."""
     coarse = tu.coarse_problem(n)
     slots = []
     slot = slot0
@@ -75,8 +79,13 @@ def collect(closure: gm.Closure, n: int, seeds, per_seed: int, warm: int, gap: i
             if set_input_norm and slot == 0:
                 closure.in_mean, closure.in_std = primitive_stats(coarse)
                 closure.set_norm(closure.in_mean, closure.in_std, np.ones(8), np.ones(5))
-            fine.step()
-            fine.step()
+            t_prev = tb
+            for q in range(2):
+                fine.step()
+                if faces:
+                    t_now = fine.status()["time"]
+                    closure.accum_fine(fine, t_now - t_prev, reset=(q == 0))
+                    t_prev = t_now
             tc = fine.status()["time"]
             coarse.set_scalars(tb, tc - tb, 0.0, 1, tb, ta)
             closure.capture(slot, coarse, fine)
@@ -104,7 +113,20 @@ def set_output_norm(closure: gm.Closure, n: int, slots):
     dt = float(np.mean(dts))
     flux = np.concatenate([rms, rms[1:4]]) * dx / dt
     closure.set_norm(closure.in_mean, closure.in_std, flux, rms)
+    closure.res_scale = rms
     return rms, flux
+
+
+def set_output_norm_faces(closure: gm.Closure, slots):
+    """Flux scale from the face targets: the rms over the samples of target / area per flux, so an O(1) net
+    output is a correction of the targets' size."""
+    acc = np.zeros(8)
+    for s in slots:
+        r, _ = closure.face_stats(s)
+        acc += r ** 2
+    flux = np.maximum(np.sqrt(acc / len(slots)), 1e-12)
+    closure.set_norm(closure.in_mean, closure.in_std, flux, closure.res_scale)
+    return flux
 
 
 def train(closure: gm.Closure, slots, epochs: int, lr: float, seed: int = 0, log=None):
@@ -260,10 +282,12 @@ def main(argv=None):
     ap.add_argument("--rollouts", type=int, default=2)
     ap.add_argument("--three-levels", type=int, default=0,
                     help="also evaluate this many held-out seeds against a truth run at 4n (needs (4n)^3 to fit)")
+    ap.add_argument("--loss", choices=["cell", "face"], default="face",
+                    help="fit the cell residual through the divergence, or the face targets directly")
     ap.add_argument("--out", default=None)
     a = ap.parse_args(argv)
     report = train_and_evaluate(a.n, _seeds(a.train_seeds), _seeds(a.eval_seeds), a.per_seed, a.epochs, a.lr,
-                                a.warm, a.gap, a.t_end, a.rollouts, three=a.three_levels)
+                                a.warm, a.gap, a.t_end, a.rollouts, three=a.three_levels, loss=a.loss)
     s = json.dumps(report, indent=1)
     if a.out:
         with open(a.out, "w") as f:
@@ -272,15 +296,21 @@ def main(argv=None):
 
 
 def train_and_evaluate(n, train_seeds, eval_seeds, per_seed, epochs, lr, warm, gap, t_end, rollouts, log=print,
-                       three=0):
+                       three=0, loss="cell"):
     t0 = time.perf_counter()
     closure = gm.Closure(n, n, n, seed=0)
     closure.reserve(per_seed * (len(train_seeds) + len(eval_seeds)))
+    faces = loss == "face"
     # the input normalisation comes from the first sample's restricted state
-    tr = collect(closure, n, train_seeds, per_seed, warm, gap, 0)
-    ev = collect(closure, n, eval_seeds, per_seed, warm, gap, len(tr), set_input_norm=False)
+    tr = collect(closure, n, train_seeds, per_seed, warm, gap, 0, faces=faces)
+    ev = collect(closure, n, eval_seeds, per_seed, warm, gap, len(tr), set_input_norm=False, faces=faces)
     t_data = time.perf_counter() - t0
     rms, flux = set_output_norm(closure, n, tr)
+    face_check = None
+    if faces:
+        flux = set_output_norm_faces(closure, tr)
+        closure.set_loss(gm.GAM_CLOSURE_LOSS_FACE)
+        face_check = closure.face_stats(tr[0])[1].tolist()
     before = closure.eval(ev)
     t1 = time.perf_counter()
     hist = train(closure, tr, epochs, lr, log=log)
@@ -293,7 +323,8 @@ def train_and_evaluate(n, train_seeds, eval_seeds, per_seed, epochs, lr, warm, g
     closure.close()
     return {
         "n_coarse": n, "n_fine": 2 * n, "train_seeds": list(train_seeds), "eval_seeds": list(eval_seeds),
-        "samples": {"train": len(tr), "eval": len(ev)}, "epochs": epochs, "lr": lr,
+        "samples": {"train": len(tr), "eval": len(ev)}, "epochs": epochs, "lr": lr, "loss": loss,
+        "face_target_vs_residual": face_check,
         "seconds": {"data": t_data, "train": t_train},
         "residual_rms": rms.tolist(), "flux_scale": flux.tolist(),
         "loss_history": hist,

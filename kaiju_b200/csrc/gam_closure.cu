@@ -48,6 +48,13 @@ struct gam_closure {
     std::vector<float*> sRes;
     std::vector<double> sDt;
     __nv_bfloat16* act0 = nullptr;   // the net's own input planes (act[0] is pointed at a sample in training)
+    // face targets: per slot the area-scaled correction that turns the plain coarse step's face fluxes into
+    // the restricted, time-integrated fine fluxes (24 float planes, made when the sample's fine steps were
+    // accumulated); fAcc sums dt_f x the restricted fine fluxes of those steps (24 double planes)
+    std::vector<float*> sFace;
+    double* fAcc = nullptr;
+    int fAccSteps = 0;
+    int lossMode = 0;   // GAM_CLOSURE_LOSS_CELL or GAM_CLOSURE_LOSS_FACE
 };
 
 namespace {
@@ -323,6 +330,154 @@ __global__ void k_loss_grad(Lay L, const float* w, const float* geom, NormP n, _
 
 inline unsigned nblk256(long long n) { return (unsigned)((n + 255) / 256); }
 
+// ---------------------------------------------------------------- face targets
+// Area-scaled interface fluxes of a solver, plane d*8+v: the 5 gas fluxes, then the 3 magnetic-stress
+// momentum fluxes, of direction d
+struct FluxPlanes { const double* f[24]; };
+FluxPlanes flux_planes(const Handle& h) {
+    FluxPlanes F;
+    for (int d = 0; d < 3; ++d) {
+        for (int v = 0; v < 5; ++v) F.f[d * 8 + v] = h.gflx[d][v];
+        for (int x = 0; x < 3; ++x) F.f[d * 8 + 5 + x] = h.mflx[d][x];
+    }
+    return F;
+}
+
+// the coarse face sites: lower faces of the active cells and the upper boundary faces; a d-face needs the
+// other two indices active
+__device__ __forceinline__ bool face_site(const Lay& L, long long t, int& i, int& j, int& k) {
+    const int ni = L.Nip + 1, nj = L.Njp + 1, nk = L.Nkp + 1;
+    if (t >= (long long)ni * nj * nk) return false;
+    i = L.is() + (int)(t % ni); j = L.js() + (int)((t / ni) % nj); k = L.ks() + (int)(t / ((long long)ni * nj));
+    return true;
+}
+__device__ __forceinline__ bool face_of_active(const Lay& L, int d, int i, int j, int k) {
+    return (d == 0 || i <= L.ie()) && (d == 1 || j <= L.je()) && (d == 2 || k <= L.ke());
+}
+
+// w x the fine fluxes through each coarse face (the sum over its 2 x 2 fine sub-faces) added into acc
+__global__ void k_accum_fine(Lay Lc, Lay Lf, FluxPlanes F, int nv, double w, double* acc) {
+    int i, j, k;
+    if (!face_site(Lc, blockIdx.x * (long long)blockDim.x + threadIdx.x, i, j, k)) return;
+    const long long c = Lc.at(i, j, k);
+    const int fi = Lf.is() + 2 * (i - Lc.is()), fj = Lf.js() + 2 * (j - Lc.js()), fk = Lf.ks() + 2 * (k - Lc.ks());
+    for (int d = 0; d < 3; ++d) {
+        if (!face_of_active(Lc, d, i, j, k)) continue;
+        long long sub[4];
+        for (int a = 0; a < 2; ++a)
+            for (int b = 0; b < 2; ++b)
+                sub[2 * a + b] = d == 0 ? Lf.at(fi, fj + a, fk + b) : d == 1 ? Lf.at(fi + a, fj, fk + b)
+                                                                           : Lf.at(fi + a, fj + b, fk);
+        for (int v = 0; v < nv; ++v) {
+            const double* q = F.f[d * 8 + v];
+            acc[(long long)(d * 8 + v) * Lc.E + c] += w * (q[sub[0]] + q[sub[1]] + q[sub[2]] + q[sub[3]]);
+        }
+    }
+}
+
+// target = acc / dt - (the plain coarse step's flux), per face site and direction
+__global__ void k_face_target(Lay L, const double* acc, double dt, FluxPlanes F, int nv, float* tgt) {
+    int i, j, k;
+    if (!face_site(L, blockIdx.x * (long long)blockDim.x + threadIdx.x, i, j, k)) return;
+    const long long c = L.at(i, j, k);
+    for (int d = 0; d < 3; ++d) {
+        if (!face_of_active(L, d, i, j, k)) continue;
+        for (int v = 0; v < 8; ++v) {
+            const long long o = (long long)(d * 8 + v) * L.E + c;
+            tgt[o] = v < nv ? (float)(acc[o] / dt - F.f[d * 8 + v][c]) : 0.f;
+        }
+    }
+}
+
+// face-target loss of one sample: over the lower d-faces of the active cells (a non-periodic boundary face
+// carries no correction), e = y - target / (fluxScale_v * area), L = mean of e^2 over faces and the 8
+// variables of 3 directions; the net-output gradient dL/dy = 2e / N goes to gout (when given); y = 0
+// without a net output
+__global__ void k_loss_face(Lay L, const float* out, const float* tgt, const float* geom, NormP n,
+                            __nv_bfloat16* gout, float* part) {
+    __shared__ float red[256];
+    const long long nact = (long long)L.Nip * L.Njp * L.Nkp;
+    const float N = (float)nact * 24.f;
+    float acc = 0.f;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < nact; t += (long long)gridDim.x * blockDim.x) {
+        const int idx[3] = {L.is() + (int)(t % L.Nip), L.js() + (int)((t / L.Nip) % L.Njp),
+                            L.ks() + (int)(t / ((long long)L.Nip * L.Njp))};
+        const int lo[3] = {L.is(), L.js(), L.ks()};
+        const long long c = L.at(idx[0], idx[1], idx[2]);
+        for (int d = 0; d < 3; ++d) {
+            const bool none = idx[d] == lo[d] && !n.per[d];
+            const float A = geom[(long long)(1 + d) * L.E + c];
+            for (int v = 0; v < 8; ++v) {
+                const long long o = (long long)(d * 8 + v) * L.E + c;
+                float e = 0.f;
+                if (!none) {
+                    const float y = out ? out[o] : 0.f;
+                    e = y - tgt[o] / (n.fluxScale[v] * A);
+                    acc += e * e;
+                }
+                if (gout) gout[c * NET_PITCH + d * 8 + v] = __float2bfloat16_rn(2.f * e / N);
+            }
+        }
+    }
+    red[threadIdx.x] = acc / N;
+    __syncthreads();
+    for (int s2 = blockDim.x / 2; s2 > 0; s2 >>= 1) {
+        if (threadIdx.x < s2) red[threadIdx.x] += red[threadIdx.x + s2];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) part[blockIdx.x] = red[0];
+}
+
+// statistics of one sample's face targets: acc[0..7] sums of (target_v / area)^2 over the lower faces of the
+// active cells; acc[8..12] sums of (dt / V * div(target)_v - residual_v)^2 and acc[13..17] of residual_v^2
+// (how closely the face targets account for the cell residual)
+__global__ void k_face_stats(Lay L, const float* tgt, const float* res, const float* geom, double dt, double* acc) {
+    __shared__ double red[18][128];
+    double s[18];
+    for (int q = 0; q < 18; ++q) s[q] = 0.0;
+    const long long nact = (long long)L.Nip * L.Njp * L.Nkp;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < nact; t += (long long)gridDim.x * blockDim.x) {
+        const int i = L.is() + (int)(t % L.Nip), j = L.js() + (int)((t / L.Nip) % L.Njp),
+                  k = L.ks() + (int)(t / ((long long)L.Nip * L.Njp));
+        const long long c = L.at(i, j, k);
+        const long long nb[3] = {c + 1, c + L.P, c + (long long)L.P * L.Q};
+        for (int d = 0; d < 3; ++d) {
+            const double A = geom[(long long)(1 + d) * L.E + c];
+            for (int v = 0; v < 8; ++v) {
+                const double y = tgt[(long long)(d * 8 + v) * L.E + c] / A;
+                s[v] += y * y;
+            }
+        }
+        double dU[5];
+        for (int v = 0; v < 5; ++v) {
+            double q = 0.0;
+            for (int d = 0; d < 3; ++d) {
+                const float* f = tgt + (long long)(d * 8 + v) * L.E;
+                q += (double)f[c] - (double)f[nb[d]];
+            }
+            dU[v] = q;
+        }
+        for (int x = 0; x < 3; ++x)
+            for (int d = 0; d < 3; ++d) {
+                const float* f = tgt + (long long)(d * 8 + 5 + x) * L.E;
+                dU[1 + x] += (double)f[c] - (double)f[nb[d]];
+            }
+        const double fV = dt / geom[c];
+        for (int v = 0; v < 5; ++v) {
+            const double r = res[(long long)v * L.E + c], e = fV * dU[v] - r;
+            s[8 + v] += e * e;
+            s[13 + v] += r * r;
+        }
+    }
+    for (int q = 0; q < 18; ++q) red[q][threadIdx.x] = s[q];
+    __syncthreads();
+    if (threadIdx.x < 18) {
+        double a = 0.0;
+        for (int b = 0; b < (int)blockDim.x; ++b) a += red[threadIdx.x][b];
+        atomicAdd(&acc[threadIdx.x], a);
+    }
+}
+
 // sums of the residual squares per gas variable over the active cells (statistics for the normalisation)
 __global__ void k_res_sq(Lay L, const float* res, double* acc) {
     __shared__ double red[5][256];
@@ -445,6 +600,8 @@ void gam_closure_destroy(gam_closure_t* C) {
     cudaFree(C->corr); cudaFree(C->geom); cudaFree(C->wts); cudaFree(C->lossAcc); cudaFree(C->lossPart);
     for (auto* q : C->sIn) cudaFree(q);
     for (auto* q : C->sRes) cudaFree(q);
+    for (auto* q : C->sFace) cudaFree(q);
+    cudaFree(C->fAcc);
     if (C->stream) cudaStreamDestroy(C->stream);
     delete C;
 }
@@ -577,6 +734,7 @@ int gam_closure_reserve(gam_closure_t* C, int n) {
         C->sIn.push_back(in);
         C->sRes.push_back(res);
         C->sDt.push_back(0.0);
+        C->sFace.push_back(nullptr);   // made by a capture that follows accumulated fine steps
     }
     CKC(cudaStreamSynchronize(C->stream));
     return GAM_OK;
@@ -605,7 +763,65 @@ int gam_closure_capture(gam_closure_t* C, int slot, gam_gpu_t* coarse, gam_gpu_t
     CKC(cudaStreamSynchronize(hf.stream));
     k_closure_residual<<<nblk256((long long)L.Nip * L.Njp * L.Nkp), 256, 0, hc.stream>>>(
         L, hf.L, hf.S[hf.cur], hf.volume, hc.S[hc.cur], C->sRes[slot]);
+    if (C->fAccSteps > 0) {   // the fine steps of this sample were accumulated: its face target
+        if (hc.prec != PREC_FP64) return GAM_ERR_ARG;
+        if (!C->sFace[slot]) {
+            CKC(cudaMalloc(&C->sFace[slot], sizeof(float) * L.E * NET_OUT));
+            CKC(cudaMemsetAsync(C->sFace[slot], 0, sizeof(float) * L.E * NET_OUT, hc.stream));
+        }
+        CKC(cudaStreamSynchronize(C->stream));
+        k_face_target<<<nblk256((long long)(L.Nip + 1) * (L.Njp + 1) * (L.Nkp + 1)), 256, 0, hc.stream>>>(
+            L, C->fAcc, C->sDt[slot], flux_planes(hc), hc.p.doMHD ? 8 : 5, C->sFace[slot]);
+        C->fAccSteps = 0;
+    }
     CKC(cudaStreamSynchronize(hc.stream));
+    return GAM_OK;
+}
+
+// dt_f x the fine fluxes of the fine handle's last step, restricted to the coarse faces, added to the
+// accumulation of the next capture's sample (reset: start a new sample)
+int gam_closure_accum_fine(gam_closure_t* C, gam_gpu_t* fine, double weight, int reset) {
+    if (!C || !fine) return GAM_ERR_ARG;
+    Handle& hf = capi_handle(fine);
+    const Lay& L = C->L;
+    if (hf.L.Nip != 2 * L.Nip || hf.L.Njp != 2 * L.Njp || hf.L.Nkp != 2 * L.Nkp || hf.prec != PREC_FP64)
+        return GAM_ERR_ARG;
+    if (!C->fAcc) {
+        CKC(cudaMalloc(&C->fAcc, sizeof(double) * L.E * NET_OUT));
+        reset = 1;
+    }
+    CKC(cudaStreamSynchronize(hf.stream));
+    if (reset || C->fAccSteps == 0) CKC(cudaMemsetAsync(C->fAcc, 0, sizeof(double) * L.E * NET_OUT, C->stream));
+    k_accum_fine<<<nblk256((long long)(L.Nip + 1) * (L.Njp + 1) * (L.Nkp + 1)), 256, 0, C->stream>>>(
+        L, hf.L, flux_planes(hf), hf.p.doMHD ? 8 : 5, weight, C->fAcc);
+    C->fAccSteps = (reset ? 0 : C->fAccSteps) + 1;
+    CKC(cudaStreamSynchronize(C->stream));
+    return GAM_OK;
+}
+
+int gam_closure_set_loss(gam_closure_t* C, int mode) {
+    if (!C || (mode != GAM_CLOSURE_LOSS_CELL && mode != GAM_CLOSURE_LOSS_FACE)) return GAM_ERR_ARG;
+    C->lossMode = mode;
+    return GAM_OK;
+}
+
+// rms[0..7]: rms of the slot's face targets over area (per variable, lower faces of the active cells);
+// rel[0..4]: || dt / V * div(target) - residual || / || residual || per gas variable
+int gam_closure_face_stats(gam_closure_t* C, int slot, double* rms, double* rel) {
+    if (!C || !rms || !rel || slot < 0 || slot >= (int)C->sIn.size() || !C->sFace[slot] || !C->haveGeom)
+        return GAM_ERR_ARG;
+    double* acc = nullptr;
+    CKC(cudaMalloc(&acc, sizeof(double) * 18));
+    cudaMemsetAsync(acc, 0, sizeof(double) * 18, C->stream);
+    k_face_stats<<<256, 128, 0, C->stream>>>(C->L, C->sFace[slot], C->sRes[slot], C->geom, C->sDt[slot], acc);
+    double h[18];
+    cudaMemcpyAsync(h, acc, sizeof(h), cudaMemcpyDeviceToHost, C->stream);
+    cudaError_t e = cudaStreamSynchronize(C->stream);
+    cudaFree(acc);
+    if (e != cudaSuccess) return GAM_ERR_CUDA;
+    const double n = 3.0 * C->L.Nip * C->L.Njp * C->L.Nkp;
+    for (int v = 0; v < 8; ++v) rms[v] = std::sqrt(h[v] / n);
+    for (int v = 0; v < 5; ++v) rel[v] = h[13 + v] > 0 ? std::sqrt(h[8 + v] / h[13 + v]) : 0.0;
     return GAM_OK;
 }
 
@@ -616,13 +832,20 @@ static int closure_sample_pass(gam_closure* C, int slot, bool train, float lr) {
     C->nb.act[0] = C->sIn[slot];
     if (net_forward(C->box, C->wfwd, C->params, C->nb, train, C->err, C->stream) != 0) return GAM_ERR_CUDA;
     const long long nf = (long long)(L.Nip + 1) * (L.Njp + 1) * (L.Nkp + 1);
-    k_closure_corr<<<nblk256(nf), 256, 0, C->stream>>>(L, C->nb.out, n, C->geom, C->corr);
     const int nb = 1024;
-    k_loss_w<<<nb, 256, 0, C->stream>>>(L, C->corr, C->sRes[slot], C->geom, n, C->sDt[slot], C->wts, C->lossPart);
-    k_loss_sum<<<1, 32, 0, C->stream>>>(C->lossPart, nb, C->lossAcc);
+    if (C->lossMode == GAM_CLOSURE_LOSS_FACE) {
+        k_loss_face<<<nb, 256, 0, C->stream>>>(L, C->nb.out, C->sFace[slot], C->geom, n,
+                                               train ? C->nb.grad[NET_LAYERS - 1] : nullptr, C->lossPart);
+        k_loss_sum<<<1, 32, 0, C->stream>>>(C->lossPart, nb, C->lossAcc);
+    } else {
+        k_closure_corr<<<nblk256(nf), 256, 0, C->stream>>>(L, C->nb.out, n, C->geom, C->corr);
+        k_loss_w<<<nb, 256, 0, C->stream>>>(L, C->corr, C->sRes[slot], C->geom, n, C->sDt[slot], C->wts, C->lossPart);
+        k_loss_sum<<<1, 32, 0, C->stream>>>(C->lossPart, nb, C->lossAcc);
+    }
     if (train) {
-        k_loss_grad<<<nblk256((long long)L.Nip * L.Njp * L.Nkp), 256, 0, C->stream>>>(L, C->wts, C->geom, n,
-                                                                                       C->nb.grad[NET_LAYERS - 1]);
+        if (C->lossMode != GAM_CLOSURE_LOSS_FACE)
+            k_loss_grad<<<nblk256((long long)L.Nip * L.Njp * L.Nkp), 256, 0, C->stream>>>(L, C->wts, C->geom, n,
+                                                                                           C->nb.grad[NET_LAYERS - 1]);
         if (net_backward(C->box, C->wbwd, C->nb, C->grads, C->err, C->stream) != 0) return GAM_ERR_CUDA;
         C->adamStep++;
         if (net_adam(C->params, C->grads, C->m, C->v, C->np, lr, 0.9f, 0.999f, 1e-8f, C->adamStep, C->stream) != 0)
@@ -637,7 +860,9 @@ static int closure_sample_pass(gam_closure* C, int slot, bool train, float lr) {
 int gam_closure_train(gam_closure_t* C, const int* slots, int n, float lr, double* meanLoss) {
     if (!C || !slots || n < 1 || !(lr > 0.f) || !C->haveGeom) return GAM_ERR_ARG;
     for (int q = 0; q < n; ++q)
-        if (slots[q] < 0 || slots[q] >= (int)C->sIn.size()) return GAM_ERR_ARG;
+        if (slots[q] < 0 || slots[q] >= (int)C->sIn.size() ||
+            (C->lossMode == GAM_CLOSURE_LOSS_FACE && !C->sFace[slots[q]]))
+            return GAM_ERR_ARG;
     CKC(cudaMemsetAsync(C->lossAcc, 0, sizeof(double) * 2, C->stream));
     for (int q = 0; q < n; ++q) {
         int rc = closure_sample_pass(C, slots[q], true, lr);
@@ -655,7 +880,9 @@ int gam_closure_train(gam_closure_t* C, const int* slots, int n, float lr, doubl
 int gam_closure_eval(gam_closure_t* C, const int* slots, int n, double* loss, double* lossNone) {
     if (!C || !slots || n < 1 || !C->haveGeom) return GAM_ERR_ARG;
     for (int q = 0; q < n; ++q)
-        if (slots[q] < 0 || slots[q] >= (int)C->sIn.size()) return GAM_ERR_ARG;
+        if (slots[q] < 0 || slots[q] >= (int)C->sIn.size() ||
+            (C->lossMode == GAM_CLOSURE_LOSS_FACE && !C->sFace[slots[q]]))
+            return GAM_ERR_ARG;
     const Lay& L = C->L;
     NormP nrm = norm_of(C);
     double acc[2] = {0, 0};
@@ -665,6 +892,10 @@ int gam_closure_eval(gam_closure_t* C, const int* slots, int n, double* loss, do
             if (pass == 0) {
                 int rc = closure_sample_pass(C, slots[q], false, 0.f);
                 if (rc) return rc;
+            } else if (C->lossMode == GAM_CLOSURE_LOSS_FACE) {   // no correction: the targets alone
+                k_loss_face<<<1024, 256, 0, C->stream>>>(L, nullptr, C->sFace[slots[q]], C->geom, nrm, nullptr,
+                                                         C->lossPart);
+                k_loss_sum<<<1, 32, 0, C->stream>>>(C->lossPart, 1024, C->lossAcc);
             } else {   // no correction: the residual alone
                 CKC(cudaMemsetAsync(C->corr, 0, sizeof(float) * L.E * NET_OUT, C->stream));
                 k_loss_w<<<1024, 256, 0, C->stream>>>(L, C->corr, C->sRes[slots[q]], C->geom, nrm, C->sDt[slots[q]],

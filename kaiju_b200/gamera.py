@@ -33,6 +33,7 @@ GAM_IC_OT2D, GAM_IC_BW, GAM_IC_LFMBW, GAM_IC_KH = 0, 1, 2, 3
 GAM_SLICE_FAT = 1
 GAM_B0_UNIFORM, GAM_B0_DIPOLE = 1, 2
 GAM_TILE_FLUX_ROWS, GAM_TILE_FUSED_UPDATE, GAM_TILE_TMA = 1, 2, 3
+GAM_CLOSURE_LOSS_CELL, GAM_CLOSURE_LOSS_FACE = 0, 1
 TINY, HUGE = 1.0e-12, 1.0e12
 
 
@@ -141,6 +142,9 @@ SIGNATURES = {
     "gam_closure_train": (C.c_int, [C.c_void_p, C.POINTER(C.c_int), C.c_int, C.c_float, _DP]),
     "gam_closure_eval": (C.c_int, [C.c_void_p, C.POINTER(C.c_int), C.c_int, _DP, _DP]),
     "gam_closure_residual_rms": (C.c_int, [C.c_void_p, C.c_int, _DP]),
+    "gam_closure_accum_fine": (C.c_int, [C.c_void_p, C.c_void_p, C.c_double, C.c_int]),
+    "gam_closure_set_loss": (C.c_int, [C.c_void_p, C.c_int]),
+    "gam_closure_face_stats": (C.c_int, [C.c_void_p, C.c_int, _DP, _DP]),
     "gam_gpu_set_closure": (C.c_int, [C.c_void_p, C.c_void_p]),
     "gam_gpu_closure_rejects": (C.c_int, [C.c_void_p, C.POINTER(C.c_int)]),
     "gam_gpu_restrict": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint]),
@@ -746,6 +750,20 @@ class Closure:
         out = np.zeros(6)
         self._call("gam_closure_residual_rms", slot, out.ctypes.data_as(_DP))
         return out[:5], out[5]
+
+    def accum_fine(self, fine: "GameraGPU", weight: float, reset: bool = False):
+        """Add weight x the fine problem's last-step fluxes, restricted to the coarse faces, to the next
+        capture's face target (gam_closure_accum_fine)."""
+        self._call("gam_closure_accum_fine", fine.h, float(weight), int(reset))
+
+    def set_loss(self, mode: int):
+        self._call("gam_closure_set_loss", int(mode))
+
+    def face_stats(self, slot: int):
+        """(rms of target / area per flux [8], relative mismatch of dt/V div(target) vs the residual [5])"""
+        rms, rel = np.zeros(8), np.zeros(5)
+        self._call("gam_closure_face_stats", slot, rms.ctypes.data_as(_DP), rel.ctypes.data_as(_DP))
+        return rms, rel
 
     def train(self, slots, lr: float) -> float:
         arr = (C.c_int * len(slots))(*slots)
