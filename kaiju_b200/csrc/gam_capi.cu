@@ -16,8 +16,11 @@ using namespace gam;
 
 struct gam_gpu {
     Handle h;
-    double* stage = nullptr;        // contiguous staging for Fortran<->pencil repacking
+    double* stage = nullptr;        // contiguous staging for Fortran<->pencil repacking (two buffers that
+    double* stage2 = nullptr;       // alternate, copies on xfer, repacking on the step stream)
     size_t stagePlanes = 0;
+    cudaStream_t xfer = nullptr;
+    cudaEvent_t xferEv[2] = {}, packEv[2] = {};
     double* scratch = nullptr;      // reduction partials
     size_t scratchDoubles = 0;
     int lastStatus = 0;
@@ -67,11 +70,25 @@ struct Ext { int ni, nj, nk; long long n() const { return (long long)ni * nj * n
 Ext cellExt(const Lay& L) { return {L.Ni, L.Nj, L.Nk}; }
 Ext faceExt(const Lay& L) { return {L.Ni + 1, L.Nj + 1, L.Nk + 1}; }
 
+// Host <-> device planes: the host copies run on their own stream through two staging buffers that
+// alternate, so the repacking of one plane (on the step stream) overlaps the host copy of the next; events
+// order each buffer's copy after its previous reader and each repack after its copy. When these return,
+// the step stream is ordered after every copy.
 int h2d_planes(gam_gpu* G, double* const* planes, int np, const double* host, Ext e) {
     Handle& h = G->h;
+    double* const st[2] = {G->stage, G->stage2};
+    const size_t bytes = sizeof(double) * e.n();
+    // a buffer's last reader so far is earlier work on the step stream
+    CK(cudaEventRecord(G->packEv[0], h.stream));
+    CK(cudaEventRecord(G->packEv[1], h.stream));
     for (int q = 0; q < np; ++q) {
-        CK(cudaMemcpyAsync(G->stage, host + q * e.n(), sizeof(double) * e.n(), cudaMemcpyHostToDevice, h.stream));
-        k_pack_in<<<(unsigned)((e.n() + 255) / 256), 256, 0, h.stream>>>(h.L, planes[q], G->stage, e.ni, e.nj, e.nk);
+        const int b = q & 1;
+        CK(cudaStreamWaitEvent(G->xfer, G->packEv[b], 0));
+        CK(cudaMemcpyAsync(st[b], host + q * e.n(), bytes, cudaMemcpyHostToDevice, G->xfer));
+        CK(cudaEventRecord(G->xferEv[b], G->xfer));
+        CK(cudaStreamWaitEvent(h.stream, G->xferEv[b], 0));
+        k_pack_in<<<(unsigned)((e.n() + 255) / 256), 256, 0, h.stream>>>(h.L, planes[q], st[b], e.ni, e.nj, e.nk);
+        CK(cudaEventRecord(G->packEv[b], h.stream));
         h.launches++;
     }
     CK(cudaGetLastError());
@@ -79,11 +96,19 @@ int h2d_planes(gam_gpu* G, double* const* planes, int np, const double* host, Ex
 }
 int d2h_planes(gam_gpu* G, double* const* planes, int np, double* host, Ext e) {
     Handle& h = G->h;
+    double* const st[2] = {G->stage, G->stage2};
+    const size_t bytes = sizeof(double) * e.n();
     for (int q = 0; q < np; ++q) {
-        k_pack_out<<<(unsigned)((e.n() + 255) / 256), 256, 0, h.stream>>>(h.L, G->stage, planes[q], e.ni, e.nj, e.nk);
+        const int b = q & 1;
+        if (q >= 2) CK(cudaStreamWaitEvent(h.stream, G->xferEv[b], 0));   // the buffer's copy of plane q-2 is done
+        k_pack_out<<<(unsigned)((e.n() + 255) / 256), 256, 0, h.stream>>>(h.L, st[b], planes[q], e.ni, e.nj, e.nk);
+        CK(cudaEventRecord(G->packEv[b], h.stream));
         h.launches++;
-        CK(cudaMemcpyAsync(host + q * e.n(), G->stage, sizeof(double) * e.n(), cudaMemcpyDeviceToHost, h.stream));
+        CK(cudaStreamWaitEvent(G->xfer, G->packEv[b], 0));
+        CK(cudaMemcpyAsync(host + q * e.n(), st[b], bytes, cudaMemcpyDeviceToHost, G->xfer));
+        CK(cudaEventRecord(G->xferEv[b], G->xfer));
     }
+    for (int b = 0; b < 2 && b < np; ++b) CK(cudaStreamWaitEvent(h.stream, G->xferEv[b], 0));
     CK(cudaGetLastError());
     return GAM_OK;
 }
@@ -224,6 +249,12 @@ int alloc_handle(gam_gpu* G, const gam_model_c* m) {
 
     Ext fe = faceExt(L);
     CK(cudaMalloc(&G->stage, sizeof(double) * fe.n()));
+    CK(cudaMalloc(&G->stage2, sizeof(double) * fe.n()));
+    CK(cudaStreamCreateWithFlags(&G->xfer, cudaStreamNonBlocking));
+    for (int b = 0; b < 2; ++b) {
+        CK(cudaEventCreateWithFlags(&G->xferEv[b], cudaEventDisableTiming));
+        CK(cudaEventCreateWithFlags(&G->packEv[b], cudaEventDisableTiming));
+    }
     G->scratchDoubles = (size_t)((long long)L.Nip * L.Njp * L.Nkp / 256 + 1024);
     CK(cudaMalloc(&G->scratch, sizeof(double) * G->scratchDoubles));
     CK(cudaMalloc(&h.dScal, sizeof(Scal)));
@@ -747,7 +778,14 @@ void gam_gpu_destroy(gam_gpu_t* G) {
     if (h.bgpool) cudaFree(h.bgpool);
     if (h.ringpool) cudaFree(h.ringpool);
     if (h.f32pool) cudaFree(h.f32pool);
+    if (G->xfer) cudaStreamSynchronize(G->xfer);
     if (G->stage) cudaFree(G->stage);
+    if (G->stage2) cudaFree(G->stage2);
+    for (int b = 0; b < 2; ++b) {
+        if (G->xferEv[b]) cudaEventDestroy(G->xferEv[b]);
+        if (G->packEv[b]) cudaEventDestroy(G->packEv[b]);
+    }
+    if (G->xfer) cudaStreamDestroy(G->xfer);
     if (G->scratch) cudaFree(G->scratch);
     if (G->copyStream) cudaStreamSynchronize(G->copyStream);
     if (G->iobuf) cudaFree(G->iobuf);
