@@ -107,9 +107,6 @@ __device__ __forceinline__ double dmax(double a, double b) { return (a > b) ? a 
 __device__ __forceinline__ double dmin(double a, double b) { return (a < b) ? a : b; }
 
 // recon.F90:22-32 -- weights are integer/840 (exact sum 1) and integer/420
-struct W8 {
-    double w[8];
-};
 __device__ __forceinline__ double wC8(int n) {
     const double c[8] = {-3.0 / 840.0, 29.0 / 840.0, -139.0 / 840.0, 533.0 / 840.0,
                          533.0 / 840.0, -139.0 / 840.0, 29.0 / 840.0, -3.0 / 840.0};

@@ -1,5 +1,6 @@
 // Kernel-side helpers shared by the step kernels: launch regions, pointer bundles, the one-sided
-// kinetic fluxes, and cooperative staging of a box of a pencil plane into shared memory.
+// kinetic fluxes, and row-wise cp.async staging of a box of a pencil plane into shared memory (the
+// variant the tile kernels use where tensor copies do not apply; gam_tma.cuh has the tensor copies).
 #pragma once
 #include <vector>
 #include "gam_common.cuh"
@@ -160,25 +161,6 @@ __device__ __forceinline__ void magKin(const Par& p, T sg, const T* W, const T* 
     }
 }
 
-// Cooperative copy of the box [bi0,bi0+ni) x [bj0,bj0+nj) x [bk0,bk0+nk) of one pencil plane into
-// shared memory (i fastest), converting to T. Elements outside the allocated index range are zero;
-// they only ever feed interfaces/edges outside the launch region.
-template <typename T>
-__device__ __forceinline__ void stage_box(T* dst, const double* __restrict__ src, const Lay& L, int bi0, int ni, int bj0,
-                                          int nj, int bk0, int nk, int tid, int nth) {
-    int n = ni * nj * nk;
-    for (int t = tid; t < n; t += nth) {
-        int a = t % ni;
-        int q = t / ni;
-        int b = q % nj;
-        int c = q / nj;
-        int i = bi0 + a, j = bj0 + b, k = bk0 + c;
-        T v = T(0);
-        if (i >= 0 && i <= L.Ni && j >= 0 && j <= L.Nj && k >= 0 && k <= L.Nk) v = T(__ldg(&src[L.at(i, j, k)]));
-        dst[t] = v;
-    }
-}
-
 // Asynchronous global->shared copies (cp.async, 8 bytes each): every thread keeps all of its copies in
 // flight at once instead of one load at a time.
 __device__ __forceinline__ void cp_async8(void* smem, const void* gmem) {
@@ -186,21 +168,6 @@ __device__ __forceinline__ void cp_async8(void* smem, const void* gmem) {
     asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(sa), "l"(gmem) : "memory");
 }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
-
-// stage_box with cp.async for double planes; the caller waits with cp_async_wait_all + __syncthreads
-__device__ __forceinline__ void stage_box_async(double* dst, const double* __restrict__ src, const Lay& L, int bi0,
-                                                int ni, int bj0, int nj, int bk0, int nk, int tid, int nth) {
-    int n = ni * nj * nk;
-    for (int t = tid; t < n; t += nth) {
-        int a = t % ni;
-        int q = t / ni;
-        int b = q % nj;
-        int c = q / nj;
-        int i = bi0 + a, j = bj0 + b, k = bk0 + c;
-        if (i >= 0 && i <= L.Ni && j >= 0 && j <= L.Nj && k >= 0 && k <= L.Nk) cp_async8(dst + t, src + L.at(i, j, k));
-        else dst[t] = 0.0;
-    }
-}
 
 __device__ __forceinline__ void cp_async4(void* smem, const void* gmem) {
     unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
