@@ -169,9 +169,11 @@ __device__ __forceinline__ T PDM(T pdmb, T q0, T q1, T q2, T qI) {
 }
 
 // GetLRs on one interface: dV[8] volumes, Q[8] values (stencil cells f-4..f+3), nQ[4] limiter values
-// (cells f-2..f+1), Vi = Central8(dV). Cen8LRs (recon.F90:125-158) or Up7LRs (:162-198).
+// (cells f-2..f+1), iVi = 1 / Central8(dV): the reference divides each variable's sum by Central8(dV);
+// here one reciprocal per interface serves all of them (the results differ by an ulp or so).
+// Cen8LRs (recon.F90:125-158) or Up7LRs (:162-198).
 template <typename T>
-__device__ __forceinline__ void getLR(int rmeth, T pdmb, const T* dV, const T* Q, const T* nQ, T Vi, T& Ql, T& Qr) {
+__device__ __forceinline__ void getLR(int rmeth, T pdmb, const T* dV, const T* Q, const T* nQ, T iVi, T& Ql, T& Qr) {
     T QdV[8];
 #pragma unroll
     for (int n = 0; n < 8; ++n) QdV[n] = dV[n] * Q[n];
@@ -179,15 +181,15 @@ __device__ __forceinline__ void getLR(int rmeth, T pdmb, const T* dV, const T* Q
         T s = T(0);
 #pragma unroll
         for (int n = 0; n < 8; ++n) s = s + T(wC8(n)) * QdV[n];
-        T Qi = s / Vi;
+        T Qi = s * iVi;
         pdmLR<T>(pdmb, nQ[0], nQ[1], nQ[2], nQ[3], Qi, Ql, Qr);
     } else {
         T l = QdV[0] * T(wU7(0)) + QdV[1] * T(wU7(1)) + QdV[2] * T(wU7(2)) + QdV[3] * T(wU7(3)) +
               QdV[4] * T(wU7(4)) + QdV[5] * T(wU7(5)) + QdV[6] * T(wU7(6));
         T r = QdV[7] * T(wU7(0)) + QdV[6] * T(wU7(1)) + QdV[5] * T(wU7(2)) + QdV[4] * T(wU7(3)) +
               QdV[3] * T(wU7(4)) + QdV[2] * T(wU7(5)) + QdV[1] * T(wU7(6));
-        Ql = PDM<T>(pdmb, nQ[0], nQ[1], nQ[2], l / Vi);
-        Qr = PDM<T>(pdmb, nQ[3], nQ[2], nQ[1], r / Vi);
+        Ql = PDM<T>(pdmb, nQ[0], nQ[1], nQ[2], l * iVi);
+        Qr = PDM<T>(pdmb, nQ[3], nQ[2], nQ[1], r * iVi);
     }
 }
 

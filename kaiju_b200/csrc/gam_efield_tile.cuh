@@ -136,7 +136,8 @@ k_edge_tile(Lay L, Par p, const __grid_constant__ EdgeMaps maps, EdgeSrc<S> in, 
     }
     T fA1 = central8<T>(Ab);
     T dA = fA1 > T(TINY) ? fA1 : T(TINY);
-    Vc0 = Vc0 / dA; Vc1 = Vc1 / dA; Vc2 = Vc2 / dA;
+    T idA = T(1) / dA;   // one reciprocal where the reference divides three times
+    Vc0 = Vc0 * idA; Vc1 = Vc1 * idA; Vc2 = Vc2 * idA;
     T v1 = Vc0 * T(__ldg(&in.Te[ED][0][c])) + Vc1 * T(__ldg(&in.Te[ED][1][c])) + Vc2 * T(__ldg(&in.Te[ED][2][c]));
     T v2 = Vc0 * T(__ldg(&in.Te[ED][3][c])) + Vc1 * T(__ldg(&in.Te[ED][4][c])) + Vc2 * T(__ldg(&in.Te[ED][5][c]));
     T vDiff = sqrt(v1 * v1 + v2 * v2);
@@ -162,7 +163,8 @@ k_edge_tile(Lay L, Par p, const __grid_constant__ EdgeMaps maps, EdgeSrc<S> in, 
     }
     T pdmb = T(p.pdmb);
     T l1, r1;
-    getLR<T>(p.rmeth, pdmb, Ab, Bb, nBb, fA1, l1, r1);
+    const T ifA1 = T(1) / fA1;
+    getLR<T>(p.rmeth, pdmb, Ab, Bb, nBb, ifA1, l1, r1);
     T bT1L = l1 * fA1, bT1R = r1 * fA1;
     // ... and of the dT2 faces along dT1
     T A2[8], B2[8], nB2[4];
@@ -181,16 +183,17 @@ k_edge_tile(Lay L, Par p, const __grid_constant__ EdgeMaps maps, EdgeSrc<S> in, 
         nB2[m] = T(sm[TL::oN2 + bidx(b4t1, di, dj, dk)]);
     }
     T fA2 = central8<T>(A2);
+    const T ifA2 = T(1) / fA2;
     T l2, r2;
-    getLR<T>(p.rmeth, pdmb, A2, B2, nB2, fA2, l2, r2);
+    getLR<T>(p.rmeth, pdmb, A2, B2, nB2, ifA2, l2, r2);
     T bT2L = l2 * fA2, bT2R = r2 * fA2;
     T xni = T(__ldg(&in.Teb[ED][0][c])), yni = T(__ldg(&in.Teb[ED][1][c]));
     T xnj = T(__ldg(&in.Teb[ED][2][c])), ynj = T(__ldg(&in.Teb[ED][3][c]));
     T detT = T(1) / (xni * ynj - xnj * yni);
-    T bT1 = T(0.5) * (bT1L + bT1R) / fA1;
-    T bT2 = T(0.5) * (bT2L + bT2R) / fA2;
-    T db1 = (bT1R - bT1L) / fA1;
-    T db2 = (bT2R - bT2L) / fA2;
+    T bT1 = T(0.5) * (bT1L + bT1R) * ifA1;
+    T bT2 = T(0.5) * (bT2L + bT2R) * ifA2;
+    T db1 = (bT1R - bT1L) * ifA1;
+    T db2 = (bT2R - bT2L) * ifA2;
     T Jd = db2 - db1;
     T b1 = detT * (ynj * bT1 - yni * bT2);
     T b2 = detT * (-(xnj * bT1) + xni * bT2);
@@ -199,8 +202,8 @@ k_edge_tile(Lay L, Par p, const __grid_constant__ EdgeMaps maps, EdgeSrc<S> in, 
         b2 = b2 + T(__ldg(&in.edgB0[ED][1][c]));
     }
     // diffusive speed and EMF (fields.F90:204-221)
-    T vA = sqrt(b1 * b1 + b2 * b2) / sqrt(Dc);
-    if (p.doBoris) { T Ca = T(p.Ca); vA = Ca * vA / sqrt(Ca * Ca + vA * vA); }
+    T vA = sqrt(b1 * b1 + b2 * b2) * rsq(Dc);
+    if (p.doBoris) { T Ca = T(p.Ca); vA = Ca * vA * rsq(Ca * Ca + vA * vA); }
     vDiff = vDiff + vA;
     double edg = double(__ldg(&in.edge[ED][c]));
     T lim = T(p.CFL * edg / sc->dt);

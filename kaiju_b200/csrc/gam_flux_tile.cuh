@@ -95,7 +95,7 @@ __device__ __forceinline__ void flux_tile_body(const Lay& L, const Par& p, const
     T Vol[8];
 #pragma unroll
     for (int m = 0; m < 8; ++m) Vol[m] = T(sRec[5 * RB + ro(m)]);
-    T Vi = central8<T>(Vol);
+    T iVi = T(1) / central8<T>(Vol);
     T pdmb = T(p.pdmb);
     T WL[5], WR[5];
 #pragma unroll
@@ -105,7 +105,7 @@ __device__ __forceinline__ void flux_tile_body(const Lay& L, const Par& p, const
         for (int m = 0; m < 8; ++m) Q[m] = T(sRec[v * RB + ro(m)]);
 #pragma unroll
         for (int m = 0; m < 4; ++m) nQ[m] = T(sLim[v * LB + lo(m)]);
-        getLR<T>(p.rmeth, pdmb, Vol, Q, nQ, Vi, WL[v], WR[v]);
+        getLR<T>(p.rmeth, pdmb, Vol, Q, nQ, iVi, WL[v], WR[v]);
     }
     T Tf[9];
 #pragma unroll
@@ -121,7 +121,7 @@ __device__ __forceinline__ void flux_tile_body(const Lay& L, const Par& p, const
             for (int m = 0; m < 8; ++m) Q[m] = T(sRec[(6 + x) * RB + ro(m)]);
 #pragma unroll
             for (int m = 0; m < 4; ++m) nQ[m] = T(sLim[(5 + x) * LB + lo(m)]);
-            getLR<T>(p.rmeth, pdmb, Vol, Q, nQ, Vi, BL[x], BR[x]);
+            getLR<T>(p.rmeth, pdmb, Vol, Q, nQ, iVi, BL[x], BR[x]);
         }
         // FP64: the half-state flux over the area (stress.F90:301); FP32: the stored flux/area
         T Bn;
@@ -154,9 +154,9 @@ __device__ __forceinline__ void flux_tile_body(const Lay& L, const Par& p, const
         for (int x = 0; x < 3; ++x) F.m[x][c] = S(faB * double(mF[x]));
     }
     T gF[5] = {T(0), T(0), T(0), T(0), T(0)}, dW[5] = {T(0), T(0), T(0), T(0), T(0)};
-    T gm1 = T(p.gamma - 1);
-    gasKin<T>(gm1, T(-1), WL, Tf, gF, dW);
-    gasKin<T>(gm1, T(1), WR, Tf, gF, dW);
+    const T igm1 = T(1.0 / (p.gamma - 1));
+    gasKin<T>(igm1, T(-1), WL, Tf, gF, dW);
+    gasKin<T>(igm1, T(1), WR, Tf, gF, dW);
     T cH = T(p.cHogH);
 #pragma unroll
     for (int v = 0; v < 5; ++v) gF[v] = gF[v] - cH * VaD * dW[v];
@@ -256,7 +256,7 @@ k_flux_tile(Lay L, Par p, const __grid_constant__ FluxMaps maps, FluxSrc<S> in, 
     T Vol[8];
 #pragma unroll
     for (int m = 0; m < 8; ++m) Vol[m] = T(sRec[5 * RB + ro(m)]);
-    T Vi = central8<T>(Vol);
+    T iVi = T(1) / central8<T>(Vol);
     T pdmb = T(p.pdmb);
     T WL[5], WR[5];
 #pragma unroll
@@ -266,7 +266,7 @@ k_flux_tile(Lay L, Par p, const __grid_constant__ FluxMaps maps, FluxSrc<S> in, 
         for (int m = 0; m < 8; ++m) Q[m] = T(sRec[v * RB + ro(m)]);
 #pragma unroll
         for (int m = 0; m < 4; ++m) nQ[m] = T(sLim[v * LB + lo(m)]);
-        getLR<T>(p.rmeth, pdmb, Vol, Q, nQ, Vi, WL[v], WR[v]);
+        getLR<T>(p.rmeth, pdmb, Vol, Q, nQ, iVi, WL[v], WR[v]);
     }
     T Tf[9];
 #pragma unroll
@@ -282,7 +282,7 @@ k_flux_tile(Lay L, Par p, const __grid_constant__ FluxMaps maps, FluxSrc<S> in, 
             for (int m = 0; m < 8; ++m) Q[m] = T(sRec[(6 + x) * RB + ro(m)]);
 #pragma unroll
             for (int m = 0; m < 4; ++m) nQ[m] = T(sLim[(5 + x) * LB + lo(m)]);
-            getLR<T>(p.rmeth, pdmb, Vol, Q, nQ, Vi, BL[x], BR[x]);
+            getLR<T>(p.rmeth, pdmb, Vol, Q, nQ, iVi, BL[x], BR[x]);
         }
         // FP64: the half-state flux over the area (stress.F90:301); FP32: the stored flux/area
         T Bn;
@@ -315,9 +315,9 @@ k_flux_tile(Lay L, Par p, const __grid_constant__ FluxMaps maps, FluxSrc<S> in, 
         for (int x = 0; x < 3; ++x) F.m[x][c] = S(faB * double(mF[x]));
     }
     T gF[5] = {T(0), T(0), T(0), T(0), T(0)}, dW[5] = {T(0), T(0), T(0), T(0), T(0)};
-    T gm1 = T(p.gamma - 1);
-    gasKin<T>(gm1, T(-1), WL, Tf, gF, dW);
-    gasKin<T>(gm1, T(1), WR, Tf, gF, dW);
+    const T igm1 = T(1.0 / (p.gamma - 1));
+    gasKin<T>(igm1, T(-1), WL, Tf, gF, dW);
+    gasKin<T>(igm1, T(1), WR, Tf, gF, dW);
     T cH = T(p.cHogH);
 #pragma unroll
     for (int v = 0; v < 5; ++v) gF[v] = gF[v] - cH * VaD * dW[v];

@@ -102,17 +102,24 @@ void launch_flux_queue64(const FluxJob<double>* jobs, int njobs, long long ntile
 void launch_flux_queue32(const FluxJob<float>* jobs, int njobs, long long ntiles, unsigned long long* counter,
                          int grid, cudaStream_t st);
 
-// One-sided gas kinetic flux (stress.F90:432-511)
+// 1 / sqrt(x) from the math library's reciprocal square root, in the precision of T
+__device__ __forceinline__ double rsq(double x) { return rsqrt(x); }
+__device__ __forceinline__ float rsq(float x) { return rsqrtf(x); }
+
+// One-sided gas kinetic flux (stress.F90:432-511). igm1 = 1 / (gamma - 1). The reference's sqrt(lambda)
+// and 1 / sqrt(pi lambda) come from one reciprocal square root of lambda (divisions are the FP64 flux
+// kernel's costliest operations; the results differ by an ulp or so).
 template <typename T>
-__device__ __forceinline__ void gasKin(T gm1, T sg, const T* W, const T* Tf, T* gF, T* dW) {
+__device__ __forceinline__ void gasKin(T igm1, T sg, const T* W, const T* Tf, T* gF, T* dW) {
     T D = W[0], Vx = W[1], Vy = W[2], Vz = W[3], P = W[4];
-    T E = T(0.5) * D * (Vx * Vx + Vy * Vy + Vz * Vz) + P / gm1;
+    T E = T(0.5) * D * (Vx * Vx + Vy * Vy + Vz * Vz) + P * igm1;
     T lambda = D / (T(2) * P);
+    T rl = rsq(lambda);   // 1 / sqrt(lambda)
     T Vn = Tf[0] * Vx + Tf[1] * Vy + Tf[2] * Vz;
     T Vt1 = Tf[3] * Vx + Tf[4] * Vy + Tf[5] * Vz;
     T Vt2 = Tf[6] * Vx + Tf[7] * Vy + Tf[8] * Vz;
-    T Vn0 = T(0.5) * erfc(sg * sqrt(lambda) * Vn);
-    T Vn1 = Vn * Vn0 - T(0.5) * sg * exp(-(lambda * Vn * Vn)) / sqrt(T(PI) * lambda);
+    T Vn0 = T(0.5) * erfc(sg * (lambda * rl) * Vn);
+    T Vn1 = Vn * Vn0 - T(0.5) * sg * exp(-(lambda * Vn * Vn)) * (rl * T(0.56418958354775628695));   // 1/sqrt(pi)
     gF[0] = gF[0] + D * Vn1;
     gF[4] = gF[4] + (E + T(0.5) * P) * Vn1 + T(0.5) * P * Vn0 * Vn;
     T fMn = D * Vn * Vn1 + P * Vn0;
@@ -134,20 +141,21 @@ template <typename T, bool BG = false>
 __device__ __forceinline__ void magKin(const Par& p, T sg, const T* W, const T* B, T Bn, const T* Tf, T* mF, T& bbD,
                                        T& VaD, const T* B0 = nullptr, T B0n = T(0)) {
     T D = W[0], P = W[4];
+    T iD = T(1) / D;   // one reciprocal for the reference's three divisions by rho
     T dPb = T(0.5) * (B[0] * B[0] + B[1] * B[1] + B[2] * B[2]);
     T Va2;
     if constexpr (BG) {
         T Bt0 = B[0] + B0[0], Bt1 = B[1] + B0[1], Bt2 = B[2] + B0[2];
-        Va2 = (Bt0 * Bt0 + Bt1 * Bt1 + Bt2 * Bt2) / D;
+        Va2 = (Bt0 * Bt0 + Bt1 * Bt1 + Bt2 * Bt2) * iD;
         bbD = bbD + T(0.5) * (Bt0 * Bt0 + Bt1 * Bt1 + Bt2 * Bt2);
     } else {
-        Va2 = T(2) * dPb / D;
+        Va2 = T(2) * dPb * iD;
         bbD = bbD + T(0.5) * (B[0] * B[0] + B[1] * B[1] + B[2] * B[2]);
     }
     T Vac2 = Va2;
-    if (p.doBoris) { T Ca = T(p.Ca); Vac2 = Va2 / (T(1) + (Va2 / (Ca * Ca))); }
+    if (p.doBoris) Vac2 = Va2 / (T(1) + Va2 * T(1.0 / (p.Ca * p.Ca)));
     T Vn = Tf[0] * W[1] + Tf[1] * W[2] + Tf[2] * W[3];
-    T lambda = T(1) / (T(2) * P / D + Vac2);
+    T lambda = T(1) / (T(2) * P * iD + Vac2);
     T Vn0 = T(0.5) * erfc(sg * sqrt(lambda) * Vn);
     VaD = VaD + T(0.5) * sqrt(Vac2);
     mF[0] = mF[0] + Vn0 * (dPb * Tf[0] - B[0] * Bn);
