@@ -117,10 +117,12 @@ __device__ __forceinline__ double wU7(int n) {
     return c[n];
 }
 
-// Cell conversions (gamutils.F90:301-321, 362-383)
+// Cell conversions (gamutils.F90:301-321, 362-383). Where the reference divides several values by the same
+// density or volume, one reciprocal serves them all here (FP64 divisions are long instruction sequences;
+// the results differ by an ulp or so).
 __device__ __forceinline__ void cellC2P(const Par& p, const double* Con, double* Prim) {
-    double rho = Con[0];
-    double Vx = Con[1] / rho, Vy = Con[2] / rho, Vz = Con[3] / rho;
+    double rho = Con[0], ir = 1.0 / rho;
+    double Vx = Con[1] * ir, Vy = Con[2] * ir, Vz = Con[3] * ir;
     double KinE = 0.5 * rho * (sq(Vx) + sq(Vy) + sq(Vz));
     Prim[0] = dmax(rho, p.dFloor);
     Prim[1] = Vx; Prim[2] = Vy; Prim[3] = Vz;
@@ -134,10 +136,10 @@ __device__ __forceinline__ void cellP2C(const Par& p, const double* Prim, double
 }
 // BlockCon2Prim (recon.F90:66-92): density floored first, kinetic energy from momenta
 __device__ __forceinline__ void blockC2P(const Par& p, const double* Con, double* W) {
-    double D = dmax(Con[0], p.dFloor);
-    double KinE = 0.5 * (sq(Con[1]) + sq(Con[2]) + sq(Con[3])) / D;
+    double D = dmax(Con[0], p.dFloor), iD = 1.0 / D;
+    double KinE = 0.5 * (sq(Con[1]) + sq(Con[2]) + sq(Con[3])) * iD;
     double P = dmax((p.gamma - 1) * (Con[4] - KinE), p.pFloor);
-    W[0] = D; W[1] = Con[1] / D; W[2] = Con[2] / D; W[3] = Con[3] / D; W[4] = P;
+    W[0] = D; W[1] = Con[1] * iD; W[2] = Con[2] * iD; W[3] = Con[3] * iD; W[4] = P;
 }
 
 // pdmLR (recon.F90:231-272) on one interface
@@ -203,7 +205,7 @@ __device__ __forceinline__ T central8(const T* q) {
 
 // gamCellBxyz (gridutils.F90:648-680): second-order cell field from the six face fluxes
 __device__ __forceinline__ void cellBxyz(const Lay& L, const GridP& g, double* const* mf, long long c, double* B) {
-    double dV = g.volume[c];
+    double idV = 1.0 / g.volume[c];
     double fI = mf[0][c], fJ = mf[1][c], fK = mf[2][c];
     long long ci = c + 1, cj = c + L.P, ck = c + (long long)L.P * L.Q;
     double fIp = mf[0][ci], fJp = mf[1][cj], fKp = mf[2][ck];
@@ -211,8 +213,8 @@ __device__ __forceinline__ void cellBxyz(const Lay& L, const GridP& g, double* c
 #pragma unroll
     for (int x = 0; x < 3; ++x) {
         double b = (fIp * g.xfc[0][x][ci] + fJp * g.xfc[1][x][cj] + fKp * g.xfc[2][x][ck] - fI * g.xfc[0][x][c] -
-                    fJ * g.xfc[1][x][c] - fK * g.xfc[2][x][c]) / dV;
-        B[x] = b - Div * g.xyzcc[x][c] / dV;
+                    fJ * g.xfc[1][x][c] - fK * g.xfc[2][x][c]) * idV;
+        B[x] = b - Div * g.xyzcc[x][c] * idV;
     }
 }
 

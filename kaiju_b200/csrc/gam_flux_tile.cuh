@@ -44,6 +44,14 @@ template <typename S, int D, int FR, bool TMA = false> constexpr size_t flux_sme
 struct FluxMaps { CUtensorMap rec[9]; CUtensorMap lim[8]; };
 constexpr uint32_t FLUX_WAIT = 1u << 20;   // mbarrier polls before the staging wait gives up
 
+// A flux times the face area in the storage type: for float storage a float product, which is the double
+// product of the two floats (exact) rounded once, so the same value without the conversions
+template <typename S, typename T>
+__device__ __forceinline__ S area_scaled(double faB, T f) {
+    if constexpr (std::is_same<S, float>::value) return float(faB) * float(f);
+    else return S(faB * double(f));
+}
+
 // One tile (bx, by, bz) of interfaces: the body of the per-problem flux kernel and of the ensembles'
 // persistent tile-queue kernel. Every thread of the CTA calls it for the same tile.
 template <typename T, typename S, int D, bool MHD, bool BG, int FR>
@@ -151,7 +159,7 @@ __device__ __forceinline__ void flux_tile_body(const Lay& L, const Par& p, const
             }
         }
 #pragma unroll
-        for (int x = 0; x < 3; ++x) F.m[x][c] = S(faB * double(mF[x]));
+        for (int x = 0; x < 3; ++x) F.m[x][c] = area_scaled<S>(faB, mF[x]);
     }
     T gF[5] = {T(0), T(0), T(0), T(0), T(0)}, dW[5] = {T(0), T(0), T(0), T(0), T(0)};
     const T igm1 = T(1.0 / (p.gamma - 1));
@@ -170,7 +178,7 @@ __device__ __forceinline__ void flux_tile_body(const Lay& L, const Par& p, const
         }
     }
 #pragma unroll
-    for (int v = 0; v < 5; ++v) F.g[v][c] = S(faB * double(gF[v]));
+    for (int v = 0; v < 5; ++v) F.g[v][c] = area_scaled<S>(faB, gF[v]);
 }
 
 // The per-problem kernel keeps its own copy of the tile body: calling flux_tile_body from the kernel
@@ -312,7 +320,7 @@ k_flux_tile(Lay L, Par p, const __grid_constant__ FluxMaps maps, FluxSrc<S> in, 
             }
         }
 #pragma unroll
-        for (int x = 0; x < 3; ++x) F.m[x][c] = S(faB * double(mF[x]));
+        for (int x = 0; x < 3; ++x) F.m[x][c] = area_scaled<S>(faB, mF[x]);
     }
     T gF[5] = {T(0), T(0), T(0), T(0), T(0)}, dW[5] = {T(0), T(0), T(0), T(0), T(0)};
     const T igm1 = T(1.0 / (p.gamma - 1));
@@ -331,7 +339,7 @@ k_flux_tile(Lay L, Par p, const __grid_constant__ FluxMaps maps, FluxSrc<S> in, 
         }
     }
 #pragma unroll
-    for (int v = 0; v < 5; ++v) F.g[v][c] = S(faB * double(gF[v]));
+    for (int v = 0; v < 5; ++v) F.g[v][c] = area_scaled<S>(faB, gF[v]);
 }
 
 // Tensor maps of the staged planes of sweep D; false when a plane cannot be mapped or the tiles' x origins

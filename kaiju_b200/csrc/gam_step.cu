@@ -85,9 +85,9 @@ __global__ void k_predict_cells(Lay L, Par p, GridP g, StateP n, StateP o, State
     for (int v = 0; v < 5; ++v) { Q[v] = n.gas[v][c]; oQ[v] = o.gas[v][c]; }
     cellC2P(p, oQ, oW);
     cellC2P(p, Q, W);
-    double pdt = sc->pdt, odt = sc->odt;
+    double pdt = sc->pdt, iodt = 1.0 / sc->odt;
 #pragma unroll
-    for (int v = 0; v < 5; ++v) { double dQ = (W[v] - oW[v]) / odt; pW[v] = W[v] + pdt * dQ; }
+    for (int v = 0; v < 5; ++v) { double dQ = (W[v] - oW[v]) * iodt; pW[v] = W[v] + pdt * dQ; }
     pW[0] = dmax(pW[0], p.dFloor);
     pW[4] = dmax(pW[4], p.pFloor);
     cellP2C(p, pW, pQ);
@@ -99,8 +99,8 @@ __global__ void k_predict_cells(Lay L, Par p, GridP g, StateP n, StateP o, State
     }
     // Mom2Face summand VolB*MomB/max(DenB,dFloor) (fields.F90:265-271), a pointwise cell value
     {
-        double vol = g.volume[c], den = dmax(pQ[0], p.dFloor);
-        double v0 = vol * pQ[1] / den, v1 = vol * pQ[2] / den, v2 = vol * pQ[3] / den;
+        double vol = g.volume[c], iden = 1.0 / dmax(pQ[0], p.dFloor);
+        double v0 = vol * pQ[1] * iden, v1 = vol * pQ[2] * iden, v2 = vol * pQ[3] * iden;
         if (f32) { f.VdV[0][c] = float(v0); f.VdV[1][c] = float(v1); f.VdV[2][c] = float(v2); }
         else { VdV.v[0][c] = v0; VdV.v[1][c] = v1; VdV.v[2][c] = v2; }
     }
@@ -135,7 +135,7 @@ __device__ __forceinline__ void cellDeltas(const Lay& L, const Par& p, const Gri
                                            const FluxOut<O>& FJ, const FluxOut<O>& FK, const float* corr,
                                            long long c, double* dh, double* dm) {
     long long cj = c + L.P, ck = c + (long long)L.P * L.Q;
-    double dV = g.volume[c];
+    double idV = 1.0 / g.volume[c];
     auto cr = [&](int d, int v, long long lo, long long hi) {
         if (!corr) return 0.0;
         const float* q = corr + (long long)(d * 8 + v) * L.E;
@@ -145,13 +145,13 @@ __device__ __forceinline__ void cellDeltas(const Lay& L, const Par& p, const Gri
     for (int v = 0; v < 5; ++v)
         dh[v] = (double(FI.g[v][c]) - double(FI.g[v][c + 1]) + double(FJ.g[v][c]) - double(FJ.g[v][cj]) +
                  double(FK.g[v][c]) - double(FK.g[v][ck]) +
-                 (cr(0, v, c, c + 1) + cr(1, v, c, cj) + cr(2, v, c, ck))) / dV;
+                 (cr(0, v, c, c + 1) + cr(1, v, c, cj) + cr(2, v, c, ck))) * idV;
     if (p.doMHD) {
 #pragma unroll
         for (int x = 0; x < 3; ++x)
             dm[x] = (double(FI.m[x][c]) - double(FI.m[x][c + 1]) + double(FJ.m[x][c]) - double(FJ.m[x][cj]) +
                      double(FK.m[x][c]) - double(FK.m[x][ck]) +
-                     (cr(0, 5 + x, c, c + 1) + cr(1, 5 + x, c, cj) + cr(2, 5 + x, c, ck))) / dV;
+                     (cr(0, 5 + x, c, c + 1) + cr(1, 5 + x, c, cj) + cr(2, 5 + x, c, ck))) * idV;
         if (p.doBackground) {   // background momentum source (stress.F90:185-188)
 #pragma unroll
             for (int x = 0; x < 3; ++x) dm[x] = dm[x] + g.dpB0[x][c];
@@ -299,12 +299,13 @@ __global__ void k_update_gas(Lay L, Par p, GridP g, StateP nS, StateP oNew, Prim
                 cellBoris(p, U, U0, B2, B0, dh, dPm, dt);
             } else {
                 double D = dmax(U[0], p.dFloor), Mx = U[1], My = U[2], Mz = U[3], TotE = U[4];
-                double KinE = 0.5 * (sq(Mx) + sq(My) + sq(Mz)) / D;
+                const double iD = 1.0 / D;
+                double KinE = 0.5 * (sq(Mx) + sq(My) + sq(Mz)) * iD;
                 double P = dmax((p.gamma - 1) * (TotE - KinE), p.pFloor);
                 Mx = Mx + dt * dPm[0];
                 My = My + dt * dPm[1];
                 Mz = Mz + dt * dPm[2];
-                KinE = 0.5 * (sq(Mx) + sq(My) + sq(Mz)) / D;
+                KinE = 0.5 * (sq(Mx) + sq(My) + sq(Mz)) * iD;
                 U[0] = D; U[1] = Mx; U[2] = My; U[3] = Mz; U[4] = KinE + P / (p.gamma - 1);
             }
         }
@@ -374,20 +375,20 @@ __global__ void k_calcdt(Lay L, Par p, GridP g, StateP s, Scal* sc) {
     bool isnan_ = false;
     if (reg_plane(r, i, j, k)) {
         long long c = L.at(i, j, k);
-        double rho = s.gas[0][c];
-        double Vx = s.gas[1][c] / rho, Vy = s.gas[2][c] / rho, Vz = s.gas[3][c] / rho;
+        double rho = s.gas[0][c], ir = 1.0 / rho;   // one reciprocal for the reference's divisions by rho
+        double Vx = s.gas[1][c] * ir, Vy = s.gas[2][c] * ir, Vz = s.gas[3][c] * ir;
         double MagV = sqrt(sq(Vx) + sq(Vy) + sq(Vz));
         double ke = 0.5 * rho * sq(MagV);
         double e = s.gas[4][c] - ke;
         double P = (p.gamma - 1) * e;
-        double Cs = sqrt(p.gamma * P / rho);
+        double Cs = sqrt(p.gamma * P * ir);
         double Valf = 0.0;
         if (p.doMHD) {
             double Bx = s.b[0][c], By = s.b[1][c], Bz = s.b[2][c];
             if (p.doBackground) { Bx = Bx + g.B0[0][c]; By = By + g.B0[1][c]; Bz = Bz + g.B0[2][c]; }  // gridutils.F90:82-86
             double MagB = sqrt(sq(Bx) + sq(By) + sq(Bz));
-            Valf = MagB / sqrt(rho);
-            if (p.doBoris) Valf = p.Ca * Valf / sqrt(p.Ca * p.Ca + Valf * Valf);
+            Valf = MagB * rsq(rho);
+            if (p.doBoris) Valf = p.Ca * Valf * rsq(p.Ca * p.Ca + Valf * Valf);
         }
         double vCFL = MagV + sqrt(sq(Cs) + sq(Valf)) + 0.0;
         double dl = g.di[c];
