@@ -155,8 +155,8 @@ __device__ __forceinline__ void magKin(const Par& p, T sg, const T* W, const T* 
     T Vac2 = Va2;
     if (p.doBoris) Vac2 = Va2 / (T(1) + Va2 * T(1.0 / (p.Ca * p.Ca)));
     T Vn = Tf[0] * W[1] + Tf[1] * W[2] + Tf[2] * W[3];
-    T lambda = T(1) / (T(2) * P * iD + Vac2);
-    T Vn0 = T(0.5) * erfc(sg * sqrt(lambda) * Vn);
+    // lambda = 1 / (2P/rho + Va^2) enters only as sqrt(lambda): one reciprocal square root
+    T Vn0 = T(0.5) * erfc(sg * rsq(T(2) * P * iD + Vac2) * Vn);
     VaD = VaD + T(0.5) * sqrt(Vac2);
     mF[0] = mF[0] + Vn0 * (dPb * Tf[0] - B[0] * Bn);
     mF[1] = mF[1] + Vn0 * (dPb * Tf[1] - B[1] * Bn);
