@@ -119,7 +119,8 @@ void efield_kernels_init() {
 void enqueue_efield(Handle& h, const StateP& nS, cudaStream_t st) {
     (void)nS;   // the limiter values come from the precomputed nbA planes
     const Lay& L = h.L;
-    cudaMemsetAsync(h.E[0], 0, sizeof(double) * L.E * 3, st);   // E planes are contiguous in the pool
+    // E = 0 (fields.F90:88) needs no pass per step: the edge kernels rewrite the same edges every step, and
+    // every edge outside them stays zero from the pool's zeroing (initialisation clears its scratch use)
     Vec3P Vf = {{h.Vf[0], h.Vf[1], h.Vf[2]}}, VdV = {{h.VdV[0], h.VdV[1], h.VdV[2]}};
     GridP g = h.gridP();
     Vec3F Vf32{};

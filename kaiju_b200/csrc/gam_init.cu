@@ -602,6 +602,8 @@ int init_problem(Handle& h, int ic, const BgSpec* bg, const double* icPar) {
             long long ne = (long long)(L.Ni - 1) * (L.Nj - 1) * (L.Nk - 1);
             k_ic_bw_la<<<nb(ne, 128), 128, 0, st>>>(L, X, lA, bScl);
             k_ic_bw_flux<<<nb(ne, 256), 256, 0, st>>>(L, lA, s);
+            // the step relies on every E edge its kernels do not write being zero
+            cudaMemsetAsync(h.E[0], 0, sizeof(double) * L.E * 3, st);   // the E planes are contiguous
             h.launches += 2;
         }
         h.launches++;

@@ -812,7 +812,7 @@ int ensure_f32(Handle& h) {
 
 int kernels_per_step(const Handle& h) {
     int n = 1 + 1;                      // begin, predict cells
-    if (h.p.doMHD) n += 1 + 1 + 6;      // predict faces, E memset (counted), 3x(mom2face + edge)
+    if (h.p.doMHD) n += 1 + 6;          // predict faces, 3x(mom2face + edge)
     n += (h.p.do25D ? 2 : 3) + ((h.fuseUpdate && !h.closure) ? 0 : 1);   // fluxes + flux2deltas
     n += 1 + 1 + 1;                     // e2flux/copy, bflux2fld, update gas
     n += 2 + 3 + 1;                     // calcdt + finalize, 3 BC kernels, final bflux2fld
