@@ -195,6 +195,16 @@ __device__ __forceinline__ void getLR(int rmeth, T pdmb, const T* dV, const T* Q
     }
 }
 
+// Cen8LRs with the stencil weights already applied to the volumes: c8[n] = w8[n] * dV[n], shared by all the
+// variables of an interface (the reference weights dV[n] * Q[n] per variable), iVi = 1 / sum(c8)
+template <typename T>
+__device__ __forceinline__ void getLR8(T pdmb, const T* c8, const T* Q, const T* nQ, T iVi, T& Ql, T& Qr) {
+    T s = T(0);
+#pragma unroll
+    for (int n = 0; n < 8; ++n) s = s + c8[n] * Q[n];
+    pdmLR<T>(pdmb, nQ[0], nQ[1], nQ[2], nQ[3], s * iVi, Ql, Qr);
+}
+
 template <typename T>
 __device__ __forceinline__ T central8(const T* q) {
     T s = T(0);

@@ -100,11 +100,22 @@ __device__ __forceinline__ void flux_tile_body(const Lay& L, const Par& p, const
     auto ro = [&](int m) { return D == 0 ? (lane + m) + (FL + 8) * row : lane + FL * (row + m); };
     auto lo = [&](int m) { return D == 0 ? (lane + m) + (FL + 4) * row : lane + FL * (row + m); };
     const long long c = L.at(i, j, k), s = L.stride(D);
-    T Vol[8];
+    // the Central8 weights applied to the stencil volumes once for all the variables (8CENT); 7UP reads
+    // the volumes again where it needs them
+    T c8[8], Vi = T(0);
 #pragma unroll
-    for (int m = 0; m < 8; ++m) Vol[m] = T(sRec[5 * RB + ro(m)]);
-    T iVi = T(1) / central8<T>(Vol);
-    T pdmb = T(p.pdmb);
+    for (int m = 0; m < 8; ++m) { c8[m] = T(wC8(m)) * T(sRec[5 * RB + ro(m)]); Vi = Vi + c8[m]; }
+    const T iVi = T(1) / Vi;
+    const T pdmb = T(p.pdmb);
+    auto recon = [&](const T* Q, const T* nQ, T& Ql, T& Qr) {
+        if (p.rmeth == RM_8CENT) getLR8<T>(pdmb, c8, Q, nQ, iVi, Ql, Qr);
+        else {
+            T Vol[8];
+#pragma unroll
+            for (int m = 0; m < 8; ++m) Vol[m] = T(sRec[5 * RB + ro(m)]);
+            getLR<T>(p.rmeth, pdmb, Vol, Q, nQ, iVi, Ql, Qr);
+        }
+    };
     T WL[5], WR[5];
 #pragma unroll
     for (int v = 0; v < 5; ++v) {
@@ -113,7 +124,7 @@ __device__ __forceinline__ void flux_tile_body(const Lay& L, const Par& p, const
         for (int m = 0; m < 8; ++m) Q[m] = T(sRec[v * RB + ro(m)]);
 #pragma unroll
         for (int m = 0; m < 4; ++m) nQ[m] = T(sLim[v * LB + lo(m)]);
-        getLR<T>(p.rmeth, pdmb, Vol, Q, nQ, iVi, WL[v], WR[v]);
+        recon(Q, nQ, WL[v], WR[v]);
     }
     T Tf[9];
 #pragma unroll
@@ -129,7 +140,7 @@ __device__ __forceinline__ void flux_tile_body(const Lay& L, const Par& p, const
             for (int m = 0; m < 8; ++m) Q[m] = T(sRec[(6 + x) * RB + ro(m)]);
 #pragma unroll
             for (int m = 0; m < 4; ++m) nQ[m] = T(sLim[(5 + x) * LB + lo(m)]);
-            getLR<T>(p.rmeth, pdmb, Vol, Q, nQ, iVi, BL[x], BR[x]);
+            recon(Q, nQ, BL[x], BR[x]);
         }
         // FP64: the half-state flux over the area (stress.F90:301); FP32: the stored flux/area
         T Bn;
@@ -261,11 +272,22 @@ k_flux_tile(Lay L, Par p, const __grid_constant__ FluxMaps maps, FluxSrc<S> in, 
     constexpr int LW = TMA ? FL + 8 : FL + 4, LX = TMA ? 2 : 0;   // I-sweep limiter row width and stencil shift
     auto lo = [&](int m) { return D == 0 ? (lane + m + LX) + LW * row : lane + FL * (row + m); };
     const long long c = L.at(i, j, k), s = L.stride(D);
-    T Vol[8];
+    // the Central8 weights applied to the stencil volumes once for all the variables (8CENT); 7UP reads
+    // the volumes again where it needs them
+    T c8[8], Vi = T(0);
 #pragma unroll
-    for (int m = 0; m < 8; ++m) Vol[m] = T(sRec[5 * RB + ro(m)]);
-    T iVi = T(1) / central8<T>(Vol);
-    T pdmb = T(p.pdmb);
+    for (int m = 0; m < 8; ++m) { c8[m] = T(wC8(m)) * T(sRec[5 * RB + ro(m)]); Vi = Vi + c8[m]; }
+    const T iVi = T(1) / Vi;
+    const T pdmb = T(p.pdmb);
+    auto recon = [&](const T* Q, const T* nQ, T& Ql, T& Qr) {
+        if (p.rmeth == RM_8CENT) getLR8<T>(pdmb, c8, Q, nQ, iVi, Ql, Qr);
+        else {
+            T Vol[8];
+#pragma unroll
+            for (int m = 0; m < 8; ++m) Vol[m] = T(sRec[5 * RB + ro(m)]);
+            getLR<T>(p.rmeth, pdmb, Vol, Q, nQ, iVi, Ql, Qr);
+        }
+    };
     T WL[5], WR[5];
 #pragma unroll
     for (int v = 0; v < 5; ++v) {
@@ -274,7 +296,7 @@ k_flux_tile(Lay L, Par p, const __grid_constant__ FluxMaps maps, FluxSrc<S> in, 
         for (int m = 0; m < 8; ++m) Q[m] = T(sRec[v * RB + ro(m)]);
 #pragma unroll
         for (int m = 0; m < 4; ++m) nQ[m] = T(sLim[v * LB + lo(m)]);
-        getLR<T>(p.rmeth, pdmb, Vol, Q, nQ, iVi, WL[v], WR[v]);
+        recon(Q, nQ, WL[v], WR[v]);
     }
     T Tf[9];
 #pragma unroll
@@ -290,7 +312,7 @@ k_flux_tile(Lay L, Par p, const __grid_constant__ FluxMaps maps, FluxSrc<S> in, 
             for (int m = 0; m < 8; ++m) Q[m] = T(sRec[(6 + x) * RB + ro(m)]);
 #pragma unroll
             for (int m = 0; m < 4; ++m) nQ[m] = T(sLim[(5 + x) * LB + lo(m)]);
-            getLR<T>(p.rmeth, pdmb, Vol, Q, nQ, iVi, BL[x], BR[x]);
+            recon(Q, nQ, BL[x], BR[x]);
         }
         // FP64: the half-state flux over the area (stress.F90:301); FP32: the stored flux/area
         T Bn;
