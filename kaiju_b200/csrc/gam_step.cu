@@ -40,7 +40,7 @@ __global__ void k_predict_faces(long long E, Par p, GridP g, Vec3P mf, Vec3P omf
                                 F32FaceOut o, const Scal* sc) {
     long long l = 2 * (blockIdx.x * (long long)blockDim.x + threadIdx.x);
     if (l >= E) return;
-    double pdt = sc->pdt, odt = sc->odt;
+    const double pdt = sc->pdt, iodt = 1.0 / sc->odt;   // reciprocals where the reference divides repeatedly
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
         const double2 Q2 = *reinterpret_cast<const double2*>(mf.v[c] + l);
@@ -50,11 +50,11 @@ __global__ void k_predict_faces(long long E, Par p, GridP g, Vec3P mf, Vec3P omf
         const double Q[2] = {Q2.x, Q2.y}, oQ[2] = {oQ2.x, oQ2.y}, A[2] = {a2.x, a2.y};
 #pragma unroll
         for (int e = 0; e < 2; ++e) {
-            double dQ = (Q[e] - oQ[e]) / odt;
+            double dQ = (Q[e] - oQ[e]) * iodt;
             H[e] = Q[e] + pdt * dQ;
-            double a = dmax(A[e], TINY);
-            hb[e] = H[e] / a;
-            nb[e] = (p.doLFMLim ? Q[e] : H[e]) / a;
+            const double ia = 1.0 / dmax(A[e], TINY);
+            hb[e] = H[e] * ia;
+            nb[e] = (p.doLFMLim ? Q[e] : H[e]) * ia;
         }
         // the half-state flux: bFlux2Fld of the half state reads it
         *reinterpret_cast<double2*>(hmf.v[c] + l) = make_double2(H[0], H[1]);
