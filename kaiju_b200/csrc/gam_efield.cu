@@ -28,8 +28,8 @@ __device__ __forceinline__ void mom2face_sum(const A* wV, const A* w0, const A* 
         s1 = fma(w, w1[n], s1);
         s2 = fma(w, w2[n], s2);
     }
-    A dV = sV > A(TINY) ? sV : A(TINY);
-    f0 = s0 / dV; f1 = s1 / dV; f2 = s2 / dV;
+    const A idV = A(1) / (sV > A(TINY) ? sV : A(TINY));   // one reciprocal for the three quotients
+    f0 = s0 * idV; f1 = s1 * idV; f2 = s2 * idV;
 }
 
 // Faces along i (dT1 = I): one face per thread; the stencil runs along the warp, so neighbouring lanes
@@ -79,10 +79,10 @@ __global__ void k_mom2face_run(Lay L, const GS* vol, VS v0, VS v1, VS v2, A* o0,
         for (int n = 0; n < 8; ++n) acc = fma(A(wC8(n)), w[n], acc);
         return acc;
     };
-    A w[NW + 7], dV[NW];
+    A w[NW + 7], idV[NW];   // the reciprocal of each face's volume sum serves its three quotients
     window(vol, w);
 #pragma unroll
-    for (int q = 0; q < NW; ++q) { A sV = sum8(w + q); dV[q] = sV > A(TINY) ? sV : A(TINY); }
+    for (int q = 0; q < NW; ++q) { A sV = sum8(w + q); idV[q] = A(1) / (sV > A(TINY) ? sV : A(TINY)); }
     A* const out[3] = {o0, o1, o2};
     VS const src[3] = {v0, v1, v2};
 #pragma unroll
@@ -90,7 +90,7 @@ __global__ void k_mom2face_run(Lay L, const GS* vol, VS v0, VS v1, VS v2, A* o0,
         window(src[x], w);
 #pragma unroll
         for (int q = 0; q < NW; ++q)
-            if (a0 + q < n1) out[x][c + (long long)q * s] = sum8(w + q) / dV[q];
+            if (a0 + q < n1) out[x][c + (long long)q * s] = sum8(w + q) * idV[q];
     }
 }
 

@@ -137,8 +137,10 @@ k_edge_tile(Lay L, Par p, const __grid_constant__ EdgeMaps maps, EdgeSrc<S> in, 
         Vc1 = Vc1 + cA[m] * T(sm[TL::oVf + TL::sVf + q]);
         Vc2 = Vc2 + cA[m] * T(sm[TL::oVf + 2 * TL::sVf + q]);
     }
-    T dA = fA1 > T(TINY) ? fA1 : T(TINY);
-    T idA = T(1) / dA;   // one reciprocal where the reference divides three times
+    // 1 / max(fA1, TINY), where the reference divides three times; for fA1 > TINY it is the 1 / fA1 the
+    // face-field reconstruction uses as well
+    const T ifA1 = T(1) / fA1;
+    T idA = fA1 > T(TINY) ? ifA1 : T(1.0 / TINY);
     Vc0 = Vc0 * idA; Vc1 = Vc1 * idA; Vc2 = Vc2 * idA;
     T v1 = Vc0 * T(__ldg(&in.Te[ED][0][c])) + Vc1 * T(__ldg(&in.Te[ED][1][c])) + Vc2 * T(__ldg(&in.Te[ED][2][c]));
     T v2 = Vc0 * T(__ldg(&in.Te[ED][3][c])) + Vc1 * T(__ldg(&in.Te[ED][4][c])) + Vc2 * T(__ldg(&in.Te[ED][5][c]));
@@ -165,7 +167,6 @@ k_edge_tile(Lay L, Par p, const __grid_constant__ EdgeMaps maps, EdgeSrc<S> in, 
     }
     T pdmb = T(p.pdmb);
     T l1, r1;
-    const T ifA1 = T(1) / fA1;
     if (p.rmeth == RM_8CENT) getLR8<T>(pdmb, cA, Bb, nBb, ifA1, l1, r1);
     else {
         T Ab[8];
