@@ -119,24 +119,22 @@ k_edge_tile(Lay L, Par p, const __grid_constant__ EdgeMaps maps, EdgeSrc<S> in, 
     auto off = [&](int s, int m, int& di, int& dj, int& dk) {
         di = ti + (s == 0 ? m : 0); dj = tj + (s == 1 ? m : 0); dk = tk + (s == 2 ? m : 0);
     };
-    // GetCornerV (fields.F90:457-517): area-weighted Central8 of Vf along dT2, mapped with Te. The Central8
-    // weights are applied to the stencil areas once (cA) and serve Vf's three sums, the area sum and the
-    // 8CENT reconstruction of the face field (the reference weights each product separately); 7UP reads
-    // the areas again where it needs them.
-    T cA[8], Bb[8], nBb[4];
-    T Vc0 = T(0), Vc1 = T(0), Vc2 = T(0), fA1 = T(0);
+    // GetCornerV (fields.F90:457-517): area-weighted Central8 of Vf along dT2, mapped with Te
+    T Ab[8], Bb[8], nBb[4];
+    T Vc0 = T(0), Vc1 = T(0), Vc2 = T(0);
 #pragma unroll
     for (int m = 0; m < 8; ++m) {
         int di, dj, dk;
         off(dT2, m - 4, di, dj, dk);
         int q = bidx(b8t2, di, dj, dk);
-        cA[m] = T(wC8(m)) * T(sm[TL::oA1 + q]);
-        fA1 = fA1 + cA[m];
+        Ab[m] = T(sm[TL::oA1 + q]);
         Bb[m] = T(sm[TL::oB1 + q]);
-        Vc0 = Vc0 + cA[m] * T(sm[TL::oVf + q]);
-        Vc1 = Vc1 + cA[m] * T(sm[TL::oVf + TL::sVf + q]);
-        Vc2 = Vc2 + cA[m] * T(sm[TL::oVf + 2 * TL::sVf + q]);
+        T w = T(wC8(m));
+        Vc0 = Vc0 + w * (Ab[m] * T(sm[TL::oVf + q]));
+        Vc1 = Vc1 + w * (Ab[m] * T(sm[TL::oVf + TL::sVf + q]));
+        Vc2 = Vc2 + w * (Ab[m] * T(sm[TL::oVf + 2 * TL::sVf + q]));
     }
+    T fA1 = central8<T>(Ab);
     // 1 / max(fA1, TINY), where the reference divides three times; for fA1 > TINY it is the 1 / fA1 the
     // face-field reconstruction uses as well
     const T ifA1 = T(1) / fA1;
@@ -167,29 +165,16 @@ k_edge_tile(Lay L, Par p, const __grid_constant__ EdgeMaps maps, EdgeSrc<S> in, 
     }
     T pdmb = T(p.pdmb);
     T l1, r1;
-    if (p.rmeth == RM_8CENT) getLR8<T>(pdmb, cA, Bb, nBb, ifA1, l1, r1);
-    else {
-        T Ab[8];
-#pragma unroll
-        for (int m = 0; m < 8; ++m) {
-            int di, dj, dk;
-            off(dT2, m - 4, di, dj, dk);
-            Ab[m] = T(sm[TL::oA1 + bidx(b8t2, di, dj, dk)]);
-        }
-        getLR<T>(p.rmeth, pdmb, Ab, Bb, nBb, ifA1, l1, r1);
-    }
+    getLR<T>(p.rmeth, pdmb, Ab, Bb, nBb, ifA1, l1, r1);
     T bT1L = l1 * fA1, bT1R = r1 * fA1;
     // ... and of the dT2 faces along dT1
-    T A2[8], B2[8], nB2[4];   // A2: the weighted areas cA2 for 8CENT, the areas for 7UP
-    T fA2 = T(0);
+    T A2[8], B2[8], nB2[4];
 #pragma unroll
     for (int m = 0; m < 8; ++m) {
         int di, dj, dk;
         off(dT1, m - 4, di, dj, dk);
         int q = bidx(b8t1, di, dj, dk);
-        const T a = T(sm[TL::oA2 + q]), ca = T(wC8(m)) * a;
-        fA2 = fA2 + ca;
-        A2[m] = p.rmeth == RM_8CENT ? ca : a;
+        A2[m] = T(sm[TL::oA2 + q]);
         B2[m] = T(sm[TL::oB2 + q]);
     }
 #pragma unroll
@@ -198,10 +183,10 @@ k_edge_tile(Lay L, Par p, const __grid_constant__ EdgeMaps maps, EdgeSrc<S> in, 
         off(dT1, m - 2, di, dj, dk);
         nB2[m] = T(sm[TL::oN2 + bidx(b4t1, di, dj, dk)]);
     }
+    T fA2 = central8<T>(A2);
     const T ifA2 = T(1) / fA2;
     T l2, r2;
-    if (p.rmeth == RM_8CENT) getLR8<T>(pdmb, A2, B2, nB2, ifA2, l2, r2);
-    else getLR<T>(p.rmeth, pdmb, A2, B2, nB2, ifA2, l2, r2);
+    getLR<T>(p.rmeth, pdmb, A2, B2, nB2, ifA2, l2, r2);
     T bT2L = l2 * fA2, bT2R = r2 * fA2;
     T xni = T(__ldg(&in.Teb[ED][0][c])), yni = T(__ldg(&in.Teb[ED][1][c]));
     T xnj = T(__ldg(&in.Teb[ED][2][c])), ynj = T(__ldg(&in.Teb[ED][3][c]));
