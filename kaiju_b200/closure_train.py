@@ -282,7 +282,7 @@ def main(argv=None):
     ap.add_argument("--rollouts", type=int, default=2)
     ap.add_argument("--three-levels", type=int, default=0,
                     help="also evaluate this many held-out seeds against a truth run at 4n (needs (4n)^3 to fit)")
-    ap.add_argument("--loss", choices=["cell", "face"], default="face",
+    ap.add_argument("--loss", choices=["cell", "face"], default="cell",
                     help="fit the cell residual through the divergence, or the face targets directly")
     ap.add_argument("--out", default=None)
     a = ap.parse_args(argv)
