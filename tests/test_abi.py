@@ -54,6 +54,12 @@ def test_errstr_and_argument_checks(lib):
     assert lib.gam_gpu_create(C.byref(h), C.byref(m), C.byref(g), dp, dp, dp, dp, dp, dp, 0.0, 0.0) == gm.GAM_ERR_ARG
     assert lib.gam_gpu_step(None, None, None, None) == gm.GAM_ERR_ARG
     assert lib.gam_gpu_fetch(None, b"gas", None, 0) == gm.GAM_ERR_ARG
+    # tile switches and the closure's face-target entry points reject null handles before any CUDA call
+    assert lib.gam_gpu_set_tile(None, gm.GAM_TILE_TMA, 1) == gm.GAM_ERR_ARG
+    assert lib.gam_closure_accum_fine(None, None, 1.0, 1) == gm.GAM_ERR_ARG
+    assert lib.gam_closure_set_loss(None, gm.GAM_CLOSURE_LOSS_FACE) == gm.GAM_ERR_ARG
+    assert lib.gam_closure_face_stats(None, 0, None, None) == gm.GAM_ERR_ARG
+    assert gm.errstr(gm.GAM_ERR_TIMEOUT)
 
 
 def test_model_defaults_follow_initmodel():
