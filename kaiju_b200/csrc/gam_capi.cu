@@ -194,7 +194,7 @@ int alloc_handle(gam_gpu* G, const gam_model_c* m) {
     ring_kernels_init();
     CK(cudaStreamCreateWithFlags(&h.stream, cudaStreamNonBlocking));
     h.ownStream = true;
-    const size_t planes = 11 * 3 + 10 + 14 + 9 + 24 + 91;
+    const size_t planes = 11 * 3 + 10 + 14 + 9 + 24 + 91 + 6;   // + the I and J edges' face velocities
     h.poolPlanes = planes;
     CK(cudaMalloc(&h.pool, sizeof(double) * L.E * planes));
     CK(cudaMemsetAsync(h.pool, 0, sizeof(double) * L.E * planes, h.stream));
@@ -212,6 +212,7 @@ int alloc_handle(gam_gpu* G, const gam_model_c* m) {
     for (int v = 0; v < 5; ++v) h.Wn[v] = take();
     for (int x = 0; x < 3; ++x) h.E[x] = take();   // contiguous: memset as one range
     for (int x = 0; x < 3; ++x) h.Vf[x] = take();
+    for (int e = 0; e < 2; ++e) for (int x = 0; x < 3; ++x) h.VfE[e][x] = take();
     for (int x = 0; x < 3; ++x) h.VdV[x] = take();
     for (int x = 0; x < 3; ++x) h.hbA[x] = take();
     for (int x = 0; x < 3; ++x) h.nbA[x] = take();

@@ -765,7 +765,7 @@ void refresh_f32_background(Handle& h) {
 int ensure_f32(Handle& h) {
     if (h.f32pool) return 0;
     const long long E = h.L.E;
-    const int nplanes = 29 + 24 + 64 + (h.p.doBackground ? 18 : 0);
+    const int nplanes = 29 + 24 + 64 + 6 + (h.p.doBackground ? 18 : 0);   // 6: the I and J edges' face velocities
     if (cudaMalloc(&h.f32pool, sizeof(float) * E * nplanes) != cudaSuccess) return 3;
     cudaMemsetAsync(h.f32pool, 0, sizeof(float) * E * nplanes, h.stream);
     float* q = h.f32pool;
@@ -778,6 +778,7 @@ int ensure_f32(Handle& h) {
     for (int x = 0; x < 3; ++x) f.hbA[x] = take();
     for (int x = 0; x < 3; ++x) f.nbA[x] = take();
     for (int x = 0; x < 3; ++x) f.Vf[x] = take();
+    for (int e = 0; e < 2; ++e) for (int x = 0; x < 3; ++x) f.VfE[e][x] = take();
     f.rho = take();
     for (int x = 0; x < 3; ++x) f.VdV[x] = take();
     for (int d = 0; d < 3; ++d) {
@@ -812,7 +813,7 @@ int ensure_f32(Handle& h) {
 
 int kernels_per_step(const Handle& h) {
     int n = 1 + 1;                      // begin, predict cells
-    if (h.p.doMHD) n += 1 + 6;          // predict faces, 3x(mom2face + edge)
+    if (h.p.doMHD) n += 1 + 1 + 3;      // predict faces, Mom2Face (all directions), 3 edge kernels
     n += (h.p.do25D ? 2 : 3) + ((h.fuseUpdate && !h.closure) ? 0 : 1);   // fluxes + flux2deltas
     n += 1 + 1 + 1;                     // e2flux/copy, bflux2fld, update gas
     n += 2 + 3 + 1;                     // calcdt + finalize, 3 BC kernels, final bflux2fld

@@ -14,6 +14,7 @@ enum Prec { PREC_FP64 = 0, PREC_FP32FLUX = 1 };
 // metric planes converted once
 struct F32Planes {
     float* Wh[5]; float* Wn[5]; float* hb[3]; float* nb[3]; float* hbA[3]; float* nbA[3]; float* Vf[3]; float* rho;
+    float* VfE[2][3];   // face velocities for the I and J edges (Vf: the K edges')
     float* VdV[3];
     float* gflx[3][5]; float* mflx[3][3];   // area-scaled interface fluxes
     float* volume; float* face[3]; float* edge[3]; float* Tf[3][9]; float* Te[3][6]; float* Teb[3][4];
@@ -51,7 +52,8 @@ struct Handle {
     double* VdV[3];       // half-state volume * momentum / max(rho, dFloor) per cell (Mom2Face summand)
     double* hbA[3];       // half-state face flux / max(face area, TINY) (EdgeLRs reconstruction values)
     double* nbA[3];       // limiter-state face flux / max(face area, TINY) (EdgeLRs limiter values)
-    double* Vf[3];        // face velocities pushed along dT1
+    double* Vf[3];        // face velocities pushed along dT1 for the K edges (the last direction, as the reference leaves it)
+    double* VfE[2][3];    // the same for the I and J edges (all three come from one Mom2Face pass)
     double* dGasH[5];
     double* dGasM[3];
     double* gflx[3][5];   // interface gas fluxes per direction (area-scaled)
