@@ -22,6 +22,7 @@ import json
 import os
 import subprocess
 import sys
+import tempfile
 import time
 
 import numpy as np
@@ -74,12 +75,13 @@ def model_for(n):
 
 
 class ClockSampler:
-    """nvidia-smi clocks during the timed region."""
+    """nvidia-smi clocks every 50 ms with timestamps; started before the warm-up so that it is sampling when
+    the timed region starts, and summarised over the samples inside that region (window())."""
 
     def __init__(self, index):
         self.index = index
         self.proc = None
-        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_rank{index}.csv")
+        self.path = os.path.join(tempfile.gettempdir(), f"kaiju_b200_clocks_rank{index}_{os.getpid()}.csv")
 
     def __enter__(self):
         try:
@@ -87,10 +89,10 @@ class ClockSampler:
             self.f = open(self.path, "w")
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--id={self.index}",
-                 "--query-gpu=index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+                 "--query-gpu=timestamp,index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
                  "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
                  "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap",
-                 "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.f, stderr=subprocess.DEVNULL)
+                 "--format=csv,noheader,nounits", "-lms", "50"], stdout=self.f, stderr=subprocess.DEVNULL)
         except Exception:
             self.proc = None
         return self
@@ -104,19 +106,35 @@ class ClockSampler:
                 self.proc.kill()
             self.f.close()
 
+    def window(self, t0, t1):
+        """wall-clock bounds (time.time()) of the timed region"""
+        self.t0, self.t1 = t0, t1
+
     def summary(self):
+        import datetime
         try:
-            rows = [r.split(",") for r in open(self.path).read().strip().splitlines() if r.strip()]
+            rows = [[x.strip() for x in r.split(",")] for r in open(self.path).read().strip().splitlines() if r.strip()]
         except Exception:
             return None
+
+        def stamp(r):
+            try:
+                return datetime.datetime.strptime(r[0], "%Y/%m/%d %H:%M:%S.%f").timestamp()
+            except Exception:
+                return None
+        t0, t1 = getattr(self, "t0", None), getattr(self, "t1", None)
+        inside = [r for r in rows if t0 is not None and stamp(r) is not None and t0 - 0.05 <= stamp(r) <= t1 + 0.05]
+        if inside:
+            rows = inside
         if not rows:
             return None
-        sm = [float(r[1]) for r in rows if r[1].strip().replace(".", "").isdigit()]
-        mx = [float(r[2]) for r in rows if r[2].strip().replace(".", "").isdigit()]
+        num = lambda x: x.replace(".", "").isdigit()
+        sm = [float(r[2]) for r in rows if len(r) > 2 and num(r[2])]
+        mx = [float(r[3]) for r in rows if len(r) > 3 and num(r[3])]
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[q] for r in rows for q in range(4) if len(r) > 5 + q and r[5 + q].strip() == "Active"})
+        reasons = sorted({names[q] for r in rows for q in range(4) if len(r) > 6 + q and r[6 + q] == "Active"})
         return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
-                "reasons": reasons, "samples": len(rows)}
+                "reasons": reasons, "samples": len(rows), "in_timed_region": bool(inside)}
 
 
 def traffic_per_unit(kernel, prec):
@@ -169,15 +187,17 @@ def run_ours(args, rank, world, local):
     if args.prec == "fp32flux":
         g.set_precision(gm.GAM_FP32FLUX)
     zones = n * n * n
-    # warm-up (also builds the two step graphs)
-    g.run_steps(max(args.warmup, 3), check=False)
-    torch.cuda.synchronize()
-    if world > 1:
-        torch.distributed.barrier()
-    launches0 = g.status()["kernelLaunches"]
     with ClockSampler(local) as clk:
+        # warm-up (also builds the two step graphs)
+        g.run_steps(max(args.warmup, 3), check=False)
+        torch.cuda.synchronize()
+        if world > 1:
+            torch.distributed.barrier()
+        launches0 = g.status()["kernelLaunches"]
+        t0 = time.time()
         ms, rc = g.run_steps_timed(args.steps)
-    torch.cuda.synchronize()
+        torch.cuda.synchronize()
+        clk.window(t0, time.time())
     # the library's own count of the kernels its step graphs launched in the timed region
     timed_launches = g.status()["kernelLaunches"] - launches0
     if world > 1:
