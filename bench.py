@@ -45,8 +45,9 @@ def parse():
     ap.add_argument("--prec", default="fp64", choices=["fp64", "fp32flux"])
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--fp32-steps", type=int, default=200,
+                    help="steps of the FP32-flux vs FP64 comparison (the configuration's 200)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--cpu-n", type=int, default=64)
     ap.add_argument("--no-extras", action="store_true",
                     help="skip the FP32-flux and closure side measurements (run on 1 GPU only)")
     return ap.parse_args()
@@ -271,9 +272,9 @@ def run_ours(args, rank, world, local):
         "roofline": roof, "clocks": clocks, "status": st["status"], "t_sim": st["t"], "dt": st["dt"],
     }
     if world == 1 and not args.no_extras:
-        out["headline_extras"] = headline_extras(n, args.steps)
+        out["headline_extras"] = headline_extras(n, args.fp32_steps)
     if rank == 0 and not args.no_cpu_baseline:
-        out["cpu_baseline"] = cpu_baseline(args.cpu_n, steps=2)
+        out["cpu_baseline"] = cpu_baseline(n, steps=2)
     if world > 1:
         import torch.distributed as dist
         dist.barrier()
@@ -283,8 +284,8 @@ def run_ours(args, rank, world, local):
 
 def headline_extras(n, steps):
     """The rest of the headline metric on the same GPU: the FP32-flux path against the FP64 path on the
-    same problem (device ms per step and the L1 difference of the gas state after `steps` steps, relative
-    to the mean |value| per variable), and the cost of a step with the learned closure on the coarse
+    same problem (device ms per step and the L1 difference of the gas state after `steps` steps -- the
+    configuration's 200 by default -- relative to the mean |value| per variable), and the cost of a step with the learned closure on the coarse
     turbulence grid next to the plain coarse and the fine step (the closure's accuracy comes from its
     training run, kaiju_b200/closure_train.py)."""
     from kaiju_b200 import gamera as gm, turbulence as tu
@@ -331,47 +332,62 @@ def headline_extras(n, steps):
     return out
 
 
-def cpu_baseline(n, steps=2):
-    """The oracle (C++ restatement of the reference, OpenMP) on an n^3 sample of the same problem."""
+# The CPU sample: a 256 x 256 x 16 k-slab (|z| <= 8/256, through the blast centre) of the same warped
+# blast wave -- the GPU workload's own i-j planes and cell spacing, 1/16 of its cells, with zero-gradient
+# boundaries on every face. Its set-up (Corners2Grid and the 12^3-point IC quadrature on the host) is
+# excluded from the timing.
+SAMPLE_NK = 16
+
+
+def oracle_sample(n, threads):
     from oracle import pyoracle as po
     po.build()
+    h = SAMPLE_NK / (2.0 * n)
+    return po.Oracle(n, n, SAMPLE_NK, ic="BW", grid="warp", warp_amp=0.04, bounds=(-0.5, 0.5, -0.5, 0.5, -h, h),
+                     CFL=0.3, bc=[1] * 6, threads=threads)
+
+
+def sample_text(n, steps, warm, threads):
+    return (f"{n}x{n}x{SAMPLE_NK} k-slab (|z| <= {SAMPLE_NK}/{2 * n}, through the blast centre) of the same "
+            f"warped blast wave, {steps} timed steps after {warm} warm-up steps (set-up excluded), OpenMP "
+            f"{threads} threads; the oracle (C++ restatement of the Fortran reference, which cannot be "
+            f"compiled on this image)")
+
+
+def cpu_baseline(n, steps=2):
+    """The oracle (C++ restatement of the reference, OpenMP on all host cores) on the CPU sample."""
     threads = os.cpu_count() or 1
-    o = po.Oracle(n, n, n, ic="BW", grid="warp", warp_amp=0.04, bounds=(-0.5, 0.5) * 3, CFL=0.3, bc=[1] * 6,
-                  threads=threads)
+    o = oracle_sample(n, threads)
     o.step(1)
     t0 = time.perf_counter()
     o.step(steps)
     dt = time.perf_counter() - t0
     o.close()
-    return {"value": n ** 3 * steps / dt, "unit": "zone-updates/s", "cores": threads, "kind": "port",
-            "sample": f"{n}^3 sample of the same warped blast wave, {steps} timed steps after 1 warm-up "
-                      f"(set-up excluded), OpenMP {threads} threads"}
+    return {"value": n * n * SAMPLE_NK * steps / dt, "unit": "zone-updates/s", "cores": threads, "kind": "port",
+            "sample": sample_text(n, steps, 1, threads)}
 
 
 def run_reference(args, rank, world):
+    """The reference arm: the oracle on the CPU sample of this arm's workload, K timed steps after W
+    warm-up steps, on rank 0 only (the other ranks exit without work)."""
     if rank != 0:
         return None
-    n = args.cpu_n
-    from oracle import pyoracle as po
-    po.build()
+    n = args.n
     threads = os.cpu_count() or 1
-    o = po.Oracle(n, n, n, ic="BW", grid="warp", warp_amp=0.04, bounds=(-0.5, 0.5) * 3, CFL=0.3, bc=[1] * 6,
-                  threads=threads)
-    o.step(max(1, min(args.warmup, 2)))
-    steps = max(1, min(args.steps, 4))
+    o = oracle_sample(n, threads)
+    o.step(max(1, args.warmup))
+    steps = max(1, args.steps)
     t0 = time.perf_counter()
     o.step(steps)
     dt = time.perf_counter() - t0
     o.close()
-    v = n ** 3 * steps / dt
-    sample = (f"{n}^3 sample of the same warped blast wave (256^3 is the GPU workload), {steps} timed steps, "
-              f"OpenMP {threads} threads; C++ restatement of the Fortran reference (no Fortran compiler on "
-              f"this image)")
+    v = n * n * SAMPLE_NK * steps / dt
     return {"metric": METRIC, "value": v, "unit": "zone-updates/s", "n_gpus": world, "steps": steps,
             "warmup": args.warmup, "ms_per_step": dt / steps * 1e3, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference",
-            "config": workload_config(args.n, "fp64"),
-            "cpu_baseline": {"value": v, "unit": "zone-updates/s", "cores": threads, "kind": "port", "sample": sample},
+            "config": workload_config(n, "fp64", {"parallelism": f"replicas x{world}"}),
+            "cpu_baseline": {"value": v, "unit": "zone-updates/s", "cores": threads, "kind": "port",
+                             "sample": sample_text(n, steps, max(1, args.warmup), threads)},
             "e2e": {"value": v, "unit": "zone-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
 
 

@@ -141,6 +141,16 @@ int gam_gpu_create_from_corners(gam_gpu_t** h, const gam_model_c* m, const doubl
  *   reference), sampled at cell centres: rho = 1, P = 1, Vx = 0.5 tanh((y-0.5)/a), Vy = amp*(2u-1) with u
  *   a counter-based hash of (seed, i, j, k), B = (Bx, 0, 0). icPar = {a, Bx, amp, seed}, nPar >= 4. */
 #define GAM_IC_KH 3
+/*   The accuracy cases of the reference's tests/cases/testCases.pf, with the values of their decks
+ *   (tests/cases/*.xml) in icPar and Model%gamma as the deck leaves it (1.4 for ADV1D):
+ *   GAM_IC_ADV1D:  initADV1D (src/gamera/prob.F90:671-736), four density shapes at Vx = 1, no field; nPar 0.
+ *   GAM_IC_ADV2D:  initADV2D (prob.F90:739-797), icPar = {d0, P0, V0, alpha, R0, x0, y0}.
+ *   GAM_IC_LOOP2D: initLoop (prob.F90:436-500), icPar = {d0, P0, V0, Vz0, alpha, A0, R0, x0, y0}.
+ *   GAM_IC_ALFVEN: initALFVEN (prob.F90:1027-1083), icPar = {d0, P0, B_para, V_para, alp}. */
+#define GAM_IC_ADV1D 4
+#define GAM_IC_ADV2D 5
+#define GAM_IC_LOOP2D 6
+#define GAM_IC_ALFVEN 7
 int gam_gpu_create_from_corners_ic(gam_gpu_t** h, const gam_model_c* m, const double* xyz, int ic,
                                    const double* icPar, int nPar);
 
@@ -252,23 +262,35 @@ int gam_gpu_ensemble_set_queue(gam_ensemble_t* e, int on);
  * tensor-memory-accelerator copies (cp.async.bulk.tensor, one thread per tile); 0 with per-element
  * cp.async. Results do not depend on it. */
 #define GAM_TILE_TMA 3
+/* GAM_TILE_STAGE_WAIT: 1 (default) the flux and E-field kernels wait for their staged tile up to a bound of
+ * 2^20 mbarrier polls; 0 makes that wait give up at once. Either way a CTA whose wait gave up still waits
+ * (with a far larger bound) for its own tensor copies to land before it exits, writes nothing, and the step
+ * returns GAM_ERR_TIMEOUT. Setting 0 exercises a host's handling of that error without a hung GPU; the
+ * state of that step is not valid. */
+#define GAM_TILE_STAGE_WAIT 4
 int gam_gpu_set_tile(gam_gpu_t* h, int what, int value);
 int gam_gpu_ensemble_autotune(gam_ensemble_t* e, int steps, int* fluxRows, int* queue);
 
-/* DivB for callers that cannot allocate device memory (no counterpart in the reference).
+/* DivB for callers that cannot allocate device memory. This entry point has no counterpart in the
+ * reference; its formula is the reference's DivB (src/gamera/gridutils.F90:717-770).
  * Some hosts cannot call cudaMalloc: device arrays owned by another runtime (OpenACC or CUDA Fortran
  * data regions, a coupler's memory pool) or code running where an allocation would synchronise the
  * device or upset its memory accounting. This entry point needs no handle and allocates nothing: it
  * reads magflux_dev, a device copy of State%magFlux in the Fortran layout (Ni+1,Nj+1,Nk+1,3) with
- * Ni = Nip+2*nG etc., and writes the sum over active cells of |net face flux| (DivB,
- * src/gamera/gridutils.F90:717-770) to the device double *tot_dev. Its only scratch is a file-scope
- * device array sized for GAM_DIVB_NOALLOC_MAX_CELLS active cells (512 KiB per GPU that loads the
- * library, held until exit); larger grids are rejected with GAM_ERR_ARG. The first call on a device
- * looks up that array's device address, so make it before capturing a stream. Kernels run on the
- * legacy default stream; synchronise before reading *tot_dev. All calls share the scratch array, so
- * calls that overlap on the GPU (from several host threads or streams) race. */
+ * Ni = Nip+2*nG etc., and bflux0_dev, a device copy of Grid%bFlux0 (Ni,Nj,Nk,3) for a problem with a
+ * background field (Model%doBackground) or NULL without one, and writes the sum over active cells of
+ * |net face flux| (magFlux plus bFlux0, as DivB sums it with doTot) to the device double *tot_dev. Its
+ * only scratch is a file-scope device array sized for GAM_DIVB_NOALLOC_MAX_CELLS active cells (512 KiB
+ * per GPU that loads the library, held until exit); larger grids are rejected with GAM_ERR_ARG. The
+ * first call on a device looks up that array's device address, so make it before capturing a stream;
+ * the address is kept until exit, so the entry point is not for use on a device after cudaDeviceReset.
+ * Kernels run on the legacy default stream; synchronise before reading *tot_dev. A CUDA error already
+ * pending when it is called is returned as GAM_ERR_CUDA (and left pending) and nothing is launched. All
+ * calls share the scratch array, so calls that overlap on the GPU (from several host threads or
+ * streams) race. */
 #define GAM_DIVB_NOALLOC_MAX_CELLS (256LL * 256LL * 256LL)
-int gam_divb_noalloc(const double* magflux_dev, int Nip, int Njp, int Nkp, int nG, double* tot_dev);
+int gam_divb_noalloc(const double* magflux_dev, const double* bflux0_dev, int Nip, int Njp, int Nkp, int nG,
+                     double* tot_dev);
 /* ---- tiled runs: one problem split along k into tiles (src/gamera/mpi/gamapp_mpi.F90) ----
  * A tile is a handle created for its k range (its corners with 4 ghost layers of the global grid)
  * with GAM_BC_HALO on every k face that borders another tile (both k faces of every tile when the

@@ -182,6 +182,7 @@ int alloc_handle(gam_gpu* G, const gam_model_c* m) {
     p.predFixLFM = m->predFixLFM ? 1 : 0;
     p.dtActive = m->dtActive ? 1 : 0;
     p.bwD0 = m->bwD0; p.bwP0 = m->bwP0;
+    p.stageWait = STAGE_WAIT;
     if (m->doRing) {
         h.ring.NumR = m->ringNumR;
         for (int r = 0; r < 32; ++r) h.ring.Nch[r] = r < m->ringNumR ? m->ringNch[r] : 0;
@@ -400,7 +401,9 @@ static int create_from_corners(gam_gpu_t** out, const gam_model_c* m, const doub
     *out = nullptr;
     int rc = check_model(m);
     if (rc) return rc;
-    if (ic != GAM_IC_OT2D && ic != GAM_IC_BW && ic != GAM_IC_LFMBW && !(ic == GAM_IC_KH && icPar)) return GAM_ERR_ARG;
+    bool caseIC = ic == GAM_IC_ADV1D || ic == GAM_IC_ADV2D || ic == GAM_IC_LOOP2D || ic == GAM_IC_ALFVEN;
+    if (ic != GAM_IC_OT2D && ic != GAM_IC_BW && ic != GAM_IC_LFMBW && !((ic == GAM_IC_KH || caseIC) && icPar))
+        return GAM_ERR_ARG;
     if ((m->Nip % 8) != 0) return GAM_ERR_ARG;   // Corners2Grid divisibility check (init.F90:830-834)
     if ((bg != nullptr) != (m->doBackground != 0)) return GAM_ERR_ARG;
     gam_gpu* G = new (std::nothrow) gam_gpu();
@@ -429,6 +432,14 @@ int gam_gpu_create_from_corners(gam_gpu_t** out, const gam_model_c* m, const dou
 int gam_gpu_create_from_corners_ic(gam_gpu_t** out, const gam_model_c* m, const double* xyz, int ic,
                                    const double* icPar, int nPar) {
     if (ic == GAM_IC_KH && (!icPar || nPar < 4 || !(icPar[0] > 0.0) || icPar[3] < 0.0)) return GAM_ERR_ARG;
+    static const int casePars[4] = {0, 7, 9, 5};   // ADV1D, ADV2D, LOOP2D, ALFVEN
+    if (ic >= GAM_IC_ADV1D && ic <= GAM_IC_ALFVEN) {
+        int need = casePars[ic - GAM_IC_ADV1D];
+        if (nPar < need || (need > 0 && !icPar) || nPar > 10) return GAM_ERR_ARG;
+        double par[10] = {0.0};
+        for (int n = 0; n < nPar; ++n) par[n] = icPar[n];
+        return create_from_corners(out, m, xyz, ic, nullptr, par);
+    }
     return create_from_corners(out, m, xyz, ic, nullptr, icPar);
 }
 
@@ -498,7 +509,7 @@ int gam_gpu_set_scalars(gam_gpu_t* G, double t, double dt, double dt0, int ts, d
     Handle& h = G->h;
     h.hScal->t = t; h.hScal->dt = dt; h.hScal->dt0 = dt0; h.hScal->ts = ts; h.hScal->time = time;
     h.hScal->otime = otime; h.hScal->dtMinBits = 0x7FF0000000000000ull; h.hScal->nanCount = 0;
-    h.hScal->status = 0; h.hScal->sticky = 0;
+    h.hScal->status = 0; h.hScal->sticky = 0; h.hScal->waitFail = 0u;
     int rc = upload_scalars(G);
     if (rc) return rc;
     CK(cudaStreamSynchronize(h.stream));
@@ -619,6 +630,12 @@ int gam_gpu_set_tile(gam_gpu_t* G, int what, int value) {
     if (what == GAM_TILE_TMA) {
         if (value != 0 && value != 1) return GAM_ERR_ARG;
         if (h.tileTma != (value != 0)) { h.tileTma = value != 0; destroy_graphs(h); }
+        return GAM_OK;
+    }
+    if (what == GAM_TILE_STAGE_WAIT) {   // 1: the normal bound; 0: give up at once (tests the timeout path)
+        if (value != 0 && value != 1) return GAM_ERR_ARG;
+        unsigned int polls = value ? STAGE_WAIT : 0u;
+        if (h.p.stageWait != polls) { h.p.stageWait = polls; destroy_graphs(h); }
         return GAM_OK;
     }
     if (what != GAM_TILE_FLUX_ROWS || (value != 4 && value != 8)) return GAM_ERR_ARG;

@@ -51,7 +51,13 @@ struct Par {
     int predFixLFM;                 // the LFM blast wave's predictor fix
     int dtActive;                   // CalcDT over the active cells only
     double bwD0, bwP0;              // gas of the LFM blast wave's fixed shells
+    // mbarrier polls before the flux and E-field kernels' wait on their staged tile gives up (GAM_TILE_STAGE_WAIT;
+    // default STAGE_WAIT). After giving up a CTA still waits, with the far larger STAGE_DRAIN bound, for its own
+    // copies to land before it exits, and the step reports GAM_ERR_TIMEOUT.
+    unsigned int stageWait;
 };
+constexpr unsigned int STAGE_WAIT = 1u << 20;
+constexpr unsigned int STAGE_DRAIN = 1u << 28;
 
 // Time-dependent scalars kept on the device so a whole step can be captured and replayed.
 struct Scal {

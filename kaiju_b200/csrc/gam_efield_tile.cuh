@@ -54,7 +54,6 @@ template <int ED, bool TMA = false> struct ETile {
 };
 // Tensor maps of the staged planes in layout order: Vf 0-2, face/hbA/nbA of dT1, face/hbA/nbA of dT2, rho
 struct EdgeMaps { CUtensorMap m[10]; };
-constexpr uint32_t EDGE_WAIT = 1u << 20;   // mbarrier polls before the staging wait gives up
 __device__ __forceinline__ int bidx(BoxC b, int di, int dj, int dk) {
     return (di - b.oi) + b.ni * ((dj - b.oj) + b.nj * (dk - b.ok));
 }
@@ -92,9 +91,9 @@ k_edge_tile(Lay L, Par p, const __grid_constant__ EdgeMaps maps, EdgeSrc<S> in, 
             ld(8, TL::oN2, b4t1);
             ld(9, TL::oR, bR);
         }
-        if (!tc::mbar_wait(bar, 0u, EDGE_WAIT)) {
+        if (!tc::mbar_wait(bar, 0u, p.stageWait)) {
             if (tid == 0) atomicOr(&sc->waitFail, 1u);
-            tc::mbar_wait(bar, 0u, EDGE_WAIT);   // let copies in flight land before the CTA's shared memory goes
+            tc::mbar_wait(bar, 0u, STAGE_DRAIN);   // let copies in flight land before the CTA's shared memory goes
             return;
         }
     } else {

@@ -42,7 +42,6 @@ template <typename S, int D, int FR, bool TMA = false> constexpr size_t flux_sme
 // Tensor maps of the staged planes: the reconstruction planes (W 0-4, volume, B 0-2) and the limiter
 // planes (W 0-4, B 0-2), each with the box of the sweep direction
 struct FluxMaps { CUtensorMap rec[9]; CUtensorMap lim[8]; };
-constexpr uint32_t FLUX_WAIT = 1u << 20;   // mbarrier polls before the staging wait gives up
 
 // A flux times the face area in the storage type: for float storage a float product, which is the double
 // product of the two floats (exact) rounded once, so the same value without the conversions
@@ -231,9 +230,9 @@ k_flux_tile(Lay L, Par p, const __grid_constant__ FluxMaps maps, FluxSrc<S> in, 
 #pragma unroll
             for (int q = 0; q < NL; ++q) tma::load3(sLim + q * LB, &maps.lim[q], rx, ly, lz, bar);
         }
-        if (!tc::mbar_wait(bar, 0u, FLUX_WAIT)) {
+        if (!tc::mbar_wait(bar, 0u, p.stageWait)) {
             if (tid == 0) atomicOr(&sc->waitFail, 1u);
-            tc::mbar_wait(bar, 0u, FLUX_WAIT);   // let copies in flight land before the CTA's shared memory goes
+            tc::mbar_wait(bar, 0u, STAGE_DRAIN);   // let copies in flight land before the CTA's shared memory goes
             return;
         }
     } else {

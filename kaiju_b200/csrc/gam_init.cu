@@ -291,6 +291,7 @@ __device__ __forceinline__ unsigned long long splitmix64(unsigned long long x) {
     return z ^ (z >> 31);
 }
 struct KHPar { double a, Bx, amp; unsigned long long seed; };
+struct ICPar { double v[10]; };
 __global__ void k_ic_kh(Lay L, Par p, GridP g, StateP s, KHPar kh) {
     int ni = L.Nip + 1, nj = L.Njp + 1, nk = L.Nkp + 1;
     long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
@@ -325,8 +326,9 @@ struct BWGas {
 // prob.F90:190-298 deck defaults (the Cartesian blast wave) and tests/gamera/lfmbw.xml (ICs/lfmbw.F90:33-104)
 static const BWGas kBW = {0.0, 0.0, 0.0, 1.0, 0.1, 100.0, 1.0, 0.1};
 static const BWGas kLFMBW = {-50.0, 30.0, 0.0, 1.0, 0.1, 10.0, 1.0, 20.0};
-// GasIC2State (gridutils.F90:144-189) on active cells
-__global__ void k_ic_bw_gas(Lay L, Par p, Corners X, const double* vol, StateP s, BWGas ic) {
+// GasIC2State (gridutils.F90:144-189) on active cells, for a primitive-state functor W(x, y, z, W[5])
+template <class GasF>
+__global__ void k_ic_quad_gas(Lay L, Par p, Corners X, const double* vol, StateP s, GasF ic) {
     long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (t >= (long long)L.Nip * L.Njp * L.Nkp) return;
     int i = L.is() + (int)(t % L.Nip);
@@ -343,21 +345,23 @@ __global__ void k_ic_bw_gas(Lay L, Par p, Corners X, const double* vol, StateP s
     double IntE = P / (p.gamma - 1.0);
     s.gas[0][c] = D; s.gas[1][c] = Mx; s.gas[2][c] = My; s.gas[3][c] = Mz; s.gas[4][c] = IntE + KinE;
 }
-// VectorPot2Flux (gridutils.F90:193-237), A = (0, bSclz*x, bScl*(y-x)), bScl = 1/sqrt(2.0) in single
-// precision as the reference literal, bSclz = 0; edge integrals with the 12-point rule
-__device__ double edgeIntegralA(const double* e1, const double* e2, double bScl) {
+// VectorPot2Flux (gridutils.F90:193-237): 12-point edge integrals of a vector potential A(x, y, z, A[3])
+// on the lower edges of every cell but the last ghost layer, then the face fluxes as their circulations
+template <class PotF>
+__device__ double edgeIntegral(const double* e1, const double* e2, const PotF& A) {   // quadrature.F90:345-370
     double dR2[3], xBar[3], eInt[3] = {0.0, 0.0, 0.0};
     for (int x = 0; x < 3; ++x) { dR2[x] = 0.5 * (e2[x] - e1[x]); xBar[x] = 0.5 * (e2[x] + e1[x]); }
     for (int a = 0; a < 12; ++a) {
-        double xp[3];
+        double xp[3], Ap[3];
         for (int x = 0; x < 3; ++x) xp[x] = xBar[x] + c_gA[a] * dR2[x];
-        double Ap[3] = {0.0, 0.0 * xp[0], bScl * (xp[1] - xp[0])};
+        A(xp[0], xp[1], xp[2], Ap);
         for (int x = 0; x < 3; ++x) eInt[x] = eInt[x] + 0.5 * c_gW[a] * Ap[x];
     }
     double dR[3] = {e1[0] - e2[0], e1[1] - e2[1], e1[2] - e2[2]};
     return eInt[0] * dR[0] + eInt[1] * dR[1] + eInt[2] * dR[2];
 }
-__global__ void k_ic_bw_la(Lay L, Corners X, Out3 lA, double bScl) {
+template <class PotF>
+__global__ void k_ic_vecpot_la(Lay L, Corners X, Out3 lA, PotF A) {
     int ni = L.Ni - 1, nj = L.Nj - 1, nk = L.Nk - 1;
     long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (t >= (long long)ni * nj * nk) return;
@@ -367,11 +371,11 @@ __global__ void k_ic_bw_la(Lay L, Corners X, Out3 lA, double bScl) {
     double e0[3], eI[3], eJ[3], eK[3];
     corner(L, X, i, j, k, e0); corner(L, X, i + 1, j, k, eI); corner(L, X, i, j + 1, k, eJ); corner(L, X, i, j, k + 1, eK);
     long long c = L.at(i, j, k);
-    lA.v[0][c] = edgeIntegralA(eI, e0, bScl);
-    lA.v[1][c] = edgeIntegralA(eJ, e0, bScl);
-    lA.v[2][c] = edgeIntegralA(eK, e0, bScl);
+    lA.v[0][c] = edgeIntegral(eI, e0, A);
+    lA.v[1][c] = edgeIntegral(eJ, e0, A);
+    lA.v[2][c] = edgeIntegral(eK, e0, A);
 }
-__global__ void k_ic_bw_flux(Lay L, Out3 lA, StateP s) {
+__global__ void k_ic_vecpot_flux(Lay L, Out3 lA, StateP s) {
     int ni = L.Ni - 1, nj = L.Nj - 1, nk = L.Nk - 1;
     long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (t >= (long long)ni * nj * nk) return;
@@ -384,6 +388,88 @@ __global__ void k_ic_bw_flux(Lay L, Out3 lA, StateP s) {
     s.mf[1][c] = -(A0[c] - A0[ck] + A2[c + 1] - A2[c]);
     s.mf[2][c] = A0[c] - A0[cj] + A1[c + 1] - A1[c];
 }
+// the blast waves' A = (0, 0*x, bScl*(y-x)), bScl = B0/sqrt(2.0) with sqrt(2.0) a default-real literal
+// (prob.F90:271-278, ICs/lfmbw.F90)
+struct BWPot {
+    double bScl;
+    __device__ void operator()(double x, double y, double z, double* A) const {
+        (void)z;
+        A[0] = 0.0; A[1] = 0.0 * x; A[2] = bScl * (y - x);
+    }
+};
+
+// ---- the accuracy cases of tests/cases/testCases.pf. Fortran default-real literals keep their float values.
+#define F32L(x) ((double)(x##f))
+// cell-centre primitive state written as conserved Gas on the cells is..ie+1 (the loops of prob.F90)
+__device__ __forceinline__ void putPrim(const Par& p, StateP& s, long long c, double Rho, double Vx, double Vy,
+                                        double Vz, double P) {
+    s.gas[0][c] = Rho;
+    s.gas[1][c] = Rho * Vx; s.gas[2][c] = Rho * Vy; s.gas[3][c] = Rho * Vz;
+    double KinE = 0.5 * Rho * (sq(Vx) + sq(Vy) + sq(Vz));
+    s.gas[4][c] = KinE + P / (p.gamma - 1);
+}
+// ic: 4 ADV1D (prob.F90:671-736), 5 ADV2D (:739-797), 6 the gas of LOOP2D (:436-482); pr = the deck values
+__global__ void k_ic_cases_cc(Lay L, Par p, GridP g, StateP s, int ic, ICPar pr) {
+    int ni = L.Nip + 1, nj = L.Njp + 1, nk = L.Nkp + 1;
+    long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (t >= (long long)ni * nj * nk) return;
+    int i = L.is() + (int)(t % ni);
+    long long q = t / ni;
+    int j = L.js() + (int)(q % nj), k = L.ks() + (int)(q / nj);
+    long long c = L.at(i, j, k);
+    double xc = g.xyzcc[0][c], yc = g.xyzcc[1][c];
+    if (ic == 4) {
+        const double f01sq = (double)(0.1f * 0.1f);   // 0.1**2 of two default reals
+        double Rho0 = F32L(0.1);
+        double Rho1 = exp(-sq((xc + F32L(0.7)) / F32L(0.05)));
+        double Rho2 = (fabs(xc + F32L(0.3)) <= F32L(0.1)) ? 1.0 : 0.0;
+        double Rho3 = (fabs(xc - F32L(0.1)) <= F32L(0.1)) ? 1.0 - fabs(10.0 * (xc - F32L(0.1))) : 0.0;
+        double Rho4 = ((f01sq - sq(xc - F32L(0.5))) >= 0) ? 10.0 * sqrt(f01sq - sq(xc - F32L(0.5))) : 0.0;
+        putPrim(p, s, c, Rho0 + Rho1 + Rho2 + Rho3 + Rho4, 1.0, 0.0, 0.0, 1.0);
+    } else if (ic == 5) {   // {d0, P0, V0, alpha, R0, x0, y0}
+        double Vx = pr.v[2] * sin(pr.v[3] * PI / 180.0), Vy = pr.v[2] * cos(pr.v[3] * PI / 180.0);
+        double r = sqrt(sq(xc - pr.v[5]) + sq(yc - pr.v[6]));
+        double Rho = (r < pr.v[4]) ? pr.v[0] * 2.0 : pr.v[0];
+        putPrim(p, s, c, Rho, Vx, Vy, 0.0, pr.v[1]);
+    } else {                // {d0, P0, V0, Vz0, alpha, A0, R0, x0, y0}
+        double Vx = pr.v[2] * sin(pr.v[4] * PI / 180.0), Vy = pr.v[2] * cos(pr.v[4] * PI / 180.0);
+        putPrim(p, s, c, pr.v[0], Vx, Vy, pr.v[3], pr.v[1]);
+        return;
+    }
+    s.mf[0][c] = 0.0; s.mf[1][c] = 0.0; s.mf[2][c] = 0.0;
+}
+// VectorPot_Loop2D (prob.F90:489-499): Az = max(0, A0 (R0 - r)) about (x0, y0)
+struct LoopPot {
+    double A0, R0, x0, y0;
+    __device__ void operator()(double x, double y, double z, double* A) const {
+        (void)z;
+        double r = sqrt(sq(x - x0) + sq(y - y0));
+        A[0] = 0.0; A[1] = 0.0;
+        A[2] = dmax(0.0, A0 * (R0 - r));
+    }
+};
+// initALFVEN (prob.F90:1027-1083): GasIC_ALF (:1072-1082) and VectorPot_ALF (:1063-1070)
+struct AlfGas {
+    double Rho0, P0, Bpar, Vpar, alp;
+    __device__ void operator()(double x, double y, double z, double* W) const {
+        (void)z;
+        double ph = 2 * PI * (x * cos(alp) + y * sin(alp));
+        W[0] = Rho0;
+        W[1] = Vpar * cos(alp) - F32L(0.1) * sin(ph) * sin(alp);
+        W[2] = Vpar * sin(alp) + F32L(0.1) * sin(ph) * cos(alp);
+        W[3] = F32L(0.1) * cos(ph);
+        W[4] = P0;
+    }
+};
+struct AlfPot {
+    double Bpar, alp;
+    __device__ void operator()(double x, double y, double z, double* A) const {
+        double ph = 2 * PI * (x * cos(alp) + y * sin(alp));
+        A[0] = Bpar * sin(alp) * z;
+        A[1] = -1.0 * Bpar * cos(alp) * z + F32L(0.1) * sin(ph) / (2 * PI * cos(alp));
+        A[2] = F32L(0.1) * cos(ph) / (2 * PI);
+    }
+};
 
 // ------------------------------------------------------------------------------------ background field
 // AddB0 (background.F90:20-167) for the built-in background functions: per cell, the 12x12-point face
@@ -589,10 +675,33 @@ int init_problem(Handle& h, int ic, const BgSpec* bg, const double* icPar) {
         long long n = (long long)(L.Nip + 1) * (L.Njp + 1) * (L.Nkp + 1);
         k_ic_kh<<<nb(n, 256), 256, 0, st>>>(L, h.p, g, s, kh);
         h.launches++;
+    } else if (ic >= 4 && ic <= 7) {
+        if (!icPar) return 1;
+        ICPar pr;
+        for (int n = 0; n < 10; ++n) pr.v[n] = icPar[n];
+        Corners X = {{h.xyz[0], h.xyz[1], h.xyz[2]}};
+        if (ic == 7) {
+            long long n = (long long)L.Nip * L.Njp * L.Nkp;
+            AlfGas W = {pr.v[0], pr.v[1], pr.v[2], pr.v[3], pr.v[4]};
+            k_ic_quad_gas<<<nb(n, 128), 128, 0, st>>>(L, h.p, X, h.volume, s, W);
+        } else {
+            long long n = (long long)(L.Nip + 1) * (L.Njp + 1) * (L.Nkp + 1);
+            k_ic_cases_cc<<<nb(n, 256), 256, 0, st>>>(L, h.p, g, s, ic, pr);
+        }
+        h.launches++;
+        if (ic == 6 || ic == 7) {
+            Out3 lA = {{h.E[0], h.E[1], h.E[2]}};   // E planes as scratch for the edge integrals of A
+            long long ne = (long long)(L.Ni - 1) * (L.Nj - 1) * (L.Nk - 1);
+            if (ic == 6) k_ic_vecpot_la<<<nb(ne, 128), 128, 0, st>>>(L, X, lA, LoopPot{pr.v[5], pr.v[6], pr.v[7], pr.v[8]});
+            else k_ic_vecpot_la<<<nb(ne, 128), 128, 0, st>>>(L, X, lA, AlfPot{pr.v[2], pr.v[4]});
+            k_ic_vecpot_flux<<<nb(ne, 256), 256, 0, st>>>(L, lA, s);
+            cudaMemsetAsync(h.E[0], 0, sizeof(double) * L.E * 3, st);   // the step relies on unwritten E edges being zero
+            h.launches += 2;
+        }
     } else {
         Corners X = {{h.xyz[0], h.xyz[1], h.xyz[2]}};
         long long n = (long long)L.Nip * L.Njp * L.Nkp;
-        k_ic_bw_gas<<<nb(n, 128), 128, 0, st>>>(L, h.p, X, h.volume, s, ic == 2 ? kLFMBW : kBW);
+        k_ic_quad_gas<<<nb(n, 128), 128, 0, st>>>(L, h.p, X, h.volume, s, ic == 2 ? kLFMBW : kBW);
         // prob/doBack (prob.F90:228-269): with a uniform background the blast field is held as B0 and
         // the residual field starts at zero
         bool fieldAsBackground = bg && bg->type == 1;
@@ -600,8 +709,8 @@ int init_problem(Handle& h, int ic, const BgSpec* bg, const double* icPar) {
             Out3 lA = {{h.E[0], h.E[1], h.E[2]}};   // E planes as scratch for the edge integrals of A
             double bScl = 1.0 / (double)sqrtf(2.0f);
             long long ne = (long long)(L.Ni - 1) * (L.Nj - 1) * (L.Nk - 1);
-            k_ic_bw_la<<<nb(ne, 128), 128, 0, st>>>(L, X, lA, bScl);
-            k_ic_bw_flux<<<nb(ne, 256), 256, 0, st>>>(L, lA, s);
+            k_ic_vecpot_la<<<nb(ne, 128), 128, 0, st>>>(L, X, lA, BWPot{bScl});
+            k_ic_vecpot_flux<<<nb(ne, 256), 256, 0, st>>>(L, lA, s);
             // the step relies on every E edge its kernels do not write being zero
             cudaMemsetAsync(h.E[0], 0, sizeof(double) * L.E * 3, st);   // the E planes are contiguous
             h.launches += 2;

@@ -4,11 +4,12 @@
 // arrays are owned by another runtime (OpenACC/CUDA Fortran data regions, a coupler's memory pool), or
 // a caller running inside a section where allocation is forbidden because it would synchronise the
 // device or break its memory accounting. gam_gpu_divb needs a handle, and the handle owns a pool
-// allocated with cudaMalloc. gam_divb_noalloc computes the same diagnostic (DivB,
-// src/gamera/gridutils.F90:717-770) straight from a caller-provided device copy of magFlux and writes
-// the total to a caller-provided device double; its only scratch -- one partial sum per 256-cell
-// block -- lives in the file-scope array below, which every GPU that loads this library holds until
-// the process exits (512 KiB).
+// allocated with cudaMalloc. gam_divb_noalloc computes the same diagnostic straight from caller-provided
+// device copies of magFlux (and of the background face fluxes bFlux0 when the problem has a background
+// field) and writes the total to a caller-provided device double. The formula is the reference's DivB
+// (src/gamera/gridutils.F90:717-770; the function itself has no counterpart there). Its only scratch --
+// one partial sum per 256-cell block -- lives in the file-scope array below, which every GPU that loads
+// this library holds until the process exits (512 KiB).
 #include <cstdio>
 #include <mutex>
 #include <cuda_runtime.h>
@@ -29,8 +30,10 @@ constexpr int kMaxDevices = 64;
 std::mutex g_mu;
 double* g_addr[kMaxDevices] = {nullptr};   // host-side device address of g_divb_partials, per device
 
-// magFlux(isg:ieg+1, jsg:jeg+1, ksg:keg+1, 1:3) in the Fortran layout; active cells only
-__global__ void k_divb_blocks(const double* __restrict__ mf, int Nip, int Njp, int Nkp, int nG, double* partials) {
+// magFlux(isg:ieg+1, jsg:jeg+1, ksg:keg+1, 1:3) and, when given, Grid%bFlux0(isg:ieg, jsg:jeg, ksg:keg, 1:3)
+// in the Fortran layout; active cells only. Per cell |dFi + dFj + dFk + dFi0 + dFj0 + dFk0| as DivB sums it.
+__global__ void k_divb_blocks(const double* __restrict__ mf, const double* __restrict__ bf0, int Nip, int Njp,
+                              int Nkp, int nG, double* partials) {
     long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     long long n = (long long)Nip * Njp * Nkp;
     double v = 0.0;
@@ -44,7 +47,15 @@ __global__ void k_divb_blocks(const double* __restrict__ mf, int Nip, int Njp, i
         double dFi = mf[c] - mf[c + 1];
         double dFj = mf[plane + c] - mf[plane + c + fi];
         double dFk = mf[2 * plane + c] - mf[2 * plane + c + fi * fj];
-        v = fabs(dFi + dFj + dFk);
+        double dFi0 = 0.0, dFj0 = 0.0, dFk0 = 0.0;
+        if (bf0) {
+            long long ci = fi - 1, cj = fj - 1, cplane = ci * cj * (fk - 1);
+            long long b = i + ci * (j + cj * k);
+            dFi0 = bf0[b] - bf0[b + 1];
+            dFj0 = bf0[cplane + b] - bf0[cplane + b + ci];
+            dFk0 = bf0[2 * cplane + b] - bf0[2 * cplane + b + ci * cj];
+        }
+        v = fabs(dFi + dFj + dFk + dFi0 + dFj0 + dFk0);
     }
     for (int off = 16; off > 0; off >>= 1) v += __shfl_down_sync(0xffffffffu, v, off);
     __shared__ double ws[kThreads / 32];
@@ -75,7 +86,9 @@ __global__ void k_divb_total(const double* partials, int nb, double* out) {
     }
 }
 
-// Device address of the static scratch on the current device, looked up once per device.
+// Device address of the static scratch on the current device, looked up once per device and kept for the
+// life of the process (a cudaDeviceReset of that device invalidates it; the entry point is not for use on
+// a device after a reset).
 int scratch_address(double** out) {
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
@@ -97,8 +110,15 @@ int scratch_address(double** out) {
 
 }  // namespace
 
-extern "C" int gam_divb_noalloc(const double* magflux_dev, int Nip, int Njp, int Nkp, int nG, double* tot_dev) {
+extern "C" int gam_divb_noalloc(const double* magflux_dev, const double* bflux0_dev, int Nip, int Njp, int Nkp,
+                                int nG, double* tot_dev) {
     if (!magflux_dev || !tot_dev || Nip < 1 || Njp < 1 || Nkp < 1 || nG < 0) return GAM_ERR_ARG;
+    // an error left pending by the caller's own work is reported, not cleared, and nothing is launched
+    cudaError_t pending = cudaPeekAtLastError();
+    if (pending != cudaSuccess) {
+        std::fprintf(stderr, "gam_divb_noalloc: an earlier CUDA error is pending: %s\n", cudaGetErrorString(pending));
+        return GAM_ERR_CUDA;
+    }
     long long n = (long long)Nip * Njp * Nkp;
     if (n > kMaxCells) {
         std::fprintf(stderr, "gam_divb_noalloc: %lld active cells exceed the static limit of %lld\n", n, kMaxCells);
@@ -108,7 +128,7 @@ extern "C" int gam_divb_noalloc(const double* magflux_dev, int Nip, int Njp, int
     int rc = scratch_address(&partials);
     if (rc) return rc;
     int nb = (int)((n + kThreads - 1) / kThreads);
-    k_divb_blocks<<<nb, kThreads>>>(magflux_dev, Nip, Njp, Nkp, nG, partials);
+    k_divb_blocks<<<nb, kThreads>>>(magflux_dev, bflux0_dev, Nip, Njp, Nkp, nG, partials);
     k_divb_total<<<1, 1024>>>(partials, nb, tot_dev);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) { std::fprintf(stderr, "gam_divb_noalloc: launch: %s\n", cudaGetErrorString(e)); return GAM_ERR_CUDA; }

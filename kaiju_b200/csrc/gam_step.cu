@@ -8,6 +8,7 @@
 // CT update, C2P with floors and the dt reduction stay FP64 in both.
 #include <cstdio>
 #include <cmath>
+#include <nvtx3/nvToolsExt.h>
 #include "gam_common.cuh"
 #include "gam_step.cuh"
 #include "gam_lfm.cuh"
@@ -457,6 +458,7 @@ __global__ void k_dt_finalize(Par p, Scal* sc, int mode) {
     sc->lastNan = sc->nanCount;
     sc->dtMinBits = 0x7FF0000000000000ull;
     sc->nanCount = 0u;
+    sc->waitFail = 0u;   // reported in this step's status (and the sticky OR); the next step starts clear
 }
 
 // ================================================================================ boundary conditions
@@ -822,9 +824,26 @@ int kernels_per_step(const Handle& h) {
     return n;
 }
 
+// NVTX ranges named after the reference's timers of the step (mhdgroup.F90:30-70, stress.F90:78-150,
+// gamapp.F90:76-99): a profiler attached to an eager (non-graph) step sees its kernels under the same
+// names as the reference's printClocks tree (Advance > Gamera > Predictor, E-Field, Fluxes, ...).
+static const char* const kPhaseRange[NPHASE] = {"Predictor", "E-Field", "Fluxes", "Flux2Deltas", "Update", "DT",
+                                                "BCs"};   // BCs is pushed by step_enqueue_bcs
+
 int step_enqueue(Handle& h, int cur, cudaEvent_t* ev, bool split, int part) {
     cudaStream_t st = h.stream;
-    auto mark = [&](int ph) { if (ev) cudaEventRecord(ev[ph], st); };
+    int openRange = -1;
+    auto mark = [&](int ph) {
+        if (ev) cudaEventRecord(ev[ph], st);
+        if (openRange >= 0) nvtxRangePop();
+        openRange = ph < NPHASE ? ph : -1;
+        if (openRange >= 0) nvtxRangePushA(kPhaseRange[ph]);
+    };
+    struct Outer {   // "Advance" around the whole enqueue, closing any open phase range on return
+        int& open;
+        explicit Outer(int& o) : open(o) { nvtxRangePushA("Advance"); }
+        ~Outer() { if (open >= 0) nvtxRangePop(); nvtxRangePop(); }
+    } outer(openRange);
     const Lay& L = h.L;
     const Par& p = h.p;
     GridP g = h.gridP();
@@ -924,7 +943,9 @@ void step_enqueue_bcs(Handle& h, int cur, cudaEvent_t* ev) {
     cudaStream_t st = h.stream;
     launch_dt_finalize(h, 0, st);
     if (ev) cudaEventRecord(ev[PH_BCS], st);
+    nvtxRangePushA("BCs");
     launch_bcs(h, h.S[cur ^ 1], st);
+    nvtxRangePop();
 }
 
 // bFlux2Fld of the ghost cells of the new state S[cur ^ 1], after the BCs (and the halo fill of a tile)

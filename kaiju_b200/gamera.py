@@ -29,10 +29,10 @@ GAM_HALO_STATE, GAM_HALO_OSTATE, GAM_HALO_BXYZ = 1, 2, 4
 GAM_RING_PLM, GAM_RING_PPM, GAM_RING_PCM = 0, 1, 2
 GAM_RM_8CENT, GAM_RM_7UP = 0, 1
 GAM_SYNC_STATE, GAM_SYNC_OSTATE = 1, 2
-GAM_IC_OT2D, GAM_IC_BW, GAM_IC_LFMBW, GAM_IC_KH = 0, 1, 2, 3
+GAM_IC_OT2D, GAM_IC_BW, GAM_IC_LFMBW, GAM_IC_KH, GAM_IC_ADV1D, GAM_IC_ADV2D, GAM_IC_LOOP2D, GAM_IC_ALFVEN = range(8)
 GAM_SLICE_FAT = 1
 GAM_B0_UNIFORM, GAM_B0_DIPOLE = 1, 2
-GAM_TILE_FLUX_ROWS, GAM_TILE_FUSED_UPDATE, GAM_TILE_TMA = 1, 2, 3
+GAM_TILE_FLUX_ROWS, GAM_TILE_FUSED_UPDATE, GAM_TILE_TMA, GAM_TILE_STAGE_WAIT = 1, 2, 3, 4
 GAM_CLOSURE_LOSS_CELL, GAM_CLOSURE_LOSS_FACE = 0, 1
 TINY, HUGE = 1.0e-12, 1.0e12
 
@@ -113,7 +113,7 @@ SIGNATURES = {
     "gam_gpu_fetch": (C.c_int, [C.c_void_p, C.c_char_p, _DP, C.c_longlong]),
     "gam_gpu_destroy": (None, [C.c_void_p]),
     "gam_gpu_errstr": (C.c_char_p, [C.c_int]),
-    "gam_divb_noalloc": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_void_p]),
+    "gam_divb_noalloc": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_void_p]),
     "gam_tiles_create": (C.c_int, [C.POINTER(C.c_void_p), C.POINTER(C.c_void_p), C.c_int, C.c_int]),
     "gam_tiles_run_steps": (C.c_int, [C.c_void_p, C.c_int]),
     "gam_tiles_run_steps_timed": (C.c_int, [C.c_void_p, C.c_int, _DP]),
@@ -402,7 +402,10 @@ class GameraGPU:
         xyz = np.asfortranarray(xyz, dtype=np.float64)
         h = C.c_void_p()
         m = model.to_c()
-        icn = {"OT2D": GAM_IC_OT2D, "BW": GAM_IC_BW, "LFMBW": GAM_IC_LFMBW, "KH": GAM_IC_KH}[ic]
+        icn = {"OT2D": GAM_IC_OT2D, "BW": GAM_IC_BW, "LFMBW": GAM_IC_LFMBW, "KH": GAM_IC_KH, "ADV1D": GAM_IC_ADV1D,
+               "ADV2D": GAM_IC_ADV2D, "LOOP2D": GAM_IC_LOOP2D, "ALFVEN": GAM_IC_ALFVEN}[ic]
+        if icn == GAM_IC_ADV1D and ic_par is None:
+            ic_par = np.zeros(0)
         if ic_par is not None:
             par = np.ascontiguousarray(ic_par, dtype=np.float64)
             rc = L.gam_gpu_create_from_corners_ic(C.byref(h), C.byref(m), _dp(xyz), icn, par.ctypes.data_as(_DP),

@@ -6,6 +6,7 @@ the plain FP64 path and the FP32-flux path side by side.
     python -m kaiju_b200.runs spherical --n 96 96 128 --steps 2000
     python -m kaiju_b200.runs closure-step --n 128 --steps 20
     python -m kaiju_b200.runs ensemble --steps 20          # 96 Kelvin-Helmholtz members, FP32-flux
+    python -m kaiju_b200.runs ensemble-run --t-end 2       # the same members run to t = 2
     python -m kaiju_b200.runs tiles --n 256 --steps 10     # the 256^3 blast wave as 1, 2 and 4 k-tiles
 """
 from __future__ import annotations
@@ -115,6 +116,36 @@ def ensemble(steps: int = 20, members: int = 96, seed: int = 0):
     return out
 
 
+def ensemble_run(t_end: float = 2.0, members: int = 96, seed: int = 0, chunk: int = 16):
+    """The batched-ensemble configuration to its end time: 96 Kelvin-Helmholtz members (FP32-flux, uneven
+    sizes) advanced together to t_end, members dropping out as CalcDT's tFin clamp lands them on t_end.
+    The tile shapes (and queue or branches) come from the autotuner, whose timing steps are ordinary steps
+    of the run. Throughput = the members' zone-updates over the wall time of the whole advance (the host
+    checks the members' times every `chunk` batch steps)."""
+    import time
+    pars = gm.kh_ensemble_params(members, seed)
+    mem = [gm.kh_member(p, True, tFin=t_end) for p in pars]
+    cells = [p["nx"] * (p["nx"] // 2) * 4 for p in pars]
+    out = {"members": members, "cells": sum(cells), "t_end": t_end}
+    with gm.Ensemble(mem) as e:
+        rows = e.autotune(4)
+        ts0 = [g.status()["ts"] for g in mem]
+        t0 = time.perf_counter()
+        rc, batch_steps = e.advance(t_end, chunk=chunk)
+        wall = time.perf_counter() - t0
+        st = [g.status() for g in mem]
+    zone_updates = sum(c * (s["ts"] - a) for c, s, a in zip(cells, st, ts0))
+    out.update({"status": rc, "batch_steps": batch_steps, "wall_s": wall, "zone_updates": zone_updates,
+                "zone_updates_per_s": zone_updates / wall, "autotune_rows": sorted(set(rows)),
+                "queue": bool(e.queue), "member_steps_min": min(s["ts"] for s in st),
+                "member_steps_max": max(s["ts"] for s in st),
+                "t_min": min(s["t"] for s in st), "t_max": max(s["t"] for s in st),
+                "worst_status": max(s["status"] for s in st)})
+    for g in mem:
+        g.close()
+    return out
+
+
 def tiles(n: int = 256, steps: int = 10):
     """Device ms per step of the n^3 warped blast wave undivided and as 2 and 4 k-tiles on this GPU (one
     graph per step over all tiles), FP64 and FP32-flux."""
@@ -143,7 +174,8 @@ def tiles(n: int = 256, steps: int = 10):
 
 def main(argv=None):
     ap = argparse.ArgumentParser()
-    ap.add_argument("run", choices=["spherical", "closure-step", "ensemble", "tiles"])
+    ap.add_argument("run", choices=["spherical", "closure-step", "ensemble", "ensemble-run", "tiles"])
+    ap.add_argument("--t-end", type=float, default=2.0)
     ap.add_argument("--n", type=int, nargs="+", default=None)
     ap.add_argument("--steps", type=int, default=None)
     a = ap.parse_args(argv)
@@ -151,6 +183,8 @@ def main(argv=None):
         print(json.dumps(spherical(tuple(a.n or [96, 96, 128]), a.steps or 2000), indent=1))
     elif a.run == "ensemble":
         print(json.dumps(ensemble(a.steps or 20), indent=1))
+    elif a.run == "ensemble-run":
+        print(json.dumps(ensemble_run(a.t_end), indent=1))
     elif a.run == "tiles":
         print(json.dumps(tiles((a.n or [256])[0], a.steps or 10), indent=1))
     else:

@@ -62,7 +62,9 @@ enum { INI = 1, OUTI, INJ, OUTJ, INK, OUTK };
 // and the LFM blast-wave problem's fixed inner/outer shells (ICs/lfmbw.F90:141-249) for INI/OUTI
 // BC_HALO: a tile face inside a decomposed domain (no physical BC; gamapp_mpi.F90's halo exchange fills
 // the ghosts, and the dt domain takes no ghost layer there, init.F90:519-538)
-enum { BC_PERIODIC = 0, BC_ZEROGRAD = 1, BC_LFMPOLE = 2, BC_LFMBW = 3, BC_HALO = 4 };
+// BC_ION / BC_WIND: the magnetosphere's ionospheric inner boundary (IonInner, voltron/ICs/earthcmi.F90:378-522)
+// and solar-wind outer boundary (WindBC, apps/wind.F90:206-374)
+enum { BC_PERIODIC = 0, BC_ZEROGRAD = 1, BC_LFMPOLE = 2, BC_LFMBW = 3, BC_HALO = 4, BC_ION = 5, BC_WIND = 6 };
 enum { SPOLE = 1, EPOLE = 2 };
 enum { RR_PLM = 0, RR_PPM = 1, RR_PCM = 2, RR_WENO = 3 };
 static const int NFTMAX = 2;
@@ -125,6 +127,21 @@ struct Model {
     Ring R;
     bool predFixLFM = false;   // the LFM blast-wave problem's HackPredictor (ICs/lfmbw.F90:227-248)
     double bwD0 = 1.0, bwP0 = 0.1;   // its fixed-shell gas state (prob/D0, prob/P0)
+    // gravity (Model%doGrav, doSphGrav; background.F90:170-252, mhdgroup.F90:620-705)
+    bool doGrav = false, doSphGrav = false;
+    // the magnetosphere problem's hooks (voltron/ICs/earthcmi.F90 initUser): HackE = EFix, HackFlux = IonFlux,
+    // HackStep = PerStep, with a constant solar wind and no ionospheric coupling (inExyz = inEijk = 0)
+    struct Msph {
+        bool on = false;
+        double M0 = 0.0, GM0 = 0.0;   // dipole moment and gravity coefficient in code units (setMagsphere)
+        double rCut = 16.0, lCut = 8.0, dcScl = 4.0;   // cut dipole (msphutils.F90:47-50)
+        double xSun = 20.0, xTail = -225.0, yMax = 75.0, sInner = 0.96;   // initial-field cut (:440-444)
+        double wD = 0.0, wP = 0.0, wV[3] = {0, 0, 0}, wB[3] = {0, 0, 0};   // the wind, code units
+        double dtCpl = 0.0;   // PushIon coupling time scale (ibc dtCpl, earthcmi.F90:368-369)
+        double gT0 = 1.0;     // the time unit in seconds (NudgeSW's one-minute nudge time)
+        int nIonP = 1;        // ibc/nIonP
+        bool doIonPush = true;
+    } W;
 };
 
 struct Grid {
@@ -133,6 +150,7 @@ struct Grid {
     int isDT, ieDT, jsDT, jeDT, ksDT, keDT;
     Arr xyz, xyzcc, xfc, di, dj, dk, volume, Tf, Te, Teb, face, edge;
     Arr fcB0, edgB0, B0, bFlux0, dpB0;   // background field (background.F90:20-167), cell-sized arrays
+    Arr gxyz;                            // gravitational acceleration (AddGrav, background.F90:170-252)
     int bc[6] = {BC_PERIODIC, BC_PERIODIC, BC_PERIODIC, BC_PERIODIC, BC_PERIODIC, BC_PERIODIC};
 };
 
@@ -510,6 +528,32 @@ static void RingFlux(const Model& M, const Grid& G, Arr& gFlx, Arr& mFlx) {
         }
 }
 
+// IonFlux, the magnetosphere's HackFlux (voltron/ICs/earthcmi.F90:282-331): the I fluxes of the first shell at
+// the two cells next to the axis (js, je) replaced by their average over k
+static void IonFlux(const Model& M, const Grid& G, Arr& gFlx, Arr& mFlx) {
+    if (!M.doRing) return;
+    const int Np = M.R.Np;
+    auto avg = [&](int j) {
+        double im[3] = {0, 0, 0}, ig[5] = {0, 0, 0, 0, 0};
+        for (int c = 1; c <= 3; ++c) {
+            double s = 0.0;
+            for (int k = G.ks; k <= G.ke; ++k) s = s + mFlx(G.is, j, k, c, IDIR);
+            im[c - 1] = s / Np;
+        }
+        for (int v = 1; v <= NVAR; ++v) {
+            double s = 0.0;
+            for (int k = G.ks; k <= G.ke; ++k) s = s + gFlx(G.is, j, k, v, IDIR);
+            ig[v - 1] = s / Np;
+        }
+        for (int k = G.ks; k <= G.ke; ++k) {
+            for (int c = 1; c <= 3; ++c) mFlx(G.is, j, k, c, IDIR) = im[c - 1];
+            for (int v = 1; v <= NVAR; ++v) gFlx(G.is, j, k, v, IDIR) = ig[v - 1];
+        }
+    };
+    if (M.R.doE) avg(G.je);
+    if (M.R.doS) avg(G.js);
+}
+
 static void CalcStress(const Model& M, const Grid& G, const State& nS, const State& hS, Arr& gFlx, Arr& mFlx,
                        Arr& dGasH, Arr& dGasM) {  // stress.F90:41-198
     int nFlx = NDIM, ks = G.ks, ke = G.ke;
@@ -533,6 +577,7 @@ static void CalcStress(const Model& M, const Grid& G, const State& nS, const Sta
         }
     }
     if (M.doRing) RingFlux(M, G, gFlx, mFlx);   // stress.F90:134-139
+    if (M.W.on) IonFlux(M, G, gFlx, mFlx);      // HackFlux, stress.F90:141-143
     bool doMaxwell = M.doMHD;
 #pragma omp parallel for collapse(2) schedule(static)
     for (int k = G.ks; k <= G.ke; ++k)
@@ -1253,6 +1298,174 @@ static void lfmbwShellBC(const Model& M, const Grid& G, State& S, int dir) {
             }
 }
 
+// ---------------------------------------------------------------- the magnetosphere problem's boundaries
+// A constant solar wind (its GetWindAt is the same state everywhere: RefreshWind's front velocity is along x
+// with ByC = BzC = 0, wind.F90:112-161) and no ionospheric coupling (IonInnerBC_T%inExyz = inEijk = 0).
+static double RampDownE(double r, double rC, double lC) {   // RampDown, math.F90:97-111
+    if (r <= rC) return 1.0;
+    if (r >= rC + lC) return 0.0;
+    double rScl = (r - rC) / lC;
+    double eArg = -1.0 / (1.0 - rScl * rScl);
+    return std::exp(eArg + 1.0);
+}
+// wgtWind (wind.F90:185-203): the weight of the solar wind at a point, 1 on the sunward half
+static double wgtWind(const Model& M, const double* xyz) {
+    double nHat[3], vHat[3];
+    normVec3(xyz, nHat);
+    normVec3(M.W.wV, vHat);
+    double d = 0.0;
+    for (int c = 0; c < 3; ++c) d = d + (-vHat[c]) * nHat[c];
+    double dTh = std::acos(d) * 180.0 / PI;
+    return RampDownE(dTh, 90.0, 90.0);
+}
+// Con2Fast (gamutils.F90:343-360) with CellPress2Cs (:324-341): fast magnetosonic speed of a cell
+static double Con2Fast(const Model& M, const double* gCon, const double* B) {
+    double rho = fmaxd(gCon[0], M.dFloor);
+    double Vx = gCon[1] / rho, Vy = gCon[2] / rho, Vz = gCon[3] / rho;
+    double KinE = 0.5 * rho * (sq(Vx) + sq(Vy) + sq(Vz));
+    double P = fmaxd((M.gamma - 1) * (gCon[4] - KinE), M.pFloor);
+    double Cs = std::sqrt(M.gamma * P / rho);
+    double D = gCon[0];
+    double MagB = norm2v(B, 3);
+    double Va = MagB / std::sqrt(D);
+    if (M.doBoris) Va = M.Ca * Va / std::sqrt(sq(M.Ca) + sq(Va));
+    return std::sqrt(sq(Cs) + sq(Va));
+}
+static double Project2Face(const Grid& G, const double* V, int d, int i, int j, int k) {   // bcs.F90:250-263
+    double n[3] = {G.Tf(i, j, k, NORMX, d), G.Tf(i, j, k, NORMY, d), G.Tf(i, j, k, NORMZ, d)};
+    return G.face(i, j, k, d) * dot3(n, V);
+}
+// WindBC (wind.F90:206-374), outer I shells
+static void WindBC(const Model& M, const Grid& G, State& S) {
+    const double MinMach = 1.0;
+#pragma omp parallel for collapse(2) schedule(dynamic)
+    for (int k = G.ksg; k <= G.keg + 1; ++k)
+        for (int j = G.jsg; j <= G.jeg + 1; ++j) {
+            const int ip = G.ie;
+            for (int n = 1; n <= M.nG; ++n) {
+                const int ig = G.ie + n;
+                if (j <= G.jeg && k <= G.keg) {   // isCellCenterG
+                    double xcc[3] = {G.xyzcc(ig, j, k, 1), G.xyzcc(ig, j, k, 2), G.xyzcc(ig, j, k, 3)};
+                    double wSW = wgtWind(M, xcc), wMHD = 1.0 - wSW;
+                    double gW_sw[5] = {0, 0, 0, 0, 0}, gW_in[5] = {0, 0, 0, 0, 0};
+                    if (wSW > TINY) {
+                        gW_sw[0] = M.W.wD; gW_sw[4] = M.W.wP;
+                        for (int c = 0; c < 3; ++c) gW_sw[1 + c] = M.W.wV[c];
+                    }
+                    if (wMHD > TINY) {
+                        double gCon[5], B_in[3];
+                        for (int v = 0; v < 5; ++v) gCon[v] = S.Gas(ip, j, k, v + 1);
+                        for (int c = 0; c < 3; ++c) B_in[c] = S.Bxyz(ip, j, k, c + 1);
+                        CellC2P(M, gCon, gW_in);
+                        double Cx = Con2Fast(M, gCon, B_in);
+                        double V[3] = {gW_in[1], gW_in[2], gW_in[3]};
+                        double nHat[3] = {G.Tf(ip + 1, j, k, NORMX, IDIR), G.Tf(ip + 1, j, k, NORMY, IDIR),
+                                          G.Tf(ip + 1, j, k, NORMZ, IDIR)};
+                        if (dot3(V, nHat) < MinMach * Cx) {
+                            double Vp[3];
+                            Vec2Para(V, nHat, Vp);
+                            for (int c = 0; c < 3; ++c) V[c] = V[c] - Vp[c] + MinMach * Cx * nHat[c];
+                        }
+                        for (int c = 0; c < 3; ++c) gW_in[1 + c] = V[c];
+                    }
+                    double gW[5], gCon[5];
+                    for (int v = 0; v < 5; ++v) gW[v] = wSW * gW_sw[v] + wMHD * gW_in[v];
+                    CellP2C(M, gW, gCon);
+                    for (int v = 0; v < 5; ++v) S.Gas(ig, j, k, v + 1) = gCon[v];
+                }
+                // face fluxes: the wind's flux blended with the last active face's
+                for (int d = 1; d <= 3; ++d) {
+                    int fi = d == IDIR ? ig + 1 : ig, si = d == IDIR ? ip + 1 : ip;
+                    double xf[3] = {G.xfc(fi, j, k, 1, d), G.xfc(fi, j, k, 2, d), G.xfc(fi, j, k, 3, d)};
+                    double wSW = wgtWind(M, xf);
+                    double swFlx = Project2Face(G, M.W.wB, d, fi, j, k);
+                    double inFlx = S.magFlux(si, j, k, d);
+                    S.magFlux(fi, j, k, d) = wSW * swFlx + (1 - wSW) * inFlx;
+                }
+            }
+        }
+#pragma omp parallel for collapse(2) schedule(static)
+    for (int k = G.ksg; k <= G.keg; ++k)
+        for (int j = G.jsg; j <= G.jeg; ++j)
+            for (int n = 1; n <= M.nG; ++n) {
+                int ig = G.ie + n, ip, jp, kp;
+                lfmIJKcc(M, G, ig, j, k, ip, jp, kp);
+                double B[3];
+                gamCellBxyz(G, S.magFlux, ip, jp, kp, B);
+                for (int c = 0; c < 3; ++c) S.Bxyz(ig, j, k, c + 1) = B[c];
+            }
+#pragma omp parallel for collapse(2) schedule(static)
+    for (int k = G.ksg; k <= G.keg; ++k)
+        for (int i = G.ie + 1; i <= G.ieg; ++i)
+            for (int n = 1; n <= M.nG; ++n) {
+                int ip, jp, kp;
+                if (M.R.doS) {
+                    int jg = G.js - n;
+                    lfmIJKcc(M, G, i, jg, k, ip, jp, kp);
+                    for (int c = 1; c <= 3; ++c) S.Bxyz(i, jg, k, c) = S.Bxyz(ip, jp, kp, c);
+                }
+                if (M.R.doE) {
+                    int jg = G.je + n;
+                    lfmIJKcc(M, G, i, jg, k, ip, jp, kp);
+                    for (int c = 1; c <= 3; ++c) S.Bxyz(i, jg, k, c) = S.Bxyz(ip, jp, kp, c);
+                }
+            }
+}
+// IonInner (voltron/ICs/earthcmi.F90:378-522) with CellPlasmaBC (apps/msphingest.F90:268-372) for one fluid
+// without ingestion or ionospheric E field: the ghost takes the mirrored active cell's density and pressure at
+// rest (Veb = 0), the ghost face fluxes are zero (the dipole is the background field), the ghost B comes from
+// the (conjugate) cell's faces
+static void IonInnerBC(const Model& M, const Grid& G, State& S) {
+#pragma omp parallel for collapse(2) schedule(static)
+    for (int k = G.ksg; k <= G.keg + 1; ++k)
+        for (int j = G.jsg; j <= G.jeg + 1; ++j)
+            for (int n = 1; n <= M.nG; ++n) {
+                const int ig = G.is - n, ip = G.is + n - 1;
+                if (j <= G.jeg && k <= G.keg) {   // isCellCenterG
+                    int idip, jp, kp;
+                    lfmIJKcc(M, G, ig, j, k, idip, jp, kp);
+                    double pU[5], pW[5], gW[5], gU[5];
+                    for (int v = 0; v < 5; ++v) pU[v] = S.Gas(ip, jp, kp, v + 1);
+                    CellC2P(M, pU, pW);
+                    gW[0] = pW[0]; gW[4] = pW[4];
+                    gW[1] = gW[2] = gW[3] = 0.0;   // Vec2Perp(Veb, rHat) + min(Vr, 0) rHat with Veb = 0
+                    CellP2C(M, gW, gU);
+                    for (int v = 0; v < 5; ++v) S.Gas(ig, j, k, v + 1) = gU[v];
+                }
+                for (int d = 1; d <= 3; ++d) {   // isGoodFaceIJK (gridutils.F90:985-1009)
+                    bool good = (d == IDIR) ? (j <= G.jeg && k <= G.keg)
+                                            : (d == JDIR) ? (k <= G.keg) : (j <= G.jeg);
+                    if (good) S.magFlux(ig, j, k, d) = 0.0;
+                }
+            }
+#pragma omp parallel for collapse(2) schedule(static)
+    for (int k = G.ksg; k <= G.keg; ++k)
+        for (int j = G.jsg; j <= G.jeg; ++j)
+            for (int n = 1; n <= M.nG; ++n) {
+                int ig = G.is - n, ip, jp, kp;
+                lfmIJKcc(M, G, ig, j, k, ip, jp, kp);
+                double B[3];
+                gamCellBxyz(G, S.magFlux, ip, jp, kp, B);
+                for (int c = 0; c < 3; ++c) S.Bxyz(ig, j, k, c + 1) = B[c];
+            }
+#pragma omp parallel for collapse(2) schedule(static)
+    for (int k = G.ksg; k <= G.keg; ++k)
+        for (int i = G.isg; i <= G.is - 1; ++i)
+            for (int n = 1; n <= M.nG; ++n) {
+                int ip, jp, kp;
+                if (M.R.doS) {
+                    int jg = G.js - n;
+                    lfmIJKcc(M, G, i, jg, k, ip, jp, kp);
+                    for (int c = 1; c <= 3; ++c) S.Bxyz(i, jg, k, c) = S.Bxyz(ip, jp, kp, c);
+                }
+                if (M.R.doE) {
+                    int jg = G.je + n;
+                    lfmIJKcc(M, G, i, jg, k, ip, jp, kp);
+                    for (int c = 1; c <= 3; ++c) S.Bxyz(i, jg, k, c) = S.Bxyz(ip, jp, kp, c);
+                }
+            }
+}
+
 static void EnforceBCs(const Model& M, const Grid& G, State& S) {  // step.F90:17-55
     for (int n = 1; n <= 6; ++n) {
         int kind = G.bc[n - 1];
@@ -1260,6 +1473,8 @@ static void EnforceBCs(const Model& M, const Grid& G, State& S) {  // step.F90:1
         if (kind == BC_PERIODIC) periodicBC(M, G, S, n);
         else if (kind == BC_LFMPOLE) lfmPoleBC(M, G, S, n);
         else if (kind == BC_LFMBW) lfmbwShellBC(M, G, S, n);
+        else if (kind == BC_ION) { if (n == INI) IonInnerBC(M, G, S); }
+        else if (kind == BC_WIND) { if (n == OUTI) WindBC(M, G, S); }
         else zeroGradBC(M, G, S, n);
     }
 }
@@ -1410,6 +1625,16 @@ static void CalcSmoothE(const Model& M, const Grid& G, const State& S, Arr& Smoo
         }
     }
 }
+// FixEFieldLFM (gamdebug.F90:149-175): the I and J edges of the periodic K seam take the average of the two copies
+static void FixEFieldLFM(const Grid& G, Arr& E) {
+    for (int j = G.js; j <= G.je + 1; ++j)
+        for (int i = G.is; i <= G.ie + 1; ++i) {
+            double Ei = 0.5 * (E(i, j, G.ks, IDIR) + E(i, j, G.ke + 1, IDIR));
+            double Ej = 0.5 * (E(i, j, G.ks, JDIR) + E(i, j, G.ke + 1, JDIR));
+            E(i, j, G.ks, IDIR) = Ei; E(i, j, G.ke + 1, IDIR) = Ei;
+            E(i, j, G.ks, JDIR) = Ej; E(i, j, G.ke + 1, JDIR) = Ej;
+        }
+}
 // PoleE (ringav.F90:376-411) for the LFM axis, then FixEFieldLFM (gamdebug.F90:149-175)
 static void PoleE(const Model& M, const Grid& G, Arr& E) {
     const int Np = M.R.Np;
@@ -1423,13 +1648,7 @@ static void PoleE(const Model& M, const Grid& G, Arr& E) {
         if (M.R.doS) pole(G.js);
         if (M.R.doE) pole(G.je + 1);
     }
-    for (int j = G.js; j <= G.je + 1; ++j)
-        for (int i = G.is; i <= G.ie + 1; ++i) {
-            double Ei = 0.5 * (E(i, j, G.ks, IDIR) + E(i, j, G.ke + 1, IDIR));
-            double Ej = 0.5 * (E(i, j, G.ks, JDIR) + E(i, j, G.ke + 1, JDIR));
-            E(i, j, G.ks, IDIR) = Ei; E(i, j, G.ke + 1, IDIR) = Ei;
-            E(i, j, G.ks, JDIR) = Ej; E(i, j, G.ke + 1, JDIR) = Ej;
-        }
+    FixEFieldLFM(G, E);
 }
 // CleanLoops (ringav.F90:339-373): remove the net K flux around the first/last ring
 static void CleanLoops(const Model& M, const Grid& G, State& S) {
@@ -1499,18 +1718,181 @@ static void RingAverage(const Model& M, const Grid& G, State& S, Arr& SmoothE) {
     if (M.R.doE) SmoothGas(M, G, S, EPOLE);
 }
 
+// ---------------------------------------------------------------- the magnetosphere problem's hooks
+// DiffuseOuter (wind.F90:568-618): diffusive E of the outermost I edge from the face-field current
+static void DiffuseOuter(const Model& M, const Grid& G, const State& S, int i, int j, int k, double vSW, double* Ed) {
+    double db2, db1, bP, bM, Jd[3] = {0.0, 0.0, 0.0};
+    bP = S.magFlux(i, j, k, JDIR) / fmaxd(G.face(i, j, k, JDIR), TINY);
+    bM = S.magFlux(i - 1, j, k, JDIR) / fmaxd(G.face(i - 1, j, k, JDIR), TINY);
+    db2 = bP - bM;
+    bP = S.magFlux(i, j, k, IDIR) / G.face(i, j, k, IDIR);
+    bM = S.magFlux(i, j - 1, k, IDIR) / G.face(i, j - 1, k, IDIR);
+    db1 = bP - bM;
+    Jd[2] = db2 - db1;
+    bP = S.magFlux(i, j, k, IDIR) / G.face(i, j, k, IDIR);
+    bM = S.magFlux(i, j, k - 1, IDIR) / G.face(i, j, k - 1, IDIR);
+    db2 = bP - bM;
+    bP = S.magFlux(i, j, k, KDIR) / G.face(i, j, k, KDIR);
+    bM = S.magFlux(i - 1, j, k, KDIR) / G.face(i - 1, j, k, KDIR);
+    db1 = bP - bM;
+    Jd[1] = db2 - db1;
+    double dl = std::sqrt(G.edge(i, j, k, JDIR) * G.edge(i, j, k, KDIR));
+    double Vd = fmind(vSW, M.CFL * dl / M.dt);
+    Ed[0] = 0.0;
+    Ed[1] = Vd * Jd[1] * dl;
+    Ed[2] = Vd * Jd[2] * dl;
+}
+// WindEFix (wind.F90:489-565): the E of the outer shells' edges blended toward the wind's -V x B
+static void WindEFix(const Model& M, const Grid& G, State& S) {
+    const double vSW = fmind(norm2v(M.W.wV, 3), M.Ca);   // norm2 of the front velocity (-|V|, 0, 0)
+    double swE[3];
+    cross3(M.W.wV, M.W.wB, swE);
+    for (int c = 0; c < 3; ++c) swE[c] = -swE[c];
+    Arr& E = S.Efld;
+#pragma omp parallel for collapse(2) schedule(static)
+    for (int k = G.ks; k <= G.ke + 1; ++k)
+        for (int j = G.js; j <= G.je + 1; ++j)
+            for (int i = G.ie - 2; i <= G.ie + 1; ++i) {
+                double wSW = 0.0;
+                for (int n = IDIR; n <= KDIR; ++n) {
+                    double e1[3], e2[3], ecc[3];
+                    for (int c = 0; c < 3; ++c) {
+                        e1[c] = G.xyz(i, j, k, c + 1);
+                        e2[c] = G.xyz(i + (n == IDIR), j + (n == JDIR), k + (n == KDIR), c + 1);
+                        ecc[c] = 0.5 * (e1[c] + e2[c]);
+                    }
+                    wSW = wgtWind(M, ecc);
+                    if (wSW > TINY) {
+                        if (i <= G.ie) wSW = wSW / (1.0 + G.ie + 1 - i);
+                        double de[3] = {e2[0] - e1[0], e2[1] - e1[1], e2[2] - e1[2]};
+                        E(i, j, k, n) = (1.0 - wSW) * E(i, j, k, n) + wSW * dot3(swE, de);
+                    }
+                }
+                if (i == G.ie + 1) {   // doSWDiffuse, with the weight of the last (K) edge
+                    double Ed[3];
+                    DiffuseOuter(M, G, S, i, j, k, vSW, Ed);
+                    for (int c = 0; c < 3; ++c) E(i, j, k, c + 1) = E(i, j, k, c + 1) + wSW * Ed[c];
+                }
+            }
+    if (M.doRing) {
+        const int Np = M.R.Np;
+        for (int n = G.ie - 2; n <= G.ie + 1; ++n) {
+            auto ring = [&](int j) {
+                double s = 0.0;
+                for (int k = G.ks; k <= G.ke; ++k) s = s + E(n, j, k, IDIR);
+                double avg = s / Np;
+                for (int k = G.ksg; k <= G.keg; ++k) { E(n, j, k, IDIR) = avg; E(n, j, k, KDIR) = 0.0; }
+            };
+            if (M.R.doE) ring(G.je + 1);
+            if (M.R.doS) ring(G.js);
+        }
+    }
+}
+// EFix, the magnetosphere's HackE (earthcmi.F90:260-280): IonEFix (msphutils.F90:214-240) with zero
+// ionospheric E on the first shell's J and K edges, WindEFix, FixEFieldLFM
+static void EFix(const Model& M, const Grid& G, State& S) {
+    for (int k = G.ksg; k <= G.keg; ++k)
+        for (int j = G.jsg; j <= G.jeg; ++j) {
+            S.Efld(G.is, j, k, JDIR) = G.edge(G.is, j, k, JDIR) * 0.0;
+            S.Efld(G.is, j, k, KDIR) = G.edge(G.is, j, k, KDIR) * 0.0;
+        }
+    WindEFix(M, G, S);
+    FixEFieldLFM(G, S.Efld);
+}
+// PushIon (earthcmi.F90:524-606): the first nIonP shells' velocity pushed toward the (zero) E x B drift
+static void PushIon(const Model& M, const Grid& G, State& S) {
+    if (!M.W.doIonPush) return;
+#pragma omp parallel for collapse(2) schedule(static)
+    for (int k = G.ks; k <= G.ke; ++k)
+        for (int j = G.js; j <= G.je; ++j)
+            for (int i = G.is; i <= G.is + M.W.nIonP - 1; ++i) {
+                double pCon[5], pW[5];
+                for (int v = 0; v < 5; ++v) pCon[v] = S.Gas(i, j, k, v + 1);
+                CellC2P(M, pCon, pW);
+                if (pCon[0] < 0.0) continue;
+                int dN = i - G.is + 1;
+                double dt = M.dt / (dN * M.W.dtCpl);
+                dt = fmind(dt, 1.0);
+                for (int c = 1; c <= 3; ++c) pW[c] = pW[c] + dt * (0.0 - pW[c]);
+                CellP2C(M, pW, pCon);
+                for (int v = 0; v < 5; ++v) S.Gas(i, j, k, v + 1) = pCon[v];
+            }
+}
+// NudgeSW (wind.F90:392-486): the outermost active shell nudged toward the wind over a minute, and the cells
+// next to the axis at the back of the grid kept flowing out
+static void NudgeSW(const Model& M, const Grid& G, State& S) {
+    const int ip = G.ie;
+    const double dtSW0 = 60.0 / M.W.gT0;
+#pragma omp parallel for collapse(2) schedule(dynamic)
+    for (int k = G.ks; k <= G.ke; ++k)
+        for (int j = G.js; j <= G.je; ++j) {
+            double xcc[3] = {G.xyzcc(ip, j, k, 1), G.xyzcc(ip, j, k, 2), G.xyzcc(ip, j, k, 3)};
+            double wSW = wgtWind(M, xcc);
+            if (wSW > TINY) {
+                double dtSW = fmaxd(dtSW0 / wSW, M.dt);
+                double gW_sw[5] = {M.W.wD, M.W.wV[0], M.W.wV[1], M.W.wV[2], M.W.wP};
+                double gCon[5], gW_mhd[5], gW[5];
+                for (int v = 0; v < 5; ++v) gCon[v] = S.Gas(ip, j, k, v + 1);
+                CellC2P(M, gCon, gW_mhd);
+                for (int v = 0; v < 5; ++v) gW[v] = gW_mhd[v] + (M.dt / dtSW) * (gW_sw[v] - gW_mhd[v]);
+                CellP2C(M, gW, gCon);
+                for (int v = 0; v < 5; ++v) S.Gas(ip, j, k, v + 1) = gCon[v];
+            }
+        }
+    if (M.doRing && M.R.doE) {
+        for (int k = G.ks; k <= G.ke; ++k)
+            for (int n = 0; n <= 1; ++n) {
+                int i = G.ie, j = G.je + n;
+                if (S.Gas(i, j, k, MOMX) > 0) {
+                    double gCon[5], B[3], gW[5];
+                    for (int v = 0; v < 5; ++v) gCon[v] = S.Gas(i, j, k, v + 1);
+                    for (int c = 0; c < 3; ++c) B[c] = S.Bxyz(i, j, k, c + 1);
+                    double Cx = Con2Fast(M, gCon, B);
+                    CellC2P(M, gCon, gW);
+                    gW[1] = -Cx;
+                    CellP2C(M, gW, gCon);
+                    for (int v = 0; v < 5; ++v) S.Gas(i, j, k, v + 1) = gCon[v];
+                }
+            }
+    }
+}
+// applyGrav (mhdgroup.F90:620-705), one fluid, classical momentum (doBorisGrav = .false.)
+static void applyGrav(const Model& M, const Grid& G, State& S, const State& oS) {
+#pragma omp parallel for collapse(2) schedule(static)
+    for (int k = G.ks; k <= G.ke; ++k)
+        for (int j = G.js; j <= G.je; ++j)
+            for (int i = G.is; i <= G.ie; ++i) {
+                if (!(S.Gas(i, j, k, DEN) >= 0.0)) continue;
+                double pCon[5], pW[5];
+                for (int v = 0; v < 5; ++v) pCon[v] = S.Gas(i, j, k, v + 1);
+                CellC2P(M, pCon, pW);
+                double IntE = pW[4] / (M.gamma - 1);
+                double Dhf = 0.5 * (S.Gas(i, j, k, DEN) + oS.Gas(i, j, k, DEN));
+                double cM[3];
+                for (int c = 0; c < 3; ++c) cM[c] = pCon[1 + c] + M.dt * Dhf * G.gxyz(i, j, k, c + 1);
+                for (int c = 0; c < 3; ++c) pCon[1 + c] = cM[c];
+                pCon[4] = IntE + 0.5 * dot3(cM, cM) / pCon[0];
+                for (int v = 0; v < 5; ++v) S.Gas(i, j, k, v + 1) = pCon[v];
+            }
+}
+
 // ---------------------------------------------------------------- one step (gamapp.F90:73-116, mhdgroup.F90:16-76)
 static void AdvanceMHD(App& A, double dt) {
     Model& M = A.M;
     if (std::fabs(A.oS.time - A.S.time) < TINY) A.oS.time = A.S.time - M.dt;
     Predictor(M, A.G, A.S, A.oS, A.V.StateHf, 0.5 * dt);
-    if (M.doMHD) CalcElecField(M, A.G, A.S, A.V.StateHf, A.V.Vf, A.S.Efld);
+    if (M.doMHD) {
+        CalcElecField(M, A.G, A.S, A.V.StateHf, A.V.Vf, A.S.Efld);
+        if (M.W.on) EFix(M, A.G, A.S);   // HackE, mhdgroup.F90:40-44
+    }
     CalcStress(M, A.G, A.S, A.V.StateHf, A.V.gFlx, A.V.mFlx, A.V.dGasH, A.V.dGasM);
     applyUpdate(M, A.G, A.S, A.oS, dt, A.V.dGasH, A.V.dGasM, A.S.Efld);
+    if (M.doGrav) applyGrav(M, A.G, A.S, A.oS);   // mhdgroup.F90:60-65
     if (M.doRing && (M.R.doS || M.R.doE)) RingAverage(M, A.G, A.S, A.V.SmoothE);   // mhdgroup.F90:68-74
 }
 static void stepGamera(App& A) {
     AdvanceMHD(A, A.M.dt);
+    if (A.M.W.on) { PushIon(A.M, A.G, A.S); NudgeSW(A.M, A.G, A.S); }   // HackStep, gamapp.F90:104-109
     A.M.ts = A.M.ts + 1;
     A.M.t = A.M.t + A.M.dt;
     A.M.dt = CalcDT(A.M, A.G, A.S);
@@ -1704,6 +2086,24 @@ static void RingGridFix(const Model& M, Grid& G) {
                     for (int c = 0; c < 3; ++c) G.Tf(ig, jg, kg, NORMX + c, KDIR) = -G.Tf(ip, jp, kp, NORMX + c, KDIR);
                     G.face(ig, jg, kg, KDIR) = G.face(ip, jp, kp, KDIR);
                 }
+}
+
+// The arrays Corners2Grid fills, allocated with its shapes but left for the caller to set (a grid whose
+// metrics come from elsewhere, e.g. a slab of a device-built grid)
+static void allocGridMetrics(Grid& G) {
+    int lo[5] = {G.isg, G.jsg, G.ksg, 1, 1};
+    int hi[5] = {G.ieg, G.jeg, G.keg, 3, 3};
+    G.xyzcc.alloc(4, lo, hi);
+    G.volume.alloc(3, lo, hi); G.di.alloc(3, lo, hi); G.dj.alloc(3, lo, hi); G.dk.alloc(3, lo, hi);
+    hi[0] = G.ieg + 1; hi[1] = G.jeg + 1; hi[2] = G.keg + 1;
+    G.xfc.alloc(5, lo, hi);
+    G.face.alloc(4, lo, hi);
+    G.edge.alloc(4, lo, hi);
+    hi[3] = 9;
+    G.Tf.alloc(5, lo, hi);
+    G.Te.alloc(5, lo, hi);
+    hi[3] = 4;
+    G.Teb.alloc(5, lo, hi);
 }
 
 static int Corners2Grid(const Model& M, Grid& G) {  // init.F90:801-1080
@@ -2148,6 +2548,104 @@ static void initLFMBW(const Model& M, const Grid& G, State& S, const double* bw)
     if (M.doMHD) VectorPot2Flux(G, S, VectorPot_BW, &b);
 }
 
+// ---------------------------------------------------------------- the accuracy cases of tests/cases/testCases.pf
+// Single-precision (default-real) literals of the Fortran keep their float values: a literal such as 0.1 is
+// written (double)0.1f, and 0.1**2 is evaluated in float, as gfortran does.
+static const double F01 = (double)0.1f, F03 = (double)0.3f, F05 = (double)0.5f, F07 = (double)0.7f,
+                    F005 = (double)0.05f;
+
+// cell-centre primitive state written as conserved Gas on the cells is..ie+1 (the loops of prob.F90)
+static void putPrim(const Model& M, State& S, int i, int j, int k, double Rho, double Vx, double Vy, double Vz, double P) {
+    S.Gas(i, j, k, DEN) = Rho;
+    S.Gas(i, j, k, MOMX) = Rho * Vx;
+    S.Gas(i, j, k, MOMY) = Rho * Vy;
+    S.Gas(i, j, k, MOMZ) = Rho * Vz;
+    double KinE = 0.5 * Rho * (sq(Vx) + sq(Vy) + sq(Vz));
+    S.Gas(i, j, k, ENERGY) = KinE + P / (M.gamma - 1);
+}
+
+// initADV1D (prob.F90:671-736): four density shapes advected at Vx = 1 on [-1, 1], P = 1, no field
+static void initADV1D(const Model& M, Grid& G, State& S) {
+    const double f01sq = (double)(0.1f * 0.1f);   // 0.1**2 of two default reals
+    for (int k = G.ks; k <= G.ke + 1; ++k)
+        for (int j = G.js; j <= G.je + 1; ++j)
+            for (int i = G.is; i <= G.ie + 1; ++i) {
+                double xc = G.xyzcc(i, j, k, 1);
+                double Rho0 = F01;
+                double Rho1 = std::exp(-sq((xc + F07) / F005));
+                double Rho2 = (std::fabs(xc + F03) <= F01) ? 1.0 : 0.0;
+                double Rho3 = (std::fabs(xc - F01) <= F01) ? 1.0 - std::fabs(10.0 * (xc - F01)) : 0.0;
+                double Rho4 = ((f01sq - sq(xc - F05)) >= 0) ? 10.0 * std::sqrt(f01sq - sq(xc - F05)) : 0.0;
+                double Rho = Rho0 + Rho1 + Rho2 + Rho3 + Rho4;
+                putPrim(M, S, i, j, k, Rho, 1.0, 0.0, 0.0, 1.0);
+                S.magFlux(i, j, k, IDIR) = 0.0; S.magFlux(i, j, k, JDIR) = 0.0; S.magFlux(i, j, k, KDIR) = 0.0;
+            }
+}
+
+// initADV2D (prob.F90:739-797): a disc of radius R0 with twice the density, advected at V0 along alpha
+// degrees from +y; prob = {d0, P0, V0, alpha, R0, x0, y0}
+static void initADV2D(const Model& M, Grid& G, State& S, const double* pr) {
+    double Rho0 = pr[0], P0 = pr[1], V0 = pr[2], alpha = pr[3], R0 = pr[4], x0 = pr[5], y0 = pr[6];
+    for (int k = G.ks; k <= G.ke + 1; ++k)
+        for (int j = G.js; j <= G.je + 1; ++j)
+            for (int i = G.is; i <= G.ie + 1; ++i) {
+                double xc = G.xyzcc(i, j, k, 1), yc = G.xyzcc(i, j, k, 2);
+                double Vx = V0 * std::sin(alpha * PI / 180.0), Vy = V0 * std::cos(alpha * PI / 180.0);
+                double r = std::sqrt(sq(xc - x0) + sq(yc - y0));
+                double Rho = (r < R0) ? Rho0 * 2.0 : Rho0;
+                putPrim(M, S, i, j, k, Rho, Vx, Vy, 0.0, P0);
+                S.magFlux(i, j, k, IDIR) = 0.0; S.magFlux(i, j, k, JDIR) = 0.0; S.magFlux(i, j, k, KDIR) = 0.0;
+            }
+}
+
+// initLoop (prob.F90:436-500): uniform flow along alpha, a field loop from Az = max(0, A0 (R0 - r));
+// prob = {d0, P0, V0, Vz0, alpha, A0, R0, x0, y0}
+struct LoopCtx { double A0, R0, x0, y0; };
+static void VectorPot_Loop2D(double x, double y, double z, double* A, void* c) {   // prob.F90:489-499
+    (void)z;
+    LoopCtx* l = (LoopCtx*)c;
+    double r = std::sqrt(sq(x - l->x0) + sq(y - l->y0));
+    A[0] = 0.0; A[1] = 0.0;
+    A[2] = fmaxd(0.0, l->A0 * (l->R0 - r));
+}
+static void initLoop2D(const Model& M, Grid& G, State& S, const double* pr) {
+    double Rho0 = pr[0], P0 = pr[1], V0 = pr[2], Vz0 = pr[3], alpha = pr[4];
+    for (int k = G.ks; k <= G.ke + 1; ++k)
+        for (int j = G.js; j <= G.je + 1; ++j)
+            for (int i = G.is; i <= G.ie + 1; ++i) {
+                double Vx = V0 * std::sin(alpha * PI / 180.0), Vy = V0 * std::cos(alpha * PI / 180.0);
+                putPrim(M, S, i, j, k, Rho0, Vx, Vy, Vz0, P0);
+            }
+    LoopCtx l = {pr[5], pr[6], pr[7], pr[8]};
+    VectorPot2Flux(G, S, VectorPot_Loop2D, &l);
+}
+
+// initALFVEN (prob.F90:1027-1083): the nonlinear circularly polarised Alfven wave along angle alp;
+// prob = {d0, P0, B_para, V_para, alp}
+struct AlfCtx { double Rho0, P0, Bpar, Vpar, alp; };
+static void GasIC_ALF(double x, double y, double z, double* W, void* c) {   // prob.F90:1072-1082
+    (void)z;
+    AlfCtx* a = (AlfCtx*)c;
+    double ph = 2 * PI * (x * std::cos(a->alp) + y * std::sin(a->alp));
+    W[0] = a->Rho0;
+    W[1] = a->Vpar * std::cos(a->alp) - F01 * std::sin(ph) * std::sin(a->alp);
+    W[2] = a->Vpar * std::sin(a->alp) + F01 * std::sin(ph) * std::cos(a->alp);
+    W[3] = F01 * std::cos(ph);
+    W[4] = a->P0;
+}
+static void VectorPot_ALF(double x, double y, double z, double* A, void* c) {   // prob.F90:1063-1070
+    AlfCtx* a = (AlfCtx*)c;
+    double ph = 2 * PI * (x * std::cos(a->alp) + y * std::sin(a->alp));
+    A[0] = a->Bpar * std::sin(a->alp) * z;
+    A[1] = -1.0 * a->Bpar * std::cos(a->alp) * z + F01 * std::sin(ph) / (2 * PI * std::cos(a->alp));
+    A[2] = F01 * std::cos(ph) / (2 * PI);
+}
+static void initALFVEN(const Model& M, Grid& G, State& S, const double* pr) {
+    AlfCtx a = {pr[0], pr[1], pr[2], pr[3], pr[4]};
+    GasIC2State(M, G, S, GasIC_ALF, &a);
+    VectorPot2Flux(G, S, VectorPot_ALF, &a);
+}
+
 }  // namespace orc
 
 // =========================================================================================== C ABI
@@ -2157,7 +2655,7 @@ extern "C" {
 
 struct orc_params {
     int Nip, Njp, Nkp;
-    int icType;            // 0 = OT2D, 1 = BW
+    int icType;            // 0 = OT2D, 1 = BW, 2 = LFM blast wave, 3 = KH, 4..7 = ADV1D, ADV2D, LOOP2D, ALFVEN
     int gridType;          // 0 = uniform Cartesian, 1 = sinusoidal warp x'=x+A sin(2 pi y) sin(2 pi z) (cyclic)
     double xyzBds[6];
     double warpAmp;
@@ -2180,6 +2678,12 @@ struct orc_params {
     // are bc 3 and its predictor fix is on
     double bw[8];
     double kh[4];           // icType 3: Kelvin-Helmholtz shear layer {a, Bx, amp, seed}
+    // icType 4 ADV1D, 5 ADV2D {d0, P0, V0, alpha, R0, x0, y0}, 6 LOOP2D {d0, P0, V0, Vz0, alpha, A0, R0, x0, y0},
+    // 7 ALFVEN {d0, P0, B_para, V_para, alp}: the deck values of tests/cases/*.xml with prob.F90's defaults
+    double prob[10];
+    // 1: no set-up -- allocate the grid, State and Solver only; the caller sets the metrics, State, oState and
+    // the scalars (orc_set, orc_set_scalars) before stepping. Used to step a slab of a grid built elsewhere.
+    int noSetup;
     const double* xyzIn;    // corners (Ni+1,Nj+1,Nk+1,3), Fortran layout, replacing the generated ones (a tile)
 };
 
@@ -2237,30 +2741,41 @@ void* orc_create(const orc_params* p) {
     if (G.bc[3] == BC_HALO) G.jeDT = G.je;
     if (G.bc[4] == BC_HALO) G.ksDT = G.ks;
     if (G.bc[5] == BC_HALO) G.keDT = G.ke;
-    if (Corners2Grid(M, G) != 0) { delete A; return nullptr; }
-    allocState(M, G, A->S);
-    allocState(M, G, A->oS);
-    if (p->icType == 0) initOT2D(M, G, A->S);
-    else if (p->icType == 3) initKH(M, G, A->S, p->kh);
-    else if (p->icType == 2) {
-        M.predFixLFM = true;
-        M.bwD0 = p->bw[5]; M.bwP0 = p->bw[3];
-        initLFMBW(M, G, A->S, p->bw);
+    if (p->noSetup) {
+        if (p->doRing || p->b0Type != 0) { delete A; return nullptr; }
+        allocGridMetrics(G);
+        allocState(M, G, A->S);
+        allocState(M, G, A->oS);
+    } else {
+        if (Corners2Grid(M, G) != 0) { delete A; return nullptr; }
+        allocState(M, G, A->S);
+        allocState(M, G, A->oS);
+        if (p->icType == 0) initOT2D(M, G, A->S);
+        else if (p->icType == 3) initKH(M, G, A->S, p->kh);
+        else if (p->icType == 4) initADV1D(M, G, A->S);
+        else if (p->icType == 5) initADV2D(M, G, A->S, p->prob);
+        else if (p->icType == 6) initLoop2D(M, G, A->S, p->prob);
+        else if (p->icType == 7) initALFVEN(M, G, A->S, p->prob);
+        else if (p->icType == 2) {
+            M.predFixLFM = true;
+            M.bwD0 = p->bw[5]; M.bwP0 = p->bw[3];
+            initLFMBW(M, G, A->S, p->bw);
+        }
+        else initBW(M, G, A->S, p->b0Type == 1);
+        if (p->b0Type != 0) {   // CalcGridInfo: AddB0 after the IC (init.F90:180-184)
+            M.doBackground = true;
+            B0ctx bc;
+            bc.type = p->b0Type; bc.bx = p->b0[0]; bc.by = p->b0[1]; bc.bz = p->b0[2]; bc.M0 = p->b0[3];
+            AddB0(M, G, &bc);
+        }
+        // CalcGridInfo (init.F90:204-244)
+        if (M.doMHD) bFlux2Fld(M, G, A->S.magFlux, A->S.Bxyz);
+        EnforceBCs(M, G, A->S);
+        A->oS.Gas.d = A->S.Gas.d; A->oS.magFlux.d = A->S.magFlux.d; A->oS.Bxyz.d = A->S.Bxyz.d;
+        A->oS.time = A->S.time;
+        M.dt = CalcDT(M, G, A->S);
+        A->oS.time = A->S.time - M.dt;
     }
-    else initBW(M, G, A->S, p->b0Type == 1);
-    if (p->b0Type != 0) {   // CalcGridInfo: AddB0 after the IC (init.F90:180-184)
-        M.doBackground = true;
-        B0ctx bc;
-        bc.type = p->b0Type; bc.bx = p->b0[0]; bc.by = p->b0[1]; bc.bz = p->b0[2]; bc.M0 = p->b0[3];
-        AddB0(M, G, &bc);
-    }
-    // CalcGridInfo (init.F90:204-244)
-    if (M.doMHD) bFlux2Fld(M, G, A->S.magFlux, A->S.Bxyz);
-    EnforceBCs(M, G, A->S);
-    A->oS.Gas.d = A->S.Gas.d; A->oS.magFlux.d = A->S.magFlux.d; A->oS.Bxyz.d = A->S.Bxyz.d;
-    A->oS.time = A->S.time;
-    M.dt = CalcDT(M, G, A->S);
-    A->oS.time = A->S.time - M.dt;
     // initSolver (init.F90:494-516)
     Solver& V = A->V;
     int lo[6] = {G.isg, G.jsg, G.ksg, 1, 1, 0};

@@ -17,7 +17,7 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "_build", "libgamora.so")
 
-IC_OT2D, IC_BW, IC_LFMBW, IC_KH = 0, 1, 2, 3
+IC_OT2D, IC_BW, IC_LFMBW, IC_KH, IC_ADV1D, IC_ADV2D, IC_LOOP2D, IC_ALFVEN = range(8)
 GRID_UNIFORM, GRID_WARP, GRID_LFM = 0, 1, 2
 BC_PERIODIC, BC_ZEROGRAD, BC_LFMPOLE, BC_LFMBW, BC_HALO = 0, 1, 2, 3, 4
 # the reference's LFM blast-wave deck (tests/gamera/lfmbw.xml): prob x0, y0, z0, P0, pRat, D0, rC, B0
@@ -37,8 +37,8 @@ class OrcParams(C.Structure):
         ("b0Type", C.c_int), ("b0", C.c_double * 4),
         ("lfm", C.c_double * 4), ("dFloor", C.c_double), ("pFloor", C.c_double),
         ("doRing", C.c_int), ("ringNumR", C.c_int), ("ringNch", C.c_int * 32), ("ringRecon", C.c_int),
-        ("dtActive", C.c_int), ("bw", C.c_double * 8), ("kh", C.c_double * 4),
-        ("xyzIn", C.POINTER(C.c_double)),
+        ("dtActive", C.c_int), ("bw", C.c_double * 8), ("kh", C.c_double * 4), ("prob", C.c_double * 10),
+        ("noSetup", C.c_int), ("xyzIn", C.POINTER(C.c_double)),
     ]
 
 
@@ -113,10 +113,14 @@ class Oracle:
                  gamma=5.0 / 3.0, pdmb=0.75, Vd0=0.5, cHogH=0.25, cHogM=0.25, Ca=1.0e12, tFin=1.0e30,
                  doMHD=True, doBoris=False, rmeth="8CENT", doLFMLim=True, bc=None, threads=0, b0=None,
                  lfm=None, dFloor=0.0, pFloor=0.0, ring=None, dtActive=False, bw=LFMBW_DECK,
-                 kh=(0.03, 0.1, 0.01, 0), xyz=None):
+                 kh=(0.03, 0.1, 0.01, 0), prob=None, xyz=None, no_setup=False):
         p = OrcParams()
         p.Nip, p.Njp, p.Nkp = Nip, Njp, Nkp
-        p.icType = {"OT2D": IC_OT2D, "BW": IC_BW, "LFMBW": IC_LFMBW, "KH": IC_KH}[ic]
+        p.icType = {"OT2D": IC_OT2D, "BW": IC_BW, "LFMBW": IC_LFMBW, "KH": IC_KH, "ADV1D": IC_ADV1D,
+                    "ADV2D": IC_ADV2D, "LOOP2D": IC_LOOP2D, "ALFVEN": IC_ALFVEN}[ic]
+        if prob is not None:   # the problem's deck values (see CASE_DECKS)
+            for n, v in enumerate(prob):
+                p.prob[n] = v
         for n in range(4):   # Kelvin-Helmholtz {a, Bx, amp, seed}
             p.kh[n] = kh[n]
         p.gridType = {"uniform": GRID_UNIFORM, "warp": GRID_WARP, "lfm": GRID_LFM}[grid]
@@ -131,6 +135,7 @@ class Oracle:
                 p.ringNch[n] = c
             p.ringRecon = {"PLM": 0, "PPM": 1, "PCM": 2}[ring.get("recon", "PPM")]
         p.dtActive = int(dtActive)
+        p.noSetup = int(no_setup)   # allocate only: metrics, State, oState and scalars come from set()
         for n in range(8):
             p.bw[n] = bw[n]
         if xyz is not None:   # corners of a tile, (Ni+1, Nj+1, Nk+1, 3) Fortran order

@@ -303,3 +303,4 @@ def test_tma_staging_equals_cp_async(gpu_lib, oracle_lib, name, prec):
         assert a.status()["status"] == 0
         for nm in ("gas", "magflux", "bxyz"):
             assert np.array_equal(a.fetch(nm), b.fetch(nm)), (name, prec, nm)
+
