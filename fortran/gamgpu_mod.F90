@@ -14,7 +14,8 @@ module gamgpu_mod
                                  GAM_ERR_TIMEOUT = 4, GAM_ERR_UNSUPPORTED = 5, GAM_ERR_ARG = 6
     integer(c_int), parameter :: GAM_FP64 = 0, GAM_FP32FLUX = 1
     integer(c_int), parameter :: GAM_BC_PERIODIC = 0, GAM_BC_ZEROGRAD = 1, GAM_BC_LFMPOLE = 2, GAM_BC_LFMBW = 3, &
-                                 GAM_BC_HALO = 4
+                                 GAM_BC_HALO = 4, GAM_BC_ION = 5, GAM_BC_WIND = 6
+    integer(c_int), parameter :: GAM_NMSPH = 23
     integer(c_int), parameter :: GAM_RING_PLM = 0, GAM_RING_PPM = 1, GAM_RING_PCM = 2
     integer(c_int), parameter :: GAM_RM_8CENT = 0, GAM_RM_7UP = 1
     integer(c_int), parameter :: GAM_HALO_STATE = 1, GAM_HALO_OSTATE = 2, GAM_HALO_BXYZ = 4
@@ -163,6 +164,15 @@ module gamgpu_mod
             type(c_ptr), value :: h
             integer(c_int), value :: what, val
         end function gam_gpu_set_tile
+
+        ! the magnetosphere's hooks and gravity (voltron/ICs/earthcmi.F90 initUser) for a problem created from
+        ! Hatch's arrays; par = the GAM_NMSPH code-unit values (include/gamgpu.h, GAM_IC_MAGSPHERE)
+        integer(c_int) function gam_gpu_set_magnetosphere(h, par, n) bind(C, name="gam_gpu_set_magnetosphere")
+            import :: c_int, c_ptr, c_double
+            type(c_ptr), value :: h
+            real(c_double), intent(in) :: par(*)
+            integer(c_int), value :: n
+        end function gam_gpu_set_magnetosphere
 
         integer(c_int) function gam_gpu_divb(h, tot) bind(C, name="gam_gpu_divb")
             import :: c_int, c_ptr, c_double

@@ -38,6 +38,8 @@ extern "C" {
 #define GAM_BC_LFMPOLE 2       /* INJ/OUTJ across the LFM axis: lfmIn/lfmOut, src/gamera/bcs.F90:1020-1106 */
 #define GAM_BC_LFMBW 3         /* INI/OUTI fixed-gas shells of the LFM blast wave: bw_ibcI/bw_obcI,
                                   src/gamera/ICs/lfmbw.F90:141-225 (gas state gam_model_c.bwD0/bwP0) */
+#define GAM_BC_ION 5           /* INI: the magnetosphere's ionospheric boundary (IonInner, src/voltron/ICs/earthcmi.F90:378-522) */
+#define GAM_BC_WIND 6          /* OUTI: the magnetosphere's solar-wind boundary (WindBC, src/gamera/apps/wind.F90:206-374) */
 #define GAM_BC_HALO 4          /* INK/OUTK of a k-tile inside a decomposed problem: no physical BC, the ghost
                                   layers are filled from the neighbouring tile (the reference's mpiNullBc_T,
                                   src/gamera/mpi/gamapp_mpi.F90:428-463); not with doRing or do25D */
@@ -151,6 +153,17 @@ int gam_gpu_create_from_corners(gam_gpu_t** h, const gam_model_c* m, const doubl
 #define GAM_IC_ADV2D 5
 #define GAM_IC_LOOP2D 6
 #define GAM_IC_ALFVEN 7
+/*   GAM_IC_MAGSPHERE: the magnetosphere of the reference's Earth deck (tests/voltron/cmriD_Earth.xml, its Gamera
+ *   part: voltron/ICs/earthcmi.F90 initUser) with a constant solar wind and no ionospheric coupling -- the cut
+ *   dipole as background field with the elliptically cut initial field (apps/msphutils.F90:419-532), uniform gas
+ *   at rest, gravity (background.F90:170-252), the ionospheric inner boundary with zero potential and the
+ *   solar-wind outer boundary (bc {GAM_BC_ION, GAM_BC_WIND, GAM_BC_LFMPOLE x2, GAM_BC_PERIODIC x2} on an LFM
+ *   grid with rings; Model%doBackground = 1), and the hooks EFix, IonFlux and PerStep. icPar (GAM_NMSPH values,
+ *   code units) = {M0, GM0, rCut, lCut, dcScl, xSun, xTail, yMax, sInner, wind D, P, Vx, Vy, Vz, Bx, By, Bz,
+ *   dtCpl, gT0 [s], Rho0, P0, nIonP, doIonPush}; kaiju_b200/magnetosphere.py computes them from physical units
+ *   as setMagsphere and readWind do (apps/msphutils.F90:65-185, apps/wind.F90:620-700). */
+#define GAM_IC_MAGSPHERE 8
+#define GAM_NMSPH 23
 int gam_gpu_create_from_corners_ic(gam_gpu_t** h, const gam_model_c* m, const double* xyz, int ic,
                                    const double* icPar, int nPar);
 
@@ -386,6 +399,12 @@ int gam_closure_face_stats(gam_closure_t* c, int slot, double* rms, double* rel)
  * before Flux2Deltas; a step whose corrected update would make rho or P non-positive uses the plain
  * fluxes instead (counted by gam_gpu_closure_rejects). One handle per closure at a time. */
 int gam_gpu_set_closure(gam_gpu_t* h, gam_closure_t* c);
+/* The magnetosphere's hooks and gravity for a problem created with gam_gpu_create (its Grid and State as the
+ * reference's Hatch leaves them: bc {GAM_BC_ION, GAM_BC_WIND, ...}, the cut-dipole background arrays and
+ * gam_grid_c.xyz given): par = the GAM_NMSPH values of GAM_IC_MAGSPHERE. AddGrav runs on the device from the
+ * grid's metrics. Replaces: initUser's hooks and Model%Phi of voltron/ICs/earthcmi.F90:150-177 for one problem
+ * without ionospheric coupling. */
+int gam_gpu_set_magnetosphere(gam_gpu_t* h, const double* par, int n);
 int gam_gpu_closure_rejects(gam_gpu_t* h, int* n);
 /* restriction of a fine problem's State (2x the cells per direction) into a coarse problem's State
  * (GAM_SYNC_STATE) or oState (GAM_SYNC_OSTATE): gas volume-weighted, magnetic fluxes summed per face

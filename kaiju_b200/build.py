@@ -11,7 +11,7 @@ CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libgamgpu.so")
 SOURCES = ["gam_capi.cu", "gam_step.cu", "gam_flux.cu", "gam_efield.cu", "gam_init.cu", "gam_ring.cu",
            "gam_noalloc.cu", "gam_flux_f32.cu", "gam_efield_f32.cu", "gam_io.cu", "gam_tiles.cu",
-           "gam_net.cu", "gam_closure.cu"]
+           "gam_net.cu", "gam_closure.cu", "gam_msph.cu"]
 # The FP32-flux kernels use approximate single-precision division and square root (their error budget is
 # the FP32 path's 1e-5 L1 bound); every other unit keeps IEEE arithmetic. These flags touch
 # single-precision operations only.

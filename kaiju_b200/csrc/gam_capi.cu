@@ -140,7 +140,10 @@ int check_model(const gam_model_c* m) {
     for (int n = 0; n < 6; ++n) {
         int b = m->bc[n];
         bool ok = b == GAM_BC_PERIODIC || b == GAM_BC_ZEROGRAD || (b == GAM_BC_LFMPOLE && (n == 2 || n == 3)) ||
-                  (b == GAM_BC_LFMBW && n < 2) || (b == GAM_BC_HALO && n >= 4);
+                  (b == GAM_BC_LFMBW && n < 2) || (b == GAM_BC_HALO && n >= 4) || (b == GAM_BC_ION && n == 0) ||
+                  (b == GAM_BC_WIND && n == 1);
+        // the magnetosphere's boundaries work across the LFM axis (its ring maps)
+        if ((b == GAM_BC_ION || b == GAM_BC_WIND) && !m->doRing) return GAM_ERR_ARG;
         if (!ok) return GAM_ERR_UNSUPPORTED;
         // k tiles: ring averaging needs whole rings in k, 2.5D replicates the single k layer
         if (b == GAM_BC_HALO && (m->doRing || m->do25D)) return GAM_ERR_UNSUPPORTED;
@@ -183,6 +186,7 @@ int alloc_handle(gam_gpu* G, const gam_model_c* m) {
     p.dtActive = m->dtActive ? 1 : 0;
     p.bwD0 = m->bwD0; p.bwP0 = m->bwP0;
     p.stageWait = STAGE_WAIT;
+    p.msph = MsphPar{};
     if (m->doRing) {
         h.ring.NumR = m->ringNumR;
         for (int r = 0; r < 32; ++r) h.ring.Nch[r] = r < m->ringNumR ? m->ringNch[r] : 0;
@@ -315,6 +319,8 @@ int build_graphs(gam_gpu* G) {
 
 int launch_one_step(gam_gpu* G) {
     Handle& h = G->h;
+    // the magnetosphere's boundaries need its parameters (gam_gpu_set_magnetosphere or GAM_IC_MAGSPHERE)
+    if ((h.p.bc[0] == BC_ION || h.p.bc[1] == BC_WIND) && !h.p.msph.on) return GAM_ERR_ARG;
     if (h.useGraph) {
         if (!h.graph[0]) {
             int rc = build_graphs(G);
@@ -401,9 +407,11 @@ static int create_from_corners(gam_gpu_t** out, const gam_model_c* m, const doub
     *out = nullptr;
     int rc = check_model(m);
     if (rc) return rc;
-    bool caseIC = ic == GAM_IC_ADV1D || ic == GAM_IC_ADV2D || ic == GAM_IC_LOOP2D || ic == GAM_IC_ALFVEN;
+    bool caseIC = ic == GAM_IC_ADV1D || ic == GAM_IC_ADV2D || ic == GAM_IC_LOOP2D || ic == GAM_IC_ALFVEN ||
+                  ic == GAM_IC_MAGSPHERE;
     if (ic != GAM_IC_OT2D && ic != GAM_IC_BW && ic != GAM_IC_LFMBW && !((ic == GAM_IC_KH || caseIC) && icPar))
         return GAM_ERR_ARG;
+    if (ic == GAM_IC_MAGSPHERE && (m->bc[0] != GAM_BC_ION || m->bc[1] != GAM_BC_WIND)) return GAM_ERR_ARG;
     if ((m->Nip % 8) != 0) return GAM_ERR_ARG;   // Corners2Grid divisibility check (init.F90:830-834)
     if ((bg != nullptr) != (m->doBackground != 0)) return GAM_ERR_ARG;
     gam_gpu* G = new (std::nothrow) gam_gpu();
@@ -432,6 +440,14 @@ int gam_gpu_create_from_corners(gam_gpu_t** out, const gam_model_c* m, const dou
 int gam_gpu_create_from_corners_ic(gam_gpu_t** out, const gam_model_c* m, const double* xyz, int ic,
                                    const double* icPar, int nPar) {
     if (ic == GAM_IC_KH && (!icPar || nPar < 4 || !(icPar[0] > 0.0) || icPar[3] < 0.0)) return GAM_ERR_ARG;
+    if (ic == GAM_IC_MAGSPHERE) {   // its background is the cut dipole (genCutDipole)
+        if (!icPar || nPar < GAM_NMSPH || !m || !m->doBackground) return GAM_ERR_ARG;
+        BgSpec bg;
+        bg.type = 3;
+        bg.par[0] = bg.par[1] = bg.par[2] = 0.0; bg.par[3] = icPar[0];
+        bg.cut[0] = icPar[2]; bg.cut[1] = icPar[3]; bg.cut[2] = icPar[4];
+        return create_from_corners(out, m, xyz, ic, &bg, icPar);
+    }
     static const int casePars[4] = {0, 7, 9, 5};   // ADV1D, ADV2D, LOOP2D, ALFVEN
     if (ic >= GAM_IC_ADV1D && ic <= GAM_IC_ALFVEN) {
         int need = casePars[ic - GAM_IC_ADV1D];
@@ -646,6 +662,19 @@ int gam_gpu_set_tile(gam_gpu_t* G, int what, int value) {
     return GAM_OK;
 }
 
+int gam_gpu_set_magnetosphere(gam_gpu_t* G, const double* par, int n) {
+    if (!G || !par || n < GAM_NMSPH) return GAM_ERR_ARG;
+    Handle& h = G->h;
+    // WindEFix needs Grid%xyz (gam_grid_c.xyz)
+    if (h.p.bc[0] != BC_ION || h.p.bc[1] != BC_WIND || !h.p.doBackground || !G->haveCorners) return GAM_ERR_ARG;
+    if (h.closure) return GAM_ERR_UNSUPPORTED;
+    int rc = msph_setup(h, par, n);
+    if (rc) return GAM_ERR_CUDA;
+    destroy_graphs(h);
+    CK(cudaStreamSynchronize(h.stream));
+    return GAM_OK;
+}
+
 int gam_gpu_set_closure(gam_gpu_t* G, gam_closure_t* c) {
     if (!G) return GAM_ERR_ARG;
     Handle& h = G->h;
@@ -814,6 +843,7 @@ void gam_gpu_destroy(gam_gpu_t* G) {
     if (h.dScal) cudaFree(h.dScal);
     if (h.hScal) cudaFreeHost(h.hScal);
     if (h.stream && h.ownStream) cudaStreamDestroy(h.stream);
+    if (h.msphpool) cudaFree(h.msphpool);
     delete G;
 }
 

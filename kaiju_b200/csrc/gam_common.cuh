@@ -23,7 +23,18 @@ enum { IDIR = 0, JDIR = 1, KDIR = 2 };
 enum { RM_8CENT = 0, RM_7UP = 1 };
 // BC_HALO: a face between two k-tiles of one problem; no physical BC runs there, its ghost layers are
 // filled from the neighbouring tile after the step (the reference's mpiNullBc_T, gamapp_mpi.F90:428-463)
-enum { BC_PERIODIC = 0, BC_ZEROGRAD = 1, BC_LFMPOLE = 2, BC_LFMBW = 3, BC_HALO = 4 };
+// BC_ION / BC_WIND: the magnetosphere's ionospheric inner and solar-wind outer I boundaries (gam_msph.cu)
+enum { BC_PERIODIC = 0, BC_ZEROGRAD = 1, BC_LFMPOLE = 2, BC_LFMBW = 3, BC_HALO = 4, BC_ION = 5, BC_WIND = 6 };
+
+// The magnetosphere problem (voltron/ICs/earthcmi.F90 initUser with a constant solar wind and no
+// ionospheric coupling), code units: the wind, PushIon's coupling time, NudgeSW's time unit, gravity
+struct MsphPar {
+    int on;
+    double wD, wP, wV[3], wB[3];   // the solar wind
+    double dtCpl, gT0;             // ibc dtCpl; the time unit in seconds
+    int nIonP, doIonPush;
+    int doGrav;                    // gravitational acceleration planes present (AddGrav)
+};
 
 struct Lay {
     int Nip, Njp, Nkp;     // active cells
@@ -55,6 +66,7 @@ struct Par {
     // default STAGE_WAIT). After giving up a CTA still waits, with the far larger STAGE_DRAIN bound, for its own
     // copies to land before it exits, and the step reports GAM_ERR_TIMEOUT.
     unsigned int stageWait;
+    MsphPar msph;
 };
 constexpr unsigned int STAGE_WAIT = 1u << 20;
 constexpr unsigned int STAGE_DRAIN = 1u << 28;

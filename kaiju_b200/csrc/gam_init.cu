@@ -6,6 +6,7 @@
 #include "gam_common.cuh"
 #include "gam_step.cuh"
 #include "gam_init.cuh"
+#include "gamgpu.h"
 
 namespace gam {
 
@@ -471,21 +472,105 @@ struct AlfPot {
     }
 };
 
+// RampUp (math.F90:174-189); exp(1.0) there is of a default-real literal
+__device__ __forceinline__ double rampUp(double r, double rC, double lC) {
+    double rScl = (r - rC) / lC;
+    if (rScl <= 0.0) return 0.0;
+    if (rScl >= 1.0) return 1.0;
+    double eArg = -1.0 / (rScl * rScl);
+    return (double)expf(1.0f) * exp(eArg);
+}
+// PenticRampDown (math.F90:156-172), msphutils' magRampDown
+__device__ __forceinline__ double penticRampDown(double r, double rC, double lC) {
+    double rScl = (r - rC) / lC;
+    if (rScl <= 0.0) return 1.0;
+    if (rScl >= 1.0) return 0.0;
+    double Mc = 6 * pow(rScl, 5.0) - 15 * pow(rScl, 4.0) + 10 * pow(rScl, 3.0);
+    return 1.0 - Mc;
+}
+// ---- the magnetosphere problem's set-up (voltron/ICs/earthcmi.F90 initUser, apps/msphutils.F90 genCutDipole)
+// VP_Init (msphutils.F90:503-532): the dipole's vector potential cut off outside an ellipse about the planet
+struct VPInitPot {
+    double M0, x0, Aq, Bq, sInner;
+    __device__ void operator()(double x, double y, double z, double* A) const {
+        double r[3] = {x, y, z};
+        double nr = norm2v3(r), rh[3] = {x / nr, y / nr, z / nr};
+        double rr = x * x + y * y + z * z;
+        double cr[3] = {0.0 * rh[2] - 1.0 * rh[1], 1.0 * rh[0] - 0.0 * rh[2], 0.0 * rh[1] - 0.0 * rh[0]};
+        for (int c = 0; c < 3; ++c) A[c] = M0 * cr[c] / rr;   // VP_Dipole
+        double s = sqrt(sq((x + x0) / Aq) + (sq(y) + sq(z)) / sq(Bq));
+        double M = penticRampDown(s, sInner, 1.0 - sInner);
+        A[0] = M * A[0]; A[1] = M * A[1]; A[2] = M * A[2];
+    }
+};
+// uniform gas at rest (earthcmi.F90:183-200 GasIC)
+struct GasConst {
+    double D, P;
+    __device__ void operator()(double, double, double, double* W) const {
+        W[0] = D; W[1] = 0.0; W[2] = 0.0; W[3] = 0.0; W[4] = P;
+    }
+};
+// genCutDipole's guard (msphutils.F90:469-485): no background force in cells reaching inside rCut
+__global__ void k_cut_dpb0(Lay L, Corners X, double rCut, Out3 dp) {
+    long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (t >= (long long)L.Nip * L.Njp * L.Nkp) return;
+    int i = L.is() + (int)(t % L.Nip);
+    long long q = t / L.Nip;
+    int j = L.js() + (int)(q % L.Njp), k = L.ks() + (int)(q / L.Njp);
+    double xyzC[8][3];
+    cellCorners(L, X, i, j, k, xyzC);
+    double rMin = 0.0;
+    for (int p = 0; p < 8; ++p) {
+        double r = norm2v3(xyzC[p]);
+        rMin = (p == 0 || r < rMin) ? r : rMin;
+    }
+    if (rMin + TINY < rCut) {
+        long long c = L.at(i, j, k);
+        dp.v[0][c] = 0.0; dp.v[1][c] = 0.0; dp.v[2][c] = 0.0;
+    }
+}
+// the initial residual field (genCutDipole's last lines): the vector potential's fluxes on the cells
+// isg..ieg-1 (VectorPot2Flux's range) minus the background's face fluxes there; zero elsewhere (VectorField2Flux
+// and the background give the same fluxes on the last cell layer, and the outermost faces are never set)
+__global__ void k_msph_residual(Lay L, Out3 bF0, StateP s) {
+    long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    int ni = L.Ni + 1, nj = L.Nj + 1, nk = L.Nk + 1;
+    if (t >= (long long)ni * nj * nk) return;
+    int i = (int)(t % ni);
+    long long q = t / ni;
+    int j = (int)(q % nj), k = (int)(q / nj);
+    long long c = L.at(i, j, k);
+    bool vp = i <= L.Ni - 2 && j <= L.Nj - 2 && k <= L.Nk - 2;
+    for (int d = 0; d < 3; ++d) s.mf[d][c] = vp ? s.mf[d][c] - bF0.v[d][c] : 0.0;
+}
+
 // ------------------------------------------------------------------------------------ background field
 // AddB0 (background.F90:20-167) for the built-in background functions: per cell, the 12x12-point face
 // flux, face average and Maxwell stress of B0 on its three lower faces, the 12-point edge averages on
 // its three lower edges (mapped to the edge frame T1/T2), and the 12^3-point cell average.
 struct B0Fn {
     int type;                // GAM_B0_UNIFORM (1): (bx, by, bz); GAM_B0_DIPOLE (2): moment M0 along z at (bx, by, bz)
-    double bx, by, bz, M0;
-    __device__ void operator()(double x, double y, double z, double* A) const {
-        if (type == 1) { A[0] = bx; A[1] = by; A[2] = bz; return; }
+    double bx, by, bz, M0;   // 3: the magnetosphere's cut dipole (moment M0 at the origin)
+    double rCut = 0.0, lCut = 0.0, dcScl = 1.0;
+    __device__ void dipole(double x, double y, double z, double* A) const {
         // Dipole (apps/msphutils.F90:534-551): 3 (m.r) r / rad**5 - m / rad**3
         double r[3] = {x - bx, y - by, z - bz};
         double rad = norm2v3(r);
         double m[3] = {0.0, 0.0, M0};
         double mr = m[0] * r[0] + m[1] * r[1] + m[2] * r[2];
         for (int c = 0; c < 3; ++c) A[c] = 3 * mr * r[c] / pow(rad, 5.0) - m[c] / pow(rad, 3.0);
+    }
+    __device__ void operator()(double x, double y, double z, double* A) const {
+        if (type == 1) { A[0] = bx; A[1] = by; A[2] = bz; return; }
+        dipole(x, y, z, A);
+        if (type == 3) {   // cutDipole (msphutils.F90:561-579)
+            double r = sqrt(sq(x) + sq(y) + sq(z));
+            double yp = sqrt(sq(y) + sq(z));
+            double phid = atan2(yp, x) * 180.0 / PI;
+            double rScl = 1.0 + rampUp(phid, 0.0, 180.0) * (dcScl - 1.0);
+            double M = penticRampDown(r, rCut * rScl, lCut * rScl);
+            A[0] = M * A[0]; A[1] = M * A[1]; A[2] = M * A[2];
+        }
     }
 };
 struct B0Vol {   // the vector wrapped as a 5-variable integrand for volumeIntegral
@@ -641,7 +726,7 @@ int add_background(Handle& h, const BgSpec& bg) {
     cudaStream_t st = h.stream;
     if (!h.bgpool) return 1;
     Corners X = {{h.xyz[0], h.xyz[1], h.xyz[2]}};
-    B0Fn F{bg.type, bg.par[0], bg.par[1], bg.par[2], bg.par[3]};
+    B0Fn F{bg.type, bg.par[0], bg.par[1], bg.par[2], bg.par[3], bg.cut[0], bg.cut[1], bg.cut[2]};
     BgOut o;
     for (int d = 0; d < 3; ++d) {
         for (int x = 0; x < 3; ++x) { o.fcB0[d][x] = h.fcB0[d][x]; o.fS[d][x] = h.gflx[d][x]; }   // gflx: scratch
@@ -660,6 +745,30 @@ int add_background(Handle& h, const BgSpec& bg) {
     return 0;
 }
 
+// The magnetosphere's parameters (GAM_IC_MAGSPHERE order: M0, GM0, rCut, lCut, dcScl, xSun, xTail, yMax,
+// sInner, the wind's D, P, V (3), B (3), dtCpl, gT0, Rho0, P0, nIonP, doIonPush) into h.p.msph; the gravity
+// planes allocated (once) and filled by AddGrav from the grid's metrics
+int msph_setup(Handle& h, const double* par, int n) {
+    if (!par || n < GAM_NMSPH) return 1;
+    const Lay& L = h.L;
+    MsphPar& m = h.p.msph;
+    m.on = 1;
+    m.wD = par[9]; m.wP = par[10];
+    for (int c = 0; c < 3; ++c) { m.wV[c] = par[11 + c]; m.wB[c] = par[14 + c]; }
+    m.dtCpl = par[17]; m.gT0 = par[18];
+    m.nIonP = (int)par[21]; m.doIonPush = par[22] != 0.0 ? 1 : 0;
+    if (!h.msphpool) {
+        if (cudaMalloc(&h.msphpool, sizeof(double) * L.E * 3) != cudaSuccess) return 3;
+        if (cudaMemsetAsync(h.msphpool, 0, sizeof(double) * L.E * 3, h.stream) != cudaSuccess) return 3;
+        for (int c = 0; c < 3; ++c) h.gxyz[c] = h.msphpool + (size_t)c * L.E;
+    }
+    m.doGrav = 1;
+    launch_add_grav(h, par[1], h.stream);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) { std::fprintf(stderr, "gamgpu: magnetosphere set-up: %s\n", cudaGetErrorString(e)); return 3; }
+    return 0;
+}
+
 int init_problem(Handle& h, int ic, const BgSpec* bg, const double* icPar) {
     const Lay& L = h.L;
     cudaStream_t st = h.stream;
@@ -675,6 +784,29 @@ int init_problem(Handle& h, int ic, const BgSpec* bg, const double* icPar) {
         long long n = (long long)(L.Nip + 1) * (L.Njp + 1) * (L.Nkp + 1);
         k_ic_kh<<<nb(n, 256), 256, 0, st>>>(L, h.p, g, s, kh);
         h.launches++;
+    } else if (ic == 8) {   // the magnetosphere
+        if (!icPar || !bg || bg->type != 3) return 1;
+        int rc = add_background(h, *bg);   // genCutDipole: AddB0 of the cut dipole first
+        if (rc) return rc;
+        Corners X = {{h.xyz[0], h.xyz[1], h.xyz[2]}};
+        Out3 dp = {{h.dpB0[0], h.dpB0[1], h.dpB0[2]}};
+        long long na = (long long)L.Nip * L.Njp * L.Nkp;
+        k_cut_dpb0<<<nb(na, 128), 128, 0, st>>>(L, X, icPar[2], dp);
+        Out3 lA = {{h.E[0], h.E[1], h.E[2]}};   // E planes as scratch for the edge integrals of A
+        long long ne = (long long)(L.Ni - 1) * (L.Nj - 1) * (L.Nk - 1);
+        VPInitPot vp;
+        vp.M0 = icPar[0]; vp.Aq = 0.5 * (icPar[5] - icPar[6]); vp.x0 = vp.Aq - icPar[5]; vp.Bq = icPar[7];
+        vp.sInner = icPar[8];
+        k_ic_vecpot_la<<<nb(ne, 128), 128, 0, st>>>(L, X, lA, vp);
+        k_ic_vecpot_flux<<<nb(ne, 256), 256, 0, st>>>(L, lA, s);
+        cudaMemsetAsync(h.E[0], 0, sizeof(double) * L.E * 3, st);
+        Out3 bF0 = {{h.bFlux0[0], h.bFlux0[1], h.bFlux0[2]}};
+        long long nf = (long long)(L.Ni + 1) * (L.Nj + 1) * (L.Nk + 1);
+        k_msph_residual<<<nb(nf, 256), 256, 0, st>>>(L, bF0, s);
+        k_ic_quad_gas<<<nb(na, 128), 128, 0, st>>>(L, h.p, X, h.volume, s, GasConst{icPar[19], icPar[20]});
+        h.launches += 5;
+        rc = msph_setup(h, icPar, GAM_NMSPH);
+        if (rc) return rc;
     } else if (ic >= 4 && ic <= 7) {
         if (!icPar) return 1;
         ICPar pr;
@@ -718,7 +850,7 @@ int init_problem(Handle& h, int ic, const BgSpec* bg, const double* icPar) {
         h.launches++;
     }
     // CalcGridInfo: AddB0 after the IC (init.F90:180-184), then the tail (init.F90:204-244)
-    if (bg) {
+    if (bg && ic != 8) {
         int rc = add_background(h, *bg);
         if (rc) return rc;
     }

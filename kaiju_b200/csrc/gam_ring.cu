@@ -475,6 +475,12 @@ void launch_pole_e(Handle& h, double* const* E, cudaStream_t st) {
     k_fix_e_lfm<<<nblk1((long long)(L.Nip + 1) * (L.Njp + 1), 256), 256, 0, st>>>(L, e);
     h.launches += 2;
 }
+void launch_fix_e_lfm(Handle& h, double* const* E, cudaStream_t st) {
+    const Lay& L = h.L;
+    Vec3P e = {{E[0], E[1], E[2]}};
+    k_fix_e_lfm<<<nblk1((long long)(L.Nip + 1) * (L.Njp + 1), 256), 256, 0, st>>>(L, e);
+    h.launches++;
+}
 void launch_ring_average(Handle& h, const StateP& s, cudaStream_t st) {
     const Lay& L = h.L;
     const Par& p = h.p;

@@ -510,7 +510,7 @@ __global__ void k_bc_i(Lay L, Par p, GridP g, StateP s) {
         long long d = L.at(is - n, j, k), sidx = L.at(ie - n + 1, j, k);
         if (cell) cpcell(s, d, sidx, true);
         cpmf(s, d, sidx);
-    } else if (cell) {
+    } else if (p.bc[0] != BC_ION && cell) {   // BC_ION: launch_msph_bcs
         long long d = L.at(is - n, j, k), sidx = L.at(is, j, k);
         cpcell(s, d, sidx, false);
         cpmf(s, d, sidx);
@@ -522,7 +522,7 @@ __global__ void k_bc_i(Lay L, Par p, GridP g, StateP s) {
         s.mf[1][d] = s.mf[1][sidx];
         s.mf[2][d] = s.mf[2][sidx];
         s.mf[0][d + 1] = s.mf[0][L.at(is + n, j, k)];
-    } else if (cell) {
+    } else if (p.bc[1] != BC_WIND && cell) {   // BC_WIND: launch_msph_bcs
         double B[3];
         cellBxyz(L, g, s.mf, L.at(ie, j, k), B);
         int ig = ie + n;
@@ -720,6 +720,7 @@ void launch_bflux2fld(Handle& h, const StateP& s, cudaStream_t st) {
 void launch_bcs(Handle& h, const StateP& s, cudaStream_t st) {
     const Lay& L = h.L;
     k_bc_i<<<nblk((long long)L.nG * (L.Nj + 1) * (L.Nk + 1), TPB), TPB, 0, st>>>(L, h.p, h.gridP(), s);
+    if (h.p.bc[0] == BC_ION || h.p.bc[1] == BC_WIND) launch_msph_bcs(h, s, st);   // IonInner, WindBC
     k_bc_j<<<nblk((long long)(L.Ni + 1) * (L.Nk + 1), TPB), TPB, 0, st>>>(L, h.p, s);
     k_bc_k<<<nblk((long long)(L.Ni + 1) * (L.Nj + 1), TPB), TPB, 0, st>>>(L, h.p, s);
     h.launches += 3;
@@ -820,6 +821,7 @@ int kernels_per_step(const Handle& h) {
     n += 1 + 1 + 1;                     // e2flux/copy, bflux2fld, update gas
     n += 2 + 3 + 1;                     // calcdt + finalize, 3 BC kernels, final bflux2fld
     n += ring_kernels_per_step(h);
+    n += msph_kernels_per_step(h);
     if (h.closure) n += closure_kernels_per_step(h) + 1;   // + the conditional Flux2Deltas
     return n;
 }
@@ -876,7 +878,10 @@ int step_enqueue(Handle& h, int cur, cudaEvent_t* ev, bool split, int part) {
     if (p.doRing) launch_ring_bfix(h, h.H, st, h.prec == PREC_FP32FLUX);   // bFlux2Fld's ring fix
     if (p.predFixLFM) launch_predfix_lfm(h, h.H, st, h.prec == PREC_FP32FLUX);   // HackPredictor
     mark(PH_EFIELD);
-    if (p.doMHD) enqueue_efield(h, nS, st);
+    if (p.doMHD) {
+        enqueue_efield(h, nS, st);
+        if (p.msph.on) launch_msph_efix(h, nS, st);   // HackE (mhdgroup.F90:40-44)
+    }
     }
     if (part == STEP_PRE) return (int)cudaGetLastError();
     if (part == STEP_ALL) {
@@ -884,6 +889,7 @@ int step_enqueue(Handle& h, int cur, cudaEvent_t* ev, bool split, int part) {
         enqueue_fluxes(h, nS, st);
     }
     if (p.doRing) launch_ring_flux(h, st);   // stress.F90:134-139
+    if (p.msph.on) launch_ion_flux(h, st);    // HackFlux (stress.F90:141-143)
     mark(PH_DELTAS);
     PrimP dGH;
     for (int v = 0; v < 5; ++v) dGH.w[v] = h.dGasH[v];
@@ -926,7 +932,9 @@ int step_enqueue(Handle& h, int cur, cudaEvent_t* ev, bool split, int part) {
         else k_update_gas<double, false><<<grid_plane(cells, TPB), TPB, 0, st>>>(L, p, g, nS, oS, dGH, dGM, F64[0], F64[1], F64[2], h.dScal);
     }
     h.launches += 4;
+    if (p.msph.on) launch_apply_grav(h, oS, nS, st);   // mhdgroup.F90:60-65 (oS holds the new state)
     if (p.doRing) launch_ring_average(h, oS, st);   // mhdgroup.F90:68-74
+    if (p.msph.on) launch_msph_perstep(h, oS, st);   // HackStep (gamapp.F90:104-109)
     // CalcDT (the per-cell minimum; finalized below, or after the tiles' minimum for a tiled run)
     mark(PH_DT);
     launch_calcdt_partial(h, oS, st);

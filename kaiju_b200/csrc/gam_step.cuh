@@ -68,6 +68,9 @@ struct Handle {
     // ring-average smoothing E field (own allocation, only with Model%doRing)
     double* ringpool = nullptr;
     double* SmoothE[3] = {};
+    // gravitational acceleration (own allocation, only with the magnetosphere's gravity), Grid_T gxyz
+    double* msphpool = nullptr;
+    double* gxyz[3] = {};
     // FP32 copies for the FP32-flux mode (allocated on first use)
     float* f32pool = nullptr;
     F32Planes f32{};
@@ -130,6 +133,15 @@ void launch_ring_bfix(Handle& h, const StateP& s, cudaStream_t st, bool withF32 
 void launch_predfix_lfm(Handle& h, const StateP& s, cudaStream_t st, bool withF32 = false);  // lfmbw PredFix
 void launch_ring_flux(Handle& h, cudaStream_t st);                              // RingFlux + FixGasFluxLFM
 void launch_pole_e(Handle& h, double* const* E, cudaStream_t st);               // PoleE + FixEFieldLFM
+void launch_fix_e_lfm(Handle& h, double* const* E, cudaStream_t st);            // FixEFieldLFM alone
+// the magnetosphere problem (gam_msph.cu): its I boundaries, EFix, IonFlux, gravity and PerStep hooks
+void launch_msph_bcs(Handle& h, const StateP& s, cudaStream_t st);
+void launch_msph_efix(Handle& h, const StateP& nS, cudaStream_t st);
+void launch_ion_flux(Handle& h, cudaStream_t st);
+void launch_apply_grav(Handle& h, const StateP& S, const StateP& O, cudaStream_t st);
+void launch_msph_perstep(Handle& h, const StateP& S, cudaStream_t st);
+void launch_add_grav(Handle& h, double GM0, cudaStream_t st);
+int msph_kernels_per_step(const Handle& h);
 void launch_ring_average(Handle& h, const StateP& s, cudaStream_t st);          // RingAverage
 int ring_kernels_per_step(const Handle& h);
 // slice output (gam_io.cu): doubles of a slice, and the kernels that compute one into dst (device) from

@@ -24,12 +24,14 @@ LIB_PATH = os.path.join(HERE, "libgamgpu.so")
 
 GAM_OK, GAM_ERR_NAN, GAM_ERR_DT_COLLAPSE, GAM_ERR_CUDA, GAM_ERR_TIMEOUT, GAM_ERR_UNSUPPORTED, GAM_ERR_ARG = range(7)
 GAM_FP64, GAM_FP32FLUX = 0, 1
-GAM_BC_PERIODIC, GAM_BC_ZEROGRAD, GAM_BC_LFMPOLE, GAM_BC_LFMBW, GAM_BC_HALO = 0, 1, 2, 3, 4
+GAM_BC_PERIODIC, GAM_BC_ZEROGRAD, GAM_BC_LFMPOLE, GAM_BC_LFMBW, GAM_BC_HALO, GAM_BC_ION, GAM_BC_WIND = range(7)
 GAM_HALO_STATE, GAM_HALO_OSTATE, GAM_HALO_BXYZ = 1, 2, 4
 GAM_RING_PLM, GAM_RING_PPM, GAM_RING_PCM = 0, 1, 2
 GAM_RM_8CENT, GAM_RM_7UP = 0, 1
 GAM_SYNC_STATE, GAM_SYNC_OSTATE = 1, 2
-GAM_IC_OT2D, GAM_IC_BW, GAM_IC_LFMBW, GAM_IC_KH, GAM_IC_ADV1D, GAM_IC_ADV2D, GAM_IC_LOOP2D, GAM_IC_ALFVEN = range(8)
+(GAM_IC_OT2D, GAM_IC_BW, GAM_IC_LFMBW, GAM_IC_KH, GAM_IC_ADV1D, GAM_IC_ADV2D, GAM_IC_LOOP2D, GAM_IC_ALFVEN,
+ GAM_IC_MAGSPHERE) = range(9)
+GAM_NMSPH = 23
 GAM_SLICE_FAT = 1
 GAM_B0_UNIFORM, GAM_B0_DIPOLE = 1, 2
 GAM_TILE_FLUX_ROWS, GAM_TILE_FUSED_UPDATE, GAM_TILE_TMA, GAM_TILE_STAGE_WAIT = 1, 2, 3, 4
@@ -146,6 +148,7 @@ SIGNATURES = {
     "gam_closure_set_loss": (C.c_int, [C.c_void_p, C.c_int]),
     "gam_closure_face_stats": (C.c_int, [C.c_void_p, C.c_int, _DP, _DP]),
     "gam_gpu_set_closure": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "gam_gpu_set_magnetosphere": (C.c_int, [C.c_void_p, _DP, C.c_int]),
     "gam_gpu_closure_rejects": (C.c_int, [C.c_void_p, C.POINTER(C.c_int)]),
     "gam_gpu_restrict": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint]),
     "gam_gpu_init_dt": (C.c_int, [C.c_void_p]),
@@ -403,7 +406,8 @@ class GameraGPU:
         h = C.c_void_p()
         m = model.to_c()
         icn = {"OT2D": GAM_IC_OT2D, "BW": GAM_IC_BW, "LFMBW": GAM_IC_LFMBW, "KH": GAM_IC_KH, "ADV1D": GAM_IC_ADV1D,
-               "ADV2D": GAM_IC_ADV2D, "LOOP2D": GAM_IC_LOOP2D, "ALFVEN": GAM_IC_ALFVEN}[ic]
+               "ADV2D": GAM_IC_ADV2D, "LOOP2D": GAM_IC_LOOP2D, "ALFVEN": GAM_IC_ALFVEN,
+               "MAGSPHERE": GAM_IC_MAGSPHERE}[ic]
         if icn == GAM_IC_ADV1D and ic_par is None:
             ic_par = np.zeros(0)
         if ic_par is not None:
@@ -550,6 +554,14 @@ class GameraGPU:
         rc = load_library().gam_gpu_set_tile(self.h, what, value)
         if rc:
             raise GamError(rc, "gam_gpu_set_tile")
+
+    def set_magnetosphere(self, par: np.ndarray):
+        """The magnetosphere's hooks and gravity for a problem created from Hatch's arrays
+        (gam_gpu_set_magnetosphere); par: kaiju_b200.magnetosphere.Magnetosphere().code_params()."""
+        par = np.ascontiguousarray(par, dtype=np.float64)
+        rc = load_library().gam_gpu_set_magnetosphere(self.h, par.ctypes.data_as(_DP), len(par))
+        if rc:
+            raise GamError(rc, "gam_gpu_set_magnetosphere")
 
     def set_closure(self, closure: Optional["Closure"]):
         rc = load_library().gam_gpu_set_closure(self.h, closure.c if closure is not None else None)

@@ -4,6 +4,7 @@ and ionosphere boundaries are not built, so the reference's LFM blast wave suppl
 the plain FP64 path and the FP32-flux path side by side.
 
     python -m kaiju_b200.runs spherical --n 96 96 128 --steps 2000
+    python -m kaiju_b200.runs magnetosphere --n 96 96 128 --steps 2000   # the Earth deck with a solar wind
     python -m kaiju_b200.runs closure-step --n 128 --steps 20
     python -m kaiju_b200.runs ensemble --steps 20          # 96 Kelvin-Helmholtz members, FP32-flux
     python -m kaiju_b200.runs ensemble-run --t-end 2       # the same members run to t = 2
@@ -60,6 +61,44 @@ def spherical(n=(96, 96, 128), steps=2000, dipole=2000.0, grid=(10.0, 100.0, 1.0
     out["fp32flux"]["l1_rel_vs_fp64_per_var"] = l1
     out["fp32flux"]["speedup_vs_fp64_per_step"] = out["fp64"]["ms_per_step"] / out["fp32flux"]["ms_per_step"]
     out["divb"] = {"fp64": g64.divb(), "fp32flux": g32.divb()}
+    g64.close()
+    g32.close()
+    return out
+
+
+def magnetosphere(n=(96, 96, 128), steps: int = 2000):
+    """The spherical configuration as specified: the Earth deck's magnetosphere (kaiju_b200/magnetosphere.py)
+    on the 96x96x128 LFM-type grid r in [2, 30] with a 3.1e4 nT dipole and a constant solar wind
+    (5 amu/cc, -400 km/s, Bz = -5 nT, 1e5 K) entering at the outer shell. The FP64 path for `steps` steps
+    (device-timed), then the FP32-flux path from the same start to the same end time, and their difference."""
+    import dataclasses
+    from . import magnetosphere as ms
+    cells = n[0] * n[1] * n[2]
+    out = {"cells": list(n), "steps": steps, "grid_r_stretch_theta0": list(ms.GRID),
+           "code_params": [float(v) for v in ms.Magnetosphere().code_params()]}
+    g64 = ms.magnetosphere_problem(n)
+    ms64, rc = g64.run_steps_timed(steps)
+    st = g64.status()
+    t_end = st["t"]
+    out["fp64"] = {"ms_per_step": ms64 / steps, "zone_updates_per_s": cells * steps / (ms64 / 1e3), "status": rc,
+                   "t_end_code": t_end, "t_end_s": t_end * ms.Magnetosphere().gT0}
+    g32 = ms.magnetosphere_problem(n, tFin=t_end)
+    g32.set_precision(gm.GAM_FP32FLUX)
+    ms32, done, rc32 = 0.0, 0, 0
+    while g32.status()["t"] < t_end * (1.0 - 1e-14) and done < 4 * steps:
+        m, rc32 = g32.run_steps_timed(100)
+        ms32 += m
+        done += 100
+    st32 = g32.status()
+    out["fp32flux"] = {"ms_per_step": ms32 / done, "zone_updates_per_s": cells * done / (ms32 / 1e3),
+                       "steps_to_t_end": int(st32["ts"]), "t": st32["t"], "status": rc32}
+    a, b = g64.fetch("gas")[4:-4, 4:-4, 4:-4], g32.fetch("gas")[4:-4, 4:-4, 4:-4]
+    out["fp32flux"]["l1_rel_vs_fp64_per_var"] = [
+        float(np.mean(np.abs(a[..., v] - b[..., v])) / np.mean(np.abs(a[..., v]))) for v in range(5)]
+    out["fp32flux"]["speedup_vs_fp64_per_step"] = out["fp64"]["ms_per_step"] / out["fp32flux"]["ms_per_step"]
+    out["divb"] = {"fp64": g64.divb(), "fp32flux": g32.divb()}
+    rho = a[..., 0]
+    out["fp64"]["density_min_max"] = [float(rho.min()), float(rho.max())]
     g64.close()
     g32.close()
     return out
@@ -174,13 +213,15 @@ def tiles(n: int = 256, steps: int = 10):
 
 def main(argv=None):
     ap = argparse.ArgumentParser()
-    ap.add_argument("run", choices=["spherical", "closure-step", "ensemble", "ensemble-run", "tiles"])
+    ap.add_argument("run", choices=["spherical", "magnetosphere", "closure-step", "ensemble", "ensemble-run", "tiles"])
     ap.add_argument("--t-end", type=float, default=2.0)
     ap.add_argument("--n", type=int, nargs="+", default=None)
     ap.add_argument("--steps", type=int, default=None)
     a = ap.parse_args(argv)
     if a.run == "spherical":
         print(json.dumps(spherical(tuple(a.n or [96, 96, 128]), a.steps or 2000), indent=1))
+    elif a.run == "magnetosphere":
+        print(json.dumps(magnetosphere(tuple(a.n or [96, 96, 128]), a.steps or 2000), indent=1))
     elif a.run == "ensemble":
         print(json.dumps(ensemble(a.steps or 20), indent=1))
     elif a.run == "ensemble-run":

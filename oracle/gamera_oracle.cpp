@@ -2408,10 +2408,36 @@ static void VectorPot2Flux(const Grid& G, State& S, VecFun Axyz, void* ctx) {  /
 // ---------------------------------------------------------------- background field (background.F90:20-167)
 // type 1: uniform (bx,by,bz); 2: dipole of moment M0 along z centred at (bx,by,bz) (the reference's
 // magnetosphere dipole is the centre-at-origin case; the offset keeps the singularity off a test domain)
-struct B0ctx { int type; double bx, by, bz, M0; };
+struct B0ctx { int type; double bx, by, bz, M0; double rCut = 0, lCut = 0, dcScl = 1; };
+static double RampUpE(double r, double rC, double lC) {   // RampUp, math.F90:174-189
+    double rScl = (r - rC) / lC;
+    if (rScl <= 0.0) return 0.0;
+    if (rScl >= 1.0) return 1.0;
+    double eArg = -1.0 / (rScl * rScl);
+    return (double)std::exp(1.0f) * std::exp(eArg);   // exp(1.0) of a default-real literal
+}
+static double PenticRampDown(double r, double rC, double lC) {   // math.F90:156-172 (msphutils' magRampDown)
+    double rScl = (r - rC) / lC;
+    if (rScl <= 0.0) return 1.0;
+    if (rScl >= 1.0) return 0.0;
+    double Mc = 6 * std::pow(rScl, 5.0) - 15 * std::pow(rScl, 4.0) + 10 * std::pow(rScl, 3.0);
+    return 1.0 - Mc;
+}
 static void B0fun(double x, double y, double z, double* A, void* c) {
     B0ctx* b = (B0ctx*)c;
     if (b->type == 1) { A[0] = b->bx; A[1] = b->by; A[2] = b->bz; return; }
+    if (b->type == 3) {   // cutDipole (apps/msphutils.F90:561-579): the dipole at the origin, ramped down
+        double r = std::sqrt(sq(x) + sq(y) + sq(z));
+        B0ctx d = *b;
+        d.type = 2; d.bx = d.by = d.bz = 0.0;
+        B0fun(x, y, z, A, &d);
+        double yp = std::sqrt(sq(y) + sq(z));
+        double phid = std::atan2(yp, x) * 180.0 / PI;
+        double rScl = 1.0 + RampUpE(phid, 0.0, 180.0) * (b->dcScl - 1.0);
+        double M = PenticRampDown(r, b->rCut * rScl, b->lCut * rScl);
+        A[0] = M * A[0]; A[1] = M * A[1]; A[2] = M * A[2];
+        return;
+    }
     // Dipole (apps/msphutils.F90:534-551): 3 (m.r) r / rad**5 - m / rad**3
     double r[3] = {x - b->bx, y - b->by, z - b->bz};
     double rad = norm2v(r, 3);
@@ -2646,6 +2672,106 @@ static void initALFVEN(const Model& M, Grid& G, State& S, const double* pr) {
     VectorPot2Flux(G, S, VectorPot_ALF, &a);
 }
 
+// ---------------------------------------------------------------- the magnetosphere problem's set-up
+// (voltron/ICs/earthcmi.F90 initUser with apps/msphutils.F90 genCutDipole, background.F90 AddGrav)
+struct VPInitCtx { double M0, x0, Aq, Bq, sInner; };
+static void VP_Init(double x, double y, double z, double* A, void* c) {   // msphutils.F90:503-532
+    VPInitCtx* v = (VPInitCtx*)c;
+    double r[3] = {x, y, z}, nr = norm2v(r, 3), rhat[3] = {x / nr, y / nr, z / nr};
+    double m[3] = {0.0, 0.0, 1.0}, cr[3];
+    cross3(m, rhat, cr);
+    double rr = dot(r, r, 3);
+    for (int c2 = 0; c2 < 3; ++c2) A[c2] = v->M0 * cr[c2] / rr;   // VP_Dipole
+    double s = std::sqrt(sq((x + v->x0) / v->Aq) + (sq(y) + sq(z)) / sq(v->Bq));
+    double M = PenticRampDown(s, v->sInner, 1.0 - v->sInner);
+    A[0] = M * A[0]; A[1] = M * A[1]; A[2] = M * A[2];
+}
+struct PhiCtx { double GM0; };
+static double PhiGrav(double x, double y, double z, double GM0) {   // msphutils.F90:626-633
+    double rad = std::sqrt(sq(x) + sq(y) + sq(z));
+    return -GM0 / rad;
+}
+// AddGrav (background.F90:170-252) with the spherical gravity of the magnetosphere (doSphGrav)
+static void AddGrav(const Model& M, Grid& G) {
+    int lo[4] = {G.isg, G.jsg, G.ksg, 1}, hi[4] = {G.ieg, G.jeg, G.keg, 3};
+    G.gxyz.alloc(4, lo, hi);
+#pragma omp parallel for collapse(2) schedule(static)
+    for (int k = G.ks; k <= G.ke; ++k)
+        for (int j = G.js; j <= G.je; ++j)
+            for (int i = G.is; i <= G.ie; ++i) {
+                double dV = G.volume(i, j, k);
+                const int fi[6] = {i, i, i, i + 1, i, i}, fj[6] = {j, j, j, j, j + 1, j}, fk[6] = {k, k, k, k, k, k + 1};
+                const int fd[6] = {IDIR, JDIR, KDIR, IDIR, JDIR, KDIR};
+                double Phi[6], da[6], n[6][3];
+                for (int f = 0; f < 6; ++f) {
+                    Phi[f] = PhiGrav(G.xfc(fi[f], fj[f], fk[f], 1, fd[f]), G.xfc(fi[f], fj[f], fk[f], 2, fd[f]),
+                                     G.xfc(fi[f], fj[f], fk[f], 3, fd[f]), M.W.GM0);
+                    da[f] = G.face(fi[f], fj[f], fk[f], fd[f]);
+                    for (int c = 0; c < 3; ++c) n[f][c] = G.Tf(fi[f], fj[f], fk[f], NORMX + c, fd[f]);
+                }
+                // g = -(PhiIp daIp nIp - PhiI daI nI + PhiJp daJp nJp - PhiJ daJ nJ + PhiKp daKp nKp - PhiK daK nK)/dV
+                double g[3], rhat[3], xc[3] = {G.xyzcc(i, j, k, 1), G.xyzcc(i, j, k, 2), G.xyzcc(i, j, k, 3)};
+                for (int c = 0; c < 3; ++c)
+                    g[c] = -(Phi[3] * da[3] * n[3][c] - Phi[0] * da[0] * n[0][c] + Phi[4] * da[4] * n[4][c] -
+                             Phi[1] * da[1] * n[1][c] + Phi[5] * da[5] * n[5][c] - Phi[2] * da[2] * n[2][c]) / dV;
+                normVec3(xc, rhat);
+                double gp[3];
+                Vec2Para(g, rhat, gp);
+                for (int c = 0; c < 3; ++c) G.gxyz(i, j, k, c + 1) = gp[c];
+            }
+}
+struct GasConstCtx { double D, P; };
+static void GasIC_Const(double, double, double, double* W, void* c) {   // earthcmi.F90:183-200 GasIC
+    GasConstCtx* g = (GasConstCtx*)c;
+    W[0] = g->D; W[1] = 0.0; W[2] = 0.0; W[3] = 0.0; W[4] = g->P;
+}
+// initUser's field and gas (earthcmi.F90:86-132): the cut dipole as background (genCutDipole, msphutils.F90:
+// 419-498: AddB0, dpB0 zeroed inside rCut, the initial residual field = flux of the elliptically cut dipole's
+// vector potential minus the background's face flux), uniform gas at rest, gravity
+static void initMagsphere(Model& M, Grid& G, State& S, double Rho0, double P0) {
+    B0ctx bc;
+    bc.type = 3; bc.bx = bc.by = bc.bz = 0.0; bc.M0 = M.W.M0;
+    bc.rCut = M.W.rCut; bc.lCut = M.W.lCut; bc.dcScl = M.W.dcScl;
+    M.doBackground = true;
+    AddB0(M, G, &bc);
+#pragma omp parallel for collapse(2) schedule(static)
+    for (int k = G.ks; k <= G.ke; ++k)
+        for (int j = G.js; j <= G.je; ++j)
+            for (int i = G.is; i <= G.ie; ++i) {
+                double xyzC[8][3], rMin = 0.0;
+                cellCoords(G, i, j, k, xyzC);
+                for (int p = 0; p < 8; ++p) {
+                    double r = norm2v(xyzC[p], 3);
+                    rMin = (p == 0 || r < rMin) ? r : rMin;
+                }
+                if (rMin + TINY < M.W.rCut)
+                    for (int c = 1; c <= 3; ++c) G.dpB0(i, j, k, c) = 0.0;
+            }
+    // VectorField2Flux (gridutils.F90:240-278) of the cut dipole: the background's face fluxes, cells isg..ieg
+    Arr bF0 = S.magFlux;
+#pragma omp parallel for collapse(2) schedule(static)
+    for (int k = G.ksg; k <= G.keg; ++k)
+        for (int j = G.jsg; j <= G.jeg; ++j)
+            for (int i = G.isg; i <= G.ieg; ++i)
+                for (int d = 1; d <= 3; ++d) {
+                    double f0[3], f1[3], f2[3], f3[3], flx, Mbb[3];
+                    faceCoords(G, i, j, k, d, f0, f1, f2, f3);
+                    GaussianFaceFluxStress(f0, f1, f2, f3, B0fun, &bc, &flx, Mbb);
+                    S.magFlux(i, j, k, d) = flx;
+                }
+    bF0.d = S.magFlux.d;
+    VPInitCtx v;
+    v.M0 = M.W.M0; v.Aq = 0.5 * (M.W.xSun - M.W.xTail); v.x0 = v.Aq - M.W.xSun; v.Bq = M.W.yMax;
+    v.sInner = M.W.sInner;
+    VectorPot2Flux(G, S, VP_Init, &v);
+    for (size_t q = 0; q < S.magFlux.d.size(); ++q) S.magFlux.d[q] = S.magFlux.d[q] - bF0.d[q];
+    GasConstCtx gc = {Rho0, P0};
+    GasIC2State(M, G, S, GasIC_Const, &gc);
+    M.doGrav = true;
+    M.doSphGrav = true;
+    AddGrav(M, G);
+}
+
 }  // namespace orc
 
 // =========================================================================================== C ABI
@@ -2684,6 +2810,10 @@ struct orc_params {
     // 1: no set-up -- allocate the grid, State and Solver only; the caller sets the metrics, State, oState and
     // the scalars (orc_set, orc_set_scalars) before stepping. Used to step a slab of a grid built elsewhere.
     int noSetup;
+    // icType 8, the magnetosphere (voltron/ICs/earthcmi.F90 initUser) with a constant solar wind, in code units:
+    // {M0, GM0, rCut, lCut, dcScl, xSun, xTail, yMax, sInner, windD, windP, windVx, windVy, windVz, windBx,
+    //  windBy, windBz, dtCpl, gT0, Rho0, P0, nIonP, doIonPush}; bc {BC_ION, BC_WIND, lfm, lfm, periodic x2}
+    double msph[24];
     const double* xyzIn;    // corners (Ni+1,Nj+1,Nk+1,3), Fortran layout, replacing the generated ones (a tile)
 };
 
@@ -2756,13 +2886,24 @@ void* orc_create(const orc_params* p) {
         else if (p->icType == 5) initADV2D(M, G, A->S, p->prob);
         else if (p->icType == 6) initLoop2D(M, G, A->S, p->prob);
         else if (p->icType == 7) initALFVEN(M, G, A->S, p->prob);
+        else if (p->icType == 8) {
+            const double* w = p->msph;
+            Model::Msph& W = M.W;
+            W.on = true;
+            W.M0 = w[0]; W.GM0 = w[1]; W.rCut = w[2]; W.lCut = w[3]; W.dcScl = w[4];
+            W.xSun = w[5]; W.xTail = w[6]; W.yMax = w[7]; W.sInner = w[8];
+            W.wD = w[9]; W.wP = w[10];
+            for (int c = 0; c < 3; ++c) { W.wV[c] = w[11 + c]; W.wB[c] = w[14 + c]; }
+            W.dtCpl = w[17]; W.gT0 = w[18]; W.nIonP = (int)w[21]; W.doIonPush = w[22] != 0.0;
+            initMagsphere(M, G, A->S, w[19], w[20]);
+        }
         else if (p->icType == 2) {
             M.predFixLFM = true;
             M.bwD0 = p->bw[5]; M.bwP0 = p->bw[3];
             initLFMBW(M, G, A->S, p->bw);
         }
         else initBW(M, G, A->S, p->b0Type == 1);
-        if (p->b0Type != 0) {   // CalcGridInfo: AddB0 after the IC (init.F90:180-184)
+        if (p->b0Type != 0 && p->icType != 8) {   // CalcGridInfo: AddB0 after the IC (init.F90:180-184)
             M.doBackground = true;
             B0ctx bc;
             bc.type = p->b0Type; bc.bx = p->b0[0]; bc.by = p->b0[1]; bc.bz = p->b0[2]; bc.M0 = p->b0[3];

@@ -17,9 +17,9 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "_build", "libgamora.so")
 
-IC_OT2D, IC_BW, IC_LFMBW, IC_KH, IC_ADV1D, IC_ADV2D, IC_LOOP2D, IC_ALFVEN = range(8)
+IC_OT2D, IC_BW, IC_LFMBW, IC_KH, IC_ADV1D, IC_ADV2D, IC_LOOP2D, IC_ALFVEN, IC_MAGSPHERE = range(9)
 GRID_UNIFORM, GRID_WARP, GRID_LFM = 0, 1, 2
-BC_PERIODIC, BC_ZEROGRAD, BC_LFMPOLE, BC_LFMBW, BC_HALO = 0, 1, 2, 3, 4
+BC_PERIODIC, BC_ZEROGRAD, BC_LFMPOLE, BC_LFMBW, BC_HALO, BC_ION, BC_WIND = range(7)
 # the reference's LFM blast-wave deck (tests/gamera/lfmbw.xml): prob x0, y0, z0, P0, pRat, D0, rC, B0
 LFMBW_DECK = (-50.0, 30.0, 0.0, 0.1, 10.0, 1.0, 20.0, 1.0)
 RM_8CENT, RM_7UP = 0, 1
@@ -38,7 +38,7 @@ class OrcParams(C.Structure):
         ("lfm", C.c_double * 4), ("dFloor", C.c_double), ("pFloor", C.c_double),
         ("doRing", C.c_int), ("ringNumR", C.c_int), ("ringNch", C.c_int * 32), ("ringRecon", C.c_int),
         ("dtActive", C.c_int), ("bw", C.c_double * 8), ("kh", C.c_double * 4), ("prob", C.c_double * 10),
-        ("noSetup", C.c_int), ("xyzIn", C.POINTER(C.c_double)),
+        ("noSetup", C.c_int), ("msph", C.c_double * 24), ("xyzIn", C.POINTER(C.c_double)),
     ]
 
 
@@ -113,11 +113,14 @@ class Oracle:
                  gamma=5.0 / 3.0, pdmb=0.75, Vd0=0.5, cHogH=0.25, cHogM=0.25, Ca=1.0e12, tFin=1.0e30,
                  doMHD=True, doBoris=False, rmeth="8CENT", doLFMLim=True, bc=None, threads=0, b0=None,
                  lfm=None, dFloor=0.0, pFloor=0.0, ring=None, dtActive=False, bw=LFMBW_DECK,
-                 kh=(0.03, 0.1, 0.01, 0), prob=None, xyz=None, no_setup=False):
+                 kh=(0.03, 0.1, 0.01, 0), prob=None, xyz=None, no_setup=False, msph=None):
         p = OrcParams()
         p.Nip, p.Njp, p.Nkp = Nip, Njp, Nkp
         p.icType = {"OT2D": IC_OT2D, "BW": IC_BW, "LFMBW": IC_LFMBW, "KH": IC_KH, "ADV1D": IC_ADV1D,
-                    "ADV2D": IC_ADV2D, "LOOP2D": IC_LOOP2D, "ALFVEN": IC_ALFVEN}[ic]
+                    "ADV2D": IC_ADV2D, "LOOP2D": IC_LOOP2D, "ALFVEN": IC_ALFVEN, "MAGSPHERE": IC_MAGSPHERE}[ic]
+        if msph is not None:   # the magnetosphere's 23 code-unit parameters (GAM_IC_MAGSPHERE order)
+            for n, v in enumerate(msph):
+                p.msph[n] = v
         if prob is not None:   # the problem's deck values (see CASE_DECKS)
             for n, v in enumerate(prob):
                 p.prob[n] = v

@@ -58,6 +58,16 @@ def problem(kind, n=(32, 32, 4), **kw):
         okw = dict(ic="LFMBW", grid="lfm", lfm=(10.0, 100.0, 1.03, 0.05), CFL=0.3, pdmb=1.0, rmeth="7UP",
                    dFloor=1e-4, pFloor=1e-6, doBoris=True, Ca=10.0, bc=[3, 3, 2, 2, 0, 0],
                    ring=dict(NumR=4, Nch=[8, 16, 32, 32]), dtActive=True)
+    elif kind == "msph":
+        # the magnetosphere of the Earth deck with a constant solar wind (kaiju_b200/magnetosphere.py)
+        from kaiju_b200 import magnetosphere as ms
+        model = ms.magnetosphere_model(Nip, Njp, Nkp, tFin=kw.pop("tFin", 1.0e30))
+        okw = dict(ic="MAGSPHERE", grid="lfm", lfm=ms.GRID, CFL=model.cfl(), pdmb=model.pdmb, rmeth="7UP",
+                   dFloor=model.dFloor, pFloor=model.pFloor, doBoris=True, Ca=model.Ca, bc=[5, 6, 2, 2, 0, 0],
+                   ring=dict(NumR=0, Nch=[]), dtActive=True, msph=tuple(ms.Magnetosphere().code_params()),
+                   tFin=model.tFin)
+        okw.update(kw)
+        return okw, model
     else:
         raise ValueError(kind)
     okw.update(kw)
