@@ -1,7 +1,8 @@
-"""Long runs of the spherical configuration on the device: the LFM-type grid with ring averaging about the
-axis, the axis boundaries, Boris and a dipole background (the magnetosphere-like set-up; its solar-wind
-and ionosphere boundaries are not built, so the reference's LFM blast wave supplies the flow), run with
-the plain FP64 path and the FP32-flux path side by side.
+"""Long runs on the device. The spherical configuration: `magnetosphere` runs the Earth deck's Gamera part
+(ionospheric inner and solar-wind outer boundaries, cut dipole, gravity) on the LFM-type grid; `spherical`
+runs the reference's LFM blast-wave deck on the same kind of grid with ring averaging about the axis, the
+axis boundaries, Boris and a dipole background. Both run the plain FP64 path and the FP32-flux path side by
+side. The learned closure's step cost, the Kelvin-Helmholtz ensemble and k-tiling have their own runs.
 
     python -m kaiju_b200.runs spherical --n 96 96 128 --steps 2000
     python -m kaiju_b200.runs magnetosphere --n 96 96 128 --steps 2000   # the Earth deck with a solar wind
@@ -18,6 +19,23 @@ import json
 import numpy as np
 
 from . import gamera as gm
+
+
+def _fp32_to_t_end(g32, t_end, steps, cells, fresh):
+    """The FP32-flux path to the FP64 run's end time: g32 (created with tFin = t_end) takes single steps until
+    its time reaches t_end, which counts the steps it needs (CalcDT's tFin clamp lands the last one on t_end;
+    steps after it would advance by TINY). A second problem from `fresh()` times `steps` graph steps."""
+    done, rc = 0, 0
+    while g32.status()["t"] < t_end * (1.0 - 1e-14) and done < 4 * steps:
+        g32.step()
+        done += 1
+    g = fresh()
+    g.set_precision(gm.GAM_FP32FLUX)
+    ms32, rc = g.run_steps_timed(steps)
+    g.close()
+    st = g32.status()
+    return {"ms_per_step": ms32 / steps, "zone_updates_per_s": cells * steps / (ms32 / 1e3),
+            "steps_to_t_end": done, "t": st["t"], "status": rc}
 
 
 def spherical_model(Nip: int, Njp: int, Nkp: int) -> gm.Model:
@@ -46,16 +64,8 @@ def spherical(n=(96, 96, 128), steps=2000, dipole=2000.0, grid=(10.0, 100.0, 1.0
     m32 = dataclasses.replace(model, tFin=t_end)
     g32 = gm.GameraGPU.from_corners(m32, xyz, "LFMBW", b0=("dipole", dipole))
     g32.set_precision(gm.GAM_FP32FLUX)
-    ms32, done = 0.0, 0
-    while g32.status()["t"] < t_end * (1.0 - 1e-14):
-        chunk = 100
-        m, rc32 = g32.run_steps_timed(chunk)
-        ms32 += m
-        done += chunk
-    # the last chunk may have stepped past the clamp at dt = tFin - t (TINY steps); count only real steps
-    st32 = g32.status()
-    out["fp32flux"] = {"ms_per_step": ms32 / done, "zone_updates_per_s": cells * done / (ms32 / 1e3),
-                       "steps_to_t_end": int(st32["ts"]), "t": st32["t"], "status": rc32}
+    out["fp32flux"] = _fp32_to_t_end(g32, t_end, steps, cells,
+                                     lambda: gm.GameraGPU.from_corners(m32, xyz, "LFMBW", b0=("dipole", dipole)))
     a, b = g64.fetch("gas")[4:-4, 4:-4, 4:-4], g32.fetch("gas")[4:-4, 4:-4, 4:-4]
     l1 = [float(np.mean(np.abs(a[..., v] - b[..., v])) / np.mean(np.abs(a[..., v]))) for v in range(5)]
     out["fp32flux"]["l1_rel_vs_fp64_per_var"] = l1
@@ -84,14 +94,7 @@ def magnetosphere(n=(96, 96, 128), steps: int = 2000):
                    "t_end_code": t_end, "t_end_s": t_end * ms.Magnetosphere().gT0}
     g32 = ms.magnetosphere_problem(n, tFin=t_end)
     g32.set_precision(gm.GAM_FP32FLUX)
-    ms32, done, rc32 = 0.0, 0, 0
-    while g32.status()["t"] < t_end * (1.0 - 1e-14) and done < 4 * steps:
-        m, rc32 = g32.run_steps_timed(100)
-        ms32 += m
-        done += 100
-    st32 = g32.status()
-    out["fp32flux"] = {"ms_per_step": ms32 / done, "zone_updates_per_s": cells * done / (ms32 / 1e3),
-                       "steps_to_t_end": int(st32["ts"]), "t": st32["t"], "status": rc32}
+    out["fp32flux"] = _fp32_to_t_end(g32, t_end, steps, cells, lambda: ms.magnetosphere_problem(n, tFin=t_end))
     a, b = g64.fetch("gas")[4:-4, 4:-4, 4:-4], g32.fetch("gas")[4:-4, 4:-4, 4:-4]
     out["fp32flux"]["l1_rel_vs_fp64_per_var"] = [
         float(np.mean(np.abs(a[..., v] - b[..., v])) / np.mean(np.abs(a[..., v]))) for v in range(5)]

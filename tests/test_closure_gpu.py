@@ -1,7 +1,9 @@
 """The closure network's tensor-core kernels (tcgen05 implicit GEMMs) against the CPU oracle: forward
 outputs and parameter gradients on random inputs and weights. Both sides round to BF16 at the same
-points; the remaining differences are FP32 summation order and BF16 rounding of the backward's
-intermediate gradients, so the bounds are relative L2 errors of 1e-2 (forward) and 3e-2 (gradients)."""
+points; the remaining differences are FP32 summation order (which moves a value near a BF16 rounding
+boundary to the neighbouring BF16 value, 2^-8 relative in that element) and BF16 rounding of the backward's
+intermediate gradients. Measured on a B200: 3.6e-4..4.5e-4 relative L2 forward, 1.3e-3..4.6e-3 per gradient
+block; the bounds are 2e-3 (forward) and 1.5e-2 (gradients)."""
 import numpy as np
 import pytest
 
@@ -27,7 +29,7 @@ def test_forward_matches_oracle(shape):
     y = c.forward_host(x)
     ref = co.net_forward(p, x)
     rel = np.linalg.norm(y - ref) / np.linalg.norm(ref)
-    assert rel < 1e-2, rel
+    assert rel < 2e-3, rel
     c.close()
 
 
@@ -44,6 +46,6 @@ def test_gradients_match_oracle(shape):
         for n in (27 * cin * cout, cout):
             a, b = g[o:o + n], ref[o:o + n]
             rel = np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-30)
-            assert rel < 3e-2, (cin, cout, n, rel)
+            assert rel < 1.5e-2, (cin, cout, n, rel)
             o += n
     c.close()
