@@ -91,6 +91,21 @@ k_edge_tile(Lay L, Par p, const __grid_constant__ EdgeMaps maps, EdgeSrc<S> in, 
             ld(8, TL::oN2, b4t1);
             ld(9, TL::oR, bR);
         }
+        if constexpr (sizeof(S) == 8) {
+            // while the tile lands, prefetch this edge's metric values (read from HBM after the wait) into L1:
+            // the FP64 kernel otherwise stalls on their latency (measured 6-7% of the FP64 E-field phase; the
+            // FP32 kernel measured slower with it)
+            const int pi = i0 + ti, pj = j0 + tj, pk = k0 + tk;
+            if (pi < r.i0 + r.ni && pj < r.j0 + r.nj && pk < r.k0 + r.nk) {
+                const long long pc = L.at(pi, pj, pk);
+                auto pf = [](const S* a) { asm volatile("prefetch.global.L1 [%0];" :: "l"(a)); };
+#pragma unroll
+                for (int q = 0; q < 6; ++q) pf(&in.Te[ED][q][pc]);
+#pragma unroll
+                for (int q = 0; q < 4; ++q) pf(&in.Teb[ED][q][pc]);
+                pf(&in.edge[ED][pc]);
+            }
+        }
         if (!tc::mbar_wait(bar, 0u, p.stageWait)) {
             if (tid == 0) atomicOr(&sc->waitFail, 1u);
             tc::mbar_wait(bar, 0u, STAGE_DRAIN);   // let copies in flight land before the CTA's shared memory goes
