@@ -258,6 +258,14 @@ def run_ours(args, rank, world, local):
             "dominant_phase": dom, "phase_ms": {k: round(v, 4) for k, v in ph.items()},
             "step_bytes_per_zone": STEP_BYTES_PER_ZONE,
             "step_hbm_frac": round(STEP_BYTES_PER_ZONE * zones / (ms / args.steps / 1e3) / 1e9 / hbm, 4)}
+    spz = traffic_per_unit("step", args.prec)
+    if spz:
+        # measured DRAM bytes of one whole step (all its kernels) per active zone, times this run's zones
+        roof["step_traffic"] = {"bytes_per_zone": spz, "bytes_per_step": round(spz * zones),
+                                "over_compulsory": round(spz / STEP_BYTES_PER_ZONE, 2),
+                                "achieved_gbs": round(spz * zones / (ms / args.steps / 1e3) / 1e9, 1),
+                                "source": "ncu dram bytes of one step at 128^3, per active zone "
+                                          "(profiles/step_traffic_128cubed_fp64.md)"}
     clocks = clk.summary()
     g.close()
     out = {
