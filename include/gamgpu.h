@@ -349,8 +349,9 @@ int gam_gpu_halo_unpack(gam_gpu_t* h, int side, unsigned what, const void* srcDe
 /* ---- learned flux closure (no counterpart in the reference; the device analogue of its HackFlux hook,
  * src/base/types/gamtypes.F90:137-144) ----
  * A 3D convolution net over a grid's cells: 8 normalised primitives (rho, v, P, B) in, 4 layers of 3x3x3
- * kernels with 32 channels and GELU, 24 outputs = corrections to the 5 gas fluxes and the 3 magnetic-stress
- * momentum fluxes through each cell's lower I, J and K face. BF16 weights and activations, FP32
+ * kernels with 32 channels and GELU, 27 outputs = corrections to the 5 gas fluxes and the 3 magnetic-stress
+ * momentum fluxes through each cell's lower I, J and K face (outputs 0..23, direction d and flux v at d*8+v),
+ * then to the EMF on each cell's lower I, J and K edge (24..26). BF16 weights and activations, FP32
  * accumulation on the tensor cores (tcgen05); FP32 master weights and Adam moments. Parameters are
  * W[27][cout][cin] (tap = (di+1) + 3(dj+1) + 9(dk+1)) then b[cout], layer after layer. */
 typedef struct gam_closure gam_closure_t;
@@ -360,9 +361,9 @@ long long gam_closure_num_params(const gam_closure_t* c);
 int gam_closure_set_params(gam_closure_t* c, const float* p, long long n);
 int gam_closure_get_params(gam_closure_t* c, float* p, long long n);
 int gam_closure_get_grads(gam_closure_t* c, float* g, long long n);
-/* the net on host inputs (Ni,Nj,Nk,8), ghosts included, Fortran layout; out: (Nip,Njp,Nkp,24) */
+/* the net on host inputs (Ni,Nj,Nk,8), ghosts included, Fortran layout; out: (Nip,Njp,Nkp,27) */
 int gam_closure_forward_host(gam_closure_t* c, const float* in, float* out);
-/* parameter gradients (gam_closure_get_grads) of sum(out * gout) for gout (Nip,Njp,Nkp,24) */
+/* parameter gradients (gam_closure_get_grads) of sum(out * gout) for gout (Nip,Njp,Nkp,27) */
 int gam_closure_backward_host(gam_closure_t* c, const float* in, const float* gout);
 /* normalisation: net input q = (primitive q - inMean[q]) / inScale[q] for rho, vx, vy, vz, P, Bx, By, Bz;
  * the face correction of flux v (rho, 3 momenta, energy, 3 magnetic-stress momenta) is the net output times
@@ -380,6 +381,14 @@ int gam_closure_train(gam_closure_t* c, const int* slots, int n, float lr, doubl
 int gam_closure_eval(gam_closure_t* c, const int* slots, int n, double* loss, double* lossNone);
 /* rms over the active cells of a sample's residual per gas variable (rms[0..4]) and its dt (rms[5]) */
 int gam_closure_residual_rms(gam_closure_t* c, int slot, double* rms);
+/* EMF corrections (grids periodic in all three directions): the edge EMF of direction e gains net output 24+e
+ * times emfScale[e] times the edge length, before E2Flux (so div B stays at round-off); the cell loss adds,
+ * per face direction d, ((-dt curl(EMF corrections))_d - magnetic-flux residual_d) / resScaleB[d] squared over
+ * the lower faces of the active cells. emfScale all zero (the default) turns both off. */
+int gam_closure_set_norm_emf(gam_closure_t* c, const float* emfScale, const float* resScaleB);
+/* rms over the lower faces of the active cells of a sample's magnetic-flux residual (restricted fine minus plain
+ * coarse face flux), per face direction (rms[0..2]) */
+int gam_closure_residual_rms_b(gam_closure_t* c, int slot, double* rms);
 /* Face targets. After each fine step of a sample (reset = 1 on its first), add weight (that step's dt) times
  * the fine problem's interface fluxes, summed over the 2 x 2 fine sub-faces of every coarse face; the next
  * capture then also stores the face target: the accumulation over the coarse dt minus the plain coarse

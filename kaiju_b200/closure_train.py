@@ -98,9 +98,10 @@ def collect(closure: gm.Closure, n: int, seeds, per_seed: int, warm: int, gap: i
     return slots
 
 
-def set_output_norm(closure: gm.Closure, n: int, slots):
+def set_output_norm(closure: gm.Closure, n: int, slots, emf: bool = True):
     """Residual rms per gas variable over the samples, and the flux scale that turns an O(1) net output
-    into a correction of that size in one step."""
+    into a correction of that size in one step. emf: also the EMF scale from the face magnetic-flux residual
+    (an O(1) output changes a face's flux by about that residual in one step) and the loss's B terms."""
     rms = np.zeros(5)
     dts = []
     for s in slots:
@@ -114,6 +115,10 @@ def set_output_norm(closure: gm.Closure, n: int, slots):
     flux = np.concatenate([rms, rms[1:4]]) * dx / dt
     closure.set_norm(closure.in_mean, closure.in_std, flux, rms)
     closure.res_scale = rms
+    if emf:
+        rb = np.sqrt(np.mean([closure.residual_rms_b(s) ** 2 for s in slots], axis=0))
+        rb = np.maximum(rb, 1e-15)
+        closure.set_norm_emf(rb / (dt * dx), rb)
     return rms, flux
 
 
@@ -144,7 +149,8 @@ def train(closure: gm.Closure, slots, epochs: int, lr: float, seed: int = 0, log
 
 def l1_error(a: gm.GameraGPU, b: gm.GameraGPU):
     """Mean over the gas variables of the L1 difference of the active cells, relative to b's mean |value|
-    (the momenta relative to the rms momentum)."""
+    (the momenta relative to the rms momentum); the per-variable list ends with the cell magnetic field's L1
+    difference relative to b's rms field (reported, not in the mean)."""
     G = 4
     x, y = a.fetch("gas")[G:-G, G:-G, G:-G], b.fetch("gas")[G:-G, G:-G, G:-G]
     errs = []
@@ -152,7 +158,10 @@ def l1_error(a: gm.GameraGPU, b: gm.GameraGPU):
     for v in range(5):
         den = mom if v in (1, 2, 3) else np.mean(np.abs(y[..., v]))
         errs.append(float(np.mean(np.abs(x[..., v] - y[..., v])) / den))
-    return float(np.mean(errs)), errs
+    bx, by = a.fetch("bxyz")[G:-G, G:-G, G:-G], b.fetch("bxyz")[G:-G, G:-G, G:-G]
+    brms = np.sqrt(np.mean((by ** 2).sum(-1)))
+    b_err = float(np.mean(np.abs(bx - by).sum(-1)) / brms)
+    return float(np.mean(errs)), errs + [b_err]
 
 
 def _timed_advance(g: gm.GameraGPU, t_end: float):
@@ -284,10 +293,13 @@ def main(argv=None):
                     help="also evaluate this many held-out seeds against a truth run at 4n (needs (4n)^3 to fit)")
     ap.add_argument("--loss", choices=["cell", "face"], default="cell",
                     help="fit the cell residual through the divergence, or the face targets directly")
+    ap.add_argument("--no-emf", action="store_true",
+                    help="leave the EMF outputs unused (face-flux corrections only)")
     ap.add_argument("--out", default=None)
     a = ap.parse_args(argv)
     report = train_and_evaluate(a.n, _seeds(a.train_seeds), _seeds(a.eval_seeds), a.per_seed, a.epochs, a.lr,
-                                a.warm, a.gap, a.t_end, a.rollouts, three=a.three_levels, loss=a.loss)
+                                a.warm, a.gap, a.t_end, a.rollouts, three=a.three_levels, loss=a.loss,
+                                emf=not a.no_emf)
     s = json.dumps(report, indent=1)
     if a.out:
         with open(a.out, "w") as f:
@@ -296,7 +308,7 @@ def main(argv=None):
 
 
 def train_and_evaluate(n, train_seeds, eval_seeds, per_seed, epochs, lr, warm, gap, t_end, rollouts, log=print,
-                       three=0, loss="cell"):
+                       three=0, loss="cell", emf=True):
     t0 = time.perf_counter()
     closure = gm.Closure(n, n, n, seed=0)
     closure.reserve(per_seed * (len(train_seeds) + len(eval_seeds)))
@@ -305,7 +317,7 @@ def train_and_evaluate(n, train_seeds, eval_seeds, per_seed, epochs, lr, warm, g
     tr = collect(closure, n, train_seeds, per_seed, warm, gap, 0, faces=faces)
     ev = collect(closure, n, eval_seeds, per_seed, warm, gap, len(tr), set_input_norm=False, faces=faces)
     t_data = time.perf_counter() - t0
-    rms, flux = set_output_norm(closure, n, tr)
+    rms, flux = set_output_norm(closure, n, tr, emf=emf and not faces)
     face_check = None
     if faces:
         flux = set_output_norm_faces(closure, tr)
@@ -324,6 +336,7 @@ def train_and_evaluate(n, train_seeds, eval_seeds, per_seed, epochs, lr, warm, g
     return {
         "n_coarse": n, "n_fine": 2 * n, "train_seeds": list(train_seeds), "eval_seeds": list(eval_seeds),
         "samples": {"train": len(tr), "eval": len(ev)}, "epochs": epochs, "lr": lr, "loss": loss,
+        "emf": bool(emf and not faces),
         "face_target_vs_residual": face_check,
         "seconds": {"data": t_data, "train": t_train},
         "residual_rms": rms.tolist(), "flux_scale": flux.tolist(),

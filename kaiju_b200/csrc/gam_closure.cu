@@ -36,11 +36,16 @@ struct gam_closure {
     // correction of variable v = net output * fluxScale[v] * face area; loss terms / resScale[v]
     float inMean[8] = {0, 0, 0, 0, 0, 0, 0, 0}, inScale[8] = {1, 1, 1, 1, 1, 1, 1, 1};
     float fluxScale[8] = {1, 1, 1, 1, 1, 1, 1, 1}, resScale[5] = {1, 1, 1, 1, 1};
+    // EMF corrections: the EMF of an edge of direction e gains output 24+e times emfScale[e] times the edge
+    // length (all zero: no EMF corrections), and the cell loss adds the magnetic-flux residual of the faces of
+    // each direction over resScaleB[d]. Only on grids periodic in all three directions (the edge owner map
+    // below assumes it); elsewhere the EMF outputs are left unused.
+    float emfScale[3] = {0, 0, 0}, resScaleB[3] = {1, 1, 1};
     int periodic[3] = {0, 0, 0};
-    float* corr = nullptr;       // 24 face-correction planes
-    float* geom = nullptr;       // volume, face I, J, K (float planes, copied from a solver handle)
+    float* corr = nullptr;       // 24 face-correction planes (area-scaled), then 3 edge EMF-correction planes
+    float* geom = nullptr;       // volume, face I, J, K, edge I, J, K (float planes, copied from a solver handle)
     bool haveGeom = false;
-    float* wts = nullptr;        // loss weights w_v = dL/d(dU_v) * dt / V, 5 planes
+    float* wts = nullptr;        // loss weights: w_v = dL/d(dU_v) * dt / V (5 planes), u_d = dL/d(curl_d) (3)
     double* lossAcc = nullptr;   // device loss accumulators [2]
     float* lossPart = nullptr;   // per-block loss partials
     // training samples: net input (8 bf16 planes) and residual (5 float planes) per slot, and its dt
@@ -109,13 +114,17 @@ __global__ void k_gout_from_fortran(Lay L, const float* src, int nc, __nv_bfloat
 
 struct NormP {
     float inMean[8], inScale[8], fluxScale[8], resScale[5];
+    float emfScale[3], resScaleB[3];
     int per[3];
+    int emf;   // EMF corrections and the magnetic-flux loss terms on
 };
 NormP norm_of(const gam_closure* C) {
     NormP n;
     for (int q = 0; q < 8; ++q) { n.inMean[q] = C->inMean[q]; n.inScale[q] = C->inScale[q]; n.fluxScale[q] = C->fluxScale[q]; }
     for (int q = 0; q < 5; ++q) n.resScale[q] = C->resScale[q];
-    for (int d = 0; d < 3; ++d) n.per[d] = C->periodic[d];
+    for (int d = 0; d < 3; ++d) { n.per[d] = C->periodic[d]; n.emfScale[d] = C->emfScale[d]; n.resScaleB[d] = C->resScaleB[d]; }
+    n.emf = (C->emfScale[0] != 0.f || C->emfScale[1] != 0.f || C->emfScale[2] != 0.f) && C->periodic[0] &&
+            C->periodic[1] && C->periodic[2];
     return n;
 }
 
@@ -168,6 +177,32 @@ __global__ void k_closure_corr(Lay L, const float* out, NormP n, const float* ge
             corr[o + c] = zero ? 0.f : out[o + own] * n.fluxScale[v] * A;
         }
     }
+    // EMF corrections (edge-integrated, like the solver's E) on the edges of direction e: the edges of the
+    // active cells and, across the periodic boundaries, the upper boundary edges repeating the lower ones
+    const long long st[3] = {1, L.P, (long long)L.P * L.Q};
+    const int cnt[3] = {L.Nip, L.Njp, L.Nkp};
+    for (int e = 0; e < 3; ++e) {
+        const long long o = (long long)(NET_FACE_OUT + e) * L.E;
+        if (!n.emf || idx[e] > hi[e]) { corr[o + c] = 0.f; continue; }
+        long long own = c;
+        for (int d = 0; d < 3; ++d)
+            if (d != e && idx[d] == hi[d] + 1) own -= (long long)cnt[d] * st[d];
+        corr[o + c] = out[o + own] * n.emfScale[e] * geom[(long long)(4 + e) * L.E + c];
+    }
+}
+
+// the closure's EMF corrections added to the step's edge EMFs (before E2Flux), unless this step's corrected
+// update failed positivity (the plain step is then taken whole)
+__global__ void k_closure_emf(Lay L, const float* corr, Vec3P E, const Scal* sc) {
+    if (sc->closureReject) return;
+    const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    const int ni = L.Nip + 1, nj = L.Njp + 1, nk = L.Nkp + 1;
+    if (t >= (long long)ni * nj * nk) return;
+    const int idx[3] = {L.is() + (int)(t % ni), L.js() + (int)((t / ni) % nj), L.ks() + (int)(t / ((long long)ni * nj))};
+    const int hi[3] = {L.ie(), L.je(), L.ke()};
+    const long long c = L.at(idx[0], idx[1], idx[2]);
+    for (int e = 0; e < 3; ++e)
+        if (idx[e] <= hi[e]) E.v[e][c] += (double)corr[(long long)(NET_FACE_OUT + e) * L.E + c];
 }
 
 // closure positivity: the Reynolds stage of the corrected update must keep rho > 0 and P > 0 (before floors)
@@ -194,6 +229,8 @@ __global__ void k_closure_count(Scal* sc) {
 // the residual of one coarse step: the volume-weighted restriction of the fine state minus the coarse
 // state, gas variables, active coarse cells (fine cells 2x2x2 per coarse cell)
 __global__ void k_closure_residual(Lay Lc, Lay Lf, StateP fine, const double* fineVol, StateP coarse, float* res) {
+    // (planes 5..7: the magnetic-flux residual of each active cell's lower I, J, K face: the sum of the 2 x 2
+    // fine sub-face fluxes minus the coarse flux)
     const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (t >= (long long)Lc.Nip * Lc.Njp * Lc.Nkp) return;
     const int I = (int)(t % Lc.Nip), J = (int)((t / Lc.Nip) % Lc.Njp), K = (int)(t / ((long long)Lc.Nip * Lc.Njp));
@@ -208,6 +245,16 @@ __global__ void k_closure_residual(Lay Lc, Lay Lf, StateP fine, const double* fi
                 for (int v = 0; v < 5; ++v) sum[v] += fine.gas[v][cf] * V;
             }
     for (int v = 0; v < 5; ++v) res[(long long)v * Lc.E + cc] = (float)(sum[v] / vol - coarse.gas[v][cc]);
+    const int fi = Lf.is() + 2 * I, fj = Lf.js() + 2 * J, fk = Lf.ks() + 2 * K;
+    const double f0 = fine.mf[0][Lf.at(fi, fj, fk)] + fine.mf[0][Lf.at(fi, fj + 1, fk)] +
+                      fine.mf[0][Lf.at(fi, fj, fk + 1)] + fine.mf[0][Lf.at(fi, fj + 1, fk + 1)];
+    const double f1 = fine.mf[1][Lf.at(fi, fj, fk)] + fine.mf[1][Lf.at(fi + 1, fj, fk)] +
+                      fine.mf[1][Lf.at(fi, fj, fk + 1)] + fine.mf[1][Lf.at(fi + 1, fj, fk + 1)];
+    const double f2 = fine.mf[2][Lf.at(fi, fj, fk)] + fine.mf[2][Lf.at(fi + 1, fj, fk)] +
+                      fine.mf[2][Lf.at(fi, fj + 1, fk)] + fine.mf[2][Lf.at(fi + 1, fj + 1, fk)];
+    res[5LL * Lc.E + cc] = (float)(f0 - coarse.mf[0][cc]);
+    res[6LL * Lc.E + cc] = (float)(f1 - coarse.mf[1][cc]);
+    res[7LL * Lc.E + cc] = (float)(f2 - coarse.mf[2][cc]);
 }
 
 // restriction into a coarse state: gas volume-weighted, magnetic fluxes summed over the 4 fine faces of
@@ -284,6 +331,19 @@ __global__ void k_loss_w(Lay L, const float* corr, const float* res, const float
             acc += e * e;
             w[(long long)v * L.E + c] = 2.f * e / n.resScale[v] / (float)nact * f;
         }
+        if (n.emf) {   // magnetic flux of the lower faces: -dt x the curl of the EMF corrections (E2Flux's stencil)
+            const float* Ei = corr + (long long)NET_FACE_OUT * L.E;
+            const float* Ej = Ei + L.E;
+            const float* Ek = Ej + L.E;
+            const long long cj = c + L.P, ck = c + (long long)L.P * L.Q;
+            const float df[3] = {Ek[cj] - Ek[c] - Ej[ck] + Ej[c], Ei[ck] - Ei[c] - Ek[c + 1] + Ek[c],
+                                 Ej[c + 1] - Ej[c] - Ei[cj] + Ei[c]};
+            for (int d = 0; d < 3; ++d) {
+                const float e = (-(float)dt * df[d] - res[(long long)(5 + d) * L.E + c]) / n.resScaleB[d];
+                acc += e * e;
+                w[(long long)(5 + d) * L.E + c] = 2.f * e / n.resScaleB[d] / (float)nact * (-(float)dt);
+            }
+        }
     }
     red[threadIdx.x] = acc / (float)nact;
     __syncthreads();
@@ -326,6 +386,20 @@ __global__ void k_loss_grad(Lay L, const float* w, const float* geom, NormP n, _
             gout[c * NET_PITCH + d * 8 + v] = __float2bfloat16_rn(g);
         }
     }
+    // EMF outputs: the transpose of the curl (E2Flux's stencil), u_d = dL/d(curl_d) on the lower faces of the
+    // active cells, the neighbours below wrapping across the periodic boundaries
+    float ge[3] = {0.f, 0.f, 0.f};
+    if (n.emf) {
+        auto below = [&](int d) { return idx[d] == lo[d] ? c + (long long)(cnt[d] - 1) * st[d] : c - st[d]; };
+        auto u = [&](int d, long long x) { return w[(long long)(5 + d) * L.E + x]; };
+        const long long bi = below(0), bj = below(1), bk = below(2);
+        ge[0] = -u(1, c) + u(1, bk) + u(2, c) - u(2, bj);
+        ge[1] = u(0, c) - u(0, bk) + u(2, bi) - u(2, c);
+        ge[2] = u(0, bj) - u(0, c) - u(1, bi) + u(1, c);
+    }
+    for (int e = 0; e < 3; ++e)
+        gout[c * NET_PITCH + NET_FACE_OUT + e] =
+            __float2bfloat16_rn(n.emf ? n.emfScale[e] * geom[(long long)(4 + e) * L.E + c] * ge[e] : 0.f);
 }
 
 inline unsigned nblk256(long long n) { return (unsigned)((n + 255) / 256); }
@@ -418,6 +492,8 @@ __global__ void k_loss_face(Lay L, const float* out, const float* tgt, const flo
                 if (gout) gout[c * NET_PITCH + d * 8 + v] = __float2bfloat16_rn(2.f * e / N);
             }
         }
+        if (gout)   // the face targets carry no EMF; those outputs get no gradient
+            for (int e = 0; e < 3; ++e) gout[c * NET_PITCH + NET_FACE_OUT + e] = __float2bfloat16_rn(0.f);
     }
     red[threadIdx.x] = acc / N;
     __syncthreads();
@@ -478,15 +554,16 @@ __global__ void k_face_stats(Lay L, const float* tgt, const float* res, const fl
     }
 }
 
-// sums of the residual squares per gas variable over the active cells (statistics for the normalisation)
-__global__ void k_res_sq(Lay L, const float* res, double* acc) {
+// sums of the residual squares per plane (nv <= 5 planes from res) over the active cells (statistics for the
+// normalisation)
+__global__ void k_res_sq(Lay L, const float* res, int nv, double* acc) {
     __shared__ double red[5][256];
     double s[5] = {0, 0, 0, 0, 0};
     const long long nact = (long long)L.Nip * L.Njp * L.Nkp;
     for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < nact; t += (long long)gridDim.x * blockDim.x) {
         const long long c = L.at(L.is() + (int)(t % L.Nip), L.js() + (int)((t / L.Nip) % L.Njp),
                                  L.ks() + (int)(t / ((long long)L.Nip * L.Njp)));
-        for (int v = 0; v < 5; ++v) { const double r = res[(long long)v * L.E + c]; s[v] += r * r; }
+        for (int v = 0; v < nv; ++v) { const double r = res[(long long)v * L.E + c]; s[v] += r * r; }
     }
     for (int v = 0; v < 5; ++v) red[v][threadIdx.x] = s[v];
     __syncthreads();
@@ -560,13 +637,13 @@ int gam_closure_create(gam_closure_t** out, int Nip, int Njp, int Nkp, unsigned 
     C->nb.partialFloats = net_partial_floats(net_dw_blocks());
     if (cudaMalloc(&C->nb.partial, sizeof(float) * C->nb.partialFloats) != cudaSuccess) return fail(GAM_ERR_CUDA);
     C->act0 = C->nb.act[0];
-    if (cudaMalloc(&C->corr, sizeof(float) * E * NET_OUT) || cudaMalloc(&C->geom, sizeof(float) * E * 4) ||
-        cudaMalloc(&C->wts, sizeof(float) * E * 5) || cudaMalloc(&C->lossAcc, sizeof(double) * 2) ||
+    if (cudaMalloc(&C->corr, sizeof(float) * E * NET_OUT) || cudaMalloc(&C->geom, sizeof(float) * E * 7) ||
+        cudaMalloc(&C->wts, sizeof(float) * E * 8) || cudaMalloc(&C->lossAcc, sizeof(double) * 2) ||
         cudaMalloc(&C->lossPart, sizeof(float) * 2 * 4096))
         return fail(GAM_ERR_CUDA);
     cudaMemsetAsync(C->corr, 0, sizeof(float) * E * NET_OUT, C->stream);
-    cudaMemsetAsync(C->wts, 0, sizeof(float) * E * 5, C->stream);
-    cudaMemsetAsync(C->geom, 0, sizeof(float) * E * 4, C->stream);
+    cudaMemsetAsync(C->wts, 0, sizeof(float) * E * 8, C->stream);
+    cudaMemsetAsync(C->geom, 0, sizeof(float) * E * 7, C->stream);
     const long long stageFloats = (long long)L.Ni * L.Nj * L.Nk * NET_OUT;
     if (cudaMalloc(&C->stage, sizeof(float) * stageFloats) != cudaSuccess) return fail(GAM_ERR_CUDA);
     cudaMemsetAsync(C->err, 0, sizeof(int), C->stream);
@@ -684,7 +761,18 @@ void closure_enqueue_check(Handle& h, const StateP& nS, cudaStream_t st) {
     h.launches += 2;
 }
 
-int closure_kernels_per_step(const Handle& h) { return h.closure ? 2 + NET_LAYERS + 2 : 0; }
+void closure_enqueue_emf(Handle& h, cudaStream_t st) {
+    gam_closure* C = h.closure;
+    if (!norm_of(C).emf) return;
+    const Lay& L = h.L;
+    Vec3P E = {{h.E[0], h.E[1], h.E[2]}};
+    k_closure_emf<<<nblk256((long long)(L.Nip + 1) * (L.Njp + 1) * (L.Nkp + 1)), 256, 0, st>>>(L, C->corr, E, h.dScal);
+    h.launches++;
+}
+
+int closure_kernels_per_step(const Handle& h) {
+    return h.closure ? 2 + NET_LAYERS + 2 + (norm_of(h.closure).emf ? 1 : 0) : 0;
+}
 
 // shape check and geometry for a handle the closure is attached to
 int closure_attach(Handle& h, gam_closure* C) {
@@ -694,6 +782,7 @@ int closure_attach(Handle& h, gam_closure* C) {
     for (int d = 0; d < 3; ++d) C->periodic[d] = h.p.bc[2 * d] == BC_PERIODIC && h.p.bc[2 * d + 1] == BC_PERIODIC;
     k_to_float<<<nblk256(L.E), 256, 0, h.stream>>>(h.volume, C->geom, L.E);
     for (int d = 0; d < 3; ++d) k_to_float<<<nblk256(L.E), 256, 0, h.stream>>>(h.face[d], C->geom + (1 + d) * L.E, L.E);
+    for (int d = 0; d < 3; ++d) k_to_float<<<nblk256(L.E), 256, 0, h.stream>>>(h.edge[d], C->geom + (4 + d) * L.E, L.E);
     C->haveGeom = true;
     return cudaStreamSynchronize(h.stream) == cudaSuccess ? GAM_OK : GAM_ERR_CUDA;
 }
@@ -728,9 +817,9 @@ int gam_closure_reserve(gam_closure_t* C, int n) {
         __nv_bfloat16* in = nullptr;
         float* res = nullptr;
         if (cudaMalloc(&in, sizeof(__nv_bfloat16) * E * NET_IN_PITCH) != cudaSuccess) return GAM_ERR_CUDA;
-        if (cudaMalloc(&res, sizeof(float) * E * 5) != cudaSuccess) { cudaFree(in); return GAM_ERR_CUDA; }
+        if (cudaMalloc(&res, sizeof(float) * E * 8) != cudaSuccess) { cudaFree(in); return GAM_ERR_CUDA; }
         cudaMemsetAsync(in, 0, sizeof(__nv_bfloat16) * E * NET_IN_PITCH, C->stream);
-        cudaMemsetAsync(res, 0, sizeof(float) * E * 5, C->stream);
+        cudaMemsetAsync(res, 0, sizeof(float) * E * 8, C->stream);
         C->sIn.push_back(in);
         C->sRes.push_back(res);
         C->sDt.push_back(0.0);
@@ -939,7 +1028,7 @@ int gam_closure_residual_rms(gam_closure_t* C, int slot, double* rms) {
     double* acc = nullptr;
     CKC(cudaMalloc(&acc, sizeof(double) * 5));
     cudaMemsetAsync(acc, 0, sizeof(double) * 5, C->stream);
-    k_res_sq<<<256, 256, 0, C->stream>>>(C->L, C->sRes[slot], acc);
+    k_res_sq<<<256, 256, 0, C->stream>>>(C->L, C->sRes[slot], 5, acc);
     double h[5];
     cudaMemcpyAsync(h, acc, sizeof(h), cudaMemcpyDeviceToHost, C->stream);
     cudaError_t e = cudaStreamSynchronize(C->stream);
@@ -948,6 +1037,31 @@ int gam_closure_residual_rms(gam_closure_t* C, int slot, double* rms) {
     const double n = (double)C->L.Nip * C->L.Njp * C->L.Nkp;
     for (int v = 0; v < 5; ++v) rms[v] = std::sqrt(h[v] / n);
     rms[5] = C->sDt[slot];
+    return GAM_OK;
+}
+
+int gam_closure_set_norm_emf(gam_closure_t* C, const float* emfScale, const float* resScaleB) {
+    if (!C || !emfScale || !resScaleB) return GAM_ERR_ARG;
+    for (int d = 0; d < 3; ++d)
+        if (!(emfScale[d] >= 0.f) || !(resScaleB[d] > 0.f)) return GAM_ERR_ARG;
+    for (int d = 0; d < 3; ++d) { C->emfScale[d] = emfScale[d]; C->resScaleB[d] = resScaleB[d]; }
+    return GAM_OK;
+}
+
+// rms of a sample's magnetic-flux residual over the lower faces of the active cells, per face direction
+int gam_closure_residual_rms_b(gam_closure_t* C, int slot, double* rms) {
+    if (!C || !rms || slot < 0 || slot >= (int)C->sIn.size()) return GAM_ERR_ARG;
+    double* acc = nullptr;
+    CKC(cudaMalloc(&acc, sizeof(double) * 5));
+    cudaMemsetAsync(acc, 0, sizeof(double) * 5, C->stream);
+    k_res_sq<<<256, 256, 0, C->stream>>>(C->L, C->sRes[slot] + 5LL * C->L.E, 3, acc);   // planes 5..7
+    double h[5];
+    cudaMemcpyAsync(h, acc, sizeof(h), cudaMemcpyDeviceToHost, C->stream);
+    cudaError_t e = cudaStreamSynchronize(C->stream);
+    cudaFree(acc);
+    if (e != cudaSuccess) return GAM_ERR_CUDA;
+    const double n = (double)C->L.Nip * C->L.Njp * C->L.Nkp;
+    for (int d = 0; d < 3; ++d) rms[d] = std::sqrt(h[d] / n);
     return GAM_OK;
 }
 

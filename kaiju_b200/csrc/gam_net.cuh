@@ -3,9 +3,10 @@
 // (cell-major, 16 or 32 channels per cell, so the channels of one cell are one to four 16-byte chunks),
 // FP32 master weights.
 //
-//   input 8 (normalised primitives rho, v, P, B; padded to 16) -> 32 -> 32 -> 32 -> 24 (8 face-flux
+//   input 8 (normalised primitives rho, v, P, B; padded to 16) -> 32 -> 32 -> 32 -> 27 (8 face-flux
 //   corrections per direction: the 5 gas fluxes and the 3 magnetic-stress momentum fluxes of each cell's
-//   lower face), 3x3x3 kernels, GELU between layers.
+//   lower face; then one EMF correction per direction on each cell's lower I, J and K edge), 3x3x3 kernels,
+//   GELU between layers.
 //
 // Every convolution is an implicit GEMM on the tensor cores (tcgen05.mma kind::f16, BF16 x BF16 -> FP32
 // in TMEM): a CTA owns 128 consecutive cells (M = 128) and all output channels (N = 32). For each of the
@@ -23,7 +24,8 @@
 namespace gam {
 
 constexpr int NET_LAYERS = 4;
-constexpr int NET_IN = 8, NET_WIDTH = 32, NET_OUT = 24;
+constexpr int NET_IN = 8, NET_WIDTH = 32, NET_OUT = 27;
+constexpr int NET_FACE_OUT = 24;   // outputs 0..23: face fluxes (direction d, flux v at d*8+v); 24..26: edge EMFs
 
 struct NetShape {
     int cin[NET_LAYERS], cout[NET_LAYERS];

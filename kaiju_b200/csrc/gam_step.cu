@@ -919,6 +919,7 @@ int step_enqueue(Handle& h, int cur, cudaEvent_t* ev, bool split, int part) {
     // applyUpdate into the oState buffer (which becomes State n+1)
     Vec3P E = {{h.E[0], h.E[1], h.E[2]}};
     if (p.doRing && p.doMHD) launch_pole_e(h, h.E, st);   // mhdgroup.F90:139-142
+    if (h.closure && p.doMHD) closure_enqueue_emf(h, st);
     k_e2flux<<<grid_plane(Reg{0, L.Ni + 1, 0, L.Nj + 1, 0, L.Nk + 1}, TPB), TPB, 0, st>>>(L, p, E, nS, oS, h.dScal);
     // bFlux2Fld of the update; with ring averaging its ring fix is left to the RingAverage bFlux2Fld,
     // which recomputes every cell before anything reads a ghost B

@@ -116,6 +116,8 @@ int kernels_per_step(const Handle& h);
 // planes, area-scaled) before Flux2Deltas; after it the positivity check that sets Scal::closureReject
 const float* closure_enqueue_corr(Handle& h, const StateP& nS, cudaStream_t st);
 void closure_enqueue_check(Handle& h, const StateP& nS, cudaStream_t st);
+// the closure's EMF corrections added to the edge EMFs before E2Flux (skipped when the step fell back)
+void closure_enqueue_emf(Handle& h, cudaStream_t st);
 int closure_kernels_per_step(const Handle& h);
 int closure_attach(Handle& h, ::gam_closure* c);   // shape check, geometry and periodicity from h
 // interface fluxes of all directions (gam_flux.cu)

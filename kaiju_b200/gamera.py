@@ -36,6 +36,8 @@ GAM_SLICE_FAT = 1
 GAM_B0_UNIFORM, GAM_B0_DIPOLE = 1, 2
 GAM_TILE_FLUX_ROWS, GAM_TILE_FUSED_UPDATE, GAM_TILE_TMA, GAM_TILE_STAGE_WAIT = 1, 2, 3, 4
 GAM_CLOSURE_LOSS_CELL, GAM_CLOSURE_LOSS_FACE = 0, 1
+# closure network outputs per cell: 24 face-flux corrections (direction d, flux v at d*8+v), 3 edge EMF corrections
+CLOSURE_OUT = 27
 TINY, HUGE = 1.0e-12, 1.0e12
 
 
@@ -144,6 +146,8 @@ SIGNATURES = {
     "gam_closure_train": (C.c_int, [C.c_void_p, C.POINTER(C.c_int), C.c_int, C.c_float, _DP]),
     "gam_closure_eval": (C.c_int, [C.c_void_p, C.POINTER(C.c_int), C.c_int, _DP, _DP]),
     "gam_closure_residual_rms": (C.c_int, [C.c_void_p, C.c_int, _DP]),
+    "gam_closure_set_norm_emf": (C.c_int, [C.c_void_p, _FP, _FP]),
+    "gam_closure_residual_rms_b": (C.c_int, [C.c_void_p, C.c_int, _DP]),
     "gam_closure_accum_fine": (C.c_int, [C.c_void_p, C.c_void_p, C.c_double, C.c_int]),
     "gam_closure_set_loss": (C.c_int, [C.c_void_p, C.c_int]),
     "gam_closure_face_stats": (C.c_int, [C.c_void_p, C.c_int, _DP, _DP]),
@@ -737,10 +741,10 @@ class Closure:
         return g
 
     def forward_host(self, x: np.ndarray) -> np.ndarray:
-        """x: (Ni, Nj, Nk, 8) float32, ghosts included; returns (Nip, Njp, Nkp, 24)."""
+        """x: (Ni, Nj, Nk, 8) float32, ghosts included; returns (Nip, Njp, Nkp, CLOSURE_OUT)."""
         Nip, Njp, Nkp = self.shape
         x = np.asfortranarray(x, dtype=np.float32)
-        out = np.zeros((Nip, Njp, Nkp, 24), dtype=np.float32, order="F")
+        out = np.zeros((Nip, Njp, Nkp, CLOSURE_OUT), dtype=np.float32, order="F")
         self._call("gam_closure_forward_host", _fp(x), _fp(out))
         return out
 
@@ -754,6 +758,20 @@ class Closure:
         a = [np.ascontiguousarray(x, dtype=np.float32) for x in (in_mean, in_scale, flux_scale, res_scale)]
         assert [len(x) for x in a] == [8, 8, 8, 5]
         self._call("gam_closure_set_norm", *[_fp(x) for x in a])
+
+    def set_norm_emf(self, emf_scale, res_scale_b):
+        """EMF corrections: the EMF on an edge of direction e gains net output 24+e times emf_scale[e] times the
+        edge length; the cell loss adds the face magnetic-flux residual of each direction over res_scale_b.
+        emf_scale all zero (the default) leaves the EMFs and the loss as without them."""
+        a = [np.ascontiguousarray(x, dtype=np.float32) for x in (emf_scale, res_scale_b)]
+        assert [len(x) for x in a] == [3, 3]
+        self._call("gam_closure_set_norm_emf", *[_fp(x) for x in a])
+
+    def residual_rms_b(self, slot: int):
+        """rms over the lower faces of the active cells of a sample's magnetic-flux residual per direction."""
+        out = np.zeros(3)
+        self._call("gam_closure_residual_rms_b", slot, out.ctypes.data_as(_DP))
+        return out
 
     def reserve(self, n: int):
         self._call("gam_closure_reserve", n)

@@ -4,16 +4,16 @@ written with torch on the CPU in FP32, with the device's BF16 roundings reproduc
 the hidden pre-activations and the GELU outputs are rounded to BF16, the output layer stays FP32.
 
 Parameter layout (the device's): for each layer, W[27][cout][cin] with tap t = (di+1) + 3(dj+1) + 9(dk+1)
-applied as out(i,j,k) += W[t] . in(i+di, j+dj, k+dk), then b[cout]. Layers 8 -> 32 -> 32 -> 32 -> 24,
+applied as out(i,j,k) += W[t] . in(i+di, j+dj, k+dk), then b[cout]. Layers 8 -> 32 -> 32 -> 32 -> 27,
 GELU (the erf form) after the first three. Arrays use the solver's Fortran layout: inputs (Ni,Nj,Nk,8)
-with 4 ghost layers, outputs (Nip,Njp,Nkp,24) on the active cells (each layer is a "valid" 3x3x3
+with 4 ghost layers, outputs (Nip,Njp,Nkp,27) on the active cells (each layer is a "valid" 3x3x3
 convolution, so 4 layers consume exactly the 4 ghost layers).
 """
 from __future__ import annotations
 
 import numpy as np
 
-LAYERS = ((8, 32), (32, 32), (32, 32), (32, 24))
+LAYERS = ((8, 32), (32, 32), (32, 32), (32, 27))
 
 
 def unpack(params: np.ndarray):

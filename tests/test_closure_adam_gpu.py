@@ -5,7 +5,8 @@ transpose of the divergence, k_loss_grad) against autograd of the same loss writ
 The sample is a real capture (a 16^3 coarse turbulence problem and its 32^3 fine run). The loss-gradient test
 feeds autograd's dL/d(output) through the device's own backward (gam_closure_backward_host), so the two
 parameter gradients differ only where the output gradient differs; the output gradient is rounded to BF16 on
-both routes, which bounds the agreement at about 1e-2 relative L2."""
+both routes, which bounds the agreement at about 1e-2 relative L2. It runs with and without the EMF outputs
+(the face magnetic-flux residual through the curl of the EMF corrections)."""
 import numpy as np
 import pytest
 
@@ -13,9 +14,10 @@ pytestmark = pytest.mark.gpu
 G = 4
 
 
-def _captured_sample(n=16, seed=7):
+def _captured_sample(n=16, seed=7, emf=False):
     """A closure with one captured sample, the net input of that sample (host float, the device's
-    normalisation), and the host restriction residual."""
+    normalisation), the host restriction residuals (gas, and with emf the face magnetic fluxes), the sample's
+    dt and the flux and EMF scales."""
     from kaiju_b200 import gamera as gm, turbulence as tu, closure_train as ct
     c = gm.Closure(n, n, n, seed=0)
     c.set_params(c.params() * 4.0)
@@ -30,6 +32,9 @@ def _captured_sample(n=16, seed=7):
     c.in_mean, c.in_std = ct.primitive_stats(coarse)
     flux_scale = np.full(8, 2e-3)
     c.set_norm(c.in_mean, c.in_std, flux_scale, np.full(5, 1e-3))
+    emf_scale = np.array([3e-3, 2e-3, 4e-3]) if emf else np.zeros(3)
+    if emf:
+        c.set_norm_emf(emf_scale, np.full(3, 1e-4))
     fine.step(); fine.step()
     tc = fine.status()["time"]
     coarse.set_scalars(tb, tc - tb, 0.0, 1, tb, ta)
@@ -45,13 +50,23 @@ def _captured_sample(n=16, seed=7):
     x = ((w - mean) / std).astype(np.float32)
     fg = fine.fetch("gas")[G:-G, G:-G, G:-G]
     res = fg.reshape(n, 2, n, 2, n, 2, 5).mean(axis=(1, 3, 5)) - coarse.fetch("gas")[G:-G, G:-G, G:-G]
+    # magnetic flux of each active coarse cell's lower faces: the 2 x 2 fine sub-faces minus the coarse flux
+    fm, cm = fine.fetch("magflux"), coarse.fetch("magflux")
+    s = slice(G, G + 2 * n, 2)
+    f0 = fm[s, s, s, 0] + fm[s, G + 1:G + 2 * n:2, s, 0] + fm[s, s, G + 1:G + 2 * n:2, 0] + \
+        fm[s, G + 1:G + 2 * n:2, G + 1:G + 2 * n:2, 0]
+    f1 = fm[s, s, s, 1] + fm[G + 1:G + 2 * n:2, s, s, 1] + fm[s, s, G + 1:G + 2 * n:2, 1] + \
+        fm[G + 1:G + 2 * n:2, s, G + 1:G + 2 * n:2, 1]
+    f2 = fm[s, s, s, 2] + fm[G + 1:G + 2 * n:2, s, s, 2] + fm[s, G + 1:G + 2 * n:2, s, 2] + \
+        fm[G + 1:G + 2 * n:2, G + 1:G + 2 * n:2, s, 2]
+    resb = np.stack([f0, f1, f2], axis=-1) - cm[G:G + n, G:G + n, G:G + n, :]
     fine.close(); coarse.close()
-    return c, x, res.astype(np.float32), tc - tb, flux_scale
+    return c, x, res.astype(np.float32), resb.astype(np.float32), tc - tb, flux_scale, emf_scale
 
 
 def test_adam_matches_torch():
     torch = pytest.importorskip("torch")
-    c, x, res, dt, fs = _captured_sample()
+    c, x, res, resb, dt, fs, es = _captured_sample()
     p0 = c.params().astype(np.float32)
     lr = 1e-3
     t = torch.tensor(p0, dtype=torch.float32, requires_grad=True)
@@ -70,13 +85,16 @@ def test_adam_matches_torch():
     c.close()
 
 
-def test_cell_loss_gradient_matches_autograd():
+@pytest.mark.parametrize("emf", [False, True])
+def test_cell_loss_gradient_matches_autograd(emf):
+    """With emf the net's EMF outputs correct the edge EMFs and the loss adds the face magnetic-flux residual
+    through the curl (E2Flux's stencil) on the periodic grid."""
     torch = pytest.importorskip("torch")
-    c, x, res, dt, fs = _captured_sample()
+    c, x, res, resb, dt, fs, es = _captured_sample(emf=emf)
     n = res.shape[0]
     p0 = c.params()
-    out = torch.tensor(c.forward_host(x), dtype=torch.float32, requires_grad=True)   # (n, n, n, 24)
-    # uniform periodic unit cube: face area h^2, volume h^3
+    out = torch.tensor(c.forward_host(x), dtype=torch.float32, requires_grad=True)   # (n, n, n, 27)
+    # uniform periodic unit cube: face area h^2, volume h^3, edge length h
     h = 1.0 / n
     A, V = h * h, h * h * h
     fsT = torch.tensor(fs, dtype=torch.float32)
@@ -92,12 +110,20 @@ def test_cell_loss_gradient_matches_autograd():
     for v in range(5):
         e = (float(dt) / V * dU[v] - r[..., v]) / 1e-3
         loss = loss + (e * e).mean()
+    if emf:
+        Ei, Ej, Ek = (out[..., 24 + q] * float(es[q]) * h for q in range(3))
+        up = lambda a, d: torch.roll(a, shifts=-1, dims=d)
+        df = [up(Ek, 1) - Ek - up(Ej, 2) + Ej, up(Ei, 2) - Ei - up(Ek, 0) + Ek, up(Ej, 0) - Ej - up(Ei, 1) + Ei]
+        rb = torch.tensor(resb)
+        for d in range(3):
+            e = (-float(dt) * df[d] - rb[..., d]) / 1e-4
+            loss = loss + (e * e).mean()
     loss.backward()
     gout = out.grad.numpy().copy()
     # the device's training pass: its loss and its parameter gradient at p0
     dev_loss = c.train([0], 1e-6)
     g_train = c.grads().copy()
-    assert dev_loss == pytest.approx(float(loss), rel=1e-3)
+    assert dev_loss == pytest.approx(float(loss.detach()), rel=1e-3)
     c.set_params(p0)
     g_auto = c.backward_host(x, gout)
     rel = np.linalg.norm(g_train - g_auto) / np.linalg.norm(g_auto)

@@ -35,10 +35,11 @@ def test_forward_matches_oracle(shape):
 
 @pytest.mark.parametrize("shape", [(16, 8, 8), (32, 16, 12)])
 def test_gradients_match_oracle(shape):
+    from kaiju_b200 import gamera as gm
     from oracle import closure_oracle as co
     c, p, x = _rand_case(shape, 5)
     rng = np.random.default_rng(7)
-    gout = rng.normal(size=shape + (24,)).astype(np.float32)
+    gout = rng.normal(size=shape + (gm.CLOSURE_OUT,)).astype(np.float32)
     g = c.backward_host(x, gout)
     ref = co.net_grads(p, x, gout)
     o = 0

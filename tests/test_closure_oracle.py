@@ -26,9 +26,10 @@ def test_oracle_shapes_and_gradient():
     p = (rng.normal(size=n) * 0.1).astype(np.float32)
     x = rng.normal(size=(10, 9, 9, 8)).astype(np.float32)
     y = co.net_forward(p, x)
-    assert y.shape == (2, 1, 1, 24)
+    nout = co.LAYERS[-1][1]
+    assert nout == 27 and y.shape == (2, 1, 1, nout)
     g = rng.normal(size=y.shape).astype(np.float32)
     grads = co.net_grads(p, x, g)
     assert grads.shape == (n,)
     # the bias of the output layer enters every output once: its gradient is the sum of gout
-    assert np.allclose(grads[-24:], g.reshape(-1, 24).sum(axis=0), rtol=1e-5, atol=1e-5)
+    assert np.allclose(grads[-nout:], g.reshape(-1, nout).sum(axis=0), rtol=1e-5, atol=1e-5)

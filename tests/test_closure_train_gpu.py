@@ -64,6 +64,30 @@ def test_closure_step_conserves_mass_momentum_and_divb():
     g.close(); h.close(); c.close()
 
 
+def test_emf_corrections_keep_divb_and_change_the_field():
+    """The EMF outputs enter through E2Flux: the magnetic field changes against the step without them and
+    div B stays at round-off; the gas update (mass and momentum totals) stays conservative."""
+    from kaiju_b200 import turbulence as tu
+    g = tu.turbulence_problem(32, seed=5)
+    h = tu.turbulence_problem(32, seed=5)
+    c = _closure_for(32)
+    d = _closure_for(32)
+    c.set_norm_emf(np.full(3, 1e-3), np.ones(3))
+    g.set_closure(c)
+    h.set_closure(d)
+    t0 = _totals(g)
+    g.run_steps(4)
+    h.run_steps(4)
+    t1 = _totals(g)
+    assert g.closure_rejects() == 0
+    assert abs(g.divb()) < 1e-12
+    assert abs(t1[0] - t0[0]) <= 1e-13 * abs(t0[0])
+    dmf = np.abs(g.fetch("magflux") - h.fetch("magflux")).max()
+    assert dmf > 1e-9 * np.abs(h.fetch("magflux")).max(), dmf
+    g.set_closure(None); h.set_closure(None)
+    g.close(); h.close(); c.close(); d.close()
+
+
 def test_rejected_correction_is_the_plain_step():
     from kaiju_b200 import turbulence as tu
     g = tu.turbulence_problem(32, seed=6)
@@ -71,6 +95,7 @@ def test_rejected_correction_is_the_plain_step():
     c = _closure_for(32)
     c.set_norm(np.array([1, 0, 0, 0, 0.6, 0, 0, 0.3]), np.array([0.1, 0.3, 0.3, 0.3, 0.1, 0.1, 0.1, 0.1]),
                np.full(8, 1e6), np.ones(5))   # corrections far too large: every step fails positivity
+    c.set_norm_emf(np.full(3, 1e6), np.ones(3))   # the EMF corrections are dropped with the rest
     g.set_closure(c)
     g.run_steps(2)
     h.run_steps(2)
