@@ -58,9 +58,11 @@ __device__ __forceinline__ int bidx(BoxC b, int di, int dj, int dk) {
     return (di - b.oi) + b.ni * ((dj - b.oj) + b.nj * (dk - b.ok));
 }
 
-// TMA: the footprint arrives by tensor copies issued by one thread; otherwise by cp.async row copies
+// TMA: the footprint arrives by tensor copies issued by one thread; otherwise by cp.async row copies. The
+// FP64 I-edge tile's 59 KB footprint allows three CTAs per SM whatever their registers, so that kernel gets the
+// 80 registers three CTAs leave (it spills at 64); the J and K edges keep four CTAs at 64.
 template <typename T, typename S, int ED, bool TMA>
-__global__ void __launch_bounds__(256, sizeof(S) == 4 ? 6 : 4)
+__global__ void __launch_bounds__(256, sizeof(S) == 4 ? 6 : (ED == 0 && TMA ? 3 : 4))
 k_edge_tile(Lay L, Par p, const __grid_constant__ EdgeMaps maps, EdgeSrc<S> in, double* Eout, Reg r, Scal* sc) {
     using TL = ETile<ED, TMA>;
     constexpr int dT1 = TL::dT1, dT2 = TL::dT2;
