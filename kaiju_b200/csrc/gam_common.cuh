@@ -160,32 +160,40 @@ __device__ __forceinline__ void blockC2P(const Par& p, const double* Con, double
     W[0] = D; W[1] = Con[1] * iD; W[2] = Con[2] * iD; W[3] = Con[3] * iD; W[4] = P;
 }
 
+// The limiter's max and min: a > b ? a : b and a < b ? a : b. In single precision fmaxf/fminf, one instruction
+// each and the same value for every non-NaN input (the FP32 flux kernel measured 1-3% faster); in double
+// precision the comparisons measured faster than fmax/fmin.
+template <typename T> __device__ __forceinline__ T lmax(T a, T b) { return a > b ? a : b; }
+template <typename T> __device__ __forceinline__ T lmin(T a, T b) { return a < b ? a : b; }
+template <> __device__ __forceinline__ float lmax<float>(float a, float b) { return fmaxf(a, b); }
+template <> __device__ __forceinline__ float lmin<float>(float a, float b) { return fminf(a, b); }
+
 // pdmLR (recon.F90:231-272) on one interface
 template <typename T>
 __device__ __forceinline__ void pdmLR(T pdmb, T v0, T v1, T v2, T v3, T Qi, T& Ql, T& Qr) {
-    T maxV = v1 > v2 ? v1 : v2, minV = v1 < v2 ? v1 : v2;
-    T c = Qi < maxV ? Qi : maxV;
-    T vN = minV > c ? minV : c;
+    T maxV = lmax(v1, v2), minV = lmin(v1, v2);
+    T c = lmin(Qi, maxV);
+    T vN = lmax(minV, c);
     T dv0 = pdmb * (v1 - v0), dv1 = pdmb * (v2 - v1), dv2 = pdmb * (v3 - v2);
     T s0 = copysign(T(1), dv0), s1 = copysign(T(1), dv1), s2 = copysign(T(1), dv2);
     T q0 = fabs(s0 + s1), q1 = fabs(s1 + s2);
     T dvL = vN - v1, dvR = v2 - vN;
     T aL = fabs(dvL) - q0 * fabs(dv0), aR = fabs(dvR) - q1 * fabs(dv2);
-    Ql = vN - s1 * (T(0) > aL ? T(0) : aL);
-    Qr = vN + s1 * (T(0) > aR ? T(0) : aR);
+    Ql = vN - s1 * lmax(T(0), aL);
+    Qr = vN + s1 * lmax(T(0), aR);
 }
 // PDM (recon.F90:275-301)
 template <typename T>
 __device__ __forceinline__ T PDM(T pdmb, T q0, T q1, T q2, T qI) {
-    T maxQ = q1 > q2 ? q1 : q2, minQ = q1 < q2 ? q1 : q2;
-    T c = qI < maxQ ? qI : maxQ;
-    T qN = minQ > c ? minQ : c;
+    T maxQ = lmax(q1, q2), minQ = lmin(q1, q2);
+    T c = lmin(qI, maxQ);
+    T qN = lmax(minQ, c);
     T dq0 = pdmb * (q1 - q0), dq1 = pdmb * (q2 - q1);
     T s0 = copysign(T(1), dq0), s1 = copysign(T(1), dq1);
     T s01 = fabs(s0 + s1);
     T dqL = qN - q1;
     T a = fabs(dqL) - s01 * fabs(dq0);
-    return qN - s1 * (T(0) > a ? T(0) : a);
+    return qN - s1 * lmax(T(0), a);
 }
 
 // GetLRs on one interface: dV[8] volumes, Q[8] values (stencil cells f-4..f+3), nQ[4] limiter values
