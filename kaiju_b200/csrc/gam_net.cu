@@ -90,8 +90,11 @@ __global__ void __launch_bounds__(160) k_conv(ConvArgs a) {
     __shared__ __align__(8) uint64_t full[S::NS], empty[S::NS], tfull[2], tempty[2], wready;
     __shared__ uint32_t tmemBase;
     __shared__ int failed;
+    __shared__ float sBias[32];
     const int tid = threadIdx.x, warp = tid >> 5;
 
+    // the bias, once per CTA: the epilogue reads it from shared memory instead of 32 global loads per tile
+    if (tid < 32) sBias[tid] = (MODE != MODE_BWD && tid < a.cout) ? a.bias[tid] : 0.f;
     if (tid == 0) {
         for (int q = 0; q < S::NS; ++q) { tc::mbar_init(&full[q], 128); tc::mbar_init(&empty[q], 1); }
         for (int q = 0; q < 2; ++q) { tc::mbar_init(&tfull[q], 1); tc::mbar_init(&tempty[q], 128); }
@@ -123,7 +126,7 @@ __global__ void __launch_bounds__(160) k_conv(ConvArgs a) {
             if (MODE == MODE_OUT) {
 #pragma unroll
                 for (int co = 0; co < 32; ++co)
-                    if (co < a.cout) a.yf[(long long)co * a.E + cell] = v[co] + a.bias[co];
+                    if (co < a.cout) a.yf[(long long)co * a.E + cell] = v[co] + sBias[co];
                 return true;
             }
             uint32_t py[16], pz[16];
@@ -144,8 +147,8 @@ __global__ void __launch_bounds__(160) k_conv(ConvArgs a) {
 #pragma unroll
                 for (int q = 0; q < 16; ++q) {
                     const int c0 = 2 * q, c1 = 2 * q + 1;
-                    const float z0 = c0 < a.cout ? v[c0] + a.bias[c0] : 0.f;
-                    const float z1 = c1 < a.cout ? v[c1] + a.bias[c1] : 0.f;
+                    const float z0 = c0 < a.cout ? v[c0] + sBias[c0] : 0.f;
+                    const float z1 = c1 < a.cout ? v[c1] + sBias[c1] : 0.f;
                     pz[q] = pack2(z0, z1);
                     py[q] = pack2(gelu(z0), gelu(z1));
                 }
