@@ -129,31 +129,36 @@ NormP norm_of(const gam_closure* C) {
 }
 
 // the net's input from a state: normalised rho, v, P, B of every cell (ghosts included), channels-last
+// launched over (i, j) planes (gam_kern.cuh reg_plane); the 8 channels of a cell go out as one 16-byte store
 __global__ void k_closure_input(Lay L, double gamma, StateP s, NormP n, __nv_bfloat16* in) {
-    const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-    if (t >= (long long)L.Ni * L.Nj * L.Nk) return;
-    const int i = (int)(t % L.Ni), j = (int)((t / L.Ni) % L.Nj), k = (int)(t / ((long long)L.Ni * L.Nj));
+    int i, j, k;
+    if (!reg_plane(Reg{0, L.Ni, 0, L.Nj, 0, L.Nk}, i, j, k)) return;
     const long long c = L.at(i, j, k);
     const double rho = s.gas[0][c];
     const double vx = s.gas[1][c] / rho, vy = s.gas[2][c] / rho, vz = s.gas[3][c] / rho;
     const double P = (gamma - 1.0) * (s.gas[4][c] - 0.5 * rho * (vx * vx + vy * vy + vz * vz));
     const double w[8] = {rho, vx, vy, vz, P, s.b[0][c], s.b[1][c], s.b[2][c]};
+    float f[8];
 #pragma unroll
     for (int q = 0; q < 8; ++q) {
-        float f = (float)((w[q] - n.inMean[q]) / n.inScale[q]);
-        if (!(f == f) || fabsf(f) > 1e4f) f = 0.f;   // keep the net's input finite
-        in[c * NET_IN_PITCH + q] = __float2bfloat16_rn(f);
+        f[q] = (float)((w[q] - n.inMean[q]) / n.inScale[q]);
+        if (!(f[q] == f[q]) || fabsf(f[q]) > 1e4f) f[q] = 0.f;   // keep the net's input finite
     }
+    uint32_t pk[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        __nv_bfloat162 h2 = __floats2bfloat162_rn(f[2 * q], f[2 * q + 1]);   // channel 2q at the lower address
+        pk[q] = *reinterpret_cast<uint32_t*>(&h2);
+    }
+    *reinterpret_cast<uint4*>(in + c * NET_IN_PITCH) = make_uint4(pk[0], pk[1], pk[2], pk[3]);
 }
 
 // face corrections (area-scaled): plane d*8+v at the index of the lower d-face of the owner cell, for the
 // faces of the active cells and the upper boundary faces. A boundary face of a non-periodic direction gets
 // none; across a periodic one the upper boundary face repeats the lower boundary face.
 __global__ void k_closure_corr(Lay L, const float* out, NormP n, const float* geom, float* corr) {
-    const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-    const int ni = L.Nip + 1, nj = L.Njp + 1, nk = L.Nkp + 1;
-    if (t >= (long long)ni * nj * nk) return;
-    const int i = L.is() + (int)(t % ni), j = L.js() + (int)((t / ni) % nj), k = L.ks() + (int)(t / ((long long)ni * nj));
+    int i, j, k;
+    if (!reg_plane(Reg{L.is(), L.Nip + 1, L.js(), L.Njp + 1, L.ks(), L.Nkp + 1}, i, j, k)) return;
     const long long c = L.at(i, j, k);
     const int idx[3] = {i, j, k};
     const int lo[3] = {L.is(), L.js(), L.ks()}, hi[3] = {L.ie(), L.je(), L.ke()};
@@ -744,10 +749,10 @@ const float* closure_enqueue_corr(Handle& h, const StateP& nS, cudaStream_t st) 
     const Lay& L = h.L;
     NormP n = norm_of(C);
     C->nb.act[0] = C->act0;
-    k_closure_input<<<nblk256((long long)L.Ni * L.Nj * L.Nk), 256, 0, st>>>(L, h.p.gamma, nS, n, C->act0);
+    k_closure_input<<<grid_plane(Reg{0, L.Ni, 0, L.Nj, 0, L.Nk}, 256), 256, 0, st>>>(L, h.p.gamma, nS, n, C->act0);
     net_forward(C->box, C->wfwd, C->params, C->nb, false, C->err, st);
-    const long long nf = (long long)(L.Nip + 1) * (L.Njp + 1) * (L.Nkp + 1);
-    k_closure_corr<<<nblk256(nf), 256, 0, st>>>(L, C->nb.out, n, C->geom, C->corr);
+    k_closure_corr<<<grid_plane(Reg{L.is(), L.Nip + 1, L.js(), L.Njp + 1, L.ks(), L.Nkp + 1}, 256), 256, 0, st>>>(
+        L, C->nb.out, n, C->geom, C->corr);
     h.launches += 2 + NET_LAYERS;
     return C->corr;
 }
@@ -840,8 +845,8 @@ int gam_closure_capture(gam_closure_t* C, int slot, gam_gpu_t* coarse, gam_gpu_t
     if (rc) return rc;
     const Lay& L = hc.L;
     NormP n = norm_of(C);
-    k_closure_input<<<nblk256((long long)L.Ni * L.Nj * L.Nk), 256, 0, hc.stream>>>(L, hc.p.gamma, hc.S[hc.cur], n,
-                                                                                  C->sIn[slot]);
+    k_closure_input<<<grid_plane(Reg{0, L.Ni, 0, L.Nj, 0, L.Nk}, 256), 256, 0, hc.stream>>>(L, hc.p.gamma,
+                                                                                           hc.S[hc.cur], n, C->sIn[slot]);
     rc = capi_download_scalars(coarse);
     if (rc) return rc;
     C->sDt[slot] = hc.hScal->dt;
@@ -920,14 +925,14 @@ static int closure_sample_pass(gam_closure* C, int slot, bool train, float lr) {
     NormP n = norm_of(C);
     C->nb.act[0] = C->sIn[slot];
     if (net_forward(C->box, C->wfwd, C->params, C->nb, train, C->err, C->stream) != 0) return GAM_ERR_CUDA;
-    const long long nf = (long long)(L.Nip + 1) * (L.Njp + 1) * (L.Nkp + 1);
     const int nb = 1024;
     if (C->lossMode == GAM_CLOSURE_LOSS_FACE) {
         k_loss_face<<<nb, 256, 0, C->stream>>>(L, C->nb.out, C->sFace[slot], C->geom, n,
                                                train ? C->nb.grad[NET_LAYERS - 1] : nullptr, C->lossPart);
         k_loss_sum<<<1, 32, 0, C->stream>>>(C->lossPart, nb, C->lossAcc);
     } else {
-        k_closure_corr<<<nblk256(nf), 256, 0, C->stream>>>(L, C->nb.out, n, C->geom, C->corr);
+        k_closure_corr<<<grid_plane(Reg{L.is(), L.Nip + 1, L.js(), L.Njp + 1, L.ks(), L.Nkp + 1}, 256), 256, 0,
+                         C->stream>>>(L, C->nb.out, n, C->geom, C->corr);
         k_loss_w<<<nb, 256, 0, C->stream>>>(L, C->corr, C->sRes[slot], C->geom, n, C->sDt[slot], C->wts, C->lossPart);
         k_loss_sum<<<1, 32, 0, C->stream>>>(C->lossPart, nb, C->lossAcc);
     }
