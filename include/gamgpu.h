@@ -23,7 +23,7 @@ extern "C" {
 #define GAM_ERR_DT_COLLAPSE 2  /* CalcDT's isDisaster / isBad (src/gamera/step.F90:103-135)      */
 #define GAM_ERR_CUDA 3         /* a CUDA call failed; the handle should be destroyed              */
 #define GAM_ERR_TIMEOUT 4      /* a bounded device wait gave up                                   */
-#define GAM_ERR_UNSUPPORTED 5  /* a Model option this build does not run on the device           */
+#define GAM_ERR_UNSUPPORTED 5  /* a Model option this library does not run on the device         */
 #define GAM_ERR_ARG 6          /* bad argument (null pointer, size, name)                          */
 
 /* precision modes (gam_gpu_set_precision) */

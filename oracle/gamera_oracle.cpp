@@ -1,7 +1,7 @@
 // CPU FP64 restatement of the GAMERA ideal-MHD step (kaiju v1.25.1) -- TEST INFRASTRUCTURE ONLY.
 //
-// This file is the oracle: the parity tests, the smoke check and the bench's CPU-baseline leg call it
-// as the checker. The product path (kaiju_b200/csrc, libgamgpu.so) never links or calls it.
+// This file is the oracle: the parity tests, the smoke check and the bench's CPU-baseline leg check the
+// device results against it. The product path (kaiju_b200/csrc, libgamgpu.so) never links or calls it.
 //
 // It restates, routine by routine and in the Fortran evaluation order, the reference's
 //   src/gamera/mhdgroup.F90   AdvanceMHD :16-76, applyUpdate :79-259, CellReynolds :263-297,

@@ -1,7 +1,7 @@
 """ctypes front end of the CPU oracle (oracle/gamera_oracle.cpp) -- test infrastructure only.
 
 Only the tests, ``__graft_entry__.smoke()`` and the CPU-baseline leg of ``bench.py`` use this module,
-as the checker; the product path never imports it.
+to check the device results against; the product path never imports it.
 
 Arrays come back in the reference's Fortran layout (column-major, ghosts included), reshaped to numpy
 arrays indexed ``[i, j, k, var]`` with ``order='F'`` and zero-based offsets from ``isg``.
